@@ -1,0 +1,218 @@
+/*
+ * nnkifmm.h -- C ABI of the B200 KIFMM / mobility library (libnnkifmm.so).
+ *
+ * Drop-in for the Stokes-NNKIFMM MATLAB path
+ *   OcTree(...)                      Classes/OcTree.m:77-129
+ *   nearestMatrix(...)               Tools/Nearest/nearestMatrix.m:17-41
+ *   KIFMM(tree,[eps mu],...)         Classes/KIFMM.m:46-61
+ *   KIFMM.computeVel                 Classes/KIFMM.m:63-105
+ *   KIFMM.computeVelSparse           Classes/KIFMM.m:107-155
+ *   KIFMM.reducedComputeVel          Classes/KIFMM.m:157-198
+ *   KIFMM.reducedSolve               Classes/KIFMM.m:200-242
+ *   gmres(@(x) fmm.computeVel(x),..) Data Generation/DirectMethodComparison.m:28
+ *   mobilityProblem(...)             Mobility/mobilityProblem.m:1-72
+ *
+ * Conventions
+ *   - Every function returns an int status (NNK_OK = 0).  No C++ exception
+ *     crosses the ABI.  nnk_last_error() gives a message for the last failure
+ *     on a context.
+ *   - Points are row-major (n,3) FP64 arrays [x0 y0 z0 x1 y1 z1 ...].
+ *   - Node ids, list entries and pointIndex are exported as the reference's
+ *     1-based node ids (DFS block numbering, OcTree.m:174-175).
+ *   - Vector layouts (KIFMM.m:83-103): NNK_LAYOUT_ROWS = (N,3) row-major,
+ *     which is also the 'GMRES',1,'format',1 interleaved vector;
+ *     NNK_LAYOUT_BLOCKED = 'format',2 [x1..xN y1..yN z1..zN].
+ *   - Buffers are owned by the caller.  on_device = 0: host pointers;
+ *     on_device = 1: device pointers on the context's device.
+ *   - A handle is used by one thread at a time.  Work is issued on the
+ *     context's CUDA stream (nnk_ctx_set_stream).
+ */
+#ifndef NNKIFMM_H
+#define NNKIFMM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NNK_OK 0
+#define NNK_E_ARG 1        /* bad argument or unsupported combination          */
+#define NNK_E_MAXDEPTH 2   /* OcTree.m:168-170 'Max level reached'              */
+#define NNK_E_NONFINITE 3  /* NaN/Inf in input or result                        */
+#define NNK_E_NOCONV 4     /* GMRES stopped at maxit above tol                  */
+#define NNK_E_OOM 5        /* device or host allocation failed                  */
+#define NNK_E_CUDA 6       /* CUDA runtime error (message in nnk_last_error)    */
+#define NNK_E_TIMEOUT 7    /* a bounded device wait gave up                     */
+#define NNK_E_STATE 8      /* call out of order / object not ready              */
+
+#define NNK_LAYOUT_ROWS 1
+#define NNK_LAYOUT_BLOCKED 2
+
+#define NNK_PREC_FP64 0    /* every FMM step in FP64                            */
+#define NNK_PREC_MIXED 1   /* FP32 pair kernels, tensor-core M2L, FP64 C2E ops   */
+
+typedef struct nnk_ctx nnk_ctx;
+typedef struct nnk_tree nnk_tree;
+typedef struct nnk_fmm nnk_fmm;
+typedef struct nnk_mob nnk_mob;
+
+/* OcTree name-value options (OcTree.m:86-95). */
+typedef struct nnk_tree_params {
+  int32_t node_capacity; /* 'nodeCapacity' (default 200)                      */
+  int32_t max_depth;     /* 'maxDepth' (default 21; at most 23 here)           */
+  int32_t nearest;       /* 'nearest' 0/1                                      */
+  int32_t reserved;
+} nnk_tree_params;
+
+typedef struct nnk_tree_info {
+  int64_t num_points;     /* unique points (OcTree.m:80)                        */
+  int64_t num_potentials; /* sum(tree.potentials)                               */
+  int64_t num_targets;    /* sum(tree.targets)                                  */
+  int64_t num_fine;       /* Q (NEAREST)                                        */
+  int64_t nn_nnz;         /* nonzeros of NN (NEAREST)                           */
+  int64_t source_entries; /* leaf source entries (fine points per leaf, NEAREST;
+                             potential points otherwise)                        */
+  int64_t u_total, v_total, w_total, x_total; /* list lengths summed over nodes */
+  int32_t node_count;     /* tree.nodeCount                                     */
+  int32_t max_level;      /* max(tree.nodeLevel)                                */
+  int32_t node_capacity;  /* min(nodeCapacity, numPts-1) (OcTree.m:105)         */
+  int32_t nearest;
+} nnk_tree_info;
+
+/* KIFMM name-value options (KIFMM.m:50-60) plus the precision mode. */
+typedef struct nnk_fmm_params {
+  double eps;            /* kernelPar(1)                                       */
+  double mu;             /* kernelPar(2)                                       */
+  int32_t corona_res;    /* 'coronaRes' (default 6)                            */
+  int32_t corona_shells; /* 'coronaShells' (default 1)                         */
+  int32_t precision;     /* NNK_PREC_FP64 or NNK_PREC_MIXED                    */
+  int32_t reserved;
+  double reg;            /* relative Tikhonov weight of the check-to-equivalent
+                            pseudo-inverse in NNK_PREC_MIXED (0 = default)      */
+} nnk_fmm_params;
+
+/* Algorithmic work of one matvec, from the tree statistics (for rooflines). */
+typedef struct nnk_fmm_stats {
+  int64_t pairs_leaf;   /* U-list P2P + W-list M2T + L2T target-source pairs   */
+  int64_t pairs_p2p;    /* U-list P2P pairs only                               */
+  int64_t pairs_up;     /* S2M + M2M pairs                                     */
+  int64_t pairs_down;   /* M2L + P2L + L2L pairs (pair-kernel form)            */
+  int64_t m2l_pairs;    /* V-list (target node, source node) pairs             */
+  int64_t c2e_columns;  /* check-to-equivalent applications (up + down)        */
+  int32_t surface_points;
+  int32_t levels;
+} nnk_fmm_stats;
+
+/* GMRES options/result (MATLAB gmres(A,b,restart,tol,maxit), x0 = 0). */
+typedef struct nnk_solve_params {
+  double tol;       /* relative residual ||b-Ax||/||b|| (default 1e-6)        */
+  int32_t maxit;    /* total inner iterations                                 */
+  int32_t restart;  /* 0 = unrestarted (restart = [])                         */
+} nnk_solve_params;
+
+typedef struct nnk_solve_info {
+  int32_t flag;     /* 0 converged, 1 maxit reached                           */
+  int32_t iters;    /* inner iterations used                                  */
+  double relres;    /* true relative residual at exit                         */
+} nnk_solve_info;
+
+/* ------------------------------------------------------------ context -- */
+int nnk_ctx_create(int32_t device, nnk_ctx** out);
+int nnk_ctx_destroy(nnk_ctx* ctx);
+/* Use this stream (a cudaStream_t) for all later work on the context. */
+int nnk_ctx_set_stream(nnk_ctx* ctx, void* stream);
+int nnk_ctx_synchronize(nnk_ctx* ctx);
+const char* nnk_last_error(const nnk_ctx* ctx);
+/* Library version string, e.g. "nnkifmm 0.1 sm_100a". */
+const char* nnk_version(void);
+
+/* ------------------------------------------------- nearest neighbours -- */
+/* nearestMatrix(coarse,fine) (nearestMatrix.m:17-41): FP64 d2 = (dx^2+dy^2)+dz^2,
+ * ties share 1/k.  Returns CSR by fine point: *nnz is set; if rowptr is NULL
+ * only the count is returned, else rowptr (q+1), col (0-based coarse index)
+ * and val (weights) are filled. */
+int nnk_nearest_matrix(nnk_ctx* ctx, const double* coarse, int64_t n,
+                       const double* fine, int64_t q, int64_t* nnz,
+                       int64_t* rowptr, int32_t* col, double* val);
+
+/* --------------------------------------------------------------- tree -- */
+/* OcTree(potPoints, targetPoints, ...) (OcTree.m:77-129).
+ * NEAREST: fine (q,3) and the NN CSR (rowptr q+1, 0-based col into potPoints,
+ * val).  If nn_rowptr is NULL and params->nearest, NN is built as
+ * nnk_nearest_matrix(potPoints, fine).  NEAREST requires targetPoints ==
+ * potPoints (the reference gathers NEAREST sources by pointIndex over all
+ * points, downwardPass.m:92,221).  Returns NNK_E_MAXDEPTH with the
+ * reference message when any node reaches level maxDepth-1. */
+int nnk_tree_build(nnk_ctx* ctx, const double* pot, int64_t n_pot,
+                   const double* tgt, int64_t n_tgt, const double* fine,
+                   int64_t q, const int64_t* nn_rowptr, const int32_t* nn_col,
+                   const double* nn_val, const nnk_tree_params* params,
+                   nnk_tree** out);
+int nnk_tree_info_get(const nnk_tree* tree, nnk_tree_info* info);
+/* nodeLevel, nodeParents (0 for the root), nodeChildren (8 per node, 0 for
+ * leaves), nodeCorners (6 per node) and pointIndex (per unique point).
+ * Any pointer may be NULL. */
+int nnk_tree_export_nodes(const nnk_tree* tree, int32_t* level,
+                          int32_t* parent, int32_t* children, double* corners,
+                          int32_t* point_index);
+/* potentials / targets masks (OcTree.m:81-82) and the unique points (n,3). */
+int nnk_tree_export_points(const nnk_tree* tree, double* points,
+                           uint8_t* potentials, uint8_t* targets);
+/* tree.interactions{:,k}, k = 0 U, 1 V, 2 W, 3 X: offsets (nodeCount+1, by
+ * reference node id - 1) and 1-based ids in the reference's order. */
+int nnk_tree_export_list(const nnk_tree* tree, int32_t which, int64_t* offsets,
+                         int32_t* ids);
+int nnk_tree_destroy(nnk_tree* tree);
+
+/* ---------------------------------------------------------------- FMM -- */
+/* KIFMM(tree,[eps mu],...).  The tree must outlive the FMM. */
+int nnk_fmm_create(nnk_ctx* ctx, const nnk_tree* tree,
+                   const nnk_fmm_params* params, nnk_fmm** out);
+/* computeVel: in = potentials (num_potentials x 3), out = velocities
+ * (num_targets x 3), in the given layout, nrhs right-hand sides stored one
+ * after another. */
+int nnk_fmm_apply(nnk_fmm* fmm, const double* in, double* out, int32_t layout,
+                  int32_t nrhs, int32_t on_device);
+/* computeVelSparse: the same with coronaRes 4 (KIFMM.m:136-145). */
+int nnk_fmm_apply_sparse(nnk_fmm* fmm, const double* in, double* out,
+                         int32_t layout, int32_t nrhs, int32_t on_device);
+/* reducedComputeVel (reducedPass.m) and reducedSolve (ReducedSolve.m). */
+int nnk_fmm_reduced_apply(nnk_fmm* fmm, const double* in, double* out,
+                          int32_t layout, int32_t on_device);
+int nnk_fmm_reduced_solve(nnk_fmm* fmm, const double* in, double* out,
+                          int32_t layout, int32_t on_device);
+int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats);
+int nnk_fmm_destroy(nnk_fmm* fmm);
+
+/* Device GMRES on the FMM operator: solves computeVel(x) = b, the resistance
+ * solve of DirectMethodComparison.m:28 / Rigid_Resistance.m:23. */
+int nnk_fmm_solve(nnk_fmm* fmm, const double* b, double* x, int32_t layout,
+                  const nnk_solve_params* sp, nnk_solve_info* info,
+                  int32_t on_device);
+
+/* ----------------------------------------------------------- mobility -- */
+/* Rigid bodies (Swimmers.m) on one NEAREST tree: body b owns force points
+ * [body_start[b], body_start[b+1]) of the tree's points and fine points
+ * [fine_start[b], fine_start[b+1]); points after body_start[nb] are boundary
+ * points (no rigid unknowns).  rel_points / rel_fine are the rotated,
+ * untranslated positions (Swimmers.m:177-189) used for torques. */
+int nnk_mob_create(nnk_fmm* fmm, int32_t nbodies, const int64_t* body_start,
+                   const int64_t* fine_start, const double* rel_points,
+                   const double* rel_fine, nnk_mob** out);
+/* Mobility matvec (mobilityMatrixMulti.m:17-36) on [f (3N blocked); U; Omega]. */
+int nnk_mob_apply(nnk_mob* mob, const double* x, double* y, int32_t on_device);
+/* Block preconditioner (MobilityPrecon.m:17-40). */
+int nnk_mob_precon(nnk_mob* mob, const double* x, double* y, int32_t on_device);
+/* gmres(afunc, rhs, [], tol, maxit) with optional right preconditioning
+ * (mobilityProblem.m:48-58); x receives the (preconditioned-back) solution. */
+int nnk_mob_solve(nnk_mob* mob, const double* rhs, double* x,
+                  const nnk_solve_params* sp, int32_t precondition,
+                  nnk_solve_info* info, int32_t on_device);
+int nnk_mob_destroy(nnk_mob* mob);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NNKIFMM_H */

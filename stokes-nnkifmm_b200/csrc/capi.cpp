@@ -1,0 +1,377 @@
+// extern "C" entry points of libnnkifmm.so (declared in include/nnkifmm.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <new>
+
+#include "../../include/nnkifmm.h"
+#include "common.h"
+#include "fmm.h"
+#include "gmres.h"
+#include "mobility.h"
+#include "tree.h"
+
+struct nnk_tree {
+  nnk_ctx* ctx;
+  nnk::HostTree t;
+};
+struct nnk_fmm {
+  nnk_ctx* ctx;
+  const nnk_tree* tree;
+  std::unique_ptr<nnk::Fmm> f;
+};
+struct nnk_mob {
+  nnk_fmm* fmm;
+  std::unique_ptr<nnk::Mobility> m;
+};
+
+namespace {
+
+int fail(nnk_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return code;
+}
+
+#define API_TRY try {
+#define API_CATCH(ctx)                                                       \
+  }                                                                          \
+  catch (const nnk::Error& e) { return fail(ctx, e.code, e.what()); }        \
+  catch (const std::bad_alloc&) { return fail(ctx, NNK_E_OOM, "out of host memory"); } \
+  catch (const std::exception& e) { return fail(ctx, NNK_E_ARG, e.what()); } \
+  return NNK_OK;
+
+void need_gpu(nnk_ctx* ctx) {
+  if (!ctx->has_gpu) throw nnk::Error(NNK_E_CUDA, "no CUDA device available: the FMM runs only on the GPU");
+  NNK_CUDA(cudaSetDevice(ctx->device));
+}
+
+// Copies a host or device input to device memory owned by `buf` if needed.
+const double* stage_in(nnk_ctx* ctx, nnk::DBuf<double>& buf, const double* p, size_t count, int on_device) {
+  if (on_device) return p;
+  if (buf.n < count) buf.alloc(count);
+  if (count)
+    NNK_CUDA(cudaMemcpyAsync(buf.p, p, count * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  return buf.p;
+}
+double* stage_out(nnk::DBuf<double>& buf, double* p, size_t count, int on_device) {
+  if (on_device) return p;
+  if (buf.n < count) buf.alloc(count);
+  return buf.p;
+}
+void finish_out(nnk_ctx* ctx, nnk::DBuf<double>& buf, double* p, size_t count, int on_device) {
+  if (!on_device && count)
+    NNK_CUDA(cudaMemcpyAsync(p, buf.p, count * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (!on_device) NNK_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* nnk_version(void) { return "nnkifmm 0.1 sm_100a"; }
+
+int nnk_ctx_create(int32_t device, nnk_ctx** out) {
+  if (!out) return NNK_E_ARG;
+  nnk_ctx* c = new (std::nothrow) nnk_ctx();
+  if (!c) return NNK_E_OOM;
+  c->device = device;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) == cudaSuccess && device >= 0 && device < count &&
+      cudaSetDevice(device) == cudaSuccess) {
+    c->has_gpu = true;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      return NNK_E_CUDA;
+    }
+    c->own_stream = true;
+  } else {
+    cudaGetLastError();  // clear the sticky "no device" error
+    c->has_gpu = false;
+  }
+  *out = c;
+  return NNK_OK;
+}
+
+int nnk_ctx_destroy(nnk_ctx* ctx) {
+  if (!ctx) return NNK_E_ARG;
+  if (ctx->has_gpu && ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return NNK_OK;
+}
+
+int nnk_ctx_set_stream(nnk_ctx* ctx, void* stream) {
+  if (!ctx) return NNK_E_ARG;
+  API_TRY
+  need_gpu(ctx);
+  if (ctx->own_stream && ctx->stream) NNK_CUDA(cudaStreamDestroy(ctx->stream));
+  ctx->stream = (cudaStream_t)stream;
+  ctx->own_stream = false;
+  API_CATCH(ctx)
+}
+
+int nnk_ctx_synchronize(nnk_ctx* ctx) {
+  if (!ctx) return NNK_E_ARG;
+  API_TRY
+  need_gpu(ctx);
+  NNK_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_CATCH(ctx)
+}
+
+const char* nnk_last_error(const nnk_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int nnk_nearest_matrix(nnk_ctx* ctx, const double* coarse, int64_t n, const double* fine, int64_t q,
+                       int64_t* nnz, int64_t* rowptr, int32_t* col, double* val) {
+  if (!ctx || !nnz || n < 0 || q < 0 || (n && !coarse) || (q && !fine)) return fail(ctx, NNK_E_ARG, "bad arguments");
+  API_TRY
+  std::vector<int64_t> rp;
+  std::vector<int32_t> cl;
+  std::vector<double> vl;
+  nnk::nearest_matrix(coarse, n, fine, q, rp, cl, vl);
+  *nnz = rp.empty() ? 0 : rp.back();
+  if (rowptr) {
+    std::memcpy(rowptr, rp.data(), rp.size() * sizeof(int64_t));
+    if (col) std::memcpy(col, cl.data(), cl.size() * sizeof(int32_t));
+    if (val) std::memcpy(val, vl.data(), vl.size() * sizeof(double));
+  }
+  API_CATCH(ctx)
+}
+
+int nnk_tree_build(nnk_ctx* ctx, const double* pot, int64_t n_pot, const double* tgt, int64_t n_tgt,
+                   const double* fine, int64_t q, const int64_t* nn_rowptr, const int32_t* nn_col,
+                   const double* nn_val, const nnk_tree_params* params, nnk_tree** out) {
+  if (!ctx || !out) return NNK_E_ARG;
+  API_TRY
+  nnk::TreeParams p;
+  if (params) {
+    p.node_capacity = params->node_capacity;
+    p.max_depth = params->max_depth;
+    p.nearest = params->nearest;
+  }
+  std::unique_ptr<nnk_tree> t(new nnk_tree());
+  t->ctx = ctx;
+  std::string msg;
+  const int rc = nnk::build_tree(pot, n_pot, tgt, n_tgt, fine, q, nn_rowptr, nn_col, nn_val, p, t->t, msg);
+  if (rc != NNK_OK) return fail(ctx, rc, msg);
+  *out = t.release();
+  API_CATCH(ctx)
+}
+
+int nnk_tree_info_get(const nnk_tree* tree, nnk_tree_info* info) {
+  if (!tree || !info) return NNK_E_ARG;
+  const nnk::HostTree& t = tree->t;
+  std::memset(info, 0, sizeof(*info));
+  info->num_points = t.n;
+  info->num_potentials = t.n_pot;
+  info->num_targets = t.n_tgt;
+  info->num_fine = t.q;
+  info->nn_nnz = t.nn_rowptr.empty() ? 0 : t.nn_rowptr.back();
+  info->source_entries = t.src_start.empty() ? 0 : t.src_start.back();
+  info->u_total = (int64_t)t.U.idx.size();
+  info->v_total = (int64_t)t.V.idx.size();
+  info->w_total = (int64_t)t.W.idx.size();
+  info->x_total = (int64_t)t.X.idx.size();
+  info->node_count = t.nodes;
+  info->max_level = t.max_level;
+  info->node_capacity = t.capacity;
+  info->nearest = t.params.nearest;
+  return NNK_OK;
+}
+
+int nnk_tree_export_nodes(const nnk_tree* tree, int32_t* level, int32_t* parent, int32_t* children,
+                          double* corners, int32_t* point_index) {
+  if (!tree) return NNK_E_ARG;
+  const nnk::HostTree& t = tree->t;
+  for (int32_t i = 0; i < t.nodes; ++i) {
+    if (level) level[i] = t.level[i];
+    if (parent) parent[i] = t.parent[i] + 1;  // root parent 0 (OcTree.m:102)
+    if (children)
+      for (int k = 0; k < 8; ++k) children[8 * i + k] = t.child0[i] < 0 ? 0 : t.child0[i] + k + 1;
+    if (corners) std::memcpy(corners + 6 * i, &t.corners[6 * i], 6 * sizeof(double));
+  }
+  if (point_index)
+    for (int64_t k = 0; k < t.n; ++k) point_index[k] = t.point_index[k] + 1;
+  return NNK_OK;
+}
+
+int nnk_tree_export_points(const nnk_tree* tree, double* points, uint8_t* potentials, uint8_t* targets) {
+  if (!tree) return NNK_E_ARG;
+  const nnk::HostTree& t = tree->t;
+  if (points) std::memcpy(points, t.pts.data(), t.pts.size() * sizeof(double));
+  if (potentials) std::memcpy(potentials, t.is_pot.data(), t.is_pot.size());
+  if (targets) std::memcpy(targets, t.is_tgt.data(), t.is_tgt.size());
+  return NNK_OK;
+}
+
+int nnk_tree_export_list(const nnk_tree* tree, int32_t which, int64_t* offsets, int32_t* ids) {
+  if (!tree || which < 0 || which > 3) return NNK_E_ARG;
+  const nnk::HostTree& t = tree->t;
+  const nnk::Csr& L = which == 0 ? t.U : which == 1 ? t.V : which == 2 ? t.W : t.X;
+  if (offsets) std::memcpy(offsets, L.off.data(), L.off.size() * sizeof(int64_t));
+  if (ids)
+    for (size_t k = 0; k < L.idx.size(); ++k) ids[k] = L.idx[k] + 1;
+  return NNK_OK;
+}
+
+int nnk_tree_destroy(nnk_tree* tree) {
+  delete tree;
+  return NNK_OK;
+}
+
+int nnk_fmm_create(nnk_ctx* ctx, const nnk_tree* tree, const nnk_fmm_params* params, nnk_fmm** out) {
+  if (!ctx || !tree || !params || !out) return NNK_E_ARG;
+  API_TRY
+  need_gpu(ctx);
+  nnk::FmmParams p;
+  p.eps = params->eps;
+  p.mu = params->mu;
+  p.res = params->corona_res ? params->corona_res : 6;
+  p.shells = params->corona_shells ? params->corona_shells : 1;
+  p.precision = params->precision;
+  p.reg = params->reg;
+  if (p.precision != NNK_PREC_FP64 && p.precision != NNK_PREC_MIXED)
+    return fail(ctx, NNK_E_ARG, "unknown precision mode");
+  std::unique_ptr<nnk_fmm> f(new nnk_fmm());
+  f->ctx = ctx;
+  f->tree = tree;
+  f->f.reset(new nnk::Fmm(ctx, &tree->t, p));
+  *out = f.release();
+  API_CATCH(ctx)
+}
+
+static int fmm_apply_common(nnk_fmm* fmm, const double* in, double* out, int32_t layout, int32_t nrhs,
+                            int32_t on_device, int which) {
+  if (!fmm || !in || !out || nrhs < 1 || (layout != NNK_LAYOUT_ROWS && layout != NNK_LAYOUT_BLOCKED))
+    return fail(fmm ? fmm->ctx : nullptr, NNK_E_ARG, "bad arguments");
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Fmm& F = *fmm->f;
+  const nnk::HostTree& t = F.tree();
+  const size_t nin = (size_t)nrhs * 3 * (which >= 2 ? t.n_tgt : t.n_pot);
+  const size_t nout = (size_t)nrhs * 3 * t.n_tgt;
+  const double* din = stage_in(ctx, F.io_in, in, nin, on_device);
+  double* dout = stage_out(F.io_out, out, nout, on_device);
+  if (which == 0) F.apply(din, dout, layout, nrhs);
+  else if (which == 1) F.sparse().apply(din, dout, layout, nrhs);
+  else if (which == 2) F.reduced_apply(din, dout, layout);
+  else F.reduced_solve(din, dout, layout);
+  finish_out(ctx, F.io_out, out, nout, on_device);
+  API_CATCH(ctx)
+}
+
+int nnk_fmm_apply(nnk_fmm* fmm, const double* in, double* out, int32_t layout, int32_t nrhs,
+                  int32_t on_device) {
+  return fmm_apply_common(fmm, in, out, layout, nrhs, on_device, 0);
+}
+int nnk_fmm_apply_sparse(nnk_fmm* fmm, const double* in, double* out, int32_t layout, int32_t nrhs,
+                         int32_t on_device) {
+  return fmm_apply_common(fmm, in, out, layout, nrhs, on_device, 1);
+}
+int nnk_fmm_reduced_apply(nnk_fmm* fmm, const double* in, double* out, int32_t layout, int32_t on_device) {
+  return fmm_apply_common(fmm, in, out, layout, 1, on_device, 2);
+}
+int nnk_fmm_reduced_solve(nnk_fmm* fmm, const double* in, double* out, int32_t layout, int32_t on_device) {
+  return fmm_apply_common(fmm, in, out, layout, 1, on_device, 3);
+}
+
+int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats) {
+  if (!fmm || !stats) return NNK_E_ARG;
+  *stats = fmm->f->stats();
+  return NNK_OK;
+}
+
+int nnk_fmm_destroy(nnk_fmm* fmm) {
+  if (!fmm) return NNK_E_ARG;
+  if (fmm->ctx && fmm->ctx->has_gpu) cudaSetDevice(fmm->ctx->device);
+  delete fmm;
+  return NNK_OK;
+}
+
+int nnk_fmm_solve(nnk_fmm* fmm, const double* b, double* x, int32_t layout, const nnk_solve_params* sp,
+                  nnk_solve_info* info, int32_t on_device) {
+  if (!fmm || !b || !x || !sp) return fail(fmm ? fmm->ctx : nullptr, NNK_E_ARG, "bad arguments");
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Fmm& F = *fmm->f;
+  const nnk::HostTree& t = F.tree();
+  if (t.n_pot != t.n_tgt) return fail(ctx, NNK_E_ARG, "solve needs potentials == targets");
+  const size_t n = 3 * (size_t)t.n_tgt;
+  const double* db = stage_in(ctx, F.io_in, b, n, on_device);
+  double* dx = stage_out(F.io_out, x, n, on_device);
+  nnk_solve_info inf{};
+  nnk::Gmres g(ctx, (int64_t)n);
+  auto op = [&](const double* in, double* outp) { F.apply(in, outp, layout, 1); };
+  g.solve(op, nullptr, db, dx, *sp, inf);
+  finish_out(ctx, F.io_out, x, n, on_device);
+  if (info) *info = inf;
+  if (inf.flag != 0) return fail(ctx, NNK_E_NOCONV, "gmres stopped at maxit above tol");
+  API_CATCH(ctx)
+}
+
+int nnk_mob_create(nnk_fmm* fmm, int32_t nbodies, const int64_t* body_start, const int64_t* fine_start,
+                   const double* rel_points, const double* rel_fine, nnk_mob** out) {
+  if (!fmm || !out || nbodies < 0 || !body_start) return fail(fmm ? fmm->ctx : nullptr, NNK_E_ARG, "bad arguments");
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  std::unique_ptr<nnk_mob> m(new nnk_mob());
+  m->fmm = fmm;
+  m->m.reset(new nnk::Mobility(fmm->f.get(), nbodies, body_start, fine_start, rel_points, rel_fine));
+  *out = m.release();
+  API_CATCH(ctx)
+}
+
+int nnk_mob_apply(nnk_mob* mob, const double* x, double* y, int32_t on_device) {
+  if (!mob || !x || !y) return NNK_E_ARG;
+  nnk_ctx* ctx = mob->fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Mobility& M = *mob->m;
+  const size_t n = (size_t)M.size();
+  const double* dx = stage_in(ctx, M.io_in, x, n, on_device);
+  double* dy = stage_out(M.io_out, y, n, on_device);
+  M.apply(dx, dy);
+  finish_out(ctx, M.io_out, y, n, on_device);
+  API_CATCH(ctx)
+}
+
+int nnk_mob_precon(nnk_mob* mob, const double* x, double* y, int32_t on_device) {
+  if (!mob || !x || !y) return NNK_E_ARG;
+  nnk_ctx* ctx = mob->fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Mobility& M = *mob->m;
+  const size_t n = (size_t)M.size();
+  const double* dx = stage_in(ctx, M.io_in, x, n, on_device);
+  double* dy = stage_out(M.io_out, y, n, on_device);
+  M.precon(dx, dy);
+  finish_out(ctx, M.io_out, y, n, on_device);
+  API_CATCH(ctx)
+}
+
+int nnk_mob_solve(nnk_mob* mob, const double* rhs, double* x, const nnk_solve_params* sp, int32_t precondition,
+                  nnk_solve_info* info, int32_t on_device) {
+  if (!mob || !rhs || !x || !sp) return NNK_E_ARG;
+  nnk_ctx* ctx = mob->fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Mobility& M = *mob->m;
+  const size_t n = (size_t)M.size();
+  const double* db = stage_in(ctx, M.io_in, rhs, n, on_device);
+  double* dx = stage_out(M.io_out, x, n, on_device);
+  nnk_solve_info inf{};
+  M.solve(db, dx, *sp, precondition != 0, inf);
+  finish_out(ctx, M.io_out, x, n, on_device);
+  if (info) *info = inf;
+  if (inf.flag != 0) return fail(ctx, NNK_E_NOCONV, "gmres stopped at maxit above tol");
+  API_CATCH(ctx)
+}
+
+int nnk_mob_destroy(nnk_mob* mob) {
+  delete mob;
+  return NNK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,427 @@
+// KIFMM passes on the GPU (see fmm.h for the formulation).
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+
+#include "fmm.h"
+#include "kernels.cuh"
+
+namespace nnk {
+
+namespace {
+
+// MATLAB linspace(a,b,n)(m) with exact end points (genupsurf.m:20-22).
+inline double mlin(double a, double b, int n, int m) {
+  if (m == 0) return a;
+  if (m == n - 1) return b;
+  return a + ((double)m * (b - a)) / (double)(n - 1);
+}
+
+// Lattice indices (x index i, y index j, z index k) of the outer `shells`
+// layers of a res^3 meshgrid, in column-major meshgrid order: y fastest,
+// then x, then z (genupsurf.m:24-33).
+std::vector<std::array<int, 3>> shell_lattice(int res, int shells) {
+  std::vector<std::array<int, 3>> out;
+  auto inner = [&](int a) { return a >= shells && a <= res - 1 - shells; };
+  for (int k = 0; k < res; ++k)
+    for (int i = 0; i < res; ++i)
+      for (int j = 0; j < res; ++j)
+        if (!(inner(j) && inner(i) && inner(k))) out.push_back({i, j, k});
+  return out;
+}
+
+void surface(const double* lo, const double* hi, int res,
+             const std::vector<std::array<int, 3>>& lat, double* out) {
+  for (size_t p = 0; p < lat.size(); ++p) {
+    out[3 * p + 0] = mlin(lo[0], hi[0], res, lat[p][0]);
+    out[3 * p + 1] = mlin(lo[1], hi[1], res, lat[p][1]);
+    out[3 * p + 2] = mlin(lo[2], hi[2], res, lat[p][2]);
+  }
+}
+
+// Stokeslet block S(x0 - x) without the 1/(8 pi mu) factor folded in
+// (kernel.m:23-47), added into a column-major matrix.
+void kernel_matrix(const std::vector<double>& src, const std::vector<double>& tgt, double eps,
+                   double mu, std::vector<double>& Kcm, int ld) {
+  const size_t ns = src.size() / 3, nt = tgt.size() / 3;
+  const double c = 1.0 / (8.0 * M_PI * mu);
+  for (size_t a = 0; a < nt; ++a)
+    for (size_t b = 0; b < ns; ++b) {
+      const double r[3] = {tgt[3 * a] - src[3 * b], tgt[3 * a + 1] - src[3 * b + 1],
+                           tgt[3 * a + 2] - src[3 * b + 2]};
+      const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      const double inv = c / std::pow(r2 + eps * eps, 1.5);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          const double v = (r[i] * r[j] + (i == j ? r2 + 2 * eps * eps : 0.0)) * inv;
+          Kcm[(3 * b + j) * (size_t)ld + 3 * a + i] = v;  // row 3a+i, col 3b+j
+        }
+    }
+}
+
+struct Solver {
+  cusolverDnHandle_t s = nullptr;
+  cublasHandle_t b = nullptr;
+  Solver(cudaStream_t st) {
+    if (cusolverDnCreate(&s) != CUSOLVER_STATUS_SUCCESS) throw Error(NNK_E_CUDA, "cusolverDnCreate failed");
+    cusolverDnSetStream(s, st);
+    if (cublasCreate(&b) != CUBLAS_STATUS_SUCCESS) throw Error(NNK_E_CUDA, "cublasCreate failed");
+    cublasSetStream(b, st);
+  }
+  ~Solver() {
+    if (s) cusolverDnDestroy(s);
+    if (b) cublasDestroy(b);
+  }
+};
+
+}  // namespace
+
+Fmm::Fmm(nnk_ctx* ctx, const HostTree* tree, const FmmParams& p) : ctx_(ctx), t_(tree), p_(p) {
+  if (!(p.eps > 0) || !(p.mu > 0)) throw Error(NNK_E_ARG, "kernelPar needs eps > 0 and mu > 0");
+  if (p.res < 2 || p.shells < 1 || 2 * p.shells > p.res)
+    throw Error(NNK_E_ARG, "bad coronaRes/coronaShells");
+  P_ = (int)shell_lattice(p.res, p.shells).size();
+  N_ = t_->nodes;
+  E_ = t_->src_start[N_];
+  tot_ = E_ + 2LL * P_ * N_;
+  maxl_ = t_->max_level;
+  build_points();
+  build_tasks();
+  build_operators();
+}
+
+Fmm::~Fmm() {
+  if (blas_) cublasDestroy((cublasHandle_t)blas_);
+}
+
+Fmm& Fmm::sparse() {
+  if (!sparse_) {
+    FmmParams q = p_;
+    q.res = 4;  // computeVelSparse (KIFMM.m:136-138)
+    sparse_.reset(new Fmm(ctx_, t_, q));
+  }
+  return *sparse_;
+}
+
+void Fmm::build_points() {
+  const HostTree& t = *t_;
+  cudaStream_t st = ctx_->stream;
+  const double* root = &t.corners[0];
+  for (int d = 0; d < 3; ++d) shift_[d] = 0.5 * (root[d] + root[3 + d]);
+  auto lat = shell_lattice(p_.res, p_.shells);
+  std::vector<double> pos(3 * (size_t)tot_);
+  std::copy(t.src_pos.begin(), t.src_pos.end(), pos.begin());
+  for (int n = 0; n < N_; ++n) {
+    const double* c = &t.corners[6 * n];
+    const double lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[3], c[4], c[5]};
+    surface(lo, hi, p_.res, lat, &pos[3 * (E_ + (size_t)P_ * n)]);  // genupsurf
+    double w[3], dlo[3], dhi[3];
+    for (int d = 0; d < 3; ++d) {
+      w[d] = hi[d] - lo[d];  // gendownsurf.m:23-24
+      dlo[d] = lo[d] - w[d];
+      dhi[d] = hi[d] + w[d];
+    }
+    surface(dlo, dhi, p_.res, lat, &pos[3 * (E_ + (size_t)P_ * N_ + (size_t)P_ * n)]);
+  }
+  const int64_t nt = (int64_t)t.tgt_row.size();
+  if (p_.precision == NNK_PREC_FP64) {
+    pos64_.upload(pos, st);
+    tpos64_.upload(t.tgt_pos, st);
+    str64_.alloc(3 * tot_);
+    check64_.alloc((size_t)N_ * 3 * P_);
+    vel64_.alloc(3 * nt);
+  } else {
+    std::vector<float> p4(4 * (size_t)tot_);
+    for (int64_t i = 0; i < tot_; ++i) {
+      for (int d = 0; d < 3; ++d) p4[4 * i + d] = (float)(pos[3 * i + d] - shift_[d]);
+      p4[4 * i + 3] = 0.f;
+    }
+    pos32_.upload(p4, st);
+    std::vector<float> t4(4 * (size_t)nt);
+    for (int64_t i = 0; i < nt; ++i) {
+      for (int d = 0; d < 3; ++d) t4[4 * i + d] = (float)(t.tgt_pos[3 * i + d] - shift_[d]);
+      t4[4 * i + 3] = 0.f;
+    }
+    tpos32_.upload(t4, st);
+    str32_.alloc(3 * tot_);
+    check32_.alloc((size_t)N_ * 3 * P_);
+    vel32_.alloc(3 * nt);
+  }
+  trow_.upload(t.tgt_row, st);
+  goff_.upload(t.src_goff, st);
+  gidx_.upload(t.src_gidx, st);
+  gw_.upload(t.src_gw, st);
+  NNK_CUDA(cudaStreamSynchronize(st));
+}
+
+void Fmm::build_tasks() {
+  const HostTree& t = *t_;
+  std::vector<TaskD> tasks;
+  std::vector<SegD> segs;
+  const long long upB = E_, dnB = E_ + (long long)P_ * N_;
+  auto src_seg = [&](int32_t leaf) {
+    const long long s = t.src_start[leaf], e = t.src_start[leaf + 1];
+    if (e > s) segs.push_back(SegD{s, (int)(e - s), 0});
+    return e - s;
+  };
+  int64_t pairs_up = 0, pairs_down = 0, pairs_leaf = 0, pairs_p2p = 0, m2l = 0, c2e = 0;
+  up_.assign(maxl_ + 1, {});
+  down_.assign(maxl_ + 1, {});
+  up_off_.assign(maxl_ + 2, 0);
+  up_nodes_host_.clear();
+  // upward pass (upwardPass.m:32-100): non-empty potential leaves and
+  // non-leaves, level by level from the bottom.  The root's expansion is never
+  // used by any list, so level 0 is skipped.
+  for (int L = maxl_; L >= 0; --L) {
+    up_[L].first = (int64_t)tasks.size();
+    up_off_[L] = (int64_t)up_nodes_host_.size();
+    if (L >= 1) {
+      for (int32_t n : t.by_level[L]) {
+        const bool leaf = t.child0[n] < 0;
+        if (leaf && !t.pleaf[n]) continue;
+        TaskD tk{dnB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
+        if (leaf) {
+          pairs_up += (int64_t)P_ * src_seg(n);
+        } else {
+          for (int k = 0; k < 8; ++k) segs.push_back(SegD{upB + (long long)P_ * (t.child0[n] + k), P_, 0});
+          pairs_up += 8LL * P_ * P_;
+        }
+        tk.nseg = (int)segs.size() - tk.seg0;
+        tasks.push_back(tk);
+        up_nodes_host_.push_back(n);
+      }
+    }
+    up_[L].count = (int64_t)tasks.size() - up_[L].first;
+  }
+  // up_off_ was filled top-down in reverse; rebuild as per-level ranges
+  {
+    std::vector<int32_t> nodes;
+    std::vector<int64_t> off(maxl_ + 2, 0);
+    for (int L = 0; L <= maxl_; ++L) {
+      off[L] = (int64_t)nodes.size();
+      if (L == 0) continue;
+      for (int32_t n : t.by_level[L])
+        if (t.child0[n] >= 0 || t.pleaf[n]) nodes.push_back(n);
+    }
+    off[maxl_ + 1] = (int64_t)nodes.size();
+    up_nodes_host_ = nodes;
+    up_off_ = off;
+  }
+  // downward pass (downwardPass.m:39-168): every node of levels 1..max.
+  // The root's downward expansion is zero, so its L2L term is dropped.
+  for (int L = 1; L <= maxl_; ++L) {
+    down_[L].first = (int64_t)tasks.size();
+    for (int32_t n : t.by_level[L]) {
+      TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
+      for (int64_t k = t.V.off[n]; k < t.V.off[n + 1]; ++k) {
+        segs.push_back(SegD{upB + (long long)P_ * t.V.idx[k], P_, 0});
+        pairs_down += (int64_t)P_ * P_;
+        ++m2l;
+      }
+      for (int64_t k = t.X.off[n]; k < t.X.off[n + 1]; ++k) pairs_down += (int64_t)P_ * src_seg(t.X.idx[k]);
+      if (t.parent[n] > 0) {
+        segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
+        pairs_down += (int64_t)P_ * P_;
+      }
+      tk.nseg = (int)segs.size() - tk.seg0;
+      tasks.push_back(tk);
+    }
+    down_[L].count = (int64_t)tasks.size() - down_[L].first;
+  }
+  // leaf stage (downwardPass.m:170-294): L2T + U (P2P) + W (M2T)
+  leaf_.first = (int64_t)tasks.size();
+  for (int32_t i = 0; i < N_; ++i) {
+    if (!t.tleaf[i]) continue;
+    const int nt = (int)(t.tgt_start[i + 1] - t.tgt_start[i]);
+    TaskD tk{t.tgt_start[i], t.tgt_start[i], nt, (int)segs.size(), 0, 0};
+    for (int64_t k = t.U.off[i]; k < t.U.off[i + 1]; ++k) {
+      const int64_t s = src_seg(t.U.idx[k]);
+      pairs_leaf += (int64_t)nt * s;
+      pairs_p2p += (int64_t)nt * s;
+    }
+    for (int64_t k = t.W.off[i]; k < t.W.off[i + 1]; ++k) {
+      segs.push_back(SegD{upB + (long long)P_ * t.W.idx[k], P_, 0});
+      pairs_leaf += (int64_t)nt * P_;
+    }
+    segs.push_back(SegD{dnB + (long long)P_ * i, P_, 0});
+    pairs_leaf += (int64_t)nt * P_;
+    tk.nseg = (int)segs.size() - tk.seg0;
+    tasks.push_back(tk);
+  }
+  leaf_.count = (int64_t)tasks.size() - leaf_.first;
+  // node lists per level for the downward C2E step
+  lvl_off_.assign(maxl_ + 2, 0);
+  std::vector<int32_t> ln;
+  for (int L = 0; L <= maxl_; ++L) {
+    lvl_off_[L] = (int64_t)ln.size();
+    if (L >= 1) ln.insert(ln.end(), t.by_level[L].begin(), t.by_level[L].end());
+  }
+  lvl_off_[maxl_ + 1] = (int64_t)ln.size();
+  c2e = (int64_t)ln.size() + (int64_t)up_nodes_host_.size();
+  cudaStream_t st = ctx_->stream;
+  tasks_.upload(tasks, st);
+  segs_.upload(segs, st);
+  lvl_nodes_.upload(ln, st);
+  up_nodes_.upload(up_nodes_host_, st);
+  NNK_CUDA(cudaStreamSynchronize(st));
+  stats_.pairs_leaf = pairs_leaf;
+  stats_.pairs_p2p = pairs_p2p;
+  stats_.pairs_up = pairs_up;
+  stats_.pairs_down = pairs_down;
+  stats_.m2l_pairs = m2l;
+  stats_.c2e_columns = c2e;
+  stats_.surface_points = P_;
+  stats_.levels = maxl_ + 1;
+}
+
+void Fmm::build_operators() {
+  const HostTree& t = *t_;
+  const int n = 3 * P_;
+  const double W0 = t.corners[3] - t.corners[0];
+  cudaStream_t st = ctx_->stream;
+  ops_.alloc((size_t)(maxl_ + 1) * n * n);
+  auto lat = shell_lattice(p_.res, p_.shells);
+  Solver sv(st);
+  DBuf<double> dK((size_t)n * n), dB((size_t)n * n), dG((size_t)n * n);
+  DBuf<int> dpiv(n), dinfo(1);
+  int lwork = 0;
+  if (p_.precision == NNK_PREC_FP64) {
+    if (cusolverDnDgetrf_bufferSize(sv.s, n, n, dK.p, n, &lwork) != CUSOLVER_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "getrf_bufferSize failed");
+  } else {
+    if (cusolverDnDpotrf_bufferSize(sv.s, CUBLAS_FILL_MODE_LOWER, n, dG.p, n, &lwork) !=
+        CUSOLVER_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "potrf_bufferSize failed");
+  }
+  DBuf<double> dwork(std::max(lwork, 1));
+  std::vector<double> K((size_t)n * n), I((size_t)n * n, 0.0), KT((size_t)n * n);
+  for (int i = 0; i < n; ++i) I[(size_t)i * n + i] = 1.0;
+  for (int L = 0; L <= maxl_; ++L) {
+    const double w = std::ldexp(W0, -L);
+    const double lo[3] = {0, 0, 0}, hi[3] = {w, w, w};
+    const double dlo[3] = {-w, -w, -w}, dhi[3] = {2 * w, 2 * w, 2 * w};
+    std::vector<double> us(3 * P_), ds(3 * P_);
+    surface(lo, hi, p_.res, lat, us.data());
+    surface(dlo, dhi, p_.res, lat, ds.data());
+    // K_up = kernel(upsurf, downsurf): up-equivalent densities -> down check
+    kernel_matrix(us, ds, p_.eps, p_.mu, K, n);
+    double* dst = ops_.p + (size_t)L * n * n;
+    NNK_CUDA(cudaMemcpyAsync(dK.p, K.data(), K.size() * 8, cudaMemcpyHostToDevice, st));
+    if (p_.precision == NNK_PREC_FP64) {
+      // A = K^-1 by LU with partial pivoting, as MATLAB's mldivide
+      NNK_CUDA(cudaMemcpyAsync(dst, I.data(), I.size() * 8, cudaMemcpyHostToDevice, st));
+      if (cusolverDnDgetrf(sv.s, n, n, dK.p, n, dwork.p, dpiv.p, dinfo.p) != CUSOLVER_STATUS_SUCCESS ||
+          cusolverDnDgetrs(sv.s, CUBLAS_OP_N, n, n, dK.p, n, dpiv.p, dst, n, dinfo.p) !=
+              CUSOLVER_STATUS_SUCCESS)
+        throw Error(NNK_E_CUDA, "LU of the surface matrix failed");
+    } else {
+      // A = (K^T K + lam^2 I)^-1 K^T, lam = reg * sigma_max(K)
+      double smax = 0;
+      {
+        std::vector<double> v(n, 1.0), u(n);
+        for (int it = 0; it < 40; ++it) {
+          for (int r = 0; r < n; ++r) {
+            double s = 0;
+            for (int c = 0; c < n; ++c) s += K[(size_t)c * n + r] * v[c];
+            u[r] = s;
+          }
+          double nu = 0;
+          for (int c = 0; c < n; ++c) {
+            double s = 0;
+            for (int r = 0; r < n; ++r) s += K[(size_t)c * n + r] * u[r];
+            v[c] = s;
+            nu += s * s;
+          }
+          nu = std::sqrt(nu);
+          smax = std::sqrt(nu);
+          for (double& x : v) x /= nu;
+        }
+      }
+      const double reg = p_.reg > 0 ? p_.reg : 1e-8;
+      const double lam2 = (reg * smax) * (reg * smax);
+      for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) KT[(size_t)c * n + r] = K[(size_t)r * n + c];
+      NNK_CUDA(cudaMemcpyAsync(dst, KT.data(), KT.size() * 8, cudaMemcpyHostToDevice, st));
+      const double one = 1.0, zero = 0.0;
+      if (cublasDgemm(sv.b, CUBLAS_OP_T, CUBLAS_OP_N, n, n, n, &one, dK.p, n, dK.p, n, &zero, dG.p, n) !=
+          CUBLAS_STATUS_SUCCESS)
+        throw Error(NNK_E_CUDA, "K^T K product failed");
+      std::vector<double> G((size_t)n * n);
+      NNK_CUDA(cudaMemcpyAsync(G.data(), dG.p, G.size() * 8, cudaMemcpyDeviceToHost, st));
+      NNK_CUDA(cudaStreamSynchronize(st));
+      for (int i = 0; i < n; ++i) G[(size_t)i * n + i] += lam2;
+      NNK_CUDA(cudaMemcpyAsync(dG.p, G.data(), G.size() * 8, cudaMemcpyHostToDevice, st));
+      if (cusolverDnDpotrf(sv.s, CUBLAS_FILL_MODE_LOWER, n, dG.p, n, dwork.p, lwork, dinfo.p) !=
+              CUSOLVER_STATUS_SUCCESS ||
+          cusolverDnDpotrs(sv.s, CUBLAS_FILL_MODE_LOWER, n, n, dG.p, n, dst, n, dinfo.p) !=
+              CUSOLVER_STATUS_SUCCESS)
+        throw Error(NNK_E_CUDA, "Cholesky of the regularized surface matrix failed");
+    }
+    int info = 0;
+    NNK_CUDA(cudaMemcpyAsync(&info, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NNK_CUDA(cudaStreamSynchronize(st));
+    if (info != 0) throw Error(NNK_E_CUDA, "surface matrix factorization reported info=" + std::to_string(info));
+  }
+}
+
+template <typename Real>
+void Fmm::apply_impl(const double* d_in, double* d_out, int layout) {
+  cudaStream_t st = ctx_->stream;
+  const HostTree& t = *t_;
+  Real* str = p_.precision == NNK_PREC_FP64 ? (Real*)str64_.p : (Real*)str32_.p;
+  const Real* pos = p_.precision == NNK_PREC_FP64 ? (const Real*)pos64_.p : (const Real*)pos32_.p;
+  const Real* tpos = p_.precision == NNK_PREC_FP64 ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
+  Real* check = p_.precision == NNK_PREC_FP64 ? (Real*)check64_.p : (Real*)check32_.p;
+  Real* vel = p_.precision == NNK_PREC_FP64 ? (Real*)vel64_.p : (Real*)vel32_.p;
+  const Real e2 = (Real)(p_.eps * p_.eps);
+  const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
+  const int n = 3 * P_;
+  // forces on the leaf source entries (kron(NN,I3)*f per leaf)
+  launch_gather<Real>(E_, goff_.p, gidx_.p, gw_.p, d_in, layout, t.n_pot, str, st);
+  // expansions of nodes that are not computed stay zero
+  NNK_CUDA(cudaMemsetAsync(str + 3 * E_, 0, sizeof(Real) * 3 * (size_t)P_ * N_, st));
+  NNK_CUDA(cudaMemsetAsync(str + 3 * (E_ + (size_t)P_ * N_), 0, sizeof(Real) * 3 * (size_t)P_, st));
+  // upward pass
+  for (int L = maxl_; L >= 1; --L) {
+    if (up_[L].count == 0) continue;
+    launch_p2p<Real>(tasks_.p + up_[L].first, (int)up_[L].count, segs_.p, pos, str, pos, check, e2, scale, st);
+    const int64_t nn = up_off_[L + 1] - up_off_[L];
+    launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 0, up_nodes_.p + up_off_[L], (int)nn, check,
+                     str, E_, P_, st);
+  }
+  // downward pass
+  for (int L = 1; L <= maxl_; ++L) {
+    if (down_[L].count == 0) continue;
+    launch_p2p<Real>(tasks_.p + down_[L].first, (int)down_[L].count, segs_.p, pos, str, pos, check, e2,
+                     scale, st);
+    const int64_t nn = lvl_off_[L + 1] - lvl_off_[L];
+    launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 1, lvl_nodes_.p + lvl_off_[L], (int)nn, check, str,
+                     E_ + (int64_t)P_ * N_, P_, st);
+  }
+  // leaf stage
+  if (leaf_.count)
+    launch_p2p<Real>(tasks_.p + leaf_.first, (int)leaf_.count, segs_.p, pos, str, tpos, vel, e2, scale, st);
+  launch_scatter<Real>((int64_t)t.tgt_row.size(), trow_.p, vel, layout, t.n_tgt, d_out, st);
+}
+
+void Fmm::apply(const double* d_in, double* d_out, int layout, int nrhs) {
+  const HostTree& t = *t_;
+  for (int r = 0; r < nrhs; ++r) {
+    const double* in = d_in + (size_t)r * 3 * t.n_pot;
+    double* out = d_out + (size_t)r * 3 * t.n_tgt;
+    if (t.n_tgt == 0) continue;
+    if (p_.precision == NNK_PREC_FP64)
+      apply_impl<double>(in, out, layout);
+    else
+      apply_impl<float>(in, out, layout);
+  }
+}
+
+template void Fmm::apply_impl<double>(const double*, double*, int);
+template void Fmm::apply_impl<float>(const double*, double*, int);
+
+}  // namespace nnk

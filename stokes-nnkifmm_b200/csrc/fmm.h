@@ -1,0 +1,126 @@
+// KIFMM operator on one tree (device side).
+//
+// All pair interactions of the reference passes -- S2M and M2M
+// (upwardPass.m), M2L, P2L and L2L (DownNonleaf.m), L2T, P2P and M2T
+// (Downleaf.m), with their NEAREST variants -- run through one batched pair
+// kernel over "tasks": a target point set plus a list of source segments in
+// one unified point array
+//   [ leaf source entries | up-equivalent surfaces | down-equivalent surfaces ].
+// The per-node check-to-equivalent solves (kernel(...) \ check, Up.m:31-33,
+// DownNonleaf.m:42-46) become one precomputed FP64 operator per level, applied
+// to all nodes of the level as a batched product.
+#pragma once
+#include <memory>
+#include <vector>
+
+#include "common.h"
+#include "tree.h"
+
+namespace nnk {
+
+struct TaskD {
+  long long tgt;  // first target (index into the target position array)
+  long long out;  // first output slot (3 values each)
+  int ntgt;
+  int seg0;
+  int nseg;
+  int pad;
+};
+struct SegD {
+  long long start;  // first source in the unified arrays
+  int count;
+  int pad;
+};
+
+struct TaskGroup {
+  int64_t first = 0, count = 0;  // range in the task array
+};
+
+struct FmmParams {
+  double eps = 0.0, mu = 1.0;
+  int res = 6, shells = 1;
+  int precision = NNK_PREC_FP64;
+  double reg = 0.0;
+};
+
+class Fmm {
+ public:
+  Fmm(nnk_ctx* ctx, const HostTree* tree, const FmmParams& p);
+  ~Fmm();
+  // in: potentials (n_pot x 3, FP64, device), out: velocities (n_tgt x 3, FP64, device)
+  void apply(const double* d_in, double* d_out, int layout, int nrhs);
+  // Same, but over the p=4 surfaces (computeVelSparse).
+  Fmm& sparse();
+  void reduced_apply(const double* d_in, double* d_out, int layout);
+  void reduced_solve(const double* d_in, double* d_out, int layout);
+  nnk_fmm_stats stats() const { return stats_; }
+  const HostTree& tree() const { return *t_; }
+  nnk_ctx* ctx() const { return ctx_; }
+  const FmmParams& params() const { return p_; }
+  // scratch for host-pointer calls
+  DBuf<double> io_in, io_out;
+
+ private:
+  template <typename Real> void apply_impl(const double* d_in, double* d_out, int layout);
+  void build_points();
+  void build_tasks();
+  void build_operators();
+  void build_reduced();
+
+  nnk_ctx* ctx_;
+  const HostTree* t_;
+  FmmParams p_;
+  int P_ = 0;            // surface points per node
+  int N_ = 0;            // nodes
+  int64_t E_ = 0;        // leaf source entries
+  int64_t tot_ = 0;      // E + 2 P N
+  int maxl_ = 0;
+  double shift_[3] = {0, 0, 0};  // FP32 positions are relative to the root centre
+
+  // unified point/strength arrays
+  DBuf<double> pos64_;   // tot*3
+  DBuf<float> pos32_;    // tot*4
+  DBuf<double> str64_;   // tot*3
+  DBuf<float> str32_;    // tot*3
+  // sorted targets
+  DBuf<double> tpos64_;  // ntgt*3
+  DBuf<float> tpos32_;   // ntgt*4
+  DBuf<int32_t> trow_;
+  // gather (NEAREST: kron(NN,I3)*f per entry)
+  DBuf<int64_t> goff_;
+  DBuf<int32_t> gidx_;
+  DBuf<double> gw_;
+  // tasks
+  DBuf<TaskD> tasks_;
+  DBuf<SegD> segs_;
+  std::vector<TaskGroup> up_, down_;  // per level
+  TaskGroup leaf_;
+  DBuf<int32_t> lvl_nodes_;
+  std::vector<int64_t> lvl_off_;
+  std::vector<int32_t> up_nodes_host_;  // per level: nodes whose uppot is computed
+  DBuf<int32_t> up_nodes_;
+  std::vector<int64_t> up_off_;
+  // operators: per level, uppot = A_L * check (A_L = K_up^-1 or its Tikhonov form);
+  // downpot = A_L^T * check.
+  DBuf<double> ops_;
+  // work buffers
+  DBuf<double> check64_, vel64_;
+  DBuf<float> check32_, vel32_;
+  // reduced (leaf block) solve: LU of S_leaf*NN_leaf per target leaf, padded
+  bool reduced_ready_ = false;
+  int rdim_ = 0;                 // padded block size (3 * max leaf targets)
+  DBuf<double> rlu_;             // nleaf * rdim * rdim (column-major per block)
+  DBuf<int> rpiv_, rinfo_;
+  DBuf<double*> rptr_;
+  DBuf<double> rrhs_;
+  DBuf<double*> rrhsptr_;
+  DBuf<double> rmat_;            // unfactored blocks for reduced_apply
+  std::vector<int32_t> rleaf_;   // target leaves in order
+  DBuf<int32_t> rleaf_d_;
+  DBuf<int64_t> rts_;            // tgt_start on the device
+  void* blas_ = nullptr;         // cublasHandle_t for the batched leaf solves
+  nnk_fmm_stats stats_{};
+  std::unique_ptr<Fmm> sparse_;
+};
+
+}  // namespace nnk

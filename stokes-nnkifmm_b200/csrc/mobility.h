@@ -1,0 +1,47 @@
+// Rigid-body mobility system on one FMM (Mobility/*.m):
+//   [ S*NN  BT ] [ f     ]   [ u_slip - u_bg ]
+//   [ B     0  ] [ U; Om ] = [ F; M          ]
+// Vector layout (mobilityProblem.m:45-46, MobilityMatrixMulti.m:96-107):
+//   [ f_x(1..N) f_y(1..N) f_z(1..N) | U_x(1..nb) U_y U_z | Om_x(1..nb) Om_y Om_z ].
+#pragma once
+#include <memory>
+#include <vector>
+
+#include "common.h"
+#include "fmm.h"
+
+namespace nnk {
+
+class Mobility {
+ public:
+  Mobility(Fmm* fmm, int nbodies, const int64_t* body_start, const int64_t* fine_start,
+           const double* rel_points, const double* rel_fine);
+  int64_t size() const { return 3 * N_ + 6 * (int64_t)nb_; }
+  void apply(const double* x, double* y);   // mobilityMatrixMulti.m:17-36
+  void precon(const double* x, double* y);  // MobilityPrecon.m:17-40
+  void solve(const double* rhs, double* x, const nnk_solve_params& sp, bool precondition, nnk_solve_info& info);
+  DBuf<double> io_in, io_out;
+
+ private:
+  void body_sums(const double* f, double* out6);          // B * f
+  void body_sums_t(const double* z6, double* f, double a); // f = a*f + B^T z
+  void bt_apply(const double* uo, double* y);              // y += BT * [U;Om]
+  void btt_apply(const double* v, double* out6);           // BT^T v
+  void small_solve(const std::vector<double>& inv, const double* in6, double* out6);  // host 6x6 blocks
+
+  Fmm* fmm_;
+  nnk_ctx* ctx_;
+  int nb_;
+  int64_t N_;
+  std::vector<int64_t> bstart_;
+  DBuf<int32_t> body_of_;   // per point: body or -1 (boundary)
+  DBuf<int64_t> bstart_d_;
+  DBuf<double> xrel_;       // per point rotated untranslated position (BT, Swimmers.m:177-189)
+  DBuf<double> xm_;         // per point torque arm: sum_q NN(q,n) X_q (NEAREST) or xrel (genMatrixComponets.m:217-222)
+  DBuf<double> af_;         // per point force weight: column sum of NN (NEAREST) or 1 (:208-209, :228)
+  std::vector<double> a1inv_, a2inv_;  // per body 6x6 inverses of B B^T and BT^T BT
+  DBuf<double> t6a_, t6b_, tv_, tv2_, tv3_;
+  std::vector<double> h6a_, h6b_;
+};
+
+}  // namespace nnk

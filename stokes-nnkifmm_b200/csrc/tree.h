@@ -1,0 +1,90 @@
+// Host-side octree, interaction lists and NEAREST source entries.
+//
+// The tree follows Classes/OcTree.m bit for bit: one scalar root cube from the
+// global min/max (OcTree.m:97-98), FP64 midpoints (lo+hi)/2 (:197), strict
+// p > centre (:211), children in nodeMap order (x bit most significant,
+// :200-212), DFS block numbering (:174-175), maxDepth error (:168-170).
+// Node ids are 0-based here (reference id - 1); exports add 1.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace nnk {
+
+struct TreeParams {
+  int node_capacity = 200;
+  int max_depth = 21;
+  int nearest = 0;
+};
+
+struct Csr {
+  std::vector<int64_t> off;  // size rows+1
+  std::vector<int32_t> idx;
+  int64_t rows() const { return off.empty() ? 0 : (int64_t)off.size() - 1; }
+  int64_t begin(int64_t r) const { return off[r]; }
+  int64_t end(int64_t r) const { return off[r + 1]; }
+};
+
+struct HostTree {
+  // ---- points (OcTree.m:80-82)
+  int64_t n = 0;                 // unique points
+  std::vector<double> pts;       // n*3
+  std::vector<uint8_t> is_pot, is_tgt;
+  std::vector<int64_t> pot_rank; // point -> row in the potentials input (-1)
+  std::vector<int64_t> tgt_rank; // point -> row in the velocity output (-1)
+  int64_t n_pot = 0, n_tgt = 0;
+  int capacity = 0;              // min(nodeCapacity, n-1)
+  TreeParams params;
+
+  // ---- nodes, indexed by 0-based id
+  int32_t nodes = 0;
+  int32_t max_level = 0;
+  std::vector<int32_t> level, parent, child0;  // parent -1 at root, child0 -1 leaf
+  std::vector<int32_t> ix, iy, iz;             // integer box coords at own level
+  std::vector<double> corners;                 // 6 per node [lo hi]
+  std::vector<int64_t> pstart, pcount;         // range of the node in `order`
+  std::vector<int64_t> order;                  // points sorted by leaf (orig order inside)
+  std::vector<int32_t> point_index;            // leaf id per point
+  std::vector<uint8_t> tleaf, pleaf;           // non-empty target / potential leaf
+  std::vector<uint8_t> full;                   // subtree has no empty-potential leaf
+  std::vector<std::vector<int32_t>> colleagues;  // same-level touching nodes (incl. self)
+  std::vector<std::vector<int32_t>> by_level;    // node ids per level, ascending
+
+  // ---- lists in the reference's order (0-based ids)
+  Csr U, V, W, X;
+
+  // ---- NEAREST
+  int64_t q = 0;
+  std::vector<double> fine;         // q*3
+  std::vector<int64_t> nn_rowptr;   // CSR by fine point
+  std::vector<int32_t> nn_col;      // column = row in potPoints (= point, NEAREST)
+  std::vector<double> nn_val;
+
+  // ---- leaf source entries (sorted by leaf, then fine index / point index)
+  //  entry e: position src_pos[e], force = sum_k w * f[pot row] over its gather
+  std::vector<int64_t> src_start;   // per node, size nodes+1 (only leaves non-empty)
+  std::vector<double> src_pos;      // E*3
+  std::vector<int64_t> src_goff;    // E+1
+  std::vector<int32_t> src_gidx;    // potential row
+  std::vector<double> src_gw;       // weight
+  // ---- leaf targets (sorted by leaf)
+  std::vector<int64_t> tgt_start;   // per node, size nodes+1
+  std::vector<int32_t> tgt_row;     // output row per sorted target
+  std::vector<double> tgt_pos;      // sorted target positions
+
+  bool touch(int32_t a, int32_t b) const;  // nodeintersection.m closed-box test
+};
+
+// Returns 0 or an NNK_E_* code; msg gets the reason.
+int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tgt,
+               const double* fine, int64_t q, const int64_t* nn_rowptr,
+               const int32_t* nn_col, const double* nn_val, const TreeParams& p,
+               HostTree& t, std::string& msg);
+
+// nearestMatrix (Tools/Nearest/nearestMatrix.m:17-41), exact FP64 ties.
+void nearest_matrix(const double* coarse, int64_t n, const double* fine, int64_t q,
+                    std::vector<int64_t>& rowptr, std::vector<int32_t>& col,
+                    std::vector<double>& val);
+
+}  // namespace nnk

@@ -1,0 +1,113 @@
+"""KIFMM: host mirror of Classes/KIFMM.m over the CUDA library.
+
+    fmm = KIFMM(tree, [eps, mu], GMRES=1, format=2)
+    vel = fmm.computeVel(potentials)
+
+Same name-value options as KIFMM.m:50-60 (``GPU`` and ``parThreads`` are
+accepted for compatibility; the work always runs on the GPU) plus
+``precision`` ('fp64' or 'mixed').  Inputs may be numpy arrays (host) or
+CUDA torch tensors (device); results come back the same way.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+
+class KIFMM:
+    def __init__(self, tree, kernelPar, GPU=1, parThreads=0, blockSize=0.1, GMRES=0, coronaRes=6,
+                 coronaShells=1, format=1, precision="fp64", reg=0.0):
+        self.tree = tree
+        self.ctx = tree.ctx
+        eps, mu = float(kernelPar[0]), float(kernelPar[1])
+        self.arguments = dict(GPU=GPU, parThreads=parThreads, blockSize=blockSize, GMRES=GMRES,
+                              coronaRes=coronaRes, coronaShells=coronaShells, format=format,
+                              kernelPar=(eps, mu), precision=precision)
+        prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
+        p = L.FmmParams(eps, mu, int(coronaRes), int(coronaShells), prec, 0, float(reg))
+        h = C.c_void_p()
+        L.check(L.lib.nnk_fmm_create(self.ctx.h, tree.h, C.byref(p), C.byref(h)), self.ctx.h, "KIFMM")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            L.lib.nnk_fmm_destroy(self.h)
+            self.h = None
+
+    # KIFMM.m:83-103: GMRES=1 -> vector; format 1 interleaved, 2 blocked
+    def _layout(self):
+        if self.arguments["GMRES"] == 1 and self.arguments["format"] == 2:
+            return L.LAYOUT_BLOCKED
+        return L.LAYOUT_ROWS
+
+    def _call(self, fn, x, n_in, n_out, nrhs=1, extra=True):
+        layout = self._layout()
+        gm = self.arguments["GMRES"] == 1
+        try:
+            import torch
+            is_t = isinstance(x, torch.Tensor)
+        except ImportError:
+            is_t = False
+        if is_t:
+            xin = x.contiguous().to(torch.float64)
+            if not xin.is_cuda:
+                raise ValueError("torch inputs must be CUDA tensors; pass numpy arrays for host data")
+            out = torch.empty(nrhs * 3 * n_out, dtype=torch.float64, device=xin.device)
+            dev = 1
+        else:
+            xin = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+            out = np.empty(nrhs * 3 * n_out, dtype=np.float64)
+            dev = 0
+        nin = xin.numel() if is_t else xin.size
+        if nin != nrhs * 3 * n_in:
+            raise ValueError(f"expected {nrhs * 3 * n_in} values, got {nin}")
+        args = [self.h, L.ptr(xin), L.ptr(out), layout]
+        if extra:
+            args.append(nrhs)
+        args.append(dev)
+        L.check(fn(*args), self.ctx.h)
+        if gm:
+            return out if nrhs == 1 else out.reshape(nrhs, -1)
+        return out.reshape(n_out, 3) if nrhs == 1 else out.reshape(nrhs, n_out, 3)
+
+    def computeVel(self, potentials, nrhs=1):
+        """KIFMM.computeVel (KIFMM.m:63-105)."""
+        i = self.tree.info
+        return self._call(L.lib.nnk_fmm_apply, potentials, i.num_potentials, i.num_targets, nrhs)
+
+    def computeVelSparse(self, potentials, nrhs=1):
+        """KIFMM.computeVelSparse (KIFMM.m:107-155): coronaRes 4."""
+        i = self.tree.info
+        return self._call(L.lib.nnk_fmm_apply_sparse, potentials, i.num_potentials, i.num_targets, nrhs)
+
+    def reducedComputeVel(self, potentials):
+        """KIFMM.reducedComputeVel (KIFMM.m:157-198)."""
+        i = self.tree.info
+        return self._call(L.lib.nnk_fmm_reduced_apply, potentials, i.num_potentials, i.num_targets, extra=False)
+
+    def reducedSolve(self, vel):
+        """KIFMM.reducedSolve (KIFMM.m:200-242)."""
+        i = self.tree.info
+        return self._call(L.lib.nnk_fmm_reduced_solve, vel, i.num_targets, i.num_targets, extra=False)
+
+    def stats(self):
+        s = L.FmmStats()
+        L.check(L.lib.nnk_fmm_stats_get(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in L.FmmStats._fields_}
+
+    def gmres(self, b, tol=1e-6, maxit=None, restart=0):
+        """gmres(@(x) fmm.computeVel(x), b, [], tol, maxit) on the device
+        (Data Generation/DirectMethodComparison.m:28).  Returns
+        (x, flag, relres, iters) like MATLAB's first four outputs."""
+        n = 3 * self.tree.info.num_targets
+        bb = np.ascontiguousarray(np.asarray(b, dtype=np.float64).ravel())
+        if bb.size != n:
+            raise ValueError("rhs size")
+        x = np.empty(n)
+        sp_ = L.SolveParams(float(tol), int(maxit if maxit else min(n, 10)), int(restart))
+        info = L.SolveInfo()
+        rc = L.lib.nnk_fmm_solve(self.h, L.ptr(bb), L.ptr(x), self._layout(), C.byref(sp_), C.byref(info), 0)
+        if rc not in (L.NNK_OK, L.NNK_E_NOCONV):
+            L.check(rc, self.ctx.h, "gmres")
+        return x, info.flag, info.relres, info.iters
