@@ -1,0 +1,83 @@
+"""GPU mobility solve (config 1: one rigid sphere, NEAREST, p=6, eps=0.01)
+against the dense FP64 regularized-Stokeslet system, and the known answers
+U = F/(6 pi mu a), Omega = M/(8 pi mu a^3)."""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import nnkifmm as nk
+from conftest import GOLDEN
+from oracle import mobility as om
+
+pytestmark = pytest.mark.gpu
+
+
+def sphere_body(F, M):
+    g = np.load(os.path.join(GOLDEN, "sphere10_40.npz"))
+    NN = sp.csr_matrix((g["nn_data"], g["nn_indices"], g["nn_indptr"]))
+    c, f = g["coarse"], g["fine"]
+    return c, f, NN, F, M
+
+
+def run_problem(F, M, precon, precision="fp64"):
+    c, f, NN, F, M = sphere_body(F, M)
+    sw = nk.Swimmers()
+    sw.addSwimmer(c, f, NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(c), F, M)
+    out, info = nk.mobilityProblem(sw, None, 0.0, np.array([0, 0, 0, 1, 0, 0, 0, 1, 0.0]), [0.01, 1.0],
+                                   {"nodeCapacity": 60, "nearest": 1}, tol=1e-8, maxIter=300,
+                                   PreconSettings=[1e-6, 100] if precon else None, precision=precision,
+                                   return_info=True)
+    body = om.Body(c, f, NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(c), F, M)
+    asm = om.assemble([body])
+    xd = np.linalg.solve(om.dense_mobility_matrix(asm, 0.01, 1.0, True), om.mobility_rhs(asm))
+    return out, info, xd
+
+
+@pytest.mark.parametrize("precon", [False, True])
+def test_translation_and_rotation(precon):
+    out, info, xd = run_problem([1, 0, 0], [0, 0, 0], precon)
+    assert info["flag"] == 0
+    U = out[0:3]
+    assert abs(U[0] - xd[-6]) / abs(xd[-6]) < 1e-5
+    assert abs(U[0] * 6 * np.pi - 1) < 1e-2
+    out, info, xd = run_problem([0, 0, 0], [0, 0, 1], precon)
+    Om = np.cross([1, 0, 0], out[3:6])  # out(4:6) = Om x b1 with b1 = e_x
+    assert info["flag"] == 0
+    assert abs(out[3:6][1] - xd[-1]) / abs(xd[-1]) < 1e-5  # (Om x e_x)_y = Om_z
+    assert abs(xd[-1] * 8 * np.pi - 1) < 2e-2
+    del Om
+
+
+def test_precon_reduces_iterations():
+    _, a, _ = run_problem([1, 0, 0], [0, 0, 1], False)
+    _, b, _ = run_problem([1, 0, 0], [0, 0, 1], True)
+    assert b["iters"] <= a["iters"]
+
+
+def test_mobility_matvec_vs_dense():
+    c, f, NN, _, _ = sphere_body(None, None)
+    sw = nk.Swimmers()
+    sw.addSwimmer(c, f, NN, [0.1, -0.2, 0.3], [0, 1, 0, -1, 0, 0], np.zeros_like(c), [0, 0, 0], [0, 0, 0])
+    sw.genTree(nodeCapacity=60, nearest=1)
+    sw.genKIFMM([0.01, 1.0], GMRES=1, format=2)
+    mob = sw.mobility()
+    body = om.Body(c, f, NN, [0.1, -0.2, 0.3], [0, 1, 0, -1, 0, 0], np.zeros_like(c), [0, 0, 0], [0, 0, 0])
+    A = om.dense_mobility_matrix(om.assemble([body]), 0.01, 1.0, True)
+    x = np.random.default_rng(4).standard_normal(A.shape[0])
+    y = mob.apply(x)
+    assert np.linalg.norm(y - A @ x) / np.linalg.norm(A @ x) < 1e-4
+    # rigid rows are exact (no FMM involved)
+    assert np.allclose(y[-6:], (A @ x)[-6:], rtol=1e-12, atol=1e-12)
+
+
+def test_fmm_gmres_resistance_sphere():
+    """gmres(@(x) fmm.computeVel(x), vel, [], 1e-8, 200): drag of a translating sphere."""
+    c, f, NN, _, _ = sphere_body(None, None)
+    t = nk.OcTree(c, c, nodeCapacity=60, nearest=1, finePoints=f, NN=NN)
+    fmm = nk.KIFMM(t, [0.01, 1.0], GMRES=1, format=1)
+    x, flag, relres, it = fmm.gmres(np.tile([1.0, 0, 0], len(c)), tol=1e-8, maxit=200)
+    assert flag == 0 and relres <= 1e-8
+    F = (NN @ x.reshape(-1, 3)).sum(0)
+    assert abs(F[0] / (6 * np.pi) - 1) < 5e-3

@@ -1,0 +1,126 @@
+"""The FP64 oracle against the reference's known answers and self-consistency.
+
+The reference ships no golden vectors; its one built-in known answer is the
+Stokes drag of the unit sphere, [6*pi; 0; 0]
+(Data Generation/DirectMethodComparison.m:34, Benchmarkresistance.m:12,35).
+"""
+import numpy as np
+import pytest
+
+from oracle import mobility as om
+from oracle.geometry import sphere, prolate_spheroid, velocity_modes, wall_tri
+from oracle.gmres import gmres
+from oracle.kernel import apply_kernel, kernel
+from oracle.mlab import linspace
+from oracle.nearest import nearest_matrix
+from oracle.octree import OcTree, MaxDepthError
+from oracle.surfaces import downsurf, surface_count, upsurf
+
+
+def test_matlab_linspace_endpoints_and_formula():
+    y = linspace(-1.0, 1.0, 7)
+    assert y[0] == -1.0 and y[-1] == 1.0
+    k = np.arange(7.0)
+    assert np.array_equal(y[1:-1], (-1.0 + (k * 2.0) / 6)[1:-1])
+
+
+def test_sphere_counts():
+    # n^3 - (n-2)^3 points (Geometries/Sphere.m)
+    assert sphere(1.0, [0, 0, 0], 10).shape == (488, 3)
+    assert sphere(1.0, [0, 0, 0], 40).shape == (9128, 3)
+    p = sphere(2.0, [1, 2, 3], 6)
+    assert np.allclose(np.linalg.norm(p - [1, 2, 3], axis=1), 2.0)
+
+
+def test_surfaces_counts_and_order():
+    assert surface_count(6, 1) == 152 and surface_count(4, 1) == 56
+    c = np.array([0.0, 0, 0, 1, 1, 1])
+    u = upsurf(c)
+    d = downsurf(c)
+    assert u.shape == (152, 3) and d.shape == (152, 3)
+    # column-major meshgrid order: y runs fastest, then x, then z
+    assert np.array_equal(u[0], [0, 0, 0]) and np.array_equal(u[1], [0, 0.2, 0])
+    assert d.min() == -1.0 and d.max() == 2.0
+
+
+def test_kernel_symmetry_and_blocks():
+    rng = np.random.default_rng(0)
+    x, y = rng.random((5, 3)), rng.random((4, 3))
+    S = kernel(x, y, 0.1, 1.3)
+    assert np.allclose(S, kernel(y, x, 0.1, 1.3).T, rtol=0, atol=1e-14)
+    f = rng.standard_normal((5, 3))
+    assert np.allclose((S @ f.ravel()).reshape(-1, 3), apply_kernel(x, y, f, 0.1, 1.3), rtol=1e-13)
+
+
+def test_sphere_drag_known_answer():
+    """F = 6 pi mu a U for a translating unit sphere (DirectMethodComparison.m:34)."""
+    c = sphere(1.0, [0, 0, 0], 10)
+    f = sphere(1.0, [0, 0, 0], 40)
+    NN = nearest_matrix(c, f)
+    A = kernel(f, c, 0.01, 1.0) @ np.kron(NN.toarray(), np.eye(3))
+    x = np.linalg.solve(A, np.tile([1.0, 0, 0], len(c)))
+    F = (NN @ x.reshape(-1, 3)).sum(0)
+    assert abs(F[0] - 6 * np.pi) / (6 * np.pi) < 5e-3
+    assert abs(F[1]) < 1e-10 and abs(F[2]) < 1e-10
+
+
+def test_mobility_sphere_known_answers():
+    """U = F/(6 pi mu a), Omega = M/(8 pi mu a^3) for the config-1 sphere."""
+    c = sphere(1.0, [0, 0, 0], 10)
+    f = sphere(1.0, [0, 0, 0], 40)
+    NN = nearest_matrix(c, f)
+    body = om.Body(c, f, NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(c), [1, 0, 0], [0, 0, 1])
+    asm = om.assemble([body])
+    M = om.dense_mobility_matrix(asm, 0.01, 1.0, True)
+    x = np.linalg.solve(M, om.mobility_rhs(asm))
+    assert abs(x[-6] * 6 * np.pi - 1) < 1e-2
+    assert abs(x[-1] * 8 * np.pi - 1) < 2e-2
+
+
+def test_nearest_ties_share_weight():
+    g = np.array([[i, j, k] for i in range(3) for j in range(3) for k in range(3)], float)
+    NN = nearest_matrix(g, np.array([[0.5, 0.5, 0.5], [0.1, 0, 0]]))
+    assert NN.getnnz(axis=1).tolist() == [8, 1]
+    assert np.allclose(NN.sum(axis=1), 1.0)
+    assert np.allclose(NN[0].data, 1 / 8)
+
+
+def test_octree_capacity_and_dfs_ids():
+    rng = np.random.default_rng(3)
+    x = rng.random((500, 3))
+    t = OcTree(x, x, node_capacity=20, build_lists=False)
+    leaves = np.nonzero(t.children[1:, 0] == 0)[0] + 1
+    counts = np.bincount(t.point_index, minlength=t.node_count + 1)
+    assert counts[leaves].max() <= 20
+    # children of a node are a consecutive block of 8 ids, appended in DFS order
+    for i in range(1, t.node_count + 1):
+        ch = t.children[i]
+        if ch[0]:
+            assert np.array_equal(ch, np.arange(ch[0], ch[0] + 8))
+            assert (t.parent[ch] == i).all()
+
+
+def test_octree_max_depth_error():
+    x = np.array([[0, 0, 0], [1e-9, 0, 0], [1, 1, 1]], float)
+    with pytest.raises(MaxDepthError):
+        OcTree(x, x, node_capacity=1, max_depth=8)
+
+
+def test_oracle_gmres_matches_dense_solve():
+    rng = np.random.default_rng(1)
+    A = np.eye(40) + 0.1 * rng.standard_normal((40, 40))
+    b = rng.standard_normal(40)
+    x, flag, relres, it, _ = gmres(lambda v: A @ v, b, None, 1e-12, 40)
+    assert flag == 0 and relres <= 1e-12
+    assert np.allclose(x, np.linalg.solve(A, b), rtol=1e-9, atol=1e-10)
+
+
+def test_geometry_generators():
+    p = prolate_spheroid(0.5, 1.5, 0.2)
+    assert np.allclose(p[:2], [[0, 0, 1.5], [0, 0, -1.5]])
+    r = (p[:, 0] ** 2 + p[:, 1] ** 2) / 0.25 + p[:, 2] ** 2 / 2.25
+    assert np.allclose(r, 1.0)
+    w = wall_tri([0, 0, -1.5], [1.0, 1.0], 3, 0.05)
+    assert np.allclose(w[:, 2], -1.5) and len(w) > 400
+    v = velocity_modes(np.eye(3), [1, 0, 0], [0, 0, 1])
+    assert np.allclose(v, [[1, 1, 0], [0, 0, 0], [1, 0, 0]])

@@ -1,0 +1,127 @@
+"""Bit-exact parity of the library's octree, U/V/W/X lists and NN matrix
+(through the C ABI, host part; no GPU needed) with the oracle restatement of
+Classes/OcTree.m and Tools/Nearest/nearestMatrix.m."""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import nnkifmm as nk
+from conftest import GOLDEN
+from oracle.geometry import sphere
+from oracle.nearest import nearest_matrix
+from oracle.octree import OcTree as OracleTree
+
+
+def assert_same_tree(a, b):
+    assert a.node_count == b.nodeCount
+    assert np.array_equal(a.level[1:], b.nodeLevel)
+    assert np.array_equal(a.parent[1:], b.nodeParents)
+    assert np.array_equal(a.children[1:], b.nodeChildren)
+    assert np.array_equal(a.corners[1:], b.nodeCorners)  # bit-exact FP64 midpoints
+    assert np.array_equal(a.point_index, b.pointIndex)
+    assert np.array_equal(a.potentials, b.potentials) and np.array_equal(a.targets, b.targets)
+    inter = b.interactions
+    for i in range(1, a.node_count + 1):
+        for k, lst in enumerate([a.U, a.V, a.W, a.X]):
+            assert np.array_equal(lst[i], inter[i - 1][k]), (i, "UVWX"[k], lst[i], inter[i - 1][k])
+
+
+def mixed(rng, n):
+    u = rng.random((n // 2, 3))
+    cen = rng.uniform(0.2, 0.8, (3, 3))
+    rad = rng.uniform(0.05, 0.2, 3)
+    d = rng.standard_normal((n - n // 2, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    k = rng.integers(0, 3, n - n // 2)
+    return np.concatenate([u, cen[k] + rad[k, None] * d])
+
+
+@pytest.mark.parametrize("seed,n,cap", [(0, 1500, 64), (1, 1500, 20), (2, 900, 8), (3, 3000, 50)])
+def test_tree_and_lists_match_oracle(seed, n, cap):
+    x = mixed(np.random.default_rng(seed), n)
+    assert_same_tree(OracleTree(x, x, node_capacity=cap), nk.OcTree(x, x, nodeCapacity=cap))
+
+
+def test_tree_clustered_deep():
+    rng = np.random.default_rng(7)
+    z = np.concatenate([rng.normal(0.3, 0.005, (1000, 3)), rng.random((300, 3))])
+    assert_same_tree(OracleTree(z, z, node_capacity=12), nk.OcTree(z, z, nodeCapacity=12))
+
+
+def test_tree_split_sources_targets():
+    rng = np.random.default_rng(8)
+    s = mixed(rng, 1200)
+    t = np.concatenate([rng.random((400, 3)) * 0.6, s[:50]])  # some targets coincide with sources
+    assert_same_tree(OracleTree(s, t, node_capacity=25), nk.OcTree(s, t, nodeCapacity=25))
+
+
+def test_tree_sphere_config1():
+    c = sphere(1.0, [0, 0, 0], 10)
+    assert_same_tree(OracleTree(c, c, node_capacity=60), nk.OcTree(c, c, nodeCapacity=60))
+
+
+@pytest.mark.parametrize("name", ["sphere10_40", "adaptive_plain_1600", "adaptive_nearest_1200", "split_1500_700"])
+def test_tree_matches_golden(name):
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    if "coarse" in g:
+        NN = sp.csr_matrix((g["nn_data"], g["nn_indices"], g["nn_indptr"]))
+        t = nk.OcTree(g["coarse"], g["coarse"], nodeCapacity=int(g["cap"]), nearest=1, finePoints=g["fine"], NN=NN)
+    elif "src" in g:
+        t = nk.OcTree(g["src"], g["tgt"], nodeCapacity=int(g["cap"]))
+    else:
+        t = nk.OcTree(g["points"], g["points"], nodeCapacity=int(g["cap"]))
+    assert np.array_equal(t.nodeLevel, g["level"])
+    assert np.array_equal(t.nodeParents, g["parent"])
+    assert np.array_equal(t.nodeChildren, g["children"])
+    assert np.array_equal(t.nodeCorners, g["corners"])
+    assert np.array_equal(t.pointIndex, g["point_index"])
+    for k, name_ in enumerate("UVWX"):
+        off, ids = t.interaction_list(k)
+        assert np.array_equal(off, g[f"list_{name_}_off"]) and np.array_equal(ids, g[f"list_{name_}_ids"])
+
+
+def test_nearest_matrix_matches_oracle():
+    rng = np.random.default_rng(11)
+    c = mixed(rng, 2000)
+    f = np.concatenate([rng.random((3000, 3)), c[:100] + 1e-3, rng.random((50, 3)) * 3 - 1])  # some outside
+    A, B = nearest_matrix(c, f), nk.nearestMatrix(c, f)
+    assert (A != B).nnz == 0 and A.nnz == B.nnz
+
+
+def test_nearest_matrix_exact_ties():
+    g = np.array([[i, j, k] for i in range(6) for j in range(6) for k in range(6)], float) * 0.1
+    f = np.concatenate([g[:-1] + 0.05, g + [0.05, 0, 0], g])
+    A, B = nearest_matrix(g, f), nk.nearestMatrix(g, f)
+    assert (A != B).nnz == 0
+    assert B.getnnz(axis=1).max() == 8  # cell centres tie with 8 corners
+
+
+def test_sphere_nearest_matches_oracle():
+    c, f = sphere(1.0, [0, 0, 0], 10), sphere(1.0, [0, 0, 0], 40)
+    assert (nearest_matrix(c, f) != nk.nearestMatrix(c, f)).nnz == 0
+
+
+def test_max_depth_error_message():
+    x = np.array([[0, 0, 0], [1e-9, 0, 0], [1, 1, 1]], float)
+    with pytest.raises(nk.MaxDepthError, match="Max level reached: Increase Max Depth"):
+        nk.OcTree(x, x, nodeCapacity=1, maxDepth=8)
+
+
+def test_capacity_clamped_to_points_minus_one():
+    x = np.random.default_rng(0).random((10, 3))
+    t = nk.OcTree(x, x, nodeCapacity=200)
+    assert t.nodeCapacity == 9 and t.nodeCount >= 9  # root always divides (OcTree.m:105)
+
+
+def test_bad_inputs_rejected():
+    x = np.random.default_rng(0).random((10, 3))
+    with pytest.raises(nk.NNKError):
+        nk.OcTree(np.vstack([x, x[:1]]), np.vstack([x, x[:1]]))  # duplicate potential rows
+    y = x.copy()
+    y[3, 1] = np.nan
+    with pytest.raises(nk.NNKError):
+        nk.OcTree(y, y)
+    with pytest.raises(nk.NNKError):  # NEAREST needs targets == potentials
+        nk.OcTree(x, x[:5], nearest=1, finePoints=x)
