@@ -1,0 +1,333 @@
+"""Benchmark: KIFMM matvec at scale (250k force / 1M quadrature points,
+NEAREST, eps = 1e-3, nodeCapacity 64, p = 6) on the B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one computeVel (KIFMM.m:63-105) of the whole workload with the
+forces already resident on the device.  `value` is target points per second
+over all ranks (weak scaling: every rank runs its own replica; the FMM path
+has no exchange step, so there is no collective on the data path).  `e2e`
+is the same matvec through the C ABI with pinned host buffers, the
+host->device copy of the forces and device->host copy of the velocities
+inside the timed region.  L2 is flushed (256 MiB write) between timed steps,
+outside the per-step CUDA events.
+
+--impl reference times the reference algorithm's CPU restatement (the FP64
+oracle, per-node LU as the MATLAB passes do) on a bounded sample of the same
+workload on the host cores; MATLAB itself is not installable here.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "stokes-nnkifmm_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "mobility solves/s & FMM matvec pts/s, mixed+batched vs plain FP64 GPU at ≤1e-4 err"
+WORKLOAD = ("FMM matvec at scale: 250k force / 1M quadrature points (50% uniform in the unit cube, 50% on "
+            "20 spheres r=0.05-0.2), NEAREST, eps=1e-3, mu=1, nodeCapacity 64, p=6")
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SIMT FP32 FMA pipes at max clock
+FLOPS_PER_PAIR = 32  # regularized Stokeslet pair: 3 sub, 5 r^2, 1 +eps^2, 1 rsqrt, 2 cube, 5 r.f, 3 scale, 12 acc
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--n-force", type=int, default=250_000)
+    ap.add_argument("--n-quad", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-errors", action="store_true")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def build(nk, w, precision):
+    NN = nk.nearestMatrix(w["coarse"], w["fine"])
+    tree = nk.OcTree(w["coarse"], w["coarse"], nodeCapacity=w["cap"], nearest=1, finePoints=w["fine"], NN=NN)
+    fmm = nk.KIFMM(tree, [w["eps"], w["mu"]], precision=precision)
+    return NN, tree, fmm
+
+
+def time_device(torch, fmm, fin, fout, steps, warmup, flush, prof=False):
+    st = torch.cuda.current_stream()
+    for _ in range(warmup):
+        fmm.apply_raw(fin.data_ptr(), fout.data_ptr())
+    torch.cuda.synchronize()
+    if prof:
+        fmm.profile(True)
+        fmm.profile_read()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for a, b in evs:
+        flush.zero_()
+        a.record(st)
+        fmm.apply_raw(fin.data_ptr(), fout.data_ptr())
+        b.record(st)
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    prof_out = None
+    if prof:
+        prof_out = fmm.profile_read()
+        fmm.profile(False)
+    return ms, prof_out
+
+
+def sampled_direct(torch, w, NN, idx):
+    """FP64 direct sum S(fine -> coarse[idx]) * (NN f) on the device."""
+    g = torch.tensor(NN @ w["forces"], device="cuda")
+    src = torch.tensor(w["fine"], device="cuda")
+    tgt = torch.tensor(w["coarse"][idx], device="cuda")
+    e2 = w["eps"] ** 2
+    out = torch.zeros((len(idx), 3), dtype=torch.float64, device="cuda")
+    for s in range(0, src.shape[0], 8192):
+        r = tgt[:, None, :] - src[None, s:s + 8192, :]
+        r2 = (r * r).sum(-1)
+        inv3 = (r2 + e2) ** -1.5
+        gg = g[s:s + 8192]
+        out += ((r2 + 2 * e2) * inv3) @ gg + ((r * gg[None]).sum(-1) * inv3)[..., None].mul(r).sum(1)
+    return (out / (8 * np.pi * w["mu"])).cpu().numpy()
+
+
+def cpu_baseline_sample(n_force, n_quad, steps=1):
+    """The oracle (reference structure, per-node LU, FP64 numpy, 1 thread) on a
+    reduced instance of the same workload distribution; returns pts/s."""
+    from threadpoolctl import threadpool_limits
+
+    from nnkifmm.workloads import matvec_at_scale
+    from oracle.kifmm import KIFMM as OKIFMM
+    from oracle.nearest import nearest_matrix
+    from oracle.octree import OcTree as OTree
+    w = matvec_at_scale(n_force, n_quad)
+    NN = nearest_matrix(w["coarse"], w["fine"])
+    tree = OTree(w["coarse"], w["coarse"], node_capacity=w["cap"], nearest=1, fine_points=w["fine"], NN=NN)
+    fmm = OKIFMM(tree, w["eps"], w["mu"])
+    times = []
+    with threadpool_limits(1):
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            fmm.compute_vel(w["forces"])
+            times.append(time.perf_counter() - t0)
+    return n_force / float(np.median(times)), float(np.median(times)), tree.node_count
+
+
+def reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    nf, nq = 1000, 4000
+    for _ in range(args.warmup):
+        cpu_baseline_sample(nf, nq)
+    vals, secs = [], []
+    for _ in range(args.steps):
+        v, s, nodes = cpu_baseline_sample(nf, nq)
+        vals.append(v)
+        secs.append(s)
+    value = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(secs)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": f"{nf} force / {nq} quadrature points, same distribution"},
+            "cpu_baseline": {"value": value, "unit": "pts/s", "cores": 1, "kind": "port",
+                             "sample": f"oracle KIFMM (reference per-node LU structure) on {nf} force / {nq} "
+                                       f"quadrature points ({nodes} nodes); MATLAB is not installable here"},
+            "e2e": {"value": value, "unit": "pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args)
+    if args.impl == "reference":
+        reference_arm(args, ws, rank)
+        barrier(ws)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    import nnkifmm as nk
+    from nnkifmm.workloads import matvec_at_scale
+    nk.context(local).set_stream(torch.cuda.current_stream(local).cuda_stream)
+    t0 = time.time()
+    w = matvec_at_scale(args.n_force, args.n_quad)
+    NN, tree, fmm = build(nk, w, args.precision)
+    setup_s = time.time() - t0
+    stats = fmm.stats()
+    fin = torch.tensor(w["forces"], device="cuda").contiguous()
+    fout = torch.empty_like(fin)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    clocks = Clocks(local)
+
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    ms, prof = time_device(torch, fmm, fin, fout, args.steps, args.warmup, flush, prof=True)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    step_ms = allmax(ws, float(np.mean(ms)))
+    value = ws * args.n_force / (step_ms / 1e3)
+    gpu_launches = int(sum(n for _, n in prof.values()))
+
+    # e2e: pinned host buffers through the C ABI (H2D + matvec + D2H per step)
+    hin = torch.tensor(w["forces"]).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        fmm.apply_raw(hin.data_ptr(), hout.data_ptr(), on_device=0)
+    st = torch.cuda.current_stream()
+    e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        fmm.apply_raw(hin.data_ptr(), hout.data_ptr(), on_device=0)
+        b.record(st)
+        torch.cuda.synchronize()
+        e_ms.append(a.elapsed_time(b))
+    e2e_ms = allmax(ws, float(np.mean(e_ms)))
+    e2e = {"value": ws * args.n_force / (e2e_ms / 1e3), "unit": "pts/s", "ms_per_step": e2e_ms,
+           "h2d_bytes_per_step": int(hin.numel() * 8), "d2h_bytes_per_step": int(hout.numel() * 8)}
+
+    # roofline of the dominant phase (live CUDA events over the timed region)
+    peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
+    per_step = {k: (v[0] / args.steps, v[1] / args.steps) for k, v in prof.items()}
+    dom = max((k for k in per_step if per_step[k][1] > 0), key=lambda k: per_step[k][0])
+    pairs = {"up_pairs": stats["pairs_up"], "down_pairs": stats["pairs_down"], "leaf_pairs": stats["pairs_leaf"]}
+    if dom in pairs:
+        flops = pairs[dom] * FLOPS_PER_PAIR
+        fp64 = args.precision == "fp64"
+        peak = FP32_NOMINAL_TFLOPS / (2 if fp64 else 1)
+        roof = {"kernel": f"p2p_kernel ({dom})", "bound": "fp64" if fp64 else "fp32",
+                "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "peak_source": "nominal SIMT FP32 (148 SM x 128 lanes x 2 x 1.965 GHz); MEASURED_PEAKS.json "
+                               "holds only HBM and bf16 tensor figures",
+                "launches_per_step": per_step[dom][1], "ms_per_launch": per_step[dom][0] / per_step[dom][1],
+                "algorithmic": f"{pairs[dom]} pairs x {FLOPS_PER_PAIR} flops per step", "traffic": None}
+    else:
+        n = 3 * stats["surface_points"]
+        flops = 2.0 * n * n * stats["c2e_columns"]
+        roof = {"kernel": f"c2e_kernel ({dom})", "bound": "fp64", "achieved": flops / (per_step[dom][0] / 1e3) / 1e12,
+                "peak": FP32_NOMINAL_TFLOPS / 2, "unit": "TFLOP/s", "traffic": None}
+    roof["frac"] = roof["achieved"] / roof["peak"]
+    roof["phases_ms_per_step"] = {k: round(v[0], 4) for k, v in per_step.items()}
+    if peaks:
+        roof["hbm_measured_gbs"] = peaks.get("hbm_gbs")
+
+    line = {"metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": args.precision, "parallelism": f"replicas x{ws}",
+                       "l2": "flushed between timed steps (256 MiB write, outside the step events)",
+                       "nodes": tree.nodeCount, "levels": int(tree.info.max_level) + 1,
+                       "m2l_pairs": stats["m2l_pairs"], "setup_s": round(setup_s, 2)},
+            "roofline": roof, "e2e": e2e, "gpu_launches": gpu_launches * args.steps // max(args.steps, 1),
+            "gpu_launches_per_step": gpu_launches / args.steps, "clocks": clk}
+
+    if rank == 0 and not args.no_errors:
+        rng = np.random.default_rng(7)
+        idx = np.sort(rng.choice(args.n_force, 4096, replace=False))
+        ref = sampled_direct(torch, w, NN, idx)
+        v = fout.cpu().numpy()
+        other = nk.KIFMM(tree, [w["eps"], w["mu"]], precision="fp64" if args.precision == "mixed" else "mixed")
+        fo = torch.empty_like(fin)
+        ms2, _ = time_device(torch, other, fin, fo, max(3, args.steps // 2), 2, flush)
+        v2 = fo.cpu().numpy()
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        mine, oth = ("mixed", "fp64") if args.precision == "mixed" else ("fp64", "mixed")
+        line["errors"] = {f"{mine}_vs_direct_4096": rel(v[idx], ref), f"{oth}_vs_direct_4096": rel(v2[idx], ref),
+                          "mixed_vs_fp64": rel(v if mine == "mixed" else v2, v2 if mine == "mixed" else v)}
+        line[f"{oth}_gpu"] = {"value": args.n_force / (float(np.mean(ms2)) / 1e3), "ms_per_step": float(np.mean(ms2))}
+    if rank == 0 and not args.no_cpu_baseline:
+        v, s, nodes = cpu_baseline_sample(1500, 6000)
+        line["cpu_baseline"] = {"value": v, "unit": "pts/s", "cores": 1, "kind": "port",
+                                "sample": f"oracle KIFMM (reference per-node LU structure, numpy FP64, 1 thread) "
+                                          f"on 1500 force / 6000 quadrature points of the same distribution "
+                                          f"({nodes} nodes), {s:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    barrier(ws)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

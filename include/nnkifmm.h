@@ -183,6 +183,23 @@ int nnk_fmm_reduced_apply(nnk_fmm* fmm, const double* in, double* out,
 int nnk_fmm_reduced_solve(nnk_fmm* fmm, const double* in, double* out,
                           int32_t layout, int32_t on_device);
 int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats);
+
+/* Per-phase device timing of later applies (no counterpart in the reference;
+ * it replaces the tic/toc around whole solves, DirectMethodComparison.m:25-29).
+ * enable != 0 records CUDA events around every kernel phase on the context
+ * stream; nnk_fmm_profile_read returns accumulated milliseconds and launch
+ * counts per phase (NNK_PHASE_*) since the last reset, then resets. */
+#define NNK_PHASE_GATHER 0
+#define NNK_PHASE_UP_PAIRS 1
+#define NNK_PHASE_UP_C2E 2
+#define NNK_PHASE_DOWN_PAIRS 3
+#define NNK_PHASE_DOWN_C2E 4
+#define NNK_PHASE_LEAF_PAIRS 5
+#define NNK_PHASE_SCATTER 6
+#define NNK_PHASE_M2L 7
+#define NNK_NUM_PHASES 8
+int nnk_fmm_profile(nnk_fmm* fmm, int32_t enable);
+int nnk_fmm_profile_read(nnk_fmm* fmm, double* ms, int64_t* launches);
 int nnk_fmm_destroy(nnk_fmm* fmm);
 
 /* Device GMRES on the FMM operator: solves computeVel(x) = b, the resistance

@@ -281,6 +281,21 @@ int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats) {
   return NNK_OK;
 }
 
+int nnk_fmm_profile(nnk_fmm* fmm, int32_t enable) {
+  if (!fmm) return NNK_E_ARG;
+  fmm->f->set_profile(enable != 0);
+  return NNK_OK;
+}
+
+int nnk_fmm_profile_read(nnk_fmm* fmm, double* ms, int64_t* launches) {
+  if (!fmm) return NNK_E_ARG;
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  fmm->f->read_profile(ms, launches);
+  API_CATCH(ctx)
+}
+
 int nnk_fmm_destroy(nnk_fmm* fmm) {
   if (!fmm) return NNK_E_ARG;
   if (fmm->ctx && fmm->ctx->has_gpu) cudaSetDevice(fmm->ctx->device);

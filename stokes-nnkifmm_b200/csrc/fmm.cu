@@ -96,6 +96,59 @@ Fmm::Fmm(nnk_ctx* ctx, const HostTree* tree, const FmmParams& p) : ctx_(ctx), t_
 
 Fmm::~Fmm() {
   if (blas_) cublasDestroy((cublasHandle_t)blas_);
+  for (auto& r : recs_) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : pool_) cudaEventDestroy(e);
+}
+
+cudaEvent_t Fmm::event() {
+  if (!pool_.empty()) {
+    cudaEvent_t e = pool_.back();
+    pool_.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  NNK_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+template <typename F>
+void Fmm::phase(int ph, F&& launch) {
+  if (!prof_) {
+    launch();
+    launches_[ph]++;
+    return;
+  }
+  PhaseRec r{ph, event(), event()};
+  NNK_CUDA(cudaEventRecord(r.a, ctx_->stream));
+  launch();
+  NNK_CUDA(cudaEventRecord(r.b, ctx_->stream));
+  recs_.push_back(r);
+  launches_[ph]++;
+}
+
+void Fmm::set_profile(bool on) {
+  prof_ = on;
+  if (sparse_) sparse_->set_profile(on);
+}
+
+void Fmm::read_profile(double* ms, int64_t* launches) {
+  NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
+  for (int k = 0; k < NNK_NUM_PHASES; ++k) {
+    if (ms) ms[k] = 0;
+    if (launches) launches[k] = launches_[k];
+    launches_[k] = 0;
+  }
+  for (auto& r : recs_) {
+    float t = 0;
+    NNK_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+    if (ms) ms[r.ph] += t;
+    pool_.push_back(r.a);
+    pool_.push_back(r.b);
+  }
+  recs_.clear();
 }
 
 Fmm& Fmm::sparse() {
@@ -381,31 +434,40 @@ void Fmm::apply_impl(const double* d_in, double* d_out, int layout) {
   const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
   const int n = 3 * P_;
   // forces on the leaf source entries (kron(NN,I3)*f per leaf)
-  launch_gather<Real>(E_, goff_.p, gidx_.p, gw_.p, d_in, layout, t.n_pot, str, st);
+  phase(NNK_PHASE_GATHER, [&] { launch_gather<Real>(E_, goff_.p, gidx_.p, gw_.p, d_in, layout, t.n_pot, str, st); });
   // expansions of nodes that are not computed stay zero
   NNK_CUDA(cudaMemsetAsync(str + 3 * E_, 0, sizeof(Real) * 3 * (size_t)P_ * N_, st));
   NNK_CUDA(cudaMemsetAsync(str + 3 * (E_ + (size_t)P_ * N_), 0, sizeof(Real) * 3 * (size_t)P_, st));
   // upward pass
   for (int L = maxl_; L >= 1; --L) {
     if (up_[L].count == 0) continue;
-    launch_p2p<Real>(tasks_.p + up_[L].first, (int)up_[L].count, segs_.p, pos, str, pos, check, e2, scale, st);
+    phase(NNK_PHASE_UP_PAIRS, [&] {
+      launch_p2p<Real>(tasks_.p + up_[L].first, (int)up_[L].count, segs_.p, pos, str, pos, check, e2, scale, st);
+    });
     const int64_t nn = up_off_[L + 1] - up_off_[L];
-    launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 0, up_nodes_.p + up_off_[L], (int)nn, check,
-                     str, E_, P_, st);
+    phase(NNK_PHASE_UP_C2E, [&] {
+      launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 0, up_nodes_.p + up_off_[L], (int)nn, check, str, E_, P_, st);
+    });
   }
   // downward pass
   for (int L = 1; L <= maxl_; ++L) {
     if (down_[L].count == 0) continue;
-    launch_p2p<Real>(tasks_.p + down_[L].first, (int)down_[L].count, segs_.p, pos, str, pos, check, e2,
-                     scale, st);
+    phase(NNK_PHASE_DOWN_PAIRS, [&] {
+      launch_p2p<Real>(tasks_.p + down_[L].first, (int)down_[L].count, segs_.p, pos, str, pos, check, e2, scale, st);
+    });
     const int64_t nn = lvl_off_[L + 1] - lvl_off_[L];
-    launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 1, lvl_nodes_.p + lvl_off_[L], (int)nn, check, str,
-                     E_ + (int64_t)P_ * N_, P_, st);
+    phase(NNK_PHASE_DOWN_C2E, [&] {
+      launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 1, lvl_nodes_.p + lvl_off_[L], (int)nn, check, str,
+                       E_ + (int64_t)P_ * N_, P_, st);
+    });
   }
   // leaf stage
   if (leaf_.count)
-    launch_p2p<Real>(tasks_.p + leaf_.first, (int)leaf_.count, segs_.p, pos, str, tpos, vel, e2, scale, st);
-  launch_scatter<Real>((int64_t)t.tgt_row.size(), trow_.p, vel, layout, t.n_tgt, d_out, st);
+    phase(NNK_PHASE_LEAF_PAIRS, [&] {
+      launch_p2p<Real>(tasks_.p + leaf_.first, (int)leaf_.count, segs_.p, pos, str, tpos, vel, e2, scale, st);
+    });
+  phase(NNK_PHASE_SCATTER,
+        [&] { launch_scatter<Real>((int64_t)t.tgt_row.size(), trow_.p, vel, layout, t.n_tgt, d_out, st); });
 }
 
 void Fmm::apply(const double* d_in, double* d_out, int layout, int nrhs) {

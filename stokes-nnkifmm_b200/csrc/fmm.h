@@ -54,6 +54,9 @@ class Fmm {
   void reduced_apply(const double* d_in, double* d_out, int layout);
   void reduced_solve(const double* d_in, double* d_out, int layout);
   nnk_fmm_stats stats() const { return stats_; }
+  // per-phase CUDA-event timing (NNK_PHASE_*)
+  void set_profile(bool on);
+  void read_profile(double* ms, int64_t* launches);
   const HostTree& tree() const { return *t_; }
   nnk_ctx* ctx() const { return ctx_; }
   const FmmParams& params() const { return p_; }
@@ -120,6 +123,13 @@ class Fmm {
   DBuf<int64_t> rts_;            // tgt_start on the device
   void* blas_ = nullptr;         // cublasHandle_t for the batched leaf solves
   nnk_fmm_stats stats_{};
+  template <typename F> void phase(int ph, F&& launch);
+  struct PhaseRec { int ph; cudaEvent_t a, b; };
+  bool prof_ = false;
+  std::vector<PhaseRec> recs_;
+  std::vector<cudaEvent_t> pool_;
+  int64_t launches_[NNK_NUM_PHASES] = {0};
+  cudaEvent_t event();
   std::unique_ptr<Fmm> sparse_;
 };
 

@@ -24,6 +24,7 @@ LAYOUT_ROWS = 1
 LAYOUT_BLOCKED = 2
 PREC_FP64 = 0
 PREC_MIXED = 1
+PHASES = ["gather", "up_pairs", "up_c2e", "down_pairs", "down_c2e", "leaf_pairs", "scatter", "m2l"]
 
 _i32, _i64, _f64, _vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
 _pd, _pi32, _pi64, _pu8 = (C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
@@ -82,6 +83,8 @@ SIGNATURES = {
     "nnk_fmm_reduced_solve": (_i32, [_vp, _vp, _vp, _i32, _i32]),
     "nnk_fmm_stats_get": (_i32, [_vp, C.POINTER(FmmStats)]),
     "nnk_fmm_destroy": (_i32, [_vp]),
+    "nnk_fmm_profile": (_i32, [_vp, _i32]),
+    "nnk_fmm_profile_read": (_i32, [_vp, _vp, _vp]),
     "nnk_fmm_solve": (_i32, [_vp, _vp, _vp, _i32, C.POINTER(SolveParams), C.POINTER(SolveInfo), _i32]),
     "nnk_mob_create": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, C.POINTER(_vp)]),
     "nnk_mob_apply": (_i32, [_vp, _vp, _vp, _i32]),

@@ -96,6 +96,22 @@ class KIFMM:
         L.check(L.lib.nnk_fmm_stats_get(self.h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in L.FmmStats._fields_}
 
+    def profile(self, enable=True):
+        """Per-phase CUDA-event timing of later computeVel calls."""
+        L.check(L.lib.nnk_fmm_profile(self.h, int(bool(enable))))
+
+    def profile_read(self):
+        """{phase: (milliseconds, launches)} accumulated since the last read."""
+        ms = np.zeros(len(L.PHASES))
+        n = np.zeros(len(L.PHASES), np.int64)
+        L.check(L.lib.nnk_fmm_profile_read(self.h, L.ptr(ms), L.ptr(n)), self.ctx.h)
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(L.PHASES)}
+
+    def apply_raw(self, d_in, d_out, layout=L.LAYOUT_ROWS, on_device=1, nrhs=1):
+        """computeVel on raw pointers (device or pinned host) without any
+        Python-side staging; used by the benchmark."""
+        L.check(L.lib.nnk_fmm_apply(self.h, d_in, d_out, layout, nrhs, on_device), self.ctx.h, "computeVel")
+
     def gmres(self, b, tol=1e-6, maxit=None, restart=0):
         """gmres(@(x) fmm.computeVel(x), b, [], tol, maxit) on the device
         (Data Generation/DirectMethodComparison.m:28).  Returns

@@ -1,0 +1,42 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+matvec_at_scale: 250k force points (half uniform in [0,1]^3, half on the
+surfaces of 20 spheres with centres U[0.2,0.8]^3 and radii U[0.05,0.2]) and
+1M quadrature points drawn the same way on the same spheres; forces
+N(0,1); eps = 1e-3, mu = 1, nodeCapacity 64, p = 6.
+sphere: the single-sphere mobility case (Sphere(1,[0 0 0],10) force nodes,
+Sphere(...,40) quadrature, eps = 0.01, nodeCapacity 60).
+"""
+import numpy as np
+
+
+def cube_sphere(r, centre, n):
+    """Cube-surface lattice projected radially onto a sphere, n points per edge
+    (the construction of Geometries/Sphere.m, n^3-(n-2)^3 points)."""
+    lin = np.linspace(-r, r, n)
+    k, i, j = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    j, i, k = j.ravel(), i.ravel(), k.ravel()
+    shell = (j == 0) | (j == n - 1) | (i == 0) | (i == n - 1) | (k == 0) | (k == n - 1)
+    X, Y, Z = lin[i[shell]], lin[j[shell]], lin[k[shell]]
+    az = np.arctan2(Y, X)
+    el = np.arctan2(Z, np.sqrt(X ** 2 + Y ** 2))
+    return np.stack([r * np.cos(el) * np.cos(az) + centre[0], r * np.cos(el) * np.sin(az) + centre[1],
+                     r * np.sin(el) + centre[2]], axis=1)
+
+
+def mixed_cloud(rng, n, centres, radii):
+    u = rng.random((n // 2, 3))
+    d = rng.standard_normal((n - n // 2, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    k = rng.integers(0, len(centres), n - n // 2)
+    return np.concatenate([u, centres[k] + radii[k, None] * d])
+
+
+def matvec_at_scale(n_force=250_000, n_quad=1_000_000, n_spheres=20, seed=20261204):
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(0.2, 0.8, (n_spheres, 3))
+    radii = rng.uniform(0.05, 0.2, n_spheres)
+    coarse = mixed_cloud(rng, n_force, centres, radii)
+    fine = mixed_cloud(rng, n_quad, centres, radii)
+    forces = rng.standard_normal((n_force, 3))
+    return dict(coarse=coarse, fine=fine, forces=forces, eps=1e-3, mu=1.0, cap=64)
