@@ -66,7 +66,13 @@ class KIFMM:
         if extra:
             args.append(nrhs)
         args.append(dev)
+        if is_t:
+            # the library works on its context stream: order it after torch's
+            # producers of xin, and torch's consumers of out after it
+            torch.cuda.current_stream(xin.device).synchronize()
         L.check(fn(*args), self.ctx.h)
+        if is_t:
+            self.ctx.synchronize()
         if gm:
             return out if nrhs == 1 else out.reshape(nrhs, -1)
         return out.reshape(n_out, 3) if nrhs == 1 else out.reshape(nrhs, n_out, 3)
