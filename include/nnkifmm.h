@@ -228,6 +228,29 @@ int nnk_mob_solve(nnk_mob* mob, const double* rhs, double* x,
                   nnk_solve_info* info, int32_t on_device);
 int nnk_mob_destroy(nnk_mob* mob);
 
+/* ------------------------------------------------- allocation-free call -- */
+/* No counterpart in the reference: an extra entry point for callers that
+ * cannot allocate device memory when they call (during CUDA graph capture,
+ * inside a MEX gateway whose device memory MATLAB owns, or in a loop with a
+ * fixed memory budget).  It evaluates the NEAREST velocity by direct
+ * summation, vel(t) = S(fine -> t) * kron(NN,I3) * forces, the dense product
+ * of nearestBlockComputation.m, with every input and output a device pointer
+ * supplied by the caller (forces n x 3, NN CSR by fine point with 0-based
+ * columns into forces, fine q x 3, targets m x 3, vel m x 3, row-major FP64),
+ * issued on `stream`.  Its one scratch buffer, the fine-point forces, is a
+ * static device array of NNK_NOALLOC_MAX_FINE rows that every GPU loading the
+ * library holds until exit; larger q is rejected with NNK_E_ARG.  The first
+ * call on a device looks up that array's address and should come before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU race.
+ * Returns without synchronizing. */
+#define NNK_NOALLOC_MAX_FINE 262144
+int nnk_direct_nearest_noalloc(int32_t device, void* stream, const double* forces,
+                               int64_t n, const int64_t* nn_rowptr,
+                               const int32_t* nn_col, const double* nn_val,
+                               const double* fine, int64_t q,
+                               const double* targets, int64_t m, double eps,
+                               double mu, double* vel);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,7 @@ LAYOUT_ROWS = 1
 LAYOUT_BLOCKED = 2
 PREC_FP64 = 0
 PREC_MIXED = 1
+NOALLOC_MAX_FINE = 262144
 PHASES = ["gather", "up_pairs", "up_c2e", "down_pairs", "down_c2e", "leaf_pairs", "scatter", "m2l"]
 
 _i32, _i64, _f64, _vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
@@ -91,6 +92,8 @@ SIGNATURES = {
     "nnk_mob_precon": (_i32, [_vp, _vp, _vp, _i32]),
     "nnk_mob_solve": (_i32, [_vp, _vp, _vp, C.POINTER(SolveParams), _i32, C.POINTER(SolveInfo), _i32]),
     "nnk_mob_destroy": (_i32, [_vp]),
+    "nnk_direct_nearest_noalloc": (_i32, [_i32, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _i64, _f64, _f64,
+                                          _vp]),
 }
 
 
