@@ -271,7 +271,19 @@ def main():
     per_step = {k: (v[0] / args.steps, v[1] / args.steps) for k, v in prof.items()}
     dom = max((k for k in per_step if per_step[k][1] > 0), key=lambda k: per_step[k][0])
     pairs = {"up_pairs": stats["pairs_up"], "down_pairs": stats["pairs_down"], "leaf_pairs": stats["pairs_leaf"]}
-    if dom in pairs:
+    if dom == "m2l":
+        n3 = 3 * stats["surface_points"]
+        flops = 2.0 * n3 * n3 * stats["m2l_pairs"]
+        tf32_peak = peaks.get("bf16_tflops", 1590.0) / 2
+        roof = {"kernel": "m2l_tf32_kernel (tcgen05 kind::tf32, TMEM accumulator)", "bound": "tensor",
+                "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": tf32_peak, "unit": "TFLOP/s",
+                "peak_source": "TF32 dense = 1/2 of the measured cuBLAS bf16 burst peak in MEASURED_PEAKS.json"
+                               if peaks else "TF32 dense = 1/2 of the fallback bf16 peak",
+                "algorithmic": f"{stats['m2l_pairs']} V pairs x 2 x {n3}^2 flops per step (useful, no padding)",
+                "padded_rows_over_useful": stats["m2l_tile_rows"] / max(stats["m2l_pairs"], 1),
+                "launches_per_step": per_step[dom][1], "ms_per_launch": per_step[dom][0] / per_step[dom][1],
+                "traffic": None}
+    elif dom in pairs:
         flops = pairs[dom] * FLOPS_PER_PAIR
         fp64 = args.precision == "fp64"
         peak = FP32_NOMINAL_TFLOPS / (2 if fp64 else 1)
@@ -285,6 +297,7 @@ def main():
         n = 3 * stats["surface_points"]
         flops = 2.0 * n * n * stats["c2e_columns"]
         roof = {"kernel": f"c2e_kernel ({dom})", "bound": "fp64", "achieved": flops / (per_step[dom][0] / 1e3) / 1e12,
+                "algorithmic": "2 x (3P)^2 flops per node per pass",
                 "peak": FP32_NOMINAL_TFLOPS / 2, "unit": "TFLOP/s", "traffic": None}
     roof["frac"] = roof["achieved"] / roof["peak"]
     roof["phases_ms_per_step"] = {k: round(v[0], 4) for k, v in per_step.items()}

@@ -89,7 +89,7 @@ typedef struct nnk_fmm_params {
   int32_t precision;     /* NNK_PREC_FP64 or NNK_PREC_MIXED                    */
   int32_t reserved;
   double reg;            /* relative Tikhonov weight of the check-to-equivalent
-                            pseudo-inverse in NNK_PREC_MIXED (0 = default)      */
+                            pseudo-inverse in NNK_PREC_MIXED (0 = default 1e-5) */
 } nnk_fmm_params;
 
 /* Algorithmic work of one matvec, from the tree statistics (for rooflines). */
@@ -100,6 +100,7 @@ typedef struct nnk_fmm_stats {
   int64_t pairs_down;   /* M2L + P2L + L2L pairs (pair-kernel form)            */
   int64_t m2l_pairs;    /* V-list (target node, source node) pairs             */
   int64_t c2e_columns;  /* check-to-equivalent applications (up + down)        */
+  int64_t m2l_tile_rows; /* tensor-core M2L rows processed, padding included     */
   int32_t surface_points;
   int32_t levels;
 } nnk_fmm_stats;

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <array>
+#include <type_traits>
 #include <cmath>
 #include <cstring>
 
@@ -136,6 +137,7 @@ void Fmm::set_profile(bool on) {
 
 void Fmm::read_profile(double* ms, int64_t* launches) {
   NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
+  if (tensor_m2l_) check_m2l_error(m2l_, ctx_->stream);
   for (int k = 0; k < NNK_NUM_PHASES; ++k) {
     if (ms) ms[k] = 0;
     if (launches) launches[k] = launches_[k];
@@ -266,6 +268,20 @@ void Fmm::build_tasks() {
   }
   // downward pass (downwardPass.m:39-168): every node of levels 1..max.
   // The root's downward expansion is zero, so its L2L term is dropped.
+  // Two task sets: with the V-list as pair segments (FP64 mode), and without
+  // it (mixed mode, where M2L runs on the tensor cores before the pass).
+  down_nov_.assign(maxl_ + 1, {});
+  for (int L = 1; L <= maxl_; ++L) {
+    down_nov_[L].first = (int64_t)tasks.size();
+    for (int32_t n : t.by_level[L]) {
+      TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
+      for (int64_t k = t.X.off[n]; k < t.X.off[n + 1]; ++k) src_seg(t.X.idx[k]);
+      if (t.parent[n] > 0) segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
+      tk.nseg = (int)segs.size() - tk.seg0;
+      tasks.push_back(tk);
+    }
+    down_nov_[L].count = (int64_t)tasks.size() - down_nov_[L].first;
+  }
   for (int L = 1; L <= maxl_; ++L) {
     down_[L].first = (int64_t)tasks.size();
     for (int32_t n : t.by_level[L]) {
@@ -333,6 +349,11 @@ void Fmm::build_tasks() {
 
 void Fmm::build_operators() {
   const HostTree& t = *t_;
+  if (p_.precision == NNK_PREC_MIXED) {
+    build_m2l_plan(t, p_.res, p_.shells, p_.eps, p_.mu, m2l_, ctx_->stream);
+    tensor_m2l_ = true;
+    stats_.m2l_tile_rows = m2l_.tile_slots * 128;
+  }
   const int n = 3 * P_;
   const double W0 = t.corners[3] - t.corners[0];
   cudaStream_t st = ctx_->stream;
@@ -394,7 +415,7 @@ void Fmm::build_operators() {
           for (double& x : v) x /= nu;
         }
       }
-      const double reg = p_.reg > 0 ? p_.reg : 1e-8;
+      const double reg = p_.reg > 0 ? p_.reg : 1e-5;
       const double lam2 = (reg * smax) * (reg * smax);
       for (int r = 0; r < n; ++r)
         for (int c = 0; c < n; ++c) KT[(size_t)c * n + r] = K[(size_t)r * n + c];
@@ -438,6 +459,9 @@ void Fmm::apply_impl(const double* d_in, double* d_out, int layout) {
   // expansions of nodes that are not computed stay zero
   NNK_CUDA(cudaMemsetAsync(str + 3 * E_, 0, sizeof(Real) * 3 * (size_t)P_ * N_, st));
   NNK_CUDA(cudaMemsetAsync(str + 3 * (E_ + (size_t)P_ * N_), 0, sizeof(Real) * 3 * (size_t)P_, st));
+  const bool tm = tensor_m2l_ && std::is_same<Real, float>::value;
+  if (tm && m2l_.h_err && *m2l_.h_err)
+    throw Error(NNK_E_TIMEOUT, "tensor-core M2L gave up a bounded wait in an earlier call");
   // upward pass
   for (int L = maxl_; L >= 1; --L) {
     if (up_[L].count == 0) continue;
@@ -446,14 +470,22 @@ void Fmm::apply_impl(const double* d_in, double* d_out, int layout) {
     });
     const int64_t nn = up_off_[L + 1] - up_off_[L];
     phase(NNK_PHASE_UP_C2E, [&] {
-      launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 0, up_nodes_.p + up_off_[L], (int)nn, check, str, E_, P_, st);
+      launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 0, up_nodes_.p + up_off_[L], (int)nn, check, str, E_, P_, st,
+                       tm ? m2l_.src.p : nullptr, m2l_.NP);
     });
   }
   // downward pass
+  if (tm) {
+    // M2L of every level at once: the V-list only reads up densities
+    NNK_CUDA(cudaMemsetAsync(check, 0, sizeof(Real) * (size_t)N_ * n, st));
+    phase(NNK_PHASE_M2L, [&] { launch_m2l(m2l_, (float*)check, n, st); });
+  }
+  const std::vector<TaskGroup>& dgroups = tm ? down_nov_ : down_;
   for (int L = 1; L <= maxl_; ++L) {
-    if (down_[L].count == 0) continue;
+    if (dgroups[L].count == 0) continue;
     phase(NNK_PHASE_DOWN_PAIRS, [&] {
-      launch_p2p<Real>(tasks_.p + down_[L].first, (int)down_[L].count, segs_.p, pos, str, pos, check, e2, scale, st);
+      launch_p2p<Real>(tasks_.p + dgroups[L].first, (int)dgroups[L].count, segs_.p, pos, str, pos, check, e2, scale,
+                       st, tm ? 1 : 0);
     });
     const int64_t nn = lvl_off_[L + 1] - lvl_off_[L];
     phase(NNK_PHASE_DOWN_C2E, [&] {

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "common.h"
+#include "m2l.h"
 #include "tree.h"
 
 namespace nnk {
@@ -97,6 +98,9 @@ class Fmm {
   DBuf<TaskD> tasks_;
   DBuf<SegD> segs_;
   std::vector<TaskGroup> up_, down_;  // per level
+  std::vector<TaskGroup> down_nov_;   // per level, without the V-list (M2L on the tensor cores)
+  M2LPlan m2l_;
+  bool tensor_m2l_ = false;
   TaskGroup leaf_;
   DBuf<int32_t> lvl_nodes_;
   std::vector<int64_t> lvl_off_;

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
                                                  const Real* __restrict__ spos,
                                                  const Real* __restrict__ sstr,
                                                  const Real* __restrict__ tpos, Real* __restrict__ out,
-                                                 Real e2, Real scale) {
+                                                 Real e2, Real scale, int accumulate) {
   __shared__ Real sx[BS], sy[BS], sz[BS], gx[BS], gy[BS], gz[BS];
   __shared__ Real red[3 * BS];
   const TaskD tk = tasks[blockIdx.x];
@@ -135,9 +135,15 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
         vz += red[2 * BS + tid + k * nt];
       }
       const long long o = 3 * (tk.out + t0 + tid);
-      out[o] = scale * vx;
-      out[o + 1] = scale * vy;
-      out[o + 2] = scale * vz;
+      if (accumulate) {
+        out[o] += scale * vx;
+        out[o + 1] += scale * vy;
+        out[o + 2] += scale * vz;
+      } else {
+        out[o] = scale * vx;
+        out[o + 1] = scale * vy;
+        out[o + 2] = scale * vz;
+      }
     }
     __syncthreads();
   }
@@ -145,9 +151,9 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
 
 template <typename Real>
 inline void launch_p2p(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
-                       const Real* tpos, Real* out, Real e2, Real scale, cudaStream_t st) {
+                       const Real* tpos, Real* out, Real e2, Real scale, cudaStream_t st, int accumulate = 0) {
   if (ntasks == 0) return;
-  p2p_kernel<Real, 128><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, e2, scale);
+  p2p_kernel<Real, 128><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, e2, scale, accumulate);
   NNK_CHECK_LAUNCH();
 }
 
@@ -160,7 +166,7 @@ template <typename Real>
 __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ A, int n, int trans,
                                                   const int* __restrict__ nodes, int nnodes,
                                                   const Real* __restrict__ check, Real* __restrict__ dst,
-                                                  long long base, int P) {
+                                                  long long base, int P, float* __restrict__ m2l_dst, int NP) {
   constexpr int BM = 64, BN = 32, BK = 16;
   __shared__ double As[BK][BM + 1];
   __shared__ double Bs[BK][BN + 1];
@@ -206,16 +212,23 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ A, 
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const int r = m0 + tr + 16 * i, jj = n0 + tc + 16 * j;
-      if (r < n && jj < nnodes) dst[(base + (long long)P * nodes[jj]) * 3 + r] = (Real)acc[i][j];
+      if (r < n && jj < nnodes) {
+        dst[(base + (long long)P * nodes[jj]) * 3 + r] = (Real)acc[i][j];
+        if (m2l_dst) {
+          uint32_t t;
+          asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"((float)acc[i][j]));
+          m2l_dst[(size_t)nodes[jj] * NP + r] = __uint_as_float(t);
+        }
+      }
     }
 }
 
 template <typename Real>
 inline void launch_c2e(const double* A, int n, int trans, const int32_t* nodes, int nnodes, const Real* check,
-                       Real* dst, int64_t base, int P, cudaStream_t st) {
+                       Real* dst, int64_t base, int P, cudaStream_t st, float* m2l_dst = nullptr, int NP = 0) {
   if (nnodes == 0) return;
   dim3 grid((n + 63) / 64, (nnodes + 31) / 32);
-  c2e_kernel<Real><<<grid, 256, 0, st>>>(A, n, trans, nodes, nnodes, check, dst, base, P);
+  c2e_kernel<Real><<<grid, 256, 0, st>>>(A, n, trans, nodes, nnodes, check, dst, base, P, m2l_dst, NP);
   NNK_CHECK_LAUNCH();
 }
 

@@ -1,0 +1,420 @@
+// TF32 tcgen05 M2L (see m2l.h).
+//
+// Shared memory per stage (2 stages):
+//   A: 128 rows x 128 B (32 TF32 of K), K-major, 128-byte swizzle
+//   B: NP rows x 128 B, same layout, one bulk copy of a pre-swizzled chunk
+// One thread issues the MMAs (kind::tf32, M = 128, N = NP or NP/2, K = 8 per
+// instruction, four per 32-wide K chunk); all 128 threads gather A rows; the
+// accumulator (128 lanes x NP columns FP32) lives in TMEM.  Every mbarrier
+// wait is bounded; a timeout sets the error flag and the CTA drains and exits.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <map>
+
+#include "m2l.h"
+
+namespace nnk {
+
+namespace {
+
+constexpr int kTileRows = 128;
+constexpr int kSlotsPerUnit = 24;
+constexpr uint32_t kWaitLimit = 1u << 26;  // ~1-3 s of polling
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ float to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on an mbarrier phase; false after kWaitLimit polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+    if (mbar_test(bar, parity)) return true;
+    if (i > 32) __nanosleep(20);
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 B apart (SBO), LBO unused for this layout, descriptor version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+// Instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t tf32_idesc(int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__global__ void __launch_bounds__(128, 1)
+    m2l_tf32_kernel(const M2LUnit* __restrict__ units, const int* __restrict__ tile_nodes,
+                    const int* __restrict__ tile_slot0, const int* __restrict__ slot_op,
+                    const int* __restrict__ slot_src, const float* __restrict__ images,
+                    const float* __restrict__ src, float* __restrict__ check, int ldc, int NP, int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* sbase = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+  const uint32_t A_BYTES = kTileRows * 128, B_BYTES = (uint32_t)NP * 128;
+  uint8_t* sA0 = sbase;
+  uint8_t* sB0 = sbase + 2 * A_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + 2 * A_BYTES + 2 * B_BYTES);  // full[2] done[2] acc
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 5);
+  volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const M2LUnit u = units[blockIdx.x];
+  const int nchunks = NP / 32;
+  const int nhalves = NP > 256 ? 2 : 1;
+  const int nh = NP / nhalves;
+  const uint32_t ncols = NP > 256 ? 512u : 256u;
+  const uint32_t idesc = tf32_idesc(nh);
+
+  if (tid == 0) {
+    for (int k = 0; k < 5; ++k) mbar_init(&bars[k], 1);
+    *abort_s = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0) tmem_alloc(tmem_slot, ncols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int node = tile_nodes[u.tile * kTileRows + tid];
+  const int slot_base = tile_slot0[u.tile] + u.slot0;
+  const int nsteps = u.nslot * nchunks;
+  int issued = 0;  // MMA steps committed
+  int copies = 0;  // B copies issued
+  for (int s = 0; s < nsteps; ++s) {
+    const int st = s & 1;
+    const int slot = slot_base + s / nchunks;
+    const int c = s % nchunks;
+    uint8_t* sA = sA0 + st * A_BYTES;
+    uint8_t* sB = sB0 + st * B_BYTES;
+    // stage st is free once the MMAs of step s-2 are done
+    if (s >= 2 && !mbar_wait(&bars[2 + st], ((s - 2) >> 1) & 1)) {
+      *abort_s = 1;
+      atomicOr(err, 1);
+    }
+    if (tid == 0 && !*abort_s) {
+      mbar_expect_tx(&bars[st], B_BYTES);
+      const float* gB = images + (size_t)slot_op[slot] * ((size_t)nchunks * NP * 32) + (size_t)c * NP * 32;
+      bulk_g2s(sB, gB, B_BYTES, &bars[st]);
+      ++copies;
+    }
+    // A row tid: 32 TF32 values of the source node's density, swizzled
+    const int v = slot_src[(size_t)slot * kTileRows + tid];
+    float4* dA = reinterpret_cast<float4*>(sA + tid * 128);
+    if (v >= 0) {
+      const float4* g4 = reinterpret_cast<const float4*>(src + (size_t)v * NP + c * 32);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) dA[j ^ (tid & 7)] = __ldg(g4 + j);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) dA[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (*abort_s) break;
+    if (tid == 0) {
+      if (!mbar_wait(&bars[st], (s >> 1) & 1)) {
+        *abort_s = 1;
+        atomicOr(err, 2);
+      } else {
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+        for (int k8 = 0; k8 < 4; ++k8)
+          for (int h = 0; h < nhalves; ++h)
+            umma_tf32(tmem + (uint32_t)(h * nh), sw128_desc(a0 + k8 * 32), sw128_desc(b0 + h * nh * 128 + k8 * 32),
+                      idesc, (s > 0 || k8 > 0) ? 1u : 0u);
+        umma_commit(&bars[2 + st]);
+        ++issued;
+      }
+    }
+  }
+  __syncthreads();
+  // drain: every MMA this thread issued completes before acc (commit tracks all)
+  bool acc_ok = true;
+  if (tid == 0) umma_commit(&bars[4]);
+  if (!mbar_wait(&bars[4], 0)) {
+    acc_ok = false;
+    atomicOr(err, 4);
+  }
+  // a B copy issued for a step whose MMA never ran must land before exit
+  if (tid == 0 && copies > issued) {
+    const int s = copies - 1;
+    if (!mbar_wait(&bars[s & 1], (s >> 1) & 1)) atomicOr(err, 8);
+  }
+  tc_fence_after();
+  if (!*abort_s && acc_ok && nsteps > 0) {
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int col = 0; col < NP; col += 16) {
+      float vals[16];
+      tmem_ld16(lane_addr + col, vals);
+      if (node >= 0) {
+        float* dst = check + (size_t)node * ldc;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int c0 = col + 4 * q;
+          if (c0 < ldc)
+            atomicAdd(reinterpret_cast<float4*>(dst + c0), make_float4(vals[4 * q], vals[4 * q + 1],
+                                                                       vals[4 * q + 2], vals[4 * q + 3]));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// T_{L,o}[n = 3a+al][k = 3b+be] = S_al,be(x_a - y_b) / (8 pi mu),
+// x_a = lattice_a * h, y_b = lattice_b * h + o * w, h = w/(res-1), rounded to
+// TF32 and written at its SW128 K-major position of chunk k/32.
+__global__ void m2l_operator_kernel(int nimg, const int* __restrict__ img_code, const double* __restrict__ img_w,
+                                    const int* __restrict__ lat, int P, int res, double eps, double mu, int NP,
+                                    float* __restrict__ images) {
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per = (long long)P * P;
+  if (gid >= per * nimg) return;
+  const int img = (int)(gid / per);
+  const int a = (int)((gid % per) / P), b = (int)(gid % P);
+  const int code = img_code[img];
+  const int ox = code / 49 - 3, oy = (code / 7) % 7 - 3, oz = code % 7 - 3;
+  const double w = img_w[img], h = w / (res - 1);
+  const double r[3] = {(lat[3 * a] - lat[3 * b]) * h - ox * w, (lat[3 * a + 1] - lat[3 * b + 1]) * h - oy * w,
+                       (lat[3 * a + 2] - lat[3 * b + 2]) * h - oz * w};
+  const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+  const double e2 = eps * eps;
+  const double inv = 1.0 / (8.0 * M_PI * mu * (r2 + e2) * sqrt(r2 + e2));
+  uint8_t* base = reinterpret_cast<uint8_t*>(images) + (size_t)img * ((size_t)NP / 32) * NP * 128;
+  for (int al = 0; al < 3; ++al)
+    for (int be = 0; be < 3; ++be) {
+      const double val = (r[al] * r[be] + (al == be ? r2 + 2 * e2 : 0.0)) * inv;
+      const int n = 3 * a + al, k = 3 * b + be;
+      const int c = k >> 5, kl = k & 31, j = kl >> 2, e = kl & 3;
+      float* dst = reinterpret_cast<float*>(base + (size_t)c * NP * 128 + (size_t)n * 128 + ((j ^ (n & 7)) << 4) +
+                                            e * 4);
+      *dst = to_tf32((float)val);
+    }
+}
+
+}  // namespace
+
+M2LPlan::~M2LPlan() {
+  if (h_err) cudaFreeHost(h_err);
+}
+
+void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double mu, M2LPlan& plan,
+                    cudaStream_t st) {
+  // surface lattice (same order as the unified surface points)
+  std::vector<int> lat;
+  auto inner = [&](int a) { return a >= shells && a <= res - 1 - shells; };
+  for (int k = 0; k < res; ++k)
+    for (int i = 0; i < res; ++i)
+      for (int j = 0; j < res; ++j)
+        if (!(inner(j) && inner(i) && inner(k))) {
+          lat.push_back(i);
+          lat.push_back(j);
+          lat.push_back(k);
+        }
+  const int P = (int)lat.size() / 3;
+  const int NP = ((3 * P + 31) / 32) * 32;
+  if (NP > 512 || NP / (NP > 256 ? 2 : 1) % 16 != 0)
+    throw Error(NNK_E_ARG, "tensor-core M2L supports 3P up to 512 with N halves a multiple of 16");
+  plan.NP = NP;
+  const double W0 = t.corners[3] - t.corners[0];
+  std::vector<int> tile_nodes, tile_slot0, slot_op, slot_src;
+  std::vector<M2LUnit> units;
+  std::vector<int> img_code;
+  std::vector<double> img_w;
+  int64_t useful = 0, tslots = 0;
+  for (int L = 1; L <= t.max_level; ++L) {
+    std::vector<int32_t> nodes;
+    for (int32_t n : t.by_level[L])
+      if (t.V.off[n + 1] > t.V.off[n]) nodes.push_back(n);
+    if (nodes.empty()) continue;
+    auto oct = [&](int32_t n) { return ((t.ix[n] & 1) << 2) | ((t.iy[n] & 1) << 1) | (t.iz[n] & 1); };
+    std::stable_sort(nodes.begin(), nodes.end(), [&](int32_t a, int32_t b) { return oct(a) < oct(b); });
+    std::map<int, int> img_of;  // offset code -> image
+    const int first_tile = (int)tile_slot0.size();
+    std::vector<std::vector<int>> tile_groups;  // per tile in this level: slot counts
+    for (size_t t0 = 0; t0 < nodes.size(); t0 += kTileRows) {
+      const int tile = (int)tile_slot0.size();
+      const int rows = (int)std::min<size_t>(kTileRows, nodes.size() - t0);
+      std::map<int, std::vector<int>> by_code;  // code -> 128 sources
+      for (int r = 0; r < rows; ++r) {
+        const int32_t i = nodes[t0 + r];
+        for (int64_t k = t.V.off[i]; k < t.V.off[i + 1]; ++k) {
+          const int32_t v = t.V.idx[k];
+          const int ox = t.ix[v] - t.ix[i], oy = t.iy[v] - t.iy[i], oz = t.iz[v] - t.iz[i];
+          if (std::abs(ox) > 3 || std::abs(oy) > 3 || std::abs(oz) > 3)
+            throw Error(NNK_E_STATE, "V-list offset outside [-3,3]^3");
+          const int code = (ox + 3) * 49 + (oy + 3) * 7 + (oz + 3);
+          auto& vec = by_code[code];
+          if (vec.empty()) vec.assign(kTileRows, -1);
+          vec[r] = v;
+          ++useful;
+        }
+      }
+      tile_slot0.push_back((int)slot_op.size());
+      for (int r = 0; r < kTileRows; ++r) tile_nodes.push_back(r < rows ? nodes[t0 + r] : -1);
+      int nslots = 0;
+      for (auto& kv : by_code) {
+        auto it = img_of.find(kv.first);
+        if (it == img_of.end()) {
+          it = img_of.emplace(kv.first, (int)img_code.size()).first;
+          img_code.push_back(kv.first);
+          img_w.push_back(std::ldexp(W0, -L));
+        }
+        slot_op.push_back(it->second);
+        slot_src.insert(slot_src.end(), kv.second.begin(), kv.second.end());
+        ++nslots;
+      }
+      tslots += nslots;
+      (void)tile;
+      tile_groups.push_back({nslots});
+    }
+    // units ordered by slot group, then tile, so tiles of a level share
+    // operator images in L2 at about the same time
+    int maxg = 0;
+    for (auto& g : tile_groups) maxg = std::max(maxg, (g[0] + kSlotsPerUnit - 1) / kSlotsPerUnit);
+    for (int gi = 0; gi < maxg; ++gi)
+      for (size_t ti = 0; ti < tile_groups.size(); ++ti) {
+        const int ns = tile_groups[ti][0];
+        const int s0 = gi * kSlotsPerUnit;
+        if (s0 >= ns) continue;
+        units.push_back(M2LUnit{first_tile + (int)ti, s0, std::min(kSlotsPerUnit, ns - s0), 0});
+      }
+  }
+  plan.ntiles = (int)tile_slot0.size();
+  plan.nunits = (int)units.size();
+  plan.useful_pairs = useful;
+  plan.tile_slots = tslots;
+  plan.tile_nodes.upload(tile_nodes, st);
+  plan.tile_slot0.upload(tile_slot0, st);
+  plan.slot_op.upload(slot_op, st);
+  plan.slot_src.upload(slot_src, st);
+  plan.units.upload(units, st);
+  const size_t img_floats = (size_t)(NP / 32) * NP * 32;
+  plan.images.alloc(std::max<size_t>(1, img_code.size()) * img_floats);
+  plan.images.zero(st);
+  if (!img_code.empty()) {
+    DBuf<int> dcode, dlat;
+    DBuf<double> dw;
+    dcode.upload(img_code, st);
+    dw.upload(img_w, st);
+    dlat.upload(lat, st);
+    const long long total = (long long)P * P * (long long)img_code.size();
+    m2l_operator_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+        (int)img_code.size(), dcode.p, dw.p, dlat.p, P, res, eps, mu, NP, plan.images.p);
+    NNK_CHECK_LAUNCH();
+    NNK_CUDA(cudaStreamSynchronize(st));
+  }
+  plan.src.alloc((size_t)t.nodes * NP);
+  plan.src.zero(st);
+  plan.err.alloc(1);
+  plan.err.zero(st);
+  if (!plan.h_err) NNK_CUDA(cudaMallocHost((void**)&plan.h_err, sizeof(int)));
+  *plan.h_err = 0;
+  plan.smem_bytes = 1024 + 2 * (size_t)kTileRows * 128 + 2 * (size_t)NP * 128 + 64;
+  // the attribute is per kernel, shared by every plan: set it for the largest NP
+  const int max_smem = 1024 + 2 * kTileRows * 128 + 2 * 512 * 128 + 64;
+  NNK_CUDA(cudaFuncSetAttribute(m2l_tf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  NNK_CUDA(cudaStreamSynchronize(st));
+  plan.ready = true;
+}
+
+void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st) {
+  if (!plan.nunits) return;
+  m2l_tf32_kernel<<<plan.nunits, 128, plan.smem_bytes, st>>>(plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p,
+                                                             plan.slot_op.p, plan.slot_src.p, plan.images.p,
+                                                             plan.src.p, check, ldc, plan.NP, plan.err.p);
+  NNK_CHECK_LAUNCH();
+  NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+}
+
+void check_m2l_error(M2LPlan& plan, cudaStream_t st) {
+  if (!plan.h_err) return;
+  NNK_CUDA(cudaStreamSynchronize(st));
+  if (*plan.h_err) throw Error(NNK_E_TIMEOUT, "tensor-core M2L gave up a bounded wait (flag " +
+                                                  std::to_string(*plan.h_err) + ")");
+}
+
+}  // namespace nnk

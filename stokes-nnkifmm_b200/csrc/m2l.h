@@ -1,0 +1,58 @@
+// M2L (V-list, DownNonleaf.m:34-38 / downwardPass.m:59-74) on the tensor cores.
+//
+// For a target node i at level L and a source node v in V(i), the reference
+// adds kernel(upsurf(v), upsurf(i)) * uppot(v) to the check potential of i.
+// Both surfaces are the same lattice shifted by o = (v - i) in box widths,
+// |o|_inf in {2,3}, so the 3P x 3P matrix T_{L,o} depends only on the level
+// and the offset.  Here, for each level, target nodes are tiled 128 at a time
+// (grouped by octant inside the parent, which fixes the set of offsets their
+// V-lists can use) and
+//     D[node, row] += sum_o sum_k U_o[node, k] * T_{L,o}[row, k]
+// runs as a TF32 tcgen05 GEMM with the accumulator in TMEM: M = 128 nodes,
+// N = 3P padded to a multiple of 32 (480 for p = 6), K = 3P per offset,
+// U_o gathered from the TF32 copy of the up densities, T_{L,o} streamed from
+// pre-swizzled operator images with cp.async.bulk.  The result is added into
+// the check buffer, which the P2L / L2L pair tasks then add to.
+#pragma once
+#include <vector>
+
+#include "common.h"
+#include "tree.h"
+
+namespace nnk {
+
+struct M2LUnit {
+  int tile;   // tile of 128 target nodes
+  int slot0;  // first offset slot of the tile handled by this unit
+  int nslot;  // number of offset slots
+  int pad;
+};
+
+struct M2LPlan {
+  int NP = 0;                   // padded 3P (multiple of 32)
+  int ntiles = 0, nunits = 0;
+  int64_t useful_pairs = 0;     // V pairs (node, source)
+  int64_t tile_slots = 0;       // sum over tiles of offset slots (x128 rows each)
+  DBuf<int> tile_nodes;         // ntiles * 128, -1 for empty rows
+  DBuf<int> tile_slot0;         // per tile: first global slot
+  DBuf<int> slot_op;            // per global slot: operator image
+  DBuf<int> slot_src;           // per global slot: 128 source nodes (-1 none)
+  DBuf<M2LUnit> units;
+  DBuf<float> images;           // per (level, offset): NP/32 chunks of NP x 32 TF32, SW128 K-major
+  DBuf<float> src;              // nodes * NP: TF32 copy of the up densities
+  DBuf<int> err;                // bounded-wait timeout flag
+  int* h_err = nullptr;         // pinned mirror of err
+  size_t smem_bytes = 0;
+  bool ready = false;
+  ~M2LPlan();
+};
+
+// Builds tiles, slot tables and operator images for every level with V pairs.
+void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double mu, M2LPlan& plan,
+                    cudaStream_t st);
+// check[node * ldc + row] += M2L contribution, for every node with a V-list.
+void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st);
+// Throws NNK_E_TIMEOUT if an earlier M2L launch gave up a bounded wait.
+void check_m2l_error(M2LPlan& plan, cudaStream_t st);
+
+}  // namespace nnk

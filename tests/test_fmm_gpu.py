@@ -3,9 +3,9 @@ oracle's per-node-LU restatement of the reference passes (golden fixtures
 made by tests/golden/make_golden.py) and against dense direct sums.
 
 Tolerances: FP64 mode reproduces the oracle to <= 1e-6 relative L2 on every
-fixture (measured 1e-9 .. 4e-8).  Mixed mode (FP32 pair kernels, FP64 check-to-equivalent operators with
-Tikhonov regularization) must stay within 1e-4 of the FP64 direct sum on
-well-posed inputs and of the FP64 GPU result everywhere."""
+fixture (measured 1e-9 .. 4e-8).  Mixed mode (FP32 pair kernels, TF32 tensor-core M2L, FP64 check-to-equivalent
+operators with Tikhonov regularization) must stay within 1e-4 of the FP64
+direct sum and of the FP64 GPU result on well-posed inputs."""
 import os
 
 import numpy as np
