@@ -21,7 +21,7 @@ namespace nnk {
 namespace {
 
 constexpr int kTileRows = 128;
-constexpr int kSlotsPerUnit = 24;
+constexpr int kCodesPerUnit = 32;  // offset codes per work unit (7^3 = 343 codes)
 constexpr uint32_t kWaitLimit = 1u << 26;  // ~1-3 s of polling
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -160,26 +160,20 @@ __global__ void __launch_bounds__(128, 1)
   const int nsteps = u.nslot * nchunks;
   int issued = 0;  // MMA steps committed
   int copies = 0;  // B copies issued
-  for (int s = 0; s < nsteps; ++s) {
+  // Step s uses stage s & 1: thread 0 bulk-copies the operator chunk into B,
+  // every thread gathers its own A row (32 TF32 of its source node's density).
+  auto prepare = [&](int s) {
     const int st = s & 1;
     const int slot = slot_base + s / nchunks;
     const int c = s % nchunks;
-    uint8_t* sA = sA0 + st * A_BYTES;
-    uint8_t* sB = sB0 + st * B_BYTES;
-    // stage st is free once the MMAs of step s-2 are done
-    if (s >= 2 && !mbar_wait(&bars[2 + st], ((s - 2) >> 1) & 1)) {
-      *abort_s = 1;
-      atomicOr(err, 1);
-    }
-    if (tid == 0 && !*abort_s) {
+    if (tid == 0) {
       mbar_expect_tx(&bars[st], B_BYTES);
       const float* gB = images + (size_t)slot_op[slot] * ((size_t)nchunks * NP * 32) + (size_t)c * NP * 32;
-      bulk_g2s(sB, gB, B_BYTES, &bars[st]);
+      bulk_g2s(sB0 + st * B_BYTES, gB, B_BYTES, &bars[st]);
       ++copies;
     }
-    // A row tid: 32 TF32 values of the source node's density, swizzled
     const int v = slot_src[(size_t)slot * kTileRows + tid];
-    float4* dA = reinterpret_cast<float4*>(sA + tid * 128);
+    float4* dA = reinterpret_cast<float4*>(sA0 + st * A_BYTES + tid * 128);
     if (v >= 0) {
       const float4* g4 = reinterpret_cast<const float4*>(src + (size_t)v * NP + c * 32);
 #pragma unroll
@@ -189,15 +183,18 @@ __global__ void __launch_bounds__(128, 1)
       for (int j = 0; j < 8; ++j) dA[j] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     fence_proxy_async();
-    __syncthreads();
-    if (*abort_s) break;
-    if (tid == 0) {
+  };
+  if (nsteps > 0) prepare(0);
+  __syncthreads();
+  for (int s = 0; s < nsteps; ++s) {
+    const int st = s & 1;
+    if (tid == 0 && !*abort_s) {
       if (!mbar_wait(&bars[st], (s >> 1) & 1)) {
         *abort_s = 1;
         atomicOr(err, 2);
       } else {
         tc_fence_after();
-        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+        const uint32_t a0 = smem_u32(sA0 + st * A_BYTES), b0 = smem_u32(sB0 + st * B_BYTES);
 #pragma unroll
         for (int k8 = 0; k8 < 4; ++k8)
           for (int h = 0; h < nhalves; ++h)
@@ -207,6 +204,17 @@ __global__ void __launch_bounds__(128, 1)
         ++issued;
       }
     }
+    // while the MMAs of step s run, fill the other stage with step s+1 once
+    // the MMAs of step s-1 (its previous user) are done
+    if (s + 1 < nsteps) {
+      if (s >= 1 && !mbar_wait(&bars[2 + (st ^ 1)], ((s - 1) >> 1) & 1)) {
+        *abort_s = 1;
+        atomicOr(err, 1);
+      }
+      if (!*abort_s) prepare(s + 1);
+    }
+    __syncthreads();
+    if (*abort_s) break;
   }
   __syncthreads();
   // drain: every MMA this thread issued completes before acc (commit tracks all)
@@ -311,10 +319,23 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
       if (t.V.off[n + 1] > t.V.off[n]) nodes.push_back(n);
     if (nodes.empty()) continue;
     auto oct = [&](int32_t n) { return ((t.ix[n] & 1) << 2) | ((t.iy[n] & 1) << 1) | (t.iz[n] & 1); };
-    std::stable_sort(nodes.begin(), nodes.end(), [&](int32_t a, int32_t b) { return oct(a) < oct(b); });
+    // signature: octant, then the bitset of V offsets (343 codes), so that
+    // nodes using the same offsets share tiles and padding rows stay few
+    std::map<int32_t, std::array<uint64_t, 7>> sig;
+    for (int32_t n : nodes) {
+      std::array<uint64_t, 7> b{};
+      b[0] = (uint64_t)oct(n) << 60;
+      for (int64_t k = t.V.off[n]; k < t.V.off[n + 1]; ++k) {
+        const int32_t v = t.V.idx[k];
+        const int code = (t.ix[v] - t.ix[n] + 3) * 49 + (t.iy[v] - t.iy[n] + 3) * 7 + (t.iz[v] - t.iz[n] + 3);
+        if (code >= 0 && code < 343) b[1 + code / 64] |= 1ull << (code % 64);
+      }
+      sig[n] = b;
+    }
+    std::stable_sort(nodes.begin(), nodes.end(), [&](int32_t a, int32_t b) { return sig[a] > sig[b]; });
     std::map<int, int> img_of;  // offset code -> image
     const int first_tile = (int)tile_slot0.size();
-    std::vector<std::vector<int>> tile_groups;  // per tile in this level: slot counts
+    std::vector<std::vector<int>> tile_codes;  // per tile in this level: its offset codes, ascending
     for (size_t t0 = 0; t0 < nodes.size(); t0 += kTileRows) {
       const int tile = (int)tile_slot0.size();
       const int rows = (int)std::min<size_t>(kTileRows, nodes.size() - t0);
@@ -335,7 +356,7 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
       }
       tile_slot0.push_back((int)slot_op.size());
       for (int r = 0; r < kTileRows; ++r) tile_nodes.push_back(r < rows ? nodes[t0 + r] : -1);
-      int nslots = 0;
+      std::vector<int> codes;
       for (auto& kv : by_code) {
         auto it = img_of.find(kv.first);
         if (it == img_of.end()) {
@@ -345,23 +366,23 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
         }
         slot_op.push_back(it->second);
         slot_src.insert(slot_src.end(), kv.second.begin(), kv.second.end());
-        ++nslots;
+        codes.push_back(kv.first);
       }
-      tslots += nslots;
+      tslots += (int64_t)codes.size();
       (void)tile;
-      tile_groups.push_back({nslots});
+      tile_codes.push_back(codes);
     }
-    // units ordered by slot group, then tile, so tiles of a level share
-    // operator images in L2 at about the same time
-    int maxg = 0;
-    for (auto& g : tile_groups) maxg = std::max(maxg, (g[0] + kSlotsPerUnit - 1) / kSlotsPerUnit);
-    for (int gi = 0; gi < maxg; ++gi)
-      for (size_t ti = 0; ti < tile_groups.size(); ++ti) {
-        const int ns = tile_groups[ti][0];
-        const int s0 = gi * kSlotsPerUnit;
-        if (s0 >= ns) continue;
-        units.push_back(M2LUnit{first_tile + (int)ti, s0, std::min(kSlotsPerUnit, ns - s0), 0});
+    // Work units cut the (code-sorted) slot list of every tile at fixed code
+    // boundaries and run range by range over all tiles of the level, so the
+    // CTAs resident at one time read the same operator images (L2 reuse).
+    for (int c0 = 0; c0 < 343; c0 += kCodesPerUnit) {
+      for (size_t ti = 0; ti < tile_codes.size(); ++ti) {
+        const auto& codes = tile_codes[ti];
+        const int lo = (int)(std::lower_bound(codes.begin(), codes.end(), c0) - codes.begin());
+        const int hi = (int)(std::lower_bound(codes.begin(), codes.end(), c0 + kCodesPerUnit) - codes.begin());
+        if (hi > lo) units.push_back(M2LUnit{first_tile + (int)ti, lo, hi - lo, 0});
       }
+    }
   }
   plan.ntiles = (int)tile_slot0.size();
   plan.nunits = (int)units.size();
