@@ -310,7 +310,9 @@ def main():
             "config": {"workload": WORKLOAD, "precision": args.precision, "parallelism": f"replicas x{ws}",
                        "l2": "flushed between timed steps (256 MiB write, outside the step events)",
                        "nodes": tree.nodeCount, "levels": int(tree.info.max_level) + 1,
-                       "m2l_pairs": stats["m2l_pairs"], "setup_s": round(setup_s, 2)},
+                       "m2l_pairs": stats["m2l_pairs"], "pairs_leaf": stats["pairs_leaf"],
+                       "pairs_p2p": stats["pairs_p2p"], "pairs_up": stats["pairs_up"],
+                       "pairs_down": stats["pairs_down"], "setup_s": round(setup_s, 2)},
             "roofline": roof, "e2e": e2e, "gpu_launches": gpu_launches * args.steps // max(args.steps, 1),
             "gpu_launches_per_step": gpu_launches / args.steps, "clocks": clk}
 

@@ -332,6 +332,7 @@ void Fmm::build_tasks() {
   lvl_off_[maxl_ + 1] = (int64_t)ln.size();
   c2e = (int64_t)ln.size() + (int64_t)up_nodes_host_.size();
   cudaStream_t st = ctx_->stream;
+  split_tasks(tasks, segs);
   tasks_.upload(tasks, st);
   segs_.upload(segs, st);
   lvl_nodes_.upload(ln, st);
@@ -345,6 +346,99 @@ void Fmm::build_tasks() {
   stats_.c2e_columns = c2e;
   stats_.surface_points = P_;
   stats_.levels = maxl_ + 1;
+}
+
+// Load balance: within each launch group, tasks run heaviest first, and a
+// task above kMaxPairs target-source pairs is cut into pieces over its
+// flattened sources; each piece writes its own partial-sum slot and one
+// reduction per task adds the slots in a fixed order.
+void Fmm::split_tasks(std::vector<TaskD>& tasks, std::vector<SegD>& segs) {
+  constexpr int64_t kMaxPairs = 1 << 16;
+  constexpr int64_t kMinSources = 64;
+  std::vector<TaskD> nt;
+  std::vector<SegD> ns;
+  std::vector<RedD> reds;
+  int64_t pbase = 0;
+  nt.reserve(tasks.size());
+  ns.reserve(segs.size());
+  auto process = [&](TaskGroup& g) {
+    std::vector<int64_t> cost(g.count), nsrc(g.count), order(g.count);
+    for (int64_t i = 0; i < g.count; ++i) {
+      const TaskD& r = tasks[g.first + i];
+      int64_t c = 0;
+      for (int k = 0; k < r.nseg; ++k) c += segs[r.seg0 + k].count;
+      nsrc[i] = c;
+      cost[i] = c * r.ntgt;
+      order[i] = i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+    const int64_t first = (int64_t)nt.size(), rfirst = (int64_t)reds.size();
+    for (int64_t i : order) {
+      const TaskD r = tasks[g.first + i];
+      int64_t k = (cost[i] + kMaxPairs - 1) / kMaxPairs;
+      k = std::max<int64_t>(1, std::min<int64_t>(k, nsrc[i] / kMinSources));
+      if (k <= 1) {
+        TaskD c = r;
+        c.seg0 = (int)ns.size();
+        c.partial = 0;
+        for (int q = 0; q < r.nseg; ++q) ns.push_back(segs[r.seg0 + q]);
+        nt.push_back(c);
+        continue;
+      }
+      const int64_t per = (nsrc[i] + k - 1) / k;
+      int q = 0;
+      int64_t used = 0;  // sources of segment q already assigned
+      for (int64_t piece = 0; piece < k; ++piece) {
+        TaskD c = r;
+        c.seg0 = (int)ns.size();
+        c.partial = 1;
+        c.out = pbase + piece * r.ntgt;
+        int64_t need = per;
+        while (need > 0 && q < r.nseg) {
+          const SegD sg = segs[r.seg0 + q];
+          const int64_t take = std::min<int64_t>(need, sg.count - used);
+          if (take > 0) ns.push_back(SegD{sg.start + used, (int)take, 0});
+          used += take;
+          need -= take;
+          if (used == sg.count) {
+            ++q;
+            used = 0;
+          }
+        }
+        c.nseg = (int)ns.size() - c.seg0;
+        nt.push_back(c);
+      }
+      reds.push_back(RedD{r.out, pbase, r.ntgt, (int)k});
+      pbase += k * r.ntgt;
+    }
+    g.first = first;
+    g.count = (int64_t)nt.size() - first;
+    g.red_first = rfirst;
+    g.red_count = (int64_t)reds.size() - rfirst;
+  };
+  for (auto& g : up_) process(g);
+  for (auto& g : down_nov_) process(g);
+  for (auto& g : down_) process(g);
+  process(leaf_);
+  tasks.swap(nt);
+  segs.swap(ns);
+  reds_.upload(reds, ctx_->stream);
+  if (p_.precision == NNK_PREC_FP64) partial64_.alloc(std::max<int64_t>(3 * pbase, 1));
+  else partial32_.alloc(std::max<int64_t>(3 * pbase, 1));
+}
+
+template <typename Real>
+void Fmm::run_group(const TaskGroup& g, const Real* spos, const Real* sstr, const Real* tpos, Real* out, Real e2,
+                    Real scale, int accumulate, int phase_id) {
+  if (g.count == 0) return;
+  cudaStream_t st = ctx_->stream;
+  Real* partial = std::is_same<Real, double>::value ? (Real*)partial64_.p : (Real*)partial32_.p;
+  phase(phase_id, [&] {
+    launch_p2p<Real>(tasks_.p + g.first, (int)g.count, segs_.p, spos, sstr, tpos, out, partial, e2, scale, st,
+                     accumulate);
+  });
+  if (g.red_count)
+    phase(phase_id, [&] { launch_reduce<Real>(reds_.p + g.red_first, (int)g.red_count, partial, out, accumulate, st); });
 }
 
 void Fmm::build_operators() {
@@ -465,9 +559,7 @@ void Fmm::apply_impl(const double* d_in, double* d_out, int layout) {
   // upward pass
   for (int L = maxl_; L >= 1; --L) {
     if (up_[L].count == 0) continue;
-    phase(NNK_PHASE_UP_PAIRS, [&] {
-      launch_p2p<Real>(tasks_.p + up_[L].first, (int)up_[L].count, segs_.p, pos, str, pos, check, e2, scale, st);
-    });
+    run_group<Real>(up_[L], pos, str, pos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS);
     const int64_t nn = up_off_[L + 1] - up_off_[L];
     phase(NNK_PHASE_UP_C2E, [&] {
       launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 0, up_nodes_.p + up_off_[L], (int)nn, check, str, E_, P_, st,
@@ -483,10 +575,7 @@ void Fmm::apply_impl(const double* d_in, double* d_out, int layout) {
   const std::vector<TaskGroup>& dgroups = tm ? down_nov_ : down_;
   for (int L = 1; L <= maxl_; ++L) {
     if (dgroups[L].count == 0) continue;
-    phase(NNK_PHASE_DOWN_PAIRS, [&] {
-      launch_p2p<Real>(tasks_.p + dgroups[L].first, (int)dgroups[L].count, segs_.p, pos, str, pos, check, e2, scale,
-                       st, tm ? 1 : 0);
-    });
+    run_group<Real>(dgroups[L], pos, str, pos, check, e2, scale, tm ? 1 : 0, NNK_PHASE_DOWN_PAIRS);
     const int64_t nn = lvl_off_[L + 1] - lvl_off_[L];
     phase(NNK_PHASE_DOWN_C2E, [&] {
       launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 1, lvl_nodes_.p + lvl_off_[L], (int)nn, check, str,
@@ -494,10 +583,7 @@ void Fmm::apply_impl(const double* d_in, double* d_out, int layout) {
     });
   }
   // leaf stage
-  if (leaf_.count)
-    phase(NNK_PHASE_LEAF_PAIRS, [&] {
-      launch_p2p<Real>(tasks_.p + leaf_.first, (int)leaf_.count, segs_.p, pos, str, tpos, vel, e2, scale, st);
-    });
+  run_group<Real>(leaf_, pos, str, tpos, vel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS);
   phase(NNK_PHASE_SCATTER,
         [&] { launch_scatter<Real>((int64_t)t.tgt_row.size(), trow_.p, vel, layout, t.n_tgt, d_out, st); });
 }

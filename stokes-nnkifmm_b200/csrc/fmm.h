@@ -25,7 +25,14 @@ struct TaskD {
   int ntgt;
   int seg0;
   int nseg;
-  int pad;
+  int partial;    // 1: a piece of a split task, writes its partial-sum slot at `out`
+};
+// Sum of the k partial-sum slots of a split task, added in a fixed order.
+struct RedD {
+  long long out;    // output slot of the task
+  long long pbase;  // first partial slot; piece i uses pbase + i * ntgt
+  int ntgt;
+  int k;
 };
 struct SegD {
   long long start;  // first source in the unified arrays
@@ -35,6 +42,7 @@ struct SegD {
 
 struct TaskGroup {
   int64_t first = 0, count = 0;  // range in the task array
+  int64_t red_first = 0, red_count = 0;  // reductions of its split tasks
 };
 
 struct FmmParams {
@@ -70,6 +78,10 @@ class Fmm {
   void build_tasks();
   void build_operators();
   void build_reduced();
+  void split_tasks(std::vector<TaskD>& tasks, std::vector<SegD>& segs);
+  template <typename Real>
+  void run_group(const TaskGroup& g, const Real* spos, const Real* sstr, const Real* tpos, Real* out, Real e2,
+                 Real scale, int accumulate, int phase_id);
 
   nnk_ctx* ctx_;
   const HostTree* t_;
@@ -97,6 +109,9 @@ class Fmm {
   // tasks
   DBuf<TaskD> tasks_;
   DBuf<SegD> segs_;
+  DBuf<RedD> reds_;
+  DBuf<double> partial64_;
+  DBuf<float> partial32_;
   std::vector<TaskGroup> up_, down_;  // per level
   std::vector<TaskGroup> down_nov_;   // per level, without the V-list (M2L on the tensor cores)
   M2LPlan m2l_;

@@ -63,76 +63,139 @@ inline void launch_gather(int64_t E, const int64_t* goff, const int32_t* gidx, c
 }
 
 // ------------------------------------------------------------ pair kernel
-// One CTA per task.  Targets of the task are split over the CTA; when a task
-// has fewer targets than threads, several threads share a target and split
-// its sources, then reduce through shared memory.  Sources stream through
-// shared memory one segment tile at a time.
+// One CTA per task.  The task's source segments are flattened: each tile of
+// BS sources may span several segments (a thread finds its segment by binary
+// search over the segment prefix sums in shared memory).  Sources are staged
+// as (x,y,z,f_x) + (f_y,f_z).  A chunk of up to 2*BS targets is processed per
+// pass: above BS targets every thread carries two targets (the second shares
+// the source loads); below, several threads share a target and split its
+// sources, then reduce through shared memory.
 //   u(t) = 1/(8 pi mu) sum_s [ (r^2 + 2 eps^2) f_s + (r.f_s) r ] / (r^2+eps^2)^{3/2},
 //   r = t - s (Tools/kernel.m:23-47).
+template <typename Real> struct Vec4T;
+template <> struct Vec4T<float> { using t4 = float4; using t2 = float2; };
+template <> struct Vec4T<double> { using t4 = double4; using t2 = double2; };
+
+template <typename Real>
+__device__ __forceinline__ void pair_acc(Real tx, Real ty, Real tz, const typename Vec4T<Real>::t4& s4,
+                                         const typename Vec4T<Real>::t2& s2, Real e2, Real& ax, Real& ay,
+                                         Real& az) {
+  const Real dx = tx - s4.x, dy = ty - s4.y, dz = tz - s4.z;
+  const Real r2 = dx * dx + dy * dy + dz * dz;
+  const Real d = r2 + e2;
+  const Real inv = rsq(d);
+  const Real inv3 = inv * inv * inv;
+  const Real a = (d + e2) * inv3;
+  const Real b = (dx * s4.w + dy * s2.x + dz * s2.y) * inv3;
+  ax += a * s4.w + b * dx;
+  ay += a * s2.x + b * dy;
+  az += a * s2.y + b * dz;
+}
+
 template <typename Real, int BS>
 __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks,
                                                  const SegD* __restrict__ segs,
                                                  const Real* __restrict__ spos,
                                                  const Real* __restrict__ sstr,
-                                                 const Real* __restrict__ tpos, Real* __restrict__ out,
-                                                 Real e2, Real scale, int accumulate) {
-  __shared__ Real sx[BS], sy[BS], sz[BS], gx[BS], gy[BS], gz[BS];
+                                                 const Real* __restrict__ tpos, Real* __restrict__ out_main,
+                                                 Real* __restrict__ partial, Real e2, Real scale,
+                                                 int accumulate_main) {
+  using T4 = typename Vec4T<Real>::t4;
+  using T2 = typename Vec4T<Real>::t2;
+  __shared__ T4 s4[BS];
+  __shared__ T2 s2[BS];
+  __shared__ long long seg_start[BS];
+  __shared__ int seg_end[BS];  // inclusive prefix sums of the counts
   __shared__ Real red[3 * BS];
   const TaskD tk = tasks[blockIdx.x];
   const int tid = threadIdx.x;
-  for (int t0 = 0; t0 < tk.ntgt; t0 += BS) {
-    const int nt = min(BS, tk.ntgt - t0);
-    const int splits = BS / nt;
-    const int mt = tid % nt, ms = tid / nt;
-    const bool active = ms < splits;
-    Real tx = 0, ty = 0, tz = 0;
-    if (active) ldpos(tpos, tk.tgt + t0 + mt, tx, ty, tz);
-    Real ax = 0, ay = 0, az = 0;
-    for (int s = 0; s < tk.nseg; ++s) {
-      const SegD sg = segs[tk.seg0 + s];
-      for (int j0 = 0; j0 < sg.count; j0 += BS) {
-        const int nj = min(BS, sg.count - j0);
+  Real* __restrict__ out = tk.partial ? partial : out_main;
+  const int accumulate = tk.partial ? 0 : accumulate_main;
+  for (int t0 = 0; t0 < tk.ntgt; t0 += 2 * BS) {
+    const int nt = min(2 * BS, tk.ntgt - t0);
+    const bool two = nt > BS;
+    const int n1 = two ? BS : nt;              // targets in the first slot
+    const int splits = two ? 1 : BS / nt;
+    const int mt = tid % n1, ms = tid / n1;
+    const bool act0 = ms < splits;
+    const bool act1 = two && tid + BS < nt;
+    Real tx = 0, ty = 0, tz = 0, ux = 0, uy = 0, uz = 0;
+    if (act0) ldpos(tpos, tk.tgt + t0 + mt, tx, ty, tz);
+    if (act1) ldpos(tpos, tk.tgt + t0 + BS + tid, ux, uy, uz);
+    Real ax = 0, ay = 0, az = 0, bx = 0, by = 0, bz = 0;
+    for (int sb = 0; sb < tk.nseg; sb += BS) {
+      const int nsb = min(BS, tk.nseg - sb);
+      __syncthreads();
+      int cnt = 0;
+      if (tid < nsb) {
+        const SegD sg = segs[tk.seg0 + sb + tid];
+        seg_start[tid] = sg.start;
+        cnt = sg.count;
+      }
+      seg_end[tid] = cnt;
+      __syncthreads();
+      for (int o = 1; o < BS; o <<= 1) {  // inclusive scan
+        const int v = tid >= o ? seg_end[tid - o] : 0;
         __syncthreads();
-        if (tid < nj) {
-          const long long j = sg.start + j0 + tid;
-          Real x, y, z;
-          ldpos(spos, j, x, y, z);
-          sx[tid] = x;
-          sy[tid] = y;
-          sz[tid] = z;
-          gx[tid] = sstr[3 * j];
-          gy[tid] = sstr[3 * j + 1];
-          gz[tid] = sstr[3 * j + 2];
+        seg_end[tid] += v;
+        __syncthreads();
+      }
+      const int total = seg_end[nsb - 1];
+      // software pipeline: the next tile's source is fetched into registers
+      // while the current tile is computed from shared memory
+      auto fetch = [&](int f, T4& a, T2& b) {
+        int lo = 0, hi = nsb - 1;  // first k with seg_end[k] > f
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (seg_end[mid] > f) hi = mid;
+          else lo = mid + 1;
+        }
+        const long long j = seg_start[lo] + (f - (lo ? seg_end[lo - 1] : 0));
+        Real x, y, z;
+        ldpos(spos, j, x, y, z);
+        a.x = x;
+        a.y = y;
+        a.z = z;
+        a.w = sstr[3 * j];
+        b.x = sstr[3 * j + 1];
+        b.y = sstr[3 * j + 2];
+      };
+      T4 pa;
+      T2 pb;
+      if (tid < total) fetch(tid, pa, pb);
+      for (int f0 = 0; f0 < total; f0 += BS) {
+        if (f0 + tid < total) {
+          s4[tid] = pa;
+          s2[tid] = pb;
         }
         __syncthreads();
-        if (active) {
+        if (f0 + BS + tid < total) fetch(f0 + BS + tid, pa, pb);
+        const int nj = min(BS, total - f0);
+        if (two) {
 #pragma unroll 4
-          for (int j = ms; j < nj; j += splits) {
-            const Real dx = tx - sx[j], dy = ty - sy[j], dz = tz - sz[j];
-            const Real r2 = dx * dx + dy * dy + dz * dz;
-            const Real d = r2 + e2;
-            const Real inv = rsq(d);
-            const Real inv3 = inv * inv * inv;
-            const Real fx = gx[j], fy = gy[j], fz = gz[j];
-            const Real a = (d + e2) * inv3;
-            const Real b = (dx * fx + dy * fy + dz * fz) * inv3;
-            ax += a * fx + b * dx;
-            ay += a * fy + b * dy;
-            az += a * fz + b * dz;
+          for (int j = 0; j < nj; ++j) {
+            const T4 a = s4[j];
+            const T2 b = s2[j];
+            pair_acc<Real>(tx, ty, tz, a, b, e2, ax, ay, az);
+            if (act1) pair_acc<Real>(ux, uy, uz, a, b, e2, bx, by, bz);
           }
+        } else if (act0) {
+#pragma unroll 4
+          for (int j = ms; j < nj; j += splits) pair_acc<Real>(tx, ty, tz, s4[j], s2[j], e2, ax, ay, az);
         }
+        __syncthreads();
       }
     }
     red[tid] = ax;
     red[BS + tid] = ay;
     red[2 * BS + tid] = az;
     __syncthreads();
-    if (tid < nt) {
+    if (tid < n1) {
       Real vx = 0, vy = 0, vz = 0;
       for (int k = 0; k < splits; ++k) {
-        vx += red[tid + k * nt];
-        vy += red[BS + tid + k * nt];
-        vz += red[2 * BS + tid + k * nt];
+        vx += red[tid + k * n1];
+        vy += red[BS + tid + k * n1];
+        vz += red[2 * BS + tid + k * n1];
       }
       const long long o = 3 * (tk.out + t0 + tid);
       if (accumulate) {
@@ -145,15 +208,51 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
         out[o + 2] = scale * vz;
       }
     }
+    if (act1) {
+      const long long o = 3 * (tk.out + t0 + BS + tid);
+      if (accumulate) {
+        out[o] += scale * bx;
+        out[o + 1] += scale * by;
+        out[o + 2] += scale * bz;
+      } else {
+        out[o] = scale * bx;
+        out[o + 1] = scale * by;
+        out[o + 2] = scale * bz;
+      }
+    }
     __syncthreads();
   }
 }
 
 template <typename Real>
 inline void launch_p2p(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
-                       const Real* tpos, Real* out, Real e2, Real scale, cudaStream_t st, int accumulate = 0) {
+                       const Real* tpos, Real* out, Real* partial, Real e2, Real scale, cudaStream_t st,
+                       int accumulate = 0) {
   if (ntasks == 0) return;
-  p2p_kernel<Real, 128><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, e2, scale, accumulate);
+  p2p_kernel<Real, 128><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale, accumulate);
+  NNK_CHECK_LAUNCH();
+}
+
+// out(task) (+)= sum_i partial(piece i), pieces summed in index order so the
+// result does not depend on scheduling.
+template <typename Real>
+__global__ void reduce_partials_kernel(const RedD* __restrict__ reds, const Real* __restrict__ partial,
+                                       Real* __restrict__ out, int accumulate) {
+  const RedD r = reds[blockIdx.x];
+  const int n = 3 * r.ntgt;
+  for (int v = threadIdx.x; v < n; v += blockDim.x) {
+    Real s = 0;
+    for (int i = 0; i < r.k; ++i) s += partial[3 * (r.pbase + (long long)i * r.ntgt) + v];
+    if (accumulate) out[3 * r.out + v] += s;
+    else out[3 * r.out + v] = s;
+  }
+}
+
+template <typename Real>
+inline void launch_reduce(const RedD* reds, int nreds, const Real* partial, Real* out, int accumulate,
+                          cudaStream_t st) {
+  if (nreds == 0) return;
+  reduce_partials_kernel<Real><<<nreds, 128, 0, st>>>(reds, partial, out, accumulate);
   NNK_CHECK_LAUNCH();
 }
 
