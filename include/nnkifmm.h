@@ -87,7 +87,8 @@ typedef struct nnk_fmm_params {
   int32_t corona_res;    /* 'coronaRes' (default 6)                            */
   int32_t corona_shells; /* 'coronaShells' (default 1)                         */
   int32_t precision;     /* NNK_PREC_FP64 or NNK_PREC_MIXED                    */
-  int32_t reserved;
+  int32_t m2l_mode;      /* mixed mode M2L operators: 0 auto (images when they
+                            fit 8 GiB), 1 streamed images, 2 generated in-kernel */
   double reg;            /* relative Tikhonov weight of the check-to-equivalent
                             pseudo-inverse in NNK_PREC_MIXED (0 = default 1e-5) */
 } nnk_fmm_params;
@@ -227,6 +228,13 @@ int nnk_mob_precon(nnk_mob* mob, const double* x, double* y, int32_t on_device);
 int nnk_mob_solve(nnk_mob* mob, const double* rhs, double* x,
                   const nnk_solve_params* sp, int32_t precondition,
                   nnk_solve_info* info, int32_t on_device);
+/* Mixed-precision iterative refinement for nnk_mob_solve (no counterpart in
+ * the reference, which solves in FP64 only): when `fp64` is an FP64 FMM on
+ * the same tree as the mobility object's (mixed) FMM, each solve repeats
+ * "GMRES on the mixed operator for r, x += d, r = b - A_fp64 x" until the
+ * FP64 residual meets tol (at most max_outer times; inner tolerance at least
+ * inner_tol).  fp64 = NULL switches refinement off. */
+int nnk_mob_set_refinement(nnk_mob* mob, nnk_fmm* fp64, int32_t max_outer, double inner_tol);
 int nnk_mob_destroy(nnk_mob* mob);
 
 /* ------------------------------------------------- allocation-free call -- */

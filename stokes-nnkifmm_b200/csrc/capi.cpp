@@ -228,6 +228,7 @@ int nnk_fmm_create(nnk_ctx* ctx, const nnk_tree* tree, const nnk_fmm_params* par
   p.res = params->corona_res ? params->corona_res : 6;
   p.shells = params->corona_shells ? params->corona_shells : 1;
   p.precision = params->precision;
+  p.m2l_mode = params->m2l_mode;
   p.reg = params->reg;
   if (p.precision != NNK_PREC_FP64 && p.precision != NNK_PREC_MIXED)
     return fail(ctx, NNK_E_ARG, "unknown precision mode");
@@ -381,6 +382,16 @@ int nnk_mob_solve(nnk_mob* mob, const double* rhs, double* x, const nnk_solve_pa
   finish_out(ctx, M.io_out, x, n, on_device);
   if (info) *info = inf;
   if (inf.flag != 0) return fail(ctx, NNK_E_NOCONV, "gmres stopped at maxit above tol");
+  API_CATCH(ctx)
+}
+
+int nnk_mob_set_refinement(nnk_mob* mob, nnk_fmm* fp64, int32_t max_outer, double inner_tol) {
+  if (!mob) return NNK_E_ARG;
+  nnk_ctx* ctx = mob->fmm->ctx;
+  API_TRY
+  if (fp64 && fp64->f->params().precision != NNK_PREC_FP64)
+    return fail(ctx, NNK_E_ARG, "refinement needs an FP64 FMM");
+  mob->m->set_refinement(fp64 ? fp64->f.get() : nullptr, max_outer, inner_tol);
   API_CATCH(ctx)
 }
 

@@ -444,6 +444,8 @@ void Fmm::run_group(const TaskGroup& g, const Real* spos, const Real* sstr, cons
 void Fmm::build_operators() {
   const HostTree& t = *t_;
   if (p_.precision == NNK_PREC_MIXED) {
+    if (p_.m2l_mode == 1) m2l_.image_budget = ~(size_t)0;
+    if (p_.m2l_mode == 2) m2l_.image_budget = 0;
     build_m2l_plan(t, p_.res, p_.shells, p_.eps, p_.mu, m2l_, ctx_->stream);
     tensor_m2l_ = true;
     stats_.m2l_tile_rows = m2l_.tile_slots * 128;

@@ -49,6 +49,7 @@ struct FmmParams {
   double eps = 0.0, mu = 1.0;
   int res = 6, shells = 1;
   int precision = NNK_PREC_FP64;
+  int m2l_mode = 0;
   double reg = 0.0;
 };
 

@@ -123,7 +123,169 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 __global__ void __launch_bounds__(128, 1)
-    m2l_tf32_kernel(const M2LUnit* __restrict__ units, const int* __restrict__ tile_nodes,
+    m2l_gen_kernel(const M2LUnit* __restrict__ units, const int* __restrict__ tile_nodes,
+                    const int* __restrict__ tile_slot0, const int* __restrict__ slot_code,
+                    const float* __restrict__ slot_h, const int* __restrict__ slot_src,
+                    const int* __restrict__ lat_packed, int P, int res, float e2, float scale,
+                    const float* __restrict__ src, float* __restrict__ check, int ldc, int NP, int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* sbase = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+  const uint32_t A_BYTES = kTileRows * 128, B_BYTES = (uint32_t)NP * 128;
+  uint8_t* sA0 = sbase;
+  uint8_t* sB0 = sbase + 2 * A_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + 2 * A_BYTES + 2 * B_BYTES);  // done[2] acc
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3);
+  volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  int* lat = reinterpret_cast<int*>(tmem_slot + 2);  // P packed lattice indices
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const M2LUnit u = units[blockIdx.x];
+  const int nchunks = NP / 32;
+  const int nhalves = NP > 256 ? 2 : 1;
+  const int nh = NP / nhalves;
+  const uint32_t ncols = NP > 256 ? 512u : 256u;
+  const uint32_t idesc = tf32_idesc(nh);
+  const int n3 = 3 * P;
+
+  if (tid == 0) {
+    for (int k = 0; k < 3; ++k) mbar_init(&bars[k], 1);
+    *abort_s = 0;
+    fence_barrier_init();
+  }
+  for (int p = tid; p < P; p += blockDim.x) lat[p] = lat_packed[p];
+  // operator rows >= 3P stay zero in both stages
+  for (int i = tid; i < (int)(2 * B_BYTES / 16); i += blockDim.x)
+    reinterpret_cast<float4*>(sB0)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (warp == 0) tmem_alloc(tmem_slot, ncols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int node = tile_nodes[u.tile * kTileRows + tid];
+  const int slot_base = tile_slot0[u.tile] + u.slot0;
+  const int nsteps = u.nslot * nchunks;
+  int issued = 0;
+  // Step s uses stage s & 1: every thread gathers its A row (32 TF32 of its
+  // source node's density) and computes a share of the operator chunk
+  //   T[n = 3a+al][k = 3b+be] = S_al,be(r) / (8 pi mu),  r = (lat_a - lat_b - (res-1) o) h,
+  // k in [32c, 32c+32), rounded to TF32 into the swizzled B tile.
+  auto prepare = [&](int s) {
+    const int st = s & 1;
+    const int slot = slot_base + s / nchunks;
+    const int c = s % nchunks;
+    const int v = slot_src[(size_t)slot * kTileRows + tid];
+    float4* dA = reinterpret_cast<float4*>(sA0 + st * A_BYTES + tid * 128);
+    if (v >= 0) {
+      const float4* g4 = reinterpret_cast<const float4*>(src + (size_t)v * NP + c * 32);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) dA[j ^ (tid & 7)] = __ldg(g4 + j);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) dA[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    const int code = slot_code[slot];
+    const float h = slot_h[slot];
+    const int ox = (code / 49 - 3) * (res - 1), oy = ((code / 7) % 7 - 3) * (res - 1), oz = (code % 7 - 3) * (res - 1);
+    const int k0 = 32 * c;
+    const int b0 = k0 / 3, b1 = min(P - 1, (k0 + 31) / 3);
+    const int nbp = b1 - b0 + 1;
+    uint8_t* sB = sB0 + st * B_BYTES;
+    for (int pr = tid; pr < P * nbp; pr += blockDim.x) {
+      const int a = pr / nbp, b = b0 + pr % nbp;
+      const int la = lat[a], lb = lat[b];
+      const float rx = (float)((la & 15) - (lb & 15) - ox) * h;
+      const float ry = (float)(((la >> 4) & 15) - ((lb >> 4) & 15) - oy) * h;
+      const float rz = (float)(((la >> 8) & 15) - ((lb >> 8) & 15) - oz) * h;
+      const float r2 = rx * rx + ry * ry + rz * rz;
+      const float d = r2 + e2;
+      const float inv = rsqrtf(d);
+      const float w3 = inv * inv * inv * scale;
+      const float r[3] = {rx, ry, rz};
+#pragma unroll
+      for (int be = 0; be < 3; ++be) {
+        const int kl = 3 * b + be - k0;
+        if (kl < 0 || kl >= 32) continue;
+        const int j = kl >> 2, e = kl & 3;
+#pragma unroll
+        for (int al = 0; al < 3; ++al) {
+          const int n = 3 * a + al;
+          const float val = (r[al] * r[be] + (al == be ? d + e2 : 0.f)) * w3;
+          *reinterpret_cast<float*>(sB + n * 128 + ((j ^ (n & 7)) << 4) + e * 4) = to_tf32(val);
+        }
+      }
+    }
+    if (k0 + 32 > n3) {  // padded K columns of the last chunk
+      const int kpad = k0 + 32 - n3;
+      for (int q = tid; q < n3 * kpad; q += blockDim.x) {
+        const int n = q / kpad, kl = (n3 - k0) + q % kpad;
+        const int j = kl >> 2, e = kl & 3;
+        *reinterpret_cast<float*>(sB + n * 128 + ((j ^ (n & 7)) << 4) + e * 4) = 0.f;
+      }
+    }
+    fence_proxy_async();
+  };
+  if (nsteps > 0) prepare(0);
+  __syncthreads();
+  for (int s = 0; s < nsteps; ++s) {
+    const int st = s & 1;
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(sA0 + st * A_BYTES), b0 = smem_u32(sB0 + st * B_BYTES);
+#pragma unroll
+      for (int k8 = 0; k8 < 4; ++k8)
+        for (int h = 0; h < nhalves; ++h)
+          umma_tf32(tmem + (uint32_t)(h * nh), sw128_desc(a0 + k8 * 32), sw128_desc(b0 + h * nh * 128 + k8 * 32),
+                    idesc, (s > 0 || k8 > 0) ? 1u : 0u);
+      umma_commit(&bars[st]);
+      ++issued;
+    }
+    // while the MMAs of step s run, fill the other stage with step s+1 once
+    // the MMAs of step s-1 (its previous user) are done
+    if (s + 1 < nsteps) {
+      if (s >= 1 && !mbar_wait(&bars[st ^ 1], ((s - 1) >> 1) & 1)) {
+        *abort_s = 1;
+        atomicOr(err, 1);
+      }
+      if (!*abort_s) prepare(s + 1);
+    }
+    __syncthreads();
+    if (*abort_s) break;
+  }
+  __syncthreads();
+  // drain: the commit tracks every MMA this thread issued
+  bool acc_ok = true;
+  if (tid == 0) umma_commit(&bars[2]);
+  if (!mbar_wait(&bars[2], 0)) {
+    acc_ok = false;
+    atomicOr(err, 4);
+  }
+  (void)issued;
+  tc_fence_after();
+  if (!*abort_s && acc_ok && nsteps > 0) {
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int col = 0; col < NP; col += 16) {
+      float vals[16];
+      tmem_ld16(lane_addr + col, vals);
+      if (node >= 0) {
+        float* dst = check + (size_t)node * ldc;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int c0 = col + 4 * q;
+          if (c0 < ldc)
+            atomicAdd(reinterpret_cast<float4*>(dst + c0), make_float4(vals[4 * q], vals[4 * q + 1],
+                                                                       vals[4 * q + 2], vals[4 * q + 3]));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+__global__ void __launch_bounds__(128, 1)
+    m2l_img_kernel(const M2LUnit* __restrict__ units, const int* __restrict__ tile_nodes,
                     const int* __restrict__ tile_slot0, const int* __restrict__ slot_op,
                     const int* __restrict__ slot_src, const float* __restrict__ images,
                     const float* __restrict__ src, float* __restrict__ check, int ldc, int NP, int* err) {
@@ -308,10 +470,11 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
     throw Error(NNK_E_ARG, "tensor-core M2L supports 3P up to 512 with N halves a multiple of 16");
   plan.NP = NP;
   const double W0 = t.corners[3] - t.corners[0];
-  std::vector<int> tile_nodes, tile_slot0, slot_op, slot_src;
+  std::vector<int> tile_nodes, tile_slot0, slot_code, slot_src, slot_op;
+  std::vector<float> slot_h;
   std::vector<M2LUnit> units;
-  std::vector<int> img_code;
-  std::vector<double> img_w;
+  std::vector<int> img_code;      // per operator image: offset code
+  std::vector<double> img_w;      // per operator image: box width of its level
   int64_t useful = 0, tslots = 0;
   for (int L = 1; L <= t.max_level; ++L) {
     std::vector<int32_t> nodes;
@@ -333,7 +496,7 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
       sig[n] = b;
     }
     std::stable_sort(nodes.begin(), nodes.end(), [&](int32_t a, int32_t b) { return sig[a] > sig[b]; });
-    std::map<int, int> img_of;  // offset code -> image
+    std::map<int, int> img_of;  // offset code -> image of this level
     const int first_tile = (int)tile_slot0.size();
     std::vector<std::vector<int>> tile_codes;  // per tile in this level: its offset codes, ascending
     for (size_t t0 = 0; t0 < nodes.size(); t0 += kTileRows) {
@@ -354,7 +517,7 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
           ++useful;
         }
       }
-      tile_slot0.push_back((int)slot_op.size());
+      tile_slot0.push_back((int)slot_code.size());
       for (int r = 0; r < kTileRows; ++r) tile_nodes.push_back(r < rows ? nodes[t0 + r] : -1);
       std::vector<int> codes;
       for (auto& kv : by_code) {
@@ -365,6 +528,8 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
           img_w.push_back(std::ldexp(W0, -L));
         }
         slot_op.push_back(it->second);
+        slot_code.push_back(kv.first);
+        slot_h.push_back((float)(std::ldexp(W0, -L) / (res - 1)));
         slot_src.insert(slot_src.end(), kv.second.begin(), kv.second.end());
         codes.push_back(kv.first);
       }
@@ -390,13 +555,23 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
   plan.tile_slots = tslots;
   plan.tile_nodes.upload(tile_nodes, st);
   plan.tile_slot0.upload(tile_slot0, st);
-  plan.slot_op.upload(slot_op, st);
+  plan.slot_code.upload(slot_code, st);
+  plan.slot_h.upload(slot_h, st);
   plan.slot_src.upload(slot_src, st);
   plan.units.upload(units, st);
-  const size_t img_floats = (size_t)(NP / 32) * NP * 32;
-  plan.images.alloc(std::max<size_t>(1, img_code.size()) * img_floats);
-  plan.images.zero(st);
-  if (!img_code.empty()) {
+  std::vector<int> packed(P);
+  for (int p = 0; p < P; ++p) packed[p] = lat[3 * p] | (lat[3 * p + 1] << 4) | (lat[3 * p + 2] << 8);
+  plan.lat.upload(packed, st);
+  // Operator images (one NP x NP TF32 matrix per level and offset, streamed
+  // by the image kernel) when they fit the budget; otherwise the generating
+  // kernel computes each chunk in shared memory.
+  const size_t img_bytes = img_code.size() * (size_t)NP * NP * sizeof(float);
+  plan.use_images = img_bytes <= plan.image_budget;
+  plan.image_bytes = plan.use_images ? img_bytes : 0;
+  if (plan.use_images && !img_code.empty()) {
+    plan.slot_op.upload(slot_op, st);
+    plan.images.alloc(img_code.size() * (size_t)NP * NP);
+    plan.images.zero(st);
     DBuf<int> dcode, dlat;
     DBuf<double> dw;
     dcode.upload(img_code, st);
@@ -408,25 +583,38 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
     NNK_CHECK_LAUNCH();
     NNK_CUDA(cudaStreamSynchronize(st));
   }
+  plan.P = P;
+  plan.res = res;
+  plan.e2 = (float)(eps * eps);
+  plan.scale = (float)(1.0 / (8.0 * M_PI * mu));
   plan.src.alloc((size_t)t.nodes * NP);
   plan.src.zero(st);
   plan.err.alloc(1);
   plan.err.zero(st);
   if (!plan.h_err) NNK_CUDA(cudaMallocHost((void**)&plan.h_err, sizeof(int)));
   *plan.h_err = 0;
-  plan.smem_bytes = 1024 + 2 * (size_t)kTileRows * 128 + 2 * (size_t)NP * 128 + 64;
+  plan.smem_bytes = 1024 + 2 * (size_t)kTileRows * 128 + 2 * (size_t)NP * 128 + 64 + 4 * (size_t)P;
   // the attribute is per kernel, shared by every plan: set it for the largest NP
-  const int max_smem = 1024 + 2 * kTileRows * 128 + 2 * 512 * 128 + 64;
-  NNK_CUDA(cudaFuncSetAttribute(m2l_tf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  const int max_smem = 1024 + 2 * kTileRows * 128 + 2 * 512 * 128 + 64 + 4 * 512;
+  NNK_CUDA(cudaFuncSetAttribute(m2l_gen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  NNK_CUDA(cudaFuncSetAttribute(m2l_img_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
   NNK_CUDA(cudaStreamSynchronize(st));
   plan.ready = true;
 }
 
 void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st) {
   if (!plan.nunits) return;
-  m2l_tf32_kernel<<<plan.nunits, 128, plan.smem_bytes, st>>>(plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p,
-                                                             plan.slot_op.p, plan.slot_src.p, plan.images.p,
-                                                             plan.src.p, check, ldc, plan.NP, plan.err.p);
+  if (plan.use_images) {
+    m2l_img_kernel<<<plan.nunits, 128, plan.smem_bytes, st>>>(plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p,
+                                                              plan.slot_op.p, plan.slot_src.p, plan.images.p,
+                                                              plan.src.p, check, ldc, plan.NP, plan.err.p);
+    NNK_CHECK_LAUNCH();
+    NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    return;
+  }
+  m2l_gen_kernel<<<plan.nunits, 128, plan.smem_bytes, st>>>(
+      plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p, plan.slot_code.p, plan.slot_h.p, plan.slot_src.p,
+      plan.lat.p, plan.P, plan.res, plan.e2, plan.scale, plan.src.p, check, ldc, plan.NP, plan.err.p);
   NNK_CHECK_LAUNCH();
   NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
 }

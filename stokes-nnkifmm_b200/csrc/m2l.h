@@ -10,8 +10,11 @@
 //     D[node, row] += sum_o sum_k U_o[node, k] * T_{L,o}[row, k]
 // runs as a TF32 tcgen05 GEMM with the accumulator in TMEM: M = 128 nodes,
 // N = 3P padded to a multiple of 32 (480 for p = 6), K = 3P per offset,
-// U_o gathered from the TF32 copy of the up densities, T_{L,o} streamed from
-// pre-swizzled operator images with cp.async.bulk.  The result is added into
+// U_o gathered from the TF32 copy of the up densities.  T_{L,o} comes either
+// from pre-swizzled operator images streamed with cp.async.bulk (default), or,
+// when the images would exceed the memory budget (many trees of different
+// sizes), it is computed chunk by chunk from the kernel formula into shared
+// memory by the CTA itself (about 2.7x slower per chunk, no memory).  The result is added into
 // the check buffer, which the P2L / L2L pair tasks then add to.
 #pragma once
 #include <vector>
@@ -35,10 +38,18 @@ struct M2LPlan {
   int64_t tile_slots = 0;       // sum over tiles of offset slots (x128 rows each)
   DBuf<int> tile_nodes;         // ntiles * 128, -1 for empty rows
   DBuf<int> tile_slot0;         // per tile: first global slot
-  DBuf<int> slot_op;            // per global slot: operator image
+  DBuf<int> slot_code;          // per global slot: offset code (ox+3)*49 + (oy+3)*7 + (oz+3)
+  DBuf<float> slot_h;           // per global slot: lattice spacing w_L / (res-1) of its level
   DBuf<int> slot_src;           // per global slot: 128 source nodes (-1 none)
   DBuf<M2LUnit> units;
+  DBuf<int> lat;                // surface lattice indices, i | j<<4 | k<<8
+  bool use_images = false;      // stream operator images (fast) or generate chunks in the kernel
+  size_t image_budget = (size_t)8 << 30;
+  size_t image_bytes = 0;
+  DBuf<int> slot_op;            // per global slot: operator image (image kernel)
   DBuf<float> images;           // per (level, offset): NP/32 chunks of NP x 32 TF32, SW128 K-major
+  int P = 0, res = 0;
+  float e2 = 0.f, scale = 0.f;
   DBuf<float> src;              // nodes * NP: TF32 copy of the up densities
   DBuf<int> err;                // bounded-wait timeout flag
   int* h_err = nullptr;         // pinned mirror of err
@@ -47,7 +58,7 @@ struct M2LPlan {
   ~M2LPlan();
 };
 
-// Builds tiles, slot tables and operator images for every level with V pairs.
+// Builds tiles and slot tables for every level with V pairs.
 void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double mu, M2LPlan& plan,
                     cudaStream_t st);
 // check[node * ldc + row] += M2L contribution, for every node with a V-list.

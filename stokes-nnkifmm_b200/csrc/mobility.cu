@@ -247,11 +247,20 @@ void Mobility::small_solve(const std::vector<double>& inv, const double* in6, do
   NNK_CUDA(cudaMemcpyAsync(out6, h6b_.data(), 6 * nb_ * sizeof(double), cudaMemcpyHostToDevice, st));
 }
 
-void Mobility::apply(const double* x, double* y) {
+void Mobility::apply(const double* x, double* y) { apply_with(fmm_, x, y); }
+
+void Mobility::apply_with(Fmm* f, const double* x, double* y) {
   // b(1:3N) = FMM(f) + BT*UOm ; b(3N+1:end) = B*f
-  fmm_->apply(x, y, NNK_LAYOUT_BLOCKED, 1);
+  f->apply(x, y, NNK_LAYOUT_BLOCKED, 1);
   bt_apply(x + 3 * N_, y);
   body_sums(x, y + 3 * N_);
+}
+
+void Mobility::set_refinement(Fmm* fp64, int max_outer, double inner_tol) {
+  if (fp64 && &fp64->tree() != &fmm_->tree()) throw Error(NNK_E_ARG, "refinement FMM must share the tree");
+  ref64_ = fp64;
+  ref_outer_ = max_outer > 0 ? max_outer : 10;
+  ref_inner_tol_ = inner_tol > 0 ? inner_tol : 1e-4;
 }
 
 void Mobility::precon(const double* x, double* y) {
@@ -278,6 +287,39 @@ void Mobility::precon(const double* x, double* y) {
 
 void Mobility::solve(const double* rhs, double* x, const nnk_solve_params& sp, bool precondition,
                      nnk_solve_info& info) {
+  const int64_t n = size();
+  if (ref64_) {
+    // x = 0, r = b; repeat: A_mixed d ~= r (GMRES), x += d, r = b - A_fp64 x
+    DBuf<double> r(n), d(n), ax(n), scratch(1);
+    NNK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), ctx_->stream));
+    NNK_CUDA(cudaMemcpyAsync(r.p, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx_->stream));
+    const double nb = std::sqrt(dev_dot(ctx_, rhs, rhs, n, scratch));
+    const double tol = sp.tol > 0 ? sp.tol : 1e-6;
+    info = nnk_solve_info{0, 0, 0.0};
+    if (nb == 0.0) return;
+    double relres = 1.0;
+    for (int outer = 0; outer < ref_outer_; ++outer) {
+      nnk_solve_params in = sp;
+      const double target = tol / relres;  // inner tolerance relative to ||r||
+      in.tol = std::max(ref_inner_tol_, std::min(0.5, target));
+      nnk_solve_info ii{};
+      solve_plain(r.p, d.p, in, precondition, ii);
+      info.iters += ii.iters;
+      dev_axpby(ctx_, 1.0, x, 1.0, d.p, x, n);
+      apply_with(ref64_, x, ax.p);
+      dev_axpby(ctx_, 1.0, rhs, -1.0, ax.p, r.p, n);
+      relres = std::sqrt(dev_dot(ctx_, r.p, r.p, n, scratch)) / nb;
+      if (relres <= tol) break;
+    }
+    info.relres = relres;
+    info.flag = relres <= tol ? 0 : 1;
+    return;
+  }
+  solve_plain(rhs, x, sp, precondition, info);
+}
+
+void Mobility::solve_plain(const double* rhs, double* x, const nnk_solve_params& sp, bool precondition,
+                           nnk_solve_info& info) {
   const int64_t n = size();
   Gmres g(ctx_, n);
   DBuf<double> tmp(n);

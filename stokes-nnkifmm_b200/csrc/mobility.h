@@ -18,8 +18,14 @@ class Mobility {
            const double* rel_points, const double* rel_fine);
   int64_t size() const { return 3 * N_ + 6 * (int64_t)nb_; }
   void apply(const double* x, double* y);   // mobilityMatrixMulti.m:17-36
+  void apply_with(Fmm* f, const double* x, double* y);
   void precon(const double* x, double* y);  // MobilityPrecon.m:17-40
   void solve(const double* rhs, double* x, const nnk_solve_params& sp, bool precondition, nnk_solve_info& info);
+  // Mixed-precision iterative refinement: inner GMRES on this (mixed) FMM,
+  // outer residual b - A x with `fp64` (an FP64 FMM on the same tree).
+  void set_refinement(Fmm* fp64, int max_outer, double inner_tol);
+  void solve_plain(const double* rhs, double* x, const nnk_solve_params& sp, bool precondition,
+                   nnk_solve_info& info);
   DBuf<double> io_in, io_out;
 
  private:
@@ -30,6 +36,9 @@ class Mobility {
   void small_solve(const std::vector<double>& inv, const double* in6, double* out6);  // host 6x6 blocks
 
   Fmm* fmm_;
+  Fmm* ref64_ = nullptr;
+  int ref_outer_ = 0;
+  double ref_inner_tol_ = 1e-4;
   nnk_ctx* ctx_;
   int nb_;
   int64_t N_;

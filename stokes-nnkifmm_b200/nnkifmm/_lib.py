@@ -45,7 +45,7 @@ class TreeInfo(C.Structure):
 
 class FmmParams(C.Structure):
     _fields_ = [("eps", _f64), ("mu", _f64), ("corona_res", _i32), ("corona_shells", _i32),
-                ("precision", _i32), ("reserved", _i32), ("reg", _f64)]
+                ("precision", _i32), ("m2l_mode", _i32), ("reg", _f64)]
 
 
 class FmmStats(C.Structure):
@@ -92,6 +92,7 @@ SIGNATURES = {
     "nnk_mob_apply": (_i32, [_vp, _vp, _vp, _i32]),
     "nnk_mob_precon": (_i32, [_vp, _vp, _vp, _i32]),
     "nnk_mob_solve": (_i32, [_vp, _vp, _vp, C.POINTER(SolveParams), _i32, C.POINTER(SolveInfo), _i32]),
+    "nnk_mob_set_refinement": (_i32, [_vp, _vp, _i32, _f64]),
     "nnk_mob_destroy": (_i32, [_vp]),
     "nnk_direct_nearest_noalloc": (_i32, [_i32, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _i64, _f64, _f64,
                                           _vp]),

@@ -17,7 +17,7 @@ from . import _lib as L
 
 class KIFMM:
     def __init__(self, tree, kernelPar, GPU=1, parThreads=0, blockSize=0.1, GMRES=0, coronaRes=6,
-                 coronaShells=1, format=1, precision="fp64", reg=0.0):
+                 coronaShells=1, format=1, precision="fp64", reg=0.0, m2l="auto"):
         self.tree = tree
         self.ctx = tree.ctx
         eps, mu = float(kernelPar[0]), float(kernelPar[1])
@@ -25,7 +25,8 @@ class KIFMM:
                               coronaRes=coronaRes, coronaShells=coronaShells, format=format,
                               kernelPar=(eps, mu), precision=precision)
         prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
-        p = L.FmmParams(eps, mu, int(coronaRes), int(coronaShells), prec, 0, float(reg))
+        mode = {"auto": 0, "images": 1, "generate": 2}[m2l]
+        p = L.FmmParams(eps, mu, int(coronaRes), int(coronaShells), prec, mode, float(reg))
         h = C.c_void_p()
         L.check(L.lib.nnk_fmm_create(self.ctx.h, tree.h, C.byref(p), C.byref(h)), self.ctx.h, "KIFMM")
         self.h = h

@@ -87,6 +87,17 @@ def test_mixed_vs_direct_sum(name):
     assert rel(v32, g["direct"]) <= 1e-4
 
 
+@pytest.mark.parametrize("name", ["sphere10_40", "adaptive_plain_1600"])
+def test_generated_m2l_operators_match_streamed(name):
+    """M2L operators generated inside the kernel give the streamed-image result."""
+    g = load(name)
+    t = tree_of(g)
+    kp = [float(g["eps"]), float(g["mu"])]
+    a = nk.KIFMM(t, kp, precision="mixed", m2l="images").computeVel(g["F"])
+    b = nk.KIFMM(t, kp, precision="mixed", m2l="generate").computeVel(g["F"])
+    assert rel(b, a) <= 1e-5
+
+
 def test_sparse_matches_oracle():
     g = load("sphere10_40")
     fmm = nk.KIFMM(tree_of(g), [float(g["eps"]), float(g["mu"])])
