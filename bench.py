@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--n-quad", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-errors", action="store_true")
+    ap.add_argument("--no-solves", action="store_true")
+    ap.add_argument("--batch-bodies", type=int, default=4)
     return ap.parse_args()
 
 
@@ -166,6 +168,75 @@ def sampled_direct(torch, w, NN, idx):
         gg = g[s:s + 8192]
         out += ((r2 + 2 * e2) * inv3) @ gg + ((r * gg[None]).sum(-1) * inv3)[..., None].mul(r).sum(1)
     return (out / (8 * np.pi * w["mu"])).cpu().numpy()
+
+
+def solve_benchmarks(torch, nk, args):
+    """Mobility solves/s: config 1 (one sphere, 2 right-hand sides, GMRES to
+    1e-6, FP64 vs mixed) and a sample of config 4 (independent prolate bodies,
+    6 rigid-mode right-hand sides each; FP64 one body after another vs mixed
+    with bodies on concurrent streams).  Errors: rigid velocities against the
+    dense FP64 system (config 1) or against the FP64 GPU solves (config 4)."""
+    from nnkifmm.workloads import batched_bodies, sphere_problem
+    from oracle import mobility as om
+    out = {}
+    w = sphere_problem()
+    NN = nk.nearestMatrix(w["coarse"], w["fine"])
+    dense = {}
+    for F, M in [([1, 0, 0], [0, 0, 0]), ([0, 0, 0], [0, 0, 1])]:
+        body = om.Body(w["coarse"], w["fine"], NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(w["coarse"]), F, M)
+        asm = om.assemble([body])
+        dense[(tuple(F), tuple(M))] = np.linalg.solve(om.dense_mobility_matrix(asm, w["eps"], w["mu"], True),
+                                                      om.mobility_rhs(asm))[-6:]
+    for label, prec, refine in [("fp64", "fp64", None), ("mixed_refined", "mixed", True)]:
+        sw = nk.Swimmers()
+        sw.addSwimmer(w["coarse"], w["fine"], NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(w["coarse"]),
+                      [0, 0, 0], [0, 0, 0])
+        sw.genTree(nodeCapacity=w["cap"], nearest=1)
+        sw.genKIFMM([w["eps"], w["mu"]], refine=refine, GMRES=1, format=2, precision=prec)
+        mob = sw.mobility()
+        errs, times, iters = [], [], []
+        for (F, M), xd in dense.items():
+            sw.F[0], sw.Moment[0] = np.array(F, float), np.array(M, float)
+            rhs = nk.mobilityRHS(sw)
+            mob.solve(rhs, tol=1e-6, maxIter=300)
+            t0 = time.perf_counter()
+            for _ in range(3):
+                x, flag, relres, it = mob.solve(rhs, tol=1e-6, maxIter=300)
+            times.append((time.perf_counter() - t0) / 3)
+            errs.append(float(np.linalg.norm(x[-6:] - xd) / np.linalg.norm(xd)))
+            iters.append(it)
+        out[f"sphere_{label}"] = {"solves_per_s": 1.0 / float(np.mean(times)), "ms_per_solve": 1e3 * float(np.mean(times)),
+                                  "gmres_iters": iters, "rel_err_UOmega_vs_dense_fp64": max(errs)}
+    nb = args.batch_bodies
+    bodies = batched_bodies(nb)
+    res = {}
+    for label, prec, workers, refine in [("fp64_sequential", "fp64", 1, None), ("fp64_batched", "fp64", 8, None),
+                                         ("mixed_refined_batched", "mixed", 8, True)]:
+        t0 = time.perf_counter()
+        B = nk.BatchMobility(bodies, [0.005, 1.0], cap=200, precision=prec, workers=workers, refine=refine)
+        setup = time.perf_counter() - t0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        mats, its = B.solve_all(tol=1e-6, maxIter=400)
+        dt = time.perf_counter() - t0
+        res[label] = (mats, dt, setup, its)
+        del B
+    ref = res["fp64_sequential"][0]
+    n_solves = 6 * nb
+    for label, (mats, dt, setup, its) in res.items():
+        out[f"batched_{label}"] = {"solves_per_s": n_solves / dt, "s_total": dt, "setup_s": setup,
+                                   "gmres_iters_mean": float(np.mean([i[2] for it in its for i in it])),
+                                   "rel_err_vs_fp64": float(max(np.linalg.norm(a - b) / np.linalg.norm(b)
+                                                                for a, b in zip(mats, ref)))}
+    out["batched_workload"] = (f"{nb} prolate spheroids (aspect U[1,5], equal volume, force nodes U[2k,40k], "
+                               f"quadrature at h/4), eps=0.005, nodeCapacity 200, 6 rigid-mode RHS each; sizes "
+                               + str([len(c) for c, _ in bodies]))
+    out["speedup_mixed_batched_vs_fp64_sequential"] = out["batched_mixed_refined_batched"]["solves_per_s"] / \
+        out["batched_fp64_sequential"]["solves_per_s"]
+    out["notes"] = ("mixed solves: FP32 pair kernels incl. M2L, FP64 C2E, GMRES on the mixed operator with FP64 "
+                    "iterative refinement (outer residual with the FP64 FMM on the same regularized operators); "
+                    "batched = bodies on concurrent streams driven by host threads")
+    return out
 
 
 def cpu_baseline_sample(n_force, n_quad, steps=1):
@@ -330,6 +401,8 @@ def main():
         line["errors"] = {f"{mine}_vs_direct_4096": rel(v[idx], ref), f"{oth}_vs_direct_4096": rel(v2[idx], ref),
                           "mixed_vs_fp64": rel(v if mine == "mixed" else v2, v2 if mine == "mixed" else v)}
         line[f"{oth}_gpu"] = {"value": args.n_force / (float(np.mean(ms2)) / 1e3), "ms_per_step": float(np.mean(ms2))}
+    if rank == 0 and not args.no_solves:
+        line["mobility_solves"] = solve_benchmarks(torch, nk, args)
     if rank == 0 and not args.no_cpu_baseline:
         v, s, nodes = cpu_baseline_sample(1500, 6000)
         line["cpu_baseline"] = {"value": v, "unit": "pts/s", "cores": 1, "kind": "port",

@@ -87,10 +87,13 @@ typedef struct nnk_fmm_params {
   int32_t corona_res;    /* 'coronaRes' (default 6)                            */
   int32_t corona_shells; /* 'coronaShells' (default 1)                         */
   int32_t precision;     /* NNK_PREC_FP64 or NNK_PREC_MIXED                    */
-  int32_t m2l_mode;      /* mixed mode M2L operators: 0 auto (images when they
-                            fit 8 GiB), 1 streamed images, 2 generated in-kernel */
+  int32_t m2l_mode;      /* mixed mode M2L: 0 auto (tensor cores, images when
+                            they fit 8 GiB), 1 tensor cores + streamed images,
+                            2 tensor cores + in-kernel operators, 3 FP32 pair
+                            kernel (no tensor cores; FP32-rounding accuracy)  */
   double reg;            /* relative Tikhonov weight of the check-to-equivalent
-                            pseudo-inverse in NNK_PREC_MIXED (0 = default 1e-5) */
+                            pseudo-inverse: NNK_PREC_MIXED 0 = default 1e-5;
+                            NNK_PREC_FP64 0 = exact LU inverse (reference)   */
 } nnk_fmm_params;
 
 /* Algorithmic work of one matvec, from the tree statistics (for rooflines). */

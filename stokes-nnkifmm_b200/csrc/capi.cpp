@@ -44,6 +44,9 @@ int fail(nnk_ctx* ctx, int code, const std::string& msg) {
 void need_gpu(nnk_ctx* ctx) {
   if (!ctx->has_gpu) throw nnk::Error(NNK_E_CUDA, "no CUDA device available: the FMM runs only on the GPU");
   NNK_CUDA(cudaSetDevice(ctx->device));
+  // a launch check reports the last runtime error of this thread; drop any
+  // error left by an earlier call that its caller already handled
+  cudaGetLastError();
 }
 
 // Copies a host or device input to device memory owned by `buf` if needed.

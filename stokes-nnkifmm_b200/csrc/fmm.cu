@@ -72,6 +72,7 @@ struct Solver {
     cusolverDnSetStream(s, st);
     if (cublasCreate(&b) != CUBLAS_STATUS_SUCCESS) throw Error(NNK_E_CUDA, "cublasCreate failed");
     cublasSetStream(b, st);
+    cudaGetLastError();  // library set-up may leave a handled error behind
   }
   ~Solver() {
     if (s) cusolverDnDestroy(s);
@@ -443,7 +444,7 @@ void Fmm::run_group(const TaskGroup& g, const Real* spos, const Real* sstr, cons
 
 void Fmm::build_operators() {
   const HostTree& t = *t_;
-  if (p_.precision == NNK_PREC_MIXED) {
+  if (p_.precision == NNK_PREC_MIXED && p_.m2l_mode != 3) {
     if (p_.m2l_mode == 1) m2l_.image_budget = ~(size_t)0;
     if (p_.m2l_mode == 2) m2l_.image_budget = 0;
     build_m2l_plan(t, p_.res, p_.shells, p_.eps, p_.mu, m2l_, ctx_->stream);
@@ -459,7 +460,10 @@ void Fmm::build_operators() {
   DBuf<double> dK((size_t)n * n), dB((size_t)n * n), dG((size_t)n * n);
   DBuf<int> dpiv(n), dinfo(1);
   int lwork = 0;
-  if (p_.precision == NNK_PREC_FP64) {
+  // FP64 mode uses the exact inverse (the reference's LU solve) unless a
+  // Tikhonov weight is given; mixed mode always regularizes.
+  const bool exact = p_.precision == NNK_PREC_FP64 && !(p_.reg > 0);
+  if (exact) {
     if (cusolverDnDgetrf_bufferSize(sv.s, n, n, dK.p, n, &lwork) != CUSOLVER_STATUS_SUCCESS)
       throw Error(NNK_E_CUDA, "getrf_bufferSize failed");
   } else {
@@ -481,7 +485,7 @@ void Fmm::build_operators() {
     kernel_matrix(us, ds, p_.eps, p_.mu, K, n);
     double* dst = ops_.p + (size_t)L * n * n;
     NNK_CUDA(cudaMemcpyAsync(dK.p, K.data(), K.size() * 8, cudaMemcpyHostToDevice, st));
-    if (p_.precision == NNK_PREC_FP64) {
+    if (exact) {
       // A = K^-1 by LU with partial pivoting, as MATLAB's mldivide
       NNK_CUDA(cudaMemcpyAsync(dst, I.data(), I.size() * 8, cudaMemcpyHostToDevice, st));
       if (cusolverDnDgetrf(sv.s, n, n, dK.p, n, dwork.p, dpiv.p, dinfo.p) != CUSOLVER_STATUS_SUCCESS ||

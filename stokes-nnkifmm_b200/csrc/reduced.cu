@@ -151,6 +151,7 @@ void Fmm::build_reduced() {
     cublasHandle_t h;
     if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) throw Error(NNK_E_CUDA, "cublasCreate failed");
     blas_ = h;
+    cudaGetLastError();
   }
   if (nl) {
     cublasHandle_t h = (cublasHandle_t)blas_;

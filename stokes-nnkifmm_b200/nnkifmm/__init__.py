@@ -11,3 +11,4 @@ from ._lib import (NNKError, MaxDepthError, NoConvergence, context, lib, LIB_PAT
 from .octree import OcTree, nearestMatrix  # noqa: F401
 from .kifmm import KIFMM  # noqa: F401
 from .mobility import Swimmers, Mobility, mobilityProblem, mobilityRHS  # noqa: F401
+from .batch import BatchMobility  # noqa: F401

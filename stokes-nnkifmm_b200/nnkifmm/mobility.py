@@ -133,8 +133,26 @@ class Swimmers:
         self.Tree = OcTree(P, P, finePoints=Fp if len(Fp) else None, NN=NN, **treePar)
         return self
 
-    def genKIFMM(self, kernelPar, **kw):
+    def genKIFMM(self, kernelPar, refine=None, **kw):
+        """KIFMM on the current tree (Swimmers.m:400-410).  With
+        precision='mixed', refine=True (the default for mixed) also builds an
+        FP64 KIFMM used for the outer residuals of iterative refinement."""
+        if kw.get("precision", "fp64") == "mixed":
+            # Mobility systems are ill-conditioned (kappa ~ 1e4); the TF32
+            # rounding of tensor-core M2L (~5e-5) then stalls GMRES near 1e-5
+            # and slows refinement, so solves default to the FP32 pair M2L.
+            kw.setdefault("m2l", "pairs")
         self.FMM = KIFMM(self.Tree, kernelPar, **kw)
+        self.FMM64 = None
+        if kw.get("precision", "fp64") == "mixed" and refine is not False:
+            # the outer residual uses FP64 arithmetic on the same regularized
+            # check-to-equivalent operators, so the two operators differ by
+            # rounding only and the refinement contracts quickly
+            kw64 = dict(kw)
+            kw64["precision"] = "fp64"
+            kw64.pop("m2l", None)
+            kw64["reg"] = kw.get("reg", 0.0) or 1e-5
+            self.FMM64 = KIFMM(self.Tree, kernelPar, **kw64)
         self.mob = None
         return self
 
@@ -164,6 +182,14 @@ class Mobility:
         self.h = h
         self.ctx = fmm.ctx
         self.n = 3 * fmm.tree.info.num_targets + 6 * len(sizes)
+        if getattr(sw, "FMM64", None) is not None:
+            self.set_refinement(sw.FMM64)
+
+    def set_refinement(self, fmm64, max_outer=12, inner_tol=1e-3):
+        """Mixed-precision iterative refinement against an FP64 KIFMM on the same tree."""
+        self.fmm64 = fmm64
+        L.check(L.lib.nnk_mob_set_refinement(self.h, fmm64.h if fmm64 is not None else None, int(max_outer),
+                                             float(inner_tol)), self.ctx.h, "refinement")
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -214,7 +240,7 @@ def mobilityRHS(sw, fluidFunc=None, t=0.0):
 
 def mobilityProblem(swimmers, fluidFunc, t, conditions, kernelPar, TreePar, threads=0, GPU=1,
                     blockSize=0.1, tol=1e-6, maxIter=None, PreconSettings=None, precision="fp64",
-                    return_info=False):
+                    return_info=False, refine=None):
     """Mobility/mobilityProblem.m:1-72.  conditions = (9*nb) [x0; b1; b2] per
     body; returns (9*nb) [U; Om x b1; Om x b2] per body."""
     conditions = np.asarray(conditions, float).ravel()
@@ -223,8 +249,8 @@ def mobilityProblem(swimmers, fluidFunc, t, conditions, kernelPar, TreePar, thre
         d = conditions[9 * i:9 * i + 9]
         swimmers.updateSwimmmer(i + 1, d[0:3], d[3:9])
     swimmers.genTree(**dict(TreePar))
-    swimmers.genKIFMM(kernelPar, parThreads=threads, GPU=GPU, GMRES=1, format=2, blockSize=blockSize,
-                      precision=precision)
+    swimmers.genKIFMM(kernelPar, refine=refine, parThreads=threads, GPU=GPU, GMRES=1, format=2,
+                      blockSize=blockSize, precision=precision)
     mob = swimmers.mobility()
     rhs = mobilityRHS(swimmers, fluidFunc, t)
     x, flag, relres, it = mob.solve(rhs, tol=tol, maxIter=maxIter, precondition=bool(PreconSettings is not None

@@ -20,8 +20,8 @@ def _as_points(a):
 
 class OcTree:
     def __init__(self, potPoints, targetPoints, parThreads=0, nodeCapacity=200, maxDepth=21,
-                 finePoints=None, nearest=0, NN=None, blockSize=0.2, device=0):
-        self.ctx = L.context(device)
+                 finePoints=None, nearest=0, NN=None, blockSize=0.2, device=0, ctx=None):
+        self.ctx = ctx if ctx is not None else L.context(device)
         pot = _as_points(potPoints)
         same = targetPoints is potPoints or (np.shape(targetPoints) == np.shape(potPoints)
                                              and np.array_equal(np.asarray(targetPoints), np.asarray(potPoints)))

@@ -40,3 +40,55 @@ def matvec_at_scale(n_force=250_000, n_quad=1_000_000, n_spheres=20, seed=202612
     fine = mixed_cloud(rng, n_quad, centres, radii)
     forces = rng.standard_normal((n_force, 3))
     return dict(coarse=coarse, fine=fine, forces=forces, eps=1e-3, mu=1.0, cap=64)
+
+
+def prolate_spheroid(a, c, h):
+    """Rings of spacing ~h on a prolate spheroid (minor a, major c), poles
+    first: the construction of Geometries/prolateSpheroid.m."""
+    pts = [np.array([[0.0, 0.0, c], [0.0, 0.0, -c]])]
+    vN = int(np.ceil(np.pi * (3 * (a + c) - np.sqrt((3 * a + c) * (a + 3 * c))) / (2 * h)))
+    for v in np.linspace(0.0, np.pi, vN)[1:-1]:
+        z = c * np.cos(v)
+        uN = int(np.ceil(2 * np.pi * a * np.sqrt(max(0.0, 1 - (z / c) ** 2)) / h))
+        u = np.linspace(0.0, 2 * np.pi, uN + 1)[1:]
+        pts.append(np.stack([a * np.cos(u) * np.sin(v), a * np.sin(u) * np.sin(v), np.full(uN, z)], axis=1))
+    return np.concatenate(pts, axis=0)
+
+
+def _spacing_for_count(a, c, target):
+    lo, hi = 1e-4, 2.0
+    for _ in range(60):  # the point count decreases with h
+        mid = np.sqrt(lo * hi)
+        if len(prolate_spheroid(a, c, mid)) > target:
+            lo = mid
+        else:
+            hi = mid
+    return hi
+
+
+def batched_bodies(n_bodies=64, seed=20261206, nmin=2000, nmax=40000):
+    """Independent rigid prolate spheroids: aspect U[1,5] at equal volume
+    (a = aspect^-1/3, c = aspect^2/3), force-node count U[nmin, nmax] by
+    bisection on the ring spacing h, quadrature at h/4 (about 16x), uniform
+    random orientation.  Returns a list of (force points, quadrature points)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_bodies):
+        asp = rng.uniform(1.0, 5.0)
+        a, c = asp ** (-1.0 / 3.0), asp ** (2.0 / 3.0)
+        h = _spacing_for_count(a, c, int(rng.uniform(nmin, nmax)))
+        q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+        R = q * np.sign(np.diag(r))
+        if np.linalg.det(R) < 0:
+            R[:, 0] = -R[:, 0]
+        coarse = prolate_spheroid(a, c, h) @ R.T
+        fine = prolate_spheroid(a, c, h / 4) @ R.T
+        out.append((coarse, fine))
+    return out
+
+
+def sphere_problem():
+    """Config-1 geometry: Sphere(1,[0 0 0],10) force nodes and Sphere(1,[0 0 0],40)
+    quadrature nodes; eps = 0.01, mu = 1, nodeCapacity 60."""
+    return dict(coarse=cube_sphere(1.0, (0, 0, 0), 10), fine=cube_sphere(1.0, (0, 0, 0), 40), eps=0.01, mu=1.0,
+                cap=60)

@@ -21,14 +21,14 @@ def sphere_body(F, M):
     return c, f, NN, F, M
 
 
-def run_problem(F, M, precon, precision="fp64"):
+def run_problem(F, M, precon, precision="fp64", refine=None):
     c, f, NN, F, M = sphere_body(F, M)
     sw = nk.Swimmers()
     sw.addSwimmer(c, f, NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(c), F, M)
     out, info = nk.mobilityProblem(sw, None, 0.0, np.array([0, 0, 0, 1, 0, 0, 0, 1, 0.0]), [0.01, 1.0],
                                    {"nodeCapacity": 60, "nearest": 1}, tol=1e-8, maxIter=300,
                                    PreconSettings=[1e-6, 100] if precon else None, precision=precision,
-                                   return_info=True)
+                                   return_info=True, refine=refine)
     body = om.Body(c, f, NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(c), F, M)
     asm = om.assemble([body])
     xd = np.linalg.solve(om.dense_mobility_matrix(asm, 0.01, 1.0, True), om.mobility_rhs(asm))
@@ -81,3 +81,17 @@ def test_fmm_gmres_resistance_sphere():
     assert flag == 0 and relres <= 1e-8
     F = (NN @ x.reshape(-1, 3)).sum(0)
     assert abs(F[0] / (6 * np.pi) - 1) < 5e-3
+
+
+@pytest.mark.parametrize("precon", [False, True])
+def test_mixed_refined_solve_matches_dense(precon):
+    """Mixed-precision GMRES with FP64 iterative refinement reaches the FP64
+    operator's solution: rigid velocities within 1e-4 of the dense FP64 solve."""
+    out, info, xd = run_problem([1, 0, 0], [0, 0, 1], precon, precision="mixed")
+    assert info["flag"] == 0 and info["relres"] <= 1e-8
+    U = out[0:3]
+    Om_z = out[3:6][1]
+    assert abs(U[0] - xd[-6]) / abs(xd[-6]) < 1e-4
+    assert abs(Om_z - xd[-1]) / abs(xd[-1]) < 1e-4
+    ref, _, _ = run_problem([1, 0, 0], [0, 0, 1], precon, precision="fp64")
+    assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-6
