@@ -85,7 +85,7 @@ __device__ __forceinline__ void pair_acc(Real tx, Real ty, Real tz, const typena
   const Real d = r2 + e2;
   const Real inv = rsq(d);
   const Real inv3 = inv * inv * inv;
-  const Real a = (d + e2) * inv3;
+  const Real a = e2 * inv3 + inv;  // (r^2 + 2 eps^2) / d^{3/2} = d^{-1/2} + eps^2 d^{-3/2}
   const Real b = (dx * s4.w + dy * s2.x + dz * s2.y) * inv3;
   ax += a * s4.w + b * dx;
   ay += a * s2.x + b * dy;
@@ -112,16 +112,18 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
   Real* __restrict__ out = tk.partial ? partial : out_main;
   const int accumulate = tk.partial ? 0 : accumulate_main;
   for (int t0 = 0; t0 < tk.ntgt; t0 += 2 * BS) {
+    // every thread carries two targets, t and t + npair, so that each source
+    // read from shared memory serves two pair evaluations; when there are
+    // fewer target pairs than threads, threads split the sources
     const int nt = min(2 * BS, tk.ntgt - t0);
-    const bool two = nt > BS;
-    const int n1 = two ? BS : nt;              // targets in the first slot
-    const int splits = two ? 1 : BS / nt;
-    const int mt = tid % n1, ms = tid / n1;
+    const int npair = (nt + 1) >> 1;
+    const int splits = max(1, BS / npair);
+    const int mt = tid % npair, ms = tid / npair;
     const bool act0 = ms < splits;
-    const bool act1 = two && tid + BS < nt;
+    const bool act1 = act0 && mt + npair < nt;
     Real tx = 0, ty = 0, tz = 0, ux = 0, uy = 0, uz = 0;
     if (act0) ldpos(tpos, tk.tgt + t0 + mt, tx, ty, tz);
-    if (act1) ldpos(tpos, tk.tgt + t0 + BS + tid, ux, uy, uz);
+    if (act1) ldpos(tpos, tk.tgt + t0 + npair + mt, ux, uy, uz);
     Real ax = 0, ay = 0, az = 0, bx = 0, by = 0, bz = 0;
     for (int sb = 0; sb < tk.nseg; sb += BS) {
       const int nsb = min(BS, tk.nseg - sb);
@@ -171,33 +173,37 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
         __syncthreads();
         if (f0 + BS + tid < total) fetch(f0 + BS + tid, pa, pb);
         const int nj = min(BS, total - f0);
-        if (two) {
+        if (act0) {
 #pragma unroll 4
-          for (int j = 0; j < nj; ++j) {
+          for (int j = ms; j < nj; j += splits) {
             const T4 a = s4[j];
             const T2 b = s2[j];
             pair_acc<Real>(tx, ty, tz, a, b, e2, ax, ay, az);
-            if (act1) pair_acc<Real>(ux, uy, uz, a, b, e2, bx, by, bz);
+            pair_acc<Real>(ux, uy, uz, a, b, e2, bx, by, bz);  // dummy target (0,0,0) when !act1
           }
-        } else if (act0) {
-#pragma unroll 4
-          for (int j = ms; j < nj; j += splits) pair_acc<Real>(tx, ty, tz, s4[j], s2[j], e2, ax, ay, az);
         }
         __syncthreads();
       }
     }
+    __shared__ Real red2[3 * BS];
     red[tid] = ax;
     red[BS + tid] = ay;
     red[2 * BS + tid] = az;
+    red2[tid] = bx;
+    red2[BS + tid] = by;
+    red2[2 * BS + tid] = bz;
     __syncthreads();
-    if (tid < n1) {
+    for (int q = tid; q < nt; q += BS) {
+      const bool second = q >= npair;
+      const int m = second ? q - npair : q;
+      const Real* rr = second ? red2 : red;
       Real vx = 0, vy = 0, vz = 0;
       for (int k = 0; k < splits; ++k) {
-        vx += red[tid + k * n1];
-        vy += red[BS + tid + k * n1];
-        vz += red[2 * BS + tid + k * n1];
+        vx += rr[m + k * npair];
+        vy += rr[BS + m + k * npair];
+        vz += rr[2 * BS + m + k * npair];
       }
-      const long long o = 3 * (tk.out + t0 + tid);
+      const long long o = 3 * (tk.out + t0 + q);
       if (accumulate) {
         out[o] += scale * vx;
         out[o + 1] += scale * vy;
@@ -206,18 +212,6 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
         out[o] = scale * vx;
         out[o + 1] = scale * vy;
         out[o + 2] = scale * vz;
-      }
-    }
-    if (act1) {
-      const long long o = 3 * (tk.out + t0 + BS + tid);
-      if (accumulate) {
-        out[o] += scale * bx;
-        out[o + 1] += scale * by;
-        out[o + 2] += scale * bz;
-      } else {
-        out[o] = scale * bx;
-        out[o + 1] = scale * by;
-        out[o + 2] = scale * bz;
       }
     }
     __syncthreads();
