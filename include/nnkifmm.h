@@ -56,6 +56,7 @@ typedef struct nnk_ctx nnk_ctx;
 typedef struct nnk_tree nnk_tree;
 typedef struct nnk_fmm nnk_fmm;
 typedef struct nnk_mob nnk_mob;
+typedef struct nnk_batch nnk_batch;
 
 /* OcTree name-value options (OcTree.m:86-95). */
 typedef struct nnk_tree_params {
@@ -239,6 +240,46 @@ int nnk_mob_solve(nnk_mob* mob, const double* rhs, double* x,
  * inner_tol).  fp64 = NULL switches refinement off. */
 int nnk_mob_set_refinement(nnk_mob* mob, nnk_fmm* fp64, int32_t max_outer, double inner_tol);
 int nnk_mob_destroy(nnk_mob* mob);
+
+/* ---------------------------------------------------- batched mobility -- */
+/* No counterpart in the reference, which solves one swimmer system and one
+ * right-hand side per gmres call (mobilityProblem.m:53): nbodies independent
+ * free bodies, each with nrhs right-hand sides (e.g. the 6 rigid modes of
+ * Gen_Resistance.m), solved together.  Body b is trees[b] (potentials ==
+ * targets = its force points; NEAREST trees carry their NN matrix) with
+ * rel_points[b] (N_b x 3) and, for NEAREST, rel_fine[b] (Q_b x 3), the
+ * rotated, untranslated positions of Swimmers.m:177-189.  The trees may be
+ * destroyed after the call.  One FMM pass evaluates all bodies and all their
+ * right-hand sides.  The batch vector is the concatenation of the systems
+ * s = b * nrhs + r, each [f_x(1..N_b) f_y f_z | U (3) | Omega (3)]
+ * (mobilityProblem.m:45-46); system s starts at offsets[s].
+ * params->precision MIXED evaluates pairs (M2L included) in FP32. */
+int nnk_batch_create(nnk_ctx* ctx, int32_t nbodies, nnk_tree* const* trees,
+                     const double* const* rel_points, const double* const* rel_fine,
+                     const nnk_fmm_params* params, int32_t nrhs, nnk_batch** out);
+/* Length of the batch vector and, if offsets != NULL, the nbodies*nrhs + 1
+ * system offsets. */
+int nnk_batch_layout(const nnk_batch* batch, int64_t* length, int64_t* offsets);
+/* Every system's mobility matvec (mobilityMatrixMulti.m:17-36). */
+int nnk_batch_apply(nnk_batch* batch, const double* x, double* y, int32_t on_device);
+/* Unpreconditioned gmres per system (own Krylov space and stopping test,
+ * MATLAB semantics as nnk_mob_solve), all systems advancing together;
+ * info receives one record per system (may be NULL).  Returns NNK_E_NOCONV
+ * if any system stopped above tol. */
+int nnk_batch_solve(nnk_batch* batch, const double* rhs, double* x,
+                    const nnk_solve_params* sp, nnk_solve_info* info, int32_t on_device);
+/* Mixed-precision iterative refinement for a MIXED batch: fp64 != 0 builds an
+ * FP64 FMM on the same bodies (same Tikhonov weight) for the outer residuals
+ * of nnk_batch_solve, as nnk_mob_set_refinement does. */
+int nnk_batch_set_refinement(nnk_batch* batch, int32_t fp64, int32_t max_outer, double inner_tol);
+/* Total FMM matvecs issued so far (inner and outer). */
+int nnk_batch_matvecs(const nnk_batch* batch, int64_t* count);
+/* Per-phase CUDA-event timing of the batch's FMM passes, as
+ * nnk_fmm_profile / nnk_fmm_profile_read (NNK_PHASE_* order); which = 0
+ * reads the batch's own FMM, 1 the FP64 refinement FMM. */
+int nnk_batch_profile(nnk_batch* batch, int32_t enable);
+int nnk_batch_profile_read(nnk_batch* batch, int32_t which, double* ms, int64_t* launches);
+int nnk_batch_destroy(nnk_batch* batch);
 
 /* ------------------------------------------------- allocation-free call -- */
 /* No counterpart in the reference: an extra entry point for callers that

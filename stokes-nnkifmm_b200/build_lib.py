@@ -22,7 +22,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
-            "-Xcompiler", "-ffp-contract=off", "-fmad=true"]
+            "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fopenmp", "-fmad=true"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-Wall", "-Wno-unused-function",
              f"-I{CUDA}/include"]
 

@@ -9,6 +9,7 @@
 #include "common.h"
 #include "fmm.h"
 #include "gmres.h"
+#include "batch.h"
 #include "mobility.h"
 #include "tree.h"
 
@@ -24,6 +25,11 @@ struct nnk_fmm {
 struct nnk_mob {
   nnk_fmm* fmm;
   std::unique_ptr<nnk::Mobility> m;
+};
+struct nnk_batch {
+  nnk_ctx* ctx;
+  std::unique_ptr<nnk::BatchMobility> m;
+  nnk::DBuf<double> io_in, io_out;
 };
 
 namespace {
@@ -400,6 +406,115 @@ int nnk_mob_set_refinement(nnk_mob* mob, nnk_fmm* fp64, int32_t max_outer, doubl
 
 int nnk_mob_destroy(nnk_mob* mob) {
   delete mob;
+  return NNK_OK;
+}
+
+int nnk_batch_create(nnk_ctx* ctx, int32_t nbodies, nnk_tree* const* trees, const double* const* rel_points,
+                     const double* const* rel_fine, const nnk_fmm_params* params, int32_t nrhs, nnk_batch** out) {
+  if (!ctx || !trees || !rel_points || !params || !out || nbodies < 1 || nrhs < 1)
+    return fail(ctx, NNK_E_ARG, "bad arguments");
+  API_TRY
+  need_gpu(ctx);
+  std::vector<nnk::BatchBody> bodies(nbodies);
+  for (int b = 0; b < nbodies; ++b) {
+    if (!trees[b] || !rel_points[b]) return fail(ctx, NNK_E_ARG, "null tree or rel_points");
+    bodies[b] = nnk::BatchBody{&trees[b]->t, rel_points[b], rel_fine ? rel_fine[b] : nullptr};
+  }
+  nnk::FmmParams p;
+  p.eps = params->eps;
+  p.mu = params->mu;
+  p.res = params->corona_res > 0 ? params->corona_res : 6;
+  p.shells = params->corona_shells > 0 ? params->corona_shells : 1;
+  p.precision = params->precision;
+  p.m2l_mode = params->m2l_mode;
+  p.reg = params->reg;
+  if (p.precision != NNK_PREC_FP64 && p.precision != NNK_PREC_MIXED) return fail(ctx, NNK_E_ARG, "bad precision");
+  std::unique_ptr<nnk_batch> bt(new nnk_batch());
+  bt->ctx = ctx;
+  bt->m.reset(new nnk::BatchMobility(ctx, bodies, p, nrhs));
+  *out = bt.release();
+  API_CATCH(ctx)
+}
+
+int nnk_batch_layout(const nnk_batch* batch, int64_t* length, int64_t* offsets) {
+  if (!batch) return NNK_E_ARG;
+  if (length) *length = batch->m->size();
+  if (offsets) {
+    const auto& o = batch->m->offsets();
+    std::copy(o.begin(), o.end(), offsets);
+  }
+  return NNK_OK;
+}
+
+int nnk_batch_apply(nnk_batch* batch, const double* x, double* y, int32_t on_device) {
+  if (!batch || !x || !y) return NNK_E_ARG;
+  nnk_ctx* ctx = batch->ctx;
+  API_TRY
+  need_gpu(ctx);
+  const size_t n = (size_t)batch->m->size();
+  const double* dx = stage_in(ctx, batch->io_in, x, n, on_device);
+  double* dy = stage_out(batch->io_out, y, n, on_device);
+  batch->m->apply(dx, dy);
+  finish_out(ctx, batch->io_out, y, n, on_device);
+  API_CATCH(ctx)
+}
+
+int nnk_batch_solve(nnk_batch* batch, const double* rhs, double* x, const nnk_solve_params* sp, nnk_solve_info* info,
+                    int32_t on_device) {
+  if (!batch || !rhs || !x || !sp) return NNK_E_ARG;
+  nnk_ctx* ctx = batch->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::BatchMobility& M = *batch->m;
+  const size_t n = (size_t)M.size();
+  const double* db = stage_in(ctx, batch->io_in, rhs, n, on_device);
+  double* dx = stage_out(batch->io_out, x, n, on_device);
+  std::vector<nnk_solve_info> inf(M.systems());
+  M.solve(db, dx, *sp, inf.data());
+  finish_out(ctx, batch->io_out, x, n, on_device);
+  if (info) std::copy(inf.begin(), inf.end(), info);
+  for (const auto& i : inf)
+    if (i.flag != 0) return fail(ctx, NNK_E_NOCONV, "gmres stopped at maxit above tol for some system");
+  API_CATCH(ctx)
+}
+
+int nnk_batch_set_refinement(nnk_batch* batch, int32_t fp64, int32_t max_outer, double inner_tol) {
+  if (!batch) return NNK_E_ARG;
+  nnk_ctx* ctx = batch->ctx;
+  API_TRY
+  need_gpu(ctx);
+  batch->m->set_refinement(fp64 != 0, max_outer, inner_tol);
+  API_CATCH(ctx)
+}
+
+int nnk_batch_matvecs(const nnk_batch* batch, int64_t* count) {
+  if (!batch || !count) return NNK_E_ARG;
+  *count = batch->m->matvecs();
+  return NNK_OK;
+}
+
+int nnk_batch_profile(nnk_batch* batch, int32_t enable) {
+  if (!batch) return NNK_E_ARG;
+  nnk_ctx* ctx = batch->ctx;
+  API_TRY
+  batch->m->fmm().set_profile(enable != 0);
+  if (batch->m->ref64()) batch->m->ref64()->set_profile(enable != 0);
+  API_CATCH(ctx)
+}
+
+int nnk_batch_profile_read(nnk_batch* batch, int32_t which, double* ms, int64_t* launches) {
+  if (!batch || which < 0 || which > 1) return NNK_E_ARG;
+  nnk_ctx* ctx = batch->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Fmm* f = which == 0 ? &batch->m->fmm() : batch->m->ref64();
+  if (!f) return fail(ctx, NNK_E_STATE, "no refinement FMM");
+  f->read_profile(ms, launches);
+  API_CATCH(ctx)
+}
+
+int nnk_batch_destroy(nnk_batch* batch) {
+  delete batch;
   return NNK_OK;
 }
 

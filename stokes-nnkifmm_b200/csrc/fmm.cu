@@ -7,6 +7,7 @@
 #include <type_traits>
 #include <cmath>
 #include <cstring>
+#include <map>
 
 #include "fmm.h"
 #include "kernels.cuh"
@@ -86,11 +87,14 @@ Fmm::Fmm(nnk_ctx* ctx, const HostTree* tree, const FmmParams& p) : ctx_(ctx), t_
   if (!(p.eps > 0) || !(p.mu > 0)) throw Error(NNK_E_ARG, "kernelPar needs eps > 0 and mu > 0");
   if (p.res < 2 || p.shells < 1 || 2 * p.shells > p.res)
     throw Error(NNK_E_ARG, "bad coronaRes/coronaShells");
+  if (p.max_rhs < 1) throw Error(NNK_E_ARG, "max_rhs must be >= 1");
+  R_ = p.max_rhs;
   P_ = (int)shell_lattice(p.res, p.shells).size();
   N_ = t_->nodes;
   E_ = t_->src_start[N_];
   tot_ = E_ + 2LL * P_ * N_;
   maxl_ = t_->max_level;
+  assign_operators();
   build_points();
   build_tasks();
   build_operators();
@@ -166,10 +170,15 @@ Fmm& Fmm::sparse() {
 void Fmm::build_points() {
   const HostTree& t = *t_;
   cudaStream_t st = ctx_->stream;
-  const double* root = &t.corners[0];
-  for (int d = 0; d < 3; ++d) shift_[d] = 0.5 * (root[d] + root[3 + d]);
+  const int G = t.groups();
+  shift_.assign(3 * (size_t)G, 0.0);
+  for (int g = 0; g < G; ++g) {
+    const double* root = &t.corners[6 * (size_t)t.root_of(g)];
+    for (int d = 0; d < 3; ++d) shift_[3 * g + d] = 0.5 * (root[d] + root[3 + d]);
+  }
   auto lat = shell_lattice(p_.res, p_.shells);
   std::vector<double> pos(3 * (size_t)tot_);
+  std::vector<int32_t> pgroup(tot_, 0);  // tree of every unified point
   std::copy(t.src_pos.begin(), t.src_pos.end(), pos.begin());
   for (int n = 0; n < N_; ++n) {
     const double* c = &t.corners[6 * n];
@@ -182,30 +191,40 @@ void Fmm::build_points() {
       dhi[d] = hi[d] + w[d];
     }
     surface(dlo, dhi, p_.res, lat, &pos[3 * (E_ + (size_t)P_ * N_ + (size_t)P_ * n)]);
+    const int32_t g = t.group_of(n);
+    for (int64_t e = t.src_start[n]; e < t.src_start[n + 1]; ++e) pgroup[e] = g;
+    for (int k = 0; k < P_; ++k) {
+      pgroup[E_ + (size_t)P_ * n + k] = g;
+      pgroup[E_ + (size_t)P_ * N_ + (size_t)P_ * n + k] = g;
+    }
   }
   const int64_t nt = (int64_t)t.tgt_row.size();
   if (p_.precision == NNK_PREC_FP64) {
     pos64_.upload(pos, st);
     tpos64_.upload(t.tgt_pos, st);
-    str64_.alloc(3 * tot_);
-    check64_.alloc((size_t)N_ * 3 * P_);
-    vel64_.alloc(3 * nt);
+    str64_.alloc(3 * tot_ * R_);
+    check64_.alloc((size_t)N_ * 3 * P_ * R_);
+    vel64_.alloc(3 * nt * R_);
   } else {
     std::vector<float> p4(4 * (size_t)tot_);
     for (int64_t i = 0; i < tot_; ++i) {
-      for (int d = 0; d < 3; ++d) p4[4 * i + d] = (float)(pos[3 * i + d] - shift_[d]);
+      const double* sh = &shift_[3 * (size_t)pgroup[i]];
+      for (int d = 0; d < 3; ++d) p4[4 * i + d] = (float)(pos[3 * i + d] - sh[d]);
       p4[4 * i + 3] = 0.f;
     }
     pos32_.upload(p4, st);
     std::vector<float> t4(4 * (size_t)nt);
-    for (int64_t i = 0; i < nt; ++i) {
-      for (int d = 0; d < 3; ++d) t4[4 * i + d] = (float)(t.tgt_pos[3 * i + d] - shift_[d]);
-      t4[4 * i + 3] = 0.f;
+    for (int32_t n = 0; n < N_; ++n) {
+      const double* sh = &shift_[3 * (size_t)t.group_of(n)];
+      for (int64_t i = t.tgt_start[n]; i < t.tgt_start[n + 1]; ++i) {
+        for (int d = 0; d < 3; ++d) t4[4 * i + d] = (float)(t.tgt_pos[3 * i + d] - sh[d]);
+        t4[4 * i + 3] = 0.f;
+      }
     }
     tpos32_.upload(t4, st);
-    str32_.alloc(3 * tot_);
-    check32_.alloc((size_t)N_ * 3 * P_);
-    vel32_.alloc(3 * nt);
+    str32_.alloc(3 * tot_ * R_);
+    check32_.alloc((size_t)N_ * 3 * P_ * R_);
+    vel32_.alloc(3 * nt * R_);
   }
   trow_.upload(t.tgt_row, st);
   goff_.upload(t.src_goff, st);
@@ -277,7 +296,7 @@ void Fmm::build_tasks() {
     for (int32_t n : t.by_level[L]) {
       TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
       for (int64_t k = t.X.off[n]; k < t.X.off[n + 1]; ++k) src_seg(t.X.idx[k]);
-      if (t.parent[n] > 0) segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
+      if (t.level[n] >= 2) segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
       tk.nseg = (int)segs.size() - tk.seg0;
       tasks.push_back(tk);
     }
@@ -293,7 +312,7 @@ void Fmm::build_tasks() {
         ++m2l;
       }
       for (int64_t k = t.X.off[n]; k < t.X.off[n + 1]; ++k) pairs_down += (int64_t)P_ * src_seg(t.X.idx[k]);
-      if (t.parent[n] > 0) {
+      if (t.level[n] >= 2) {  // the root's downward expansion is zero
         segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
         pairs_down += (int64_t)P_ * P_;
       }
@@ -333,11 +352,23 @@ void Fmm::build_tasks() {
   lvl_off_[maxl_ + 1] = (int64_t)ln.size();
   c2e = (int64_t)ln.size() + (int64_t)up_nodes_host_.size();
   cudaStream_t st = ctx_->stream;
+  {
+    std::vector<C2ETile> ut, dt;
+    build_c2e_tiles(up_nodes_host_, up_off_, ut, up_toff_);
+    build_c2e_tiles(ln, lvl_off_, dt, dn_toff_);
+    up_tiles_.upload(ut, st);
+    dn_tiles_.upload(dt, st);
+  }
   split_tasks(tasks, segs);
   tasks_.upload(tasks, st);
   segs_.upload(segs, st);
   lvl_nodes_.upload(ln, st);
   up_nodes_.upload(up_nodes_host_, st);
+  {
+    std::vector<int32_t> roots(t.groups());
+    for (int g = 0; g < t.groups(); ++g) roots[g] = t.root_of(g);
+    roots_.upload(roots, st);
+  }
   NNK_CUDA(cudaStreamSynchronize(st));
   stats_.pairs_leaf = pairs_leaf;
   stats_.pairs_p2p = pairs_p2p;
@@ -347,6 +378,28 @@ void Fmm::build_tasks() {
   stats_.c2e_columns = c2e;
   stats_.surface_points = P_;
   stats_.levels = maxl_ + 1;
+}
+
+// Per level, runs of nodes of the same tree cut into tiles of at most 32
+// nodes; the operator index is filled in by build_operators.
+void Fmm::build_c2e_tiles(const std::vector<int32_t>& nodes, const std::vector<int64_t>& off,
+                          std::vector<C2ETile>& tiles, std::vector<int64_t>& toff) {
+  const HostTree& t = *t_;
+  toff.assign(off.size(), 0);
+  for (size_t L = 0; L + 1 < off.size(); ++L) {
+    toff[L] = (int64_t)tiles.size();
+    int64_t i = off[L];
+    while (i < off[L + 1]) {
+      const int32_t g = t.group_of(nodes[i]);
+      int64_t j = i;
+      while (j < off[L + 1] && j - i < 32 && t.group_of(nodes[j]) == g) ++j;
+      const int op = op_of_[(size_t)g * (maxl_ + 1) + L];
+      if (op < 0) throw Error(NNK_E_STATE, "node above its tree's depth");
+      tiles.push_back(C2ETile{op, (int)i, (int)(j - i), 0});
+      i = j;
+    }
+  }
+  toff[off.size() - 1] = (int64_t)tiles.size();
 }
 
 // Load balance: within each launch group, tasks run heaviest first, and a
@@ -424,23 +477,56 @@ void Fmm::split_tasks(std::vector<TaskD>& tasks, std::vector<SegD>& segs) {
   tasks.swap(nt);
   segs.swap(ns);
   reds_.upload(reds, ctx_->stream);
-  if (p_.precision == NNK_PREC_FP64) partial64_.alloc(std::max<int64_t>(3 * pbase, 1));
-  else partial32_.alloc(std::max<int64_t>(3 * pbase, 1));
+  if (p_.precision == NNK_PREC_FP64) partial64_.alloc(std::max<int64_t>(3 * pbase * R_, 1));
+  else partial32_.alloc(std::max<int64_t>(3 * pbase * R_, 1));
 }
 
 template <typename Real>
 void Fmm::run_group(const TaskGroup& g, const Real* spos, const Real* sstr, const Real* tpos, Real* out, Real e2,
-                    Real scale, int accumulate, int phase_id) {
+                    Real scale, int accumulate, int phase_id, int R) {
   if (g.count == 0) return;
   cudaStream_t st = ctx_->stream;
   Real* partial = std::is_same<Real, double>::value ? (Real*)partial64_.p : (Real*)partial32_.p;
   phase(phase_id, [&] {
     launch_p2p<Real>(tasks_.p + g.first, (int)g.count, segs_.p, spos, sstr, tpos, out, partial, e2, scale, st,
-                     accumulate);
+                     accumulate, R);
   });
   if (g.red_count)
-    phase(phase_id, [&] { launch_reduce<Real>(reds_.p + g.red_first, (int)g.red_count, partial, out, accumulate, st); });
+    phase(phase_id,
+          [&] { launch_reduce<Real>(reds_.p + g.red_first, (int)g.red_count, partial, out, accumulate, st, R); });
 }
+
+// Operator index of every (tree, level): one per distinct box width.
+void Fmm::assign_operators() {
+  const HostTree& t = *t_;
+  const int G = t.groups();
+  std::vector<int> gmax(G, 0);
+  for (int32_t n = 0; n < N_; ++n) gmax[t.group_of(n)] = std::max(gmax[t.group_of(n)], t.level[n]);
+  op_of_.assign((size_t)G * (maxl_ + 1), -1);
+  op_w_.clear();
+  std::map<double, int> by_w;
+  for (int g = 0; g < G; ++g) {
+    const double* root = &t.corners[6 * (size_t)t.root_of(g)];
+    const double W0 = root[3] - root[0];
+    for (int L = 0; L <= gmax[g]; ++L) {
+      const double w = std::ldexp(W0, -L);
+      auto it = by_w.find(w);
+      if (it == by_w.end()) {
+        it = by_w.emplace(w, (int)op_w_.size()).first;
+        op_w_.push_back(w);
+      }
+      op_of_[(size_t)g * (maxl_ + 1) + L] = it->second;
+    }
+  }
+  nops_ = (int)op_w_.size();
+}
+
+namespace {
+__global__ void add_diag_kernel(double* G, int n, double v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) G[(size_t)i * n + i] += v;
+}
+}  // namespace
 
 void Fmm::build_operators() {
   const HostTree& t = *t_;
@@ -452,17 +538,57 @@ void Fmm::build_operators() {
     stats_.m2l_tile_rows = m2l_.tile_slots * 128;
   }
   const int n = 3 * P_;
-  const double W0 = t.corners[3] - t.corners[0];
   cudaStream_t st = ctx_->stream;
-  ops_.alloc((size_t)(maxl_ + 1) * n * n);
+  ops_.alloc((size_t)nops_ * n * n);
   auto lat = shell_lattice(p_.res, p_.shells);
-  Solver sv(st);
-  DBuf<double> dK((size_t)n * n), dB((size_t)n * n), dG((size_t)n * n);
-  DBuf<int> dpiv(n), dinfo(1);
-  int lwork = 0;
   // FP64 mode uses the exact inverse (the reference's LU solve) unless a
   // Tikhonov weight is given; mixed mode always regularizes.
   const bool exact = p_.precision == NNK_PREC_FP64 && !(p_.reg > 0);
+  const double reg = p_.reg > 0 ? p_.reg : 1e-5;
+  // host part, in parallel over operators: K_up = kernel(upsurf, downsurf)
+  // (up-equivalent densities -> down check) and, for the Tikhonov form,
+  // sigma_max(K) by power iteration
+  std::vector<std::vector<double>> Ks(nops_);
+  std::vector<double> lam2(nops_, 0.0);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int o = 0; o < nops_; ++o) {
+    const double w = op_w_[o];
+    const double lo[3] = {0, 0, 0}, hi[3] = {w, w, w};
+    const double dlo[3] = {-w, -w, -w}, dhi[3] = {2 * w, 2 * w, 2 * w};
+    std::vector<double> us(3 * P_), ds(3 * P_);
+    surface(lo, hi, p_.res, lat, us.data());
+    surface(dlo, dhi, p_.res, lat, ds.data());
+    std::vector<double>& K = Ks[o];
+    K.assign((size_t)n * n, 0.0);
+    kernel_matrix(us, ds, p_.eps, p_.mu, K, n);
+    if (!exact) {
+      std::vector<double> v(n, 1.0), u(n);
+      double smax = 0;
+      for (int it = 0; it < 40; ++it) {
+        for (int r = 0; r < n; ++r) {
+          double sum = 0;
+          for (int c = 0; c < n; ++c) sum += K[(size_t)c * n + r] * v[c];
+          u[r] = sum;
+        }
+        double nu = 0;
+        for (int c = 0; c < n; ++c) {
+          double sum = 0;
+          for (int r = 0; r < n; ++r) sum += K[(size_t)c * n + r] * u[r];
+          v[c] = sum;
+          nu += sum * sum;
+        }
+        nu = std::sqrt(nu);
+        smax = std::sqrt(nu);
+        for (double& x : v) x /= nu;
+      }
+      lam2[o] = (reg * smax) * (reg * smax);
+    }
+  }
+  Solver sv(st);
+  DBuf<double> dK((size_t)n * n), dG((size_t)n * n);
+  DBuf<int> dpiv(n), dinfo(std::max(nops_, 1));
+  dinfo.zero(st);
+  int lwork = 0;
   if (exact) {
     if (cusolverDnDgetrf_bufferSize(sv.s, n, n, dK.p, n, &lwork) != CUSOLVER_STATUS_SUCCESS)
       throw Error(NNK_E_CUDA, "getrf_bufferSize failed");
@@ -472,51 +598,22 @@ void Fmm::build_operators() {
       throw Error(NNK_E_CUDA, "potrf_bufferSize failed");
   }
   DBuf<double> dwork(std::max(lwork, 1));
-  std::vector<double> K((size_t)n * n), I((size_t)n * n, 0.0), KT((size_t)n * n);
+  std::vector<double> I((size_t)n * n, 0.0), KT;
   for (int i = 0; i < n; ++i) I[(size_t)i * n + i] = 1.0;
-  for (int L = 0; L <= maxl_; ++L) {
-    const double w = std::ldexp(W0, -L);
-    const double lo[3] = {0, 0, 0}, hi[3] = {w, w, w};
-    const double dlo[3] = {-w, -w, -w}, dhi[3] = {2 * w, 2 * w, 2 * w};
-    std::vector<double> us(3 * P_), ds(3 * P_);
-    surface(lo, hi, p_.res, lat, us.data());
-    surface(dlo, dhi, p_.res, lat, ds.data());
-    // K_up = kernel(upsurf, downsurf): up-equivalent densities -> down check
-    kernel_matrix(us, ds, p_.eps, p_.mu, K, n);
-    double* dst = ops_.p + (size_t)L * n * n;
+  for (int o = 0; o < nops_; ++o) {
+    const std::vector<double>& K = Ks[o];
+    double* dst = ops_.p + (size_t)o * n * n;
     NNK_CUDA(cudaMemcpyAsync(dK.p, K.data(), K.size() * 8, cudaMemcpyHostToDevice, st));
     if (exact) {
       // A = K^-1 by LU with partial pivoting, as MATLAB's mldivide
       NNK_CUDA(cudaMemcpyAsync(dst, I.data(), I.size() * 8, cudaMemcpyHostToDevice, st));
-      if (cusolverDnDgetrf(sv.s, n, n, dK.p, n, dwork.p, dpiv.p, dinfo.p) != CUSOLVER_STATUS_SUCCESS ||
-          cusolverDnDgetrs(sv.s, CUBLAS_OP_N, n, n, dK.p, n, dpiv.p, dst, n, dinfo.p) !=
+      if (cusolverDnDgetrf(sv.s, n, n, dK.p, n, dwork.p, dpiv.p, dinfo.p + o) != CUSOLVER_STATUS_SUCCESS ||
+          cusolverDnDgetrs(sv.s, CUBLAS_OP_N, n, n, dK.p, n, dpiv.p, dst, n, dinfo.p + o) !=
               CUSOLVER_STATUS_SUCCESS)
         throw Error(NNK_E_CUDA, "LU of the surface matrix failed");
     } else {
       // A = (K^T K + lam^2 I)^-1 K^T, lam = reg * sigma_max(K)
-      double smax = 0;
-      {
-        std::vector<double> v(n, 1.0), u(n);
-        for (int it = 0; it < 40; ++it) {
-          for (int r = 0; r < n; ++r) {
-            double s = 0;
-            for (int c = 0; c < n; ++c) s += K[(size_t)c * n + r] * v[c];
-            u[r] = s;
-          }
-          double nu = 0;
-          for (int c = 0; c < n; ++c) {
-            double s = 0;
-            for (int r = 0; r < n; ++r) s += K[(size_t)c * n + r] * u[r];
-            v[c] = s;
-            nu += s * s;
-          }
-          nu = std::sqrt(nu);
-          smax = std::sqrt(nu);
-          for (double& x : v) x /= nu;
-        }
-      }
-      const double reg = p_.reg > 0 ? p_.reg : 1e-5;
-      const double lam2 = (reg * smax) * (reg * smax);
+      KT.resize((size_t)n * n);
       for (int r = 0; r < n; ++r)
         for (int c = 0; c < n; ++c) KT[(size_t)c * n + r] = K[(size_t)r * n + c];
       NNK_CUDA(cudaMemcpyAsync(dst, KT.data(), KT.size() * 8, cudaMemcpyHostToDevice, st));
@@ -524,26 +621,38 @@ void Fmm::build_operators() {
       if (cublasDgemm(sv.b, CUBLAS_OP_T, CUBLAS_OP_N, n, n, n, &one, dK.p, n, dK.p, n, &zero, dG.p, n) !=
           CUBLAS_STATUS_SUCCESS)
         throw Error(NNK_E_CUDA, "K^T K product failed");
-      std::vector<double> G((size_t)n * n);
-      NNK_CUDA(cudaMemcpyAsync(G.data(), dG.p, G.size() * 8, cudaMemcpyDeviceToHost, st));
-      NNK_CUDA(cudaStreamSynchronize(st));
-      for (int i = 0; i < n; ++i) G[(size_t)i * n + i] += lam2;
-      NNK_CUDA(cudaMemcpyAsync(dG.p, G.data(), G.size() * 8, cudaMemcpyHostToDevice, st));
-      if (cusolverDnDpotrf(sv.s, CUBLAS_FILL_MODE_LOWER, n, dG.p, n, dwork.p, lwork, dinfo.p) !=
+      add_diag_kernel<<<(n + 127) / 128, 128, 0, st>>>(dG.p, n, lam2[o]);
+      NNK_CHECK_LAUNCH();
+      if (cusolverDnDpotrf(sv.s, CUBLAS_FILL_MODE_LOWER, n, dG.p, n, dwork.p, lwork, dinfo.p + o) !=
               CUSOLVER_STATUS_SUCCESS ||
-          cusolverDnDpotrs(sv.s, CUBLAS_FILL_MODE_LOWER, n, n, dG.p, n, dst, n, dinfo.p) !=
+          cusolverDnDpotrs(sv.s, CUBLAS_FILL_MODE_LOWER, n, n, dG.p, n, dst, n, dinfo.p + o) !=
               CUSOLVER_STATUS_SUCCESS)
         throw Error(NNK_E_CUDA, "Cholesky of the regularized surface matrix failed");
     }
-    int info = 0;
-    NNK_CUDA(cudaMemcpyAsync(&info, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    // the host copies above read pageable memory; keep K alive until done
     NNK_CUDA(cudaStreamSynchronize(st));
-    if (info != 0) throw Error(NNK_E_CUDA, "surface matrix factorization reported info=" + std::to_string(info));
   }
+  std::vector<int> info(std::max(nops_, 1), 0);
+  NNK_CUDA(cudaMemcpyAsync(info.data(), dinfo.p, info.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+  NNK_CUDA(cudaStreamSynchronize(st));
+  for (int o = 0; o < nops_; ++o)
+    if (info[o] != 0)
+      throw Error(NNK_E_CUDA, "surface matrix factorization reported info=" + std::to_string(info[o]));
 }
 
+namespace {
+// Zeroes the down-equivalent densities of the roots (never computed: the
+// root's downward expansion is zero, downwardPass.m:39-40).
 template <typename Real>
-void Fmm::apply_impl(const double* d_in, double* d_out, int layout) {
+__global__ void zero_roots_kernel(const int32_t* __restrict__ roots, long long base, int P, int C,
+                                  Real* __restrict__ str) {
+  Real* p = str + (long long)C * (base + (long long)P * roots[blockIdx.x]);
+  for (int i = threadIdx.x; i < P * C; i += blockDim.x) p[i] = 0;
+}
+}  // namespace
+
+template <typename Real>
+void Fmm::apply_impl(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int k0, int R) {
   cudaStream_t st = ctx_->stream;
   const HostTree& t = *t_;
   Real* str = p_.precision == NNK_PREC_FP64 ? (Real*)str64_.p : (Real*)str32_.p;
@@ -554,21 +663,24 @@ void Fmm::apply_impl(const double* d_in, double* d_out, int layout) {
   const Real e2 = (Real)(p_.eps * p_.eps);
   const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
   const int n = 3 * P_;
+  const int C = 3 * R;
   // forces on the leaf source entries (kron(NN,I3)*f per leaf)
-  phase(NNK_PHASE_GATHER, [&] { launch_gather<Real>(E_, goff_.p, gidx_.p, gw_.p, d_in, layout, t.n_pot, str, st); });
-  // expansions of nodes that are not computed stay zero
-  NNK_CUDA(cudaMemsetAsync(str + 3 * E_, 0, sizeof(Real) * 3 * (size_t)P_ * N_, st));
-  NNK_CUDA(cudaMemsetAsync(str + 3 * (E_ + (size_t)P_ * N_), 0, sizeof(Real) * 3 * (size_t)P_, st));
+  phase(NNK_PHASE_GATHER, [&] { launch_gather<Real>(E_, goff_.p, gidx_.p, gw_.p, d_in, in, k0, R, str, st); });
+  // up-equivalent densities of nodes that are not computed stay zero
+  NNK_CUDA(cudaMemsetAsync(str + C * E_, 0, sizeof(Real) * C * (size_t)P_ * N_, st));
+  zero_roots_kernel<Real><<<(unsigned)roots_.n, 256, 0, st>>>(roots_.p, E_ + (long long)P_ * N_, P_, C, str);
+  NNK_CHECK_LAUNCH();
   const bool tm = tensor_m2l_ && std::is_same<Real, float>::value;
+  if (tm && R != 1) throw Error(NNK_E_STATE, "tensor-core M2L takes one right-hand side per pass");
   if (tm && m2l_.h_err && *m2l_.h_err)
     throw Error(NNK_E_TIMEOUT, "tensor-core M2L gave up a bounded wait in an earlier call");
   // upward pass
   for (int L = maxl_; L >= 1; --L) {
     if (up_[L].count == 0) continue;
-    run_group<Real>(up_[L], pos, str, pos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS);
-    const int64_t nn = up_off_[L + 1] - up_off_[L];
+    run_group<Real>(up_[L], pos, str, pos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS, R);
+    const int64_t nt = up_toff_[L + 1] - up_toff_[L];
     phase(NNK_PHASE_UP_C2E, [&] {
-      launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 0, up_nodes_.p + up_off_[L], (int)nn, check, str, E_, P_, st,
+      launch_c2e<Real>(ops_.p, n, 0, up_tiles_.p + up_toff_[L], (int)nt, up_nodes_.p, check, str, E_, P_, R, st,
                        tm ? m2l_.src.p : nullptr, m2l_.NP);
     });
   }
@@ -581,33 +693,42 @@ void Fmm::apply_impl(const double* d_in, double* d_out, int layout) {
   const std::vector<TaskGroup>& dgroups = tm ? down_nov_ : down_;
   for (int L = 1; L <= maxl_; ++L) {
     if (dgroups[L].count == 0) continue;
-    run_group<Real>(dgroups[L], pos, str, pos, check, e2, scale, tm ? 1 : 0, NNK_PHASE_DOWN_PAIRS);
-    const int64_t nn = lvl_off_[L + 1] - lvl_off_[L];
+    run_group<Real>(dgroups[L], pos, str, pos, check, e2, scale, tm ? 1 : 0, NNK_PHASE_DOWN_PAIRS, R);
+    const int64_t nt = dn_toff_[L + 1] - dn_toff_[L];
     phase(NNK_PHASE_DOWN_C2E, [&] {
-      launch_c2e<Real>(ops_.p + (size_t)L * n * n, n, 1, lvl_nodes_.p + lvl_off_[L], (int)nn, check, str,
-                       E_ + (int64_t)P_ * N_, P_, st);
+      launch_c2e<Real>(ops_.p, n, 1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str,
+                       E_ + (int64_t)P_ * N_, P_, R, st);
     });
   }
   // leaf stage
-  run_group<Real>(leaf_, pos, str, tpos, vel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS);
+  run_group<Real>(leaf_, pos, str, tpos, vel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS, R);
   phase(NNK_PHASE_SCATTER,
-        [&] { launch_scatter<Real>((int64_t)t.tgt_row.size(), trow_.p, vel, layout, t.n_tgt, d_out, st); });
+        [&] { launch_scatter<Real>((int64_t)t.tgt_row.size(), trow_.p, vel, out, k0, R, d_out, st); });
 }
 
 void Fmm::apply(const double* d_in, double* d_out, int layout, int nrhs) {
   const HostTree& t = *t_;
-  for (int r = 0; r < nrhs; ++r) {
-    const double* in = d_in + (size_t)r * 3 * t.n_pot;
-    double* out = d_out + (size_t)r * 3 * t.n_tgt;
-    if (t.n_tgt == 0) continue;
+  IoMap in, out;
+  in.layout = out.layout = layout;
+  in.nrows = t.n_pot;
+  out.nrows = t.n_tgt;
+  apply_mapped(d_in, in, d_out, out, nrhs);
+}
+
+void Fmm::apply_mapped(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int nrhs) {
+  if (t_->n_tgt == 0) return;
+  const int cap = tensor_m2l_ ? 1 : R_;
+  for (int k0 = 0; k0 < nrhs;) {
+    const int R = rhs_chunk(nrhs - k0, cap);
     if (p_.precision == NNK_PREC_FP64)
-      apply_impl<double>(in, out, layout);
+      apply_impl<double>(d_in, in, d_out, out, k0, R);
     else
-      apply_impl<float>(in, out, layout);
+      apply_impl<float>(d_in, in, d_out, out, k0, R);
+    k0 += R;
   }
 }
 
-template void Fmm::apply_impl<double>(const double*, double*, int);
-template void Fmm::apply_impl<float>(const double*, double*, int);
+template void Fmm::apply_impl<double>(const double*, const IoMap&, double*, const IoMap&, int, int);
+template void Fmm::apply_impl<float>(const double*, const IoMap&, double*, const IoMap&, int, int);
 
 }  // namespace nnk

@@ -51,6 +51,29 @@ struct FmmParams {
   int precision = NNK_PREC_FP64;
   int m2l_mode = 0;
   double reg = 0.0;
+  int max_rhs = 1;  // right-hand sides evaluated together (work buffers scale with it)
+};
+
+// Where the x, y and z components of row r of right-hand side k live in a
+// caller's FP64 vector: x at off(r) + k * rstr(r), y and z at +cstr(r) and
+// +2 cstr(r) (device tables).  Without per-row tables (off == nullptr) the
+// standard layouts apply: rows (interleaved, KIFMM format 1) or blocked
+// (format 2), with the right-hand sides 3 * nrows apart.
+struct IoMap {
+  const long long* off = nullptr;
+  const int* cstr = nullptr;
+  const long long* rstr = nullptr;
+  int layout = NNK_LAYOUT_ROWS;
+  long long nrows = 0;
+};
+
+// Nodes nodes[first .. first+count) of one level (count <= 32) that share
+// the check-to-equivalent operator `op`.
+struct C2ETile {
+  int op;
+  int first;
+  int count;
+  int pad;
 };
 
 class Fmm {
@@ -59,6 +82,8 @@ class Fmm {
   ~Fmm();
   // in: potentials (n_pot x 3, FP64, device), out: velocities (n_tgt x 3, FP64, device)
   void apply(const double* d_in, double* d_out, int layout, int nrhs);
+  // Same with explicit per-row placement of the input and output vectors.
+  void apply_mapped(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int nrhs);
   // Same, but over the p=4 surfaces (computeVelSparse).
   Fmm& sparse();
   void reduced_apply(const double* d_in, double* d_out, int layout);
@@ -74,15 +99,19 @@ class Fmm {
   DBuf<double> io_in, io_out;
 
  private:
-  template <typename Real> void apply_impl(const double* d_in, double* d_out, int layout);
+  template <typename Real>
+  void apply_impl(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int k0, int R);
   void build_points();
   void build_tasks();
+  void assign_operators();
   void build_operators();
   void build_reduced();
   void split_tasks(std::vector<TaskD>& tasks, std::vector<SegD>& segs);
   template <typename Real>
   void run_group(const TaskGroup& g, const Real* spos, const Real* sstr, const Real* tpos, Real* out, Real e2,
-                 Real scale, int accumulate, int phase_id);
+                 Real scale, int accumulate, int phase_id, int R);
+  void build_c2e_tiles(const std::vector<int32_t>& nodes, const std::vector<int64_t>& off,
+                       std::vector<C2ETile>& tiles, std::vector<int64_t>& toff);
 
   nnk_ctx* ctx_;
   const HostTree* t_;
@@ -92,7 +121,8 @@ class Fmm {
   int64_t E_ = 0;        // leaf source entries
   int64_t tot_ = 0;      // E + 2 P N
   int maxl_ = 0;
-  double shift_[3] = {0, 0, 0};  // FP32 positions are relative to the root centre
+  int R_ = 1;            // right-hand sides the work buffers hold
+  std::vector<double> shift_;  // per tree of the forest: FP32 positions are relative to its root centre
 
   // unified point/strength arrays
   DBuf<double> pos64_;   // tot*3
@@ -119,13 +149,20 @@ class Fmm {
   bool tensor_m2l_ = false;
   TaskGroup leaf_;
   DBuf<int32_t> lvl_nodes_;
+  DBuf<int32_t> roots_;
   std::vector<int64_t> lvl_off_;
   std::vector<int32_t> up_nodes_host_;  // per level: nodes whose uppot is computed
   DBuf<int32_t> up_nodes_;
   std::vector<int64_t> up_off_;
-  // operators: per level, uppot = A_L * check (A_L = K_up^-1 or its Tikhonov form);
-  // downpot = A_L^T * check.
+  // operators: per (tree, level), uppot = A * check (A = K_up^-1 or its
+  // Tikhonov form), downpot = A^T * check.  A depends only on the box width,
+  // so trees and levels of equal width share one operator.
   DBuf<double> ops_;
+  int nops_ = 0;
+  std::vector<double> op_w_;          // box width of each operator
+  std::vector<int> op_of_;            // (group * (maxl + 1) + level) -> operator
+  DBuf<C2ETile> up_tiles_, dn_tiles_;  // per level, tiles of nodes sharing an operator
+  std::vector<int64_t> up_toff_, dn_toff_;
   // work buffers
   DBuf<double> check64_, vel64_;
   DBuf<float> check32_, vel32_;

@@ -24,41 +24,59 @@ __device__ __forceinline__ void ldpos(const float* __restrict__ p, long long j, 
 __device__ __forceinline__ double rsq(double d) { return rsqrt(d); }
 __device__ __forceinline__ float rsq(float d) { return rsqrtf(d); }
 
+// ------------------------------------------------------------ vector I/O
+__device__ __forceinline__ void io_index(const IoMap& m, long long r, long long& off, long long& cs,
+                                         long long& rs) {
+  if (m.off) {
+    off = m.off[r];
+    cs = m.cstr[r];
+    rs = m.rstr[r];
+  } else if (m.layout == NNK_LAYOUT_BLOCKED) {
+    off = r;
+    cs = m.nrows;
+    rs = 3 * m.nrows;
+  } else {
+    off = 3 * r;
+    cs = 1;
+    rs = 3 * m.nrows;
+  }
+}
+
 // ----------------------------------------------------------------- gather
-// Force density of each leaf source entry: sum_k w_k f(row_k), i.e. the row of
-// kron(NN_sub, I3) * f for NEAREST entries (nearestBlockComputation.m:28-29),
-// or the potential itself in plain mode.  f is FP64 in the caller's layout.
+// Force density of each leaf source entry for right-hand sides k0..k0+R-1:
+// sum_k w_k f(row_k), i.e. the row of kron(NN_sub, I3) * f for NEAREST
+// entries (nearestBlockComputation.m:28-29), or the potential itself in plain
+// mode.  Strengths are stored entry-major: str[(e * R + k) * 3 + c].
 template <typename Real>
 __global__ void gather_kernel(long long E, const long long* __restrict__ goff, const int* __restrict__ gidx,
-                              const double* __restrict__ gw, const double* __restrict__ f, int layout,
-                              long long npot, Real* __restrict__ str) {
+                              const double* __restrict__ gw, const double* __restrict__ f, IoMap m, int k0, int R,
+                              Real* __restrict__ str) {
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= E) return;
-  double x = 0, y = 0, z = 0;
-  for (long long k = goff[e]; k < goff[e + 1]; ++k) {
-    const double w = gw[k];
-    const long long r = gidx[k];
-    if (layout == NNK_LAYOUT_BLOCKED) {
-      x += w * f[r];
-      y += w * f[npot + r];
-      z += w * f[2 * npot + r];
-    } else {
-      x += w * f[3 * r];
-      y += w * f[3 * r + 1];
-      z += w * f[3 * r + 2];
+  for (int k = 0; k < R; ++k) {
+    double x = 0, y = 0, z = 0;
+    for (long long g = goff[e]; g < goff[e + 1]; ++g) {
+      const double w = gw[g];
+      long long off, cs, rs;
+      io_index(m, gidx[g], off, cs, rs);
+      const double* v = f + off + (k0 + k) * rs;
+      x += w * v[0];
+      y += w * v[cs];
+      z += w * v[2 * cs];
     }
+    Real* o = str + 3 * (e * R + k);
+    o[0] = (Real)x;
+    o[1] = (Real)y;
+    o[2] = (Real)z;
   }
-  str[3 * e] = (Real)x;
-  str[3 * e + 1] = (Real)y;
-  str[3 * e + 2] = (Real)z;
 }
 
 template <typename Real>
 inline void launch_gather(int64_t E, const int64_t* goff, const int32_t* gidx, const double* gw,
-                          const double* f, int layout, int64_t npot, Real* str, cudaStream_t st) {
+                          const double* f, const IoMap& m, int k0, int R, Real* str, cudaStream_t st) {
   if (E == 0) return;
-  gather_kernel<Real><<<(unsigned)((E + 255) / 256), 256, 0, st>>>(
-      E, (const long long*)goff, gidx, gw, f, layout, npot, str);
+  gather_kernel<Real><<<(unsigned)((E + 255) / 256), 256, 0, st>>>(E, (const long long*)goff, gidx, gw, f, m, k0,
+                                                                    R, str);
   NNK_CHECK_LAUNCH();
 }
 
@@ -218,57 +236,219 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
   }
 }
 
+// The same pair sum for R right-hand sides at once: the geometry (r, the
+// inverse square root and the Stokeslet weight) is shared, and each source
+// carries R force vectors, str[(j * R + k) * 3 + c]; outputs are stored the
+// same way.  One target per thread; below BS targets, threads split the
+// sources and reduce through shared memory.
+template <typename Real, int BS, int R>
+__global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__ tasks,
+                                                       const SegD* __restrict__ segs,
+                                                       const Real* __restrict__ spos,
+                                                       const Real* __restrict__ sstr,
+                                                       const Real* __restrict__ tpos, Real* __restrict__ out_main,
+                                                       Real* __restrict__ partial, Real e2, Real scale,
+                                                       int accumulate_main) {
+  using T4 = typename Vec4T<Real>::t4;
+  constexpr int C = 3 * R;
+  __shared__ T4 sp[BS];
+  __shared__ Real sf[BS][C];
+  __shared__ long long seg_start[BS];
+  __shared__ int seg_end[BS];
+  __shared__ Real red[C][BS];
+  const TaskD tk = tasks[blockIdx.x];
+  const int tid = threadIdx.x;
+  Real* __restrict__ out = tk.partial ? partial : out_main;
+  const int accumulate = tk.partial ? 0 : accumulate_main;
+  for (int t0 = 0; t0 < tk.ntgt; t0 += BS) {
+    const int nt = min(BS, tk.ntgt - t0);
+    const int splits = max(1, BS / nt);
+    const int mt = tid % nt, ms = tid / nt;
+    const bool act = ms < splits;
+    Real tx = 0, ty = 0, tz = 0;
+    if (act) ldpos(tpos, tk.tgt + t0 + mt, tx, ty, tz);
+    Real acc[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = 0;
+    for (int sb = 0; sb < tk.nseg; sb += BS) {
+      const int nsb = min(BS, tk.nseg - sb);
+      __syncthreads();
+      int cnt = 0;
+      if (tid < nsb) {
+        const SegD sg = segs[tk.seg0 + sb + tid];
+        seg_start[tid] = sg.start;
+        cnt = sg.count;
+      }
+      seg_end[tid] = cnt;
+      __syncthreads();
+      for (int o = 1; o < BS; o <<= 1) {  // inclusive scan
+        const int v = tid >= o ? seg_end[tid - o] : 0;
+        __syncthreads();
+        seg_end[tid] += v;
+        __syncthreads();
+      }
+      const int total = seg_end[nsb - 1];
+      auto fetch = [&](int f, T4& a, Real* b) {
+        int lo = 0, hi = nsb - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (seg_end[mid] > f) hi = mid;
+          else lo = mid + 1;
+        }
+        const long long j = seg_start[lo] + (f - (lo ? seg_end[lo - 1] : 0));
+        Real x, y, z;
+        ldpos(spos, j, x, y, z);
+        a.x = x;
+        a.y = y;
+        a.z = z;
+        a.w = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) b[c] = sstr[j * C + c];
+      };
+      T4 pa;
+      Real pb[C];
+      if (tid < total) fetch(tid, pa, pb);
+      for (int f0 = 0; f0 < total; f0 += BS) {
+        if (f0 + tid < total) {
+          sp[tid] = pa;
+#pragma unroll
+          for (int c = 0; c < C; ++c) sf[tid][c] = pb[c];
+        }
+        __syncthreads();
+        if (f0 + BS + tid < total) fetch(f0 + BS + tid, pa, pb);
+        const int nj = min(BS, total - f0);
+        if (act) {
+#pragma unroll 2
+          for (int j = ms; j < nj; j += splits) {
+            const T4 q = sp[j];
+            const Real dx = tx - q.x, dy = ty - q.y, dz = tz - q.z;
+            const Real d = dx * dx + dy * dy + dz * dz + e2;
+            const Real inv = rsq(d);
+            const Real inv3 = inv * inv * inv;
+            const Real a = e2 * inv3 + inv;
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+              const Real fx = sf[j][3 * k], fy = sf[j][3 * k + 1], fz = sf[j][3 * k + 2];
+              const Real b = (dx * fx + dy * fy + dz * fz) * inv3;
+              acc[3 * k] += a * fx + b * dx;
+              acc[3 * k + 1] += a * fy + b * dy;
+              acc[3 * k + 2] += a * fz + b * dz;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) red[c][tid] = acc[c];
+    __syncthreads();
+    for (int v = tid; v < nt * C; v += BS) {
+      const int q = v / C, c = v - q * C;
+      Real sum = 0;
+      for (int k = 0; k < splits; ++k) sum += red[c][q + k * nt];
+      const long long o = (long long)C * (tk.out + t0 + q) + c;
+      if (accumulate) out[o] += scale * sum;
+      else out[o] = scale * sum;
+    }
+    __syncthreads();
+  }
+}
+
 template <typename Real>
 inline void launch_p2p(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
                        const Real* tpos, Real* out, Real* partial, Real e2, Real scale, cudaStream_t st,
-                       int accumulate = 0) {
+                       int accumulate = 0, int R = 1) {
   if (ntasks == 0) return;
-  p2p_kernel<Real, 128><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale, accumulate);
+  switch (R) {
+    case 1:
+      p2p_kernel<Real, 128><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
+                                                     accumulate);
+      break;
+    case 2:
+      p2p_multi_kernel<Real, 128, 2><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
+                                                              accumulate);
+      break;
+    case 3:
+      p2p_multi_kernel<Real, 128, 3><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
+                                                              accumulate);
+      break;
+    case 4:
+      p2p_multi_kernel<Real, 128, 4><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
+                                                              accumulate);
+      break;
+    case 6:
+      p2p_multi_kernel<Real, 128, 6><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
+                                                              accumulate);
+      break;
+    default:
+      throw Error(NNK_E_ARG, "pair kernel supports 1, 2, 3, 4 or 6 right-hand sides per launch");
+  }
   NNK_CHECK_LAUNCH();
 }
 
+// Right-hand-side counts with a pair kernel, largest first.
+inline int rhs_chunk(int remaining, int max_rhs) {
+  static const int sizes[] = {6, 4, 3, 2, 1};
+  for (int r : sizes)
+    if (r <= remaining && r <= max_rhs) return r;
+  return 1;
+}
+
 // out(task) (+)= sum_i partial(piece i), pieces summed in index order so the
-// result does not depend on scheduling.
+// result does not depend on scheduling.  C = 3 R values per target.
 template <typename Real>
 __global__ void reduce_partials_kernel(const RedD* __restrict__ reds, const Real* __restrict__ partial,
-                                       Real* __restrict__ out, int accumulate) {
+                                       Real* __restrict__ out, int accumulate, int C) {
   const RedD r = reds[blockIdx.x];
-  const int n = 3 * r.ntgt;
+  const int n = C * r.ntgt;
   for (int v = threadIdx.x; v < n; v += blockDim.x) {
     Real s = 0;
-    for (int i = 0; i < r.k; ++i) s += partial[3 * (r.pbase + (long long)i * r.ntgt) + v];
-    if (accumulate) out[3 * r.out + v] += s;
-    else out[3 * r.out + v] = s;
+    for (int i = 0; i < r.k; ++i) s += partial[C * (r.pbase + (long long)i * r.ntgt) + v];
+    if (accumulate) out[C * r.out + v] += s;
+    else out[C * r.out + v] = s;
   }
 }
 
 template <typename Real>
 inline void launch_reduce(const RedD* reds, int nreds, const Real* partial, Real* out, int accumulate,
-                          cudaStream_t st) {
+                          cudaStream_t st, int R = 1) {
   if (nreds == 0) return;
-  reduce_partials_kernel<Real><<<nreds, 128, 0, st>>>(reds, partial, out, accumulate);
+  reduce_partials_kernel<Real><<<nreds, 128, 0, st>>>(reds, partial, out, accumulate, 3 * R);
   NNK_CHECK_LAUNCH();
 }
 
 // -------------------------------------------------------------------- C2E
-// Check-to-equivalent step for all nodes of one level:
-//   dst(node) = Aop * check(node), Aop = A (upward) or A^T (downward),
-// A stored column-major (n x n), FP64 arithmetic.  dst(node) is the
-// strength block of the node's surface points in the unified arrays.
+// Check-to-equivalent step for the nodes of one level:
+//   dst(node, k) = Aop * check(node, k), Aop = A (upward) or A^T (downward),
+// for right-hand sides k < R, FP64 arithmetic.  A tile is up to 32 nodes that
+// share one operator (a level of one tree of the forest); A is the n x n
+// column-major operator ops + op * n^2.  check and dst hold, per surface
+// point p of a node, R consecutive 3-vectors: check[(node * P + p) * R + k].
 template <typename Real>
-__global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ A, int n, int trans,
-                                                  const int* __restrict__ nodes, int nnodes,
+__global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops, int n, int trans,
+                                                  const C2ETile* __restrict__ tiles, const int* __restrict__ nodes,
                                                   const Real* __restrict__ check, Real* __restrict__ dst,
-                                                  long long base, int P, float* __restrict__ m2l_dst, int NP) {
+                                                  long long base, int P, int R, float* __restrict__ m2l_dst, int NP) {
   constexpr int BM = 64, BN = 32, BK = 16;
   __shared__ double As[BK][BM + 1];
   __shared__ double Bs[BK][BN + 1];
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  __shared__ int col_node[BN];
+  __shared__ int col_k[BN];
+  const C2ETile tl = tiles[blockIdx.y];
+  const int m0 = blockIdx.x * BM, j0 = blockIdx.z * BN;
+  const int ncol = tl.count * R;
+  if (j0 >= ncol) return;
+  const double* __restrict__ A = ops + (size_t)tl.op * n * n;
   const int tid = threadIdx.x;
+  if (tid < BN) {
+    const int j = j0 + tid;
+    col_node[tid] = j < ncol ? nodes[tl.first + j / R] : -1;
+    col_k[tid] = j < ncol ? j % R : 0;
+  }
+  __syncthreads();
   const int tr = tid % 16, tc = tid / 16;
   double acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
   for (int k0 = 0; k0 < n; k0 += BK) {
-    // A tile: rows m0..m0+63, k k0..k0+15
     for (int e = tid; e < BK * BM; e += 256) {
       int kk, mm;
       if (!trans) { mm = e % BM; kk = e / BM; }   // A[r][c] at c*n + r: contiguous in r
@@ -280,9 +460,12 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ A, 
     }
     for (int e = tid; e < BK * BN; e += 256) {
       const int kk = e % BK, nn = e / BK;
-      const int c = k0 + kk, j = n0 + nn;
+      const int c = k0 + kk, node = col_node[nn];
       double v = 0;
-      if (c < n && j < nnodes) v = (double)check[(size_t)nodes[j] * n + c];
+      if (c < n && node >= 0) {
+        const int p = c / 3, comp = c - 3 * p;
+        v = (double)check[(((size_t)node * P + p) * R + col_k[nn]) * 3 + comp];
+      }
       Bs[kk][nn] = v;
     }
     __syncthreads();
@@ -304,52 +487,55 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ A, 
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      const int r = m0 + tr + 16 * i, jj = n0 + tc + 16 * j;
-      if (r < n && jj < nnodes) {
-        dst[(base + (long long)P * nodes[jj]) * 3 + r] = (Real)acc[i][j];
+      const int r = m0 + tr + 16 * i, jj = tc + 16 * j;
+      const int node = col_node[jj];
+      if (r < n && node >= 0) {
+        const int p = r / 3, comp = r - 3 * p;
+        dst[((base + (long long)P * node + p) * R + col_k[jj]) * 3 + comp] = (Real)acc[i][j];
         if (m2l_dst) {
           uint32_t t;
           asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"((float)acc[i][j]));
-          m2l_dst[(size_t)nodes[jj] * NP + r] = __uint_as_float(t);
+          m2l_dst[(size_t)node * NP + r] = __uint_as_float(t);
         }
       }
     }
 }
 
 template <typename Real>
-inline void launch_c2e(const double* A, int n, int trans, const int32_t* nodes, int nnodes, const Real* check,
-                       Real* dst, int64_t base, int P, cudaStream_t st, float* m2l_dst = nullptr, int NP = 0) {
-  if (nnodes == 0) return;
-  dim3 grid((n + 63) / 64, (nnodes + 31) / 32);
-  c2e_kernel<Real><<<grid, 256, 0, st>>>(A, n, trans, nodes, nnodes, check, dst, base, P, m2l_dst, NP);
+inline void launch_c2e(const double* ops, int n, int trans, const C2ETile* tiles, int ntiles, const int32_t* nodes,
+                       const Real* check, Real* dst, int64_t base, int P, int R, cudaStream_t st,
+                       float* m2l_dst = nullptr, int NP = 0) {
+  if (ntiles == 0) return;
+  dim3 grid((n + 63) / 64, ntiles, R);
+  c2e_kernel<Real><<<grid, 256, 0, st>>>(ops, n, trans, tiles, nodes, check, dst, base, P, R, m2l_dst, NP);
   NNK_CHECK_LAUNCH();
 }
 
 // ---------------------------------------------------------------- scatter
 // Sorted-by-leaf velocities back to the reference's target order
-// (downwardPass.m:297-305), in the caller's layout.
+// (downwardPass.m:297-305), in the caller's layout, right-hand sides
+// k0..k0+R-1.
 template <typename Real>
-__global__ void scatter_kernel(long long nt, const int* __restrict__ row, const Real* __restrict__ vel,
-                               int layout, long long ntgt, double* __restrict__ out) {
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nt) return;
-  const long long r = row[k];
-  if (layout == NNK_LAYOUT_BLOCKED) {
-    out[r] = (double)vel[3 * k];
-    out[ntgt + r] = (double)vel[3 * k + 1];
-    out[2 * ntgt + r] = (double)vel[3 * k + 2];
-  } else {
-    out[3 * r] = (double)vel[3 * k];
-    out[3 * r + 1] = (double)vel[3 * k + 1];
-    out[3 * r + 2] = (double)vel[3 * k + 2];
+__global__ void scatter_kernel(long long nt, const int* __restrict__ row, const Real* __restrict__ vel, IoMap m,
+                               int k0, int R, double* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  long long off, cs, rs;
+  io_index(m, row[t], off, cs, rs);
+  for (int k = 0; k < R; ++k) {
+    const Real* v = vel + 3 * (t * R + k);
+    double* o = out + off + (k0 + k) * rs;
+    o[0] = (double)v[0];
+    o[cs] = (double)v[1];
+    o[2 * cs] = (double)v[2];
   }
 }
 
 template <typename Real>
-inline void launch_scatter(int64_t nt, const int32_t* row, const Real* vel, int layout, int64_t ntgt,
+inline void launch_scatter(int64_t nt, const int32_t* row, const Real* vel, const IoMap& m, int k0, int R,
                            double* out, cudaStream_t st) {
   if (nt == 0) return;
-  scatter_kernel<Real><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nt, row, vel, layout, ntgt, out);
+  scatter_kernel<Real><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nt, row, vel, m, k0, R, out);
   NNK_CHECK_LAUNCH();
 }
 

@@ -469,17 +469,21 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
   if (NP > 512 || NP / (NP > 256 ? 2 : 1) % 16 != 0)
     throw Error(NNK_E_ARG, "tensor-core M2L supports 3P up to 512 with N halves a multiple of 16");
   plan.NP = NP;
-  const double W0 = t.corners[3] - t.corners[0];
   std::vector<int> tile_nodes, tile_slot0, slot_code, slot_src, slot_op;
   std::vector<float> slot_h;
   std::vector<M2LUnit> units;
   std::vector<int> img_code;      // per operator image: offset code
   std::vector<double> img_w;      // per operator image: box width of its level
   int64_t useful = 0, tslots = 0;
-  for (int L = 1; L <= t.max_level; ++L) {
+  // one pass per (level, tree of the forest): the operators depend on the
+  // box width, which differs between trees
+  for (int L = 1; L <= t.max_level; ++L)
+  for (int g = 0; g < t.groups(); ++g) {
+    const double* root = &t.corners[6 * (size_t)t.root_of(g)];
+    const double W0 = root[3] - root[0];
     std::vector<int32_t> nodes;
     for (int32_t n : t.by_level[L])
-      if (t.V.off[n + 1] > t.V.off[n]) nodes.push_back(n);
+      if (t.group_of(n) == g && t.V.off[n + 1] > t.V.off[n]) nodes.push_back(n);
     if (nodes.empty()) continue;
     auto oct = [&](int32_t n) { return ((t.ix[n] & 1) << 2) | ((t.iy[n] & 1) << 1) | (t.iz[n] & 1); };
     // signature: octant, then the bitset of V offsets (343 codes), so that

@@ -114,9 +114,12 @@ extern "C" int nnk_direct_nearest_noalloc(int32_t device, void* stream, const do
   }
   if (rc == NNK_OK && m > 0) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    nnk::IoMap rows;
+    rows.layout = NNK_LAYOUT_ROWS;
+    rows.nrows = n;
     if (q > 0)
       nnk::gather_kernel<double><<<(unsigned)((q + 255) / 256), 256, 0, st>>>(
-          (long long)q, (const long long*)nn_rowptr, nn_col, nn_val, forces, NNK_LAYOUT_ROWS, (long long)n, scratch);
+          (long long)q, (const long long*)nn_rowptr, nn_col, nn_val, forces, rows, 0, 1, scratch);
     direct_kernel<<<(unsigned)((m + 255) / 256), 256, 0, st>>>((long long)m, targets, (long long)q, fine, scratch,
                                                               eps * eps, 1.0 / (8.0 * M_PI * mu), vel);
     if (cudaGetLastError() != cudaSuccess) rc = NNK_E_CUDA;

@@ -11,6 +11,7 @@
 #include <unordered_map>
 
 #include "../../include/nnkifmm.h"
+#include "common.h"
 
 namespace nnk {
 
@@ -579,6 +580,69 @@ void nearest_matrix(const double* coarse, int64_t n, const double* fine, int64_t
       val[rowptr[r] + k] = w;
     }
   }
+}
+
+void merge_forest(const std::vector<const HostTree*>& trees, HostTree& f) {
+  f = HostTree();
+  if (trees.empty()) throw Error(NNK_E_ARG, "empty forest");
+  f.params = trees[0]->params;
+  auto cat_csr = [](Csr& dst, const Csr& src, int32_t node_off, bool first) {
+    const int64_t base = dst.off.empty() ? 0 : dst.off.back();
+    if (first) dst.off.push_back(0);
+    for (size_t r = 1; r < src.off.size(); ++r) dst.off.push_back(base + src.off[r]);
+    for (int32_t v : src.idx) dst.idx.push_back(v + node_off);
+  };
+  int64_t E = 0, G = 0, T = 0, npot = 0, ntgt = 0;
+  for (size_t k = 0; k < trees.size(); ++k) {
+    const HostTree& t = *trees[k];
+    if (t.params.nearest != f.params.nearest) throw Error(NNK_E_ARG, "forest trees must agree on NEAREST");
+    const int32_t off = f.nodes;
+    f.roots.push_back(off);
+    f.max_level = std::max(f.max_level, t.max_level);
+    for (int32_t n = 0; n < t.nodes; ++n) {
+      f.level.push_back(t.level[n]);
+      f.parent.push_back(t.parent[n] < 0 ? -1 : t.parent[n] + off);
+      f.child0.push_back(t.child0[n] < 0 ? -1 : t.child0[n] + off);
+      f.ix.push_back(t.ix[n]);
+      f.iy.push_back(t.iy[n]);
+      f.iz.push_back(t.iz[n]);
+      f.tleaf.push_back(t.tleaf[n]);
+      f.pleaf.push_back(t.pleaf[n]);
+      f.group.push_back((int32_t)k);
+    }
+    f.corners.insert(f.corners.end(), t.corners.begin(), t.corners.end());
+    cat_csr(f.U, t.U, off, k == 0);
+    cat_csr(f.V, t.V, off, k == 0);
+    cat_csr(f.W, t.W, off, k == 0);
+    cat_csr(f.X, t.X, off, k == 0);
+    if (k == 0) {
+      f.src_start.push_back(0);
+      f.tgt_start.push_back(0);
+      f.src_goff.push_back(0);
+    }
+    for (int32_t n = 0; n < t.nodes; ++n) {
+      f.src_start.push_back(E + t.src_start[n + 1]);
+      f.tgt_start.push_back(T + t.tgt_start[n + 1]);
+    }
+    f.src_pos.insert(f.src_pos.end(), t.src_pos.begin(), t.src_pos.end());
+    for (size_t e = 1; e < t.src_goff.size(); ++e) f.src_goff.push_back(G + t.src_goff[e]);
+    for (int32_t r : t.src_gidx) f.src_gidx.push_back((int32_t)(r + npot));
+    f.src_gw.insert(f.src_gw.end(), t.src_gw.begin(), t.src_gw.end());
+    for (int32_t r : t.tgt_row) f.tgt_row.push_back((int32_t)(r + ntgt));
+    f.tgt_pos.insert(f.tgt_pos.end(), t.tgt_pos.begin(), t.tgt_pos.end());
+    f.nodes += t.nodes;
+    E += t.src_start[t.nodes];
+    G += t.src_goff.empty() ? 0 : t.src_goff.back();
+    T += (int64_t)t.tgt_row.size();
+    npot += t.n_pot;
+    ntgt += t.n_tgt;
+    f.n += t.n;
+  }
+  if (npot > INT32_MAX || ntgt > INT32_MAX) throw Error(NNK_E_ARG, "forest too large for 32-bit rows");
+  f.n_pot = npot;
+  f.n_tgt = ntgt;
+  f.by_level.assign(f.max_level + 1, {});
+  for (int32_t n = 0; n < f.nodes; ++n) f.by_level[f.level[n]].push_back(n);
 }
 
 }  // namespace nnk

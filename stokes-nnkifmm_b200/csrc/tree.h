@@ -73,6 +73,14 @@ struct HostTree {
   std::vector<int32_t> tgt_row;     // output row per sorted target
   std::vector<double> tgt_pos;      // sorted target positions
 
+  // ---- forest: several independent trees in one set of arrays (batched
+  // bodies).  A single tree is the forest of one group.
+  std::vector<int32_t> group;       // per node: tree of the forest (empty: all 0)
+  std::vector<int32_t> roots;       // root node per group (empty: {0})
+  int32_t groups() const { return roots.empty() ? 1 : (int32_t)roots.size(); }
+  int32_t group_of(int32_t n) const { return group.empty() ? 0 : group[n]; }
+  int32_t root_of(int32_t g) const { return roots.empty() ? 0 : roots[g]; }
+
   bool touch(int32_t a, int32_t b) const;  // nodeintersection.m closed-box test
 };
 
@@ -81,6 +89,13 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
                const double* fine, int64_t q, const int64_t* nn_rowptr,
                const int32_t* nn_col, const double* nn_val, const TreeParams& p,
                HostTree& t, std::string& msg);
+
+// Concatenates trees into one forest: node ids, list entries, leaf source
+// entries, gather rows and target rows of tree k are offset by the totals of
+// trees 0..k-1, and `group` records the tree of every node.  No list links
+// two trees, so the FMM of the forest is the block-diagonal operator of the
+// separate trees.  A tree may appear several times.
+void merge_forest(const std::vector<const HostTree*>& trees, HostTree& out);
 
 // nearestMatrix (Tools/Nearest/nearestMatrix.m:17-41), exact FP64 ties.
 void nearest_matrix(const double* coarse, int64_t n, const double* fine, int64_t q,

@@ -94,6 +94,15 @@ SIGNATURES = {
     "nnk_mob_solve": (_i32, [_vp, _vp, _vp, C.POINTER(SolveParams), _i32, C.POINTER(SolveInfo), _i32]),
     "nnk_mob_set_refinement": (_i32, [_vp, _vp, _i32, _f64]),
     "nnk_mob_destroy": (_i32, [_vp]),
+    "nnk_batch_create": (_i32, [_vp, _i32, _vp, _vp, _vp, C.POINTER(FmmParams), _i32, C.POINTER(_vp)]),
+    "nnk_batch_layout": (_i32, [_vp, _pi64, _vp]),
+    "nnk_batch_apply": (_i32, [_vp, _vp, _vp, _i32]),
+    "nnk_batch_solve": (_i32, [_vp, _vp, _vp, C.POINTER(SolveParams), _vp, _i32]),
+    "nnk_batch_set_refinement": (_i32, [_vp, _i32, _i32, _f64]),
+    "nnk_batch_matvecs": (_i32, [_vp, _pi64]),
+    "nnk_batch_profile": (_i32, [_vp, _i32]),
+    "nnk_batch_profile_read": (_i32, [_vp, _i32, _vp, _vp]),
+    "nnk_batch_destroy": (_i32, [_vp]),
     "nnk_direct_nearest_noalloc": (_i32, [_i32, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _i64, _f64, _f64,
                                           _vp]),
 }

@@ -1,26 +1,42 @@
-"""Many independent rigid-body mobility problems solved together.
+"""Many independent rigid-body mobility problems.
 
-Each body gets its own device context (its own CUDA stream), NEAREST tree,
-KIFMM (mixed precision with FP64 refinement, or FP64) and mobility operator;
-host threads drive the bodies concurrently so that the kernels of different
-bodies overlap on the GPU, and each body's 6 rigid-mode right-hand sides
-(unit forces and unit torques, the columns of Resistance/Gen_Resistance.m's
-modes in mobility form) are solved one after another on its stream.
+`Body` is one body solved the reference's way: its own NEAREST tree, KIFMM
+and mobility operator, one gmres call per right-hand side
+(mobilityProblem.m:53).  `BatchMobility` solves all bodies and all their
+right-hand sides together through nnk_batch_*: the bodies' trees form one
+forest, one FMM pass evaluates every body and every right-hand side (the pair
+kernels share the geometry of a pair across a body's right-hand sides), and
+GMRES runs per system with all systems advancing in lockstep.
+
+The right-hand sides of `solve_modes` are the 6 rigid modes in mobility form:
+unit force or unit torque, no slip (the columns of Gen_Resistance.m's modes),
+so the result per body is its 6 x 6 mobility matrix.
 """
-import concurrent.futures as cf
+import ctypes as C
 
 import numpy as np
 
 from . import _lib as L
 from .mobility import Swimmers, mobilityRHS
-from .octree import nearestMatrix
+from .octree import OcTree, nearestMatrix
 
 RIGID_MODES = [("F", 0), ("F", 1), ("F", 2), ("M", 0), ("M", 1), ("M", 2)]
 
 
+def mode_rhs(n_points, mode):
+    """[f (3N) = 0 | F | M] with the unit force or torque of `mode`."""
+    kind, k = mode
+    v = np.zeros(3 * n_points + 6)
+    v[3 * n_points + (0 if kind == "F" else 3) + k] = 1.0
+    return v
+
+
 class Body:
-    def __init__(self, coarse, fine, kernelPar, cap, precision, device, preconditioned, refine=None, m2l="pairs"):
-        self.ctx = L.Context(device)
+    """One body through the per-body path (Swimmers + KIFMM + nnk_mob)."""
+
+    def __init__(self, coarse, fine, kernelPar, cap, precision, device=0, preconditioned=False, refine=None,
+                 m2l="pairs", ctx=None):
+        self.ctx = ctx if ctx is not None else L.Context(device)
         self.coarse, self.fine = coarse, fine
         NN = nearestMatrix(coarse, fine)
         self.sw = Swimmers()
@@ -55,14 +71,107 @@ class Body:
 
 
 class BatchMobility:
-    def __init__(self, bodies, kernelPar, cap=200, precision="mixed", device=0, workers=8,
-                 preconditioned=False, refine=None, m2l="pairs"):
-        self.workers = workers
-        with cf.ThreadPoolExecutor(max_workers=workers) as ex:
-            self.bodies = list(ex.map(lambda b: Body(b[0], b[1], kernelPar, cap, precision, device,
-                                                     preconditioned, refine, m2l), bodies))
+    """All bodies x nrhs right-hand sides in one batch (nnk_batch_*).
 
-    def solve_all(self, tol=1e-6, maxIter=200, modes=RIGID_MODES):
-        with cf.ThreadPoolExecutor(max_workers=self.workers) as ex:
-            res = list(ex.map(lambda b: b.solve_modes(tol, maxIter, modes), self.bodies))
-        return [r[0] for r in res], [r[1] for r in res]
+    bodies: list of (force points N_b x 3, fine points Q_b x 3), each a free
+    body at rest orientation (rel points = the points themselves).
+    precision 'mixed' uses FP32 pair kernels (M2L included) with FP64
+    iterative refinement unless refine=False."""
+
+    def __init__(self, bodies, kernelPar, cap=200, precision="mixed", nrhs=6, refine=None, device=0, ctx=None,
+                 max_outer=12, inner_tol=1e-3):
+        self.ctx = ctx if ctx is not None else L.Context(device)
+        self.nrhs = int(nrhs)
+        self.sizes = []
+        trees, rel, frel = [], [], []
+        for coarse, fine in bodies:
+            coarse = np.ascontiguousarray(coarse, dtype=np.float64)
+            fine = np.ascontiguousarray(fine, dtype=np.float64)
+            NN = nearestMatrix(coarse, fine)
+            trees.append(OcTree(coarse, coarse, nodeCapacity=cap, finePoints=fine, nearest=1, NN=NN, ctx=self.ctx))
+            rel.append(coarse)
+            frel.append(fine)
+            self.sizes.append(len(coarse))
+        nb = len(trees)
+        th = (C.c_void_p * nb)(*[t.h for t in trees])
+        rp = (C.c_void_p * nb)(*[a.ctypes.data for a in rel])
+        fp = (C.c_void_p * nb)(*[a.ctypes.data for a in frel])
+        prec = L.PREC_MIXED if precision == "mixed" else L.PREC_FP64
+        params = L.FmmParams(float(kernelPar[0]), float(kernelPar[1]), 6, 1, prec, 3 if prec else 0, 0.0)
+        h = C.c_void_p()
+        L.check(L.lib.nnk_batch_create(self.ctx.h, nb, th, rp, fp, C.byref(params), self.nrhs, C.byref(h)),
+                self.ctx.h, "nnk_batch_create")
+        self.h = h
+        n = C.c_int64()
+        self.offsets = np.zeros(nb * self.nrhs + 1, np.int64)
+        L.check(L.lib.nnk_batch_layout(self.h, C.byref(n), L.ptr(self.offsets)))
+        self.n = n.value
+        if prec == L.PREC_MIXED and refine is not False:
+            L.check(L.lib.nnk_batch_set_refinement(self.h, 1, int(max_outer), float(inner_tol)), self.ctx.h,
+                    "nnk_batch_set_refinement")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            L.lib.nnk_batch_destroy(self.h)
+            self.h = None
+
+    @property
+    def systems(self):
+        return len(self.sizes) * self.nrhs
+
+    def system(self, body, r):
+        s = body * self.nrhs + r
+        return slice(int(self.offsets[s]), int(self.offsets[s + 1]))
+
+    def apply(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        L.check(L.lib.nnk_batch_apply(self.h, L.ptr(x), L.ptr(y), 0), self.ctx.h, "nnk_batch_apply")
+        return y
+
+    def solve(self, rhs, tol=1e-6, maxIter=200, restart=0):
+        """x, per-system (flag, relres, iters) for the batch right-hand side."""
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        x = np.empty_like(rhs)
+        info = (L.SolveInfo * self.systems)()
+        sp = L.SolveParams(float(tol), int(maxIter), int(restart))
+        rc = L.lib.nnk_batch_solve(self.h, L.ptr(rhs), L.ptr(x), C.byref(sp), C.cast(info, C.c_void_p), 0)
+        if rc not in (L.NNK_OK, L.NNK_E_NOCONV):
+            L.check(rc, self.ctx.h, "nnk_batch_solve")
+        return x, [(i.flag, i.relres, i.iters) for i in info]
+
+    def modes_rhs(self, modes=RIGID_MODES):
+        assert len(modes) == self.nrhs
+        rhs = np.zeros(self.n)
+        for b, N in enumerate(self.sizes):
+            for r, m in enumerate(modes):
+                rhs[self.system(b, r)] = mode_rhs(N, m)
+        return rhs
+
+    def solve_modes(self, tol=1e-6, maxIter=200, modes=RIGID_MODES):
+        """Per body the 6 x 6 mobility matrix (column j = [U; Omega] for mode j)."""
+        x, info = self.solve(self.modes_rhs(modes), tol=tol, maxIter=maxIter)
+        out = []
+        for b in range(len(self.sizes)):
+            M = np.zeros((6, self.nrhs))
+            for r in range(self.nrhs):
+                M[:, r] = x[self.system(b, r)][-6:]
+            out.append(M)
+        return out, [info[b * self.nrhs:(b + 1) * self.nrhs] for b in range(len(self.sizes))]
+
+    def profile(self, enable=True):
+        L.check(L.lib.nnk_batch_profile(self.h, int(bool(enable))), self.ctx.h, "nnk_batch_profile")
+
+    def profile_read(self, which=0):
+        """{phase: ms} and {phase: launches} since the last read (which = 0:
+        the batch's FMM, 1: the FP64 refinement FMM)."""
+        ms = np.zeros(len(L.PHASES))
+        ln = np.zeros(len(L.PHASES), np.int64)
+        L.check(L.lib.nnk_batch_profile_read(self.h, int(which), L.ptr(ms), L.ptr(ln)), self.ctx.h,
+                "nnk_batch_profile_read")
+        return dict(zip(L.PHASES, ms)), dict(zip(L.PHASES, ln))
+
+    def matvecs(self):
+        c = C.c_int64()
+        L.check(L.lib.nnk_batch_matvecs(self.h, C.byref(c)))
+        return c.value

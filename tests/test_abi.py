@@ -41,3 +41,14 @@ def test_fmm_without_gpu_fails_loudly():
     t = nk.OcTree(x, x, nodeCapacity=10)
     with pytest.raises(nk.NNKError, match="no CUDA device"):
         nk.KIFMM(t, [1e-3, 1.0])
+
+
+def test_batch_without_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from nnkifmm.batch import BatchMobility
+    x = np.random.default_rng(1).random((40, 3))
+    f = np.random.default_rng(2).random((120, 3))
+    with pytest.raises(nk.NNKError, match="no CUDA device"):
+        BatchMobility([(x, f)], [1e-3, 1.0], cap=10, precision="fp64", nrhs=2)

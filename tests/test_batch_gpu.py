@@ -1,0 +1,139 @@
+"""Batched mobility (nnk_batch_*): several free bodies x several right-hand
+sides solved together through one forest FMM.  Checked against the per-body
+path (nnk_mob_* on each body's own tree and FMM) and against the dense FP64
+mobility system of each body from the oracle."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import nnkifmm as nk
+from nnkifmm import batch as nb
+from nnkifmm.workloads import prolate_spheroid
+from oracle import mobility as om
+
+pytestmark = pytest.mark.gpu
+
+EPS, MU, CAP = 0.02, 1.0, 60
+
+
+def small_bodies():
+    """Three prolate spheroids of different size, aspect and orientation."""
+    rng = np.random.default_rng(7)
+    out = []
+    for a, c, h in [(0.8, 1.4, 0.16), (0.6, 2.2, 0.17), (1.0, 1.0, 0.15)]:
+        q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+        R = q * np.sign(np.diag(r))
+        if np.linalg.det(R) < 0:
+            R[:, 0] = -R[:, 0]
+        out.append((prolate_spheroid(a, c, h) @ R.T, prolate_spheroid(a, c, h / 2) @ R.T))
+    return out
+
+
+def dense_modes(coarse, fine):
+    """6 x 6 mobility matrix of one body from the dense FP64 system."""
+    NN = nk.nearestMatrix(coarse, fine)
+    cols = []
+    for kind, k in nb.RIGID_MODES:
+        F, M = np.zeros(3), np.zeros(3)
+        (F if kind == "F" else M)[k] = 1.0
+        body = om.Body(coarse, fine, sp.csr_matrix(NN), [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(coarse), F, M)
+        asm = om.assemble([body])
+        A = om.dense_mobility_matrix(asm, EPS, MU, True)
+        cols.append(np.linalg.solve(A, om.mobility_rhs(asm))[-6:])
+    return np.stack(cols, axis=1)
+
+
+@pytest.fixture(scope="module")
+def bodies():
+    return small_bodies()
+
+
+@pytest.fixture(scope="module")
+def per_body_fp64(bodies):
+    return [nb.Body(c, f, [EPS, MU], CAP, "fp64") for c, f in bodies]
+
+
+def random_batch_vector(B, rng):
+    return rng.standard_normal(B.n)
+
+
+def test_layout(bodies):
+    B = nb.BatchMobility(bodies, [EPS, MU], cap=CAP, precision="fp64", nrhs=6)
+    sizes = [len(c) for c, _ in bodies]
+    lens = np.diff(B.offsets)
+    assert B.systems == 18
+    assert list(lens) == [3 * n + 6 for n in sizes for _ in range(6)]
+    assert B.n == int(B.offsets[-1])
+
+
+@pytest.mark.parametrize("nrhs", [1, 2, 3, 4, 6, 8])
+def test_apply_matches_per_body_fp64(bodies, per_body_fp64, nrhs):
+    """FP64 batch matvec = each body's own mobility matvec, for every
+    right-hand-side count (pair kernels for 1, 2, 3, 4, 6 and a 6 + 2 split).
+    The multi-RHS kernels sum pairs in another order; the exact LU inverse of
+    the surface matrices (condition ~1e8) lifts that rounding to ~1e-9."""
+    B = nb.BatchMobility(bodies, [EPS, MU], cap=CAP, precision="fp64", nrhs=nrhs)
+    rng = np.random.default_rng(nrhs)
+    x = random_batch_vector(B, rng)
+    y = B.apply(x)
+    for b, body in enumerate(per_body_fp64):
+        for r in range(nrhs):
+            s = B.system(b, r)
+            ref = body.mob.apply(x[s])
+            err = np.linalg.norm(y[s] - ref) / np.linalg.norm(ref)
+            assert err < 1e-8, (b, r, err)
+
+
+def test_apply_mixed_close_to_fp64(bodies, per_body_fp64):
+    B = nb.BatchMobility(bodies, [EPS, MU], cap=CAP, precision="mixed", nrhs=6, refine=False)
+    rng = np.random.default_rng(11)
+    x = random_batch_vector(B, rng)
+    y = B.apply(x)
+    for b, body in enumerate(per_body_fp64):
+        for r in range(6):
+            s = B.system(b, r)
+            ref = body.mob.apply(x[s])
+            err = np.linalg.norm(y[s] - ref) / np.linalg.norm(ref)
+            assert err < 2e-4, (b, r, err)
+
+
+def test_fp64_batch_solve_matches_per_body(bodies, per_body_fp64):
+    """Per-system GMRES in the batch = one gmres call per body and mode.
+    (Below ~1e-9 the explicit residual of an FP64 FMM stops falling: its
+    rounding, lifted by the surface-matrix inverse, is that large.)"""
+    B = nb.BatchMobility(bodies, [EPS, MU], cap=CAP, precision="fp64", nrhs=6)
+    mats, infos = B.solve_modes(tol=1e-8, maxIter=300)
+    for b, body in enumerate(per_body_fp64):
+        ref, its = body.solve_modes(1e-8, 300)
+        assert all(flag == 0 for flag, _, _ in infos[b]), infos[b]
+        assert all(flag == 0 for flag, _, _ in its), its
+        err = np.linalg.norm(mats[b] - ref) / np.linalg.norm(ref)
+        assert err < 1e-5, (b, err)
+
+
+def test_mixed_refined_batch_solve_vs_dense(bodies):
+    """Mixed precision (FP32 pairs) with FP64 refinement meets 1e-4 against
+    the dense FP64 solution of every body."""
+    B = nb.BatchMobility(bodies, [EPS, MU], cap=CAP, precision="mixed", nrhs=6)
+    mats, infos = B.solve_modes(tol=1e-6, maxIter=300)
+    for b, (c, f) in enumerate(bodies):
+        assert all(flag == 0 for flag, _, _ in infos[b]), infos[b]
+        ref = dense_modes(c, f)
+        err = np.linalg.norm(mats[b] - ref) / np.linalg.norm(ref)
+        assert err < 1e-4, (b, err)
+
+
+def test_zero_rhs_systems(bodies):
+    """Systems with a zero right-hand side return x = 0 with flag 0 and no
+    iterations, while the others in the batch still converge."""
+    B = nb.BatchMobility(bodies, [EPS, MU], cap=CAP, precision="fp64", nrhs=2)
+    rhs = np.zeros(B.n)
+    rhs[B.system(1, 0)] = nb.mode_rhs(len(bodies[1][0]), ("F", 2))
+    x, info = B.solve(rhs, tol=1e-8, maxIter=300)
+    for s, (flag, relres, it) in enumerate(info):
+        assert flag == 0
+        if s != 2:
+            assert it == 0
+            sl = slice(int(B.offsets[s]), int(B.offsets[s + 1]))
+            assert not np.any(x[sl])
+    assert info[2][2] > 0

@@ -21,12 +21,12 @@ def sphere_body(F, M):
     return c, f, NN, F, M
 
 
-def run_problem(F, M, precon, precision="fp64", refine=None):
+def run_problem(F, M, precon, precision="fp64", refine=None, tol=1e-8):
     c, f, NN, F, M = sphere_body(F, M)
     sw = nk.Swimmers()
     sw.addSwimmer(c, f, NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(c), F, M)
     out, info = nk.mobilityProblem(sw, None, 0.0, np.array([0, 0, 0, 1, 0, 0, 0, 1, 0.0]), [0.01, 1.0],
-                                   {"nodeCapacity": 60, "nearest": 1}, tol=1e-8, maxIter=300,
+                                   {"nodeCapacity": 60, "nearest": 1}, tol=tol, maxIter=300,
                                    PreconSettings=[1e-6, 100] if precon else None, precision=precision,
                                    return_info=True, refine=refine)
     body = om.Body(c, f, NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(c), F, M)
@@ -51,8 +51,10 @@ def test_translation_and_rotation(precon):
 
 
 def test_precon_reduces_iterations():
-    _, a, _ = run_problem([1, 0, 0], [0, 0, 1], False)
-    _, b, _ = run_problem([1, 0, 0], [0, 0, 1], True)
+    # at tol 1e-6, well above the ~1e-9 rounding floor of the FP64 FMM, where
+    # iteration counts near tol 1e-8 vary from run to run
+    _, a, _ = run_problem([1, 0, 0], [0, 0, 1], False, tol=1e-6)
+    _, b, _ = run_problem([1, 0, 0], [0, 0, 1], True, tol=1e-6)
     assert b["iters"] <= a["iters"]
 
 
