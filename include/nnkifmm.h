@@ -91,7 +91,9 @@ typedef struct nnk_fmm_params {
   int32_t m2l_mode;      /* mixed mode M2L: 0 auto (tensor cores, images when
                             they fit 8 GiB), 1 tensor cores + streamed images,
                             2 tensor cores + in-kernel operators, 3 FP32 pair
-                            kernel (no tensor cores; FP32-rounding accuracy)  */
+                            kernel (no tensor cores; FP32-rounding accuracy),
+                            4 FP32 Fourier-space product (FFT of the surface
+                            lattice; FP32-rounding accuracy)                  */
   double reg;            /* relative Tikhonov weight of the check-to-equivalent
                             pseudo-inverse: NNK_PREC_MIXED 0 = default 1e-5;
                             NNK_PREC_FP64 0 = exact LU inverse (reference)   */

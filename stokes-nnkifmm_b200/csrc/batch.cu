@@ -437,7 +437,8 @@ BatchMobility::BatchMobility(nnk_ctx* ctx, const std::vector<BatchBody>& bodies,
   body_row0_.upload(body_row0, st);
   FmmParams q = fp;
   q.max_rhs = std::min(R_, 6);
-  if (q.precision == NNK_PREC_MIXED && q.m2l_mode != 3) q.m2l_mode = 3;  // several right-hand sides per pass
+  // several right-hand sides per pass: the FP32 pair or Fourier-space M2L
+  if (q.precision == NNK_PREC_MIXED && q.m2l_mode != 3) q.m2l_mode = 4;
   fp_ = q;
   fmm_.reset(new Fmm(ctx_, &forest_, q));
   NNK_CUDA(cudaStreamSynchronize(st));

@@ -530,7 +530,14 @@ __global__ void add_diag_kernel(double* G, int n, double v) {
 
 void Fmm::build_operators() {
   const HostTree& t = *t_;
-  if (p_.precision == NNK_PREC_MIXED && p_.m2l_mode != 3) {
+  if (p_.m2l_mode < 0 || p_.m2l_mode > 4) throw Error(NNK_E_ARG, "m2l_mode must be 0..4");
+  if (p_.precision == NNK_PREC_MIXED && p_.m2l_mode == 4) {
+    std::vector<int> node_op(N_);
+    for (int32_t v = 0; v < N_; ++v) node_op[v] = op_of_[(size_t)t.group_of(v) * (maxl_ + 1) + t.level[v]];
+    build_fft_m2l(t, p_.res, p_.shells, p_.eps, p_.mu, op_w_, node_op, R_, fft_, ctx_->stream);
+    fft_m2l_ = true;
+  }
+  if (p_.precision == NNK_PREC_MIXED && p_.m2l_mode != 3 && p_.m2l_mode != 4) {
     if (p_.m2l_mode == 1) m2l_.image_budget = ~(size_t)0;
     if (p_.m2l_mode == 2) m2l_.image_budget = 0;
     build_m2l_plan(t, p_.res, p_.shells, p_.eps, p_.mu, m2l_, ctx_->stream);
@@ -690,10 +697,16 @@ void Fmm::apply_impl(const double* d_in, const IoMap& in, double* d_out, const I
     NNK_CUDA(cudaMemsetAsync(check, 0, sizeof(Real) * (size_t)N_ * n, st));
     phase(NNK_PHASE_M2L, [&] { launch_m2l(m2l_, (float*)check, n, st); });
   }
-  const std::vector<TaskGroup>& dgroups = tm ? down_nov_ : down_;
+  const bool fm = fft_m2l_ && std::is_same<Real, float>::value;
+  if (fm) {
+    // M2L of every level at once in Fourier space
+    NNK_CUDA(cudaMemsetAsync(check, 0, sizeof(Real) * (size_t)N_ * n * R, st));
+    phase(NNK_PHASE_M2L, [&] { launch_fft_m2l(fft_, (const float*)str, E_, R, (float*)check, st); });
+  }
+  const std::vector<TaskGroup>& dgroups = (tm || fm) ? down_nov_ : down_;
   for (int L = 1; L <= maxl_; ++L) {
     if (dgroups[L].count == 0) continue;
-    run_group<Real>(dgroups[L], pos, str, pos, check, e2, scale, tm ? 1 : 0, NNK_PHASE_DOWN_PAIRS, R);
+    run_group<Real>(dgroups[L], pos, str, pos, check, e2, scale, (tm || fm) ? 1 : 0, NNK_PHASE_DOWN_PAIRS, R);
     const int64_t nt = dn_toff_[L + 1] - dn_toff_[L];
     phase(NNK_PHASE_DOWN_C2E, [&] {
       launch_c2e<Real>(ops_.p, n, 1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str,

@@ -15,6 +15,7 @@
 
 #include "common.h"
 #include "m2l.h"
+#include "m2l_fft.h"
 #include "tree.h"
 
 namespace nnk {
@@ -147,6 +148,8 @@ class Fmm {
   std::vector<TaskGroup> down_nov_;   // per level, without the V-list (M2L on the tensor cores)
   M2LPlan m2l_;
   bool tensor_m2l_ = false;
+  FftM2L fft_;
+  bool fft_m2l_ = false;
   TaskGroup leaf_;
   DBuf<int32_t> lvl_nodes_;
   DBuf<int32_t> roots_;

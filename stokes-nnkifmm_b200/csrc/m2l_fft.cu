@@ -1,0 +1,423 @@
+// Fourier-space M2L (see m2l_fft.h).
+//
+// Transforms are separable DFTs of length G over the zero-padded lattice,
+// written out as small sums in shared memory (G = 12 for res = 6): each pass
+// maps one axis, and only the res non-zero inputs (forward) or res needed
+// outputs (inverse) of that axis are touched.  Frequency index
+// k = (kx * G + ky) * H + kz, H = G / 2 + 1 (half spectrum along z).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+
+#include "m2l_fft.h"
+
+namespace nnk {
+
+namespace {
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ void cmac(float2& acc, float2 a, float2 b) {
+  acc.x = fmaf(a.x, b.x, fmaf(-a.y, b.y, acc.x));
+  acc.y = fmaf(a.x, b.y, fmaf(a.y, b.x, acc.y));
+}
+
+// e^{sign * 2 pi i m / G}, m in [0, G)
+__device__ __forceinline__ void twiddles(float2* tw, int G, double sign) {
+  for (int m = threadIdx.x; m < G; m += blockDim.x) {
+    double s, c;
+    sincospi(2.0 * m / G, &s, &c);
+    tw[m] = make_float2((float)c, (float)(sign * s));
+  }
+}
+
+// ------------------------------------------------------------------ setup
+// Spectrum of the kernel on the difference grid for one (box width, offset),
+// FP64, one component at a time:
+//   Kgrid[d] = K((d - (res - 1) o) h) / (8 pi mu G^3) for |d|_inf <= res - 1
+// (d the signed index of the grid point, 0 elsewhere), then three DFT passes.
+__global__ void fft_spectra_kernel(int G, int res, const double* __restrict__ slot_w,
+                                   const int* __restrict__ slot_code, double e2, double scale,
+                                   float2* __restrict__ spec, int NK) {
+  extern __shared__ double sm[];
+  const int H = G / 2 + 1;
+  double* K = sm;                         // [x][y][z]
+  double2* A = (double2*)(K + G * G * G);  // [x][y][kz]
+  double2* B = A + G * G * H;              // [x][ky][kz]
+  const int s = blockIdx.x;
+  const double h = slot_w[s] / (res - 1);
+  const int code = slot_code[s];
+  const int o[3] = {code / 49 - 3, (code / 7) % 7 - 3, code % 7 - 3};
+  const int tid = threadIdx.x, nt = blockDim.x;
+  auto sd = [&](int a) { return a < G / 2 ? a : a - G; };
+  auto tw = [&](int m, double& c, double& sn) {  // e^{-2 pi i m / G}
+    double si;
+    sincospi(2.0 * (m % G) / G, &si, &c);
+    sn = -si;
+  };
+  for (int comp = 0; comp < 6; ++comp) {
+    // xx xy xz yy yz zz
+    const int ci = comp < 3 ? 0 : (comp < 5 ? 1 : 2);
+    const int cj = comp < 3 ? comp : (comp < 5 ? comp - 2 : 2);
+    for (int e = tid; e < G * G * G; e += nt) {
+      const int d[3] = {sd(e / (G * G)), sd((e / G) % G), sd(e % G)};
+      double v = 0;
+      if (abs(d[0]) <= res - 1 && abs(d[1]) <= res - 1 && abs(d[2]) <= res - 1) {
+        double r[3];
+        for (int a = 0; a < 3; ++a) r[a] = (double)(d[a] - (res - 1) * o[a]) * h;
+        const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        const double dd = r2 + e2;
+        v = ((ci == cj ? r2 + 2.0 * e2 : 0.0) + r[ci] * r[cj]) * scale / (dd * sqrt(dd));
+      }
+      K[e] = v;
+    }
+    __syncthreads();
+    for (int e = tid; e < G * G * H; e += nt) {  // z
+      const int xy = e / H, kz = e % H;
+      double re = 0, im = 0;
+      for (int z = 0; z < G; ++z) {
+        double c, sn;
+        tw(kz * z, c, sn);
+        re += K[xy * G + z] * c;
+        im += K[xy * G + z] * sn;
+      }
+      A[e] = make_double2(re, im);
+    }
+    __syncthreads();
+    for (int e = tid; e < G * G * H; e += nt) {  // y
+      const int x = e / (G * H), ky = (e / H) % G, kz = e % H;
+      double re = 0, im = 0;
+      for (int y = 0; y < G; ++y) {
+        double c, sn;
+        tw(ky * y, c, sn);
+        const double2 a = A[(x * G + y) * H + kz];
+        re += a.x * c - a.y * sn;
+        im += a.x * sn + a.y * c;
+      }
+      B[e] = make_double2(re, im);
+    }
+    __syncthreads();
+    for (int e = tid; e < G * G * H; e += nt) {  // x
+      const int kx = e / (G * H), kyz = e % (G * H);
+      double re = 0, im = 0;
+      for (int x = 0; x < G; ++x) {
+        double c, sn;
+        tw(kx * x, c, sn);
+        const double2 b = B[x * G * H + kyz];
+        re += b.x * c - b.y * sn;
+        im += b.x * sn + b.y * c;
+      }
+      spec[((size_t)s * 6 + comp) * NK + e] = make_float2((float)re, (float)im);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- forward
+// Q_v[cr][k] for one source node: its shell densities on the res^3 lattice
+// (interior zero), transformed along z (res -> H), y (res -> G), x (res -> G).
+__global__ void fft_forward_kernel(int G, int res, int P, const int* __restrict__ lat,
+                                   const int* __restrict__ src_node, const float* __restrict__ str, long long upbase,
+                                   int R, float2* __restrict__ qhat, int NK) {
+  extern __shared__ float2 smq[];
+  const int H = G / 2 + 1, C = 3 * R, r3 = res * res * res;
+  float2* tw = smq;                          // G
+  float2* Z = tw + G;                        // [cr][x][y][kz]   C res res H
+  float2* Y = Z + C * res * res * H;         // [cr][x][ky][kz]  C res G H
+  float* g = reinterpret_cast<float*>(Y + C * res * G * H);  // [cr][x][y][z] C res^3
+  const int node = src_node[blockIdx.x];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  twiddles(tw, G, -1.0);
+  for (int e = tid; e < C * r3; e += nt) g[e] = 0.f;
+  __syncthreads();
+  const float* src = str + (upbase + (long long)P * node) * C;
+  for (int e = tid; e < P * C; e += nt) {
+    const int p = e / C, cr = e - p * C;
+    const int l = lat[p];
+    g[cr * r3 + ((l & 255) * res + ((l >> 8) & 255)) * res + (l >> 16)] = src[e];
+  }
+  __syncthreads();
+  for (int e = tid; e < C * res * res; e += nt) {  // z: one (cr, x, y) per thread
+    const float* gz = g + e * res;
+    for (int kz = 0; kz < H; ++kz) {
+      float2 a = make_float2(0.f, 0.f);
+      for (int z = 0; z < res; ++z) {
+        const float2 w = tw[(kz * z) % G];
+        a.x = fmaf(gz[z], w.x, a.x);
+        a.y = fmaf(gz[z], w.y, a.y);
+      }
+      Z[e * H + kz] = a;
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < C * res * H; e += nt) {  // y: one (cr, x, kz) per thread
+    const int crx = e / H, kz = e % H;
+    float2 in[8];
+    for (int y = 0; y < res; ++y) in[y] = Z[(crx * res + y) * H + kz];
+    for (int ky = 0; ky < G; ++ky) {
+      float2 a = make_float2(0.f, 0.f);
+      for (int y = 0; y < res; ++y) cmac(a, in[y], tw[(ky * y) % G]);
+      Y[(crx * G + ky) * H + kz] = a;
+    }
+  }
+  __syncthreads();
+  float2* out = qhat + (size_t)blockIdx.x * C * NK;
+  for (int e = tid; e < C * G * H; e += nt) {  // x: one (cr, ky, kz) per thread
+    const int cr = e / (G * H), kyz = e % (G * H);
+    float2 in[8];
+    for (int x = 0; x < res; ++x) in[x] = Y[(cr * res + x) * G * H + kyz];
+    for (int kx = 0; kx < G; ++kx) {
+      float2 a = make_float2(0.f, 0.f);
+      for (int x = 0; x < res; ++x) cmac(a, in[x], tw[(kx * x) % G]);
+      out[(size_t)cr * NK + kx * G * H + kyz] = a;
+    }
+  }
+}
+
+// ------------------------------------------------------------- accumulate
+// C_i(k) = sum_{v in V(i)} Khat_{w,o}(k) Q_v(k): one target and frequency per
+// thread; blocks run frequency-block-major so that the spectra in use at a
+// time are a slice that stays in L2.
+template <int R>
+__global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* __restrict__ voff,
+                                                             const int* __restrict__ vsrc,
+                                                             const int* __restrict__ vspec,
+                                                             const float2* __restrict__ spec,
+                                                             const float2* __restrict__ qhat,
+                                                             float2* __restrict__ chat) {
+  constexpr int C = 3 * R;
+  const int t = blockIdx.x;
+  const int k = blockIdx.y * blockDim.x + threadIdx.x;
+  if (k >= NK) return;
+  float2 acc[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) acc[c] = make_float2(0.f, 0.f);
+  const int e1 = voff[t + 1];
+  for (int e = voff[t]; e < e1; ++e) {
+    const float2* Kp = spec + (size_t)vspec[e] * 6 * NK + k;
+    const float2 kxx = Kp[0], kxy = Kp[NK], kxz = Kp[2 * NK], kyy = Kp[3 * NK], kyz = Kp[4 * NK],
+                 kzz = Kp[5 * NK];
+    const float2* Q = qhat + (size_t)vsrc[e] * C * NK + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float2 qx = Q[(3 * r) * NK], qy = Q[(3 * r + 1) * NK], qz = Q[(3 * r + 2) * NK];
+      cmac(acc[3 * r], kxx, qx);
+      cmac(acc[3 * r], kxy, qy);
+      cmac(acc[3 * r], kxz, qz);
+      cmac(acc[3 * r + 1], kxy, qx);
+      cmac(acc[3 * r + 1], kyy, qy);
+      cmac(acc[3 * r + 1], kyz, qz);
+      cmac(acc[3 * r + 2], kxz, qx);
+      cmac(acc[3 * r + 2], kyz, qy);
+      cmac(acc[3 * r + 2], kzz, qz);
+    }
+  }
+  float2* out = chat + (size_t)t * C * NK + k;
+#pragma unroll
+  for (int c = 0; c < C; ++c) out[(size_t)c * NK] = acc[c];
+}
+
+// ---------------------------------------------------------------- inverse
+// check of one target node at its shell lattice points from C_i: inverse
+// passes along x (G -> res), y (G -> res) and z (half spectrum -> res, real).
+__global__ void fft_inverse_kernel(int G, int res, int P, const int* __restrict__ lat,
+                                   const int* __restrict__ tgt_node, const float2* __restrict__ chat, int R,
+                                   float* __restrict__ check, int NK) {
+  extern __shared__ float2 smc[];
+  const int H = G / 2 + 1, C = 3 * R, r3 = res * res * res;
+  float2* tw = smc;                   // G
+  float2* X = tw + G;                 // [cr][x][ky][kz]  C res G H
+  float2* Yv = X + C * res * G * H;   // [cr][x][y][kz]   C res res H
+  float* out = reinterpret_cast<float*>(X);  // [cr][x][y][z] (X is dead by then)
+  const int node = tgt_node[blockIdx.x];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  twiddles(tw, G, 1.0);
+  __syncthreads();
+  const float2* ci = chat + (size_t)blockIdx.x * C * NK;
+  for (int e = tid; e < C * G * H; e += nt) {  // x: one (cr, ky, kz) per thread
+    const int cr = e / (G * H), kyz = e % (G * H);
+    float2 a[8];
+    for (int x = 0; x < res; ++x) a[x] = make_float2(0.f, 0.f);
+    for (int kx = 0; kx < G; ++kx) {
+      const float2 v = ci[(size_t)cr * NK + kx * G * H + kyz];
+      for (int x = 0; x < res; ++x) cmac(a[x], v, tw[(kx * x) % G]);
+    }
+    for (int x = 0; x < res; ++x) X[(cr * res + x) * G * H + kyz] = a[x];
+  }
+  __syncthreads();
+  for (int e = tid; e < C * res * H; e += nt) {  // y: one (cr, x, kz) per thread
+    const int crx = e / H, kz = e % H;
+    float2 a[8];
+    for (int y = 0; y < res; ++y) a[y] = make_float2(0.f, 0.f);
+    for (int ky = 0; ky < G; ++ky) {
+      const float2 v = X[(crx * G + ky) * H + kz];
+      for (int y = 0; y < res; ++y) cmac(a[y], v, tw[(ky * y) % G]);
+    }
+    for (int y = 0; y < res; ++y) Yv[(crx * res + y) * H + kz] = a[y];
+  }
+  __syncthreads();
+  for (int e = tid; e < C * res * res; e += nt) {  // z: one (cr, x, y) per thread, real output
+    const float2* yz = Yv + e * H;
+    for (int z = 0; z < res; ++z) {
+      float v = 0.f;
+      for (int kz = 0; kz < H; ++kz) {
+        const float w = (kz == 0 || 2 * kz == G) ? 1.f : 2.f;
+        const float2 t = tw[(kz * z) % G];
+        v = fmaf(w, yz[kz].x * t.x - yz[kz].y * t.y, v);
+      }
+      out[e * res + z] = v;
+    }
+  }
+  __syncthreads();
+  float* dst = check + (long long)P * node * C;
+  for (int e = tid; e < P * C; e += nt) {
+    const int p = e / C, cr = e - p * C;
+    const int l = lat[p];
+    dst[e] = out[cr * r3 + ((l & 255) * res + ((l >> 8) & 255)) * res + (l >> 16)];
+  }
+}
+
+size_t forward_smem(int G, int res, int R) {
+  const int H = G / 2 + 1, C = 3 * R;
+  return sizeof(float2) * (G + (size_t)C * res * res * H + (size_t)C * res * G * H) +
+         sizeof(float) * (size_t)C * res * res * res;
+}
+size_t inverse_smem(int G, int res, int R) {
+  const int H = G / 2 + 1, C = 3 * R;
+  return sizeof(float2) * (G + (size_t)C * res * G * H + (size_t)C * res * res * H);
+}
+
+}  // namespace
+
+void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu, const std::vector<double>& op_w,
+                   const std::vector<int>& node_op, int Rmax, FftM2L& f, cudaStream_t st) {
+  if (res > 8) throw Error(NNK_E_ARG, "Fourier M2L supports coronaRes up to 8");
+  f.res = res;
+  f.G = 2 * res;
+  const int G = f.G, H = G / 2 + 1;
+  f.NK = G * G * H;
+  f.Rcap = Rmax;
+  // shell lattice in the order of the surface points (genupsurf.m:24-33)
+  std::vector<int> lat;
+  auto inner = [&](int a) { return a >= shells && a <= res - 1 - shells; };
+  for (int k = 0; k < res; ++k)
+    for (int i = 0; i < res; ++i)
+      for (int j = 0; j < res; ++j)
+        if (!(inner(j) && inner(i) && inner(k))) lat.push_back(i | (j << 8) | (k << 16));
+  f.P = (int)lat.size();
+  std::vector<int> tgt, voff{0}, vsrc, vspec, src;
+  std::vector<double> slot_w;
+  std::vector<int> slot_code;
+  std::map<int32_t, int> src_slot;
+  std::map<int64_t, int> spec_slot;
+  for (int32_t i = 0; i < t.nodes; ++i) {
+    if (t.V.off[i + 1] == t.V.off[i]) continue;
+    tgt.push_back(i);
+    for (int64_t k = t.V.off[i]; k < t.V.off[i + 1]; ++k) {
+      const int32_t v = t.V.idx[k];
+      const int ox = t.ix[v] - t.ix[i], oy = t.iy[v] - t.iy[i], oz = t.iz[v] - t.iz[i];
+      if (std::abs(ox) > 3 || std::abs(oy) > 3 || std::abs(oz) > 3)
+        throw Error(NNK_E_STATE, "V-list offset outside [-3,3]^3");
+      const int code = (ox + 3) * 49 + (oy + 3) * 7 + (oz + 3);
+      const int op = node_op[i];
+      auto sit = src_slot.find(v);
+      if (sit == src_slot.end()) {
+        sit = src_slot.emplace(v, (int)src.size()).first;
+        src.push_back(v);
+      }
+      const int64_t key = (int64_t)op * 343 + code;
+      auto kit = spec_slot.find(key);
+      if (kit == spec_slot.end()) {
+        kit = spec_slot.emplace(key, (int)slot_w.size()).first;
+        slot_w.push_back(op_w[op]);
+        slot_code.push_back(code);
+      }
+      vsrc.push_back(sit->second);
+      vspec.push_back(kit->second);
+    }
+    voff.push_back((int)vsrc.size());
+  }
+  // sources in node order keep siblings' spectra adjacent
+  {
+    std::vector<int> order(src.size());
+    for (size_t a = 0; a < order.size(); ++a) order[a] = (int)a;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return src[a] < src[b]; });
+    std::vector<int> remap(src.size()), s2(src.size());
+    for (size_t a = 0; a < order.size(); ++a) {
+      remap[order[a]] = (int)a;
+      s2[a] = src[order[a]];
+    }
+    src.swap(s2);
+    for (int& s : vsrc) s = remap[s];
+  }
+  f.ntgt = (int)tgt.size();
+  f.nsrc = (int)src.size();
+  f.nspec = (int)slot_w.size();
+  f.pairs = (int64_t)vsrc.size();
+  f.lat.upload(lat, st);
+  f.tgt_node.upload(tgt, st);
+  f.src_node.upload(src, st);
+  f.voff.upload(voff, st);
+  f.vsrc.upload(vsrc, st);
+  f.vspec.upload(vspec, st);
+  f.spec.alloc(std::max<size_t>(1, (size_t)f.nspec * 6 * f.NK));
+  f.qhat.alloc(std::max<size_t>(1, (size_t)f.nsrc * 3 * Rmax * f.NK));
+  f.chat.alloc(std::max<size_t>(1, (size_t)f.ntgt * 3 * Rmax * f.NK));
+  if (f.nspec) {
+    DBuf<double> dw;
+    DBuf<int> dc;
+    dw.upload(slot_w, st);
+    dc.upload(slot_code, st);
+    const size_t sm = sizeof(double) * (size_t)G * G * G + 2 * sizeof(double2) * (size_t)G * G * H;
+    NNK_CUDA(cudaFuncSetAttribute(fft_spectra_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    fft_spectra_kernel<<<f.nspec, 256, sm, st>>>(G, res, dw.p, dc.p, eps * eps,
+                                                  1.0 / (8.0 * M_PI * mu * (double)G * G * G), f.spec.p, f.NK);
+    NNK_CHECK_LAUNCH();
+    NNK_CUDA(cudaStreamSynchronize(st));
+  }
+  f.fwd_smem = forward_smem(G, res, Rmax);
+  f.inv_smem = inverse_smem(G, res, Rmax);
+  if (f.fwd_smem > 227 * 1024 || f.inv_smem > 227 * 1024)
+    throw Error(NNK_E_ARG, "Fourier M2L: too many right-hand sides per pass for shared memory");
+  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.fwd_smem));
+  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.inv_smem));
+  NNK_CUDA(cudaStreamSynchronize(st));
+}
+
+void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float* check, cudaStream_t st) {
+  if (f.ntgt == 0) return;
+  if (R > f.Rcap) throw Error(NNK_E_STATE, "Fourier M2L sized for fewer right-hand sides");
+  const int G = f.G, res = f.res;
+  fft_forward_kernel<<<f.nsrc, 256, forward_smem(G, res, R), st>>>(G, res, f.P, f.lat.p, f.src_node.p, str, upbase,
+                                                                    R, f.qhat.p, f.NK);
+  NNK_CHECK_LAUNCH();
+  dim3 grid(f.ntgt, (f.NK + 127) / 128);
+  switch (R) {
+    case 1:
+      fft_accumulate_kernel<1><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p);
+      break;
+    case 2:
+      fft_accumulate_kernel<2><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p);
+      break;
+    case 3:
+      fft_accumulate_kernel<3><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p);
+      break;
+    case 4:
+      fft_accumulate_kernel<4><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p);
+      break;
+    case 6:
+      fft_accumulate_kernel<6><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p);
+      break;
+    default:
+      throw Error(NNK_E_ARG, "Fourier M2L supports 1, 2, 3, 4 or 6 right-hand sides per pass");
+  }
+  NNK_CHECK_LAUNCH();
+  fft_inverse_kernel<<<f.ntgt, 256, inverse_smem(G, res, R), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, f.chat.p, R,
+                                                                    check, f.NK);
+  NNK_CHECK_LAUNCH();
+}
+
+}  // namespace nnk

@@ -1,0 +1,52 @@
+// M2L (V-list, DownNonleaf.m:34-38 / downwardPass.m:59-74) in Fourier space.
+//
+// The up-equivalent surface of a node is the outer shell of a res^3 lattice
+// of spacing h = w / (res - 1) on its box.  For a target node i and a source
+// v in V(i) at offset o = (v - i) in box widths, the reference adds
+//   check_i(a) += sum_b K((a - b - (res - 1) o) h) q_v(b)
+// over lattice points a, b (the kernel matrix of upsurf(v) -> upsurf(i)).
+// This is a discrete convolution, so with the densities zero-padded to a
+// G^3 grid (G = 2 res >= 2 res - 1, no wrap-around) it becomes a pointwise
+// product of spectra:
+//   C_i(k) = sum_{v in V(i)} Khat_{w,o}(k) Q_v(k),
+// Khat the 3 x 3 (symmetric) spectrum of the kernel sampled on the difference
+// grid, Q_v the spectrum of v's densities.  Per V pair this costs
+// 9 complex multiply-adds per frequency and right-hand side on
+// G^2 (G/2 + 1) frequencies (real-to-complex), against (3P)^2 for the dense
+// matrix.  Spectra are FP32; the kernel spectra are computed in FP64 once per
+// (box width, offset) with 1/(8 pi mu) and the 1/G^3 of the inverse
+// transform folded in.
+#pragma once
+#include <vector>
+
+#include "common.h"
+#include "tree.h"
+
+namespace nnk {
+
+struct FftM2L {
+  int res = 0, G = 0, NK = 0, P = 0;
+  int nsrc = 0, ntgt = 0, nspec = 0, Rcap = 1;
+  int64_t pairs = 0;
+  DBuf<int> lat;        // per surface point: x | y << 8 | z << 16 lattice indices
+  DBuf<float2> spec;    // nspec x 6 x NK (xx, xy, xz, yy, yz, zz)
+  DBuf<int> src_node;   // per source slot: node
+  DBuf<int> tgt_node;   // per target slot: node
+  DBuf<int> voff;       // per target slot: first pair (ntgt + 1)
+  DBuf<int> vsrc;       // per pair: source slot
+  DBuf<int> vspec;      // per pair: kernel spectrum
+  DBuf<float2> qhat;    // nsrc x 3R x NK
+  DBuf<float2> chat;    // ntgt x 3R x NK
+  size_t fwd_smem = 0, inv_smem = 0;
+};
+
+// node_op[n]: check-to-equivalent operator index of node n's (tree, level);
+// op_w[op]: its box width.  Rmax: right-hand sides per pass.
+void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu, const std::vector<double>& op_w,
+                   const std::vector<int>& node_op, int Rmax, FftM2L& f, cudaStream_t st);
+// check[((P * node + p) * R + r) * 3 + c] = M2L result for every node with a
+// V-list (other entries untouched); str holds the up-equivalent densities of
+// node n at str[((upbase + P * n + p) * R + r) * 3 + c].
+void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float* check, cudaStream_t st);
+
+}  // namespace nnk

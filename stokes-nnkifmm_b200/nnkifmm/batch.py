@@ -75,11 +75,12 @@ class BatchMobility:
 
     bodies: list of (force points N_b x 3, fine points Q_b x 3), each a free
     body at rest orientation (rel points = the points themselves).
-    precision 'mixed' uses FP32 pair kernels (M2L included) with FP64
-    iterative refinement unless refine=False."""
+    precision 'mixed' uses FP32 pair kernels and an FP32 M2L (m2l='fft':
+    Fourier-space product, 'pairs': pair kernel) with FP64 iterative
+    refinement unless refine=False."""
 
     def __init__(self, bodies, kernelPar, cap=200, precision="mixed", nrhs=6, refine=None, device=0, ctx=None,
-                 max_outer=12, inner_tol=1e-3):
+                 max_outer=12, inner_tol=1e-3, m2l="fft"):
         self.ctx = ctx if ctx is not None else L.Context(device)
         self.nrhs = int(nrhs)
         self.sizes = []
@@ -97,7 +98,8 @@ class BatchMobility:
         rp = (C.c_void_p * nb)(*[a.ctypes.data for a in rel])
         fp = (C.c_void_p * nb)(*[a.ctypes.data for a in frel])
         prec = L.PREC_MIXED if precision == "mixed" else L.PREC_FP64
-        params = L.FmmParams(float(kernelPar[0]), float(kernelPar[1]), 6, 1, prec, 3 if prec else 0, 0.0)
+        mode = {"fft": 4, "pairs": 3}[m2l] if prec == L.PREC_MIXED else 0
+        params = L.FmmParams(float(kernelPar[0]), float(kernelPar[1]), 6, 1, prec, mode, 0.0)
         h = C.c_void_p()
         L.check(L.lib.nnk_batch_create(self.ctx.h, nb, th, rp, fp, C.byref(params), self.nrhs, C.byref(h)),
                 self.ctx.h, "nnk_batch_create")

@@ -25,7 +25,7 @@ class KIFMM:
                               coronaRes=coronaRes, coronaShells=coronaShells, format=format,
                               kernelPar=(eps, mu), precision=precision)
         prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
-        mode = {"auto": 0, "images": 1, "generate": 2, "pairs": 3}[m2l]
+        mode = {"auto": 0, "images": 1, "generate": 2, "pairs": 3, "fft": 4}[m2l]
         p = L.FmmParams(eps, mu, int(coronaRes), int(coronaShells), prec, mode, float(reg))
         h = C.c_void_p()
         L.check(L.lib.nnk_fmm_create(self.ctx.h, tree.h, C.byref(p), C.byref(h)), self.ctx.h, "KIFMM")

@@ -97,6 +97,19 @@ def test_apply_mixed_close_to_fp64(bodies, per_body_fp64):
             assert err < 2e-4, (b, r, err)
 
 
+@pytest.mark.parametrize("nrhs", [2, 6])
+def test_fourier_m2l_batch_matches_pair_m2l(bodies, nrhs):
+    """Several right-hand sides per pass through the Fourier-space M2L give
+    the FP32 pair-kernel M2L result."""
+    a = nb.BatchMobility(bodies, [EPS, MU], cap=CAP, precision="mixed", nrhs=nrhs, refine=False, m2l="pairs")
+    b = nb.BatchMobility(bodies, [EPS, MU], cap=CAP, precision="mixed", nrhs=nrhs, refine=False, m2l="fft")
+    x = random_batch_vector(a, np.random.default_rng(5))
+    ya, yb = a.apply(x), b.apply(x)
+    for s in range(a.systems):
+        sl = slice(int(a.offsets[s]), int(a.offsets[s + 1]))
+        assert np.linalg.norm(yb[sl] - ya[sl]) <= 1e-5 * np.linalg.norm(ya[sl]), s
+
+
 def test_fp64_batch_solve_matches_per_body(bodies, per_body_fp64):
     """Per-system GMRES in the batch = one gmres call per body and mode.
     (Below ~1e-9 the explicit residual of an FP64 FMM stops falling: its

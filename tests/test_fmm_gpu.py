@@ -98,6 +98,18 @@ def test_generated_m2l_operators_match_streamed(name):
     assert rel(b, a) <= 1e-5
 
 
+@pytest.mark.parametrize("name", sorted(FP64_TOL))
+def test_fourier_m2l_matches_pair_m2l(name):
+    """The Fourier-space M2L (FP32 spectra) gives the FP32 pair-kernel M2L
+    result."""
+    g = load(name)
+    t = tree_of(g)
+    kp = [float(g["eps"]), float(g["mu"])]
+    a = nk.KIFMM(t, kp, precision="mixed", m2l="pairs").computeVel(g["F"])
+    b = nk.KIFMM(t, kp, precision="mixed", m2l="fft").computeVel(g["F"])
+    assert rel(b, a) <= 1e-5
+
+
 def test_sparse_matches_oracle():
     g = load("sphere10_40")
     fmm = nk.KIFMM(tree_of(g), [float(g["eps"]), float(g["mu"])])
