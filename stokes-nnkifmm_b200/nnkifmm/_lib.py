@@ -150,6 +150,8 @@ def check(rc, ctx=None, what=""):
 class Context:
     """One CUDA device and stream (nnk_ctx)."""
 
+    _destroy = lib.nnk_ctx_destroy  # held by the class: module globals may be gone at exit
+
     def __init__(self, device=0):
         h = _vp()
         check(lib.nnk_ctx_create(device, C.byref(h)))
@@ -164,7 +166,7 @@ class Context:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib.nnk_ctx_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
 

@@ -112,9 +112,11 @@ class BatchMobility:
             L.check(L.lib.nnk_batch_set_refinement(self.h, 1, int(max_outer), float(inner_tol)), self.ctx.h,
                     "nnk_batch_set_refinement")
 
+    _destroy = L.lib.nnk_batch_destroy  # held by the class: module globals may be gone at exit
+
     def __del__(self):
         if getattr(self, "h", None):
-            L.lib.nnk_batch_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     @property

@@ -31,9 +31,11 @@ class KIFMM:
         L.check(L.lib.nnk_fmm_create(self.ctx.h, tree.h, C.byref(p), C.byref(h)), self.ctx.h, "KIFMM")
         self.h = h
 
+    _destroy = L.lib.nnk_fmm_destroy  # held by the class: module globals may be gone at exit
+
     def __del__(self):
         if getattr(self, "h", None):
-            L.lib.nnk_fmm_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     # KIFMM.m:83-103: GMRES=1 -> vector; format 1 interleaved, 2 blocked

@@ -191,9 +191,11 @@ class Mobility:
         L.check(L.lib.nnk_mob_set_refinement(self.h, fmm64.h if fmm64 is not None else None, int(max_outer),
                                              float(inner_tol)), self.ctx.h, "refinement")
 
+    _destroy = L.lib.nnk_mob_destroy  # held by the class: module globals may be gone at exit
+
     def __del__(self):
         if getattr(self, "h", None):
-            L.lib.nnk_mob_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     def _vec(self, x):

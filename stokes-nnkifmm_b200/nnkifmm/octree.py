@@ -57,9 +57,11 @@ class OcTree:
         self.finePoints = fine if nearest else None
         self._cache = {}
 
+    _destroy = L.lib.nnk_tree_destroy  # held by the class: module globals may be gone at exit
+
     def __del__(self):
         if getattr(self, "h", None):
-            L.lib.nnk_tree_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     # ---- exported arrays (lazy)
