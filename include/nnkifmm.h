@@ -206,6 +206,24 @@ int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats);
 #define NNK_PHASE_SCATTER 6
 #define NNK_PHASE_M2L 7
 #define NNK_NUM_PHASES 8
+/* ------------------------------------------------------------- adjoint -- */
+/* No counterpart in the reference (gradients are new here).  The exact
+ * transpose of nnk_fmm_apply: in (targets, n_tgt x 3 per right-hand side),
+ * out (potentials, n_pot x 3); <y, apply(x)> = <apply_adjoint(y), x>.  The
+ * same passes run on the same tree with the point sets' roles exchanged and
+ * the interaction lists inverted. */
+int nnk_fmm_apply_adjoint(nnk_fmm* fmm, const double* in, double* out, int32_t layout,
+                          int32_t nrhs, int32_t on_device);
+/* Number of source origins: fine points (NEAREST) or potential rows. */
+int nnk_fmm_source_count(const nnk_fmm* fmm, int64_t* count);
+/* Gradient of <weights, apply(forces)> with respect to the positions, with
+ * the kernel's derivative (Tools/kernel.m:23-47 differentiated):
+ * grad_targets (n_tgt x 3, row-major) at the targets, grad_sources
+ * (nnk_fmm_source_count x 3) at the fine points (NEAREST) or potentials.
+ * forces and weights in `layout`; either output may be NULL. */
+int nnk_fmm_grad_positions(nnk_fmm* fmm, const double* forces, const double* weights, int32_t layout,
+                           double* grad_targets, double* grad_sources, int32_t on_device);
+
 int nnk_fmm_profile(nnk_fmm* fmm, int32_t enable);
 int nnk_fmm_profile_read(nnk_fmm* fmm, double* ms, int64_t* launches);
 int nnk_fmm_destroy(nnk_fmm* fmm);
@@ -241,6 +259,21 @@ int nnk_mob_solve(nnk_mob* mob, const double* rhs, double* x,
  * FP64 residual meets tol (at most max_outer times; inner tolerance at least
  * inner_tol).  fp64 = NULL switches refinement off. */
 int nnk_mob_set_refinement(nnk_mob* mob, nnk_fmm* fp64, int32_t max_outer, double inner_tol);
+/* Adjoint of the mobility matvec, A^T = [F^T B^T; BT^T 0] (F = the FMM block). */
+int nnk_mob_apply_adjoint(nnk_mob* mob, const double* x, double* y, int32_t on_device);
+/* The mobility matvec with another FMM on the same tree (e.g. at eps +- d
+ * for the eps-derivative of the operator). */
+int nnk_mob_apply_fmm(nnk_mob* mob, nnk_fmm* fmm, const double* x, double* y, int32_t on_device);
+/* gmres on A^T (refined like nnk_mob_solve when refinement is set). */
+int nnk_mob_solve_adjoint(nnk_mob* mob, const double* rhs, double* x, const nnk_solve_params* sp,
+                          nnk_solve_info* info, int32_t on_device);
+/* -lam^T (dA/dpositions) z for z = A^-1 b and lam = A^-T dL/dz: the
+ * position gradient of a loss L(z) (b independent of positions, as for
+ * forces, torques and a zero slip): grad_points (N x 3, force points,
+ * row-major) and grad_fine (Q x 3, fine points, NEAREST; may be NULL).
+ * NN is held fixed (it is piecewise constant in the positions). */
+int nnk_mob_grad_positions(nnk_mob* mob, const double* z, const double* lam, double* grad_points,
+                           double* grad_fine, int32_t on_device);
 int nnk_mob_destroy(nnk_mob* mob);
 
 /* ---------------------------------------------------- batched mobility -- */

@@ -285,6 +285,62 @@ int nnk_fmm_reduced_solve(nnk_fmm* fmm, const double* in, double* out, int32_t l
   return fmm_apply_common(fmm, in, out, layout, 1, on_device, 3);
 }
 
+int nnk_fmm_apply_adjoint(nnk_fmm* fmm, const double* in, double* out, int32_t layout, int32_t nrhs,
+                          int32_t on_device) {
+  if (!fmm || !in || !out || nrhs < 1 || (layout != NNK_LAYOUT_ROWS && layout != NNK_LAYOUT_BLOCKED))
+    return fail(fmm ? fmm->ctx : nullptr, NNK_E_ARG, "bad arguments");
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Fmm& F = *fmm->f;
+  const nnk::HostTree& t = F.tree();
+  const size_t nin = (size_t)nrhs * 3 * t.n_tgt, nout = (size_t)nrhs * 3 * t.n_pot;
+  const double* din = stage_in(ctx, F.io_in, in, nin, on_device);
+  double* dout = stage_out(F.io_out, out, nout, on_device);
+  F.apply_adjoint(din, dout, layout, nrhs);
+  finish_out(ctx, F.io_out, out, nout, on_device);
+  API_CATCH(ctx)
+}
+
+int nnk_fmm_source_count(const nnk_fmm* fmm, int64_t* count) {
+  if (!fmm || !count) return NNK_E_ARG;
+  *count = fmm->f->source_origins();
+  return NNK_OK;
+}
+
+int nnk_fmm_grad_positions(nnk_fmm* fmm, const double* forces, const double* weights, int32_t layout,
+                           double* grad_targets, double* grad_sources, int32_t on_device) {
+  if (!fmm || !forces || !weights || (!grad_targets && !grad_sources) ||
+      (layout != NNK_LAYOUT_ROWS && layout != NNK_LAYOUT_BLOCKED))
+    return fail(fmm ? fmm->ctx : nullptr, NNK_E_ARG, "bad arguments");
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Fmm& F = *fmm->f;
+  const nnk::HostTree& t = F.tree();
+  const size_t nf = 3 * (size_t)t.n_pot, nw = 3 * (size_t)t.n_tgt, ns = 3 * (size_t)F.source_origins();
+  nnk::DBuf<double> buf;
+  double *df = nullptr, *dw = nullptr, *dgt = grad_targets, *dgs = grad_sources;
+  if (!on_device) {
+    buf.alloc(nf + 2 * nw + ns);
+    df = buf.p;
+    dw = buf.p + nf;
+    NNK_CUDA(cudaMemcpyAsync(df, forces, nf * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    NNK_CUDA(cudaMemcpyAsync(dw, weights, nw * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    dgt = grad_targets ? buf.p + nf + nw : nullptr;
+    dgs = grad_sources ? buf.p + nf + 2 * nw : nullptr;
+  }
+  F.grad_positions(on_device ? forces : df, on_device ? weights : dw, layout, dgt, dgs);
+  if (!on_device) {
+    if (grad_targets)
+      NNK_CUDA(cudaMemcpyAsync(grad_targets, dgt, nw * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (grad_sources)
+      NNK_CUDA(cudaMemcpyAsync(grad_sources, dgs, ns * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  NNK_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_CATCH(ctx)
+}
+
 int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats) {
   if (!fmm || !stats) return NNK_E_ARG;
   *stats = fmm->f->stats();
@@ -401,6 +457,79 @@ int nnk_mob_set_refinement(nnk_mob* mob, nnk_fmm* fp64, int32_t max_outer, doubl
   if (fp64 && fp64->f->params().precision != NNK_PREC_FP64)
     return fail(ctx, NNK_E_ARG, "refinement needs an FP64 FMM");
   mob->m->set_refinement(fp64 ? fp64->f.get() : nullptr, max_outer, inner_tol);
+  API_CATCH(ctx)
+}
+
+int nnk_mob_apply_adjoint(nnk_mob* mob, const double* x, double* y, int32_t on_device) {
+  if (!mob || !x || !y) return NNK_E_ARG;
+  nnk_ctx* ctx = mob->fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Mobility& M = *mob->m;
+  const size_t n = (size_t)M.size();
+  const double* dx = stage_in(ctx, M.io_in, x, n, on_device);
+  double* dy = stage_out(M.io_out, y, n, on_device);
+  M.apply_adjoint(dx, dy);
+  finish_out(ctx, M.io_out, y, n, on_device);
+  API_CATCH(ctx)
+}
+
+int nnk_mob_apply_fmm(nnk_mob* mob, nnk_fmm* fmm, const double* x, double* y, int32_t on_device) {
+  if (!mob || !fmm || !x || !y) return NNK_E_ARG;
+  nnk_ctx* ctx = mob->fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  if (&fmm->f->tree() != &mob->fmm->f->tree()) return fail(ctx, NNK_E_ARG, "the FMM must share the mobility tree");
+  nnk::Mobility& M = *mob->m;
+  const size_t n = (size_t)M.size();
+  const double* dx = stage_in(ctx, M.io_in, x, n, on_device);
+  double* dy = stage_out(M.io_out, y, n, on_device);
+  M.apply_with(fmm->f.get(), dx, dy);
+  finish_out(ctx, M.io_out, y, n, on_device);
+  API_CATCH(ctx)
+}
+
+int nnk_mob_solve_adjoint(nnk_mob* mob, const double* rhs, double* x, const nnk_solve_params* sp,
+                          nnk_solve_info* info, int32_t on_device) {
+  if (!mob || !rhs || !x || !sp) return NNK_E_ARG;
+  nnk_ctx* ctx = mob->fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Mobility& M = *mob->m;
+  const size_t n = (size_t)M.size();
+  const double* db = stage_in(ctx, M.io_in, rhs, n, on_device);
+  double* dx = stage_out(M.io_out, x, n, on_device);
+  nnk_solve_info inf{};
+  M.solve_adjoint(db, dx, *sp, inf);
+  finish_out(ctx, M.io_out, x, n, on_device);
+  if (info) *info = inf;
+  if (inf.flag != 0) return fail(ctx, NNK_E_NOCONV, "gmres stopped at maxit above tol");
+  API_CATCH(ctx)
+}
+
+int nnk_mob_grad_positions(nnk_mob* mob, const double* z, const double* lam, double* grad_points,
+                           double* grad_fine, int32_t on_device) {
+  if (!mob || !z || !lam || !grad_points) return NNK_E_ARG;
+  nnk_ctx* ctx = mob->fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Mobility& M = *mob->m;
+  const nnk::HostTree& t = mob->fmm->f->tree();
+  const size_t n = (size_t)M.size(), nx = 3 * (size_t)t.n_tgt;
+  const size_t ny = t.params.nearest ? 3 * (size_t)t.q : 0;
+  if (on_device) {
+    M.grad_positions(z, lam, grad_points, grad_fine);
+  } else {
+    nnk::DBuf<double> buf(2 * n + nx + std::max<size_t>(ny, 1));
+    NNK_CUDA(cudaMemcpyAsync(buf.p, z, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    NNK_CUDA(cudaMemcpyAsync(buf.p + n, lam, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    double* gx = buf.p + 2 * n;
+    double* gy = grad_fine && ny ? gx + nx : nullptr;
+    M.grad_positions(buf.p, buf.p + n, gx, gy);
+    NNK_CUDA(cudaMemcpyAsync(grad_points, gx, nx * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (gy) NNK_CUDA(cudaMemcpyAsync(grad_fine, gy, ny * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    NNK_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
   API_CATCH(ctx)
 }
 

@@ -235,114 +235,17 @@ void Fmm::build_points() {
 
 void Fmm::build_tasks() {
   const HostTree& t = *t_;
-  std::vector<TaskD> tasks;
-  std::vector<SegD> segs;
-  const long long upB = E_, dnB = E_ + (long long)P_ * N_;
-  auto src_seg = [&](int32_t leaf) {
-    const long long s = t.src_start[leaf], e = t.src_start[leaf + 1];
-    if (e > s) segs.push_back(SegD{s, (int)(e - s), 0});
-    return e - s;
-  };
-  int64_t pairs_up = 0, pairs_down = 0, pairs_leaf = 0, pairs_p2p = 0, m2l = 0, c2e = 0;
-  up_.assign(maxl_ + 1, {});
-  down_.assign(maxl_ + 1, {});
-  up_off_.assign(maxl_ + 2, 0);
-  up_nodes_host_.clear();
-  // upward pass (upwardPass.m:32-100): non-empty potential leaves and
-  // non-leaves, level by level from the bottom.  The root's expansion is never
-  // used by any list, so level 0 is skipped.
-  for (int L = maxl_; L >= 0; --L) {
-    up_[L].first = (int64_t)tasks.size();
-    up_off_[L] = (int64_t)up_nodes_host_.size();
-    if (L >= 1) {
-      for (int32_t n : t.by_level[L]) {
-        const bool leaf = t.child0[n] < 0;
-        if (leaf && !t.pleaf[n]) continue;
-        TaskD tk{dnB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
-        if (leaf) {
-          pairs_up += (int64_t)P_ * src_seg(n);
-        } else {
-          for (int k = 0; k < 8; ++k) segs.push_back(SegD{upB + (long long)P_ * (t.child0[n] + k), P_, 0});
-          pairs_up += 8LL * P_ * P_;
-        }
-        tk.nseg = (int)segs.size() - tk.seg0;
-        tasks.push_back(tk);
-        up_nodes_host_.push_back(n);
-      }
-    }
-    up_[L].count = (int64_t)tasks.size() - up_[L].first;
-  }
-  // up_off_ was filled top-down in reverse; rebuild as per-level ranges
-  {
-    std::vector<int32_t> nodes;
-    std::vector<int64_t> off(maxl_ + 2, 0);
-    for (int L = 0; L <= maxl_; ++L) {
-      off[L] = (int64_t)nodes.size();
-      if (L == 0) continue;
-      for (int32_t n : t.by_level[L])
-        if (t.child0[n] >= 0 || t.pleaf[n]) nodes.push_back(n);
-    }
-    off[maxl_ + 1] = (int64_t)nodes.size();
-    up_nodes_host_ = nodes;
-    up_off_ = off;
-  }
-  // downward pass (downwardPass.m:39-168): every node of levels 1..max.
-  // The root's downward expansion is zero, so its L2L term is dropped.
-  // Two task sets: with the V-list as pair segments (FP64 mode), and without
-  // it (mixed mode, where M2L runs on the tensor cores before the pass).
-  down_nov_.assign(maxl_ + 1, {});
-  for (int L = 1; L <= maxl_; ++L) {
-    down_nov_[L].first = (int64_t)tasks.size();
-    for (int32_t n : t.by_level[L]) {
-      TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
-      for (int64_t k = t.X.off[n]; k < t.X.off[n + 1]; ++k) src_seg(t.X.idx[k]);
-      if (t.level[n] >= 2) segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
-      tk.nseg = (int)segs.size() - tk.seg0;
-      tasks.push_back(tk);
-    }
-    down_nov_[L].count = (int64_t)tasks.size() - down_nov_[L].first;
-  }
-  for (int L = 1; L <= maxl_; ++L) {
-    down_[L].first = (int64_t)tasks.size();
-    for (int32_t n : t.by_level[L]) {
-      TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
-      for (int64_t k = t.V.off[n]; k < t.V.off[n + 1]; ++k) {
-        segs.push_back(SegD{upB + (long long)P_ * t.V.idx[k], P_, 0});
-        pairs_down += (int64_t)P_ * P_;
-        ++m2l;
-      }
-      for (int64_t k = t.X.off[n]; k < t.X.off[n + 1]; ++k) pairs_down += (int64_t)P_ * src_seg(t.X.idx[k]);
-      if (t.level[n] >= 2) {  // the root's downward expansion is zero
-        segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
-        pairs_down += (int64_t)P_ * P_;
-      }
-      tk.nseg = (int)segs.size() - tk.seg0;
-      tasks.push_back(tk);
-    }
-    down_[L].count = (int64_t)tasks.size() - down_[L].first;
-  }
-  // leaf stage (downwardPass.m:170-294): L2T + U (P2P) + W (M2T)
-  leaf_.first = (int64_t)tasks.size();
-  for (int32_t i = 0; i < N_; ++i) {
-    if (!t.tleaf[i]) continue;
-    const int nt = (int)(t.tgt_start[i + 1] - t.tgt_start[i]);
-    TaskD tk{t.tgt_start[i], t.tgt_start[i], nt, (int)segs.size(), 0, 0};
-    for (int64_t k = t.U.off[i]; k < t.U.off[i + 1]; ++k) {
-      const int64_t s = src_seg(t.U.idx[k]);
-      pairs_leaf += (int64_t)nt * s;
-      pairs_p2p += (int64_t)nt * s;
-    }
-    for (int64_t k = t.W.off[i]; k < t.W.off[i + 1]; ++k) {
-      segs.push_back(SegD{upB + (long long)P_ * t.W.idx[k], P_, 0});
-      pairs_leaf += (int64_t)nt * P_;
-    }
-    segs.push_back(SegD{dnB + (long long)P_ * i, P_, 0});
-    pairs_leaf += (int64_t)nt * P_;
-    tk.nseg = (int)segs.size() - tk.seg0;
-    tasks.push_back(tk);
-  }
-  leaf_.count = (int64_t)tasks.size() - leaf_.first;
-  // node lists per level for the downward C2E step
+  TaskRoles r;
+  r.regionA = E_;
+  r.src_range = &t.src_start;
+  r.tgt_range = &t.tgt_start;
+  r.src_leaf = &t.pleaf;
+  r.tgt_leaf = &t.tleaf;
+  r.U = &t.U;
+  r.V = &t.V;
+  r.W = &t.W;
+  r.X = &t.X;
+  // node lists per level for the downward C2E step (every node of levels >= 1)
   lvl_off_.assign(maxl_ + 2, 0);
   std::vector<int32_t> ln;
   for (int L = 0; L <= maxl_; ++L) {
@@ -350,34 +253,146 @@ void Fmm::build_tasks() {
     if (L >= 1) ln.insert(ln.end(), t.by_level[L].begin(), t.by_level[L].end());
   }
   lvl_off_[maxl_ + 1] = (int64_t)ln.size();
-  c2e = (int64_t)ln.size() + (int64_t)up_nodes_host_.size();
   cudaStream_t st = ctx_->stream;
   {
-    std::vector<C2ETile> ut, dt;
-    build_c2e_tiles(up_nodes_host_, up_off_, ut, up_toff_);
+    std::vector<C2ETile> dt;
     build_c2e_tiles(ln, lvl_off_, dt, dn_toff_);
-    up_tiles_.upload(ut, st);
     dn_tiles_.upload(dt, st);
   }
-  split_tasks(tasks, segs);
-  tasks_.upload(tasks, st);
-  segs_.upload(segs, st);
   lvl_nodes_.upload(ln, st);
-  up_nodes_.upload(up_nodes_host_, st);
   {
     std::vector<int32_t> roots(t.groups());
     for (int g = 0; g < t.groups(); ++g) roots[g] = t.root_of(g);
     roots_.upload(roots, st);
   }
-  NNK_CUDA(cudaStreamSynchronize(st));
-  stats_.pairs_leaf = pairs_leaf;
-  stats_.pairs_p2p = pairs_p2p;
-  stats_.pairs_up = pairs_up;
-  stats_.pairs_down = pairs_down;
-  stats_.m2l_pairs = m2l;
-  stats_.c2e_columns = c2e;
+  build_taskset(fwd_, r, true);
+  stats_.c2e_columns = (int64_t)ln.size() + (int64_t)fwd_.up_nodes_host.size();
   stats_.surface_points = P_;
   stats_.levels = maxl_ + 1;
+  const int64_t slots = std::max<int64_t>(3 * fwd_.partial_slots * R_, 1);
+  if (p_.precision == NNK_PREC_FP64) partial64_.alloc(slots);
+  else partial32_.alloc(slots);
+  NNK_CUDA(cudaStreamSynchronize(st));
+}
+
+void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
+  const HostTree& t = *t_;
+  std::vector<TaskD> tasks;
+  std::vector<SegD> segs;
+  const long long upB = r.regionA, dnB = r.regionA + (long long)P_ * N_;
+  const std::vector<int64_t>& sr = *r.src_range;
+  const std::vector<int64_t>& tr = *r.tgt_range;
+  auto src_seg = [&](int32_t leaf) {
+    const long long s = sr[leaf], e = sr[leaf + 1];
+    if (e > s) segs.push_back(SegD{s, (int)(e - s), 0});
+    return e - s;
+  };
+  int64_t pairs_up = 0, pairs_down = 0, pairs_leaf = 0, pairs_p2p = 0, m2l = 0;
+  ts.up.assign(maxl_ + 1, {});
+  ts.down.assign(maxl_ + 1, {});
+  ts.down_nov.assign(maxl_ + 1, {});
+  // upward pass (upwardPass.m:32-100): leaves with sources and non-leaves,
+  // level by level from the bottom.  The root's expansion is never used by
+  // any list, so level 0 is skipped.
+  for (int L = maxl_; L >= 1; --L) {
+    ts.up[L].first = (int64_t)tasks.size();
+    for (int32_t n : t.by_level[L]) {
+      const bool leaf = t.child0[n] < 0;
+      if (leaf && !(*r.src_leaf)[n]) continue;
+      TaskD tk{dnB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
+      if (leaf) {
+        pairs_up += (int64_t)P_ * src_seg(n);
+      } else {
+        for (int k = 0; k < 8; ++k) segs.push_back(SegD{upB + (long long)P_ * (t.child0[n] + k), P_, 0});
+        pairs_up += 8LL * P_ * P_;
+      }
+      tk.nseg = (int)segs.size() - tk.seg0;
+      tasks.push_back(tk);
+    }
+    ts.up[L].count = (int64_t)tasks.size() - ts.up[L].first;
+  }
+  ts.up_nodes_host.clear();
+  ts.up_off.assign(maxl_ + 2, 0);
+  for (int L = 0; L <= maxl_; ++L) {
+    ts.up_off[L] = (int64_t)ts.up_nodes_host.size();
+    if (L == 0) continue;
+    for (int32_t n : t.by_level[L])
+      if (t.child0[n] >= 0 || (*r.src_leaf)[n]) ts.up_nodes_host.push_back(n);
+  }
+  ts.up_off[maxl_ + 1] = (int64_t)ts.up_nodes_host.size();
+  // downward pass (downwardPass.m:39-168): every node of levels 1..max.
+  // The root's downward expansion is zero, so its L2L term is dropped.
+  // Two task sets: with the V-list as pair segments, and without it (M2L by
+  // the tensor-core or Fourier-space kernels before the pass).
+  for (int L = 1; L <= maxl_; ++L) {
+    ts.down_nov[L].first = (int64_t)tasks.size();
+    for (int32_t n : t.by_level[L]) {
+      TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
+      for (int64_t k = r.X->off[n]; k < r.X->off[n + 1]; ++k) src_seg(r.X->idx[k]);
+      if (t.level[n] >= 2) segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
+      tk.nseg = (int)segs.size() - tk.seg0;
+      tasks.push_back(tk);
+    }
+    ts.down_nov[L].count = (int64_t)tasks.size() - ts.down_nov[L].first;
+  }
+  for (int L = 1; L <= maxl_; ++L) {
+    ts.down[L].first = (int64_t)tasks.size();
+    for (int32_t n : t.by_level[L]) {
+      TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
+      for (int64_t k = r.V->off[n]; k < r.V->off[n + 1]; ++k) {
+        segs.push_back(SegD{upB + (long long)P_ * r.V->idx[k], P_, 0});
+        pairs_down += (int64_t)P_ * P_;
+        ++m2l;
+      }
+      for (int64_t k = r.X->off[n]; k < r.X->off[n + 1]; ++k) pairs_down += (int64_t)P_ * src_seg(r.X->idx[k]);
+      if (t.level[n] >= 2) {  // the root's downward expansion is zero
+        segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
+        pairs_down += (int64_t)P_ * P_;
+      }
+      tk.nseg = (int)segs.size() - tk.seg0;
+      tasks.push_back(tk);
+    }
+    ts.down[L].count = (int64_t)tasks.size() - ts.down[L].first;
+  }
+  // leaf stage (downwardPass.m:170-294): L2T + U (P2P) + W (M2T)
+  ts.leaf.first = (int64_t)tasks.size();
+  for (int32_t i = 0; i < N_; ++i) {
+    if (!(*r.tgt_leaf)[i]) continue;
+    const int nt = (int)(tr[i + 1] - tr[i]);
+    if (nt == 0) continue;
+    TaskD tk{tr[i], tr[i], nt, (int)segs.size(), 0, 0};
+    for (int64_t k = r.U->off[i]; k < r.U->off[i + 1]; ++k) {
+      const int64_t s = src_seg(r.U->idx[k]);
+      pairs_leaf += (int64_t)nt * s;
+      pairs_p2p += (int64_t)nt * s;
+    }
+    for (int64_t k = r.W->off[i]; k < r.W->off[i + 1]; ++k) {
+      segs.push_back(SegD{upB + (long long)P_ * r.W->idx[k], P_, 0});
+      pairs_leaf += (int64_t)nt * P_;
+    }
+    segs.push_back(SegD{dnB + (long long)P_ * i, P_, 0});
+    pairs_leaf += (int64_t)nt * P_;
+    tk.nseg = (int)segs.size() - tk.seg0;
+    tasks.push_back(tk);
+  }
+  ts.leaf.count = (int64_t)tasks.size() - ts.leaf.first;
+  cudaStream_t st = ctx_->stream;
+  {
+    std::vector<C2ETile> ut;
+    build_c2e_tiles(ts.up_nodes_host, ts.up_off, ut, ts.up_toff);
+    ts.up_tiles.upload(ut, st);
+  }
+  split_tasks(ts, tasks, segs);
+  ts.tasks.upload(tasks, st);
+  ts.segs.upload(segs, st);
+  ts.up_nodes.upload(ts.up_nodes_host, st);
+  if (stats) {
+    stats_.pairs_leaf = pairs_leaf;
+    stats_.pairs_p2p = pairs_p2p;
+    stats_.pairs_up = pairs_up;
+    stats_.pairs_down = pairs_down;
+    stats_.m2l_pairs = m2l;
+  }
 }
 
 // Per level, runs of nodes of the same tree cut into tiles of at most 32
@@ -406,7 +421,7 @@ void Fmm::build_c2e_tiles(const std::vector<int32_t>& nodes, const std::vector<i
 // task above kMaxPairs target-source pairs is cut into pieces over its
 // flattened sources; each piece writes its own partial-sum slot and one
 // reduction per task adds the slots in a fixed order.
-void Fmm::split_tasks(std::vector<TaskD>& tasks, std::vector<SegD>& segs) {
+void Fmm::split_tasks(TaskSet& ts, std::vector<TaskD>& tasks, std::vector<SegD>& segs) {
   constexpr int64_t kMaxPairs = 1 << 16;
   constexpr int64_t kMinSources = 64;
   std::vector<TaskD> nt;
@@ -470,30 +485,29 @@ void Fmm::split_tasks(std::vector<TaskD>& tasks, std::vector<SegD>& segs) {
     g.red_first = rfirst;
     g.red_count = (int64_t)reds.size() - rfirst;
   };
-  for (auto& g : up_) process(g);
-  for (auto& g : down_nov_) process(g);
-  for (auto& g : down_) process(g);
-  process(leaf_);
+  for (auto& g : ts.up) process(g);
+  for (auto& g : ts.down_nov) process(g);
+  for (auto& g : ts.down) process(g);
+  process(ts.leaf);
   tasks.swap(nt);
   segs.swap(ns);
-  reds_.upload(reds, ctx_->stream);
-  if (p_.precision == NNK_PREC_FP64) partial64_.alloc(std::max<int64_t>(3 * pbase * R_, 1));
-  else partial32_.alloc(std::max<int64_t>(3 * pbase * R_, 1));
+  ts.reds.upload(reds, ctx_->stream);
+  ts.partial_slots = pbase;
 }
 
 template <typename Real>
-void Fmm::run_group(const TaskGroup& g, const Real* spos, const Real* sstr, const Real* tpos, Real* out, Real e2,
-                    Real scale, int accumulate, int phase_id, int R) {
+void Fmm::run_group(const TaskSet& ts, const TaskGroup& g, const Real* spos, const Real* sstr, const Real* tpos,
+                    Real* out, Real e2, Real scale, int accumulate, int phase_id, int R) {
   if (g.count == 0) return;
   cudaStream_t st = ctx_->stream;
   Real* partial = std::is_same<Real, double>::value ? (Real*)partial64_.p : (Real*)partial32_.p;
   phase(phase_id, [&] {
-    launch_p2p<Real>(tasks_.p + g.first, (int)g.count, segs_.p, spos, sstr, tpos, out, partial, e2, scale, st,
+    launch_p2p<Real>(ts.tasks.p + g.first, (int)g.count, ts.segs.p, spos, sstr, tpos, out, partial, e2, scale, st,
                      accumulate, R);
   });
   if (g.red_count)
     phase(phase_id,
-          [&] { launch_reduce<Real>(reds_.p + g.red_first, (int)g.red_count, partial, out, accumulate, st, R); });
+          [&] { launch_reduce<Real>(ts.reds.p + g.red_first, (int)g.red_count, partial, out, accumulate, st, R); });
 }
 
 // Operator index of every (tree, level): one per distinct box width.
@@ -659,36 +673,33 @@ __global__ void zero_roots_kernel(const int32_t* __restrict__ roots, long long b
 }  // namespace
 
 template <typename Real>
-void Fmm::apply_impl(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int k0, int R) {
+void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R) {
   cudaStream_t st = ctx_->stream;
-  const HostTree& t = *t_;
-  Real* str = p_.precision == NNK_PREC_FP64 ? (Real*)str64_.p : (Real*)str32_.p;
-  const Real* pos = p_.precision == NNK_PREC_FP64 ? (const Real*)pos64_.p : (const Real*)pos32_.p;
-  const Real* tpos = p_.precision == NNK_PREC_FP64 ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
   Real* check = p_.precision == NNK_PREC_FP64 ? (Real*)check64_.p : (Real*)check32_.p;
-  Real* vel = p_.precision == NNK_PREC_FP64 ? (Real*)vel64_.p : (Real*)vel32_.p;
   const Real e2 = (Real)(p_.eps * p_.eps);
   const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
   const int n = 3 * P_;
   const int C = 3 * R;
-  // forces on the leaf source entries (kron(NN,I3)*f per leaf)
-  phase(NNK_PHASE_GATHER, [&] { launch_gather<Real>(E_, goff_.p, gidx_.p, gw_.p, d_in, in, k0, R, str, st); });
   // up-equivalent densities of nodes that are not computed stay zero
-  NNK_CUDA(cudaMemsetAsync(str + C * E_, 0, sizeof(Real) * C * (size_t)P_ * N_, st));
-  zero_roots_kernel<Real><<<(unsigned)roots_.n, 256, 0, st>>>(roots_.p, E_ + (long long)P_ * N_, P_, C, str);
+  NNK_CUDA(cudaMemsetAsync(str + C * regionA, 0, sizeof(Real) * C * (size_t)P_ * N_, st));
+  zero_roots_kernel<Real><<<(unsigned)roots_.n, 256, 0, st>>>(roots_.p, regionA + (long long)P_ * N_, P_, C, str);
   NNK_CHECK_LAUNCH();
-  const bool tm = tensor_m2l_ && std::is_same<Real, float>::value;
+  // the M2L kernels read V(i); the transpose needs V^-1(i), the same set
+  // when the relation is symmetric (it is for every tree of the reference)
+  const bool fast = &ts == &fwd_ || v_symmetric_;
+  const bool tm = fast && tensor_m2l_ && std::is_same<Real, float>::value;
+  const bool fm = fast && fft_m2l_ && std::is_same<Real, float>::value;
   if (tm && R != 1) throw Error(NNK_E_STATE, "tensor-core M2L takes one right-hand side per pass");
   if (tm && m2l_.h_err && *m2l_.h_err)
     throw Error(NNK_E_TIMEOUT, "tensor-core M2L gave up a bounded wait in an earlier call");
   // upward pass
   for (int L = maxl_; L >= 1; --L) {
-    if (up_[L].count == 0) continue;
-    run_group<Real>(up_[L], pos, str, pos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS, R);
-    const int64_t nt = up_toff_[L + 1] - up_toff_[L];
+    if (ts.up[L].count == 0) continue;
+    run_group<Real>(ts, ts.up[L], spos, str, spos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS, R);
+    const int64_t nt = ts.up_toff[L + 1] - ts.up_toff[L];
     phase(NNK_PHASE_UP_C2E, [&] {
-      launch_c2e<Real>(ops_.p, n, 0, up_tiles_.p + up_toff_[L], (int)nt, up_nodes_.p, check, str, E_, P_, R, st,
-                       tm ? m2l_.src.p : nullptr, m2l_.NP);
+      launch_c2e<Real>(ops_.p, n, 0, ts.up_tiles.p + ts.up_toff[L], (int)nt, ts.up_nodes.p, check, str, regionA, P_,
+                       R, st, tm ? m2l_.src.p : nullptr, m2l_.NP);
     });
   }
   // downward pass
@@ -697,26 +708,116 @@ void Fmm::apply_impl(const double* d_in, const IoMap& in, double* d_out, const I
     NNK_CUDA(cudaMemsetAsync(check, 0, sizeof(Real) * (size_t)N_ * n, st));
     phase(NNK_PHASE_M2L, [&] { launch_m2l(m2l_, (float*)check, n, st); });
   }
-  const bool fm = fft_m2l_ && std::is_same<Real, float>::value;
   if (fm) {
     // M2L of every level at once in Fourier space
     NNK_CUDA(cudaMemsetAsync(check, 0, sizeof(Real) * (size_t)N_ * n * R, st));
-    phase(NNK_PHASE_M2L, [&] { launch_fft_m2l(fft_, (const float*)str, E_, R, (float*)check, st); });
+    phase(NNK_PHASE_M2L, [&] { launch_fft_m2l(fft_, (const float*)str, regionA, R, (float*)check, st); });
   }
-  const std::vector<TaskGroup>& dgroups = (tm || fm) ? down_nov_ : down_;
+  const std::vector<TaskGroup>& dgroups = (tm || fm) ? ts.down_nov : ts.down;
   for (int L = 1; L <= maxl_; ++L) {
     if (dgroups[L].count == 0) continue;
-    run_group<Real>(dgroups[L], pos, str, pos, check, e2, scale, (tm || fm) ? 1 : 0, NNK_PHASE_DOWN_PAIRS, R);
+    run_group<Real>(ts, dgroups[L], spos, str, spos, check, e2, scale, (tm || fm) ? 1 : 0, NNK_PHASE_DOWN_PAIRS, R);
     const int64_t nt = dn_toff_[L + 1] - dn_toff_[L];
     phase(NNK_PHASE_DOWN_C2E, [&] {
       launch_c2e<Real>(ops_.p, n, 1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str,
-                       E_ + (int64_t)P_ * N_, P_, R, st);
+                       regionA + (int64_t)P_ * N_, P_, R, st);
     });
   }
+}
+
+template <typename Real>
+void Fmm::apply_impl(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int k0, int R) {
+  cudaStream_t st = ctx_->stream;
+  const HostTree& t = *t_;
+  Real* str = p_.precision == NNK_PREC_FP64 ? (Real*)str64_.p : (Real*)str32_.p;
+  const Real* pos = p_.precision == NNK_PREC_FP64 ? (const Real*)pos64_.p : (const Real*)pos32_.p;
+  const Real* tpos = p_.precision == NNK_PREC_FP64 ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
+  Real* vel = p_.precision == NNK_PREC_FP64 ? (Real*)vel64_.p : (Real*)vel32_.p;
+  const Real e2 = (Real)(p_.eps * p_.eps);
+  const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
+  // forces on the leaf source entries (kron(NN,I3)*f per leaf)
+  phase(NNK_PHASE_GATHER, [&] { launch_gather<Real>(E_, goff_.p, gidx_.p, gw_.p, d_in, in, k0, R, str, st); });
+  far_field<Real>(fwd_, pos, str, E_, R);
   // leaf stage
-  run_group<Real>(leaf_, pos, str, tpos, vel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS, R);
+  run_group<Real>(fwd_, fwd_.leaf, pos, str, tpos, vel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS, R);
   phase(NNK_PHASE_SCATTER,
         [&] { launch_scatter<Real>((int64_t)t.tgt_row.size(), trow_.p, vel, out, k0, R, d_out, st); });
+}
+
+// Transpose: the same passes on the same tree with the roles of the point
+// sets exchanged (leaf sources = sorted targets, leaf targets = entries) and
+// the lists inverted; the up and down operators are A and A^T as in the
+// matvec, since (A^T)^T = A takes the place of each.
+template <typename Real>
+void Fmm::adjoint_impl(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int k0, int R) {
+  cudaStream_t st = ctx_->stream;
+  const HostTree& t = *t_;
+  const int64_t nt = (int64_t)t.tgt_row.size();
+  Real* astr = p_.precision == NNK_PREC_FP64 ? (Real*)astr64_.p : (Real*)astr32_.p;
+  const Real* apos = p_.precision == NNK_PREC_FP64 ? (const Real*)apos64_.p : (const Real*)apos32_.p;
+  const Real* pos = p_.precision == NNK_PREC_FP64 ? (const Real*)pos64_.p : (const Real*)pos32_.p;
+  Real* avel = p_.precision == NNK_PREC_FP64 ? (Real*)avel64_.p : (Real*)avel32_.p;
+  const Real e2 = (Real)(p_.eps * p_.eps);
+  const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
+  phase(NNK_PHASE_GATHER, [&] { launch_gather<Real>(nt, agoff_.p, agidx_.p, agw_.p, d_in, in, k0, R, astr, st); });
+  far_field<Real>(adj_, apos, astr, nt, R);
+  run_group<Real>(adj_, adj_.leaf, apos, astr, pos, avel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS, R);
+  phase(NNK_PHASE_SCATTER, [&] {
+    scatter_sum_kernel<Real><<<(unsigned)((t.n_pot + 255) / 256), 256, 0, st>>>(
+        t.n_pot, (const long long*)row_off_.p, (const long long*)row_ent_.p, row_w_.p, avel, out, k0, R, d_out);
+    NNK_CHECK_LAUNCH();
+  });
+}
+
+// Gradient of <w, apply(f)> with respect to the positions:
+//   targets: sum_i w_t,i d/dt u_i(t), u the velocity field of f, from the
+//   leaf-stage sources of the matvec (entries, W up-densities, own down-density);
+//   sources: sum_j g_e,j d/de w~_j(e), w~ the field of the transpose applied
+//   to w and g_e the force of entry e, summed over the entries of each origin.
+template <typename Real>
+void Fmm::grad_impl(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs) {
+  cudaStream_t st = ctx_->stream;
+  const HostTree& t = *t_;
+  const int64_t nt = (int64_t)t.tgt_row.size();
+  Real* str = p_.precision == NNK_PREC_FP64 ? (Real*)str64_.p : (Real*)str32_.p;
+  const Real* pos = p_.precision == NNK_PREC_FP64 ? (const Real*)pos64_.p : (const Real*)pos32_.p;
+  const Real* tpos = p_.precision == NNK_PREC_FP64 ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
+  Real* vel = p_.precision == NNK_PREC_FP64 ? (Real*)vel64_.p : (Real*)vel32_.p;
+  Real* astr = p_.precision == NNK_PREC_FP64 ? (Real*)astr64_.p : (Real*)astr32_.p;
+  const Real* apos = p_.precision == NNK_PREC_FP64 ? (const Real*)apos64_.p : (const Real*)apos32_.p;
+  Real* avel = p_.precision == NNK_PREC_FP64 ? (Real*)avel64_.p : (Real*)avel32_.p;
+  Real* partial = p_.precision == NNK_PREC_FP64 ? (Real*)partial64_.p : (Real*)partial32_.p;
+  const Real e2 = (Real)(p_.eps * p_.eps);
+  const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
+  IoMap fin, win;
+  fin.layout = win.layout = layout;
+  fin.nrows = t.n_pot;
+  win.nrows = t.n_tgt;
+  // matvec far field of f; the weights w at the sorted targets
+  launch_gather<Real>(E_, goff_.p, gidx_.p, gw_.p, d_f, fin, 0, 1, str, st);
+  far_field<Real>(fwd_, pos, str, E_, 1);
+  launch_gather<Real>(nt, agoff_.p, agidx_.p, agw_.p, d_w, win, 0, 1, astr, st);
+  if (d_gt) {
+    const TaskGroup& g = fwd_.leaf;
+    launch_p2p_grad<Real>(fwd_.tasks.p + g.first, (int)g.count, fwd_.segs.p, pos, str, tpos, astr, vel, partial, e2,
+                          scale, st);
+    launch_reduce<Real>(fwd_.reds.p + g.red_first, (int)g.red_count, partial, vel, 0, st, 1);
+    IoMap rows;
+    rows.layout = NNK_LAYOUT_ROWS;
+    rows.nrows = t.n_tgt;
+    launch_scatter<Real>(nt, trow_.p, vel, rows, 0, 1, d_gt, st);
+  }
+  if (d_gs) {
+    // transpose far field of w (the gather of w into astr region A is done)
+    far_field<Real>(adj_, apos, astr, nt, 1);
+    const TaskGroup& g = adj_.leaf;
+    launch_p2p_grad<Real>(adj_.tasks.p + g.first, (int)g.count, adj_.segs.p, apos, astr, pos, str, avel, partial, e2,
+                          scale, st);
+    launch_reduce<Real>(adj_.reds.p + g.red_first, (int)g.red_count, partial, avel, 0, st, 1);
+    origin_sum_kernel<Real><<<(unsigned)((norigin_ + 255) / 256), 256, 0, st>>>(
+        norigin_, (const long long*)org_off_.p, (const long long*)org_ent_.p, avel, d_gs);
+    NNK_CHECK_LAUNCH();
+  }
 }
 
 void Fmm::apply(const double* d_in, double* d_out, int layout, int nrhs) {
@@ -739,6 +840,165 @@ void Fmm::apply_mapped(const double* d_in, const IoMap& in, double* d_out, const
       apply_impl<float>(d_in, in, d_out, out, k0, R);
     k0 += R;
   }
+}
+
+void Fmm::apply_adjoint(const double* d_in, double* d_out, int layout, int nrhs) {
+  const HostTree& t = *t_;
+  IoMap in, out;
+  in.layout = out.layout = layout;
+  in.nrows = t.n_tgt;
+  out.nrows = t.n_pot;
+  apply_adjoint_mapped(d_in, in, d_out, out, nrhs);
+}
+
+void Fmm::apply_adjoint_mapped(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int nrhs) {
+  if (t_->n_pot == 0) return;
+  build_adjoint();
+  const int cap = (tensor_m2l_ && v_symmetric_) ? 1 : R_;
+  for (int k0 = 0; k0 < nrhs;) {
+    const int R = rhs_chunk(nrhs - k0, cap);
+    if (p_.precision == NNK_PREC_FP64)
+      adjoint_impl<double>(d_in, in, d_out, out, k0, R);
+    else
+      adjoint_impl<float>(d_in, in, d_out, out, k0, R);
+    k0 += R;
+  }
+}
+
+int64_t Fmm::source_origins() const { return t_->params.nearest ? t_->q : t_->n_pot; }
+
+void Fmm::grad_positions(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs) {
+  if (t_->n_tgt == 0 || t_->n_pot == 0) return;
+  build_adjoint();
+  if (p_.precision == NNK_PREC_FP64)
+    grad_impl<double>(d_f, d_w, layout, d_gt, d_gs);
+  else
+    grad_impl<float>(d_f, d_w, layout, d_gt, d_gs);
+}
+
+namespace {
+// inverse of a list relation: out(j) = { i : j in L(i) }, ascending i
+Csr invert(const Csr& L, int32_t nodes) {
+  Csr out;
+  out.off.assign(nodes + 1, 0);
+  for (int32_t j : L.idx) out.off[j + 1]++;
+  for (int32_t j = 0; j < nodes; ++j) out.off[j + 1] += out.off[j];
+  out.idx.assign(L.idx.size(), 0);
+  std::vector<int64_t> pos(out.off.begin(), out.off.end() - 1);
+  for (int32_t i = 0; i < nodes; ++i)
+    for (int64_t k = L.off[i]; k < L.off[i + 1]; ++k) out.idx[pos[L.idx[k]]++] = i;
+  return out;
+}
+}  // namespace
+
+void Fmm::build_adjoint() {
+  if (adj_ready_) return;
+  const HostTree& t = *t_;
+  cudaStream_t st = ctx_->stream;
+  const int64_t nt = (int64_t)t.tgt_row.size();
+  inv_U_ = invert(t.U, N_);
+  inv_V_ = invert(t.V, N_);
+  inv_W_ = invert(t.W, N_);
+  inv_X_ = invert(t.X, N_);
+  v_symmetric_ = true;
+  for (int32_t i = 0; i < N_ && v_symmetric_; ++i) {
+    std::vector<int32_t> a(t.V.idx.begin() + t.V.off[i], t.V.idx.begin() + t.V.off[i + 1]);
+    std::vector<int32_t> b(inv_V_.idx.begin() + inv_V_.off[i], inv_V_.idx.begin() + inv_V_.off[i + 1]);
+    std::sort(a.begin(), a.end());
+    v_symmetric_ = a == b;
+  }
+  TaskRoles r;
+  r.regionA = nt;
+  r.src_range = &t.tgt_start;
+  r.tgt_range = &t.src_start;
+  r.src_leaf = &t.tleaf;
+  r.tgt_leaf = &t.pleaf;
+  r.U = &inv_U_;
+  r.V = &inv_V_;
+  r.W = &inv_X_;  // leaves s receive from upsurf(t) for t with s in X(t)
+  r.X = &inv_W_;  // node t receives from the targets of leaves s with t in W(s)
+  build_taskset(adj_, r, false);
+  const int64_t slots = 3 * std::max(fwd_.partial_slots, adj_.partial_slots) * R_;
+  if (p_.precision == NNK_PREC_FP64) {
+    if ((int64_t)partial64_.n < slots) partial64_.alloc(slots);
+  } else if ((int64_t)partial32_.n < slots) {
+    partial32_.alloc(slots);
+  }
+  // unified points of the transpose: [sorted targets | up surfaces | down surfaces]
+  const int64_t atot = nt + 2LL * P_ * N_;
+  auto lat = shell_lattice(p_.res, p_.shells);
+  std::vector<double> pos(3 * (size_t)atot);
+  std::vector<int32_t> pg(atot, 0);
+  std::copy(t.tgt_pos.begin(), t.tgt_pos.end(), pos.begin());
+  for (int32_t n = 0; n < N_; ++n) {
+    const int32_t g = t.group_of(n);
+    for (int64_t i = t.tgt_start[n]; i < t.tgt_start[n + 1]; ++i) pg[i] = g;
+    const double* c = &t.corners[6 * n];
+    const double lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[3], c[4], c[5]};
+    surface(lo, hi, p_.res, lat, &pos[3 * (nt + (size_t)P_ * n)]);
+    double dlo[3], dhi[3];
+    for (int d = 0; d < 3; ++d) {
+      const double w = hi[d] - lo[d];
+      dlo[d] = lo[d] - w;
+      dhi[d] = hi[d] + w;
+    }
+    surface(dlo, dhi, p_.res, lat, &pos[3 * (nt + (size_t)P_ * N_ + (size_t)P_ * n)]);
+    for (int k = 0; k < P_; ++k) {
+      pg[nt + (size_t)P_ * n + k] = g;
+      pg[nt + (size_t)P_ * N_ + (size_t)P_ * n + k] = g;
+    }
+  }
+  if (p_.precision == NNK_PREC_FP64) {
+    apos64_.upload(pos, st);
+    astr64_.alloc(3 * atot * R_);
+    avel64_.alloc(std::max<int64_t>(3 * E_ * R_, 1));
+  } else {
+    std::vector<float> p4(4 * (size_t)atot);
+    for (int64_t i = 0; i < atot; ++i) {
+      const double* sh = &shift_[3 * (size_t)pg[i]];
+      for (int d = 0; d < 3; ++d) p4[4 * i + d] = (float)(pos[3 * i + d] - sh[d]);
+      p4[4 * i + 3] = 0.f;
+    }
+    apos32_.upload(p4, st);
+    astr32_.alloc(3 * atot * R_);
+    avel32_.alloc(std::max<int64_t>(3 * E_ * R_, 1));
+  }
+  // identity gather of the target values in sorted order
+  std::vector<int64_t> goff(nt + 1);
+  for (int64_t i = 0; i <= nt; ++i) goff[i] = i;
+  agoff_.upload(goff, st);
+  agidx_.upload(t.tgt_row, st);
+  agw_.upload(std::vector<double>(std::max<int64_t>(nt, 1), 1.0), st);
+  // transpose of the gather: per potential row its (entry, weight) pairs
+  {
+    std::vector<int64_t> off(t.n_pot + 1, 0);
+    for (int32_t r : t.src_gidx) off[r + 1]++;
+    for (int64_t r = 0; r < t.n_pot; ++r) off[r + 1] += off[r];
+    std::vector<int64_t> ent(t.src_gidx.size()), at(off.begin(), off.end() - 1);
+    std::vector<double> w(t.src_gidx.size());
+    for (int64_t e = 0; e < E_; ++e)
+      for (int64_t k = t.src_goff[e]; k < t.src_goff[e + 1]; ++k) {
+        const int64_t q = at[t.src_gidx[k]]++;
+        ent[q] = e;
+        w[q] = t.src_gw[k];
+      }
+    row_off_.upload(off, st);
+    row_ent_.upload(ent, st);
+    row_w_.upload(w, st);
+  }
+  // entries of each source origin (fine point or potential row)
+  {
+    norigin_ = source_origins();
+    std::vector<int64_t> off(norigin_ + 1, 0);
+    for (int64_t o : t.src_origin) off[o + 1]++;
+    for (int64_t o = 0; o < norigin_; ++o) off[o + 1] += off[o];
+    std::vector<int64_t> ent(t.src_origin.size()), at(off.begin(), off.end() - 1);
+    for (int64_t e = 0; e < (int64_t)t.src_origin.size(); ++e) ent[at[t.src_origin[e]]++] = e;
+    org_off_.upload(off, st);
+    org_ent_.upload(ent, st);
+  }
+  NNK_CUDA(cudaStreamSynchronize(st));
+  adj_ready_ = true;
 }
 
 template void Fmm::apply_impl<double>(const double*, const IoMap&, double*, const IoMap&, int, int);

@@ -77,6 +77,35 @@ struct C2ETile {
   int pad;
 };
 
+// The pair tasks of one direction of the operator (the matvec, or its
+// transpose), grouped by pass and level.
+struct TaskSet {
+  DBuf<TaskD> tasks;
+  DBuf<SegD> segs;
+  DBuf<RedD> reds;
+  std::vector<TaskGroup> up, down, down_nov;  // per level
+  TaskGroup leaf;
+  std::vector<int32_t> up_nodes_host;  // nodes whose up-equivalent density is formed, by level
+  DBuf<int32_t> up_nodes;
+  std::vector<int64_t> up_off;
+  DBuf<C2ETile> up_tiles;
+  std::vector<int64_t> up_toff;
+  int64_t partial_slots = 0;
+};
+
+// Which points play the leaf sources and the leaf targets, and the lists.
+// The matvec: sources = leaf source entries, targets = sorted targets, lists
+// U, V, W, X.  Its transpose: sources = sorted targets, targets = entries,
+// lists inverted (U^-1, V^-1, and X^-1 in the role of W, W^-1 in that of X).
+struct TaskRoles {
+  int64_t regionA = 0;                       // leaf source points in the unified array
+  const std::vector<int64_t>* src_range = nullptr;  // per node: first leaf source (N + 1)
+  const std::vector<int64_t>* tgt_range = nullptr;  // per node: first leaf target (N + 1)
+  const std::vector<uint8_t>* src_leaf = nullptr;   // leaves whose up-equivalent density is formed
+  const std::vector<uint8_t>* tgt_leaf = nullptr;   // leaves with a leaf stage
+  const Csr *U = nullptr, *V = nullptr, *W = nullptr, *X = nullptr;
+};
+
 class Fmm {
  public:
   Fmm(nnk_ctx* ctx, const HostTree* tree, const FmmParams& p);
@@ -85,6 +114,14 @@ class Fmm {
   void apply(const double* d_in, double* d_out, int layout, int nrhs);
   // Same with explicit per-row placement of the input and output vectors.
   void apply_mapped(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int nrhs);
+  // The exact transpose of apply: in at the targets, out at the potentials.
+  void apply_adjoint(const double* d_in, double* d_out, int layout, int nrhs);
+  void apply_adjoint_mapped(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int nrhs);
+  // Gradient of <w, apply(f)> with respect to the positions: at the targets
+  // (n_tgt x 3, target order) and at the sources (potential rows in plain
+  // mode, fine points in NEAREST mode; n x 3).  Either output may be null.
+  void grad_positions(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs);
+  int64_t source_origins() const;
   // Same, but over the p=4 surfaces (computeVelSparse).
   Fmm& sparse();
   void reduced_apply(const double* d_in, double* d_out, int layout);
@@ -102,15 +139,24 @@ class Fmm {
  private:
   template <typename Real>
   void apply_impl(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int k0, int R);
+  template <typename Real>
+  void adjoint_impl(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int k0, int R);
+  // upward and downward passes of one direction (everything before the leaf stage)
+  template <typename Real>
+  void far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R);
+  template <typename Real>
+  void grad_impl(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs);
+  void build_adjoint();
+  void build_taskset(TaskSet& ts, const TaskRoles& roles, bool stats);
   void build_points();
   void build_tasks();
   void assign_operators();
   void build_operators();
   void build_reduced();
-  void split_tasks(std::vector<TaskD>& tasks, std::vector<SegD>& segs);
+  void split_tasks(TaskSet& ts, std::vector<TaskD>& tasks, std::vector<SegD>& segs);
   template <typename Real>
-  void run_group(const TaskGroup& g, const Real* spos, const Real* sstr, const Real* tpos, Real* out, Real e2,
-                 Real scale, int accumulate, int phase_id, int R);
+  void run_group(const TaskSet& ts, const TaskGroup& g, const Real* spos, const Real* sstr, const Real* tpos,
+                 Real* out, Real e2, Real scale, int accumulate, int phase_id, int R);
   void build_c2e_tiles(const std::vector<int32_t>& nodes, const std::vector<int64_t>& off,
                        std::vector<C2ETile>& tiles, std::vector<int64_t>& toff);
 
@@ -138,25 +184,17 @@ class Fmm {
   DBuf<int64_t> goff_;
   DBuf<int32_t> gidx_;
   DBuf<double> gw_;
-  // tasks
-  DBuf<TaskD> tasks_;
-  DBuf<SegD> segs_;
-  DBuf<RedD> reds_;
+  // tasks of the matvec; down_nov groups leave the V-list to the M2L kernels
+  TaskSet fwd_;
   DBuf<double> partial64_;
   DBuf<float> partial32_;
-  std::vector<TaskGroup> up_, down_;  // per level
-  std::vector<TaskGroup> down_nov_;   // per level, without the V-list (M2L on the tensor cores)
   M2LPlan m2l_;
   bool tensor_m2l_ = false;
   FftM2L fft_;
   bool fft_m2l_ = false;
-  TaskGroup leaf_;
   DBuf<int32_t> lvl_nodes_;
   DBuf<int32_t> roots_;
   std::vector<int64_t> lvl_off_;
-  std::vector<int32_t> up_nodes_host_;  // per level: nodes whose uppot is computed
-  DBuf<int32_t> up_nodes_;
-  std::vector<int64_t> up_off_;
   // operators: per (tree, level), uppot = A * check (A = K_up^-1 or its
   // Tikhonov form), downpot = A^T * check.  A depends only on the box width,
   // so trees and levels of equal width share one operator.
@@ -164,8 +202,26 @@ class Fmm {
   int nops_ = 0;
   std::vector<double> op_w_;          // box width of each operator
   std::vector<int> op_of_;            // (group * (maxl + 1) + level) -> operator
-  DBuf<C2ETile> up_tiles_, dn_tiles_;  // per level, tiles of nodes sharing an operator
-  std::vector<int64_t> up_toff_, dn_toff_;
+  DBuf<C2ETile> dn_tiles_;  // per level, tiles of nodes sharing an operator
+  std::vector<int64_t> dn_toff_;
+  // transpose (built on first use): tasks with inverted lists, unified
+  // points [sorted targets | surfaces], identity gather of the targets and
+  // the entry -> potential-row sums of the scatter
+  bool adj_ready_ = false;
+  bool v_symmetric_ = false;
+  TaskSet adj_;
+  Csr inv_U_, inv_V_, inv_W_, inv_X_;
+  DBuf<double> apos64_, astr64_, avel64_;
+  DBuf<float> apos32_, astr32_, avel32_;
+  DBuf<int64_t> agoff_;
+  DBuf<int32_t> agidx_;
+  DBuf<double> agw_;
+  DBuf<int64_t> row_off_;   // per potential row: its (entry, weight) pairs
+  DBuf<int64_t> row_ent_;
+  DBuf<double> row_w_;
+  DBuf<int64_t> org_off_;   // per source origin: its entries
+  DBuf<int64_t> org_ent_;
+  int64_t norigin_ = 0;
   // work buffers
   DBuf<double> check64_, vel64_;
   DBuf<float> check32_, vel32_;

@@ -241,14 +241,20 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
 // carries R force vectors, str[(j * R + k) * 3 + c]; outputs are stored the
 // same way.  One target per thread; below BS targets, threads split the
 // sources and reduce through shared memory.
-template <typename Real, int BS, int R>
+//
+// GRAD (R = 1): instead of the velocity, the gradient with respect to the
+// target position of w_t . u(t), w_t a weight vector per target (tw, indexed
+// like tpos):  d/dt [w . K(t - s) f] =
+//   [2 (w.f) r + (r.f) w + (w.r) f] / D^{3/2} - 3 [(w.f)(r^2 + 2 eps^2) + (w.r)(r.f)] r / D^{5/2},
+// r = t - s, D = r^2 + eps^2 (the derivative of Tools/kernel.m:23-47).
+template <typename Real, int BS, int R, bool GRAD = false>
 __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__ tasks,
                                                        const SegD* __restrict__ segs,
                                                        const Real* __restrict__ spos,
                                                        const Real* __restrict__ sstr,
                                                        const Real* __restrict__ tpos, Real* __restrict__ out_main,
                                                        Real* __restrict__ partial, Real e2, Real scale,
-                                                       int accumulate_main) {
+                                                       int accumulate_main, const Real* __restrict__ tw = nullptr) {
   using T4 = typename Vec4T<Real>::t4;
   constexpr int C = 3 * R;
   __shared__ T4 sp[BS];
@@ -265,8 +271,14 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
     const int splits = max(1, BS / nt);
     const int mt = tid % nt, ms = tid / nt;
     const bool act = ms < splits;
-    Real tx = 0, ty = 0, tz = 0;
+    Real tx = 0, ty = 0, tz = 0, wx = 0, wy = 0, wz = 0;
     if (act) ldpos(tpos, tk.tgt + t0 + mt, tx, ty, tz);
+    if (GRAD && act) {
+      const long long q = 3 * (tk.tgt + t0 + mt);
+      wx = tw[q];
+      wy = tw[q + 1];
+      wz = tw[q + 2];
+    }
     Real acc[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) acc[c] = 0;
@@ -317,7 +329,27 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
         __syncthreads();
         if (f0 + BS + tid < total) fetch(f0 + BS + tid, pa, pb);
         const int nj = min(BS, total - f0);
-        if (act) {
+        if (GRAD && act) {
+#pragma unroll 2
+          for (int j = ms; j < nj; j += splits) {
+            const T4 q = sp[j];
+            const Real dx = tx - q.x, dy = ty - q.y, dz = tz - q.z;
+            const Real d = dx * dx + dy * dy + dz * dz + e2;
+            const Real inv = rsq(d);
+            const Real inv2 = inv * inv;
+            const Real inv3 = inv2 * inv;
+            const Real inv5 = inv3 * inv2;
+            const Real fx = sf[j][0], fy = sf[j][1], fz = sf[j][2];
+            const Real wf = wx * fx + wy * fy + wz * fz;
+            const Real rf = dx * fx + dy * fy + dz * fz;
+            const Real wr = wx * dx + wy * dy + wz * dz;
+            const Real a = 2 * wf * inv3 - 3 * (wf * (d + e2) + wr * rf) * inv5;
+            const Real b = rf * inv3, c = wr * inv3;
+            acc[0] += a * dx + b * wx + c * fx;
+            acc[1] += a * dy + b * wy + c * fy;
+            acc[2] += a * dz + b * wz + c * fz;
+          }
+        } else if (act) {
 #pragma unroll 2
           for (int j = ms; j < nj; j += splits) {
             const T4 q = sp[j];
@@ -383,6 +415,17 @@ inline void launch_p2p(const TaskD* tasks, int ntasks, const SegD* segs, const R
     default:
       throw Error(NNK_E_ARG, "pair kernel supports 1, 2, 3, 4 or 6 right-hand sides per launch");
   }
+  NNK_CHECK_LAUNCH();
+}
+
+// Gradient pair sums (GRAD form of p2p_multi_kernel, one right-hand side).
+template <typename Real>
+inline void launch_p2p_grad(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
+                            const Real* tpos, const Real* tw, Real* out, Real* partial, Real e2, Real scale,
+                            cudaStream_t st) {
+  if (ntasks == 0) return;
+  p2p_multi_kernel<Real, 128, 1, true><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2,
+                                                                scale, 0, tw);
   NNK_CHECK_LAUNCH();
 }
 
@@ -529,6 +572,51 @@ __global__ void scatter_kernel(long long nt, const int* __restrict__ row, const 
     o[cs] = (double)v[1];
     o[2 * cs] = (double)v[2];
   }
+}
+
+// Transpose of the gather: out(row) = sum over the (entry, weight) pairs of
+// the potential row of w * vel(entry), right-hand sides k0..k0+R-1.
+template <typename Real>
+__global__ void scatter_sum_kernel(long long nrows, const long long* __restrict__ row_off,
+                                   const long long* __restrict__ row_ent, const double* __restrict__ row_w,
+                                   const Real* __restrict__ vel, IoMap m, int k0, int R, double* __restrict__ out) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrows) return;
+  long long off, cs, rs;
+  io_index(m, r, off, cs, rs);
+  for (int k = 0; k < R; ++k) {
+    double x = 0, y = 0, z = 0;
+    for (long long q = row_off[r]; q < row_off[r + 1]; ++q) {
+      const Real* v = vel + 3 * (row_ent[q] * R + k);
+      const double w = row_w[q];
+      x += w * (double)v[0];
+      y += w * (double)v[1];
+      z += w * (double)v[2];
+    }
+    double* o = out + off + (k0 + k) * rs;
+    o[0] = x;
+    o[cs] = y;
+    o[2 * cs] = z;
+  }
+}
+
+// out[3 o + c] = sum of vel over the entries of origin o (one right-hand side)
+template <typename Real>
+__global__ void origin_sum_kernel(long long norg, const long long* __restrict__ org_off,
+                                  const long long* __restrict__ org_ent, const Real* __restrict__ vel,
+                                  double* __restrict__ out) {
+  const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= norg) return;
+  double x = 0, y = 0, z = 0;
+  for (long long q = org_off[o]; q < org_off[o + 1]; ++q) {
+    const Real* v = vel + 3 * org_ent[q];
+    x += (double)v[0];
+    y += (double)v[1];
+    z += (double)v[2];
+  }
+  out[3 * o] = x;
+  out[3 * o + 1] = y;
+  out[3 * o + 2] = z;
 }
 
 template <typename Real>

@@ -191,6 +191,8 @@ Mobility::Mobility(Fmm* fmm, int nbodies, const int64_t* body_start, const int64
       throw Error(NNK_E_ARG, "singular body block in B*B' or BT'*BT (empty body?)");
   }
   cudaStream_t st = ctx_->stream;
+  hbody_ = body;
+  if (t.params.nearest && fine_start) fstart_.assign(fine_start, fine_start + nb_ + 1);
   body_of_.upload(body, st);
   bstart_d_.upload(bstart_, st);
   xrel_.upload(xrel, st);
@@ -287,35 +289,129 @@ void Mobility::precon(const double* x, double* y) {
 
 void Mobility::solve(const double* rhs, double* x, const nnk_solve_params& sp, bool precondition,
                      nnk_solve_info& info) {
-  const int64_t n = size();
   if (ref64_) {
-    // x = 0, r = b; repeat: A_mixed d ~= r (GMRES), x += d, r = b - A_fp64 x
-    DBuf<double> r(n), d(n), ax(n), scratch(1);
-    NNK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), ctx_->stream));
-    NNK_CUDA(cudaMemcpyAsync(r.p, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx_->stream));
-    const double nb = std::sqrt(dev_dot(ctx_, rhs, rhs, n, scratch));
-    const double tol = sp.tol > 0 ? sp.tol : 1e-6;
-    info = nnk_solve_info{0, 0, 0.0};
-    if (nb == 0.0) return;
-    double relres = 1.0;
-    for (int outer = 0; outer < ref_outer_; ++outer) {
-      nnk_solve_params in = sp;
-      const double target = tol / relres;  // inner tolerance relative to ||r||
-      in.tol = std::max(ref_inner_tol_, std::min(0.5, target));
-      nnk_solve_info ii{};
-      solve_plain(r.p, d.p, in, precondition, ii);
-      info.iters += ii.iters;
-      dev_axpby(ctx_, 1.0, x, 1.0, d.p, x, n);
-      apply_with(ref64_, x, ax.p);
-      dev_axpby(ctx_, 1.0, rhs, -1.0, ax.p, r.p, n);
-      relres = std::sqrt(dev_dot(ctx_, r.p, r.p, n, scratch)) / nb;
-      if (relres <= tol) break;
-    }
-    info.relres = relres;
-    info.flag = relres <= tol ? 0 : 1;
+    refine(false, rhs, x, sp, precondition, info);
     return;
   }
   solve_plain(rhs, x, sp, precondition, info);
+}
+
+void Mobility::solve_adjoint(const double* rhs, double* x, const nnk_solve_params& sp, nnk_solve_info& info) {
+  if (ref64_) {
+    refine(true, rhs, x, sp, false, info);
+    return;
+  }
+  Gmres g(ctx_, size());
+  Gmres::Op op = [&](const double* in, double* out) { apply_adjoint(in, out); };
+  g.solve(op, nullptr, rhs, x, sp, info);
+}
+
+// x = 0, r = b; repeat: A_mixed d ~= r (GMRES), x += d, r = b - A_fp64 x
+// (A^T for the adjoint)
+void Mobility::refine(bool adjoint, const double* rhs, double* x, const nnk_solve_params& sp, bool precondition,
+                      nnk_solve_info& info) {
+  const int64_t n = size();
+  DBuf<double> r(n), d(n), ax(n), scratch(1);
+  NNK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), ctx_->stream));
+  NNK_CUDA(cudaMemcpyAsync(r.p, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx_->stream));
+  const double nb = std::sqrt(dev_dot(ctx_, rhs, rhs, n, scratch));
+  const double tol = sp.tol > 0 ? sp.tol : 1e-6;
+  info = nnk_solve_info{0, 0, 0.0};
+  if (nb == 0.0) return;
+  double relres = 1.0;
+  for (int outer = 0; outer < ref_outer_; ++outer) {
+    nnk_solve_params in = sp;
+    const double target = tol / relres;  // inner tolerance relative to ||r||
+    in.tol = std::max(ref_inner_tol_, std::min(0.5, target));
+    nnk_solve_info ii{};
+    if (adjoint) {
+      Gmres g(ctx_, n);
+      Gmres::Op op = [&](const double* a, double* b) { apply_adjoint(a, b); };
+      g.solve(op, nullptr, r.p, d.p, in, ii);
+    } else {
+      solve_plain(r.p, d.p, in, precondition, ii);
+    }
+    info.iters += ii.iters;
+    dev_axpby(ctx_, 1.0, x, 1.0, d.p, x, n);
+    if (adjoint) apply_adjoint_with(ref64_, x, ax.p);
+    else apply_with(ref64_, x, ax.p);
+    dev_axpby(ctx_, 1.0, rhs, -1.0, ax.p, r.p, n);
+    relres = std::sqrt(dev_dot(ctx_, r.p, r.p, n, scratch)) / nb;
+    if (relres <= tol) break;
+  }
+  info.relres = relres;
+  info.flag = relres <= tol ? 0 : 1;
+}
+
+void Mobility::apply_adjoint(const double* x, double* y) { apply_adjoint_with(fmm_, x, y); }
+
+void Mobility::apply_adjoint_with(Fmm* f, const double* x, double* y) {
+  // y_f = F^T x_f + B^T x_UOm ; y_UOm = BT^T x_f
+  f->apply_adjoint(x, y, NNK_LAYOUT_BLOCKED, 1);
+  if (nb_ > 0) {
+    body_sums_t(x + 3 * N_, y, 1.0);
+    btt_apply(x, y + 3 * N_);
+  }
+}
+
+void Mobility::grad_positions(const double* z, const double* lam, double* gX, double* gY) {
+  cudaStream_t st = ctx_->stream;
+  const HostTree& t = fmm_->tree();
+  const int64_t Q = fmm_->source_origins();
+  DBuf<double> J(3 * N_), H(3 * std::max<int64_t>(Q, 1));
+  // the FMM block: d/dX <lam_f, F f> and d/dY <lam_f, F f>
+  fmm_->grad_positions(z, lam, NNK_LAYOUT_BLOCKED, J.p, t.params.nearest ? H.p : nullptr);
+  const int64_t n = size();
+  std::vector<double> hz(n), hl(n), hJ(3 * N_), hH(t.params.nearest ? 3 * Q : 0);
+  NNK_CUDA(cudaMemcpyAsync(hz.data(), z, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  NNK_CUDA(cudaMemcpyAsync(hl.data(), lam, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  NNK_CUDA(cudaMemcpyAsync(hJ.data(), J.p, 3 * N_ * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (!hH.empty()) NNK_CUDA(cudaMemcpyAsync(hH.data(), H.p, hH.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  NNK_CUDA(cudaStreamSynchronize(st));
+  auto fvec = [&](const std::vector<double>& v, int64_t i, double* o) {
+    for (int k = 0; k < 3; ++k) o[k] = v[k * N_ + i];
+  };
+  auto cross = [](const double* a, const double* b, double* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  // dL/dX_n = -(J_n + Om_b x lam_n): BT carries xrel = X - x0
+  std::vector<double> gx(3 * N_);
+  for (int64_t i = 0; i < N_; ++i) {
+    double add[3] = {0, 0, 0};
+    const int b = hbody_[i];
+    if (b >= 0) {
+      const double Om[3] = {hz[3 * N_ + 3 * nb_ + b], hz[3 * N_ + 4 * nb_ + b], hz[3 * N_ + 5 * nb_ + b]};
+      double l[3];
+      fvec(hl, i, l);
+      cross(Om, l, add);
+    }
+    for (int k = 0; k < 3; ++k) gx[3 * i + k] = -(hJ[3 * i + k] + add[k]);
+  }
+  NNK_CUDA(cudaMemcpyAsync(gX, gx.data(), gx.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (gY && t.params.nearest) {
+    // dL/dY_q = -(H_q + sum_n NN(q,n) f_n x lam_M,b): B's torque arm is sum_q NN(q,n) (Y_q - x0)
+    std::vector<double> gy(3 * Q);
+    for (int64_t q = 0; q < Q; ++q) {
+      double add[3] = {0, 0, 0};
+      const bool body_row = !fstart_.empty() && q < fstart_[nb_];
+      if (body_row)
+        for (int64_t k = t.nn_rowptr[q]; k < t.nn_rowptr[q + 1]; ++k) {
+          const int64_t c = t.nn_col[k];
+          const int b = c < N_ ? hbody_[c] : -1;
+          if (b < 0) continue;
+          double f[3], c3[3];
+          fvec(hz, c, f);
+          const double lM[3] = {hl[3 * N_ + 3 * nb_ + b], hl[3 * N_ + 4 * nb_ + b], hl[3 * N_ + 5 * nb_ + b]};
+          cross(f, lM, c3);
+          for (int d = 0; d < 3; ++d) add[d] += t.nn_val[k] * c3[d];
+        }
+      for (int d = 0; d < 3; ++d) gy[3 * q + d] = -(hH[3 * q + d] + add[d]);
+    }
+    NNK_CUDA(cudaMemcpyAsync(gY, gy.data(), gy.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  NNK_CUDA(cudaStreamSynchronize(st));
 }
 
 void Mobility::solve_plain(const double* rhs, double* x, const nnk_solve_params& sp, bool precondition,

@@ -19,6 +19,15 @@ class Mobility {
   int64_t size() const { return 3 * N_ + 6 * (int64_t)nb_; }
   void apply(const double* x, double* y);   // mobilityMatrixMulti.m:17-36
   void apply_with(Fmm* f, const double* x, double* y);
+  // A^T = [F^T B^T; BT^T 0], F the FMM block (exact transpose of the passes)
+  void apply_adjoint(const double* x, double* y);
+  void apply_adjoint_with(Fmm* f, const double* x, double* y);
+  // GMRES on A^T (the adjoint solve of a gradient), refined like solve
+  void solve_adjoint(const double* rhs, double* x, const nnk_solve_params& sp, nnk_solve_info& info);
+  // -lam^T (dA/dpositions) z: gX (N x 3, force points), gY (Q x 3, fine
+  // points in NEAREST mode, else null), device pointers; z the solution of
+  // A z = b and lam that of A^T lam = dL/dz.
+  void grad_positions(const double* z, const double* lam, double* gX, double* gY);
   void precon(const double* x, double* y);  // MobilityPrecon.m:17-40
   void solve(const double* rhs, double* x, const nnk_solve_params& sp, bool precondition, nnk_solve_info& info);
   // Mixed-precision iterative refinement: inner GMRES on this (mixed) FMM,
@@ -26,6 +35,8 @@ class Mobility {
   void set_refinement(Fmm* fp64, int max_outer, double inner_tol);
   void solve_plain(const double* rhs, double* x, const nnk_solve_params& sp, bool precondition,
                    nnk_solve_info& info);
+  void refine(bool adjoint, const double* rhs, double* x, const nnk_solve_params& sp, bool precondition,
+              nnk_solve_info& info);
   DBuf<double> io_in, io_out;
 
  private:
@@ -49,6 +60,8 @@ class Mobility {
   DBuf<double> xm_;         // per point torque arm: sum_q NN(q,n) X_q (NEAREST) or xrel (genMatrixComponets.m:217-222)
   DBuf<double> af_;         // per point force weight: column sum of NN (NEAREST) or 1 (:208-209, :228)
   std::vector<double> a1inv_, a2inv_;  // per body 6x6 inverses of B B^T and BT^T BT
+  std::vector<int32_t> hbody_;         // per point: body or -1 (host copy)
+  std::vector<int64_t> fstart_;        // per body: first fine row (NEAREST)
   DBuf<double> t6a_, t6b_, tv_, tv2_, tv3_;
   std::vector<double> h6a_, h6b_;
 };

@@ -427,6 +427,7 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
   t.src_goff.assign(1, 0);
   t.src_gidx.clear();
   t.src_gw.clear();
+  t.src_origin.clear();
   if (!p.nearest) {
     // plain: potential points of each leaf (upwardPass.m:299-317)
     for (int32_t i = 0; i < N; ++i) {
@@ -438,6 +439,7 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
         t.src_pos.insert(t.src_pos.end(), &t.pts[3 * pt], &t.pts[3 * pt] + 3);
         t.src_gidx.push_back((int32_t)t.pot_rank[pt]);
         t.src_gw.push_back(1.0);
+        t.src_origin.push_back(t.pot_rank[pt]);
         t.src_goff.push_back((int64_t)t.src_gidx.size());
       }
     }
@@ -469,6 +471,7 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
         if (k == cnt[i] || trip[k].q != trip[k - 1].q) {
           if (k != cnt[i]) t.src_goff.push_back((int64_t)t.src_gidx.size());
           t.src_pos.insert(t.src_pos.end(), &t.fine[3 * trip[k].q], &t.fine[3 * trip[k].q] + 3);
+          t.src_origin.push_back(trip[k].q);
           ++e;
         }
         t.src_gidx.push_back((int32_t)t.pot_rank[trip[k].col]);
@@ -627,6 +630,7 @@ void merge_forest(const std::vector<const HostTree*>& trees, HostTree& f) {
     f.src_pos.insert(f.src_pos.end(), t.src_pos.begin(), t.src_pos.end());
     for (size_t e = 1; e < t.src_goff.size(); ++e) f.src_goff.push_back(G + t.src_goff[e]);
     for (int32_t r : t.src_gidx) f.src_gidx.push_back((int32_t)(r + npot));
+    for (int64_t o : t.src_origin) f.src_origin.push_back(o + (t.params.nearest ? f.q : npot));
     f.src_gw.insert(f.src_gw.end(), t.src_gw.begin(), t.src_gw.end());
     for (int32_t r : t.tgt_row) f.tgt_row.push_back((int32_t)(r + ntgt));
     f.tgt_pos.insert(f.tgt_pos.end(), t.tgt_pos.begin(), t.tgt_pos.end());
@@ -637,6 +641,7 @@ void merge_forest(const std::vector<const HostTree*>& trees, HostTree& f) {
     npot += t.n_pot;
     ntgt += t.n_tgt;
     f.n += t.n;
+    f.q += t.q;
   }
   if (npot > INT32_MAX || ntgt > INT32_MAX) throw Error(NNK_E_ARG, "forest too large for 32-bit rows");
   f.n_pot = npot;

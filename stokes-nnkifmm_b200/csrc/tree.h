@@ -68,6 +68,7 @@ struct HostTree {
   std::vector<int64_t> src_goff;    // E+1
   std::vector<int32_t> src_gidx;    // potential row
   std::vector<double> src_gw;       // weight
+  std::vector<int64_t> src_origin;  // per entry: fine point (NEAREST) or potential row (plain)
   // ---- leaf targets (sorted by leaf)
   std::vector<int64_t> tgt_start;   // per node, size nodes+1
   std::vector<int32_t> tgt_row;     // output row per sorted target

@@ -85,6 +85,9 @@ SIGNATURES = {
     "nnk_fmm_reduced_solve": (_i32, [_vp, _vp, _vp, _i32, _i32]),
     "nnk_fmm_stats_get": (_i32, [_vp, C.POINTER(FmmStats)]),
     "nnk_fmm_destroy": (_i32, [_vp]),
+    "nnk_fmm_apply_adjoint": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32]),
+    "nnk_fmm_source_count": (_i32, [_vp, _pi64]),
+    "nnk_fmm_grad_positions": (_i32, [_vp, _vp, _vp, _i32, _vp, _vp, _i32]),
     "nnk_fmm_profile": (_i32, [_vp, _i32]),
     "nnk_fmm_profile_read": (_i32, [_vp, _vp, _vp]),
     "nnk_fmm_solve": (_i32, [_vp, _vp, _vp, _i32, C.POINTER(SolveParams), C.POINTER(SolveInfo), _i32]),
@@ -93,6 +96,10 @@ SIGNATURES = {
     "nnk_mob_precon": (_i32, [_vp, _vp, _vp, _i32]),
     "nnk_mob_solve": (_i32, [_vp, _vp, _vp, C.POINTER(SolveParams), _i32, C.POINTER(SolveInfo), _i32]),
     "nnk_mob_set_refinement": (_i32, [_vp, _vp, _i32, _f64]),
+    "nnk_mob_apply_adjoint": (_i32, [_vp, _vp, _vp, _i32]),
+    "nnk_mob_apply_fmm": (_i32, [_vp, _vp, _vp, _vp, _i32]),
+    "nnk_mob_solve_adjoint": (_i32, [_vp, _vp, _vp, C.POINTER(SolveParams), C.POINTER(SolveInfo), _i32]),
+    "nnk_mob_grad_positions": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32]),
     "nnk_mob_destroy": (_i32, [_vp]),
     "nnk_batch_create": (_i32, [_vp, _i32, _vp, _vp, _vp, C.POINTER(FmmParams), _i32, C.POINTER(_vp)]),
     "nnk_batch_layout": (_i32, [_vp, _pi64, _vp]),

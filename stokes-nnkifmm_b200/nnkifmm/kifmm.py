@@ -85,6 +85,32 @@ class KIFMM:
         i = self.tree.info
         return self._call(L.lib.nnk_fmm_apply, potentials, i.num_potentials, i.num_targets, nrhs)
 
+    def computeVelAdjoint(self, velocities, nrhs=1):
+        """The exact transpose of computeVel: velocity-space input at the
+        targets, potential-space output (<y, A x> = <A^T y, x>)."""
+        i = self.tree.info
+        return self._call(L.lib.nnk_fmm_apply_adjoint, velocities, i.num_targets, i.num_potentials, nrhs)
+
+    def sourceCount(self):
+        c = C.c_int64()
+        L.check(L.lib.nnk_fmm_source_count(self.h, C.byref(c)))
+        return c.value
+
+    def gradPositions(self, forces, weights):
+        """Gradient of <weights, computeVel(forces)> with respect to the target
+        positions (n_tgt x 3) and the source positions (fine points in NEAREST
+        mode, else the potentials; n x 3).  Host arrays in the KIFMM format."""
+        i = self.tree.info
+        f = np.ascontiguousarray(np.asarray(forces, np.float64).ravel())
+        w = np.ascontiguousarray(np.asarray(weights, np.float64).ravel())
+        if f.size != 3 * i.num_potentials or w.size != 3 * i.num_targets:
+            raise ValueError("forces must hold 3 n_pot values and weights 3 n_tgt")
+        gt = np.empty((i.num_targets, 3))
+        gs = np.empty((self.sourceCount(), 3))
+        L.check(L.lib.nnk_fmm_grad_positions(self.h, L.ptr(f), L.ptr(w), self._layout(), L.ptr(gt), L.ptr(gs), 0),
+                self.ctx.h, "gradPositions")
+        return gt, gs
+
     def computeVelSparse(self, potentials, nrhs=1):
         """KIFMM.computeVelSparse (KIFMM.m:107-155): coronaRes 4."""
         i = self.tree.info

@@ -210,6 +210,40 @@ class Mobility:
         L.check(L.lib.nnk_mob_apply(self.h, L.ptr(x), L.ptr(y), 0), self.ctx.h, "mobilityMatrixMulti")
         return y
 
+    def apply_adjoint(self, x):
+        """A^T x (the transpose of mobilityMatrixMulti)."""
+        x = self._vec(x)
+        y = np.empty(self.n)
+        L.check(L.lib.nnk_mob_apply_adjoint(self.h, L.ptr(x), L.ptr(y), 0), self.ctx.h, "adjoint")
+        return y
+
+    def apply_with(self, fmm, x):
+        """The matvec with another KIFMM on the same tree."""
+        x = self._vec(x)
+        y = np.empty(self.n)
+        L.check(L.lib.nnk_mob_apply_fmm(self.h, fmm.h, L.ptr(x), L.ptr(y), 0), self.ctx.h, "apply_with")
+        return y
+
+    def solve_adjoint(self, rhs, tol=1e-6, maxIter=None, restart=0):
+        rhs = self._vec(rhs)
+        x = np.empty(self.n)
+        sp_ = L.SolveParams(float(tol), int(maxIter if maxIter else min(self.n, 10)), int(restart))
+        info = L.SolveInfo()
+        rc = L.lib.nnk_mob_solve_adjoint(self.h, L.ptr(rhs), L.ptr(x), C.byref(sp_), C.byref(info), 0)
+        if rc not in (L.NNK_OK, L.NNK_E_NOCONV):
+            L.check(rc, self.ctx.h, "adjoint gmres")
+        return x, info.flag, info.relres, info.iters
+
+    def grad_positions(self, z, lam):
+        """-lam^T (dA/dpositions) z: (N x 3 force points, Q x 3 fine points)."""
+        z, lam = self._vec(z), self._vec(lam)
+        info = self.sw.Tree.info
+        gx = np.empty((info.num_targets, 3))
+        gy = np.empty((max(info.num_fine, 0), 3))
+        L.check(L.lib.nnk_mob_grad_positions(self.h, L.ptr(z), L.ptr(lam), L.ptr(gx),
+                                             L.ptr(gy) if info.num_fine else None, 0), self.ctx.h, "gradient")
+        return gx, gy
+
     def precon(self, x):
         x = self._vec(x)
         y = np.empty(self.n)

@@ -1,0 +1,183 @@
+"""Adjoint FMM, position gradients and the differentiable mobility solve.
+
+* nnk_fmm_apply_adjoint is the exact transpose: <y, A x> = <A^T y, x>;
+* nnk_fmm_grad_positions against central differences of <w, A f>;
+* rigid_velocity's torch gradient (adjoint GMRES + kernel derivative) against
+  the dense FP64 adjoint gradient of the oracle and against central
+  differences of the solve itself."""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import torch
+
+import nnkifmm as nk
+from conftest import GOLDEN
+from nnkifmm.autograd import rigid_velocity
+from nnkifmm.workloads import prolate_spheroid
+from oracle import gradient as og
+
+pytestmark = pytest.mark.gpu
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, name + ".npz"))
+
+
+def tree_of(g, X=None, Y=None):
+    if "coarse" in g:
+        NN = sp.csr_matrix((g["nn_data"], g["nn_indices"], g["nn_indptr"]))
+        X = g["coarse"] if X is None else X
+        return nk.OcTree(X, X, nodeCapacity=int(g["cap"]), finePoints=g["fine"] if Y is None else Y, nearest=1,
+                         NN=NN)
+    if "src" in g:
+        return nk.OcTree(g["src"], g["tgt"], nodeCapacity=int(g["cap"]))
+    return nk.OcTree(g["points"], g["points"], nodeCapacity=int(g["cap"]))
+
+
+@pytest.mark.parametrize("name", ["sphere10_40", "adaptive_plain_1600", "split_1500_700"])
+@pytest.mark.parametrize("precision", ["fp64", "fp64_reg", "mixed"])
+def test_adjoint_is_the_transpose(name, precision):
+    """A wrong transpose is off at O(1); rounding is what remains: the exact
+    LU inverse of the surface matrices (condition ~1e8-1e10) lifts FP64
+    rounding to ~1e-9 of |y| |Ax|, the Tikhonov form keeps it near 1e-12."""
+    g = load(name)
+    t = tree_of(g)
+    kw = dict(precision="fp64" if precision.startswith("fp64") else "mixed")
+    if precision == "fp64_reg":
+        kw["reg"] = 1e-5
+    if precision == "mixed":
+        kw["m2l"] = "fft"
+    fmm = nk.KIFMM(t, [float(g["eps"]), float(g["mu"])], **kw)
+    i = t.info
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(3 * i.num_potentials)
+    y = rng.standard_normal(3 * i.num_targets)
+    Ax = fmm.computeVel(x).ravel()
+    Aty = fmm.computeVelAdjoint(y).ravel()
+    a, b = float(y @ Ax), float(Aty @ x)
+    # relative to the size of the terms summed (|y| |Ax|), not to the inner
+    # product itself, which cancels
+    tol = {"fp64": 1e-8, "fp64_reg": 1e-12, "mixed": 1e-6}[precision]
+    assert abs(a - b) <= tol * np.linalg.norm(y) * np.linalg.norm(Ax), (a, b)
+
+
+def test_adjoint_several_rhs_and_tensor_m2l():
+    g = load("sphere10_40")
+    t = tree_of(g)
+    kp = [float(g["eps"]), float(g["mu"])]
+    i = t.info
+    rng = np.random.default_rng(8)
+    y = rng.standard_normal((3, 3 * i.num_targets))
+    ref = nk.KIFMM(t, kp, precision="mixed", m2l="pairs")
+    for m2l in ["auto", "fft"]:
+        fmm = nk.KIFMM(t, kp, precision="mixed", m2l=m2l)
+        out = fmm.computeVelAdjoint(y.ravel(), nrhs=3)
+        for k in range(3):
+            r = ref.computeVelAdjoint(y[k])
+            tol = 5e-4 if m2l == "auto" else 1e-5  # TF32 operands on the tensor cores
+            assert np.linalg.norm(out[k] - r) <= tol * np.linalg.norm(r)
+
+
+def same_tree(a, b):
+    return a.nodeCount == b.nodeCount and np.array_equal(a.pointIndex, b.pointIndex)
+
+
+def directions(rng, X, Y, h, count, NN=None):
+    """Random directions that change neither the tree structure nor the
+    nearest mapping at +-h (the gradient holds both fixed)."""
+    t0 = nk.OcTree(X, X, nodeCapacity=60)
+    out = []
+    for _ in range(50):
+        if len(out) == count:
+            break
+        dX, dY = rng.standard_normal(X.shape), rng.standard_normal(Y.shape)
+        ok = all(same_tree(t0, nk.OcTree(X + s * h * dX, X + s * h * dX, nodeCapacity=60)) for s in (-1, 1))
+        if ok and NN is not None:
+            ok = all((nk.nearestMatrix(X + s * h * dX, Y + s * h * dY) != NN).nnz == 0 for s in (-1, 1))
+        if ok:
+            out.append((dX, dY))
+    assert len(out) == count, "no direction keeps the tree and the nearest map"
+    return out
+
+
+def test_fmm_position_gradient_vs_finite_differences():
+    """d/dpositions <w, A f> against central differences, on FP64 Tikhonov
+    operators (rounding ~1e-11 instead of ~1e-9 for the exact inverse)."""
+    g = load("sphere10_40")
+    X, Y = g["coarse"], g["fine"]
+    kp = [float(g["eps"]), float(g["mu"])]
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal(3 * len(X))
+    w = rng.standard_normal(3 * len(X))
+
+    def value(Xp, Yp):
+        return float(w @ nk.KIFMM(tree_of(g, Xp, Yp), kp, reg=1e-5).computeVel(f).ravel())
+
+    gt, gs = nk.KIFMM(tree_of(g), kp, reg=1e-5).gradPositions(f, w)
+    h = 1e-6
+    for dX, dY in directions(rng, X, Y, h, 3):
+        fd = (value(X + h * dX, Y + h * dY) - value(X - h * dX, Y - h * dY)) / (2 * h)
+        an = float((gt * dX).sum() + (gs * dY).sum())
+        assert abs(fd - an) <= 1e-4 * abs(an), (fd, an)
+
+
+def body(n_scale=1.0):
+    """A prolate spheroid; the points are jittered so that no quadrature
+    point is equidistant from two force points (the nearest map is then
+    locally constant, as the gradient assumes)."""
+    rng = np.random.default_rng(1)
+    Xb = prolate_spheroid(0.7, 1.4, 0.22 / n_scale)
+    Yb = prolate_spheroid(0.7, 1.4, 0.11 / n_scale)
+    return Xb + 1e-2 * rng.standard_normal(Xb.shape), Yb + 1e-2 * rng.standard_normal(Yb.shape)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_mobility_gradient_vs_dense_oracle(precision):
+    Xb, Yb = body()
+    eps, mu = 0.05, 1.0
+    rng = np.random.default_rng(9)
+    F, M, Us = rng.standard_normal(3), rng.standard_normal(3), rng.standard_normal(6)
+    X = torch.tensor(Xb, requires_grad=True)
+    Y = torch.tensor(Yb, requires_grad=True)
+    e = torch.tensor(eps, dtype=torch.float64, requires_grad=True)
+    U = rigid_velocity(X, Y, e, F, M, mu=mu, cap=60, precision=precision, tol=1e-10 if precision == "fp64" else 1e-8)
+    loss = ((U - torch.tensor(Us)) ** 2).sum()
+    loss.backward()
+    NN = nk.nearestMatrix(Xb, Yb)
+    L, gX, gY, ge = og.gradient(Xb, Yb, NN, eps, mu, F, M, Us)
+    assert abs(float(loss) - L) <= 1e-4 * L
+    tol = 1e-4 if precision == "fp64" else 3e-4
+    assert np.linalg.norm(X.grad.numpy() - gX) <= tol * np.linalg.norm(gX)
+    assert np.linalg.norm(Y.grad.numpy() - gY) <= tol * np.linalg.norm(gY)
+    assert abs(float(e.grad) - ge) <= tol * abs(ge)
+
+
+def test_mobility_gradient_vs_finite_differences():
+    """Central differences of the device solve itself (FP64 Tikhonov
+    operators, GMRES to 1e-11)."""
+    Xb, Yb = body()
+    eps, mu = 0.05, 1.0
+    rng = np.random.default_rng(10)
+    F, M, Us = rng.standard_normal(3), rng.standard_normal(3), rng.standard_normal(6)
+    NN = nk.nearestMatrix(Xb, Yb)
+    opts = dict(mu=mu, tol=1e-11, reg=1e-5)
+
+    def loss(Xp, Yp, ep):
+        U = rigid_velocity(torch.tensor(Xp), torch.tensor(Yp), ep, F, M, **opts)
+        return float(((U - torch.tensor(Us)) ** 2).sum())
+
+    X = torch.tensor(Xb, requires_grad=True)
+    Y = torch.tensor(Yb, requires_grad=True)
+    e = torch.tensor(eps, dtype=torch.float64, requires_grad=True)
+    U = rigid_velocity(X, Y, e, F, M, **opts)
+    ((U - torch.tensor(Us)) ** 2).sum().backward()
+    h = 1e-6
+    for dX, dY in directions(rng, Xb, Yb, h, 2, NN):
+        fd = (loss(Xb + h * dX, Yb + h * dY, eps) - loss(Xb - h * dX, Yb - h * dY, eps)) / (2 * h)
+        an = float((X.grad.numpy() * dX).sum() + (Y.grad.numpy() * dY).sum())
+        assert abs(fd - an) <= 1e-4 * abs(an), (fd, an)
+    he = 1e-6
+    fd = (loss(Xb, Yb, eps + he) - loss(Xb, Yb, eps - he)) / (2 * he)
+    assert abs(fd - float(e.grad)) <= 1e-4 * abs(fd), (fd, float(e.grad))

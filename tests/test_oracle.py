@@ -124,3 +124,29 @@ def test_geometry_generators():
     assert np.allclose(w[:, 2], -1.5) and len(w) > 400
     v = velocity_modes(np.eye(3), [1, 0, 0], [0, 0, 1])
     assert np.allclose(v, [[1, 1, 0], [0, 0, 0], [1, 0, 0]])
+
+
+def test_dense_gradient_matches_finite_differences():
+    """The dense adjoint gradient (oracle/gradient.py) against central
+    differences of the dense loss, on a small body."""
+    from oracle import gradient as og
+    from oracle.geometry import sphere as cube_sphere
+    from oracle.nearest import nearest_matrix
+    rng = np.random.default_rng(4)
+    X = cube_sphere(1.0, (0, 0, 0), 4) * np.array([1.0, 0.8, 1.3])
+    Y = cube_sphere(1.0, (0, 0, 0), 8) * np.array([1.0, 0.8, 1.3])
+    NN = nearest_matrix(X, Y)
+    eps, mu = 0.05, 1.0
+    F, M, Us = rng.standard_normal(3), rng.standard_normal(3), rng.standard_normal(6)
+    L, gX, gY, ge = og.gradient(X, Y, NN, eps, mu, F, M, Us)
+    h = 1e-6
+    for k in range(3):
+        dX, dY = rng.standard_normal(X.shape), rng.standard_normal(Y.shape)
+        lp = og.loss(X + h * dX, Y + h * dY, NN, eps, mu, F, M, Us)
+        lm = og.loss(X - h * dX, Y - h * dY, NN, eps, mu, F, M, Us)
+        fd = (lp - lm) / (2 * h)
+        an = float((gX * dX).sum() + (gY * dY).sum())
+        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)
+    lp = og.loss(X, Y, NN, eps + h, mu, F, M, Us)
+    lm = og.loss(X, Y, NN, eps - h, mu, F, M, Us)
+    assert abs((lp - lm) / (2 * h) - ge) <= 1e-6 * max(1.0, abs(ge))
