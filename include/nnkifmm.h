@@ -214,6 +214,10 @@ int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats);
  * the interaction lists inverted. */
 int nnk_fmm_apply_adjoint(nnk_fmm* fmm, const double* in, double* out, int32_t layout,
                           int32_t nrhs, int32_t on_device);
+/* Rebuild the eps-dependent parts of the FMM (operators, M2L images or
+ * spectra) for kernelPar(1) = eps, keeping the tree-dependent task lists:
+ * the cheap way to evaluate the operator at eps +- d for its eps-derivative. */
+int nnk_fmm_set_eps(nnk_fmm* fmm, double eps);
 /* Number of source origins: fine points (NEAREST) or potential rows. */
 int nnk_fmm_source_count(const nnk_fmm* fmm, int64_t* count);
 /* Gradient of <weights, apply(forces)> with respect to the positions, with

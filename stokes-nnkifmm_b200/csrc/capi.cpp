@@ -302,6 +302,15 @@ int nnk_fmm_apply_adjoint(nnk_fmm* fmm, const double* in, double* out, int32_t l
   API_CATCH(ctx)
 }
 
+int nnk_fmm_set_eps(nnk_fmm* fmm, double eps) {
+  if (!fmm) return NNK_E_ARG;
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  fmm->f->set_eps(eps);
+  API_CATCH(ctx)
+}
+
 int nnk_fmm_source_count(const nnk_fmm* fmm, int64_t* count) {
   if (!fmm || !count) return NNK_E_ARG;
   *count = fmm->f->source_origins();

@@ -865,6 +865,17 @@ void Fmm::apply_adjoint_mapped(const double* d_in, const IoMap& in, double* d_ou
   }
 }
 
+void Fmm::set_eps(double eps) {
+  if (!(eps > 0)) throw Error(NNK_E_ARG, "eps must be > 0");
+  NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
+  p_.eps = eps;
+  tensor_m2l_ = false;
+  fft_m2l_ = false;
+  build_operators();
+  reduced_ready_ = false;
+  sparse_.reset();
+}
+
 int64_t Fmm::source_origins() const { return t_->params.nearest ? t_->q : t_->n_pot; }
 
 void Fmm::grad_positions(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs) {

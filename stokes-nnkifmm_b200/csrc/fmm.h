@@ -122,6 +122,9 @@ class Fmm {
   // mode, fine points in NEAREST mode; n x 3).  Either output may be null.
   void grad_positions(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs);
   int64_t source_origins() const;
+  // Rebuild every eps-dependent part (check-to-equivalent operators, M2L
+  // images or spectra) for a new eps; the tree-dependent task lists stay.
+  void set_eps(double eps);
   // Same, but over the p=4 surfaces (computeVelSparse).
   Fmm& sparse();
   void reduced_apply(const double* d_in, double* d_out, int layout);

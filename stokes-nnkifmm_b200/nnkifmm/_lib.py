@@ -87,6 +87,7 @@ SIGNATURES = {
     "nnk_fmm_destroy": (_i32, [_vp]),
     "nnk_fmm_apply_adjoint": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32]),
     "nnk_fmm_source_count": (_i32, [_vp, _pi64]),
+    "nnk_fmm_set_eps": (_i32, [_vp, _f64]),
     "nnk_fmm_grad_positions": (_i32, [_vp, _vp, _vp, _i32, _vp, _vp, _i32]),
     "nnk_fmm_profile": (_i32, [_vp, _i32]),
     "nnk_fmm_profile_read": (_i32, [_vp, _vp, _vp]),

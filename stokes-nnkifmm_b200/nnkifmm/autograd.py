@@ -59,12 +59,19 @@ class _RigidVelocity(torch.autograd.Function):
         if flag != 0:
             raise RuntimeError(f"adjoint GMRES stopped at relres {relres:.3e} after {it} iterations")
         gX, gY = mob.grad_positions(z, lam)
-        d = 1e-4 * e
-        kw = dict(GMRES=1, format=2, precision="fp64")
-        if opts["precision"] == "mixed" or opts["reg"] > 0:
-            kw["reg"] = opts["reg"] or 1e-5  # the operator the (refined) solution solves
-        Ap = mob.apply_with(KIFMM(sw.Tree, [e + d, opts["mu"]], **kw), z)
-        Am = mob.apply_with(KIFMM(sw.Tree, [e - d, opts["mu"]], **kw), z)
+        # dA/deps z by a central difference of FP64 matvecs on Tikhonov
+        # operators: the exact inverse (condition ~1e10) would put its rounding
+        # into the difference; the regularized FMM differs from it by the FMM
+        # approximation only, smoothly in eps
+        d = 1e-3 * e
+        f64 = getattr(sw, "FMM64", None)
+        if f64 is None:
+            f64 = KIFMM(sw.Tree, [e, opts["mu"]], GMRES=1, format=2, precision="fp64", reg=opts["reg"] or 1e-5)
+        f64.setEps(e + d)
+        Ap = mob.apply_with(f64, z)
+        f64.setEps(e - d)
+        Am = mob.apply_with(f64, z)
+        f64.setEps(e)
         geps = -float(lam @ (Ap - Am)) / (2 * d)
         ctx.grad_info = dict(iters=it, relres=relres)
         X_dtype, dev = gout.dtype, gout.device

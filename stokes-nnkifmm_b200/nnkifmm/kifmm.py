@@ -91,6 +91,11 @@ class KIFMM:
         i = self.tree.info
         return self._call(L.lib.nnk_fmm_apply_adjoint, velocities, i.num_targets, i.num_potentials, nrhs)
 
+    def setEps(self, eps):
+        """Rebuild the eps-dependent operators for a new kernelPar(1)."""
+        L.check(L.lib.nnk_fmm_set_eps(self.h, float(eps)), self.ctx.h, "setEps")
+        self.arguments["kernelPar"] = (float(eps), self.arguments["kernelPar"][1])
+
     def sourceCount(self):
         c = C.c_int64()
         L.check(L.lib.nnk_fmm_source_count(self.h, C.byref(c)))
