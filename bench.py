@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-errors", action="store_true")
     ap.add_argument("--no-solves", action="store_true")
     ap.add_argument("--batch-bodies", type=int, default=4)
+    ap.add_argument("--no-gradient", action="store_true")
+    ap.add_argument("--grad-force", type=int, default=50_000)
     return ap.parse_args()
 
 
@@ -127,6 +129,7 @@ def build(nk, w, precision):
     NN = nk.nearestMatrix(w["coarse"], w["fine"])
     tree = nk.OcTree(w["coarse"], w["coarse"], nodeCapacity=w["cap"], nearest=1, finePoints=w["fine"], NN=NN)
     fmm = nk.KIFMM(tree, [w["eps"], w["mu"]], precision=precision)
+    fmm.autotune(1)  # pair-kernel tile per launch group (part of the set-up)
     return NN, tree, fmm
 
 
@@ -249,6 +252,47 @@ def solve_benchmarks(torch, nk, args):
                     "batched = all bodies x 6 rigid-mode right-hand sides in one forest FMM (multi-RHS pair "
                     "kernels), per-system GMRES advancing in lockstep; fp64_sequential = one body and one "
                     "right-hand side per GMRES call")
+    return out
+
+
+def gradient_benchmark(torch, nk, args):
+    """Differentiation configuration: a prolate spheroid (a = 1, c = 3, about
+    50k force / 200k quadrature points, eps = 0.005) under a unit force in x;
+    loss ||[U; Om] - U*||^2.  Times the forward solve (tree, NN, FMM set-up and
+    GMRES) and the backward pass (adjoint GMRES, position gradients, eps
+    derivative) for mixed (with FP64 refinement) and FP64, and compares the
+    two gradients (their checks against finite differences and the dense
+    oracle run in tests/test_adjoint_gpu.py at sizes where those finish)."""
+    from nnkifmm.autograd import rigid_velocity
+    from nnkifmm.workloads import _spacing_for_count, prolate_spheroid
+    h = _spacing_for_count(1.0, 3.0, args.grad_force)
+    Xb = prolate_spheroid(1.0, 3.0, h)
+    Yb = prolate_spheroid(1.0, 3.0, h / 2)
+    rng = np.random.default_rng(20261208)
+    F, M, Us = np.array([1.0, 0.0, 0.0]), np.zeros(3), rng.standard_normal(6)
+    out = {"workload": f"prolate spheroid a=1 c=3, {len(Xb)} force / {len(Yb)} quadrature points (h/2), "
+                       f"eps=0.005, nodeCapacity 64, F=(1,0,0), GMRES tol 1e-6"}
+    grads = {}
+    for prec in ["mixed", "fp64"]:
+        best = None
+        for _ in range(2):  # the second run has warm caches and libraries
+            X = torch.tensor(Xb, requires_grad=True)
+            Y = torch.tensor(Yb, requires_grad=True)
+            e = torch.tensor(0.005, dtype=torch.float64, requires_grad=True)
+            t0 = time.perf_counter()
+            U = rigid_velocity(X, Y, e, F, M, cap=64, precision=prec, tol=1e-6, maxIter=1000)
+            t1 = time.perf_counter()
+            ((U - torch.tensor(Us)) ** 2).sum().backward()
+            t2 = time.perf_counter()
+            best = (t1 - t0, t2 - t1)
+        grads[prec] = (X.grad.numpy().copy(), Y.grad.numpy().copy(), float(e.grad))
+        out[prec] = {"forward_s": best[0], "backward_s": best[1],
+                     "forward_plus_adjoint_over_forward": (best[0] + best[1]) / best[0]}
+    gm, g6 = grads["mixed"], grads["fp64"]
+    out["mixed_vs_fp64_gradient"] = {
+        "X": float(np.linalg.norm(gm[0] - g6[0]) / np.linalg.norm(g6[0])),
+        "Y": float(np.linalg.norm(gm[1] - g6[1]) / np.linalg.norm(g6[1])),
+        "eps": abs(gm[2] - g6[2]) / abs(g6[2])}
     return out
 
 
@@ -406,6 +450,7 @@ def main():
         ref = sampled_direct(torch, w, NN, idx)
         v = fout.cpu().numpy()
         other = nk.KIFMM(tree, [w["eps"], w["mu"]], precision="fp64" if args.precision == "mixed" else "mixed")
+        other.autotune(1)
         fo = torch.empty_like(fin)
         ms2, _ = time_device(torch, other, fin, fo, max(3, args.steps // 2), 2, flush)
         v2 = fo.cpu().numpy()
@@ -416,6 +461,8 @@ def main():
         line[f"{oth}_gpu"] = {"value": args.n_force / (float(np.mean(ms2)) / 1e3), "ms_per_step": float(np.mean(ms2))}
     if rank == 0 and not args.no_solves:
         line["mobility_solves"] = solve_benchmarks(torch, nk, args)
+    if rank == 0 and not args.no_gradient:
+        line["gradient"] = gradient_benchmark(torch, nk, args)
     if rank == 0 and not args.no_cpu_baseline:
         v, s, nodes = cpu_baseline_sample(1500, 6000)
         line["cpu_baseline"] = {"value": v, "unit": "pts/s", "cores": 1, "kind": "port",

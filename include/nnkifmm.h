@@ -214,6 +214,12 @@ int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats);
  * the interaction lists inverted. */
 int nnk_fmm_apply_adjoint(nnk_fmm* fmm, const double* in, double* out, int32_t layout,
                           int32_t nrhs, int32_t on_device);
+/* Autotuner: times every launch group of the pair kernel (upward and
+ * downward levels, leaf stage) with source tiles of 64, 128 and 256 points
+ * for passes of nrhs right-hand sides and keeps the fastest per group.
+ * ms_before / ms_after (may be NULL): summed pair-kernel time with the
+ * default tiles and with the picked ones. */
+int nnk_fmm_autotune(nnk_fmm* fmm, int32_t nrhs, double* ms_before, double* ms_after);
 /* Rebuild the eps-dependent parts of the FMM (operators, M2L images or
  * spectra) for kernelPar(1) = eps, keeping the tree-dependent task lists:
  * the cheap way to evaluate the operator at eps +- d for its eps-derivative. */
@@ -311,6 +317,9 @@ int nnk_batch_solve(nnk_batch* batch, const double* rhs, double* x,
  * FP64 FMM on the same bodies (same Tikhonov weight) for the outer residuals
  * of nnk_batch_solve, as nnk_mob_set_refinement does. */
 int nnk_batch_set_refinement(nnk_batch* batch, int32_t fp64, int32_t max_outer, double inner_tol);
+/* Replay each matvec from a CUDA graph captured on first use (default on;
+ * off while profiling).  enable = 0 launches the kernels one by one. */
+int nnk_batch_use_graphs(nnk_batch* batch, int32_t enable);
 /* Total FMM matvecs issued so far (inner and outer). */
 int nnk_batch_matvecs(const nnk_batch* batch, int64_t* count);
 /* Per-phase CUDA-event timing of the batch's FMM passes, as

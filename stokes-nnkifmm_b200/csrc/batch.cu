@@ -164,7 +164,7 @@ std::vector<double> SegGmres::norms(const double* v) {
 }
 
 void SegGmres::solve(const Op& op, const double* b, double* x, const std::vector<double>& tol, int maxit,
-                     int restart, const std::vector<char>& want, std::vector<nnk_solve_info>& info) {
+                     int restart, const std::vector<char>& want, std::vector<nnk_solve_info>& info, bool confirm) {
   cudaStream_t st = ctx_->stream;
   const int S = S_;
   const int64_t n = n_;
@@ -323,6 +323,17 @@ void SegGmres::solve(const Op& op, const double* b, double* x, const std::vector
       NNK_CHECK_LAUNCH();
       NNK_CUDA(cudaStreamSynchronize(st));
     }
+    if (!confirm) {
+      // the caller checks the residual itself (iterative refinement): stop
+      // when every segment met tol by the recurrence or ran out of steps
+      bool done = true;
+      for (int s = 0; s < S; ++s) {
+        if (!live[s]) continue;
+        relres[s] = std::fabs(g[(size_t)s * ldh + k_of[s]]) / nb[s];
+        if (relres[s] > tol[s] && info[s].iters < maxit && k_of[s] > 0) done = false;
+      }
+      if (done) break;
+    }
     // explicit residuals r = b - A x (MATLAB gmres confirms convergence this way)
     op(x, w.p);
     ++matvecs_;
@@ -441,12 +452,59 @@ BatchMobility::BatchMobility(nnk_ctx* ctx, const std::vector<BatchBody>& bodies,
   if (q.precision == NNK_PREC_MIXED && q.m2l_mode != 3) q.m2l_mode = 4;
   fp_ = q;
   fmm_.reset(new Fmm(ctx_, &forest_, q));
+  fmm_->autotune(R_);
   NNK_CUDA(cudaStreamSynchronize(st));
 }
 
-BatchMobility::~BatchMobility() = default;
+BatchMobility::~BatchMobility() {
+  for (auto& g : graph_)
+    if (g) cudaGraphExecDestroy(g);
+}
+
+void BatchMobility::use_graphs(bool on) {
+  graphs_on_ = on;
+  for (auto& g : graph_) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+}
 
 void BatchMobility::apply_with(Fmm& f, const double* x, double* y) {
+  ++matvecs_;
+  // the legacy default stream cannot be captured
+  if (!graphs_on_ || f.profiling() || ctx_->stream == nullptr) {
+    apply_raw(f, x, y);
+    return;
+  }
+  cudaStream_t st = ctx_->stream;
+  const int slot = &f == fmm_.get() ? 0 : 1;
+  if (!gin_.p) {
+    gin_.alloc(n_);
+    gout_.alloc(n_);
+  }
+  if (!graph_[slot]) {
+    NNK_CUDA(cudaStreamSynchronize(st));
+    NNK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t g = nullptr;
+    try {
+      apply_raw(f, gin_.p, gout_.p);
+    } catch (...) {
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      throw;
+    }
+    NNK_CUDA(cudaStreamEndCapture(st, &g));
+    const cudaError_t e = cudaGraphInstantiate(&graph_[slot], g, 0);
+    cudaGraphDestroy(g);
+    NNK_CUDA(e);
+  }
+  NNK_CUDA(cudaMemcpyAsync(gin_.p, x, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  NNK_CUDA(cudaGraphLaunch(graph_[slot], st));
+  NNK_CUDA(cudaMemcpyAsync(y, gout_.p, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
+}
+
+void BatchMobility::apply_raw(Fmm& f, const double* x, double* y) {
   cudaStream_t st = ctx_->stream;
   f.apply_mapped(x, io_, y, io_, R_);
   batch_bt_kernel<<<blocks_for(Nt_), 256, 0, st>>>(Nt_, R_, row_body_.p, row_local_.p, sys_off_.p, sys_n_.p,
@@ -454,7 +512,6 @@ void BatchMobility::apply_with(Fmm& f, const double* x, double* y) {
   NNK_CHECK_LAUNCH();
   batch_bsum_kernel<<<S_, 256, 0, st>>>(body_row0_.p, R_, sys_off_.p, sys_n_.p, af_.p, xm_.p, x, y);
   NNK_CHECK_LAUNCH();
-  ++matvecs_;
 }
 
 void BatchMobility::apply(const double* x, double* y) { apply_with(*fmm_, x, y); }
@@ -466,12 +523,13 @@ void BatchMobility::set_refinement(bool fp64, int max_outer, double inner_tol) {
   }
   if (fp_.precision != NNK_PREC_MIXED) throw Error(NNK_E_ARG, "refinement needs a mixed-precision batch");
   ref_outer_ = max_outer > 0 ? max_outer : 12;
-  ref_inner_tol_ = inner_tol > 0 ? inner_tol : 1e-3;
+  ref_inner_tol_ = inner_tol > 0 ? inner_tol : 1e-4;
   if (!ref64_) {
     FmmParams q = fp_;
     q.precision = NNK_PREC_FP64;
     q.reg = fp_.reg > 0 ? fp_.reg : 1e-5;  // the same regularized operators as the mixed FMM
     ref64_.reset(new Fmm(ctx_, &forest_, q));
+    ref64_->autotune(R_);
   }
 }
 
@@ -480,7 +538,7 @@ void BatchMobility::solve_plain(const double* rhs, double* x, const nnk_solve_pa
                                 std::vector<nnk_solve_info>& info) {
   SegGmres g(ctx_, off_);
   SegGmres::Op op = [&](const double* in, double* out) { apply(in, out); };
-  g.solve(op, rhs, x, tol, sp.maxit, sp.restart, act, info);
+  g.solve(op, rhs, x, tol, sp.maxit, sp.restart, act, info, /*confirm=*/!ref64_);
 }
 
 void BatchMobility::solve(const double* rhs, double* x, const nnk_solve_params& sp, nnk_solve_info* info) {

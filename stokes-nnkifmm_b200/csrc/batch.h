@@ -37,8 +37,10 @@ class SegGmres {
   SegGmres(nnk_ctx* ctx, const std::vector<int64_t>& off);
   using Op = std::function<void(const double* in, double* out)>;
   // x = 0 start; segments with solve[s] == 0 get x_s = 0 and no iterations.
+  // confirm = false skips the closing explicit residual (the caller forms it,
+  // as iterative refinement does) and reports the recurrence's estimate.
   void solve(const Op& op, const double* b, double* x, const std::vector<double>& tol, int maxit, int restart,
-             const std::vector<char>& solve, std::vector<nnk_solve_info>& info);
+             const std::vector<char>& solve, std::vector<nnk_solve_info>& info, bool confirm = true);
   int64_t matvecs() const { return matvecs_; }
   std::vector<double> norms(const double* v);  // ||v_s|| per segment
 
@@ -73,10 +75,14 @@ class BatchMobility {
   void set_refinement(bool fp64, int max_outer, double inner_tol);
   Fmm& fmm() { return *fmm_; }
   Fmm* ref64() { return ref64_.get(); }
+  // Replay each FMM's matvec (all bodies, all right-hand sides, B and BT
+  // blocks: about 50 launches) from a CUDA graph captured on first use.
+  void use_graphs(bool on);
   int64_t matvecs() const { return matvecs_; }
 
  private:
   void apply_with(Fmm& f, const double* x, double* y);
+  void apply_raw(Fmm& f, const double* x, double* y);
   void solve_plain(const double* rhs, double* x, const nnk_solve_params& sp, const std::vector<double>& tol,
                    const std::vector<char>& act, std::vector<nnk_solve_info>& info);
 
@@ -89,7 +95,7 @@ class BatchMobility {
   std::unique_ptr<Fmm> fmm_, ref64_;
   FmmParams fp_;
   int ref_outer_ = 0;
-  double ref_inner_tol_ = 1e-3;
+  double ref_inner_tol_ = 1e-4;
   IoMap io_;
   DBuf<long long> io_off_, io_rstr_;
   DBuf<int> io_cstr_;
@@ -99,6 +105,9 @@ class BatchMobility {
   DBuf<int> sys_n_;         // per system: force points of its body
   DBuf<double> xrel_, xm_, af_;  // per force point (forest order)
   DBuf<long long> body_row0_;  // per body: first force point in forest order (B + 1)
+  bool graphs_on_ = true;
+  cudaGraphExec_t graph_[2] = {nullptr, nullptr};  // matvec of fmm_ and of ref64_
+  DBuf<double> gin_, gout_;                        // the captured matvec's input and output
   int64_t matvecs_ = 0;
 };
 

@@ -302,6 +302,17 @@ int nnk_fmm_apply_adjoint(nnk_fmm* fmm, const double* in, double* out, int32_t l
   API_CATCH(ctx)
 }
 
+int nnk_fmm_autotune(nnk_fmm* fmm, int32_t nrhs, double* ms_before, double* ms_after) {
+  if (!fmm || nrhs < 1) return NNK_E_ARG;
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  const auto r = fmm->f->autotune(nrhs);
+  if (ms_before) *ms_before = r.first;
+  if (ms_after) *ms_after = r.second;
+  API_CATCH(ctx)
+}
+
 int nnk_fmm_set_eps(nnk_fmm* fmm, double eps) {
   if (!fmm) return NNK_E_ARG;
   nnk_ctx* ctx = fmm->ctx;
@@ -622,6 +633,15 @@ int nnk_batch_set_refinement(nnk_batch* batch, int32_t fp64, int32_t max_outer, 
   API_TRY
   need_gpu(ctx);
   batch->m->set_refinement(fp64 != 0, max_outer, inner_tol);
+  API_CATCH(ctx)
+}
+
+int nnk_batch_use_graphs(nnk_batch* batch, int32_t enable) {
+  if (!batch) return NNK_E_ARG;
+  nnk_ctx* ctx = batch->ctx;
+  API_TRY
+  need_gpu(ctx);
+  batch->m->use_graphs(enable != 0);
   API_CATCH(ctx)
 }
 

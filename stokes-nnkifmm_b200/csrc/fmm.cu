@@ -7,6 +7,7 @@
 #include <type_traits>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <map>
 
 #include "fmm.h"
@@ -503,7 +504,7 @@ void Fmm::run_group(const TaskSet& ts, const TaskGroup& g, const Real* spos, con
   Real* partial = std::is_same<Real, double>::value ? (Real*)partial64_.p : (Real*)partial32_.p;
   phase(phase_id, [&] {
     launch_p2p<Real>(ts.tasks.p + g.first, (int)g.count, ts.segs.p, spos, sstr, tpos, out, partial, e2, scale, st,
-                     accumulate, R);
+                     accumulate, R, g.bs);
   });
   if (g.red_count)
     phase(phase_id,
@@ -874,6 +875,89 @@ void Fmm::set_eps(double eps) {
   build_operators();
   reduced_ready_ = false;
   sparse_.reset();
+}
+
+namespace {
+template <typename Real>
+double tune_groups(Fmm* self, std::vector<TaskGroup*>& groups, const std::vector<int>& kinds, int R,
+                   const std::function<void(const TaskGroup&, int)>& run, cudaStream_t st, bool pick) {
+  (void)self;
+  (void)kinds;
+  cudaEvent_t a, b;
+  NNK_CUDA(cudaEventCreate(&a));
+  NNK_CUDA(cudaEventCreate(&b));
+  double total = 0;
+  for (TaskGroup* g : groups) {
+    if (g->count == 0) continue;
+    float best = 1e30f;
+    int best_bs = g->bs;
+    const int cand[3] = {64, 128, 256};
+    for (int bs : cand) {
+      if (!pick && bs != g->bs) continue;
+      if (!p2p_bs_ok<Real>(bs, R)) continue;
+      TaskGroup t = *g;
+      t.bs = bs;
+      float ms = 1e30f;
+      for (int rep = 0; rep < 2; ++rep) {
+        NNK_CUDA(cudaEventRecord(a, st));
+        run(t, R);
+        NNK_CUDA(cudaEventRecord(b, st));
+        NNK_CUDA(cudaEventSynchronize(b));
+        float x = 0;
+        NNK_CUDA(cudaEventElapsedTime(&x, a, b));
+        ms = std::min(ms, x);
+      }
+      if (ms < best) {
+        best = ms;
+        best_bs = bs;
+      }
+    }
+    g->bs = best_bs;
+    total += best;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return total;
+}
+}  // namespace
+
+std::pair<double, double> Fmm::autotune(int nrhs) {
+  const HostTree& t = *t_;
+  const int R = rhs_chunk(nrhs, tensor_m2l_ ? 1 : R_);
+  cudaStream_t st = ctx_->stream;
+  // one pass with real data, so the tuned launches see the real sources
+  DBuf<double> in(3 * (size_t)t.n_pot * R), out(3 * (size_t)t.n_tgt * R);
+  in.zero(st);
+  apply(in.p, out.p, NNK_LAYOUT_ROWS, R);
+  std::vector<TaskGroup*> groups;
+  const bool nov = tensor_m2l_ || fft_m2l_;
+  for (auto& g : fwd_.up) groups.push_back(&g);
+  for (auto& g : (nov ? fwd_.down_nov : fwd_.down)) groups.push_back(&g);
+  groups.push_back(&fwd_.leaf);
+  std::pair<double, double> res;
+  auto go = [&](auto tag) {
+    using Real = decltype(tag);
+    Real* str = p_.precision == NNK_PREC_FP64 ? (Real*)str64_.p : (Real*)str32_.p;
+    const Real* pos = p_.precision == NNK_PREC_FP64 ? (const Real*)pos64_.p : (const Real*)pos32_.p;
+    const Real* tpos = p_.precision == NNK_PREC_FP64 ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
+    Real* check = p_.precision == NNK_PREC_FP64 ? (Real*)check64_.p : (Real*)check32_.p;
+    Real* vel = p_.precision == NNK_PREC_FP64 ? (Real*)vel64_.p : (Real*)vel32_.p;
+    const Real e2 = (Real)(p_.eps * p_.eps);
+    const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
+    auto run = [&](const TaskGroup& g, int r) {
+      const bool leaf = &g == &fwd_.leaf || g.first == fwd_.leaf.first;
+      run_group<Real>(fwd_, g, pos, str, leaf ? tpos : pos, leaf ? vel : check, e2, scale, 0,
+                      NNK_PHASE_LEAF_PAIRS, r);
+    };
+    std::vector<int> kinds;
+    res.first = tune_groups<Real>(this, groups, kinds, R, run, st, false);
+    res.second = tune_groups<Real>(this, groups, kinds, R, run, st, true);
+  };
+  if (p_.precision == NNK_PREC_FP64) go(double());
+  else go(float());
+  // the tuned launches overwrote work buffers: nothing to keep
+  NNK_CUDA(cudaStreamSynchronize(st));
+  return res;
 }
 
 int64_t Fmm::source_origins() const { return t_->params.nearest ? t_->q : t_->n_pot; }

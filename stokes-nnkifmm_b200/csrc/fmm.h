@@ -44,6 +44,7 @@ struct SegD {
 struct TaskGroup {
   int64_t first = 0, count = 0;  // range in the task array
   int64_t red_first = 0, red_count = 0;  // reductions of its split tasks
+  int bs = 128;                  // threads per task (source tile), set by the autotuner
 };
 
 struct FmmParams {
@@ -125,6 +126,11 @@ class Fmm {
   // Rebuild every eps-dependent part (check-to-equivalent operators, M2L
   // images or spectra) for a new eps; the tree-dependent task lists stay.
   void set_eps(double eps);
+  // Picks, per launch group of the pair kernel, the block size (source tile
+  // of bs points, target chunk of bs or 2 bs) with the shortest measured
+  // launch, from {64, 128, 256} (FP64: {64, 128}), for passes of nrhs
+  // right-hand sides.  Returns the total pair-kernel time before and after.
+  std::pair<double, double> autotune(int nrhs);
   // Same, but over the p=4 surfaces (computeVelSparse).
   Fmm& sparse();
   void reduced_apply(const double* d_in, double* d_out, int layout);
@@ -132,6 +138,7 @@ class Fmm {
   nnk_fmm_stats stats() const { return stats_; }
   // per-phase CUDA-event timing (NNK_PHASE_*)
   void set_profile(bool on);
+  bool profiling() const { return prof_; }
   void read_profile(double* ms, int64_t* launches);
   const HostTree& tree() const { return *t_; }
   nnk_ctx* ctx() const { return ctx_; }

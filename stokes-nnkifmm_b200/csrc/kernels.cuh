@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "common.h"
 #include "fmm.h"
 
@@ -386,35 +388,81 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
   }
 }
 
-template <typename Real>
-inline void launch_p2p(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
-                       const Real* tpos, Real* out, Real* partial, Real e2, Real scale, cudaStream_t st,
-                       int accumulate = 0, int R = 1) {
-  if (ntasks == 0) return;
+// Static shared memory of p2p_multi_kernel<Real, BS, R> stays under 48 KB.
+template <typename Real, int BS, int R>
+constexpr bool p2p_fits() {
+  return 4 * sizeof(Real) * BS + 2 * 3 * R * sizeof(Real) * BS + 12 * BS <= 48 * 1024;
+}
+
+template <typename Real, int BS, int R>
+inline void launch_multi(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
+                         const Real* tpos, Real* out, Real* partial, Real e2, Real scale, cudaStream_t st,
+                         int accumulate) {
+  if constexpr (p2p_fits<Real, BS, R>()) {
+    p2p_multi_kernel<Real, BS, R><<<ntasks, BS, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
+                                                          accumulate);
+  } else {
+    throw Error(NNK_E_ARG, "pair kernel tile too large for shared memory");
+  }
+}
+
+template <typename Real, int BS>
+inline void launch_p2p_bs(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
+                          const Real* tpos, Real* out, Real* partial, Real e2, Real scale, cudaStream_t st,
+                          int accumulate, int R) {
   switch (R) {
     case 1:
-      p2p_kernel<Real, 128><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
-                                                     accumulate);
+      p2p_kernel<Real, BS><<<ntasks, BS, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale, accumulate);
       break;
     case 2:
-      p2p_multi_kernel<Real, 128, 2><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
-                                                              accumulate);
+      launch_multi<Real, BS, 2>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate);
       break;
     case 3:
-      p2p_multi_kernel<Real, 128, 3><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
-                                                              accumulate);
+      launch_multi<Real, BS, 3>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate);
       break;
     case 4:
-      p2p_multi_kernel<Real, 128, 4><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
-                                                              accumulate);
+      launch_multi<Real, BS, 4>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate);
       break;
     case 6:
-      p2p_multi_kernel<Real, 128, 6><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
-                                                              accumulate);
+      launch_multi<Real, BS, 6>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate);
       break;
     default:
       throw Error(NNK_E_ARG, "pair kernel supports 1, 2, 3, 4 or 6 right-hand sides per launch");
   }
+}
+
+// Block sizes the pair kernels are built for (static shared memory stays
+// under 48 KB: FP64 tiles of 256 sources with 4-6 right-hand sides do not).
+template <typename Real>
+inline bool p2p_bs_ok(int bs, int R) {
+  auto fits = [&](auto bsc) {
+    constexpr int B = decltype(bsc)::value;
+    switch (R) {
+      case 2: return p2p_fits<Real, B, 2>();
+      case 3: return p2p_fits<Real, B, 3>();
+      case 4: return p2p_fits<Real, B, 4>();
+      case 6: return p2p_fits<Real, B, 6>();
+      default: return true;
+    }
+  };
+  if (bs == 64) return fits(std::integral_constant<int, 64>());
+  if (bs == 128) return fits(std::integral_constant<int, 128>());
+  if (bs == 256) return fits(std::integral_constant<int, 256>());
+  return false;
+}
+
+template <typename Real>
+inline void launch_p2p(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
+                       const Real* tpos, Real* out, Real* partial, Real e2, Real scale, cudaStream_t st,
+                       int accumulate = 0, int R = 1, int bs = 128) {
+  if (ntasks == 0) return;
+  if (!p2p_bs_ok<Real>(bs, R)) bs = 128;
+  if (bs == 64)
+    launch_p2p_bs<Real, 64>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R);
+  else if (bs == 256)
+    launch_p2p_bs<Real, 256>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R);
+  else
+    launch_p2p_bs<Real, 128>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R);
   NNK_CHECK_LAUNCH();
 }
 

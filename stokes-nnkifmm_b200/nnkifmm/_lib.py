@@ -88,6 +88,7 @@ SIGNATURES = {
     "nnk_fmm_apply_adjoint": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32]),
     "nnk_fmm_source_count": (_i32, [_vp, _pi64]),
     "nnk_fmm_set_eps": (_i32, [_vp, _f64]),
+    "nnk_fmm_autotune": (_i32, [_vp, _i32, _pd, _pd]),
     "nnk_fmm_grad_positions": (_i32, [_vp, _vp, _vp, _i32, _vp, _vp, _i32]),
     "nnk_fmm_profile": (_i32, [_vp, _i32]),
     "nnk_fmm_profile_read": (_i32, [_vp, _vp, _vp]),
@@ -108,6 +109,7 @@ SIGNATURES = {
     "nnk_batch_solve": (_i32, [_vp, _vp, _vp, C.POINTER(SolveParams), _vp, _i32]),
     "nnk_batch_set_refinement": (_i32, [_vp, _i32, _i32, _f64]),
     "nnk_batch_matvecs": (_i32, [_vp, _pi64]),
+    "nnk_batch_use_graphs": (_i32, [_vp, _i32]),
     "nnk_batch_profile": (_i32, [_vp, _i32]),
     "nnk_batch_profile_read": (_i32, [_vp, _i32, _vp, _vp]),
     "nnk_batch_destroy": (_i32, [_vp]),

@@ -80,7 +80,7 @@ class BatchMobility:
     refinement unless refine=False."""
 
     def __init__(self, bodies, kernelPar, cap=200, precision="mixed", nrhs=6, refine=None, device=0, ctx=None,
-                 max_outer=12, inner_tol=1e-3, m2l="fft"):
+                 max_outer=12, inner_tol=1e-4, m2l="fft"):
         self.ctx = ctx if ctx is not None else L.Context(device)
         self.nrhs = int(nrhs)
         self.sizes = []
@@ -174,6 +174,10 @@ class BatchMobility:
         L.check(L.lib.nnk_batch_profile_read(self.h, int(which), L.ptr(ms), L.ptr(ln)), self.ctx.h,
                 "nnk_batch_profile_read")
         return dict(zip(L.PHASES, ms)), dict(zip(L.PHASES, ln))
+
+    def use_graphs(self, enable=True):
+        """Replay the matvec from a CUDA graph (default) or launch kernel by kernel."""
+        L.check(L.lib.nnk_batch_use_graphs(self.h, int(bool(enable))), self.ctx.h, "use_graphs")
 
     def matvecs(self):
         c = C.c_int64()

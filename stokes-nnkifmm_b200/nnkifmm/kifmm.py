@@ -91,6 +91,13 @@ class KIFMM:
         i = self.tree.info
         return self._call(L.lib.nnk_fmm_apply_adjoint, velocities, i.num_targets, i.num_potentials, nrhs)
 
+    def autotune(self, nrhs=1):
+        """Pick the pair-kernel tile per launch group by timing; returns the
+        summed pair-kernel milliseconds before and after."""
+        a, b = C.c_double(), C.c_double()
+        L.check(L.lib.nnk_fmm_autotune(self.h, int(nrhs), C.byref(a), C.byref(b)), self.ctx.h, "autotune")
+        return a.value, b.value
+
     def setEps(self, eps):
         """Rebuild the eps-dependent operators for a new kernelPar(1)."""
         L.check(L.lib.nnk_fmm_set_eps(self.h, float(eps)), self.ctx.h, "setEps")

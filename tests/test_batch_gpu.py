@@ -110,6 +110,21 @@ def test_fourier_m2l_batch_matches_pair_m2l(bodies, nrhs):
         assert np.linalg.norm(yb[sl] - ya[sl]) <= 1e-5 * np.linalg.norm(ya[sl]), s
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_replay_is_bitwise_the_launches(bodies, precision):
+    B = nb.BatchMobility(bodies, [EPS, MU], cap=CAP, precision=precision, nrhs=6, refine=False)
+    x = random_batch_vector(B, np.random.default_rng(13))
+    B.use_graphs(False)
+    a = B.apply(x)
+    B.use_graphs(True)
+    b = B.apply(x)   # captures
+    c = B.apply(2 * x)  # replays
+    assert np.array_equal(a, b)
+    assert np.array_equal(B.apply(x), a)
+    tol = 1e-5 if precision == "mixed" else 1e-8
+    assert np.linalg.norm(c - 2 * a) <= tol * np.linalg.norm(2 * a)
+
+
 def test_fp64_batch_solve_matches_per_body(bodies, per_body_fp64):
     """Per-system GMRES in the batch = one gmres call per body and mode.
     (Below ~1e-9 the explicit residual of an FP64 FMM stops falling: its
