@@ -202,10 +202,12 @@ def solve_benchmarks(torch, nk, args):
             sw.F[0], sw.Moment[0] = np.array(F, float), np.array(M, float)
             rhs = nk.mobilityRHS(sw)
             mob.solve(rhs, tol=1e-6, maxIter=300)
-            t0 = time.perf_counter()
-            for _ in range(3):
+            ts = []
+            for _ in range(5):
+                t0 = time.perf_counter()
                 x, flag, relres, it = mob.solve(rhs, tol=1e-6, maxIter=300)
-            times.append((time.perf_counter() - t0) / 3)
+                ts.append(time.perf_counter() - t0)
+            times.append(float(np.median(ts)))
             errs.append(float(np.linalg.norm(x[-6:] - xd) / np.linalg.norm(xd)))
             iters.append(it)
         out[f"sphere_{label}"] = {"solves_per_s": 1.0 / float(np.mean(times)), "ms_per_solve": 1e3 * float(np.mean(times)),

@@ -396,8 +396,8 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
   }
 }
 
-// Per level, runs of nodes of the same tree cut into tiles of at most 32
-// nodes; the operator index is filled in by build_operators.
+// Per level, runs of nodes of the same tree cut into tiles of at most
+// kC2ETileNodes nodes, each tile with the operator of its (tree, level).
 void Fmm::build_c2e_tiles(const std::vector<int32_t>& nodes, const std::vector<int64_t>& off,
                           std::vector<C2ETile>& tiles, std::vector<int64_t>& toff) {
   const HostTree& t = *t_;
@@ -408,7 +408,7 @@ void Fmm::build_c2e_tiles(const std::vector<int32_t>& nodes, const std::vector<i
     while (i < off[L + 1]) {
       const int32_t g = t.group_of(nodes[i]);
       int64_t j = i;
-      while (j < off[L + 1] && j - i < 32 && t.group_of(nodes[j]) == g) ++j;
+      while (j < off[L + 1] && j - i < kC2ETileNodes && t.group_of(nodes[j]) == g) ++j;
       const int op = op_of_[(size_t)g * (maxl_ + 1) + L];
       if (op < 0) throw Error(NNK_E_STATE, "node above its tree's depth");
       tiles.push_back(C2ETile{op, (int)i, (int)(j - i), 0});

@@ -69,7 +69,7 @@ struct IoMap {
   long long nrows = 0;
 };
 
-// Nodes nodes[first .. first+count) of one level (count <= 32) that share
+// Nodes nodes[first .. first+count) of one level (count <= 64) that share
 // the check-to-equivalent operator `op`.
 struct C2ETile {
   int op;

@@ -515,12 +515,18 @@ inline void launch_reduce(const RedD* reds, int nreds, const Real* partial, Real
 // share one operator (a level of one tree of the forest); A is the n x n
 // column-major operator ops + op * n^2.  check and dst hold, per surface
 // point p of a node, R consecutive 3-vectors: check[(node * P + p) * R + k].
+// 64 x 64 output tile (operator rows x (node, right-hand side) columns) per
+// CTA of 256 threads, each accumulating 4 x 4 in FP64; K in steps of 16 with
+// the next step's operands fetched into registers while the current one is
+// multiplied from shared memory.
+constexpr int kC2ETileNodes = 64;
+
 template <typename Real>
 __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops, int n, int trans,
                                                   const C2ETile* __restrict__ tiles, const int* __restrict__ nodes,
                                                   const Real* __restrict__ check, Real* __restrict__ dst,
                                                   long long base, int P, int R, float* __restrict__ m2l_dst, int NP) {
-  constexpr int BM = 64, BN = 32, BK = 16;
+  constexpr int BM = 64, BN = 64, BK = 16;
   __shared__ double As[BK][BM + 1];
   __shared__ double Bs[BK][BN + 1];
   __shared__ int col_node[BN];
@@ -538,18 +544,26 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
   }
   __syncthreads();
   const int tr = tid % 16, tc = tid / 16;
-  double acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-  for (int k0 = 0; k0 < n; k0 += BK) {
-    for (int e = tid; e < BK * BM; e += 256) {
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0;
+  // register staging: 4 A values and 4 B values per thread per K step
+  double ra[4], rb[4];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q;  // 0 .. 1023 = BK * BM
       int kk, mm;
       if (!trans) { mm = e % BM; kk = e / BM; }   // A[r][c] at c*n + r: contiguous in r
       else { kk = e % BK; mm = e / BK; }          // A^T[r][c] = A[c][r] at r*n + c: contiguous in c
       const int r = m0 + mm, c = k0 + kk;
-      double v = 0;
-      if (r < n && c < n) v = trans ? A[(size_t)r * n + c] : A[(size_t)c * n + r];
-      As[kk][mm] = v;
+      ra[q] = (r < n && c < n) ? (trans ? A[(size_t)r * n + c] : A[(size_t)c * n + r]) : 0.0;
     }
-    for (int e = tid; e < BK * BN; e += 256) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q;  // BK * BN
       const int kk = e % BK, nn = e / BK;
       const int c = k0 + kk, node = col_node[nn];
       double v = 0;
@@ -557,27 +571,47 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
         const int p = c / 3, comp = c - 3 * p;
         v = (double)check[(((size_t)node * P + p) * R + col_k[nn]) * 3 + comp];
       }
-      Bs[kk][nn] = v;
+      rb[q] = v;
     }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q;
+      int kk, mm;
+      if (!trans) { mm = e % BM; kk = e / BM; }
+      else { kk = e % BK; mm = e / BK; }
+      As[kk][mm] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q;
+      Bs[e % BK][e / BK] = rb[q];
+    }
+  };
+  load(0);
+  for (int k0 = 0; k0 < n; k0 += BK) {
+    store();
     __syncthreads();
+    if (k0 + BK < n) load(k0 + BK);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
-      double a[4], b[2];
+      double a[4], b[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) a[i] = As[kk][tr + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) b[j] = Bs[kk][tc + 16 * j];
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tc + 16 * j];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) acc[i][j] += a[i] * b[j];
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     __syncthreads();
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
+    for (int j = 0; j < 4; ++j) {
       const int r = m0 + tr + 16 * i, jj = tc + 16 * j;
       const int node = col_node[jj];
       if (r < n && node >= 0) {
@@ -597,7 +631,7 @@ inline void launch_c2e(const double* ops, int n, int trans, const C2ETile* tiles
                        const Real* check, Real* dst, int64_t base, int P, int R, cudaStream_t st,
                        float* m2l_dst = nullptr, int NP = 0) {
   if (ntiles == 0) return;
-  dim3 grid((n + 63) / 64, ntiles, R);
+  dim3 grid((n + 63) / 64, ntiles, (kC2ETileNodes * R + 63) / 64);
   c2e_kernel<Real><<<grid, 256, 0, st>>>(ops, n, trans, tiles, nodes, check, dst, base, P, R, m2l_dst, NP);
   NNK_CHECK_LAUNCH();
 }
