@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--no-solves", action="store_true")
     ap.add_argument("--batch-bodies", type=int, default=4)
     ap.add_argument("--no-gradient", action="store_true")
+    ap.add_argument("--batch-apply", type=int, default=0,
+                    help="only build the mixed batch of --batch-bodies bodies and time this many matvecs "
+                         "(6 rigid-mode right-hand sides each; for profiling the batch kernels)")
     ap.add_argument("--grad-force", type=int, default=50_000)
     return ap.parse_args()
 
@@ -215,32 +218,39 @@ def solve_benchmarks(torch, nk, args):
     nb = args.batch_bodies
     bodies = batched_bodies(nb)
     res = {}
-    from nnkifmm.batch import Body
+    from nnkifmm.batch import RIGID_MODES, Body
     # plain FP64: one body, one right-hand side per gmres call (the reference's way)
     t0 = time.perf_counter()
     seq = [Body(c, f, [0.005, 1.0], 200, "fp64") for c, f in bodies]
     setup = time.perf_counter() - t0
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    outs = [b.solve_modes(1e-6, 400) for b in seq]
-    dt = time.perf_counter() - t0
-    res["fp64_sequential"] = ([o[0] for o in outs], dt, setup, [o[1] for o in outs])
+    seq[0].solve_modes(1e-6, 400, modes=RIGID_MODES[:1])  # first-call initialisation
+    dts = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        outs = [b.solve_modes(1e-6, 400) for b in seq]
+        dts.append(time.perf_counter() - t0)
+    res["fp64_sequential"] = ([o[0] for o in outs], float(np.median(dts)), setup, [o[1] for o in outs])
     del seq
     # batched: every body and all 6 right-hand sides in one forest
     for label, prec in [("fp64_batched", "fp64"), ("mixed_refined_batched", "mixed")]:
         t0 = time.perf_counter()
         B = nk.BatchMobility(bodies, [0.005, 1.0], cap=200, precision=prec, nrhs=6)
         setup = time.perf_counter() - t0
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        mats, its = B.solve_modes(tol=1e-6, maxIter=400)
-        dt = time.perf_counter() - t0
-        res[label] = (mats, dt, setup, its)
+        B.solve_modes(tol=1e-6, maxIter=400)  # first call: CUDA-graph capture
+        dts = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            mats, its = B.solve_modes(tol=1e-6, maxIter=400)
+            dts.append(time.perf_counter() - t0)
+        res[label] = (mats, float(np.median(dts)), setup, its)
         del B
     ref = res["fp64_sequential"][0]
     n_solves = 6 * nb
     for label, (mats, dt, setup, its) in res.items():
         out[f"batched_{label}"] = {"solves_per_s": n_solves / dt, "s_total": dt, "setup_s": setup,
+                                   "timing": "median of repeated solves after one warm-up solve",
                                    "gmres_iters_mean": float(np.mean([i[2] for it in its for i in it])),
                                    "rel_err_vs_fp64": float(max(np.linalg.norm(a - b) / np.linalg.norm(b)
                                                                 for a, b in zip(mats, ref)))}
@@ -255,6 +265,25 @@ def solve_benchmarks(torch, nk, args):
                     "kernels), per-system GMRES advancing in lockstep; fp64_sequential = one body and one "
                     "right-hand side per GMRES call")
     return out
+
+
+def batch_apply(torch, nk, args):
+    """Matvecs of the mixed forest batch (--batch-bodies bodies x 6 rigid-mode
+    right-hand sides), CUDA-event timed; a profiling target for the batch
+    kernels (multi-RHS pair kernels, Fourier M2L, tiled C2E)."""
+    from nnkifmm.workloads import batched_bodies
+    B = nk.BatchMobility(batched_bodies(args.batch_bodies), [0.005, 1.0], cap=200, precision="mixed", nrhs=6,
+                         refine=False)
+    x = np.random.default_rng(0).standard_normal(B.n)
+    B.apply(x)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.batch_apply):
+        B.apply(x)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / args.batch_apply
+    print(json.dumps({"batch_apply_ms": 1e3 * dt, "bodies": args.batch_bodies, "systems": B.systems,
+                      "length": B.n}), flush=True)
 
 
 def gradient_benchmark(torch, nk, args):
@@ -356,6 +385,9 @@ def main():
     import nnkifmm as nk
     from nnkifmm.workloads import matvec_at_scale
     nk.context(local).set_stream(torch.cuda.current_stream(local).cuda_stream)
+    if args.batch_apply:
+        batch_apply(torch, nk, args)
+        return
     t0 = time.time()
     w = matvec_at_scale(args.n_force, args.n_quad)
     NN, tree, fmm = build(nk, w, args.precision)

@@ -382,6 +382,15 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
     std::vector<C2ETile> ut;
     build_c2e_tiles(ts.up_nodes_host, ts.up_off, ut, ts.up_toff);
     ts.up_tiles.upload(ut, st);
+    // scratch of the K-split C2E launches (allocated here: applies may be
+    // captured into CUDA graphs, where allocation is not allowed)
+    size_t need = 0;
+    for (int R = 1; R <= R_; ++R)
+      for (int L = 1; L <= maxl_; ++L) {
+        need = std::max(need, c2e_part_size(3 * P_, (int)(ts.up_toff[L + 1] - ts.up_toff[L]), R));
+        need = std::max(need, c2e_part_size(3 * P_, (int)(dn_toff_[L + 1] - dn_toff_[L]), R));
+      }
+    if (need > c2e_part_.n) c2e_part_.alloc(need);
   }
   split_tasks(ts, tasks, segs);
   ts.tasks.upload(tasks, st);
@@ -700,7 +709,7 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     const int64_t nt = ts.up_toff[L + 1] - ts.up_toff[L];
     phase(NNK_PHASE_UP_C2E, [&] {
       launch_c2e<Real>(ops_.p, n, 0, ts.up_tiles.p + ts.up_toff[L], (int)nt, ts.up_nodes.p, check, str, regionA, P_,
-                       R, st, tm ? m2l_.src.p : nullptr, m2l_.NP);
+                       R, st, tm ? m2l_.src.p : nullptr, m2l_.NP, c2e_part_.p, c2e_part_.n);
     });
   }
   // downward pass
@@ -721,7 +730,7 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     const int64_t nt = dn_toff_[L + 1] - dn_toff_[L];
     phase(NNK_PHASE_DOWN_C2E, [&] {
       launch_c2e<Real>(ops_.p, n, 1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str,
-                       regionA + (int64_t)P_ * N_, P_, R, st);
+                       regionA + (int64_t)P_ * N_, P_, R, st, nullptr, 0, c2e_part_.p, c2e_part_.n);
     });
   }
 }

@@ -213,6 +213,7 @@ class Fmm {
   std::vector<double> op_w_;          // box width of each operator
   std::vector<int> op_of_;            // (group * (maxl + 1) + level) -> operator
   DBuf<C2ETile> dn_tiles_;  // per level, tiles of nodes sharing an operator
+  DBuf<double> c2e_part_;   // K-split partial sums of the small C2E launches
   std::vector<int64_t> dn_toff_;
   // transpose (built on first use): tasks with inverted lists, unified
   // points [sorted targets | surfaces], identity gather of the targets and

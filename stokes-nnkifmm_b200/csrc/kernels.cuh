@@ -194,12 +194,47 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
         if (f0 + BS + tid < total) fetch(f0 + BS + tid, pa, pb);
         const int nj = min(BS, total - f0);
         if (act0) {
+          if constexpr (std::is_same<Real, float>::value) {
+            // the two targets in the two lanes of packed FP32 arithmetic
+            const float2 X = make_float2(tx, ux), Y = make_float2(ty, uy), Z = make_float2(tz, uz);
+            const float2 E = make_float2(e2, e2);
+            float2 cx = make_float2(ax, bx), cy = make_float2(ay, by), cz = make_float2(az, bz);
 #pragma unroll 4
-          for (int j = ms; j < nj; j += splits) {
-            const T4 a = s4[j];
-            const T2 b = s2[j];
-            pair_acc<Real>(tx, ty, tz, a, b, e2, ax, ay, az);
-            pair_acc<Real>(ux, uy, uz, a, b, e2, bx, by, bz);  // dummy target (0,0,0) when !act1
+            for (int j = ms; j < nj; j += splits) {
+              const float4 a = s4[j];
+              const float2 b = s2[j];
+              const float2 dx = __fadd2_rn(X, make_float2(-a.x, -a.x));
+              const float2 dy = __fadd2_rn(Y, make_float2(-a.y, -a.y));
+              const float2 dz = __fadd2_rn(Z, make_float2(-a.z, -a.z));
+              float2 d = __ffma2_rn(dx, dx, E);
+              d = __ffma2_rn(dy, dy, d);
+              d = __ffma2_rn(dz, dz, d);
+              const float2 inv = make_float2(rsqrtf(d.x), rsqrtf(d.y));
+              const float2 inv3 = __fmul2_rn(__fmul2_rn(inv, inv), inv);
+              const float2 A = __ffma2_rn(E, inv3, inv);
+              const float2 fx = make_float2(a.w, a.w), fy = make_float2(b.x, b.x), fz = make_float2(b.y, b.y);
+              float2 dot = __fmul2_rn(dx, fx);
+              dot = __ffma2_rn(dy, fy, dot);
+              dot = __ffma2_rn(dz, fz, dot);
+              const float2 B = __fmul2_rn(dot, inv3);
+              cx = __ffma2_rn(A, fx, __ffma2_rn(B, dx, cx));
+              cy = __ffma2_rn(A, fy, __ffma2_rn(B, dy, cy));
+              cz = __ffma2_rn(A, fz, __ffma2_rn(B, dz, cz));
+            }
+            ax = cx.x;
+            bx = cx.y;
+            ay = cy.x;
+            by = cy.y;
+            az = cz.x;
+            bz = cz.y;
+          } else {
+#pragma unroll 4
+            for (int j = ms; j < nj; j += splits) {
+              const T4 a = s4[j];
+              const T2 b = s2[j];
+              pair_acc<Real>(tx, ty, tz, a, b, e2, ax, ay, az);
+              pair_acc<Real>(ux, uy, uz, a, b, e2, bx, by, bz);  // dummy target (0,0,0) when !act1
+            }
           }
         }
         __syncthreads();
@@ -260,7 +295,8 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
   using T4 = typename Vec4T<Real>::t4;
   constexpr int C = 3 * R;
   __shared__ T4 sp[BS];
-  __shared__ Real sf[BS][C];
+  __shared__ __align__(16) Real sf[BS][C];  // rows of 3R values; float2 pairs need 8-byte alignment
+  constexpr bool kPacked = std::is_same<Real, float>::value && R % 2 == 0 && !GRAD;
   __shared__ long long seg_start[BS];
   __shared__ int seg_end[BS];
   __shared__ Real red[C][BS];
@@ -284,6 +320,9 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
     Real acc[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) acc[c] = 0;
+    float2 acc2[kPacked ? C / 2 : 1];  // packed form: acc2[i] = (acc[2 i], acc[2 i + 1])
+#pragma unroll
+    for (int i = 0; i < (kPacked ? C / 2 : 1); ++i) acc2[i] = make_float2(0.f, 0.f);
     for (int sb = 0; sb < tk.nseg; sb += BS) {
       const int nsb = min(BS, tk.nseg - sb);
       __syncthreads();
@@ -325,8 +364,11 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
       for (int f0 = 0; f0 < total; f0 += BS) {
         if (f0 + tid < total) {
           sp[tid] = pa;
+          // component-major: sf[j][c * R + k] = f_c of right-hand side k
 #pragma unroll
-          for (int c = 0; c < C; ++c) sf[tid][c] = pb[c];
+          for (int k = 0; k < R; ++k)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) sf[tid][c * R + k] = pb[3 * k + c];
         }
         __syncthreads();
         if (f0 + BS + tid < total) fetch(f0 + BS + tid, pa, pb);
@@ -341,7 +383,7 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
             const Real inv2 = inv * inv;
             const Real inv3 = inv2 * inv;
             const Real inv5 = inv3 * inv2;
-            const Real fx = sf[j][0], fy = sf[j][1], fz = sf[j][2];
+            const Real fx = sf[j][0], fy = sf[j][R], fz = sf[j][2 * R];
             const Real wf = wx * fx + wy * fy + wz * fz;
             const Real rf = dx * fx + dy * fy + dz * fz;
             const Real wr = wx * dx + wy * dy + wz * dz;
@@ -352,35 +394,71 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
             acc[2] += a * dz + b * wz + c * fz;
           }
         } else if (act) {
+          if constexpr (kPacked) {
+            // right-hand sides in pairs in the two lanes of packed FP32 arithmetic
 #pragma unroll 2
-          for (int j = ms; j < nj; j += splits) {
-            const T4 q = sp[j];
-            const Real dx = tx - q.x, dy = ty - q.y, dz = tz - q.z;
-            const Real d = dx * dx + dy * dy + dz * dz + e2;
-            const Real inv = rsq(d);
-            const Real inv3 = inv * inv * inv;
-            const Real a = e2 * inv3 + inv;
+            for (int j = ms; j < nj; j += splits) {
+              const T4 q = sp[j];
+              const float dx = tx - q.x, dy = ty - q.y, dz = tz - q.z;
+              const float d = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, e2)));
+              const float inv = rsqrtf(d);
+              const float inv3 = inv * inv * inv;
+              const float a = fmaf(e2, inv3, inv);
+              const float2 DX = make_float2(dx, dx), DY = make_float2(dy, dy), DZ = make_float2(dz, dz);
+              const float2 A = make_float2(a, a), I3 = make_float2(inv3, inv3);
+              const float2* fr = reinterpret_cast<const float2*>(&sf[j][0]);
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-              const Real fx = sf[j][3 * k], fy = sf[j][3 * k + 1], fz = sf[j][3 * k + 2];
-              const Real b = (dx * fx + dy * fy + dz * fz) * inv3;
-              acc[3 * k] += a * fx + b * dx;
-              acc[3 * k + 1] += a * fy + b * dy;
-              acc[3 * k + 2] += a * fz + b * dz;
+              for (int m = 0; m < R / 2; ++m) {
+                const float2 fx = fr[m], fy = fr[R / 2 + m], fz = fr[R + m];
+                float2 dot = __fmul2_rn(DX, fx);
+                dot = __ffma2_rn(DY, fy, dot);
+                dot = __ffma2_rn(DZ, fz, dot);
+                const float2 B = __fmul2_rn(dot, I3);
+                acc2[m] = __ffma2_rn(A, fx, __ffma2_rn(B, DX, acc2[m]));
+                acc2[R / 2 + m] = __ffma2_rn(A, fy, __ffma2_rn(B, DY, acc2[R / 2 + m]));
+                acc2[R + m] = __ffma2_rn(A, fz, __ffma2_rn(B, DZ, acc2[R + m]));
+              }
+            }
+          } else {
+#pragma unroll 2
+            for (int j = ms; j < nj; j += splits) {
+              const T4 q = sp[j];
+              const Real dx = tx - q.x, dy = ty - q.y, dz = tz - q.z;
+              const Real d = dx * dx + dy * dy + dz * dz + e2;
+              const Real inv = rsq(d);
+              const Real inv3 = inv * inv * inv;
+              const Real a = e2 * inv3 + inv;
+#pragma unroll
+              for (int k = 0; k < R; ++k) {
+                const Real fx = sf[j][k], fy = sf[j][R + k], fz = sf[j][2 * R + k];
+                const Real b = (dx * fx + dy * fy + dz * fz) * inv3;
+                acc[k] += a * fx + b * dx;
+                acc[R + k] += a * fy + b * dy;
+                acc[2 * R + k] += a * fz + b * dz;
+              }
             }
           }
         }
         __syncthreads();
       }
     }
+    if constexpr (kPacked) {
 #pragma unroll
-    for (int c = 0; c < C; ++c) red[c][tid] = acc[c];
+      for (int i = 0; i < C / 2; ++i) {
+        red[2 * i][tid] = acc2[i].x;
+        red[2 * i + 1][tid] = acc2[i].y;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < C; ++c) red[c][tid] = acc[c];
+    }
     __syncthreads();
     for (int v = tid; v < nt * C; v += BS) {
-      const int q = v / C, c = v - q * C;
+      const int q = v / C, cc = v - q * C;  // output component cc = 3 k + c
+      const int rr = (cc % 3) * R + cc / 3;  // its accumulator c * R + k
       Real sum = 0;
-      for (int k = 0; k < splits; ++k) sum += red[c][q + k * nt];
-      const long long o = (long long)C * (tk.out + t0 + q) + c;
+      for (int k = 0; k < splits; ++k) sum += red[rr][q + k * nt];
+      const long long o = (long long)C * (tk.out + t0 + q) + cc;
       if (accumulate) out[o] += scale * sum;
       else out[o] = scale * sum;
     }
@@ -525,14 +603,18 @@ template <typename Real>
 __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops, int n, int trans,
                                                   const C2ETile* __restrict__ tiles, const int* __restrict__ nodes,
                                                   const Real* __restrict__ check, Real* __restrict__ dst,
-                                                  long long base, int P, int R, float* __restrict__ m2l_dst, int NP) {
+                                                  long long base, int P, int R, float* __restrict__ m2l_dst, int NP,
+                                                  int ksplit, int kper, double* __restrict__ part) {
   constexpr int BM = 64, BN = 64, BK = 16;
   __shared__ double As[BK][BM + 1];
   __shared__ double Bs[BK][BN + 1];
   __shared__ int col_node[BN];
   __shared__ int col_k[BN];
   const C2ETile tl = tiles[blockIdx.y];
-  const int m0 = blockIdx.x * BM, j0 = blockIdx.z * BN;
+  const int zch = gridDim.z / ksplit;
+  const int split = blockIdx.z / zch, zc = blockIdx.z - split * zch;
+  const int kbeg = split * kper, kend = min(n, kbeg + kper);
+  const int m0 = blockIdx.x * BM, j0 = zc * BN;
   const int ncol = tl.count * R;
   if (j0 >= ncol) return;
   const double* __restrict__ A = ops + (size_t)tl.op * n * n;
@@ -559,7 +641,7 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
       if (!trans) { mm = e % BM; kk = e / BM; }   // A[r][c] at c*n + r: contiguous in r
       else { kk = e % BK; mm = e / BK; }          // A^T[r][c] = A[c][r] at r*n + c: contiguous in c
       const int r = m0 + mm, c = k0 + kk;
-      ra[q] = (r < n && c < n) ? (trans ? A[(size_t)r * n + c] : A[(size_t)c * n + r]) : 0.0;
+      ra[q] = (r < n && c < kend) ? (trans ? A[(size_t)r * n + c] : A[(size_t)c * n + r]) : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -567,7 +649,7 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
       const int kk = e % BK, nn = e / BK;
       const int c = k0 + kk, node = col_node[nn];
       double v = 0;
-      if (c < n && node >= 0) {
+      if (c < kend && node >= 0) {
         const int p = c / 3, comp = c - 3 * p;
         v = (double)check[(((size_t)node * P + p) * R + col_k[nn]) * 3 + comp];
       }
@@ -589,11 +671,11 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
       Bs[e % BK][e / BK] = rb[q];
     }
   };
-  load(0);
-  for (int k0 = 0; k0 < n; k0 += BK) {
+  load(kbeg);
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
     store();
     __syncthreads();
-    if (k0 + BK < n) load(k0 + BK);
+    if (k0 + BK < kend) load(k0 + BK);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       double a[4], b[4];
@@ -614,6 +696,12 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
     for (int j = 0; j < 4; ++j) {
       const int r = m0 + tr + 16 * i, jj = tc + 16 * j;
       const int node = col_node[jj];
+      if (ksplit > 1) {
+        // partial sum of this K range: part[split][tile][column][row]
+        if (r < n && node >= 0)
+          part[(((size_t)split * gridDim.y + blockIdx.y) * (kC2ETileNodes * R) + j0 + jj) * n + r] = acc[i][j];
+        continue;
+      }
       if (r < n && node >= 0) {
         const int p = r / 3, comp = r - 3 * p;
         dst[((base + (long long)P * node + p) * R + col_k[jj]) * 3 + comp] = (Real)acc[i][j];
@@ -626,14 +714,63 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
     }
 }
 
+// Sum of the K-range partials in split order (deterministic), written out
+// like the single-pass epilogue.
+template <typename Real>
+__global__ void c2e_reduce_kernel(const C2ETile* __restrict__ tiles, const int* __restrict__ nodes, int n, int R,
+                                  int ksplit, int ntiles, const double* __restrict__ part, Real* __restrict__ dst,
+                                  long long base, int P, float* __restrict__ m2l_dst, int NP) {
+  const int tile = blockIdx.y;
+  const C2ETile tl = tiles[tile];
+  const int cols = kC2ETileNodes * R;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)cols * n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(e / n), r = (int)(e - (long long)j * n);
+    if (j >= tl.count * R) continue;
+    double s = 0;
+    for (int q = 0; q < ksplit; ++q) s += part[(((size_t)q * ntiles + tile) * cols + j) * n + r];
+    const int node = nodes[tl.first + j / R], k = j % R;
+    const int p = r / 3, comp = r - 3 * p;
+    dst[((base + (long long)P * node + p) * R + k) * 3 + comp] = (Real)s;
+    if (m2l_dst) {
+      uint32_t t;
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"((float)s));
+      m2l_dst[(size_t)node * NP + r] = __uint_as_float(t);
+    }
+  }
+}
+
+// K splits for a launch of `blocks` CTAs: enough CTAs for two per SM.
+inline int c2e_splits(int n, int blocks) {
+  int k = 1;
+  while (k < 8 && blocks * k < 2 * 148 && n / (2 * k) >= 32) k *= 2;
+  return k;
+}
+inline size_t c2e_part_size(int n, int ntiles, int R) {
+  const int blocks = ((n + 63) / 64) * ntiles * R;
+  const int k = c2e_splits(n, blocks);
+  return k > 1 ? (size_t)k * ntiles * kC2ETileNodes * R * n : 0;
+}
+
 template <typename Real>
 inline void launch_c2e(const double* ops, int n, int trans, const C2ETile* tiles, int ntiles, const int32_t* nodes,
                        const Real* check, Real* dst, int64_t base, int P, int R, cudaStream_t st,
-                       float* m2l_dst = nullptr, int NP = 0) {
+                       float* m2l_dst = nullptr, int NP = 0, double* part = nullptr, size_t part_n = 0) {
   if (ntiles == 0) return;
-  dim3 grid((n + 63) / 64, ntiles, (kC2ETileNodes * R + 63) / 64);
-  c2e_kernel<Real><<<grid, 256, 0, st>>>(ops, n, trans, tiles, nodes, check, dst, base, P, R, m2l_dst, NP);
+  const int zch = (kC2ETileNodes * R + 63) / 64;
+  const int blocks = ((n + 63) / 64) * ntiles * zch;
+  int ksplit = c2e_splits(n, blocks);
+  if (!part || part_n < c2e_part_size(n, ntiles, R)) ksplit = 1;
+  const int kper = ((n + ksplit - 1) / ksplit + 15) / 16 * 16;
+  dim3 grid((n + 63) / 64, ntiles, zch * ksplit);
+  c2e_kernel<Real><<<grid, 256, 0, st>>>(ops, n, trans, tiles, nodes, check, dst, base, P, R, m2l_dst, NP, ksplit,
+                                         kper, part);
   NNK_CHECK_LAUNCH();
+  if (ksplit > 1) {
+    dim3 g2(std::max(1, std::min(64, (kC2ETileNodes * R * n + 255) / 256)), ntiles);
+    c2e_reduce_kernel<Real><<<g2, 256, 0, st>>>(tiles, nodes, n, R, ksplit, ntiles, part, dst, base, P, m2l_dst, NP);
+    NNK_CHECK_LAUNCH();
+  }
 }
 
 // ---------------------------------------------------------------- scatter

@@ -119,10 +119,15 @@ __global__ void fft_spectra_kernel(int G, int res, const double* __restrict__ sl
 // ---------------------------------------------------------------- forward
 // Q_v[cr][k] for one source node: its shell densities on the res^3 lattice
 // (interior zero), transformed along z (res -> H), y (res -> G), x (res -> G).
-__global__ void fft_forward_kernel(int G, int res, int P, const int* __restrict__ lat,
+// RES > 0: the lattice size at compile time (loops unrolled, per-thread
+// arrays in registers); RES = 0 takes it from `res_rt`.
+template <int RES>
+__global__ void fft_forward_kernel(int G_rt, int res_rt, int P, const int* __restrict__ lat,
                                    const int* __restrict__ src_node, const float* __restrict__ str, long long upbase,
                                    int R, float2* __restrict__ qhat, int NK) {
   extern __shared__ float2 smq[];
+  const int res = RES > 0 ? RES : res_rt;
+  const int G = RES > 0 ? 2 * RES : G_rt;
   const int H = G / 2 + 1, C = 3 * R, r3 = res * res * res;
   float2* tw = smq;                          // G
   float2* Z = tw + G;                        // [cr][x][y][kz]   C res res H
@@ -142,8 +147,10 @@ __global__ void fft_forward_kernel(int G, int res, int P, const int* __restrict_
   __syncthreads();
   for (int e = tid; e < C * res * res; e += nt) {  // z: one (cr, x, y) per thread
     const float* gz = g + e * res;
+#pragma unroll
     for (int kz = 0; kz < H; ++kz) {
       float2 a = make_float2(0.f, 0.f);
+#pragma unroll
       for (int z = 0; z < res; ++z) {
         const float2 w = tw[(kz * z) % G];
         a.x = fmaf(gz[z], w.x, a.x);
@@ -156,10 +163,15 @@ __global__ void fft_forward_kernel(int G, int res, int P, const int* __restrict_
   for (int e = tid; e < C * res * H; e += nt) {  // y: one (cr, x, kz) per thread
     const int crx = e / H, kz = e % H;
     float2 in[8];
-    for (int y = 0; y < res; ++y) in[y] = Z[(crx * res + y) * H + kz];
+#pragma unroll
+    for (int y = 0; y < (RES > 0 ? RES : 8); ++y)
+      if (y < res) in[y] = Z[(crx * res + y) * H + kz];
+#pragma unroll
     for (int ky = 0; ky < G; ++ky) {
       float2 a = make_float2(0.f, 0.f);
-      for (int y = 0; y < res; ++y) cmac(a, in[y], tw[(ky * y) % G]);
+#pragma unroll
+      for (int y = 0; y < (RES > 0 ? RES : 8); ++y)
+        if (y < res) cmac(a, in[y], tw[(ky * y) % G]);
       Y[(crx * G + ky) * H + kz] = a;
     }
   }
@@ -168,10 +180,15 @@ __global__ void fft_forward_kernel(int G, int res, int P, const int* __restrict_
   for (int e = tid; e < C * G * H; e += nt) {  // x: one (cr, ky, kz) per thread
     const int cr = e / (G * H), kyz = e % (G * H);
     float2 in[8];
-    for (int x = 0; x < res; ++x) in[x] = Y[(cr * res + x) * G * H + kyz];
+#pragma unroll
+    for (int x = 0; x < (RES > 0 ? RES : 8); ++x)
+      if (x < res) in[x] = Y[(cr * res + x) * G * H + kyz];
+#pragma unroll
     for (int kx = 0; kx < G; ++kx) {
       float2 a = make_float2(0.f, 0.f);
-      for (int x = 0; x < res; ++x) cmac(a, in[x], tw[(kx * x) % G]);
+#pragma unroll
+      for (int x = 0; x < (RES > 0 ? RES : 8); ++x)
+        if (x < res) cmac(a, in[x], tw[(kx * x) % G]);
       out[(size_t)cr * NK + kx * G * H + kyz] = a;
     }
   }
@@ -223,10 +240,13 @@ __global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* 
 // ---------------------------------------------------------------- inverse
 // check of one target node at its shell lattice points from C_i: inverse
 // passes along x (G -> res), y (G -> res) and z (half spectrum -> res, real).
-__global__ void fft_inverse_kernel(int G, int res, int P, const int* __restrict__ lat,
+template <int RES>
+__global__ void fft_inverse_kernel(int G_rt, int res_rt, int P, const int* __restrict__ lat,
                                    const int* __restrict__ tgt_node, const float2* __restrict__ chat, int R,
                                    float* __restrict__ check, int NK) {
   extern __shared__ float2 smc[];
+  const int res = RES > 0 ? RES : res_rt;
+  const int G = RES > 0 ? 2 * RES : G_rt;
   const int H = G / 2 + 1, C = 3 * R, r3 = res * res * res;
   float2* tw = smc;                   // G
   float2* X = tw + G;                 // [cr][x][ky][kz]  C res G H
@@ -240,30 +260,46 @@ __global__ void fft_inverse_kernel(int G, int res, int P, const int* __restrict_
   for (int e = tid; e < C * G * H; e += nt) {  // x: one (cr, ky, kz) per thread
     const int cr = e / (G * H), kyz = e % (G * H);
     float2 a[8];
-    for (int x = 0; x < res; ++x) a[x] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int x = 0; x < 8; ++x) a[x] = make_float2(0.f, 0.f);
+#pragma unroll
     for (int kx = 0; kx < G; ++kx) {
       const float2 v = ci[(size_t)cr * NK + kx * G * H + kyz];
-      for (int x = 0; x < res; ++x) cmac(a[x], v, tw[(kx * x) % G]);
+#pragma unroll
+      for (int x = 0; x < (RES > 0 ? RES : 8); ++x)
+        if (x < res) cmac(a[x], v, tw[(kx * x) % G]);
     }
-    for (int x = 0; x < res; ++x) X[(cr * res + x) * G * H + kyz] = a[x];
+#pragma unroll
+    for (int x = 0; x < (RES > 0 ? RES : 8); ++x)
+      if (x < res) X[(cr * res + x) * G * H + kyz] = a[x];
   }
   __syncthreads();
   for (int e = tid; e < C * res * H; e += nt) {  // y: one (cr, x, kz) per thread
     const int crx = e / H, kz = e % H;
     float2 a[8];
-    for (int y = 0; y < res; ++y) a[y] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int y = 0; y < 8; ++y) a[y] = make_float2(0.f, 0.f);
+#pragma unroll
     for (int ky = 0; ky < G; ++ky) {
       const float2 v = X[(crx * G + ky) * H + kz];
-      for (int y = 0; y < res; ++y) cmac(a[y], v, tw[(ky * y) % G]);
+#pragma unroll
+      for (int y = 0; y < (RES > 0 ? RES : 8); ++y)
+        if (y < res) cmac(a[y], v, tw[(ky * y) % G]);
     }
-    for (int y = 0; y < res; ++y) Yv[(crx * res + y) * H + kz] = a[y];
+#pragma unroll
+    for (int y = 0; y < (RES > 0 ? RES : 8); ++y)
+      if (y < res) Yv[(crx * res + y) * H + kz] = a[y];
   }
   __syncthreads();
   for (int e = tid; e < C * res * res; e += nt) {  // z: one (cr, x, y) per thread, real output
     const float2* yz = Yv + e * H;
-    for (int z = 0; z < res; ++z) {
+#pragma unroll
+    for (int z = 0; z < (RES > 0 ? RES : 8); ++z) {
+      if (z >= res) break;
       float v = 0.f;
-      for (int kz = 0; kz < H; ++kz) {
+#pragma unroll
+      for (int kz = 0; kz < (RES > 0 ? RES + 1 : 9); ++kz) {
+        if (kz >= H) break;
         const float w = (kz == 0 || 2 * kz == G) ? 1.f : 2.f;
         const float2 t = tw[(kz * z) % G];
         v = fmaf(w, yz[kz].x * t.x - yz[kz].y * t.y, v);
@@ -382,8 +418,12 @@ void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu
   f.inv_smem = inverse_smem(G, res, Rmax);
   if (f.fwd_smem > 227 * 1024 || f.inv_smem > 227 * 1024)
     throw Error(NNK_E_ARG, "Fourier M2L: too many right-hand sides per pass for shared memory");
-  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.fwd_smem));
-  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.inv_smem));
+  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.fwd_smem));
+  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.inv_smem));
+  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.fwd_smem));
+  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.inv_smem));
+  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.fwd_smem));
+  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.inv_smem));
   NNK_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -391,8 +431,10 @@ void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float*
   if (f.ntgt == 0) return;
   if (R > f.Rcap) throw Error(NNK_E_STATE, "Fourier M2L sized for fewer right-hand sides");
   const int G = f.G, res = f.res;
-  fft_forward_kernel<<<f.nsrc, 256, forward_smem(G, res, R), st>>>(G, res, f.P, f.lat.p, f.src_node.p, str, upbase,
-                                                                    R, f.qhat.p, f.NK);
+  auto fwd = res == 6 ? fft_forward_kernel<6> : res == 4 ? fft_forward_kernel<4> : fft_forward_kernel<0>;
+  auto inv = res == 6 ? fft_inverse_kernel<6> : res == 4 ? fft_inverse_kernel<4> : fft_inverse_kernel<0>;
+  fwd<<<f.nsrc, 256, forward_smem(G, res, R), st>>>(G, res, f.P, f.lat.p, f.src_node.p, str, upbase, R, f.qhat.p,
+                                                    f.NK);
   NNK_CHECK_LAUNCH();
   dim3 grid(f.ntgt, (f.NK + 127) / 128);
   switch (R) {
@@ -415,8 +457,8 @@ void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float*
       throw Error(NNK_E_ARG, "Fourier M2L supports 1, 2, 3, 4 or 6 right-hand sides per pass");
   }
   NNK_CHECK_LAUNCH();
-  fft_inverse_kernel<<<f.ntgt, 256, inverse_smem(G, res, R), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, f.chat.p, R,
-                                                                    check, f.NK);
+  inv<<<f.ntgt, 256, inverse_smem(G, res, R), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, f.chat.p, R, check,
+                                                    f.NK);
   NNK_CHECK_LAUNCH();
 }
 
