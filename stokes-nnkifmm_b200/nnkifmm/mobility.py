@@ -302,3 +302,12 @@ def mobilityProblem(swimmers, fluidFunc, t, conditions, kernelPar, TreePar, thre
     if return_info:
         return out, dict(flag=flag, relres=relres, iters=it, x=x)
     return out
+
+
+def richardson(values, eps):
+    """Extrapolation to eps -> 0 of results at two regularisation widths,
+    assuming an O(eps) error (the regularized Stokeslet's leading term):
+    (e1 v2 - e2 v1) / (e1 - e2)."""
+    (v1, v2), (e1, e2) = values, eps
+    v1, v2 = np.asarray(v1, float), np.asarray(v2, float)
+    return (e1 * v2 - e2 * v1) / (e1 - e2)

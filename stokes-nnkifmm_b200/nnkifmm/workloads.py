@@ -6,6 +6,8 @@ surfaces of 20 spheres with centres U[0.2,0.8]^3 and radii U[0.05,0.2]) and
 N(0,1); eps = 1e-3, mu = 1, nodeCapacity 64, p = 6.
 sphere: the single-sphere mobility case (Sphere(1,[0 0 0],10) force nodes,
 Sphere(...,40) quadrature, eps = 0.01, nodeCapacity 60).
+two_squirmers_wall: two squirmers of radius 1 with centres 2.5 apart above a
+triangular-lattice wall (Data Generation/Squiremers.m with a wall added).
 """
 import numpy as np
 
@@ -22,6 +24,47 @@ def cube_sphere(r, centre, n):
     el = np.arctan2(Z, np.sqrt(X ** 2 + Y ** 2))
     return np.stack([r * np.cos(el) * np.cos(az) + centre[0], r * np.cos(el) * np.sin(az) + centre[1],
                      r * np.sin(el) + centre[2]], axis=1)
+
+
+def squirmer_slip(points, B1, B2=0.0):
+    """Tangential squirmer slip (B1 sin t + B2 sin t cos t) e_t on body-frame
+    surface points, t the polar angle from the swimming axis z.  B1 alone is
+    the reference's form (Data Generation/FlowField.m:39-49); B2 adds the
+    pusher/puller mode."""
+    p = np.asarray(points, float)
+    x, y, z = p[:, 0], p[:, 1], p[:, 2]
+    rho = np.hypot(x, y)
+    r = np.sqrt(x * x + y * y + z * z)
+    out = np.zeros_like(p)
+    m = rho > 0
+    # e_t = (x z, y z, -rho^2) / (r rho)
+    et = np.stack([x[m] * z[m], y[m] * z[m], -rho[m] ** 2], axis=1) / (r[m] * rho[m])[:, None]
+    st, ct = rho[m] / r[m], z[m] / r[m]
+    out[m] = ((B1 * st + B2 * st * ct))[:, None] * et
+    return out
+
+
+def wall_lattice(n, spacing, z):
+    """n x n triangular lattice in the plane z, centred at the origin (rows
+    spacing*sqrt(3)/2 apart, every other row shifted by spacing/2)."""
+    ix, iy = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    x = (ix + 0.5 * (iy % 2)) * spacing
+    y = iy * spacing * np.sqrt(3) / 2
+    pts = np.stack([x.ravel(), y.ravel(), np.full(ix.size, float(z))], axis=1)
+    pts[:, :2] -= pts[:, :2].mean(axis=0)
+    return pts
+
+
+def two_squirmers_wall(edge_force=12, edge_quad=48, wall_n=200, spacing=0.05, B1=1.0, B2=0.5):
+    """Two force- and torque-free squirmers (radius 1, centres (+-1.25, 0, 0),
+    swimming axis z) with slip (B1, B2), above a wall z = -1.5 of wall_n^2
+    lattice points whose force and quadrature points coincide (NN = I, as
+    Data Generation/Squiremers.m:19-20), wall velocity 0."""
+    body = cube_sphere(1.0, (0, 0, 0), edge_force)
+    fine = cube_sphere(1.0, (0, 0, 0), edge_quad)
+    wall = wall_lattice(wall_n, spacing, -1.5)
+    return dict(body=body, fine=fine, slip=squirmer_slip(body, B1, B2), centres=[(-1.25, 0, 0), (1.25, 0, 0)],
+                wall=wall)
 
 
 def mixed_cloud(rng, n, centres, radii):
