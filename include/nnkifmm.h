@@ -63,7 +63,11 @@ typedef struct nnk_tree_params {
   int32_t node_capacity; /* 'nodeCapacity' (default 200)                      */
   int32_t max_depth;     /* 'maxDepth' (default 21; at most 23 here)           */
   int32_t nearest;       /* 'nearest' 0/1                                      */
-  int32_t reserved;
+  int32_t builder;       /* where the octree's node structure and the NN
+                            matrix are built: 0 auto (the GPU when the
+                            context has one), 1 host, 2 GPU.  The results are
+                            identical bit for bit; the lists are built on the
+                            host from the node arrays either way.          */
 } nnk_tree_params;
 
 typedef struct nnk_tree_info {
@@ -140,6 +144,10 @@ const char* nnk_version(void);
  * ties share 1/k.  Returns CSR by fine point: *nnz is set; if rowptr is NULL
  * only the count is returned, else rowptr (q+1), col (0-based coarse index)
  * and val (weights) are filled. */
+/* nearestMatrix on the context's GPU when it has one (same result as the
+ * host search, bit for bit); nnk_nearest_matrix_host forces the host. */
+int nnk_nearest_matrix_host(nnk_ctx* ctx, const double* coarse, int64_t n, const double* fine, int64_t q,
+                            int64_t* nnz, int64_t* rowptr, int32_t* col, double* val);
 int nnk_nearest_matrix(nnk_ctx* ctx, const double* coarse, int64_t n,
                        const double* fine, int64_t q, int64_t* nnz,
                        int64_t* rowptr, int32_t* col, double* val);

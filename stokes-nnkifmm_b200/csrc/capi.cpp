@@ -129,14 +129,19 @@ int nnk_ctx_synchronize(nnk_ctx* ctx) {
 
 const char* nnk_last_error(const nnk_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
 
-int nnk_nearest_matrix(nnk_ctx* ctx, const double* coarse, int64_t n, const double* fine, int64_t q,
-                       int64_t* nnz, int64_t* rowptr, int32_t* col, double* val) {
+static int nearest_common(nnk_ctx* ctx, const double* coarse, int64_t n, const double* fine, int64_t q,
+                          int64_t* nnz, int64_t* rowptr, int32_t* col, double* val, bool host) {
   if (!ctx || !nnz || n < 0 || q < 0 || (n && !coarse) || (q && !fine)) return fail(ctx, NNK_E_ARG, "bad arguments");
   API_TRY
   std::vector<int64_t> rp;
   std::vector<int32_t> cl;
   std::vector<double> vl;
-  nnk::nearest_matrix(coarse, n, fine, q, rp, cl, vl);
+  if (!host && ctx->has_gpu) {
+    need_gpu(ctx);
+    nnk::nearest_matrix_gpu(ctx, coarse, n, fine, q, rp, cl, vl);
+  } else {
+    nnk::nearest_matrix(coarse, n, fine, q, rp, cl, vl);
+  }
   *nnz = rp.empty() ? 0 : rp.back();
   if (rowptr) {
     std::memcpy(rowptr, rp.data(), rp.size() * sizeof(int64_t));
@@ -144,6 +149,16 @@ int nnk_nearest_matrix(nnk_ctx* ctx, const double* coarse, int64_t n, const doub
     if (val) std::memcpy(val, vl.data(), vl.size() * sizeof(double));
   }
   API_CATCH(ctx)
+}
+
+int nnk_nearest_matrix(nnk_ctx* ctx, const double* coarse, int64_t n, const double* fine, int64_t q,
+                       int64_t* nnz, int64_t* rowptr, int32_t* col, double* val) {
+  return nearest_common(ctx, coarse, n, fine, q, nnz, rowptr, col, val, false);
+}
+
+int nnk_nearest_matrix_host(nnk_ctx* ctx, const double* coarse, int64_t n, const double* fine, int64_t q,
+                            int64_t* nnz, int64_t* rowptr, int32_t* col, double* val) {
+  return nearest_common(ctx, coarse, n, fine, q, nnz, rowptr, col, val, true);
 }
 
 int nnk_tree_build(nnk_ctx* ctx, const double* pot, int64_t n_pot, const double* tgt, int64_t n_tgt,
@@ -156,11 +171,16 @@ int nnk_tree_build(nnk_ctx* ctx, const double* pot, int64_t n_pot, const double*
     p.node_capacity = params->node_capacity;
     p.max_depth = params->max_depth;
     p.nearest = params->nearest;
+    p.builder = params->builder;
   }
+  if (p.builder < 0 || p.builder > 2) return fail(ctx, NNK_E_ARG, "builder must be 0, 1 or 2");
+  if (p.builder == 2 && !ctx->has_gpu) return fail(ctx, NNK_E_CUDA, "no CUDA device available for the GPU builder");
+  nnk_ctx* gpu = (p.builder == 2 || (p.builder == 0 && ctx->has_gpu)) ? ctx : nullptr;
+  if (gpu) need_gpu(ctx);
   std::unique_ptr<nnk_tree> t(new nnk_tree());
   t->ctx = ctx;
   std::string msg;
-  const int rc = nnk::build_tree(pot, n_pot, tgt, n_tgt, fine, q, nn_rowptr, nn_col, nn_val, p, t->t, msg);
+  const int rc = nnk::build_tree(pot, n_pot, tgt, n_tgt, fine, q, nn_rowptr, nn_col, nn_val, p, t->t, msg, gpu);
   if (rc != NNK_OK) return fail(ctx, rc, msg);
   *out = t.release();
   API_CATCH(ctx)

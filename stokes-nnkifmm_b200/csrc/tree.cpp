@@ -263,7 +263,7 @@ static void build_lists(HostTree& t) {
 int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tgt,
                const double* fine, int64_t q, const int64_t* nn_rowptr,
                const int32_t* nn_col, const double* nn_val, const TreeParams& p,
-               HostTree& t, std::string& msg) {
+               HostTree& t, std::string& msg, struct ::nnk_ctx* gpu) {
   t = HostTree();
   t.params = p;
   if (n_pot < 0 || n_tgt < 0 || (n_pot && !pot) || (n_tgt && !tgt)) {
@@ -345,7 +345,10 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
   for (int64_t i = 0; i < t.n; ++i) t.order[i] = i;
   t.pstart = {0};
   t.pcount = {t.n};
-  {
+  if (gpu) {
+    const int rc = build_nodes_gpu(gpu, t, msg);
+    if (rc) return rc;
+  } else {
     Builder b{t, msg};
     b.divide(0, 1);
     if (b.err) return b.err;
@@ -416,6 +419,8 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
           t.nn_val[t.nn_rowptr[r] + k] = row[k].second;
         }
       }
+    } else if (gpu) {
+      nearest_matrix_gpu(gpu, pot, n_pot, fine, q, t.nn_rowptr, t.nn_col, t.nn_val);
     } else {
       nearest_matrix(pot, n_pot, fine, q, t.nn_rowptr, t.nn_col, t.nn_val);
     }

@@ -10,12 +10,15 @@
 #include <string>
 #include <vector>
 
+struct nnk_ctx;
+
 namespace nnk {
 
 struct TreeParams {
   int node_capacity = 200;
   int max_depth = 21;
   int nearest = 0;
+  int builder = 0;  // 0 auto, 1 host, 2 GPU (node structure and NN matrix)
 };
 
 struct Csr {
@@ -85,11 +88,16 @@ struct HostTree {
   bool touch(int32_t a, int32_t b) const;  // nodeintersection.m closed-box test
 };
 
-// Returns 0 or an NNK_E_* code; msg gets the reason.
+// Returns 0 or an NNK_E_* code; msg gets the reason.  With a GPU context
+// the node structure (build_nodes_gpu) and the NN matrix
+// (nearest_matrix_gpu) are built on the device.
 int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tgt,
                const double* fine, int64_t q, const int64_t* nn_rowptr,
                const int32_t* nn_col, const double* nn_val, const TreeParams& p,
-               HostTree& t, std::string& msg);
+               HostTree& t, std::string& msg, struct ::nnk_ctx* gpu = nullptr);
+int build_nodes_gpu(struct ::nnk_ctx* ctx, HostTree& t, std::string& msg);
+void nearest_matrix_gpu(struct ::nnk_ctx* ctx, const double* coarse, int64_t n, const double* fine, int64_t q,
+                        std::vector<int64_t>& rowptr, std::vector<int32_t>& col, std::vector<double>& val);
 
 // Concatenates trees into one forest: node ids, list entries, leaf source
 // entries, gather rows and target rows of tree k are offset by the totals of

@@ -33,7 +33,7 @@ _pd, _pi32, _pi64, _pu8 = (C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTE
 
 
 class TreeParams(C.Structure):
-    _fields_ = [("node_capacity", _i32), ("max_depth", _i32), ("nearest", _i32), ("reserved", _i32)]
+    _fields_ = [("node_capacity", _i32), ("max_depth", _i32), ("nearest", _i32), ("builder", _i32)]
 
 
 class TreeInfo(C.Structure):
@@ -71,6 +71,7 @@ SIGNATURES = {
     "nnk_ctx_synchronize": (_i32, [_vp]),
     "nnk_last_error": (C.c_char_p, [_vp]),
     "nnk_nearest_matrix": (_i32, [_vp, _vp, _i64, _vp, _i64, _pi64, _vp, _vp, _vp]),
+    "nnk_nearest_matrix_host": (_i32, [_vp, _vp, _i64, _vp, _i64, _pi64, _vp, _vp, _vp]),
     "nnk_tree_build": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _vp, C.POINTER(TreeParams),
                               C.POINTER(_vp)]),
     "nnk_tree_info_get": (_i32, [_vp, C.POINTER(TreeInfo)]),

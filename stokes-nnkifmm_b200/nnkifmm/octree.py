@@ -20,7 +20,7 @@ def _as_points(a):
 
 class OcTree:
     def __init__(self, potPoints, targetPoints, parThreads=0, nodeCapacity=200, maxDepth=21,
-                 finePoints=None, nearest=0, NN=None, blockSize=0.2, device=0, ctx=None):
+                 finePoints=None, nearest=0, NN=None, blockSize=0.2, device=0, ctx=None, builder="auto"):
         self.ctx = ctx if ctx is not None else L.context(device)
         pot = _as_points(potPoints)
         same = targetPoints is potPoints or (np.shape(targetPoints) == np.shape(potPoints)
@@ -42,7 +42,9 @@ class OcTree:
                 rp = np.ascontiguousarray(nn.indptr.astype(np.int64))
                 col = np.ascontiguousarray(nn.indices.astype(np.int32))
                 val = np.ascontiguousarray(nn.data.astype(np.float64))
-        params = L.TreeParams(int(nodeCapacity), int(maxDepth), int(bool(nearest)), 0)
+        # where the node structure and NN are built: auto (GPU when present), host, gpu
+        params = L.TreeParams(int(nodeCapacity), int(maxDepth), int(bool(nearest)),
+                              {"auto": 0, "host": 1, "gpu": 2}[builder])
         h = C.c_void_p()
         rc = L.lib.nnk_tree_build(self.ctx.h, L.ptr(pot), pot.shape[0], L.ptr(tgt), tgt.shape[0],
                                   L.ptr(fine), q, L.ptr(rp), L.ptr(col), L.ptr(val),
@@ -149,18 +151,20 @@ class OcTree:
         return self.finePoints
 
 
-def nearestMatrix(coarse, fine, blockSize=0.2, threads=0, device=0):
+def nearestMatrix(coarse, fine, blockSize=0.2, threads=0, device=0, builder="auto"):
     """nearestMatrix (Tools/Nearest/nearestMatrix.m:17-41) through the library:
-    returns the (Q x N) scipy CSR matrix with exact FP64 ties sharing 1/k."""
+    returns the (Q x N) scipy CSR matrix with exact FP64 ties sharing 1/k
+    (on the GPU when there is one, or on the host with builder="host")."""
     ctx = L.context(device)
+    fn = L.lib.nnk_nearest_matrix_host if builder == "host" else L.lib.nnk_nearest_matrix
     c = _as_points(coarse)
     f = _as_points(fine)
     nnz = C.c_int64()
-    L.check(L.lib.nnk_nearest_matrix(ctx.h, L.ptr(c), c.shape[0], L.ptr(f), f.shape[0], C.byref(nnz),
-                                     None, None, None), ctx.h, "nearestMatrix")
+    L.check(fn(ctx.h, L.ptr(c), c.shape[0], L.ptr(f), f.shape[0], C.byref(nnz), None, None, None), ctx.h,
+            "nearestMatrix")
     rp = np.zeros(f.shape[0] + 1, np.int64)
     col = np.zeros(max(nnz.value, 1), np.int32)
     val = np.zeros(max(nnz.value, 1), np.float64)
-    L.check(L.lib.nnk_nearest_matrix(ctx.h, L.ptr(c), c.shape[0], L.ptr(f), f.shape[0], C.byref(nnz),
-                                     L.ptr(rp), L.ptr(col), L.ptr(val)), ctx.h, "nearestMatrix")
+    L.check(fn(ctx.h, L.ptr(c), c.shape[0], L.ptr(f), f.shape[0], C.byref(nnz), L.ptr(rp), L.ptr(col), L.ptr(val)),
+            ctx.h, "nearestMatrix")
     return sp.csr_matrix((val[:nnz.value], col[:nnz.value], rp), shape=(f.shape[0], c.shape[0]))
