@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--no-solves", action="store_true")
     ap.add_argument("--batch-bodies", type=int, default=4)
     ap.add_argument("--no-gradient", action="store_true")
+    ap.add_argument("--no-squirmers", action="store_true")
+    ap.add_argument("--m2l", default="auto", choices=["auto", "images", "generate", "pairs", "fft"],
+                    help="M2L form of the mixed matvec (auto: tcgen05 TF32 for one right-hand side)")
     ap.add_argument("--batch-apply", type=int, default=0,
                     help="only build the mixed batch of --batch-bodies bodies and time this many matvecs "
                          "(6 rigid-mode right-hand sides each; for profiling the batch kernels)")
@@ -128,10 +131,10 @@ def allmax(ws, v):
     return float(t.item())
 
 
-def build(nk, w, precision):
+def build(nk, w, precision, m2l="auto"):
     NN = nk.nearestMatrix(w["coarse"], w["fine"])
     tree = nk.OcTree(w["coarse"], w["coarse"], nodeCapacity=w["cap"], nearest=1, finePoints=w["fine"], NN=NN)
-    fmm = nk.KIFMM(tree, [w["eps"], w["mu"]], precision=precision)
+    fmm = nk.KIFMM(tree, [w["eps"], w["mu"]], precision=precision, m2l=m2l)
     fmm.autotune(1)  # pair-kernel tile per launch group (part of the set-up)
     return NN, tree, fmm
 
@@ -327,6 +330,63 @@ def gradient_benchmark(torch, nk, args):
     return out
 
 
+def squirmer_benchmark(torch, nk, args):
+    """Two squirmers above a wall at full size (force cube-spheres 12/edge, quadrature
+    48/edge, 200 x 200 wall lattice with NN = I): 7 right-hand sides per eps (unit
+    force and torque components on swimmer 1 with no slip, and the B1/B2 slip of
+    both force-free swimmers), eps in {0.02, 0.01}, GMRES to 1e-6 with the block
+    preconditioner.  Plain FP64 against mixed with FP64 refinement; Richardson
+    extrapolation of the slip solution over eps from both arms."""
+    import scipy.sparse as sp
+    from nnkifmm.workloads import two_squirmers_wall
+    c = two_squirmers_wall()
+    NN = nk.nearestMatrix(c["body"], c["fine"])
+    W = c["wall"]
+    nsw = len(c["centres"])
+    out = {"workload": f"{nsw} squirmers ({len(c['body'])} force / {len(c['fine'])} quadrature points each) above "
+                       f"a {len(W)}-point wall, B1 = 1, B2 = 0.5, nodeCapacity 60, 6 rigid modes + slip per eps, "
+                       f"eps in (0.02, 0.01), GMRES tol 1e-6, block preconditioner"}
+    res = {}
+    for label, prec in [("fp64", "fp64"), ("mixed_refined", "mixed")]:
+        total, iters, sols = 0.0, [], {}
+        for eps in (0.02, 0.01):
+            sw = nk.Swimmers()
+            for x0 in c["centres"]:
+                sw.addSwimmer(c["body"], c["fine"], NN, list(x0), [1, 0, 0, 0, 1, 0], c["slip"], [0, 0, 0], [0, 0, 0])
+            sw.updateBnd(W, W, sp.identity(len(W), format="csr"), np.zeros_like(W))
+            sw.genTree(nodeCapacity=60, nearest=1)
+            sw.genKIFMM([eps, 1.0], GMRES=1, format=2, precision=prec)
+            mob = sw.mobility()
+            slip_rhs = nk.mobilityRHS(sw)
+            rhss = []
+            for k in range(6):
+                r = np.zeros_like(slip_rhs)
+                r[slip_rhs.size - 6 * nsw + k * nsw] = 1.0  # [F_x.. F_y.. F_z.. M_x.. ...] per swimmer
+                rhss.append(r)
+            rhss.append(slip_rhs)
+            mob.solve(rhss[0], tol=1e-6, maxIter=500, precondition=True)  # first-call initialisation
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            xs = []
+            for r in rhss:
+                x, flag, relres, it = mob.solve(r, tol=1e-6, maxIter=500, precondition=True)
+                xs.append(x[-6 * nsw:].copy())
+                iters.append(int(it))
+            torch.cuda.synchronize()
+            total += time.perf_counter() - t0
+            sols[eps] = xs
+        res[label] = sols
+        out[label] = {"solves_per_s": 14 / total, "s_total": total, "gmres_iters_mean": float(np.mean(iters))}
+    err = max(np.linalg.norm(a - b) / np.linalg.norm(b) for e in (0.02, 0.01)
+              for a, b in zip(res["mixed_refined"][e], res["fp64"][e]))
+    rich = [nk.richardson([res[k][0.02][6], res[k][0.01][6]], (0.02, 0.01)) for k in ("mixed_refined", "fp64")]
+    out["rel_err_mixed_vs_fp64"] = float(err)
+    out["richardson_slip_UOm"] = {"mixed_refined": rich[0].tolist(),
+                                  "rel_diff_vs_fp64": float(np.linalg.norm(rich[0] - rich[1]) / np.linalg.norm(rich[1]))}
+    out["speedup_mixed_vs_fp64"] = out["mixed_refined"]["solves_per_s"] / out["fp64"]["solves_per_s"]
+    return out
+
+
 def cpu_baseline_sample(n_force, n_quad, steps=1):
     """The oracle (reference structure, per-node LU, FP64 numpy, 1 thread) on a
     reduced instance of the same workload distribution; returns pts/s."""
@@ -390,7 +450,7 @@ def main():
         return
     t0 = time.time()
     w = matvec_at_scale(args.n_force, args.n_quad)
-    NN, tree, fmm = build(nk, w, args.precision)
+    NN, tree, fmm = build(nk, w, args.precision, args.m2l if args.precision == "mixed" else "auto")
     setup_s = time.time() - t0
     stats = fmm.stats()
     fin = torch.tensor(w["forces"], device="cuda").contiguous()
@@ -497,6 +557,8 @@ def main():
         line["mobility_solves"] = solve_benchmarks(torch, nk, args)
     if rank == 0 and not args.no_gradient:
         line["gradient"] = gradient_benchmark(torch, nk, args)
+    if rank == 0 and not args.no_squirmers:
+        line["squirmers"] = squirmer_benchmark(torch, nk, args)
     if rank == 0 and not args.no_cpu_baseline:
         v, s, nodes = cpu_baseline_sample(1500, 6000)
         line["cpu_baseline"] = {"value": v, "unit": "pts/s", "cores": 1, "kind": "port",

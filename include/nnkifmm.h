@@ -131,6 +131,9 @@ typedef struct nnk_solve_info {
 
 /* ------------------------------------------------------------ context -- */
 int nnk_ctx_create(int32_t device, nnk_ctx** out);
+/* Releases the caller's handle.  Trees, FMMs and batches made from the
+ * context hold it too, so handles may be destroyed in any order: the context
+ * and its stream go with the last of them. */
 int nnk_ctx_destroy(nnk_ctx* ctx);
 /* Use this stream (a cudaStream_t) for all later work on the context. */
 int nnk_ctx_set_stream(nnk_ctx* ctx, void* stream);
@@ -328,6 +331,13 @@ int nnk_batch_set_refinement(nnk_batch* batch, int32_t fp64, int32_t max_outer, 
 /* Replay each matvec from a CUDA graph captured on first use (default on;
  * off while profiling).  enable = 0 launches the kernels one by one. */
 int nnk_batch_use_graphs(nnk_batch* batch, int32_t enable);
+/* Deflation by body (default on): once every right-hand side of a body has
+ * converged, its tree drops out of the forest FMM for the rest of the solve
+ * (its kernels return at once), so a batch costs the sum of its bodies'
+ * iterations rather than the slowest body's count times the batch.  The
+ * solution is bitwise the same either way; enable = 0 evaluates every tree
+ * in every matvec. */
+int nnk_batch_set_deflation(nnk_batch* batch, int32_t enable);
 /* Total FMM matvecs issued so far (inner and outer). */
 int nnk_batch_matvecs(const nnk_batch* batch, int64_t* count);
 /* Per-phase CUDA-event timing of the batch's FMM passes, as

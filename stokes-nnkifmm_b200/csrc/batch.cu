@@ -18,9 +18,11 @@ struct ChunkD {
   int seg;
 };
 
-// h[seg * ldh + i] += sum over the chunk of V_i * w (i = blockIdx.y)
-__global__ void seg_dot_kernel(const double* __restrict__ V, long long n, const double* __restrict__ w,
-                               const ChunkD* __restrict__ chunks, double* __restrict__ h, int ldh) {
+// part[i * nchunks + chunk] = sum over the chunk of V_i * w (i = blockIdx.y),
+// in a fixed order; seg_dot_sum_kernel adds a segment's chunks in order, so
+// the dot products (and the whole solve) do not depend on scheduling.
+__global__ void seg_dot_part_kernel(const double* __restrict__ V, long long n, const double* __restrict__ w,
+                                    const ChunkD* __restrict__ chunks, double* __restrict__ part, int nchunks) {
   const ChunkD c = chunks[blockIdx.x];
   const int i = blockIdx.y;
   const double* v = V + (size_t)i * n;
@@ -33,8 +35,19 @@ __global__ void seg_dot_kernel(const double* __restrict__ V, long long n, const 
   if (threadIdx.x == 0) {
     double t = 0;
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
-    atomicAdd(&h[(size_t)c.seg * ldh + i], t);
+    part[(size_t)i * nchunks + blockIdx.x] = t;
   }
+}
+
+// h[seg * ldh + i] += sum of the segment's chunk partials, in chunk order
+__global__ void seg_dot_sum_kernel(const double* __restrict__ part, int nchunks, const int* __restrict__ cfirst,
+                                   int S, int nvec, double* __restrict__ h, int ldh) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)S * nvec) return;
+  const int s = (int)(e % S), i = (int)(e / S);
+  double t = 0;
+  for (int c = cfirst[s]; c < cfirst[s + 1]; ++c) t += part[(size_t)i * nchunks + c];
+  h[(size_t)s * ldh + i] += t;
 }
 
 // w -= sum_{i<k} V_i h[seg][i] (sign = -1), or x += sum V_i y[seg][i] (sign = +1)
@@ -135,9 +148,14 @@ SegGmres::SegGmres(nnk_ctx* ctx, const std::vector<int64_t>& off) : ctx_(ctx), o
   S_ = (int)off.size() - 1;
   n_ = off.back();
   std::vector<ChunkD> ch;
-  for (int s = 0; s < S_; ++s)
+  std::vector<int32_t> cf(S_ + 1, 0);
+  for (int s = 0; s < S_; ++s) {
+    cf[s] = (int32_t)ch.size();
     for (int64_t a = off[s]; a < off[s + 1]; a += kChunk)
       ch.push_back(ChunkD{a, (int)std::min<int64_t>(kChunk, off[s + 1] - a), s});
+  }
+  cf[S_] = (int32_t)ch.size();
+  cfirst_.upload(cf, ctx_->stream);
   nchunks_ = (int)ch.size();
   std::vector<Chunk> c2(ch.size());
   std::memcpy(c2.data(), ch.data(), ch.size() * sizeof(ChunkD));
@@ -147,7 +165,15 @@ SegGmres::SegGmres(nnk_ctx* ctx, const std::vector<int64_t>& off) : ctx_(ctx), o
 
 void SegGmres::seg_dots(const double* V, int nvec, const double* w, double* h, int ldh) {
   if (nchunks_ == 0 || nvec == 0) return;
-  seg_dot_kernel<<<dim3(nchunks_, nvec), 256, 0, ctx_->stream>>>(V, n_, w, (const ChunkD*)chunks_.p, h, ldh);
+  cudaStream_t st = ctx_->stream;
+  const size_t need = (size_t)nvec * nchunks_;
+  if (need > part_.n) {
+    NNK_CUDA(cudaStreamSynchronize(st));  // the old buffer may still be read
+    part_.alloc(std::max(need, 2 * part_.n));
+  }
+  seg_dot_part_kernel<<<dim3(nchunks_, nvec), 256, 0, st>>>(V, n_, w, (const ChunkD*)chunks_.p, part_.p, nchunks_);
+  NNK_CHECK_LAUNCH();
+  seg_dot_sum_kernel<<<blocks_for((int64_t)S_ * nvec), 256, 0, st>>>(part_.p, nchunks_, cfirst_.p, S_, nvec, h, ldh);
   NNK_CHECK_LAUNCH();
 }
 
@@ -175,7 +201,22 @@ void SegGmres::solve(const Op& op, const double* b, double* x, const std::vector
   int m = restart > 0 ? std::min(restart, maxit) : maxit;
   m = (int)std::max<int64_t>(1, std::min<int64_t>(m, maxlen));
   const int ldh = m + 1;
-  DBuf<double> V((size_t)(m + 1) * n), w(n), r(n), scal(S), act(S);
+  // The Krylov basis grows on demand (doubling, up to m + 1 vectors): a batch
+  // of tens of millions of unknowns that converges in a few dozen steps must
+  // not hold maxit + 1 vectors.
+  int vcap = std::min(m + 1, 16);
+  DBuf<double> V((size_t)vcap * n), w(n), r(n), scal(S), act(S);
+  auto reserve = [&](int need) {
+    if (need <= vcap) return;
+    int nc = vcap;
+    while (nc < need) nc = std::min(m + 1, 2 * nc);
+    DBuf<double> V2((size_t)nc * n);
+    // stream order: the copy follows every step already enqueued on V
+    NNK_CUDA(cudaMemcpyAsync(V2.p, V.p, (size_t)vcap * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    NNK_CUDA(cudaStreamSynchronize(st));
+    V = std::move(V2);
+    vcap = nc;
+  };
   // per step: [pass-1 h (S x ldh) | pass-2 h (S x ldh) | ||w||^2 (S)], two slots
   const size_t slot = 2 * (size_t)S * ldh + S;
   DBuf<double> hdev(2 * slot);
@@ -197,6 +238,18 @@ void SegGmres::solve(const Op& op, const double* b, double* x, const std::vector
   } ef{ev};
 
   info.assign(S, nnk_solve_info{0, 0, 0.0});
+  struct ActiveReset {
+    const std::function<void(const std::vector<char>&)>& f;
+    int S;
+    ~ActiveReset() {
+      if (f) {
+        try {
+          f(std::vector<char>(S, 1));
+        } catch (...) {
+        }
+      }
+    }
+  } active_reset{on_active, S};
   NNK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), st));
   // ||b_s||
   std::vector<double> nb(S, 0.0), beta(S, 0.0), relres(S, 1.0);
@@ -218,6 +271,7 @@ void SegGmres::solve(const Op& op, const double* b, double* x, const std::vector
       Y((size_t)S * ldh), hact(S), hb2(S);
   std::vector<int> k_of(S, 0);
   auto enqueue_step = [&](int j) {
+    reserve(j + 2);  // reads V_0..V_j, writes V_{j+1}
     double* hs = hdev.p + (j & 1) * slot;
     double* vj = V.p + (size_t)j * n;
     op(vj, w.p);
@@ -249,6 +303,7 @@ void SegGmres::solve(const Op& op, const double* b, double* x, const std::vector
       g[(size_t)s * ldh] = beta[s];
     }
     if (nact == 0) break;
+    if (on_active) on_active(active);
     NNK_CUDA(cudaMemcpyAsync(act.p, hact.data(), S * sizeof(double), cudaMemcpyHostToDevice, st));
     NNK_CUDA(cudaMemcpyAsync(scal.p, hb2.data(), S * sizeof(double), cudaMemcpyHostToDevice, st));
     seg_normalize_kernel<<<nchunks_, 256, 0, st>>>(r.p, scal.p, act.p, chunks, V.p);
@@ -301,7 +356,10 @@ void SegGmres::solve(const Op& op, const double* b, double* x, const std::vector
         break;
       }
       // segments that stopped produce zero vectors from the next step on
-      if (changed) NNK_CUDA(cudaMemcpyAsync(act.p, hact.data(), S * sizeof(double), cudaMemcpyHostToDevice, st));
+      if (changed) {
+        NNK_CUDA(cudaMemcpyAsync(act.p, hact.data(), S * sizeof(double), cudaMemcpyHostToDevice, st));
+        if (on_active) on_active(active);
+      }
     }
     // y_s = R_s^-1 g_s, x += V y
     std::fill(Y.begin(), Y.end(), 0.0);
@@ -335,6 +393,7 @@ void SegGmres::solve(const Op& op, const double* b, double* x, const std::vector
       if (done) break;
     }
     // explicit residuals r = b - A x (MATLAB gmres confirms convergence this way)
+    if (on_active) on_active(live);
     op(x, w.p);
     ++matvecs_;
     dev_axpby(ctx_, 1.0, b, -1.0, w.p, r.p, n);
@@ -538,7 +597,16 @@ void BatchMobility::solve_plain(const double* rhs, double* x, const nnk_solve_pa
                                 std::vector<nnk_solve_info>& info) {
   SegGmres g(ctx_, off_);
   SegGmres::Op op = [&](const double* in, double* out) { apply(in, out); };
+  // bodies whose systems all converged drop out of the forest FMM
+  if (deflate_) g.on_active = [&](const std::vector<char>& a) { fmm_->set_active_trees(body_flags(a).data()); };
   g.solve(op, rhs, x, tol, sp.maxit, sp.restart, act, info, /*confirm=*/!ref64_);
+}
+
+std::vector<char> BatchMobility::body_flags(const std::vector<char>& systems) const {
+  std::vector<char> on(B_, 0);
+  for (int s = 0; s < S_; ++s)
+    if (systems[s]) on[s / R_] = 1;
+  return on;
 }
 
 void BatchMobility::solve(const double* rhs, double* x, const nnk_solve_params& sp, nnk_solve_info* info) {
@@ -574,10 +642,17 @@ void BatchMobility::solve(const double* rhs, double* x, const nnk_solve_params& 
     solve_plain(r.p, d.p, sp, itol, act, inf);
     for (int s = 0; s < S_; ++s) out[s].iters += inf[s].iters;
     dev_axpby(ctx_, 1.0, x, 1.0, d.p, x, n_);
+    // the FP64 residual of bodies with no system solved this round is the
+    // previous one (their x did not change): those trees are skipped and
+    // their relres kept
+    const std::vector<char> bon = deflate_ ? body_flags(act) : std::vector<char>(B_, 1);
+    ref64_->set_active_trees(bon.data());
     apply_with(*ref64_, x, ax.p);
+    ref64_->set_active_trees(nullptr);
     dev_axpby(ctx_, 1.0, rhs, -1.0, ax.p, r.p, n_);
     const std::vector<double> rn = seg_norms(r.p);
-    for (int s = 0; s < S_; ++s) relres[s] = nb[s] > 0 ? rn[s] / nb[s] : 0.0;
+    for (int s = 0; s < S_; ++s)
+      if (bon[s / R_]) relres[s] = nb[s] > 0 ? rn[s] / nb[s] : 0.0;
   }
   for (int s = 0; s < S_; ++s) {
     out[s].relres = relres[s];

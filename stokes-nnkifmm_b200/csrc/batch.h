@@ -43,6 +43,11 @@ class SegGmres {
              const std::vector<char>& solve, std::vector<nnk_solve_info>& info, bool confirm = true);
   int64_t matvecs() const { return matvecs_; }
   std::vector<double> norms(const double* v);  // ||v_s|| per segment
+  // Called with the segments whose op outputs the next calls use (1) and
+  // those whose outputs are ignored (0), before the calls that change; with
+  // all 1 when solve returns.  The op may skip the work of the 0 segments,
+  // provided their outputs stay finite.
+  std::function<void(const std::vector<char>& active)> on_active;
 
  private:
   struct Chunk {
@@ -56,6 +61,8 @@ class SegGmres {
   int S_;
   int64_t n_;
   DBuf<Chunk> chunks_;
+  DBuf<int32_t> cfirst_;  // per segment: first chunk (S + 1)
+  DBuf<double> part_;     // per (vector, chunk) partial dot products
   int nchunks_ = 0;
   int64_t matvecs_ = 0;
 };
@@ -77,12 +84,15 @@ class BatchMobility {
   Fmm* ref64() { return ref64_.get(); }
   // Replay each FMM's matvec (all bodies, all right-hand sides, B and BT
   // blocks: about 50 launches) from a CUDA graph captured on first use.
+  void set_deflation(bool on) { deflate_ = on; }
   void use_graphs(bool on);
   int64_t matvecs() const { return matvecs_; }
 
  private:
   void apply_with(Fmm& f, const double* x, double* y);
   void apply_raw(Fmm& f, const double* x, double* y);
+  std::vector<char> body_flags(const std::vector<char>& systems) const;  // any system of the body set
+  bool deflate_ = true;
   void solve_plain(const double* rhs, double* x, const nnk_solve_params& sp, const std::vector<double>& tol,
                    const std::vector<char>& act, std::vector<nnk_solve_info>& info);
 

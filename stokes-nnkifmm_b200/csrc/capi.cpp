@@ -47,6 +47,18 @@ int fail(nnk_ctx* ctx, int code, const std::string& msg) {
   catch (const std::exception& e) { return fail(ctx, NNK_E_ARG, e.what()); } \
   return NNK_OK;
 
+void ctx_retain(nnk_ctx* c) { c->refs.fetch_add(1, std::memory_order_relaxed); }
+
+void ctx_release(nnk_ctx* c) {
+  if (c->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+  if (c->has_gpu && c->own_stream && c->stream) {
+    cudaSetDevice(c->device);
+    cudaStreamDestroy(c->stream);
+    cudaGetLastError();  // an error here must not surface at a later call's launch check
+  }
+  delete c;
+}
+
 void need_gpu(nnk_ctx* ctx) {
   if (!ctx->has_gpu) throw nnk::Error(NNK_E_CUDA, "no CUDA device available: the FMM runs only on the GPU");
   NNK_CUDA(cudaSetDevice(ctx->device));
@@ -104,8 +116,7 @@ int nnk_ctx_create(int32_t device, nnk_ctx** out) {
 
 int nnk_ctx_destroy(nnk_ctx* ctx) {
   if (!ctx) return NNK_E_ARG;
-  if (ctx->has_gpu && ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
-  delete ctx;
+  ctx_release(ctx);
   return NNK_OK;
 }
 
@@ -183,6 +194,7 @@ int nnk_tree_build(nnk_ctx* ctx, const double* pot, int64_t n_pot, const double*
   const int rc = nnk::build_tree(pot, n_pot, tgt, n_tgt, fine, q, nn_rowptr, nn_col, nn_val, p, t->t, msg, gpu);
   if (rc != NNK_OK) return fail(ctx, rc, msg);
   *out = t.release();
+  ctx_retain(ctx);
   API_CATCH(ctx)
 }
 
@@ -243,7 +255,10 @@ int nnk_tree_export_list(const nnk_tree* tree, int32_t which, int64_t* offsets, 
 }
 
 int nnk_tree_destroy(nnk_tree* tree) {
+  if (!tree) return NNK_OK;
+  nnk_ctx* c = tree->ctx;
   delete tree;
+  ctx_release(c);
   return NNK_OK;
 }
 
@@ -266,6 +281,7 @@ int nnk_fmm_create(nnk_ctx* ctx, const nnk_tree* tree, const nnk_fmm_params* par
   f->tree = tree;
   f->f.reset(new nnk::Fmm(ctx, &tree->t, p));
   *out = f.release();
+  ctx_retain(ctx);
   API_CATCH(ctx)
 }
 
@@ -404,8 +420,11 @@ int nnk_fmm_profile_read(nnk_fmm* fmm, double* ms, int64_t* launches) {
 
 int nnk_fmm_destroy(nnk_fmm* fmm) {
   if (!fmm) return NNK_E_ARG;
-  if (fmm->ctx && fmm->ctx->has_gpu) cudaSetDevice(fmm->ctx->device);
+  nnk_ctx* c = fmm->ctx;
+  if (c->has_gpu) cudaSetDevice(c->device);
   delete fmm;
+  if (c->has_gpu) cudaGetLastError();  // destroy errors are not reported
+  ctx_release(c);
   return NNK_OK;
 }
 
@@ -602,6 +621,7 @@ int nnk_batch_create(nnk_ctx* ctx, int32_t nbodies, nnk_tree* const* trees, cons
   bt->ctx = ctx;
   bt->m.reset(new nnk::BatchMobility(ctx, bodies, p, nrhs));
   *out = bt.release();
+  ctx_retain(ctx);
   API_CATCH(ctx)
 }
 
@@ -665,6 +685,12 @@ int nnk_batch_use_graphs(nnk_batch* batch, int32_t enable) {
   API_CATCH(ctx)
 }
 
+int nnk_batch_set_deflation(nnk_batch* batch, int32_t enable) {
+  if (!batch) return NNK_E_ARG;
+  batch->m->set_deflation(enable != 0);
+  return NNK_OK;
+}
+
 int nnk_batch_matvecs(const nnk_batch* batch, int64_t* count) {
   if (!batch || !count) return NNK_E_ARG;
   *count = batch->m->matvecs();
@@ -692,7 +718,12 @@ int nnk_batch_profile_read(nnk_batch* batch, int32_t which, double* ms, int64_t*
 }
 
 int nnk_batch_destroy(nnk_batch* batch) {
+  if (!batch) return NNK_OK;
+  nnk_ctx* c = batch->ctx;
+  if (c->has_gpu) cudaSetDevice(c->device);
   delete batch;
+  if (c->has_gpu) cudaGetLastError();
+  ctx_release(c);
   return NNK_OK;
 }
 

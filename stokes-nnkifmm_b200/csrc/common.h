@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -72,4 +73,7 @@ struct nnk_ctx {
   bool own_stream = false;
   std::string last_error;
   bool has_gpu = false;
+  // the caller's handle plus one per tree, FMM and batch made from it: the
+  // context (and its stream) goes when the last of them is destroyed
+  std::atomic<int> refs{1};
 };

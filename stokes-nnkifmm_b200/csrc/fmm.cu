@@ -99,6 +99,44 @@ Fmm::Fmm(nnk_ctx* ctx, const HostTree* tree, const FmmParams& p) : ctx_(ctx), t_
   build_points();
   build_tasks();
   build_operators();
+  if (t_->groups() > 1) {
+    // tree mask of a forest, all trees on; allocated here because applies
+    // may be captured into CUDA graphs that read it by address
+    cudaStream_t st = ctx_->stream;
+    std::vector<int32_t> tl(t_->tgt_row.size(), 0);
+    for (int32_t i = 0; i < N_; ++i)
+      for (int64_t k = t_->tgt_start[i]; k < t_->tgt_start[i + 1]; ++k) tl[k] = i;
+    tgt_leaf_.upload(tl, st);
+    node_tree_.upload(t_->group, st);
+    tree_on_host_.assign(t_->groups(), 1);
+    tree_on_.upload(tree_on_host_, st);
+    node_on_.upload(std::vector<int32_t>(N_, 1), st);
+    NNK_CUDA(cudaStreamSynchronize(st));
+  }
+}
+
+namespace {
+__global__ void expand_tree_mask_kernel(int n, const int32_t* __restrict__ node_tree,
+                                        const int32_t* __restrict__ tree_on, int32_t* __restrict__ node_on) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) node_on[i] = tree_on[node_tree[i]];
+}
+}  // namespace
+
+void Fmm::set_active_trees(const char* on) {
+  if (!node_on_.p) return;  // a single tree: always evaluated
+  bool same = true;
+  for (size_t g = 0; g < tree_on_host_.size(); ++g) {
+    const int32_t v = on ? (on[g] ? 1 : 0) : 1;
+    same = same && tree_on_host_[g] == v;
+    tree_on_host_[g] = v;
+  }
+  if (same) return;
+  cudaStream_t st = ctx_->stream;
+  NNK_CUDA(cudaMemcpyAsync(tree_on_.p, tree_on_host_.data(), tree_on_host_.size() * sizeof(int32_t),
+                           cudaMemcpyHostToDevice, st));
+  expand_tree_mask_kernel<<<(N_ + 255) / 256, 256, 0, st>>>(N_, node_tree_.p, tree_on_.p, node_on_.p);
+  NNK_CHECK_LAUNCH();
 }
 
 Fmm::~Fmm() {
@@ -300,7 +338,7 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
     for (int32_t n : t.by_level[L]) {
       const bool leaf = t.child0[n] < 0;
       if (leaf && !(*r.src_leaf)[n]) continue;
-      TaskD tk{dnB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
+      TaskD tk{dnB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0, n, 0};
       if (leaf) {
         pairs_up += (int64_t)P_ * src_seg(n);
       } else {
@@ -328,7 +366,7 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
   for (int L = 1; L <= maxl_; ++L) {
     ts.down_nov[L].first = (int64_t)tasks.size();
     for (int32_t n : t.by_level[L]) {
-      TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
+      TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0, n, 0};
       for (int64_t k = r.X->off[n]; k < r.X->off[n + 1]; ++k) src_seg(r.X->idx[k]);
       if (t.level[n] >= 2) segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
       tk.nseg = (int)segs.size() - tk.seg0;
@@ -339,7 +377,7 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
   for (int L = 1; L <= maxl_; ++L) {
     ts.down[L].first = (int64_t)tasks.size();
     for (int32_t n : t.by_level[L]) {
-      TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0};
+      TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0, n, 0};
       for (int64_t k = r.V->off[n]; k < r.V->off[n + 1]; ++k) {
         segs.push_back(SegD{upB + (long long)P_ * r.V->idx[k], P_, 0});
         pairs_down += (int64_t)P_ * P_;
@@ -361,7 +399,7 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
     if (!(*r.tgt_leaf)[i]) continue;
     const int nt = (int)(tr[i + 1] - tr[i]);
     if (nt == 0) continue;
-    TaskD tk{tr[i], tr[i], nt, (int)segs.size(), 0, 0};
+    TaskD tk{tr[i], tr[i], nt, (int)segs.size(), 0, 0, i, 0};
     for (int64_t k = r.U->off[i]; k < r.U->off[i + 1]; ++k) {
       const int64_t s = src_seg(r.U->idx[k]);
       pairs_leaf += (int64_t)nt * s;
@@ -487,7 +525,7 @@ void Fmm::split_tasks(TaskSet& ts, std::vector<TaskD>& tasks, std::vector<SegD>&
         c.nseg = (int)ns.size() - c.seg0;
         nt.push_back(c);
       }
-      reds.push_back(RedD{r.out, pbase, r.ntgt, (int)k});
+      reds.push_back(RedD{r.out, pbase, r.ntgt, (int)k, r.node, 0});
       pbase += k * r.ntgt;
     }
     g.first = first;
@@ -511,13 +549,15 @@ void Fmm::run_group(const TaskSet& ts, const TaskGroup& g, const Real* spos, con
   if (g.count == 0) return;
   cudaStream_t st = ctx_->stream;
   Real* partial = std::is_same<Real, double>::value ? (Real*)partial64_.p : (Real*)partial32_.p;
+  const int* na = &ts == &fwd_ ? nact() : nullptr;  // the tree mask applies to the matvec only
   phase(phase_id, [&] {
     launch_p2p<Real>(ts.tasks.p + g.first, (int)g.count, ts.segs.p, spos, sstr, tpos, out, partial, e2, scale, st,
-                     accumulate, R, g.bs);
+                     accumulate, R, g.bs, na);
   });
   if (g.red_count)
-    phase(phase_id,
-          [&] { launch_reduce<Real>(ts.reds.p + g.red_first, (int)g.red_count, partial, out, accumulate, st, R); });
+    phase(phase_id, [&] {
+      launch_reduce<Real>(ts.reds.p + g.red_first, (int)g.red_count, partial, out, accumulate, st, R, na);
+    });
 }
 
 // Operator index of every (tree, level): one per distinct box width.
@@ -702,6 +742,7 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
   if (tm && R != 1) throw Error(NNK_E_STATE, "tensor-core M2L takes one right-hand side per pass");
   if (tm && m2l_.h_err && *m2l_.h_err)
     throw Error(NNK_E_TIMEOUT, "tensor-core M2L gave up a bounded wait in an earlier call");
+  const int* na = &ts == &fwd_ ? nact() : nullptr;
   // upward pass
   for (int L = maxl_; L >= 1; --L) {
     if (ts.up[L].count == 0) continue;
@@ -709,7 +750,7 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     const int64_t nt = ts.up_toff[L + 1] - ts.up_toff[L];
     phase(NNK_PHASE_UP_C2E, [&] {
       launch_c2e<Real>(ops_.p, n, 0, ts.up_tiles.p + ts.up_toff[L], (int)nt, ts.up_nodes.p, check, str, regionA, P_,
-                       R, st, tm ? m2l_.src.p : nullptr, m2l_.NP, c2e_part_.p, c2e_part_.n);
+                       R, st, tm ? m2l_.src.p : nullptr, m2l_.NP, c2e_part_.p, c2e_part_.n, na);
     });
   }
   // downward pass
@@ -721,7 +762,7 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
   if (fm) {
     // M2L of every level at once in Fourier space
     NNK_CUDA(cudaMemsetAsync(check, 0, sizeof(Real) * (size_t)N_ * n * R, st));
-    phase(NNK_PHASE_M2L, [&] { launch_fft_m2l(fft_, (const float*)str, regionA, R, (float*)check, st); });
+    phase(NNK_PHASE_M2L, [&] { launch_fft_m2l(fft_, (const float*)str, regionA, R, (float*)check, st, na); });
   }
   const std::vector<TaskGroup>& dgroups = (tm || fm) ? ts.down_nov : ts.down;
   for (int L = 1; L <= maxl_; ++L) {
@@ -730,7 +771,7 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     const int64_t nt = dn_toff_[L + 1] - dn_toff_[L];
     phase(NNK_PHASE_DOWN_C2E, [&] {
       launch_c2e<Real>(ops_.p, n, 1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str,
-                       regionA + (int64_t)P_ * N_, P_, R, st, nullptr, 0, c2e_part_.p, c2e_part_.n);
+                       regionA + (int64_t)P_ * N_, P_, R, st, nullptr, 0, c2e_part_.p, c2e_part_.n, na);
     });
   }
 }
@@ -750,8 +791,9 @@ void Fmm::apply_impl(const double* d_in, const IoMap& in, double* d_out, const I
   far_field<Real>(fwd_, pos, str, E_, R);
   // leaf stage
   run_group<Real>(fwd_, fwd_.leaf, pos, str, tpos, vel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS, R);
-  phase(NNK_PHASE_SCATTER,
-        [&] { launch_scatter<Real>((int64_t)t.tgt_row.size(), trow_.p, vel, out, k0, R, d_out, st); });
+  phase(NNK_PHASE_SCATTER, [&] {
+    launch_scatter<Real>((int64_t)t.tgt_row.size(), trow_.p, vel, out, k0, R, d_out, st, tgt_leaf_.p, nact());
+  });
 }
 
 // Transpose: the same passes on the same tree with the roles of the point

@@ -27,6 +27,8 @@ struct TaskD {
   int seg0;
   int nseg;
   int partial;    // 1: a piece of a split task, writes its partial-sum slot at `out`
+  int node;       // the node whose expansion or leaf targets the task computes
+  int pad;
 };
 // Sum of the k partial-sum slots of a split task, added in a fixed order.
 struct RedD {
@@ -34,6 +36,8 @@ struct RedD {
   long long pbase;  // first partial slot; piece i uses pbase + i * ntgt
   int ntgt;
   int k;
+  int node;
+  int pad;
 };
 struct SegD {
   long long start;  // first source in the unified arrays
@@ -131,6 +135,10 @@ class Fmm {
   // launch, from {64, 128, 256} (FP64: {64, 128}), for passes of nrhs
   // right-hand sides.  Returns the total pair-kernel time before and after.
   std::pair<double, double> autotune(int nrhs);
+  // Trees of the forest the matvec evaluates (flags per tree, nullptr: all).
+  // The kernels of a masked tree return at once and its output rows are
+  // zero; the transpose and the gradients always evaluate every tree.
+  void set_active_trees(const char* on);
   // Same, but over the p=4 surfaces (computeVelSparse).
   Fmm& sparse();
   void reduced_apply(const double* d_in, double* d_out, int layout);
@@ -258,6 +266,11 @@ class Fmm {
   int64_t launches_[NNK_NUM_PHASES] = {0};
   cudaEvent_t event();
   std::unique_ptr<Fmm> sparse_;
+  // tree mask of the matvec (forests only): per tree, per node (expanded on
+  // the device), and the leaf of each sorted target
+  DBuf<int32_t> tree_on_, node_on_, node_tree_, tgt_leaf_;
+  std::vector<int32_t> tree_on_host_;
+  const int* nact() const { return node_on_.p; }
 };
 
 }  // namespace nnk

@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
                                                  const Real* __restrict__ sstr,
                                                  const Real* __restrict__ tpos, Real* __restrict__ out_main,
                                                  Real* __restrict__ partial, Real e2, Real scale,
-                                                 int accumulate_main) {
+                                                 int accumulate_main, const int* __restrict__ nact = nullptr) {
   using T4 = typename Vec4T<Real>::t4;
   using T2 = typename Vec4T<Real>::t2;
   __shared__ T4 s4[BS];
@@ -128,6 +128,7 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
   __shared__ int seg_end[BS];  // inclusive prefix sums of the counts
   __shared__ Real red[3 * BS];
   const TaskD tk = tasks[blockIdx.x];
+  if (nact && !nact[tk.node]) return;  // a tree of the forest whose systems all converged
   const int tid = threadIdx.x;
   Real* __restrict__ out = tk.partial ? partial : out_main;
   const int accumulate = tk.partial ? 0 : accumulate_main;
@@ -291,7 +292,8 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
                                                        const Real* __restrict__ sstr,
                                                        const Real* __restrict__ tpos, Real* __restrict__ out_main,
                                                        Real* __restrict__ partial, Real e2, Real scale,
-                                                       int accumulate_main, const Real* __restrict__ tw = nullptr) {
+                                                       int accumulate_main, const Real* __restrict__ tw = nullptr,
+                                                       const int* __restrict__ nact = nullptr) {
   using T4 = typename Vec4T<Real>::t4;
   constexpr int C = 3 * R;
   __shared__ T4 sp[BS];
@@ -301,6 +303,7 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
   __shared__ int seg_end[BS];
   __shared__ Real red[C][BS];
   const TaskD tk = tasks[blockIdx.x];
+  if (nact && !nact[tk.node]) return;
   const int tid = threadIdx.x;
   Real* __restrict__ out = tk.partial ? partial : out_main;
   const int accumulate = tk.partial ? 0 : accumulate_main;
@@ -475,10 +478,10 @@ constexpr bool p2p_fits() {
 template <typename Real, int BS, int R>
 inline void launch_multi(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
                          const Real* tpos, Real* out, Real* partial, Real e2, Real scale, cudaStream_t st,
-                         int accumulate) {
+                         int accumulate, const int* nact) {
   if constexpr (p2p_fits<Real, BS, R>()) {
     p2p_multi_kernel<Real, BS, R><<<ntasks, BS, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
-                                                          accumulate);
+                                                          accumulate, nullptr, nact);
   } else {
     throw Error(NNK_E_ARG, "pair kernel tile too large for shared memory");
   }
@@ -487,22 +490,23 @@ inline void launch_multi(const TaskD* tasks, int ntasks, const SegD* segs, const
 template <typename Real, int BS>
 inline void launch_p2p_bs(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
                           const Real* tpos, Real* out, Real* partial, Real e2, Real scale, cudaStream_t st,
-                          int accumulate, int R) {
+                          int accumulate, int R, const int* nact) {
   switch (R) {
     case 1:
-      p2p_kernel<Real, BS><<<ntasks, BS, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale, accumulate);
+      p2p_kernel<Real, BS><<<ntasks, BS, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale, accumulate,
+                                                  nact);
       break;
     case 2:
-      launch_multi<Real, BS, 2>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate);
+      launch_multi<Real, BS, 2>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, nact);
       break;
     case 3:
-      launch_multi<Real, BS, 3>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate);
+      launch_multi<Real, BS, 3>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, nact);
       break;
     case 4:
-      launch_multi<Real, BS, 4>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate);
+      launch_multi<Real, BS, 4>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, nact);
       break;
     case 6:
-      launch_multi<Real, BS, 6>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate);
+      launch_multi<Real, BS, 6>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, nact);
       break;
     default:
       throw Error(NNK_E_ARG, "pair kernel supports 1, 2, 3, 4 or 6 right-hand sides per launch");
@@ -532,15 +536,15 @@ inline bool p2p_bs_ok(int bs, int R) {
 template <typename Real>
 inline void launch_p2p(const TaskD* tasks, int ntasks, const SegD* segs, const Real* spos, const Real* sstr,
                        const Real* tpos, Real* out, Real* partial, Real e2, Real scale, cudaStream_t st,
-                       int accumulate = 0, int R = 1, int bs = 128) {
+                       int accumulate = 0, int R = 1, int bs = 128, const int* nact = nullptr) {
   if (ntasks == 0) return;
   if (!p2p_bs_ok<Real>(bs, R)) bs = 128;
   if (bs == 64)
-    launch_p2p_bs<Real, 64>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R);
+    launch_p2p_bs<Real, 64>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R, nact);
   else if (bs == 256)
-    launch_p2p_bs<Real, 256>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R);
+    launch_p2p_bs<Real, 256>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R, nact);
   else
-    launch_p2p_bs<Real, 128>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R);
+    launch_p2p_bs<Real, 128>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R, nact);
   NNK_CHECK_LAUNCH();
 }
 
@@ -567,8 +571,9 @@ inline int rhs_chunk(int remaining, int max_rhs) {
 // result does not depend on scheduling.  C = 3 R values per target.
 template <typename Real>
 __global__ void reduce_partials_kernel(const RedD* __restrict__ reds, const Real* __restrict__ partial,
-                                       Real* __restrict__ out, int accumulate, int C) {
+                                       Real* __restrict__ out, int accumulate, int C, const int* __restrict__ nact) {
   const RedD r = reds[blockIdx.x];
+  if (nact && !nact[r.node]) return;
   const int n = C * r.ntgt;
   for (int v = threadIdx.x; v < n; v += blockDim.x) {
     Real s = 0;
@@ -580,9 +585,9 @@ __global__ void reduce_partials_kernel(const RedD* __restrict__ reds, const Real
 
 template <typename Real>
 inline void launch_reduce(const RedD* reds, int nreds, const Real* partial, Real* out, int accumulate,
-                          cudaStream_t st, int R = 1) {
+                          cudaStream_t st, int R = 1, const int* nact = nullptr) {
   if (nreds == 0) return;
-  reduce_partials_kernel<Real><<<nreds, 128, 0, st>>>(reds, partial, out, accumulate, 3 * R);
+  reduce_partials_kernel<Real><<<nreds, 128, 0, st>>>(reds, partial, out, accumulate, 3 * R, nact);
   NNK_CHECK_LAUNCH();
 }
 
@@ -604,13 +609,15 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
                                                   const C2ETile* __restrict__ tiles, const int* __restrict__ nodes,
                                                   const Real* __restrict__ check, Real* __restrict__ dst,
                                                   long long base, int P, int R, float* __restrict__ m2l_dst, int NP,
-                                                  int ksplit, int kper, double* __restrict__ part) {
+                                                  int ksplit, int kper, double* __restrict__ part,
+                                                  const int* __restrict__ nact) {
   constexpr int BM = 64, BN = 64, BK = 16;
   __shared__ double As[BK][BM + 1];
   __shared__ double Bs[BK][BN + 1];
   __shared__ int col_node[BN];
   __shared__ int col_k[BN];
   const C2ETile tl = tiles[blockIdx.y];
+  if (nact && !nact[nodes[tl.first]]) return;  // the nodes of a tile belong to one tree
   const int zch = gridDim.z / ksplit;
   const int split = blockIdx.z / zch, zc = blockIdx.z - split * zch;
   const int kbeg = split * kper, kend = min(n, kbeg + kper);
@@ -719,9 +726,11 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
 template <typename Real>
 __global__ void c2e_reduce_kernel(const C2ETile* __restrict__ tiles, const int* __restrict__ nodes, int n, int R,
                                   int ksplit, int ntiles, const double* __restrict__ part, Real* __restrict__ dst,
-                                  long long base, int P, float* __restrict__ m2l_dst, int NP) {
+                                  long long base, int P, float* __restrict__ m2l_dst, int NP,
+                                  const int* __restrict__ nact) {
   const int tile = blockIdx.y;
   const C2ETile tl = tiles[tile];
+  if (nact && !nact[nodes[tl.first]]) return;
   const int cols = kC2ETileNodes * R;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)cols * n;
        e += (long long)gridDim.x * blockDim.x) {
@@ -755,7 +764,8 @@ inline size_t c2e_part_size(int n, int ntiles, int R) {
 template <typename Real>
 inline void launch_c2e(const double* ops, int n, int trans, const C2ETile* tiles, int ntiles, const int32_t* nodes,
                        const Real* check, Real* dst, int64_t base, int P, int R, cudaStream_t st,
-                       float* m2l_dst = nullptr, int NP = 0, double* part = nullptr, size_t part_n = 0) {
+                       float* m2l_dst = nullptr, int NP = 0, double* part = nullptr, size_t part_n = 0,
+                       const int* nact = nullptr) {
   if (ntiles == 0) return;
   const int zch = (kC2ETileNodes * R + 63) / 64;
   const int blocks = ((n + 63) / 64) * ntiles * zch;
@@ -764,11 +774,12 @@ inline void launch_c2e(const double* ops, int n, int trans, const C2ETile* tiles
   const int kper = ((n + ksplit - 1) / ksplit + 15) / 16 * 16;
   dim3 grid((n + 63) / 64, ntiles, zch * ksplit);
   c2e_kernel<Real><<<grid, 256, 0, st>>>(ops, n, trans, tiles, nodes, check, dst, base, P, R, m2l_dst, NP, ksplit,
-                                         kper, part);
+                                         kper, part, nact);
   NNK_CHECK_LAUNCH();
   if (ksplit > 1) {
     dim3 g2(std::max(1, std::min(64, (kC2ETileNodes * R * n + 255) / 256)), ntiles);
-    c2e_reduce_kernel<Real><<<g2, 256, 0, st>>>(tiles, nodes, n, R, ksplit, ntiles, part, dst, base, P, m2l_dst, NP);
+    c2e_reduce_kernel<Real><<<g2, 256, 0, st>>>(tiles, nodes, n, R, ksplit, ntiles, part, dst, base, P, m2l_dst, NP,
+                                                nact);
     NNK_CHECK_LAUNCH();
   }
 }
@@ -776,20 +787,23 @@ inline void launch_c2e(const double* ops, int n, int trans, const C2ETile* tiles
 // ---------------------------------------------------------------- scatter
 // Sorted-by-leaf velocities back to the reference's target order
 // (downwardPass.m:297-305), in the caller's layout, right-hand sides
-// k0..k0+R-1.
+// k0..k0+R-1.  With a node mask (nact, tnode = leaf of each sorted target),
+// the rows of masked trees are written as zeros.
 template <typename Real>
 __global__ void scatter_kernel(long long nt, const int* __restrict__ row, const Real* __restrict__ vel, IoMap m,
-                               int k0, int R, double* __restrict__ out) {
+                               int k0, int R, double* __restrict__ out, const int* __restrict__ tnode,
+                               const int* __restrict__ nact) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nt) return;
   long long off, cs, rs;
   io_index(m, row[t], off, cs, rs);
+  const bool on = !nact || nact[tnode[t]];
   for (int k = 0; k < R; ++k) {
     const Real* v = vel + 3 * (t * R + k);
     double* o = out + off + (k0 + k) * rs;
-    o[0] = (double)v[0];
-    o[cs] = (double)v[1];
-    o[2 * cs] = (double)v[2];
+    o[0] = on ? (double)v[0] : 0.0;
+    o[cs] = on ? (double)v[1] : 0.0;
+    o[2 * cs] = on ? (double)v[2] : 0.0;
   }
 }
 
@@ -840,9 +854,9 @@ __global__ void origin_sum_kernel(long long norg, const long long* __restrict__ 
 
 template <typename Real>
 inline void launch_scatter(int64_t nt, const int32_t* row, const Real* vel, const IoMap& m, int k0, int R,
-                           double* out, cudaStream_t st) {
+                           double* out, cudaStream_t st, const int32_t* tnode = nullptr, const int* nact = nullptr) {
   if (nt == 0) return;
-  scatter_kernel<Real><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nt, row, vel, m, k0, R, out);
+  scatter_kernel<Real><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nt, row, vel, m, k0, R, out, tnode, nact);
   NNK_CHECK_LAUNCH();
 }
 

@@ -124,7 +124,7 @@ __global__ void fft_spectra_kernel(int G, int res, const double* __restrict__ sl
 template <int RES>
 __global__ void fft_forward_kernel(int G_rt, int res_rt, int P, const int* __restrict__ lat,
                                    const int* __restrict__ src_node, const float* __restrict__ str, long long upbase,
-                                   int R, float2* __restrict__ qhat, int NK) {
+                                   int R, float2* __restrict__ qhat, int NK, const int* __restrict__ nact) {
   extern __shared__ float2 smq[];
   const int res = RES > 0 ? RES : res_rt;
   const int G = RES > 0 ? 2 * RES : G_rt;
@@ -134,6 +134,7 @@ __global__ void fft_forward_kernel(int G_rt, int res_rt, int P, const int* __res
   float2* Y = Z + C * res * res * H;         // [cr][x][ky][kz]  C res G H
   float* g = reinterpret_cast<float*>(Y + C * res * G * H);  // [cr][x][y][z] C res^3
   const int node = src_node[blockIdx.x];
+  if (nact && !nact[node]) return;  // a masked tree of the forest
   const int tid = threadIdx.x, nt = blockDim.x;
   twiddles(tw, G, -1.0);
   for (int e = tid; e < C * r3; e += nt) g[e] = 0.f;
@@ -204,11 +205,14 @@ __global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* 
                                                              const int* __restrict__ vspec,
                                                              const float2* __restrict__ spec,
                                                              const float2* __restrict__ qhat,
-                                                             float2* __restrict__ chat) {
+                                                             float2* __restrict__ chat,
+                                                             const int* __restrict__ tgt_node,
+                                                             const int* __restrict__ nact) {
   constexpr int C = 3 * R;
   const int t = blockIdx.x;
   const int k = blockIdx.y * blockDim.x + threadIdx.x;
   if (k >= NK) return;
+  if (nact && !nact[tgt_node[t]]) return;
   float2 acc[C];
 #pragma unroll
   for (int c = 0; c < C; ++c) acc[c] = make_float2(0.f, 0.f);
@@ -243,7 +247,7 @@ __global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* 
 template <int RES>
 __global__ void fft_inverse_kernel(int G_rt, int res_rt, int P, const int* __restrict__ lat,
                                    const int* __restrict__ tgt_node, const float2* __restrict__ chat, int R,
-                                   float* __restrict__ check, int NK) {
+                                   float* __restrict__ check, int NK, const int* __restrict__ nact) {
   extern __shared__ float2 smc[];
   const int res = RES > 0 ? RES : res_rt;
   const int G = RES > 0 ? 2 * RES : G_rt;
@@ -253,6 +257,7 @@ __global__ void fft_inverse_kernel(int G_rt, int res_rt, int P, const int* __res
   float2* Yv = X + C * res * G * H;   // [cr][x][y][kz]   C res res H
   float* out = reinterpret_cast<float*>(X);  // [cr][x][y][z] (X is dead by then)
   const int node = tgt_node[blockIdx.x];
+  if (nact && !nact[node]) return;
   const int tid = threadIdx.x, nt = blockDim.x;
   twiddles(tw, G, 1.0);
   __syncthreads();
@@ -427,38 +432,44 @@ void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu
   NNK_CUDA(cudaStreamSynchronize(st));
 }
 
-void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float* check, cudaStream_t st) {
+void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float* check, cudaStream_t st,
+                    const int* nact) {
   if (f.ntgt == 0) return;
   if (R > f.Rcap) throw Error(NNK_E_STATE, "Fourier M2L sized for fewer right-hand sides");
   const int G = f.G, res = f.res;
   auto fwd = res == 6 ? fft_forward_kernel<6> : res == 4 ? fft_forward_kernel<4> : fft_forward_kernel<0>;
   auto inv = res == 6 ? fft_inverse_kernel<6> : res == 4 ? fft_inverse_kernel<4> : fft_inverse_kernel<0>;
   fwd<<<f.nsrc, 256, forward_smem(G, res, R), st>>>(G, res, f.P, f.lat.p, f.src_node.p, str, upbase, R, f.qhat.p,
-                                                    f.NK);
+                                                    f.NK, nact);
   NNK_CHECK_LAUNCH();
   dim3 grid(f.ntgt, (f.NK + 127) / 128);
   switch (R) {
     case 1:
-      fft_accumulate_kernel<1><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p);
+      fft_accumulate_kernel<1><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p,
+                                                       f.tgt_node.p, nact);
       break;
     case 2:
-      fft_accumulate_kernel<2><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p);
+      fft_accumulate_kernel<2><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p,
+                                                       f.tgt_node.p, nact);
       break;
     case 3:
-      fft_accumulate_kernel<3><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p);
+      fft_accumulate_kernel<3><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p,
+                                                       f.tgt_node.p, nact);
       break;
     case 4:
-      fft_accumulate_kernel<4><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p);
+      fft_accumulate_kernel<4><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p,
+                                                       f.tgt_node.p, nact);
       break;
     case 6:
-      fft_accumulate_kernel<6><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p);
+      fft_accumulate_kernel<6><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p,
+                                                       f.tgt_node.p, nact);
       break;
     default:
       throw Error(NNK_E_ARG, "Fourier M2L supports 1, 2, 3, 4 or 6 right-hand sides per pass");
   }
   NNK_CHECK_LAUNCH();
   inv<<<f.ntgt, 256, inverse_smem(G, res, R), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, f.chat.p, R, check,
-                                                    f.NK);
+                                                    f.NK, nact);
   NNK_CHECK_LAUNCH();
 }
 

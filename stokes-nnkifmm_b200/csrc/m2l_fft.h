@@ -46,7 +46,9 @@ void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu
                    const std::vector<int>& node_op, int Rmax, FftM2L& f, cudaStream_t st);
 // check[((P * node + p) * R + r) * 3 + c] = M2L result for every node with a
 // V-list (other entries untouched); str holds the up-equivalent densities of
-// node n at str[((upbase + P * n + p) * R + r) * 3 + c].
-void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float* check, cudaStream_t st);
+// node n at str[((upbase + P * n + p) * R + r) * 3 + c].  nact (per node,
+// or nullptr): nodes with nact = 0 are neither transformed nor written.
+void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float* check, cudaStream_t st,
+                    const int* nact = nullptr);
 
 }  // namespace nnk

@@ -113,6 +113,10 @@ extern "C" int nnk_direct_nearest_noalloc(int32_t device, void* stream, const do
     scratch = g_addr[device];
   }
   if (rc == NNK_OK && m > 0) {
+    // the launch check below reads this thread's last runtime error: drop
+    // one left by an earlier call of the library (a destroy function, whose
+    // errors are ignored); a sticky error still shows at the launch
+    (void)cudaGetLastError();
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     nnk::IoMap rows;
     rows.layout = NNK_LAYOUT_ROWS;

@@ -111,6 +111,7 @@ SIGNATURES = {
     "nnk_batch_set_refinement": (_i32, [_vp, _i32, _i32, _f64]),
     "nnk_batch_matvecs": (_i32, [_vp, _pi64]),
     "nnk_batch_use_graphs": (_i32, [_vp, _i32]),
+    "nnk_batch_set_deflation": (_i32, [_vp, _i32]),
     "nnk_batch_profile": (_i32, [_vp, _i32]),
     "nnk_batch_profile_read": (_i32, [_vp, _i32, _vp, _vp]),
     "nnk_batch_destroy": (_i32, [_vp]),

@@ -179,6 +179,11 @@ class BatchMobility:
         """Replay the matvec from a CUDA graph (default) or launch kernel by kernel."""
         L.check(L.lib.nnk_batch_use_graphs(self.h, int(bool(enable))), self.ctx.h, "use_graphs")
 
+    def set_deflation(self, enable=True):
+        """Drop bodies whose right-hand sides all converged out of the forest
+        FMM (default on; the solution is bitwise the same either way)."""
+        L.check(L.lib.nnk_batch_set_deflation(self.h, int(bool(enable))), self.ctx.h, "set_deflation")
+
     def matvecs(self):
         c = C.c_int64()
         L.check(L.lib.nnk_batch_matvecs(self.h, C.byref(c)))

@@ -180,6 +180,7 @@ class Mobility:
         L.check(L.lib.nnk_mob_create(fmm.h, len(sizes), L.ptr(bstart), L.ptr(fstart), L.ptr(rel), L.ptr(frel),
                                      C.byref(h)), fmm.ctx.h, "mobility")
         self.h = h
+        self.fmm = fmm  # the native operator refers to it
         self.ctx = fmm.ctx
         self.n = 3 * fmm.tree.info.num_targets + 6 * len(sizes)
         if getattr(sw, "FMM64", None) is not None:

@@ -52,3 +52,22 @@ def test_batch_without_gpu_fails_loudly():
     f = np.random.default_rng(2).random((120, 3))
     with pytest.raises(nk.NNKError, match="no CUDA device"):
         BatchMobility([(x, f)], [1e-3, 1.0], cap=10, precision="fp64", nrhs=2)
+
+
+def test_context_outlives_its_handles_in_any_order():
+    """A tree keeps its context alive: destroying the context first, then
+    using and destroying the tree, is safe (C ABI, host builder)."""
+    L = nk._lib
+    ctx = ctypes.c_void_p()
+    assert L.lib.nnk_ctx_create(0, ctypes.byref(ctx)) == L.NNK_OK
+    x = np.ascontiguousarray(np.random.default_rng(3).random((200, 3)))
+    params = L.TreeParams(20, 20, 0, 1)
+    tree = ctypes.c_void_p()
+    rc = L.lib.nnk_tree_build(ctx, L.ptr(x), 200, L.ptr(x), 200, None, 0, None, None, None, ctypes.byref(params),
+                              ctypes.byref(tree))
+    assert rc == L.NNK_OK
+    assert L.lib.nnk_ctx_destroy(ctx) == L.NNK_OK
+    info = L.TreeInfo()
+    assert L.lib.nnk_tree_info_get(tree, ctypes.byref(info)) == L.NNK_OK
+    assert info.num_points == 200
+    assert L.lib.nnk_tree_destroy(tree) == L.NNK_OK

@@ -164,3 +164,29 @@ def test_linearity():
     rhs = 2.0 * fmm.computeVel(A) - 3.0 * fmm.computeVel(B)
     # the surface matrices have cond ~2e10, so FP64 rounding shows at ~1e-9
     assert rel(lhs, rhs) < 1e-8
+
+
+def test_fmm_after_its_context_handle_is_destroyed():
+    """Trees and FMMs hold their context: with the caller's context handle
+    destroyed first, the FMM still evaluates (the same result) and the
+    handles can be destroyed afterwards."""
+    import ctypes
+    L = nk._lib
+    g = np.load(os.path.join(GOLDEN, "sphere10_40.npz"))
+    x = np.ascontiguousarray(g["coarse"])
+    n, kp = len(x), [float(g["eps"]), float(g["mu"])]
+    ref = nk.KIFMM(nk.OcTree(x, x, nodeCapacity=int(g["cap"])), kp)
+    f = np.ascontiguousarray(np.random.default_rng(4).standard_normal(3 * n))
+    ctx, tree, fmm = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    assert L.lib.nnk_ctx_create(0, ctypes.byref(ctx)) == L.NNK_OK
+    tp = L.TreeParams(int(g["cap"]), 20, 0, 0)
+    assert L.lib.nnk_tree_build(ctx, L.ptr(x), n, L.ptr(x), n, None, 0, None, None, None, ctypes.byref(tp),
+                                ctypes.byref(tree)) == L.NNK_OK
+    fp = L.FmmParams(kp[0], kp[1], 6, 1, L.PREC_FP64, 0, 0.0)
+    assert L.lib.nnk_fmm_create(ctx, tree, ctypes.byref(fp), ctypes.byref(fmm)) == L.NNK_OK
+    assert L.lib.nnk_ctx_destroy(ctx) == L.NNK_OK
+    out = np.empty(3 * n)
+    assert L.lib.nnk_fmm_apply(fmm, L.ptr(f), L.ptr(out), 1, 1, 0) == L.NNK_OK  # layout rows, host buffers
+    assert np.array_equal(out, ref.computeVel(f).ravel())
+    assert L.lib.nnk_fmm_destroy(fmm) == L.NNK_OK
+    assert L.lib.nnk_tree_destroy(tree) == L.NNK_OK
