@@ -495,13 +495,17 @@ def main():
     pairs = {"up_pairs": stats["pairs_up"], "down_pairs": stats["pairs_down"], "leaf_pairs": stats["pairs_leaf"]}
     if dom == "m2l":
         n3 = 3 * stats["surface_points"]
-        flops = 2.0 * n3 * n3 * stats["m2l_pairs"]
+        rk = stats["m2l_rank"] or n3
+        flops = 2.0 * rk * rk * stats["m2l_pairs"]
         tf32_peak = peaks.get("bf16_tflops", 1590.0) / 2
-        roof = {"kernel": "m2l_tf32_kernel (tcgen05 kind::tf32, TMEM accumulator)", "bound": "tensor",
+        roof = {"kernel": "m2l_img_kernel (tcgen05 kind::tf32, TMEM accumulator)"
+                          + (f" on rank-{rk} compressed operators" if stats["m2l_rank"] else ""),
+                "bound": "tensor",
                 "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": tf32_peak, "unit": "TFLOP/s",
                 "peak_source": "TF32 dense = 1/2 of the measured cuBLAS bf16 burst peak in MEASURED_PEAKS.json"
                                if peaks else "TF32 dense = 1/2 of the fallback bf16 peak",
-                "algorithmic": f"{stats['m2l_pairs']} V pairs x 2 x {n3}^2 flops per step (useful, no padding)",
+                "algorithmic": f"{stats['m2l_pairs']} V pairs x 2 x {rk}^2 flops per step (useful, no padding; "
+                               f"the phase also holds the basis projection and expansion)",
                 "padded_rows_over_useful": stats["m2l_tile_rows"] / max(stats["m2l_pairs"], 1),
                 "launches_per_step": per_step[dom][1], "ms_per_launch": per_step[dom][0] / per_step[dom][1],
                 "traffic": None}

@@ -92,8 +92,10 @@ typedef struct nnk_fmm_params {
   int32_t corona_res;    /* 'coronaRes' (default 6)                            */
   int32_t corona_shells; /* 'coronaShells' (default 1)                         */
   int32_t precision;     /* NNK_PREC_FP64 or NNK_PREC_MIXED                    */
-  int32_t m2l_mode;      /* mixed mode M2L: 0 auto (tensor cores, images when
-                            they fit 8 GiB), 1 tensor cores + streamed images,
+  int32_t m2l_mode;      /* mixed mode M2L: 0 auto (tensor cores on rank-256
+                            compressed operators B C_o B^T when 3P > 256, else
+                            images when they fit 8 GiB), 1 tensor cores +
+                            streamed full images,
                             2 tensor cores + in-kernel operators, 3 FP32 pair
                             kernel (no tensor cores; FP32-rounding accuracy),
                             4 FP32 Fourier-space product (FFT of the surface
@@ -114,6 +116,9 @@ typedef struct nnk_fmm_stats {
   int64_t m2l_tile_rows; /* tensor-core M2L rows processed, padding included     */
   int32_t surface_points;
   int32_t levels;
+  int32_t m2l_rank;     /* compressed tensor-core M2L: rank of the per-level
+                           bases (its GEMMs are m2l_rank square); 0 otherwise */
+  int32_t reserved;
 } nnk_fmm_stats;
 
 /* GMRES options/result (MATLAB gmres(A,b,restart,tol,maxit), x0 = 0). */

@@ -21,10 +21,16 @@ struct ChunkD {
 // part[i * nchunks + chunk] = sum over the chunk of V_i * w (i = blockIdx.y),
 // in a fixed order; seg_dot_sum_kernel adds a segment's chunks in order, so
 // the dot products (and the whole solve) do not depend on scheduling.
+// Segments with active[seg] == 0 (when given) contribute 0 without reading.
 __global__ void seg_dot_part_kernel(const double* __restrict__ V, long long n, const double* __restrict__ w,
-                                    const ChunkD* __restrict__ chunks, double* __restrict__ part, int nchunks) {
+                                    const ChunkD* __restrict__ chunks, double* __restrict__ part, int nchunks,
+                                    const double* __restrict__ active) {
   const ChunkD c = chunks[blockIdx.x];
   const int i = blockIdx.y;
+  if (active && active[c.seg] == 0.0) {
+    if (threadIdx.x == 0) part[(size_t)i * nchunks + blockIdx.x] = 0.0;
+    return;
+  }
   const double* v = V + (size_t)i * n;
   double s = 0;
   for (int k = threadIdx.x; k < c.len; k += blockDim.x) s += v[c.start + k] * w[c.start + k];
@@ -50,11 +56,14 @@ __global__ void seg_dot_sum_kernel(const double* __restrict__ part, int nchunks,
   h[(size_t)s * ldh + i] += t;
 }
 
-// w -= sum_{i<k} V_i h[seg][i] (sign = -1), or x += sum V_i y[seg][i] (sign = +1)
+// w -= sum_{i<k} V_i h[seg][i] (sign = -1), or x += sum V_i y[seg][i] (sign = +1);
+// segments with active[seg] == 0 (when given) are left as they are
 __global__ void seg_axpy_kernel(const double* __restrict__ V, long long n, int k, const double* __restrict__ h,
-                                int ldh, const ChunkD* __restrict__ chunks, double* __restrict__ w, double sign) {
+                                int ldh, const ChunkD* __restrict__ chunks, double* __restrict__ w, double sign,
+                                const double* __restrict__ active) {
   extern __shared__ double hs[];
   const ChunkD c = chunks[blockIdx.x];
+  if (active && active[c.seg] == 0.0) return;
   for (int i = threadIdx.x; i < k; i += blockDim.x) hs[i] = h[(size_t)c.seg * ldh + i];
   __syncthreads();
   for (int e = threadIdx.x; e < c.len; e += blockDim.x) {
@@ -72,7 +81,7 @@ __global__ void seg_normalize_kernel(const double* __restrict__ w, const double*
   const ChunkD c = chunks[blockIdx.x];
   const double q = nrm2[c.seg];
   const double a = (active[c.seg] != 0.0 && q > 0.0) ? 1.0 / sqrt(q) : 0.0;
-  for (int e = threadIdx.x; e < c.len; e += blockDim.x) v[c.start + e] = a * w[c.start + e];
+  for (int e = threadIdx.x; e < c.len; e += blockDim.x) v[c.start + e] = a != 0.0 ? a * w[c.start + e] : 0.0;
 }
 
 __device__ __forceinline__ void cross3(const double* a, const double* b, double* o) {
@@ -163,7 +172,7 @@ SegGmres::SegGmres(nnk_ctx* ctx, const std::vector<int64_t>& off) : ctx_(ctx), o
   chunks_.upload(c2, ctx_->stream);
 }
 
-void SegGmres::seg_dots(const double* V, int nvec, const double* w, double* h, int ldh) {
+void SegGmres::seg_dots(const double* V, int nvec, const double* w, double* h, int ldh, const double* active) {
   if (nchunks_ == 0 || nvec == 0) return;
   cudaStream_t st = ctx_->stream;
   const size_t need = (size_t)nvec * nchunks_;
@@ -171,7 +180,8 @@ void SegGmres::seg_dots(const double* V, int nvec, const double* w, double* h, i
     NNK_CUDA(cudaStreamSynchronize(st));  // the old buffer may still be read
     part_.alloc(std::max(need, 2 * part_.n));
   }
-  seg_dot_part_kernel<<<dim3(nchunks_, nvec), 256, 0, st>>>(V, n_, w, (const ChunkD*)chunks_.p, part_.p, nchunks_);
+  seg_dot_part_kernel<<<dim3(nchunks_, nvec), 256, 0, st>>>(V, n_, w, (const ChunkD*)chunks_.p, part_.p, nchunks_,
+                                                             active);
   NNK_CHECK_LAUNCH();
   seg_dot_sum_kernel<<<blocks_for((int64_t)S_ * nvec), 256, 0, st>>>(part_.p, nchunks_, cfirst_.p, S_, nvec, h, ldh);
   NNK_CHECK_LAUNCH();
@@ -279,12 +289,14 @@ void SegGmres::solve(const Op& op, const double* b, double* x, const std::vector
     NNK_CUDA(cudaMemsetAsync(hs, 0, slot * sizeof(double), st));
     for (int pass = 0; pass < 2; ++pass) {
       double* hp = hs + (size_t)pass * S * ldh;
-      seg_dots(V.p, j + 1, w.p, hp, ldh);
-      seg_axpy_kernel<<<nchunks_, 256, (j + 1) * sizeof(double), st>>>(V.p, n, j + 1, hp, ldh, chunks, w.p, -1.0);
+      // segments that stopped are skipped: their h and w are never read again
+      seg_dots(V.p, j + 1, w.p, hp, ldh, act.p);
+      seg_axpy_kernel<<<nchunks_, 256, (j + 1) * sizeof(double), st>>>(V.p, n, j + 1, hp, ldh, chunks, w.p, -1.0,
+                                                                       act.p);
       NNK_CHECK_LAUNCH();
     }
     double* nrm = hs + 2 * (size_t)S * ldh;
-    seg_dots(w.p, 1, w.p, nrm, 1);
+    seg_dots(w.p, 1, w.p, nrm, 1, act.p);
     seg_normalize_kernel<<<nchunks_, 256, 0, st>>>(w.p, nrm, act.p, chunks, V.p + (size_t)(j + 1) * n);
     NNK_CHECK_LAUNCH();
     NNK_CUDA(cudaMemcpyAsync(hhost + (j & 1) * slot, hs, slot * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -377,7 +389,8 @@ void SegGmres::solve(const Op& op, const double* b, double* x, const std::vector
     if (kmax > 0) {
       DBuf<double> dY(Y.size());
       NNK_CUDA(cudaMemcpyAsync(dY.p, Y.data(), Y.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-      seg_axpy_kernel<<<nchunks_, 256, kmax * sizeof(double), st>>>(V.p, n, kmax, dY.p, ldh, chunks, x, 1.0);
+      seg_axpy_kernel<<<nchunks_, 256, kmax * sizeof(double), st>>>(V.p, n, kmax, dY.p, ldh, chunks, x, 1.0,
+                                                                    nullptr);
       NNK_CHECK_LAUNCH();
       NNK_CUDA(cudaStreamSynchronize(st));
     }

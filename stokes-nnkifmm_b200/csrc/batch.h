@@ -55,7 +55,7 @@ class SegGmres {
     int len;
     int seg;
   };
-  void seg_dots(const double* V, int nvec, const double* w, double* h, int ldh);
+  void seg_dots(const double* V, int nvec, const double* w, double* h, int ldh, const double* active = nullptr);
   nnk_ctx* ctx_;
   std::vector<int64_t> off_;
   int S_;

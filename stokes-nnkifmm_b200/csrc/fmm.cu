@@ -604,9 +604,11 @@ void Fmm::build_operators() {
   if (p_.precision == NNK_PREC_MIXED && p_.m2l_mode != 3 && p_.m2l_mode != 4) {
     if (p_.m2l_mode == 1) m2l_.image_budget = ~(size_t)0;
     if (p_.m2l_mode == 2) m2l_.image_budget = 0;
+    m2l_.compress = p_.m2l_mode == 0;
     build_m2l_plan(t, p_.res, p_.shells, p_.eps, p_.mu, m2l_, ctx_->stream);
     tensor_m2l_ = true;
     stats_.m2l_tile_rows = m2l_.tile_slots * 128;
+    stats_.m2l_rank = m2l_.compressed ? m2l_.RC : 0;
   }
   const int n = 3 * P_;
   cudaStream_t st = ctx_->stream;
@@ -750,14 +752,17 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     const int64_t nt = ts.up_toff[L + 1] - ts.up_toff[L];
     phase(NNK_PHASE_UP_C2E, [&] {
       launch_c2e<Real>(ops_.p, n, 0, ts.up_tiles.p + ts.up_toff[L], (int)nt, ts.up_nodes.p, check, str, regionA, P_,
-                       R, st, tm ? m2l_.src.p : nullptr, m2l_.NP, c2e_part_.p, c2e_part_.n, na);
+                       R, st, tm && !m2l_.compressed ? m2l_.src.p : nullptr, m2l_.NP, c2e_part_.p, c2e_part_.n,
+                       na);
     });
   }
   // downward pass
   if (tm) {
     // M2L of every level at once: the V-list only reads up densities
     NNK_CUDA(cudaMemsetAsync(check, 0, sizeof(Real) * (size_t)N_ * n, st));
-    phase(NNK_PHASE_M2L, [&] { launch_m2l(m2l_, (float*)check, n, st); });
+    // the compressed form projects the up densities (R = 1: 3P floats per node at
+    // str + 3 (regionA + P node)) itself
+    phase(NNK_PHASE_M2L, [&] { launch_m2l(m2l_, (float*)check, n, st, (const float*)str + 3 * regionA, n); });
   }
   if (fm) {
     // M2L of every level at once in Fourier space

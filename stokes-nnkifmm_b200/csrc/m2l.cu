@@ -7,7 +7,9 @@
 // instruction, four per 32-wide K chunk); all 128 threads gather A rows; the
 // accumulator (128 lanes x NP columns FP32) lives in TMEM.  Every mbarrier
 // wait is bounded; a timeout sets the error flag and the CTA drains and exits.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
 #include <algorithm>
 #include <array>
@@ -284,18 +286,23 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 0) tmem_dealloc(tmem, ncols);
 }
 
+// src_lo (optional): a second TF32 term of the densities (src + src_lo ~= the
+// FP32 value); each step then issues the MMAs of both terms into the same
+// accumulator, so the densities carry ~21 bits instead of TF32's 11.
 __global__ void __launch_bounds__(128, 1)
     m2l_img_kernel(const M2LUnit* __restrict__ units, const int* __restrict__ tile_nodes,
                     const int* __restrict__ tile_slot0, const int* __restrict__ slot_op,
                     const int* __restrict__ slot_src, const float* __restrict__ images,
-                    const float* __restrict__ src, float* __restrict__ check, int ldc, int NP, int* err) {
+                    const float* __restrict__ src, float* __restrict__ check, int ldc, int NP, int* err,
+                    const float* __restrict__ src_lo = nullptr) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* sbase = smem_raw + (((raw + 1023u) & ~1023u) - raw);
   const uint32_t A_BYTES = kTileRows * 128, B_BYTES = (uint32_t)NP * 128;
-  uint8_t* sA0 = sbase;
-  uint8_t* sB0 = sbase + 2 * A_BYTES;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + 2 * A_BYTES + 2 * B_BYTES);  // full[2] done[2] acc
+  const int na = src_lo ? 2 : 1;  // A terms per stage
+  uint8_t* sA0 = sbase;           // stage st, term q at sA0 + (st * na + q) * A_BYTES
+  uint8_t* sB0 = sbase + 2 * na * A_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB0 + 2 * B_BYTES);  // full[2] done[2] acc
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 5);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -335,14 +342,16 @@ __global__ void __launch_bounds__(128, 1)
       ++copies;
     }
     const int v = slot_src[(size_t)slot * kTileRows + tid];
-    float4* dA = reinterpret_cast<float4*>(sA0 + st * A_BYTES + tid * 128);
-    if (v >= 0) {
-      const float4* g4 = reinterpret_cast<const float4*>(src + (size_t)v * NP + c * 32);
+    for (int q = 0; q < na; ++q) {
+      float4* dA = reinterpret_cast<float4*>(sA0 + (st * na + q) * A_BYTES + tid * 128);
+      if (v >= 0) {
+        const float4* g4 = reinterpret_cast<const float4*>((q ? src_lo : src) + (size_t)v * NP + c * 32);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) dA[j ^ (tid & 7)] = __ldg(g4 + j);
-    } else {
+        for (int j = 0; j < 8; ++j) dA[j ^ (tid & 7)] = __ldg(g4 + j);
+      } else {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) dA[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int j = 0; j < 8; ++j) dA[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
     }
     fence_proxy_async();
   };
@@ -356,12 +365,15 @@ __global__ void __launch_bounds__(128, 1)
         atomicOr(err, 2);
       } else {
         tc_fence_after();
-        const uint32_t a0 = smem_u32(sA0 + st * A_BYTES), b0 = smem_u32(sB0 + st * B_BYTES);
+        const uint32_t b0 = smem_u32(sB0 + st * B_BYTES);
 #pragma unroll
         for (int k8 = 0; k8 < 4; ++k8)
-          for (int h = 0; h < nhalves; ++h)
-            umma_tf32(tmem + (uint32_t)(h * nh), sw128_desc(a0 + k8 * 32), sw128_desc(b0 + h * nh * 128 + k8 * 32),
-                      idesc, (s > 0 || k8 > 0) ? 1u : 0u);
+          for (int q = 0; q < na; ++q) {
+            const uint32_t a0 = smem_u32(sA0 + (st * na + q) * A_BYTES);
+            for (int h = 0; h < nhalves; ++h)
+              umma_tf32(tmem + (uint32_t)(h * nh), sw128_desc(a0 + k8 * 32), sw128_desc(b0 + h * nh * 128 + k8 * 32),
+                        idesc, (s > 0 || k8 > 0 || q > 0) ? 1u : 0u);
+          }
         umma_commit(&bars[2 + st]);
         ++issued;
       }
@@ -445,6 +457,225 @@ __global__ void m2l_operator_kernel(int nimg, const int* __restrict__ img_code, 
     }
 }
 
+// T_o in FP64 for the offsets codes[i] at box width w: column-major 3P x 3P,
+// T[n = 3a+al][k = 3b+be] = S_al,be(x_a - y_b) at k * 3P + n (the matrix of
+// m2l_operator_kernel before rounding).
+__global__ void m2l_full_operator_kernel(int ncodes, const int* __restrict__ codes, double w,
+                                         const int* __restrict__ lat, int P, int res, double eps, double mu,
+                                         double* __restrict__ K) {
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per = (long long)P * P;
+  if (gid >= per * ncodes) return;
+  const int img = (int)(gid / per);
+  const int a = (int)((gid % per) / P), b = (int)(gid % P);
+  const int code = codes[img];
+  const int ox = code / 49 - 3, oy = (code / 7) % 7 - 3, oz = code % 7 - 3;
+  const double h = w / (res - 1);
+  const double r[3] = {(lat[3 * a] - lat[3 * b]) * h - ox * w, (lat[3 * a + 1] - lat[3 * b + 1]) * h - oy * w,
+                       (lat[3 * a + 2] - lat[3 * b + 2]) * h - oz * w};
+  const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+  const double e2 = eps * eps;
+  const double inv = 1.0 / (8.0 * M_PI * mu * (r2 + e2) * sqrt(r2 + e2));
+  const int n3 = 3 * P;
+  double* base = K + (size_t)img * n3 * n3;
+  for (int al = 0; al < 3; ++al)
+    for (int be = 0; be < 3; ++be)
+      base[(size_t)(3 * b + be) * n3 + 3 * a + al] = (r[al] * r[be] + (al == be ? r2 + 2 * e2 : 0.0)) * inv;
+}
+
+// Compressed operator images: C (RC x RC, column-major per image, FP64) to
+// the TF32 SW128 K-major chunks the image kernel streams (NP = RC).
+__global__ void compressed_image_kernel(int nimg, const int* __restrict__ src_of, const double* __restrict__ C,
+                                        int RC, float* __restrict__ images) {
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per = (long long)RC * RC;
+  if (gid >= per * nimg) return;
+  const int img = (int)(gid / per);
+  const int k = (int)((gid % per) / RC), n = (int)(gid % RC);
+  const double v = C[(size_t)src_of[img] * per + (size_t)k * RC + n];
+  const int c = k >> 5, kl = k & 31, j = kl >> 2, e = kl & 3;
+  uint8_t* base = reinterpret_cast<uint8_t*>(images) + (size_t)img * per * sizeof(float);
+  *reinterpret_cast<float*>(base + (size_t)c * RC * 128 + (size_t)n * 128 + ((j ^ (n & 7)) << 4) + e * 4) =
+      to_tf32((float)v);
+}
+
+// The basis in FP32, row-major 3P x RC, from its FP64 column-major form.
+__global__ void basis_float_kernel(const double* __restrict__ Bd, int n3, int RC, float* __restrict__ B) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= n3 * RC) return;
+  const int row = gid / RC, j = gid % RC;
+  B[gid] = (float)Bd[(size_t)j * n3 + row];
+}
+
+// y[node * ldy + r] = sum_k A(r, k) x[node * ldx + k] for the nodes of each
+// tile, A the tile's basis B (3P x RC, row-major):
+//   trans = 1 (projection u^ = B^T u): A(r, k) = B[k][r], r < RC, k < 3P,
+//              y written as two TF32 terms (the tensor-core operands):
+//              y = tf32(v), y_lo = tf32(v - y);
+//   trans = 0 (expansion check += B c^): A(r, k) = B[r][k], r < 3P, k < RC,
+//              y accumulated.
+// 64 x 64 output tile (rows x nodes) per CTA of 256 threads, 4 x 4 each, K in
+// steps of 16, FP32.
+__global__ void __launch_bounds__(256) basis_apply_kernel(const float* __restrict__ basis, int n3, int RC,
+                                                          int trans, const BasisTile* __restrict__ tiles,
+                                                          const int* __restrict__ nodes,
+                                                          const float* __restrict__ x, long long ldx,
+                                                          float* __restrict__ y, long long ldy,
+                                                          float* __restrict__ y_lo = nullptr) {
+  constexpr int BM = 64, BN = 64, BK = 16;
+  __shared__ float As[BK][BM + 1];
+  __shared__ float Xs[BK][BN + 1];
+  __shared__ int col_node[BN];
+  const BasisTile tl = tiles[blockIdx.y];
+  const int rows = trans ? RC : n3, K = trans ? n3 : RC;
+  const int m0 = blockIdx.x * BM;
+  const float* __restrict__ B = basis + (size_t)tl.basis * n3 * RC;
+  const int tid = threadIdx.x;
+  if (tid < BN) col_node[tid] = tid < tl.count ? nodes[tl.first + tid] : -1;
+  const int tr = tid % 16, tc = tid / 16;
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q;  // BK * BM
+      int kk, mm;
+      if (trans) { mm = e % BM; kk = e / BM; }  // B[k][r]: contiguous in r
+      else { kk = e % BK; mm = e / BK; }        // B[r][k]: contiguous in k
+      const int r = m0 + mm, k = k0 + kk;
+      As[kk][mm] = (r < rows && k < K) ? (trans ? B[(size_t)k * RC + r] : B[(size_t)r * RC + k]) : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q;  // BK * BN
+      const int kk = e % BK, nn = e / BK;
+      const int k = k0 + kk, node = col_node[nn];
+      Xs[kk][nn] = (k < K && node >= 0) ? x[(size_t)node * ldx + k] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][tr + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Xs[kk][tc + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = m0 + tr + 16 * i, node = col_node[tc + 16 * j];
+      if (r >= rows || node < 0) continue;
+      float* o = y + (size_t)node * ldy + r;
+      if (trans) {
+        const float hi = to_tf32(acc[i][j]);
+        *o = hi;
+        y_lo[(size_t)node * ldy + r] = to_tf32(acc[i][j] - hi);
+      } else {
+        *o += acc[i][j];
+      }
+    }
+}
+
+// Compression of the operators of one level pass (see m2l.h).  Builds the
+// FP64 operators of all 316 far offsets, the eigenvectors of sum_o T_o T_o^T,
+// and C_o = B^T T_o B for every offset; returns B (FP32) and C in FP64.
+struct Compressor {
+  cublasHandle_t b = nullptr;
+  cusolverDnHandle_t s = nullptr;
+  int n3 = 0, RC = 0, P = 0, res = 0;
+  std::vector<int> far_codes;
+  DBuf<int> dcodes, dlat;
+  DBuf<double> K, G, W, T, C, work, H, Br;
+  DBuf<int> info;
+  int lwork = 0;
+  Compressor(const std::vector<int>& lat, int P_, int res_, int RC_, cudaStream_t st) : n3(3 * P_), RC(RC_), P(P_), res(res_) {
+    if (cublasCreate(&b) != CUBLAS_STATUS_SUCCESS) throw Error(NNK_E_CUDA, "cublasCreate failed");
+    cublasSetStream(b, st);
+    if (cusolverDnCreate(&s) != CUSOLVER_STATUS_SUCCESS) throw Error(NNK_E_CUDA, "cusolverDnCreate failed");
+    cusolverDnSetStream(s, st);
+    cudaGetLastError();
+    for (int c = 0; c < 343; ++c) {
+      const int ox = c / 49 - 3, oy = (c / 7) % 7 - 3, oz = c % 7 - 3;
+      if (std::max(std::abs(ox), std::max(std::abs(oy), std::abs(oz))) >= 2) far_codes.push_back(c);
+    }
+    dcodes.upload(far_codes, st);
+    dlat.upload(lat, st);
+    const size_t nc = far_codes.size();
+    K.alloc(nc * n3 * n3);
+    G.alloc((size_t)n3 * n3);
+    W.alloc(n3);
+    T.alloc(nc * n3 * RC);
+    C.alloc(nc * RC * RC);
+    info.alloc(1);
+    // normalized Sylvester-Hadamard matrix (RC a power of two): rotating the
+    // basis by it spreads every vector's energy over all RC coordinates, so
+    // the TF32 rounding errors of the compressed products average out as
+    // they do over the 3P physical coordinates
+    if (RC & (RC - 1)) throw Error(NNK_E_ARG, "compressed M2L rank must be a power of two");
+    std::vector<double> h((size_t)RC * RC);
+    const double sc = 1.0 / std::sqrt((double)RC);
+    for (int i = 0; i < RC; ++i)
+      for (int j = 0; j < RC; ++j) h[(size_t)j * RC + i] = (__builtin_popcount(i & j) & 1) ? -sc : sc;
+    H.upload(h, st);
+    Br.alloc((size_t)n3 * RC);
+    if (cusolverDnDsyevd_bufferSize(s, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n3, G.p, n3, W.p, &lwork) !=
+        CUSOLVER_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "syevd_bufferSize failed");
+    work.alloc(std::max(lwork, 1));
+  }
+  ~Compressor() {
+    if (s) cusolverDnDestroy(s);
+    if (b) cublasDestroy(b);
+  }
+  int far_index(int code) const {
+    return (int)(std::lower_bound(far_codes.begin(), far_codes.end(), code) - far_codes.begin());
+  }
+  // basis (3P x RC FP32 row-major) into B_out; C (per far offset) in this->C
+  void run(double w, double eps, double mu, float* B_out, cudaStream_t st) {
+    const int nc = (int)far_codes.size();
+    const long long total = (long long)P * P * nc;
+    m2l_full_operator_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(nc, dcodes.p, w, dlat.p, P, res, eps,
+                                                                             mu, K.p);
+    NNK_CHECK_LAUNCH();
+    const double one = 1.0, zero = 0.0;
+    // G = [T_1 ... T_nc] [T_1 ... T_nc]^T
+    if (cublasDgemm(b, CUBLAS_OP_N, CUBLAS_OP_T, n3, n3, n3 * nc, &one, K.p, n3, K.p, n3, &zero, G.p, n3) !=
+        CUBLAS_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "M2L Gram product failed");
+    if (cusolverDnDsyevd(s, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n3, G.p, n3, W.p, work.p, lwork,
+                         info.p) != CUSOLVER_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "M2L basis eigendecomposition failed");
+    int h_info = 0;
+    NNK_CUDA(cudaMemcpyAsync(&h_info, info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NNK_CUDA(cudaStreamSynchronize(st));
+    if (h_info != 0) throw Error(NNK_E_CUDA, "M2L basis eigendecomposition info=" + std::to_string(h_info));
+    // B = (leading RC eigenvectors) x H, n3 x RC column-major
+    if (cublasDgemm(b, CUBLAS_OP_N, CUBLAS_OP_N, n3, RC, RC, &one, G.p + (size_t)(n3 - RC) * n3, n3, H.p, RC, &zero,
+                    Br.p, n3) != CUBLAS_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "M2L basis rotation failed");
+    const double* Bd = Br.p;
+    // T_o B, then C_o = B^T (T_o B)
+    if (cublasDgemmStridedBatched(b, CUBLAS_OP_N, CUBLAS_OP_N, n3, RC, n3, &one, K.p, n3, (long long)n3 * n3, Bd, n3,
+                                  0, &zero, T.p, n3, (long long)n3 * RC, nc) != CUBLAS_STATUS_SUCCESS ||
+        cublasDgemmStridedBatched(b, CUBLAS_OP_T, CUBLAS_OP_N, RC, RC, n3, &one, Bd, n3, 0, T.p, n3,
+                                  (long long)n3 * RC, &zero, C.p, RC, (long long)RC * RC, nc) != CUBLAS_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "M2L compressed operator products failed");
+    basis_float_kernel<<<(n3 * RC + 255) / 256, 256, 0, st>>>(Br.p, n3, RC, B_out);
+    NNK_CHECK_LAUNCH();
+  }
+};
+
 }  // namespace
 
 M2LPlan::~M2LPlan() {
@@ -465,10 +696,19 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
           lat.push_back(k);
         }
   const int P = (int)lat.size() / 3;
-  const int NP = ((3 * P + 31) / 32) * 32;
+  int NP = ((3 * P + 31) / 32) * 32;
   if (NP > 512 || NP / (NP > 256 ? 2 : 1) % 16 != 0)
     throw Error(NNK_E_ARG, "tensor-core M2L supports 3P up to 512 with N halves a multiple of 16");
+  plan.n3 = 3 * P;
+  plan.compressed = plan.compress && 3 * P > plan.RC && plan.image_budget > 0;
+  if (plan.compressed) NP = plan.RC;
   plan.NP = NP;
+  struct Pass {
+    double w;
+    std::vector<int32_t> nodes;  // V targets and V sources, ascending
+  };
+  std::vector<Pass> passes;
+  std::vector<int> img_pass;  // per image: its pass
   std::vector<int> tile_nodes, tile_slot0, slot_code, slot_src, slot_op;
   std::vector<float> slot_h;
   std::vector<M2LUnit> units;
@@ -500,6 +740,16 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
       sig[n] = b;
     }
     std::stable_sort(nodes.begin(), nodes.end(), [&](int32_t a, int32_t b) { return sig[a] > sig[b]; });
+    {
+      Pass ps{std::ldexp(W0, -L), {}};
+      for (int32_t n : nodes) {
+        ps.nodes.push_back(n);
+        for (int64_t k = t.V.off[n]; k < t.V.off[n + 1]; ++k) ps.nodes.push_back(t.V.idx[k]);
+      }
+      std::sort(ps.nodes.begin(), ps.nodes.end());
+      ps.nodes.erase(std::unique(ps.nodes.begin(), ps.nodes.end()), ps.nodes.end());
+      passes.push_back(std::move(ps));
+    }
     std::map<int, int> img_of;  // offset code -> image of this level
     const int first_tile = (int)tile_slot0.size();
     std::vector<std::vector<int>> tile_codes;  // per tile in this level: its offset codes, ascending
@@ -530,6 +780,7 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
           it = img_of.emplace(kv.first, (int)img_code.size()).first;
           img_code.push_back(kv.first);
           img_w.push_back(std::ldexp(W0, -L));
+          img_pass.push_back((int)passes.size() - 1);
         }
         slot_op.push_back(it->second);
         slot_code.push_back(kv.first);
@@ -570,9 +821,48 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
   // by the image kernel) when they fit the budget; otherwise the generating
   // kernel computes each chunk in shared memory.
   const size_t img_bytes = img_code.size() * (size_t)NP * NP * sizeof(float);
-  plan.use_images = img_bytes <= plan.image_budget;
+  plan.use_images = plan.compressed || img_bytes <= plan.image_budget;
   plan.image_bytes = plan.use_images ? img_bytes : 0;
-  if (plan.use_images && !img_code.empty()) {
+  if (plan.compressed && !img_code.empty()) {
+    // per pass: basis B and the compressed images of the offsets it uses
+    const int RC = plan.RC, n3 = 3 * P;
+    plan.slot_op.upload(slot_op, st);
+    plan.images.alloc(img_code.size() * (size_t)RC * RC);
+    plan.basis.alloc(passes.size() * (size_t)n3 * RC);
+    Compressor cmp(lat, P, res, RC, st);
+    std::vector<BasisTile> bt;
+    std::vector<int> bn;
+    DBuf<int> dsrc;
+    for (size_t ps = 0; ps < passes.size(); ++ps) {
+      cmp.run(passes[ps].w, eps, mu, plan.basis.p + ps * (size_t)n3 * RC, st);
+      std::vector<int> imgs, src_of;
+      for (size_t i = 0; i < img_code.size(); ++i)
+        if (img_pass[i] == (int)ps) {
+          imgs.push_back((int)i);
+          src_of.push_back(cmp.far_index(img_code[i]));
+        }
+      // images of a pass are consecutive (appended while its tiles were built)
+      if (imgs.empty() || imgs.back() != imgs.front() + (int)imgs.size() - 1)
+        throw Error(NNK_E_STATE, "M2L images of a level pass are not consecutive");
+      dsrc.upload(src_of, st);
+      const long long total = (long long)RC * RC * (long long)imgs.size();
+      compressed_image_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+          (int)imgs.size(), dsrc.p, cmp.C.p, RC, plan.images.p + (size_t)imgs[0] * RC * RC);
+      NNK_CHECK_LAUNCH();
+      NNK_CUDA(cudaStreamSynchronize(st));  // dsrc and cmp's buffers are reused by the next pass
+      const auto& nd = passes[ps].nodes;
+      for (size_t f = 0; f < nd.size(); f += 64) {
+        bt.push_back(BasisTile{(int)ps, (int)bn.size(), (int)std::min<size_t>(64, nd.size() - f), 0});
+        bn.insert(bn.end(), nd.begin() + f, nd.begin() + std::min(nd.size(), f + 64));
+      }
+    }
+    plan.btiles.upload(bt, st);
+    plan.bnodes.upload(bn, st);
+    plan.nbtiles = (int)bt.size();
+    plan.chat.alloc((size_t)t.nodes * RC);
+    plan.src_lo.alloc((size_t)t.nodes * RC);
+    plan.src_lo.zero(st);
+  } else if (plan.use_images && !img_code.empty()) {
     plan.slot_op.upload(slot_op, st);
     plan.images.alloc(img_code.size() * (size_t)NP * NP);
     plan.images.zero(st);
@@ -597,7 +887,8 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
   plan.err.zero(st);
   if (!plan.h_err) NNK_CUDA(cudaMallocHost((void**)&plan.h_err, sizeof(int)));
   *plan.h_err = 0;
-  plan.smem_bytes = 1024 + 2 * (size_t)kTileRows * 128 + 2 * (size_t)NP * 128 + 64 + 4 * (size_t)P;
+  plan.smem_bytes = 1024 + 2 * (plan.compressed ? 2 : 1) * (size_t)kTileRows * 128 + 2 * (size_t)NP * 128 + 64 +
+                    4 * (size_t)P;
   // the attribute is per kernel, shared by every plan: set it for the largest NP
   const int max_smem = 1024 + 2 * kTileRows * 128 + 2 * 512 * 128 + 64 + 4 * 512;
   NNK_CUDA(cudaFuncSetAttribute(m2l_gen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
@@ -606,8 +897,26 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
   plan.ready = true;
 }
 
-void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st) {
+void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st, const float* up, long long ld_up) {
   if (!plan.nunits) return;
+  if (plan.compressed) {
+    if (!up) throw Error(NNK_E_STATE, "compressed M2L needs the up densities");
+    const int RC = plan.RC;
+    basis_apply_kernel<<<dim3((RC + 63) / 64, plan.nbtiles), 256, 0, st>>>(
+        plan.basis.p, plan.n3, RC, 1, plan.btiles.p, plan.bnodes.p, up, ld_up, plan.src.p, RC, plan.src_lo.p);
+    NNK_CHECK_LAUNCH();
+    NNK_CUDA(cudaMemsetAsync(plan.chat.p, 0, plan.chat.bytes(), st));
+    m2l_img_kernel<<<plan.nunits, 128, plan.smem_bytes, st>>>(plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p,
+                                                              plan.slot_op.p, plan.slot_src.p, plan.images.p,
+                                                              plan.src.p, plan.chat.p, RC, RC, plan.err.p,
+                                                              plan.src_lo.p);
+    NNK_CHECK_LAUNCH();
+    NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    basis_apply_kernel<<<dim3((plan.n3 + 63) / 64, plan.nbtiles), 256, 0, st>>>(
+        plan.basis.p, plan.n3, RC, 0, plan.btiles.p, plan.bnodes.p, plan.chat.p, RC, check, ldc);
+    NNK_CHECK_LAUNCH();
+    return;
+  }
   if (plan.use_images) {
     m2l_img_kernel<<<plan.nunits, 128, plan.smem_bytes, st>>>(plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p,
                                                               plan.slot_op.p, plan.slot_src.p, plan.images.p,

@@ -16,6 +16,22 @@
 // sizes), it is computed chunk by chunk from the kernel formula into shared
 // memory by the CTA itself (about 2.7x slower per chunk, no memory).  The result is added into
 // the check buffer, which the P2L / L2L pair tasks then add to.
+//
+// Compressed form (default for 3P > 256): T_o^T = T_{-o} (the Stokeslet is
+// even and its 3x3 blocks symmetric), so sum_o T_o T_o^T = sum_o T_o^T T_o
+// and one orthonormal basis B_L (3P x RC, the leading RC eigenvectors of
+// that sum over the 316 far offsets) captures both sides:
+//     T_{L,o} ~= B_L C_{L,o} B_L^T,   C_{L,o} = B_L^T T_{L,o} B_L  (RC x RC).
+// B is the eigenvector basis rotated by a normalized Hadamard matrix, which
+// spreads each vector over all RC coordinates (in the eigenbasis a few
+// leading terms carry the sums, and their TF32 rounding errors do not
+// average out).  Per matvec: u^ = B^T u for every node that is a V source
+// (FP32 GEMM, split into two TF32 terms), c^ = sum_o C_o u^_v on the tensor
+// cores (the image kernel with NP = RC, both terms into one accumulator),
+// check += B c^ for every V target.  RC = 256 for p = 6: 2 x (RC/NP)^2 = 57%
+// of the tensor work and 28% of the operator bytes; the truncation error of
+// the summed M2L on physical densities is ~1e-6, the TF32 rounding of C_o
+// ~4e-5 (the full TF32 operators: ~5e-5).
 #pragma once
 #include <vector>
 
@@ -31,8 +47,16 @@ struct M2LUnit {
   int pad;
 };
 
+// Nodes nodes[first .. first+count) (count <= 64) that share basis `basis`.
+struct BasisTile {
+  int basis;
+  int first;
+  int count;
+  int pad;
+};
+
 struct M2LPlan {
-  int NP = 0;                   // padded 3P (multiple of 32)
+  int NP = 0;                   // padded 3P (multiple of 32); RC when compressed
   int ntiles = 0, nunits = 0;
   int64_t useful_pairs = 0;     // V pairs (node, source)
   int64_t tile_slots = 0;       // sum over tiles of offset slots (x128 rows each)
@@ -50,7 +74,17 @@ struct M2LPlan {
   DBuf<float> images;           // per (level, offset): NP/32 chunks of NP x 32 TF32, SW128 K-major
   int P = 0, res = 0;
   float e2 = 0.f, scale = 0.f;
-  DBuf<float> src;              // nodes * NP: TF32 copy of the up densities
+  DBuf<float> src;              // nodes * NP: TF32 copy of the up densities (compressed: B^T u)
+  bool compress = true;         // use the compressed form where 3P > RC
+  bool compressed = false;
+  int n3 = 0;                   // 3P
+  int RC = 256;                 // compressed rank
+  DBuf<float> basis;            // per level pass: B (3P x RC, row-major)
+  DBuf<BasisTile> btiles;       // V targets and sources, by pass
+  DBuf<int> bnodes;
+  int nbtiles = 0;
+  DBuf<float> chat;             // nodes * RC: compressed check potentials
+  DBuf<float> src_lo;           // nodes * RC: second TF32 term of B^T u
   DBuf<int> err;                // bounded-wait timeout flag
   int* h_err = nullptr;         // pinned mirror of err
   size_t smem_bytes = 0;
@@ -62,7 +96,10 @@ struct M2LPlan {
 void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double mu, M2LPlan& plan,
                     cudaStream_t st);
 // check[node * ldc + row] += M2L contribution, for every node with a V-list.
-void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st);
+// The compressed form first projects the up densities up[node * ld_up + k]
+// (k < 3P); the uncompressed one reads plan.src, filled by the up C2E.
+void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st, const float* up = nullptr,
+                long long ld_up = 0);
 // Throws NNK_E_TIMEOUT if an earlier M2L launch gave up a bounded wait.
 void check_m2l_error(M2LPlan& plan, cudaStream_t st);
 

@@ -51,7 +51,7 @@ class FmmParams(C.Structure):
 class FmmStats(C.Structure):
     _fields_ = [("pairs_leaf", _i64), ("pairs_p2p", _i64), ("pairs_up", _i64), ("pairs_down", _i64),
                 ("m2l_pairs", _i64), ("c2e_columns", _i64), ("m2l_tile_rows", _i64), ("surface_points", _i32),
-                ("levels", _i32)]
+                ("levels", _i32), ("m2l_rank", _i32), ("reserved", _i32)]
 
 
 class SolveParams(C.Structure):
