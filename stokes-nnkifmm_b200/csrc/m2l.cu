@@ -25,6 +25,7 @@ namespace {
 constexpr int kTileRows = 128;
 constexpr int kCodesPerUnit = 32;  // offset codes per work unit (7^3 = 343 codes)
 constexpr uint32_t kWaitLimit = 1u << 26;  // ~1-3 s of polling
+constexpr size_t kImgSmemMax = 200 * 1024;  // dynamic shared memory of the image kernel, at most
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -36,6 +37,9 @@ __device__ __forceinline__ float to_tf32(float x) {
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
@@ -256,12 +260,11 @@ __global__ void __launch_bounds__(128, 1)
   }
   __syncthreads();
   // drain: the commit tracks every MMA this thread issued
-  bool acc_ok = true;
   if (tid == 0) umma_commit(&bars[2]);
-  if (!mbar_wait(&bars[2], 0)) {
-    acc_ok = false;
-    atomicOr(err, 4);
-  }
+  // the read-back is warp-collective: a warp reads only if all its lanes saw
+  // the accumulator complete
+  const bool acc_ok = __all_sync(0xffffffffu, mbar_wait(&bars[2], 0));
+  if (!acc_ok && (tid & 31) == 0) atomicOr(err, 4);
   (void)issued;
   tc_fence_after();
   if (!*abort_s && acc_ok && nsteps > 0) {
@@ -294,16 +297,19 @@ __global__ void __launch_bounds__(128, 1)
                     const int* __restrict__ tile_slot0, const int* __restrict__ slot_op,
                     const int* __restrict__ slot_src, const float* __restrict__ images,
                     const float* __restrict__ src, float* __restrict__ check, int ldc, int NP, int* err,
-                    const float* __restrict__ src_lo = nullptr) {
+                    const float* __restrict__ src_lo, int ns) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* sbase = smem_raw + (((raw + 1023u) & ~1023u) - raw);
   const uint32_t A_BYTES = kTileRows * 128, B_BYTES = (uint32_t)NP * 128;
   const int na = src_lo ? 2 : 1;  // A terms per stage
   uint8_t* sA0 = sbase;           // stage st, term q at sA0 + (st * na + q) * A_BYTES
-  uint8_t* sB0 = sbase + 2 * na * A_BYTES;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sB0 + 2 * B_BYTES);  // full[2] done[2] acc
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 5);
+  uint8_t* sB0 = sbase + ns * na * A_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB0 + ns * B_BYTES);  // full[ns] done[ns] acc
+  uint64_t* full = bars;
+  uint64_t* done = bars + ns;
+  uint64_t* accb = bars + 2 * ns;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * ns + 1);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -315,7 +321,7 @@ __global__ void __launch_bounds__(128, 1)
   const uint32_t idesc = tf32_idesc(nh);
 
   if (tid == 0) {
-    for (int k = 0; k < 5; ++k) mbar_init(&bars[k], 1);
+    for (int k = 0; k < 2 * ns + 1; ++k) mbar_init(&bars[k], 1);
     *abort_s = 0;
     fence_barrier_init();
   }
@@ -329,16 +335,18 @@ __global__ void __launch_bounds__(128, 1)
   const int nsteps = u.nslot * nchunks;
   int issued = 0;  // MMA steps committed
   int copies = 0;  // B copies issued
-  // Step s uses stage s & 1: thread 0 bulk-copies the operator chunk into B,
-  // every thread gathers its own A row (32 TF32 of its source node's density).
+  // Step s uses stage s % ns (its k-th use completes phase k of full[] and
+  // done[], parity (s / ns) & 1): thread 0 bulk-copies the operator chunk
+  // into B, every thread gathers its own A row (32 TF32 of its source node's
+  // density, per term).
   auto prepare = [&](int s) {
-    const int st = s & 1;
+    const int st = s % ns;
     const int slot = slot_base + s / nchunks;
     const int c = s % nchunks;
     if (tid == 0) {
-      mbar_expect_tx(&bars[st], B_BYTES);
+      mbar_expect_tx(&full[st], B_BYTES);
       const float* gB = images + (size_t)slot_op[slot] * ((size_t)nchunks * NP * 32) + (size_t)c * NP * 32;
-      bulk_g2s(sB0 + st * B_BYTES, gB, B_BYTES, &bars[st]);
+      bulk_g2s(sB0 + st * B_BYTES, gB, B_BYTES, &full[st]);
       ++copies;
     }
     const int v = slot_src[(size_t)slot * kTileRows + tid];
@@ -355,12 +363,12 @@ __global__ void __launch_bounds__(128, 1)
     }
     fence_proxy_async();
   };
-  if (nsteps > 0) prepare(0);
+  for (int i = 0; i < ns - 1 && i < nsteps; ++i) prepare(i);
   __syncthreads();
   for (int s = 0; s < nsteps; ++s) {
-    const int st = s & 1;
+    const int st = s % ns;
     if (tid == 0 && !*abort_s) {
-      if (!mbar_wait(&bars[st], (s >> 1) & 1)) {
+      if (!mbar_wait(&full[st], (s / ns) & 1)) {
         *abort_s = 1;
         atomicOr(err, 2);
       } else {
@@ -374,35 +382,32 @@ __global__ void __launch_bounds__(128, 1)
               umma_tf32(tmem + (uint32_t)(h * nh), sw128_desc(a0 + k8 * 32), sw128_desc(b0 + h * nh * 128 + k8 * 32),
                         idesc, (s > 0 || k8 > 0 || q > 0) ? 1u : 0u);
           }
-        umma_commit(&bars[2 + st]);
+        umma_commit(&done[st]);
         ++issued;
       }
     }
-    // while the MMAs of step s run, fill the other stage with step s+1 once
-    // the MMAs of step s-1 (its previous user) are done
-    if (s + 1 < nsteps) {
-      if (s >= 1 && !mbar_wait(&bars[2 + (st ^ 1)], ((s - 1) >> 1) & 1)) {
+    // while the MMAs of steps s (and s-1..) run, fill stage (s-1) % ns with
+    // step s+ns-1 once the MMAs of step s-1, its previous user, are done
+    const int nxt = s + ns - 1;
+    if (nxt < nsteps) {
+      if (s >= 1 && !mbar_wait(&done[(s - 1) % ns], ((s - 1) / ns) & 1)) {
         *abort_s = 1;
         atomicOr(err, 1);
       }
-      if (!*abort_s) prepare(s + 1);
+      if (!*abort_s) prepare(nxt);
     }
     __syncthreads();
     if (*abort_s) break;
   }
   __syncthreads();
   // drain: every MMA this thread issued completes before acc (commit tracks all)
-  bool acc_ok = true;
-  if (tid == 0) umma_commit(&bars[4]);
-  if (!mbar_wait(&bars[4], 0)) {
-    acc_ok = false;
-    atomicOr(err, 4);
-  }
-  // a B copy issued for a step whose MMA never ran must land before exit
-  if (tid == 0 && copies > issued) {
-    const int s = copies - 1;
-    if (!mbar_wait(&bars[s & 1], (s >> 1) & 1)) atomicOr(err, 8);
-  }
+  if (tid == 0) umma_commit(accb);
+  const bool acc_ok = __all_sync(0xffffffffu, mbar_wait(accb, 0));
+  if (!acc_ok && (tid & 31) == 0) atomicOr(err, 4);
+  // B copies issued for steps whose MMAs never ran must land before exit
+  if (tid == 0)
+    for (int s = issued; s < copies; ++s)
+      if (!mbar_wait(&full[s % ns], (s / ns) & 1)) atomicOr(err, 8);
   tc_fence_after();
   if (!*abort_s && acc_ok && nsteps > 0) {
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
@@ -424,6 +429,166 @@ __global__ void __launch_bounds__(128, 1)
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// Warp-specialised form of m2l_img_kernel for the compressed operators
+// (NP = RC <= 256, two density terms), 160 threads:
+//   warp 0, lane 0: bulk-copies operator chunks up to ns steps ahead and
+//                   issues the MMAs of each step once its stage is full;
+//   warps 1-4:      thread r gathers A row r (both terms) of every step into
+//                   its stage as soon as the MMAs of the stage's previous use
+//                   are done, then each warp arrives on the stage's barrier.
+// full[st] completes when the 4 gather warps have arrived and the copy has
+// landed (count 5: 4 arrivals + the producer's expect_tx arrival); done[st]
+// when the stage's MMAs are done (tcgen05.commit).  Warps 1-4 read the
+// accumulator back (warp w reads TMEM lanes 32 (w % 4) ..).  Every wait is
+// bounded; a timeout sets err and the roles drain and exit.
+__global__ void __launch_bounds__(160, 1)
+    m2l_ws_kernel(const M2LUnit* __restrict__ units, const int* __restrict__ tile_nodes,
+                   const int* __restrict__ tile_slot0, const int* __restrict__ slot_op,
+                   const int* __restrict__ slot_src, const float* __restrict__ images,
+                   const float* __restrict__ src, const float* __restrict__ src_lo, float* __restrict__ out,
+                   int ldc, int NP, int* err, int ns) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* sbase = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+  const uint32_t A_BYTES = kTileRows * 128, B_BYTES = (uint32_t)NP * 128;
+  uint8_t* sA0 = sbase;  // stage st, term q at sA0 + (2 st + q) A_BYTES
+  uint8_t* sB0 = sbase + ns * 2 * A_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB0 + ns * B_BYTES);
+  uint64_t* full = bars;
+  uint64_t* done = bars + ns;
+  uint64_t* accb = bars + 2 * ns;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * ns + 1);
+  volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const M2LUnit u = units[blockIdx.x];
+  const int nchunks = NP / 32;
+  const uint32_t idesc = tf32_idesc(NP);
+  if (tid == 0) {
+    for (int k = 0; k < ns; ++k) {
+      mbar_init(&full[k], 5);
+      mbar_init(&done[k], 1);
+    }
+    mbar_init(accb, 1);
+    *abort_s = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0) tmem_alloc(tmem_slot, 256);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int slot_base = tile_slot0[u.tile] + u.slot0;
+  const int nsteps = u.nslot * nchunks;
+  int issued = 0, copies = 0;  // lane 0 of warp 0
+  if (warp == 0) {
+    if (lane == 0) {
+      auto copy = [&](int s) {
+        const int st = s % ns;
+        const int slot = slot_base + s / nchunks, c = s % nchunks;
+        mbar_expect_tx(&full[st], B_BYTES);
+        const float* gB = images + (size_t)slot_op[slot] * ((size_t)nchunks * NP * 32) + (size_t)c * NP * 32;
+        bulk_g2s(sB0 + st * B_BYTES, gB, B_BYTES, &full[st]);
+        ++copies;
+      };
+      for (int s = 0; s < ns && s < nsteps; ++s) copy(s);
+      for (int s = 0; s < nsteps && !*abort_s; ++s) {
+        const int st = s % ns;
+        if (!mbar_wait(&full[st], (s / ns) & 1)) {
+          *abort_s = 1;
+          atomicOr(err, 2);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t b0 = smem_u32(sB0 + st * B_BYTES);
+#pragma unroll
+        for (int k8 = 0; k8 < 4; ++k8)
+#pragma unroll
+          for (int q = 0; q < 2; ++q)
+            umma_tf32(tmem, sw128_desc(smem_u32(sA0 + (2 * st + q) * A_BYTES) + k8 * 32), sw128_desc(b0 + k8 * 32),
+                      idesc, (s > 0 || k8 > 0 || q > 0) ? 1u : 0u);
+        umma_commit(&done[st]);
+        ++issued;
+        // refill the stage of step s-1 with step s-1+ns once its MMAs are done
+        const int prev = s - 1, nxt = s - 1 + ns;
+        if (prev >= 0 && nxt < nsteps) {
+          if (!mbar_wait(&done[prev % ns], (prev / ns) & 1)) {
+            *abort_s = 1;
+            atomicOr(err, 1);
+            break;
+          }
+          copy(nxt);
+        }
+      }
+      umma_commit(accb);  // tracks every MMA issued above
+    }
+    __syncwarp();
+  } else {
+    const int r = tid - 32;  // A row
+    for (int s = 0; s < nsteps && !*abort_s; ++s) {
+      const int st = s % ns, use = s / ns;
+      if (use >= 1 && !mbar_wait(&done[st], (use - 1) & 1)) {
+        *abort_s = 1;
+        atomicOr(err, 16);
+        break;
+      }
+      const int slot = slot_base + s / nchunks, c = s % nchunks;
+      const int v = slot_src[(size_t)slot * kTileRows + r];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        float4* dA = reinterpret_cast<float4*>(sA0 + (2 * st + q) * A_BYTES + r * 128);
+        if (v >= 0) {
+          const float4* g4 = reinterpret_cast<const float4*>((q ? src_lo : src) + (size_t)v * NP + c * 32);
+          float4 t[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) t[j] = __ldg(g4 + j);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) dA[j ^ (r & 7)] = t[j];
+        } else {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) dA[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+      fence_proxy_async();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&full[st]);
+    }
+  }
+  // every role waits for the accumulator (committed after the last MMA); the
+  // read-back below is warp-collective, so a warp reads only if all its lanes
+  // saw the accumulator complete
+  const bool acc_ok = __all_sync(0xffffffffu, mbar_wait(accb, 0));
+  if (!acc_ok && lane == 0) atomicOr(err, 4);
+  // operator copies issued for steps whose MMAs never ran land before exit
+  if (tid == 0)
+    for (int s = issued; s < copies; ++s)
+      if (!mbar_wait(&full[s % ns], (s / ns) & 1)) atomicOr(err, 8);
+  tc_fence_after();
+  if (warp >= 1 && !*abort_s && acc_ok && nsteps > 0) {
+    const int q4 = warp & 3;  // TMEM lane quarter of this warp
+    const int row = 32 * q4 + lane;
+    const int node = tile_nodes[u.tile * kTileRows + row];
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * q4) << 16);
+    for (int col = 0; col < NP; col += 16) {
+      float vals[16];
+      tmem_ld16(lane_addr + col, vals);
+      if (node >= 0) {
+        float* dst = out + (size_t)node * ldc;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int c0 = col + 4 * q;
+          if (c0 < ldc)
+            atomicAdd(reinterpret_cast<float4*>(dst + c0), make_float4(vals[4 * q], vals[4 * q + 1],
+                                                                       vals[4 * q + 2], vals[4 * q + 3]));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 256);
 }
 
 // T_{L,o}[n = 3a+al][k = 3b+be] = S_al,be(x_a - y_b) / (8 pi mu),
@@ -887,12 +1052,17 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
   plan.err.zero(st);
   if (!plan.h_err) NNK_CUDA(cudaMallocHost((void**)&plan.h_err, sizeof(int)));
   *plan.h_err = 0;
-  plan.smem_bytes = 1024 + 2 * (plan.compressed ? 2 : 1) * (size_t)kTileRows * 128 + 2 * (size_t)NP * 128 + 64 +
-                    4 * (size_t)P;
-  // the attribute is per kernel, shared by every plan: set it for the largest NP
-  const int max_smem = 1024 + 2 * kTileRows * 128 + 2 * 512 * 128 + 64 + 4 * 512;
-  NNK_CUDA(cudaFuncSetAttribute(m2l_gen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-  NNK_CUDA(cudaFuncSetAttribute(m2l_img_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  // image kernel: 3 stages where they fit (the compressed form's 64 KB stages), else 2
+  const size_t na = plan.compressed ? 2 : 1;
+  auto img_smem = [&](size_t ns) { return 1024 + ns * (na * kTileRows * 128 + (size_t)NP * 128) + 128; };
+  plan.stages = img_smem(3) <= kImgSmemMax ? 3 : 2;
+  plan.smem_bytes = plan.use_images ? img_smem(plan.stages)
+                                    : 1024 + 2 * (size_t)kTileRows * 128 + 2 * (size_t)NP * 128 + 64 + 4 * (size_t)P;
+  // the attributes are per kernel, shared by every plan: set them for the largest
+  const int max_gen = 1024 + 2 * kTileRows * 128 + 2 * 512 * 128 + 64 + 4 * 512;
+  NNK_CUDA(cudaFuncSetAttribute(m2l_gen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_gen));
+  NNK_CUDA(cudaFuncSetAttribute(m2l_img_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kImgSmemMax));
+  NNK_CUDA(cudaFuncSetAttribute(m2l_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kImgSmemMax));
   NNK_CUDA(cudaStreamSynchronize(st));
   plan.ready = true;
 }
@@ -906,10 +1076,10 @@ void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st, const flo
         plan.basis.p, plan.n3, RC, 1, plan.btiles.p, plan.bnodes.p, up, ld_up, plan.src.p, RC, plan.src_lo.p);
     NNK_CHECK_LAUNCH();
     NNK_CUDA(cudaMemsetAsync(plan.chat.p, 0, plan.chat.bytes(), st));
-    m2l_img_kernel<<<plan.nunits, 128, plan.smem_bytes, st>>>(plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p,
-                                                              plan.slot_op.p, plan.slot_src.p, plan.images.p,
-                                                              plan.src.p, plan.chat.p, RC, RC, plan.err.p,
-                                                              plan.src_lo.p);
+    m2l_ws_kernel<<<plan.nunits, 160, plan.smem_bytes, st>>>(plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p,
+                                                             plan.slot_op.p, plan.slot_src.p, plan.images.p,
+                                                             plan.src.p, plan.src_lo.p, plan.chat.p, RC, RC,
+                                                             plan.err.p, plan.stages);
     NNK_CHECK_LAUNCH();
     NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     basis_apply_kernel<<<dim3((plan.n3 + 63) / 64, plan.nbtiles), 256, 0, st>>>(
@@ -920,7 +1090,8 @@ void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st, const flo
   if (plan.use_images) {
     m2l_img_kernel<<<plan.nunits, 128, plan.smem_bytes, st>>>(plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p,
                                                               plan.slot_op.p, plan.slot_src.p, plan.images.p,
-                                                              plan.src.p, check, ldc, plan.NP, plan.err.p);
+                                                              plan.src.p, check, ldc, plan.NP, plan.err.p, nullptr,
+                                                              plan.stages);
     NNK_CHECK_LAUNCH();
     NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     return;

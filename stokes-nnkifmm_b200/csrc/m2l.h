@@ -88,6 +88,7 @@ struct M2LPlan {
   DBuf<int> err;                // bounded-wait timeout flag
   int* h_err = nullptr;         // pinned mirror of err
   size_t smem_bytes = 0;
+  int stages = 2;               // image kernel pipeline depth
   bool ready = false;
   ~M2LPlan();
 };
