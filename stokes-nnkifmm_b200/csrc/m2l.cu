@@ -432,18 +432,20 @@ __global__ void __launch_bounds__(128, 1)
 }
 
 // Warp-specialised form of m2l_img_kernel for the compressed operators
-// (NP = RC <= 256, two density terms), 160 threads:
+// (NP = RC <= 256, two density terms), 288 threads:
 //   warp 0, lane 0: bulk-copies operator chunks up to ns steps ahead and
 //                   issues the MMAs of each step once its stage is full;
-//   warps 1-4:      thread r gathers A row r (both terms) of every step into
-//                   its stage as soon as the MMAs of the stage's previous use
-//                   are done, then each warp arrives on the stage's barrier.
-// full[st] completes when the 4 gather warps have arrived and the copy has
-// landed (count 5: 4 arrivals + the producer's expect_tx arrival); done[st]
+//   warps 1-8:      warp 1 + 4q + i gathers rows 32 i .. 32 i + 31 of term q
+//                   of every step into its stage as soon as the MMAs of the
+//                   stage's previous use are done, then arrives on the
+//                   stage's barrier.
+// full[st] completes when the 8 gather warps have arrived and the copy has
+// landed (count 9: 8 arrivals + the producer's expect_tx arrival); done[st]
 // when the stage's MMAs are done (tcgen05.commit).  Warps 1-4 read the
 // accumulator back (warp w reads TMEM lanes 32 (w % 4) ..).  Every wait is
 // bounded; a timeout sets err and the roles drain and exit.
-__global__ void __launch_bounds__(160, 1)
+constexpr int kWsGatherWarps = 8;
+__global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
     m2l_ws_kernel(const M2LUnit* __restrict__ units, const int* __restrict__ tile_nodes,
                    const int* __restrict__ tile_slot0, const int* __restrict__ slot_op,
                    const int* __restrict__ slot_src, const float* __restrict__ images,
@@ -468,7 +470,7 @@ __global__ void __launch_bounds__(160, 1)
   const uint32_t idesc = tf32_idesc(NP);
   if (tid == 0) {
     for (int k = 0; k < ns; ++k) {
-      mbar_init(&full[k], 5);
+      mbar_init(&full[k], 1 + kWsGatherWarps);
       mbar_init(&done[k], 1);
     }
     mbar_init(accb, 1);
@@ -526,7 +528,9 @@ __global__ void __launch_bounds__(160, 1)
     }
     __syncwarp();
   } else {
-    const int r = tid - 32;  // A row
+    const int g = warp - 1, q = g / 4;  // term
+    const int r = 32 * (g % 4) + lane;  // A row
+    const float* __restrict__ term = q ? src_lo : src;
     for (int s = 0; s < nsteps && !*abort_s; ++s) {
       const int st = s % ns, use = s / ns;
       if (use >= 1 && !mbar_wait(&done[st], (use - 1) & 1)) {
@@ -536,20 +540,17 @@ __global__ void __launch_bounds__(160, 1)
       }
       const int slot = slot_base + s / nchunks, c = s % nchunks;
       const int v = slot_src[(size_t)slot * kTileRows + r];
+      float4* dA = reinterpret_cast<float4*>(sA0 + (2 * st + q) * A_BYTES + r * 128);
+      if (v >= 0) {
+        const float4* g4 = reinterpret_cast<const float4*>(term + (size_t)v * NP + c * 32);
+        float4 t[8];
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        float4* dA = reinterpret_cast<float4*>(sA0 + (2 * st + q) * A_BYTES + r * 128);
-        if (v >= 0) {
-          const float4* g4 = reinterpret_cast<const float4*>((q ? src_lo : src) + (size_t)v * NP + c * 32);
-          float4 t[8];
+        for (int j = 0; j < 8; ++j) t[j] = __ldg(g4 + j);
 #pragma unroll
-          for (int j = 0; j < 8; ++j) t[j] = __ldg(g4 + j);
+        for (int j = 0; j < 8; ++j) dA[j ^ (r & 7)] = t[j];
+      } else {
 #pragma unroll
-          for (int j = 0; j < 8; ++j) dA[j ^ (r & 7)] = t[j];
-        } else {
-#pragma unroll
-          for (int j = 0; j < 8; ++j) dA[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+        for (int j = 0; j < 8; ++j) dA[j] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       fence_proxy_async();
       __syncwarp();
@@ -566,7 +567,7 @@ __global__ void __launch_bounds__(160, 1)
     for (int s = issued; s < copies; ++s)
       if (!mbar_wait(&full[s % ns], (s / ns) & 1)) atomicOr(err, 8);
   tc_fence_after();
-  if (warp >= 1 && !*abort_s && acc_ok && nsteps > 0) {
+  if (warp >= 1 && warp <= 4 && !*abort_s && acc_ok && nsteps > 0) {
     const int q4 = warp & 3;  // TMEM lane quarter of this warp
     const int row = 32 * q4 + lane;
     const int node = tile_nodes[u.tile * kTileRows + row];
@@ -1076,10 +1077,9 @@ void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st, const flo
         plan.basis.p, plan.n3, RC, 1, plan.btiles.p, plan.bnodes.p, up, ld_up, plan.src.p, RC, plan.src_lo.p);
     NNK_CHECK_LAUNCH();
     NNK_CUDA(cudaMemsetAsync(plan.chat.p, 0, plan.chat.bytes(), st));
-    m2l_ws_kernel<<<plan.nunits, 160, plan.smem_bytes, st>>>(plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p,
-                                                             plan.slot_op.p, plan.slot_src.p, plan.images.p,
-                                                             plan.src.p, plan.src_lo.p, plan.chat.p, RC, RC,
-                                                             plan.err.p, plan.stages);
+    m2l_ws_kernel<<<plan.nunits, 32 * (1 + kWsGatherWarps), plan.smem_bytes, st>>>(
+        plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p, plan.slot_op.p, plan.slot_src.p, plan.images.p,
+        plan.src.p, plan.src_lo.p, plan.chat.p, RC, RC, plan.err.p, plan.stages);
     NNK_CHECK_LAUNCH();
     NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     basis_apply_kernel<<<dim3((plan.n3 + 63) / 64, plan.nbtiles), 256, 0, st>>>(
