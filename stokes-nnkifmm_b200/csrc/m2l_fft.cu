@@ -421,14 +421,20 @@ void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu
   }
   f.fwd_smem = forward_smem(G, res, Rmax);
   f.inv_smem = inverse_smem(G, res, Rmax);
-  if (f.fwd_smem > 227 * 1024 || f.inv_smem > 227 * 1024)
+  int dev = 0, optin = 0;
+  NNK_CUDA(cudaGetDevice(&dev));
+  NNK_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (f.fwd_smem > (size_t)optin || f.inv_smem > (size_t)optin)
     throw Error(NNK_E_ARG, "Fourier M2L: too many right-hand sides per pass for shared memory");
-  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.fwd_smem));
-  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.inv_smem));
-  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.fwd_smem));
-  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.inv_smem));
-  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.fwd_smem));
-  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.inv_smem));
+  // The limit is an attribute of the kernel, shared by every plan of the
+  // process (a p = 4 plan built after a p = 6 one must not lower it): set
+  // the device's opt-in maximum.
+  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   NNK_CUDA(cudaStreamSynchronize(st));
 }
 

@@ -35,7 +35,7 @@ class Body:
     """One body through the per-body path (Swimmers + KIFMM + nnk_mob)."""
 
     def __init__(self, coarse, fine, kernelPar, cap, precision, device=0, preconditioned=False, refine=None,
-                 m2l="pairs", ctx=None):
+                 m2l="fft", ctx=None):
         self.ctx = ctx if ctx is not None else L.Context(device)
         self.coarse, self.fine = coarse, fine
         NN = nearestMatrix(coarse, fine)

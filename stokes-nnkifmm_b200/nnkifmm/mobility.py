@@ -139,9 +139,11 @@ class Swimmers:
         FP64 KIFMM used for the outer residuals of iterative refinement."""
         if kw.get("precision", "fp64") == "mixed":
             # Mobility systems are ill-conditioned (kappa ~ 1e4); the TF32
-            # rounding of tensor-core M2L (~5e-5) then stalls GMRES near 1e-5
-            # and slows refinement, so solves default to the FP32 pair M2L.
-            kw.setdefault("m2l", "pairs")
+            # rounding of tensor-core M2L (~4e-5) then stalls GMRES near 1e-5
+            # and slows refinement, so solves default to an M2L with FP32
+            # accuracy: the Fourier-space product (4x fewer flops than the
+            # FP32 pair kernel).
+            kw.setdefault("m2l", "fft")
         self.FMM = KIFMM(self.Tree, kernelPar, **kw)
         self.FMM64 = None
         if kw.get("precision", "fp64") == "mixed" and refine is not False:
