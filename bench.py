@@ -496,16 +496,19 @@ def main():
     if dom == "m2l":
         n3 = 3 * stats["surface_points"]
         rk = stats["m2l_rank"] or n3
-        flops = 2.0 * rk * rk * stats["m2l_pairs"]
+        terms = 2 if stats["m2l_rank"] else 1  # the compressed form splits the densities into two TF32 terms
+        flops = terms * 2.0 * rk * rk * stats["m2l_pairs"]
         tf32_peak = peaks.get("bf16_tflops", 1590.0) / 2
-        roof = {"kernel": "m2l_img_kernel (tcgen05 kind::tf32, TMEM accumulator)"
-                          + (f" on rank-{rk} compressed operators" if stats["m2l_rank"] else ""),
+        roof = {"kernel": ("m2l_ws_kernel (tcgen05 kind::tf32, TMEM accumulator, warp-specialised) on rank-"
+                           f"{rk} compressed operators" if stats["m2l_rank"] else
+                           "m2l_img_kernel (tcgen05 kind::tf32, TMEM accumulator)"),
                 "bound": "tensor",
                 "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": tf32_peak, "unit": "TFLOP/s",
                 "peak_source": "TF32 dense = 1/2 of the measured cuBLAS bf16 burst peak in MEASURED_PEAKS.json"
                                if peaks else "TF32 dense = 1/2 of the fallback bf16 peak",
-                "algorithmic": f"{stats['m2l_pairs']} V pairs x 2 x {rk}^2 flops per step (useful, no padding; "
-                               f"the phase also holds the basis projection and expansion)",
+                "algorithmic": f"{stats['m2l_pairs']} V pairs x {terms} TF32 density terms x 2 x {rk}^2 flops per "
+                               f"step (useful rows only, no padding; the phase also holds the FP32 basis projection "
+                               f"and expansion, 2 x 2 x 456 x {rk} flops per node)",
                 "padded_rows_over_useful": stats["m2l_tile_rows"] / max(stats["m2l_pairs"], 1),
                 "launches_per_step": per_step[dom][1], "ms_per_launch": per_step[dom][0] / per_step[dom][1],
                 "traffic": None}

@@ -273,6 +273,11 @@ int nnk_mob_create(nnk_fmm* fmm, int32_t nbodies, const int64_t* body_start,
 int nnk_mob_apply(nnk_mob* mob, const double* x, double* y, int32_t on_device);
 /* Block preconditioner (MobilityPrecon.m:17-40). */
 int nnk_mob_precon(nnk_mob* mob, const double* x, double* y, int32_t on_device);
+/* No counterpart in the reference: replay the matvec (per FMM it runs on)
+ * from a CUDA graph captured on first use, and again after nnk_fmm_set_eps
+ * or nnk_fmm_autotune (default on; the result is bitwise that of the
+ * launches).  enable = 0 launches kernel by kernel. */
+int nnk_mob_use_graphs(nnk_mob* mob, int32_t enable);
 /* gmres(afunc, rhs, [], tol, maxit) with optional right preconditioning
  * (mobilityProblem.m:48-58); x receives the (preconditioned-back) solution. */
 int nnk_mob_solve(nnk_mob* mob, const double* rhs, double* x,

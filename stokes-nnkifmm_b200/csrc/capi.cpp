@@ -477,6 +477,15 @@ int nnk_mob_apply(nnk_mob* mob, const double* x, double* y, int32_t on_device) {
   API_CATCH(ctx)
 }
 
+int nnk_mob_use_graphs(nnk_mob* mob, int32_t enable) {
+  if (!mob) return NNK_E_ARG;
+  nnk_ctx* ctx = mob->fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  mob->m->use_graphs(enable != 0);
+  API_CATCH(ctx)
+}
+
 int nnk_mob_precon(nnk_mob* mob, const double* x, double* y, int32_t on_device) {
   if (!mob || !x || !y) return NNK_E_ARG;
   nnk_ctx* ctx = mob->fmm->ctx;

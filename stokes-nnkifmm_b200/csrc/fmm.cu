@@ -926,6 +926,7 @@ void Fmm::set_eps(double eps) {
   if (!(eps > 0)) throw Error(NNK_E_ARG, "eps must be > 0");
   NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
   p_.eps = eps;
+  ++version_;
   tensor_m2l_ = false;
   fft_m2l_ = false;
   build_operators();
@@ -978,6 +979,7 @@ double tune_groups(Fmm* self, std::vector<TaskGroup*>& groups, const std::vector
 }  // namespace
 
 std::pair<double, double> Fmm::autotune(int nrhs) {
+  ++version_;
   const HostTree& t = *t_;
   const int R = rhs_chunk(nrhs, tensor_m2l_ ? 1 : R_);
   cudaStream_t st = ctx_->stream;

@@ -135,6 +135,9 @@ class Fmm {
   // launch, from {64, 128, 256} (FP64: {64, 128}), for passes of nrhs
   // right-hand sides.  Returns the total pair-kernel time before and after.
   std::pair<double, double> autotune(int nrhs);
+  // Changes whenever launches captured earlier would be stale (new operators
+  // or tiles): set_eps and autotune.
+  uint64_t version() const { return version_; }
   // Trees of the forest the matvec evaluates (flags per tree, nullptr: all).
   // The kernels of a masked tree return at once and its output rows are
   // zero; the transpose and the gradients always evaluate every tree.
@@ -266,6 +269,7 @@ class Fmm {
   int64_t launches_[NNK_NUM_PHASES] = {0};
   cudaEvent_t event();
   std::unique_ptr<Fmm> sparse_;
+  uint64_t version_ = 0;
   // tree mask of the matvec (forests only): per tree, per node (expanded on
   // the device), and the leaf of each sorted target
   DBuf<int32_t> tree_on_, node_on_, node_tree_, tgt_leaf_;

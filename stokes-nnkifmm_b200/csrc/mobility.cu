@@ -251,11 +251,71 @@ void Mobility::small_solve(const std::vector<double>& inv, const double* in6, do
 
 void Mobility::apply(const double* x, double* y) { apply_with(fmm_, x, y); }
 
-void Mobility::apply_with(Fmm* f, const double* x, double* y) {
+Mobility::~Mobility() {
+  for (auto& g : graphs_)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+}
+
+void Mobility::use_graphs(bool on) {
+  graphs_on_ = on;
+  for (auto& g : graphs_)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  graphs_.clear();
+}
+
+void Mobility::apply_raw(Fmm* f, const double* x, double* y) {
   // b(1:3N) = FMM(f) + BT*UOm ; b(3N+1:end) = B*f
   f->apply(x, y, NNK_LAYOUT_BLOCKED, 1);
   bt_apply(x + 3 * N_, y);
   body_sums(x, y + 3 * N_);
+}
+
+// A small system's matvec is some 50 short launches: replayed from a graph
+// it costs one launch.  The graph reads and writes fixed buffers; a changed
+// FMM (new eps, new tiles) is captured again.
+void Mobility::apply_with(Fmm* f, const double* x, double* y) {
+  cudaStream_t st = ctx_->stream;
+  if (!graphs_on_ || f->profiling() || st == nullptr) {  // the legacy default stream cannot be captured
+    apply_raw(f, x, y);
+    return;
+  }
+  const int64_t n = size();
+  if (!gin_.p) {
+    gin_.alloc(n);
+    gout_.alloc(n);
+  }
+  Graph* g = nullptr;
+  for (auto& e : graphs_)
+    if (e.f == f) g = &e;
+  if (g && g->version != f->version()) {
+    cudaGraphExecDestroy(g->exec);
+    g->exec = nullptr;
+  }
+  if (!g) {
+    graphs_.push_back(Graph{f, 0, nullptr});
+    g = &graphs_.back();
+  }
+  if (!g->exec) {
+    NNK_CUDA(cudaStreamSynchronize(st));
+    NNK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    try {
+      apply_raw(f, gin_.p, gout_.p);
+    } catch (...) {
+      cudaStreamEndCapture(st, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      throw;
+    }
+    NNK_CUDA(cudaStreamEndCapture(st, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&g->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    NNK_CUDA(e);
+    g->version = f->version();
+  }
+  NNK_CUDA(cudaMemcpyAsync(gin_.p, x, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  NNK_CUDA(cudaGraphLaunch(g->exec, st));
+  NNK_CUDA(cudaMemcpyAsync(y, gout_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
 }
 
 void Mobility::set_refinement(Fmm* fp64, int max_outer, double inner_tol) {

@@ -16,9 +16,17 @@ class Mobility {
  public:
   Mobility(Fmm* fmm, int nbodies, const int64_t* body_start, const int64_t* fine_start,
            const double* rel_points, const double* rel_fine);
+  ~Mobility();
+  Mobility(const Mobility&) = delete;
+  Mobility& operator=(const Mobility&) = delete;
+  // Replay each matvec (per FMM it runs on) from a CUDA graph captured on
+  // first use and again after the FMM changed (default on; off launches
+  // kernel by kernel).
+  void use_graphs(bool on);
   int64_t size() const { return 3 * N_ + 6 * (int64_t)nb_; }
   void apply(const double* x, double* y);   // mobilityMatrixMulti.m:17-36
   void apply_with(Fmm* f, const double* x, double* y);
+  void apply_raw(Fmm* f, const double* x, double* y);
   // A^T = [F^T B^T; BT^T 0], F the FMM block (exact transpose of the passes)
   void apply_adjoint(const double* x, double* y);
   void apply_adjoint_with(Fmm* f, const double* x, double* y);
@@ -64,6 +72,14 @@ class Mobility {
   std::vector<int64_t> fstart_;        // per body: first fine row (NEAREST)
   DBuf<double> t6a_, t6b_, tv_, tv2_, tv3_;
   std::vector<double> h6a_, h6b_;
+  struct Graph {
+    Fmm* f;
+    uint64_t version;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Graph> graphs_;
+  bool graphs_on_ = true;
+  DBuf<double> gin_, gout_;  // the captured matvec's input and output
 };
 
 }  // namespace nnk

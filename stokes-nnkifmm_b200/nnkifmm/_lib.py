@@ -97,6 +97,7 @@ SIGNATURES = {
     "nnk_mob_create": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, C.POINTER(_vp)]),
     "nnk_mob_apply": (_i32, [_vp, _vp, _vp, _i32]),
     "nnk_mob_precon": (_i32, [_vp, _vp, _vp, _i32]),
+    "nnk_mob_use_graphs": (_i32, [_vp, _i32]),
     "nnk_mob_solve": (_i32, [_vp, _vp, _vp, C.POINTER(SolveParams), _i32, C.POINTER(SolveInfo), _i32]),
     "nnk_mob_set_refinement": (_i32, [_vp, _vp, _i32, _f64]),
     "nnk_mob_apply_adjoint": (_i32, [_vp, _vp, _vp, _i32]),

@@ -247,6 +247,10 @@ class Mobility:
                                              L.ptr(gy) if info.num_fine else None, 0), self.ctx.h, "gradient")
         return gx, gy
 
+    def use_graphs(self, enable=True):
+        """Replay the matvec from a CUDA graph (default) or launch kernel by kernel."""
+        L.check(L.lib.nnk_mob_use_graphs(self.h, int(bool(enable))), self.ctx.h, "use_graphs")
+
     def precon(self, x):
         x = self._vec(x)
         y = np.empty(self.n)

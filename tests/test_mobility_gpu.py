@@ -97,3 +97,28 @@ def test_mixed_refined_solve_matches_dense(precon):
     assert abs(Om_z - xd[-1]) / abs(xd[-1]) < 1e-4
     ref, _, _ = run_problem([1, 0, 0], [0, 0, 1], precon, precision="fp64")
     assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_replayed_matvec_is_bitwise_the_launches(precision):
+    """The mobility matvec replayed from a CUDA graph equals the kernel-by-
+    kernel launches bit for bit, and a graph captured before set_eps is not
+    reused after it (the operators changed)."""
+    c, f, NN, F, M = sphere_body([1, 0, 0], [0, 0, 1])
+    sw = nk.Swimmers()
+    sw.addSwimmer(c, f, NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(c), F, M)
+    sw.genTree(nodeCapacity=60, nearest=1)
+    sw.genKIFMM([0.01, 1.0], GMRES=1, format=2, precision=precision)
+    mob = sw.mobility()
+    x = np.random.default_rng(3).standard_normal(mob.n)
+    mob.use_graphs(False)
+    a = mob.apply(x)
+    mob.use_graphs(True)
+    b = mob.apply(x)   # captures
+    c2 = mob.apply(x)  # replays
+    assert np.array_equal(a, b) and np.array_equal(a, c2)
+    sw.FMM.setEps(0.02)
+    d = mob.apply(x)   # captured again
+    mob.use_graphs(False)
+    e = mob.apply(x)
+    assert np.array_equal(d, e) and not np.array_equal(d, a)
