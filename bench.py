@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-errors", action="store_true")
     ap.add_argument("--no-solves", action="store_true")
-    ap.add_argument("--batch-bodies", type=int, default=4)
+    ap.add_argument("--batch-bodies", type=int, default=16)
     ap.add_argument("--no-gradient", action="store_true")
     ap.add_argument("--no-squirmers", action="store_true")
     ap.add_argument("--m2l", default="auto", choices=["auto", "images", "generate", "pairs", "fft"],
@@ -180,11 +180,13 @@ def sampled_direct(torch, w, NN, idx):
 
 
 def solve_benchmarks(torch, nk, args):
-    """Mobility solves/s: config 1 (one sphere, 2 right-hand sides, GMRES to
-    1e-6, FP64 vs mixed) and a sample of config 4 (independent prolate bodies,
-    6 rigid-mode right-hand sides each; FP64 one body after another vs mixed
-    with bodies on concurrent streams).  Errors: rigid velocities against the
-    dense FP64 system (config 1) or against the FP64 GPU solves (config 4)."""
+    """Mobility solves/s: the rigid sphere (488 force / 9128 quadrature points,
+    2 right-hand sides, GMRES to 1e-6, FP64 vs mixed) and a sample of the
+    independent prolate bodies (--batch-bodies of them, 6 rigid-mode
+    right-hand sides each): plain FP64 one body and one right-hand side per
+    GMRES call, against the FP64 and the mixed forest batch.  Errors: rigid
+    velocities against the dense FP64 system (sphere) or against the plain
+    FP64 GPU solves (bodies)."""
     from nnkifmm.workloads import batched_bodies, sphere_problem
     from oracle import mobility as om
     out = {}
@@ -228,7 +230,7 @@ def solve_benchmarks(torch, nk, args):
     setup = time.perf_counter() - t0
     seq[0].solve_modes(1e-6, 400, modes=RIGID_MODES[:1])  # first-call initialisation
     dts = []
-    for _ in range(2):
+    for _ in range(1 if nb > 8 else 2):  # one pass over 16 bodies is ~40 s
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         outs = [b.solve_modes(1e-6, 400) for b in seq]
@@ -242,7 +244,7 @@ def solve_benchmarks(torch, nk, args):
         setup = time.perf_counter() - t0
         B.solve_modes(tol=1e-6, maxIter=400)  # first call: CUDA-graph capture
         dts = []
-        for _ in range(3):
+        for _ in range(1 if (prec == "fp64" and nb > 8) else 3):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             mats, its = B.solve_modes(tol=1e-6, maxIter=400)
@@ -253,7 +255,8 @@ def solve_benchmarks(torch, nk, args):
     n_solves = 6 * nb
     for label, (mats, dt, setup, its) in res.items():
         out[f"batched_{label}"] = {"solves_per_s": n_solves / dt, "s_total": dt, "setup_s": setup,
-                                   "timing": "median of repeated solves after one warm-up solve",
+                                   "timing": "after one warm-up solve: median of 3 repeats (one pass for the FP64 "
+                                             "arms above 8 bodies)",
                                    "gmres_iters_mean": float(np.mean([i[2] for it in its for i in it])),
                                    "rel_err_vs_fp64": float(max(np.linalg.norm(a - b) / np.linalg.norm(b)
                                                                 for a, b in zip(mats, ref)))}

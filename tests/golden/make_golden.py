@@ -66,7 +66,7 @@ def mixed_points(rng, n, nsph=3):
 
 
 def sphere_case():
-    """Config 1 geometry: Sphere(1,[0 0 0],10) force nodes, Sphere(...,40) quadrature."""
+    """Rigid-sphere geometry: Sphere(1,[0 0 0],10) force nodes, Sphere(...,40) quadrature."""
     rng = np.random.default_rng(20261203)
     c = sphere(1.0, [0, 0, 0], 10)
     f = sphere(1.0, [0, 0, 0], 40)

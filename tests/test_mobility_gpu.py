@@ -1,4 +1,4 @@
-"""GPU mobility solve (config 1: one rigid sphere, NEAREST, p=6, eps=0.01)
+"""GPU mobility solve of one rigid sphere (NEAREST, p=6, eps=0.01, 488 force points)
 against the dense FP64 regularized-Stokeslet system, and the known answers
 U = F/(6 pi mu a), Omega = M/(8 pi mu a^3)."""
 import os

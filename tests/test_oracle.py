@@ -65,7 +65,7 @@ def test_sphere_drag_known_answer():
 
 
 def test_mobility_sphere_known_answers():
-    """U = F/(6 pi mu a), Omega = M/(8 pi mu a^3) for the config-1 sphere."""
+    """U = F/(6 pi mu a), Omega = M/(8 pi mu a^3) for the rigid sphere of 488 force points."""
     c = sphere(1.0, [0, 0, 0], 10)
     f = sphere(1.0, [0, 0, 0], 40)
     NN = nearest_matrix(c, f)

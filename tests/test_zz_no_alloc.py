@@ -6,7 +6,7 @@ fixed memory budget).  This entry point evaluates the NEAREST velocity by
 direct summation using only caller-supplied device buffers plus a static
 scratch array inside the library.  Here it is compared, on two calls in a row
 with different forces, with the existing allocating entry point computeVel
-(nnk_fmm_apply, FP64) on the config-1 sphere, where the FMM is within 1e-5 of
+(nnk_fmm_apply, FP64) on the 488-point rigid sphere, where the FMM is within 1e-5 of
 the direct sum, and with the oracle's FP64 direct sum.
 
 This file is collected last so that a run stopping at the first failure has
