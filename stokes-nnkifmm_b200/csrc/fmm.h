@@ -146,6 +146,10 @@ class Fmm {
   Fmm& sparse();
   void reduced_apply(const double* d_in, double* d_out, int layout);
   void reduced_solve(const double* d_in, double* d_out, int layout);
+  // The same through the explicit inverses of the leaf blocks (built on
+  // first use): not backward stable, but one batched product; for the
+  // preconditioner.
+  void reduced_solve_inv(const double* d_in, double* d_out, int layout);
   nnk_fmm_stats stats() const { return stats_; }
   // per-phase CUDA-event timing (NNK_PHASE_*)
   void set_profile(bool on);
@@ -256,6 +260,10 @@ class Fmm {
   DBuf<double> rrhs_;
   DBuf<double*> rrhsptr_;
   DBuf<double> rmat_;            // unfactored blocks for reduced_apply
+  bool rinv_ready_ = false;
+  DBuf<double> rinv_;            // explicit inverses of the blocks (reduced_solve_inv)
+  DBuf<double*> rinvptr_;
+  DBuf<double> rsol_;            // nleaf * rdim: block solutions
   std::vector<int32_t> rleaf_;   // target leaves in order
   DBuf<int32_t> rleaf_d_;
   DBuf<int64_t> rts_;            // tgt_start on the device

@@ -15,6 +15,17 @@ __device__ __forceinline__ void cross3(const double* a, const double* b, double*
 }
 
 // y_c(n) += -U_b,c + (x_n x Om_b)_c : BT*[U;Om] (genMatrixComponets.m:182-198)
+// out6 = per body its 6x6 inverse times in6 (layout [U_x(1..nb) U_y U_z Om_x Om_y Om_z])
+__global__ void small_solve_kernel(int nb, const double* __restrict__ inv, const double* __restrict__ in6,
+                                   double* __restrict__ out6) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= 6 * nb) return;
+  const int b = g / 6, i = g % 6;
+  double s = 0;
+  for (int k = 0; k < 6; ++k) s += inv[36 * b + i * 6 + k] * in6[k * nb + b];
+  out6[i * nb + b] = s;
+}
+
 __global__ void bt_kernel(int64_t N, int nb, const int* __restrict__ body, const double* __restrict__ xrel,
                           const double* __restrict__ uo, double* __restrict__ y) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -203,8 +214,8 @@ Mobility::Mobility(Fmm* fmm, int nbodies, const int64_t* body_start, const int64
   tv_.alloc(3 * N_);
   tv2_.alloc(3 * N_);
   tv3_.alloc(3 * N_);
-  h6a_.resize(6 * (size_t)nb_);
-  h6b_.resize(6 * (size_t)nb_);
+  a1inv_d_.upload(a1inv_, st);
+  a2inv_d_.upload(a2inv_, st);
   NNK_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -232,21 +243,10 @@ void Mobility::body_sums_t(const double* z6, double* f, double a) {
   NNK_CHECK_LAUNCH();
 }
 
-void Mobility::small_solve(const std::vector<double>& inv, const double* in6, double* out6) {
-  cudaStream_t st = ctx_->stream;
-  NNK_CUDA(cudaMemcpyAsync(h6a_.data(), in6, 6 * nb_ * sizeof(double), cudaMemcpyDeviceToHost, st));
-  NNK_CUDA(cudaStreamSynchronize(st));
-  for (int b = 0; b < nb_; ++b) {
-    double v[6], o[6];
-    for (int k = 0; k < 6; ++k) v[k] = h6a_[k * nb_ + b];
-    for (int i = 0; i < 6; ++i) {
-      double s = 0;
-      for (int k = 0; k < 6; ++k) s += inv[36 * b + i * 6 + k] * v[k];
-      o[i] = s;
-    }
-    for (int k = 0; k < 6; ++k) h6b_[k * nb_ + b] = o[k];
-  }
-  NNK_CUDA(cudaMemcpyAsync(out6, h6b_.data(), 6 * nb_ * sizeof(double), cudaMemcpyHostToDevice, st));
+void Mobility::small_solve(const DBuf<double>& inv, const double* in6, double* out6) {
+  if (nb_ == 0) return;
+  small_solve_kernel<<<(6 * nb_ + 127) / 128, 128, 0, ctx_->stream>>>(nb_, inv.p, in6, out6);
+  NNK_CHECK_LAUNCH();
 }
 
 void Mobility::apply(const double* x, double* y) { apply_with(fmm_, x, y); }
@@ -329,20 +329,22 @@ void Mobility::precon(const double* x, double* y) {
   cudaStream_t st = ctx_->stream;
   const double* f = x;
   const double* uo = x + 3 * N_;
-  // b_f = reducedSolve(f)
-  fmm_->reduced_solve(f, y, NNK_LAYOUT_BLOCKED);
+  // b_f = reducedSolve(f), through the leaf blocks' explicit inverses (a
+  // preconditioner needs no backward-stable solve; one batched product is
+  // several times faster than the batched triangular solves)
+  fmm_->reduced_solve_inv(f, y, NNK_LAYOUT_BLOCKED);
   if (nb_ > 0) {
     // out = -A2 \ (BT' * computeVelSparse(B' * (A1 \ UOm)))
-    small_solve(a1inv_, uo, t6a_.p);
+    small_solve(a1inv_d_, uo, t6a_.p);
     body_sums_t(t6a_.p, tv_.p, 0.0);
     fmm_->sparse().apply(tv_.p, tv2_.p, NNK_LAYOUT_BLOCKED, 1);
     btt_apply(tv2_.p, t6b_.p);
-    small_solve(a2inv_, t6b_.p, y + 3 * N_);
+    small_solve(a2inv_d_, t6b_.p, y + 3 * N_);
     dev_axpby(ctx_, -1.0, y + 3 * N_, 0.0, nullptr, y + 3 * N_, 6 * nb_);
     // b_f -= reducedSolve(BT * out)
     NNK_CUDA(cudaMemsetAsync(tv_.p, 0, 3 * N_ * sizeof(double), st));
     bt_apply(y + 3 * N_, tv_.p);
-    fmm_->reduced_solve(tv_.p, tv3_.p, NNK_LAYOUT_BLOCKED);
+    fmm_->reduced_solve_inv(tv_.p, tv3_.p, NNK_LAYOUT_BLOCKED);
     dev_axpby(ctx_, 1.0, y, -1.0, tv3_.p, y, 3 * N_);
   }
 }

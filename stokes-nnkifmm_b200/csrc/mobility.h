@@ -52,7 +52,7 @@ class Mobility {
   void body_sums_t(const double* z6, double* f, double a); // f = a*f + B^T z
   void bt_apply(const double* uo, double* y);              // y += BT * [U;Om]
   void btt_apply(const double* v, double* out6);           // BT^T v
-  void small_solve(const std::vector<double>& inv, const double* in6, double* out6);  // host 6x6 blocks
+  void small_solve(const DBuf<double>& inv, const double* in6, double* out6);  // per body 6x6 blocks
 
   Fmm* fmm_;
   Fmm* ref64_ = nullptr;
@@ -68,10 +68,10 @@ class Mobility {
   DBuf<double> xm_;         // per point torque arm: sum_q NN(q,n) X_q (NEAREST) or xrel (genMatrixComponets.m:217-222)
   DBuf<double> af_;         // per point force weight: column sum of NN (NEAREST) or 1 (:208-209, :228)
   std::vector<double> a1inv_, a2inv_;  // per body 6x6 inverses of B B^T and BT^T BT
+  DBuf<double> a1inv_d_, a2inv_d_;     // the same on the device
   std::vector<int32_t> hbody_;         // per point: body or -1 (host copy)
   std::vector<int64_t> fstart_;        // per body: first fine row (NEAREST)
   DBuf<double> t6a_, t6b_, tv_, tv2_, tv3_;
-  std::vector<double> h6a_, h6b_;
   struct Graph {
     Fmm* f;
     uint64_t version;

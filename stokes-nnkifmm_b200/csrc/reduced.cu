@@ -99,6 +99,7 @@ __global__ void block_gemv_kernel(int D, const double* __restrict__ mats, const 
 
 void Fmm::build_reduced() {
   if (reduced_ready_) return;
+  rinv_ready_ = false;
   const HostTree& t = *t_;
   if (t.n_pot != t.n_tgt || t.n_pot != t.n)
     throw Error(NNK_E_ARG, "reducedSolve needs potentials == targets");
@@ -202,6 +203,39 @@ void Fmm::reduced_solve(const double* d_in, double* d_out, int layout) {
       cublasDgetrsBatched(h, CUBLAS_OP_N, D, 1, rptr_.p, D, rpiv_.p, rrhsptr_.p, D, &info, nl);
   if (s != CUBLAS_STATUS_SUCCESS || info != 0) throw Error(NNK_E_CUDA, "batched leaf-block solve failed");
   reduced_scatter_kernel<<<nl, 128, 0, st>>>(D, rleaf_d_.p, (const long long*)rts_.p, trow_.p, rrhs_.p, layout,
+                                             t.n_tgt, d_out);
+  NNK_CHECK_LAUNCH();
+}
+
+void Fmm::reduced_solve_inv(const double* d_in, double* d_out, int layout) {
+  build_reduced();
+  const HostTree& t = *t_;
+  cudaStream_t st = ctx_->stream;
+  const int nl = (int)rleaf_.size(), D = rdim_;
+  if (!nl) return;
+  if (!rinv_ready_) {
+    rinv_.alloc((size_t)nl * D * D);
+    rsol_.alloc((size_t)nl * D);
+    std::vector<double*> ptr(nl);
+    for (int k = 0; k < nl; ++k) ptr[k] = rinv_.p + (size_t)k * D * D;
+    rinvptr_.upload(ptr, st);
+    cublasHandle_t h = (cublasHandle_t)blas_;
+    cublasSetStream(h, st);
+    if (cublasDgetriBatched(h, D, rptr_.p, D, rpiv_.p, rinvptr_.p, D, rinfo_.p, nl) != CUBLAS_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "batched inverse of the leaf blocks failed");
+    std::vector<int> info(nl);
+    NNK_CUDA(cudaMemcpyAsync(info.data(), rinfo_.p, nl * sizeof(int), cudaMemcpyDeviceToHost, st));
+    NNK_CUDA(cudaStreamSynchronize(st));
+    for (int k = 0; k < nl; ++k)
+      if (info[k] != 0) throw Error(NNK_E_ARG, "singular leaf block in reducedSolve");
+    rinv_ready_ = true;
+  }
+  reduced_gather_kernel<<<nl, 128, 0, st>>>(D, rleaf_d_.p, (const long long*)rts_.p, trow_.p, d_in, layout, t.n_tgt,
+                                            rrhs_.p);
+  NNK_CHECK_LAUNCH();
+  block_gemv_kernel<<<nl, 128, 0, st>>>(D, rinv_.p, rrhs_.p, rsol_.p);
+  NNK_CHECK_LAUNCH();
+  reduced_scatter_kernel<<<nl, 128, 0, st>>>(D, rleaf_d_.p, (const long long*)rts_.p, trow_.p, rsol_.p, layout,
                                              t.n_tgt, d_out);
   NNK_CHECK_LAUNCH();
 }
