@@ -12,3 +12,4 @@ from .octree import OcTree, nearestMatrix  # noqa: F401
 from .kifmm import KIFMM  # noqa: F401
 from .mobility import Swimmers, Mobility, mobilityProblem, mobilityRHS, richardson  # noqa: F401
 from .batch import BatchMobility  # noqa: F401
+from .resistance import Gen_Resistance, Rigid_Resistance, velocityModes  # noqa: F401

@@ -57,6 +57,7 @@ class OcTree:
         self.nodeCount = info.node_count
         self.nodeCapacity = info.node_capacity
         self.finePoints = fine if nearest else None
+        self._nn = sp.csr_matrix(NN) if (nearest and NN is not None) else None
         self._cache = {}
 
     _destroy = L.lib.nnk_tree_destroy  # held by the class: module globals may be gone at exit
@@ -112,6 +113,16 @@ class OcTree:
     @property
     def points(self):
         return self._points()[0]
+
+    @property
+    def NN(self):
+        """tree.NN (Q x N, NEAREST mode): the matrix given, or the one the tree
+        was built with (recomputed here bit for bit; both builders are exact)."""
+        if self.finePoints is None:
+            return None
+        if self._nn is None:
+            self._nn = nearestMatrix(self.points, self.finePoints, device=self.ctx.device)
+        return self._nn
 
     @property
     def potentials(self):

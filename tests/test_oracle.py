@@ -150,3 +150,40 @@ def test_dense_gradient_matches_finite_differences():
     lp = og.loss(X, Y, NN, eps + h, mu, F, M, Us)
     lm = og.loss(X, Y, NN, eps - h, mu, F, M, Us)
     assert abs((lp - lm) / (2 * h) - ge) <= 1e-6 * max(1.0, abs(ge))
+
+
+def test_resistance_formulas_invert_the_dense_mobility_matrix():
+    """The resistance problem (Rigid_Resistance.m / Gen_Resistance.m: impose
+    U + Omega x X, solve S kron(NN, I3) f = u, sum forces and moments) with
+    the dense FP64 operator gives the inverse of the dense 6 x 6 mobility
+    matrix of the same discretization, and the point velocities follow
+    velocityModes.m."""
+    import scipy.sparse as sp
+    from nnkifmm.resistance import force_moment, velocityModes
+    from oracle import mobility as om
+    from oracle.geometry import sphere, velocity_modes
+    from oracle.kernel import kernel
+    from oracle.nearest import nearest_matrix
+    c, f = sphere(1.0, [0, 0, 0], 5), sphere(1.0, [0, 0, 0], 12)
+    NN = sp.csr_matrix(nearest_matrix(c, f))
+    eps, mu = 0.05, 1.0
+    rng = np.random.default_rng(4)
+    X = rng.random((7, 3))
+    assert np.allclose(velocityModes(X, [1, 2, 3], [0.5, -1, 2]), velocity_modes(X, [1, 2, 3], [0.5, -1, 2]))
+    A = kernel(f, c, eps, mu) @ sp.kron(NN, sp.identity(3)).toarray()
+    R = np.zeros((6, 6))
+    for j in range(6):
+        vel, mom = np.zeros(3), np.zeros(3)
+        (vel if j < 3 else mom)[j % 3] = 1.0
+        fr = np.linalg.solve(A, velocityModes(c, vel, mom).ravel()).reshape(-1, 3)
+        F, M = force_moment(fr, c, NN, f)
+        R[:3, j], R[3:, j] = F, M
+    Mob = np.zeros((6, 6))
+    for j in range(6):
+        F, M = np.zeros(3), np.zeros(3)
+        (F if j < 3 else M)[j % 3] = 1.0
+        body = om.Body(c, f, NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(c), F, M)
+        asm = om.assemble([body])
+        Mob[:, j] = np.linalg.solve(om.dense_mobility_matrix(asm, eps, mu, True), om.mobility_rhs(asm))[-6:]
+    assert np.linalg.norm(R @ Mob - np.eye(6)) <= 1e-8
+    assert np.linalg.norm(R - R.T) <= 1e-6 * np.linalg.norm(R)  # the grand resistance matrix is symmetric
