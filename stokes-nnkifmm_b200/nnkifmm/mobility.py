@@ -311,6 +311,23 @@ def mobilityProblem(swimmers, fluidFunc, t, conditions, kernelPar, TreePar, thre
     return out
 
 
+def mobilityProblemGravity(swimmers, fluidFunc, t, conditions, kernelPar, TreePar, threads=0, GPU=1,
+                           blockSize=0.1, tol=1e-6, maxIter=None, PreconSettings=None, gravPar=(0, 0, -1, 0),
+                           precision="fp64", return_info=False, refine=None):
+    """Mobility/mobilityProblemGravity.m:1-74: mobilityProblem with every
+    swimmer forced by gravity, F = G and M = -4/3 pi offset (b3 x G) for
+    gravPar = [G (3); offset] (Swimmers.m:372-385), set after its centre and
+    basis are updated from `conditions`."""
+    conditions = np.asarray(conditions, float).ravel()
+    g = np.asarray(gravPar, float).ravel()
+    for i in range(conditions.size // 9):
+        d = conditions[9 * i:9 * i + 9]
+        swimmers.updateSwimmmer(i + 1, d[0:3], d[3:9])
+        swimmers.updateSwimmmerRHS(i + 1, g[0:3], g[3])
+    return mobilityProblem(swimmers, fluidFunc, t, conditions, kernelPar, TreePar, threads, GPU, blockSize, tol,
+                           maxIter, PreconSettings, precision, return_info, refine)
+
+
 def richardson(values, eps):
     """Extrapolation to eps -> 0 of results at two regularisation widths,
     assuming an O(eps) error (the regularized Stokeslet's leading term):

@@ -122,3 +122,27 @@ def test_graph_replayed_matvec_is_bitwise_the_launches(precision):
     mob.use_graphs(False)
     e = mob.apply(x)
     assert np.array_equal(d, e) and not np.array_equal(d, a)
+
+
+def test_gravity_forcing_vs_dense():
+    """mobilityProblemGravity.m: a sphere with its centre of mass offset along
+    its axis b3, under gravity G: F = G, M = -4/3 pi offset (b3 x G); rigid
+    velocities against the dense FP64 system with the same forcing."""
+    c, f, NN, _, _ = sphere_body([0, 0, 0], [0, 0, 0])
+    G, offset = np.array([0.3, 0.0, -1.0]), 0.2
+    b = [1, 0, 0, 0, 1, 0]  # b3 = e_z
+    sw = nk.Swimmers()
+    sw.addSwimmer(c, f, NN, [0, 0, 0], b, np.zeros_like(c), [0, 0, 0], [0, 0, 0])
+    out = nk.mobilityProblemGravity(sw, None, 0.0, np.array([0, 0, 0] + b, float), [0.01, 1.0],
+                                    {"nodeCapacity": 60, "nearest": 1}, tol=1e-9, maxIter=300,
+                                    gravPar=list(G) + [offset])
+    M = -4.0 / 3.0 * np.pi * offset * np.cross([0, 0, 1.0], G)
+    assert np.allclose(sw.F[0], G) and np.allclose(sw.Moment[0], M)
+    body = om.Body(c, f, NN, [0, 0, 0], b, np.zeros_like(c), G, M)
+    asm = om.assemble([body])
+    xd = np.linalg.solve(om.dense_mobility_matrix(asm, 0.01, 1.0, True), om.mobility_rhs(asm))
+    U, Om = xd[-6:-3], xd[-3:]
+    ref = np.concatenate([U, np.cross(Om, [1, 0, 0]), np.cross(Om, [0, 1, 0])])
+    assert np.linalg.norm(out - ref) <= 1e-5 * np.linalg.norm(ref)
+    # it sinks at about G / (6 pi) and turns its heavy side down
+    assert abs(out[2] * 6 * np.pi / G[2] - 1) < 1e-2 and abs(Om[1]) > 0
