@@ -134,7 +134,7 @@ def test_gravity_forcing_vs_dense():
     sw = nk.Swimmers()
     sw.addSwimmer(c, f, NN, [0, 0, 0], b, np.zeros_like(c), [0, 0, 0], [0, 0, 0])
     out = nk.mobilityProblemGravity(sw, None, 0.0, np.array([0, 0, 0] + b, float), [0.01, 1.0],
-                                    {"nodeCapacity": 60, "nearest": 1}, tol=1e-9, maxIter=300,
+                                    {"nodeCapacity": 60, "nearest": 1}, tol=1e-8, maxIter=300,
                                     gravPar=list(G) + [offset])
     M = -4.0 / 3.0 * np.pi * offset * np.cross([0, 0, 1.0], G)
     assert np.allclose(sw.F[0], G) and np.allclose(sw.Moment[0], M)
