@@ -61,6 +61,16 @@ __global__ void combine_kernel(const double* __restrict__ V, int64_t n, int k, c
   }
 }
 
+// v = w / sqrt(nrm2[0]) (zero when nrm2 <= 0): the new Arnoldi vector,
+// normalized on the device so that a step needs one host synchronisation
+__global__ void normalize_kernel(const double* __restrict__ w, const double* __restrict__ nrm2,
+                                 double* __restrict__ v, int64_t n) {
+  const double q = nrm2[0];
+  const double a = q > 0.0 ? 1.0 / sqrt(q) : 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = a * w[i];
+}
+
 unsigned grid_for(int64_t n) {
   int64_t g = (n + 255) / 256;
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, kRedBlocks));
@@ -94,11 +104,27 @@ void Gmres::solve(const Op& op, const Op* post, const double* b, double* x, cons
   const int maxit = sp.maxit > 0 ? sp.maxit : (int)std::min<int64_t>(n, 10);
   int m = sp.restart > 0 ? sp.restart : maxit;  // restart = [] -> unrestarted
   m = (int)std::min<int64_t>(m, std::max<int64_t>(n, 1));
-  V_.alloc((size_t)(m + 1) * n);
+  // The Krylov basis grows on demand (doubling up to m + 1 vectors): a solve
+  // that converges in a few dozen steps does not allocate maxit + 1 vectors
+  // (1.2 GB for 150k unknowns and maxit 1000) every time.
+  int vcap = std::min(m + 1, 32);
+  V_.alloc((size_t)vcap * n);
+  auto reserve = [&](int need) {
+    if (need <= vcap) return;
+    int nc = vcap;
+    while (nc < need) nc = std::min(m + 1, 2 * nc);
+    DBuf<double> V2((size_t)nc * n);
+    NNK_CUDA(cudaMemcpyAsync(V2.p, V_.p, (size_t)vcap * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    NNK_CUDA(cudaStreamSynchronize(st));
+    V_ = std::move(V2);
+    vcap = nc;
+  };
   w_.alloc(n);
   r_.alloc(n);
   tmp_.alloc(n);
-  h_.alloc(m + 2);
+  // per step: [pass-1 h (m+1) | pass-2 h (m+1) | ||w||^2]
+  h_.alloc(2 * (size_t)(m + 1) + 1);
+  std::vector<double> hh(2 * (size_t)(m + 1) + 1);
   NNK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), st));
   const double nb = std::sqrt(dev_dot(ctx_, b, b, n, tmp_));
   info = nnk_solve_info{0, 0, 0.0};
@@ -122,25 +148,33 @@ void Gmres::solve(const Op& op, const Op* post, const double* b, double* x, cons
     int k = 0;
     bool stop = false;
     for (int j = 0; j < m && total < maxit; ++j) {
+      reserve(j + 2);  // reads V_0..V_j, writes V_{j+1}
       double* vj = V_.p + (size_t)j * n;
       double* vn = V_.p + (size_t)(j + 1) * n;
       op(vj, w_.p);
-      // CGS2: two passes of h = V^T w, w -= V h
-      std::fill(hcol.begin(), hcol.end(), 0.0);
+      // CGS2: two passes of h = V^T w, w -= V h, then ||w||^2 and the new
+      // vector on the device; one copy of the coefficients to the host
+      double* h2 = h_.p + (j + 1);
+      double* nrm = h_.p + 2 * (j + 1);
+      NNK_CUDA(cudaMemsetAsync(h_.p, 0, (2 * (size_t)(j + 1) + 1) * sizeof(double), st));
       for (int pass = 0; pass < 2; ++pass) {
-        NNK_CUDA(cudaMemsetAsync(h_.p, 0, (j + 1) * sizeof(double), st));
-        multidot_kernel<<<dim3(grid_for(n), j + 1), 256, 0, st>>>(V_.p, n, w_.p, h_.p);
+        double* hp = pass ? h2 : h_.p;
+        multidot_kernel<<<dim3(grid_for(n), j + 1), 256, 0, st>>>(V_.p, n, w_.p, hp);
         NNK_CHECK_LAUNCH();
-        multiaxpy_kernel<<<grid_for(n), 256, (j + 1) * sizeof(double), st>>>(V_.p, n, j + 1, h_.p, w_.p);
+        multiaxpy_kernel<<<grid_for(n), 256, (j + 1) * sizeof(double), st>>>(V_.p, n, j + 1, hp, w_.p);
         NNK_CHECK_LAUNCH();
-        std::vector<double> hp(j + 1);
-        NNK_CUDA(cudaMemcpyAsync(hp.data(), h_.p, (j + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
-        NNK_CUDA(cudaStreamSynchronize(st));
-        for (int i = 0; i <= j; ++i) hcol[i] += hp[i];
       }
-      const double hn = std::sqrt(dev_dot(ctx_, w_.p, w_.p, n, tmp_));
+      multidot_kernel<<<dim3(grid_for(n), 1), 256, 0, st>>>(w_.p, n, w_.p, nrm);
+      NNK_CHECK_LAUNCH();
+      normalize_kernel<<<grid_for(n), 256, 0, st>>>(w_.p, nrm, vn, n);
+      NNK_CHECK_LAUNCH();
+      NNK_CUDA(cudaMemcpyAsync(hh.data(), h_.p, (2 * (size_t)(j + 1) + 1) * sizeof(double), cudaMemcpyDeviceToHost,
+                               st));
+      NNK_CUDA(cudaStreamSynchronize(st));
+      std::fill(hcol.begin(), hcol.end(), 0.0);
+      for (int i = 0; i <= j; ++i) hcol[i] = hh[i] + hh[j + 1 + i];
+      const double hn = std::sqrt(std::max(0.0, hh[2 * (j + 1)]));
       hcol[j + 1] = hn;
-      if (hn > 0) dev_axpby(ctx_, 1.0 / hn, w_.p, 0.0, nullptr, vn, n);
       // apply previous rotations, then a new one that zeroes hcol[j+1]
       for (int i = 0; i < j; ++i) {
         const double t0 = cs[i] * hcol[i] + sn[i] * hcol[i + 1];
