@@ -311,8 +311,8 @@ def gradient_benchmark(torch, nk, args):
                        f"eps=0.005, nodeCapacity 64, F=(1,0,0), GMRES tol 1e-6"}
     grads = {}
     for prec in ["mixed", "fp64"]:
-        best = None
-        for _ in range(2):  # the second run has warm caches and libraries
+        fw, bw = [], []
+        for rep in range(4):  # one warm-up run (first-call library set-up), then the median of 3
             X = torch.tensor(Xb, requires_grad=True)
             Y = torch.tensor(Yb, requires_grad=True)
             e = torch.tensor(0.005, dtype=torch.float64, requires_grad=True)
@@ -321,10 +321,13 @@ def gradient_benchmark(torch, nk, args):
             t1 = time.perf_counter()
             ((U - torch.tensor(Us)) ** 2).sum().backward()
             t2 = time.perf_counter()
-            best = (t1 - t0, t2 - t1)
+            if rep:
+                fw.append(t1 - t0)
+                bw.append(t2 - t1)
+        f_s, b_s = float(np.median(fw)), float(np.median(bw))
         grads[prec] = (X.grad.numpy().copy(), Y.grad.numpy().copy(), float(e.grad))
-        out[prec] = {"forward_s": best[0], "backward_s": best[1],
-                     "forward_plus_adjoint_over_forward": (best[0] + best[1]) / best[0]}
+        out[prec] = {"forward_s": f_s, "backward_s": b_s, "forward_plus_adjoint_over_forward": (f_s + b_s) / f_s,
+                     "timing": "median of 3 runs after a warm-up run"}
     gm, g6 = grads["mixed"], grads["fp64"]
     out["mixed_vs_fp64_gradient"] = {
         "X": float(np.linalg.norm(gm[0] - g6[0]) / np.linalg.norm(g6[0])),
