@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--no-gradient", action="store_true")
     ap.add_argument("--no-squirmers", action="store_true")
     ap.add_argument("--m2l", default="auto", choices=["auto", "images", "generate", "pairs", "fft"],
-                    help="M2L form of the mixed matvec (auto: tcgen05 TF32 for one right-hand side)")
+                    help="M2L form of the mixed matvec (auto: tensor cores on rank-256 compressed operators)")
     ap.add_argument("--batch-apply", type=int, default=0,
                     help="only build the mixed batch of --batch-bodies bodies and time this many matvecs "
                          "(6 rigid-mode right-hand sides each; for profiling the batch kernels)")
