@@ -594,7 +594,7 @@ inline void launch_reduce(const RedD* reds, int nreds, const Real* partial, Real
 // -------------------------------------------------------------------- C2E
 // Check-to-equivalent step for the nodes of one level:
 //   dst(node, k) = Aop * check(node, k), Aop = A (upward) or A^T (downward),
-// for right-hand sides k < R, FP64 arithmetic.  A tile is up to 32 nodes that
+// for right-hand sides k < R, FP64 arithmetic.  A tile is up to 64 nodes that
 // share one operator (a level of one tree of the forest); A is the n x n
 // column-major operator ops + op * n^2.  check and dst hold, per surface
 // point p of a node, R consecutive 3-vectors: check[(node * P + p) * R + k].

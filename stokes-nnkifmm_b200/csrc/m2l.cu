@@ -680,8 +680,9 @@ __global__ void basis_float_kernel(const double* __restrict__ Bd, int n3, int RC
 //              y = tf32(v), y_lo = tf32(v - y);
 //   trans = 0 (expansion check += B c^): A(r, k) = B[r][k], r < 3P, k < RC,
 //              y accumulated.
-// 64 x 64 output tile (rows x nodes) per CTA of 256 threads, 4 x 4 each, K in
-// steps of 16, FP32.
+// 64 x 64 output tile (rows x nodes) per CTA of 256 threads, 4 x 4 each
+// (rows 4 tr .. 4 tr + 3, nodes 4 tc .. 4 tc + 3, both read from shared memory
+// as one float4), K in steps of 16, FP32.
 __global__ void __launch_bounds__(256) basis_apply_kernel(const float* __restrict__ basis, int n3, int RC,
                                                           int trans, const BasisTile* __restrict__ tiles,
                                                           const int* __restrict__ nodes,
@@ -689,8 +690,8 @@ __global__ void __launch_bounds__(256) basis_apply_kernel(const float* __restric
                                                           float* __restrict__ y, long long ldy,
                                                           float* __restrict__ y_lo = nullptr) {
   constexpr int BM = 64, BN = 64, BK = 16;
-  __shared__ float As[BK][BM + 1];
-  __shared__ float Xs[BK][BN + 1];
+  __shared__ __align__(16) float As[BK][BM + 4];
+  __shared__ __align__(16) float Xs[BK][BN + 4];
   __shared__ int col_node[BN];
   const BasisTile tl = tiles[blockIdx.y];
   const int rows = trans ? RC : n3, K = trans ? n3 : RC;
@@ -725,11 +726,9 @@ __global__ void __launch_bounds__(256) basis_apply_kernel(const float* __restric
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
-      float a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][tr + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Xs[kk][tc + 16 * j];
+      const float4 a4 = *reinterpret_cast<const float4*>(&As[kk][4 * tr]);
+      const float4 b4 = *reinterpret_cast<const float4*>(&Xs[kk][4 * tc]);
+      const float a[4] = {a4.x, a4.y, a4.z, a4.w}, b[4] = {b4.x, b4.y, b4.z, b4.w};
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -740,7 +739,7 @@ __global__ void __launch_bounds__(256) basis_apply_kernel(const float* __restric
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int r = m0 + tr + 16 * i, node = col_node[tc + 16 * j];
+      const int r = m0 + 4 * tr + i, node = col_node[4 * tc + j];
       if (r >= rows || node < 0) continue;
       float* o = y + (size_t)node * ldy + r;
       if (trans) {
