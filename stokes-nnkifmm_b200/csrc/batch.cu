@@ -554,6 +554,10 @@ void BatchMobility::apply_with(Fmm& f, const double* x, double* y) {
     gin_.alloc(n_);
     gout_.alloc(n_);
   }
+  if (graph_[slot] && graph_version_[slot] != f.version()) {  // a new or changed FMM in this slot
+    cudaGraphExecDestroy(graph_[slot]);
+    graph_[slot] = nullptr;
+  }
   if (!graph_[slot]) {
     NNK_CUDA(cudaStreamSynchronize(st));
     NNK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -570,6 +574,7 @@ void BatchMobility::apply_with(Fmm& f, const double* x, double* y) {
     const cudaError_t e = cudaGraphInstantiate(&graph_[slot], g, 0);
     cudaGraphDestroy(g);
     NNK_CUDA(e);
+    graph_version_[slot] = f.version();
   }
   NNK_CUDA(cudaMemcpyAsync(gin_.p, x, n_ * sizeof(double), cudaMemcpyDeviceToDevice, st));
   NNK_CUDA(cudaGraphLaunch(graph_[slot], st));

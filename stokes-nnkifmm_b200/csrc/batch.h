@@ -117,6 +117,7 @@ class BatchMobility {
   DBuf<long long> body_row0_;  // per body: first force point in forest order (B + 1)
   bool graphs_on_ = true;
   cudaGraphExec_t graph_[2] = {nullptr, nullptr};  // matvec of fmm_ and of ref64_
+  uint64_t graph_version_[2] = {0, 0};             // the FMM version each was captured at
   DBuf<double> gin_, gout_;                        // the captured matvec's input and output
   int64_t matvecs_ = 0;
 };

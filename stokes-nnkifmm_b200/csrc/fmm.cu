@@ -3,6 +3,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <type_traits>
 #include <cmath>
@@ -84,7 +85,13 @@ struct Solver {
 
 }  // namespace
 
+void Fmm::bump_version() {
+  static std::atomic<uint64_t> counter{0};
+  version_ = ++counter;
+}
+
 Fmm::Fmm(nnk_ctx* ctx, const HostTree* tree, const FmmParams& p) : ctx_(ctx), t_(tree), p_(p) {
+  bump_version();
   if (!(p.eps > 0) || !(p.mu > 0)) throw Error(NNK_E_ARG, "kernelPar needs eps > 0 and mu > 0");
   if (p.res < 2 || p.shells < 1 || 2 * p.shells > p.res)
     throw Error(NNK_E_ARG, "bad coronaRes/coronaShells");
@@ -926,7 +933,7 @@ void Fmm::set_eps(double eps) {
   if (!(eps > 0)) throw Error(NNK_E_ARG, "eps must be > 0");
   NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
   p_.eps = eps;
-  ++version_;
+  bump_version();
   tensor_m2l_ = false;
   fft_m2l_ = false;
   build_operators();
@@ -979,7 +986,7 @@ double tune_groups(Fmm* self, std::vector<TaskGroup*>& groups, const std::vector
 }  // namespace
 
 std::pair<double, double> Fmm::autotune(int nrhs) {
-  ++version_;
+  bump_version();
   const HostTree& t = *t_;
   const int R = rhs_chunk(nrhs, tensor_m2l_ ? 1 : R_);
   cudaStream_t st = ctx_->stream;

@@ -136,7 +136,8 @@ class Fmm {
   // right-hand sides.  Returns the total pair-kernel time before and after.
   std::pair<double, double> autotune(int nrhs);
   // Changes whenever launches captured earlier would be stale (new operators
-  // or tiles): set_eps and autotune.
+  // or tiles: set_eps, autotune).  Drawn from one process-wide counter, so an
+  // Fmm created later at a recycled address never repeats a value either.
   uint64_t version() const { return version_; }
   // Trees of the forest the matvec evaluates (flags per tree, nullptr: all).
   // The kernels of a masked tree return at once and its output rows are
@@ -278,6 +279,7 @@ class Fmm {
   cudaEvent_t event();
   std::unique_ptr<Fmm> sparse_;
   uint64_t version_ = 0;
+  void bump_version();
   // tree mask of the matvec (forests only): per tree, per node (expanded on
   // the device), and the leaf of each sorted target
   DBuf<int32_t> tree_on_, node_on_, node_tree_, tgt_leaf_;
