@@ -10,7 +10,7 @@ from ._lib import (NNKError, MaxDepthError, NoConvergence, context, lib, LIB_PAT
                    LAYOUT_ROWS, LAYOUT_BLOCKED, PREC_FP64, PREC_MIXED)
 from .octree import OcTree, nearestMatrix  # noqa: F401
 from .kifmm import KIFMM  # noqa: F401
-from .mobility import (Swimmers, Mobility, mobilityProblem, mobilityProblemGravity,  # noqa: F401
+from .mobility import (Swimmers, Mobility, hegedus, mobilityProblem, mobilityProblemGravity,  # noqa: F401
                        mobilityRHS, richardson)
 from .batch import BatchMobility  # noqa: F401
 from .resistance import Gen_Resistance, Rigid_Resistance, velocityModes  # noqa: F401

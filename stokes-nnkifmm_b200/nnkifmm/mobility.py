@@ -257,7 +257,23 @@ class Mobility:
         L.check(L.lib.nnk_mob_precon(self.h, L.ptr(x), L.ptr(y), 0), self.ctx.h, "mobilityPrecon")
         return y
 
-    def solve(self, rhs, tol=1e-6, maxIter=None, precondition=False, restart=0):
+    def solve(self, rhs, tol=1e-6, maxIter=None, precondition=False, restart=0, x0=None):
+        """gmres(afunc, rhs, restart, tol, maxIter[, ..., x0]) on the device.
+        With an initial guess x0 (MATLAB's 8th gmres argument, used by the
+        reference's Hegedus-trick experiments, Tests/HegadusTrickTest.m and
+        Data Generation/preconditioningInitalGuess.m) the correction
+        d = A^-1 (rhs - A x0) is solved from zero to the tolerance that makes
+        ||rhs - A (x0 + d)|| / ||rhs|| <= tol, and x0 + d is returned."""
+        if x0 is not None:
+            rhs = self._vec(rhs)
+            x0 = self._vec(x0)
+            r0 = rhs - self.apply(x0)
+            nb, nr = float(np.linalg.norm(rhs)), float(np.linalg.norm(r0))
+            if nb == 0.0 or nr <= tol * nb:
+                return x0.copy(), 0, (nr / nb if nb else 0.0), 0
+            d, flag, relres, it = self.solve(r0, tol=tol * nb / nr, maxIter=maxIter, precondition=precondition,
+                                             restart=restart)
+            return x0 + d, flag, relres * nr / nb, it
         rhs = self._vec(rhs)
         x = np.empty(self.n)
         sp_ = L.SolveParams(float(tol), int(maxIter if maxIter else min(self.n, 10)), int(restart))
@@ -267,6 +283,18 @@ class Mobility:
         if rc not in (L.NNK_OK, L.NNK_E_NOCONV):
             L.check(rc, self.ctx.h, "gmres")
         return x, info.flag, info.relres, info.iters
+
+
+def hegedus(apply, b, xp):
+    """The Hegedus trick (Tests/HegadusTrickTest.m, preconditioningInitalGuess.m:
+    scale = (b' A xp) / ||A xp||^2): the multiple of a previous solution xp (of
+    a nearby system, e.g. another eps) that minimises ||b - A x0||, as the
+    initial guess x0 = scale * xp."""
+    b = np.asarray(b, dtype=np.float64).ravel()
+    xp = np.asarray(xp, dtype=np.float64).ravel()
+    Axp = np.asarray(apply(xp), dtype=np.float64).ravel()
+    den = float(Axp @ Axp)
+    return (float(b @ Axp) / den if den > 0 else 0.0) * xp
 
 
 def mobilityRHS(sw, fluidFunc=None, t=0.0):

@@ -146,3 +146,31 @@ def test_gravity_forcing_vs_dense():
     assert np.linalg.norm(out - ref) <= 1e-5 * np.linalg.norm(ref)
     # it sinks at about G / (6 pi) and turns its heavy side down
     assert abs(out[2] * 6 * np.pi / G[2] - 1) < 1e-2 and abs(Om[1]) > 0
+
+
+def test_initial_guess_and_hegedus_warm_start():
+    """The solution at eps = 0.02, scaled by the Hegedus trick, as the initial
+    guess of the eps = 0.01 solve (Data Generation/preconditioningInitalGuess.m):
+    the same solution as a cold start, in no more iterations."""
+    c, f, NN, F, M = sphere_body([1, 0, 0], [0, 0, 1])
+
+    def mob_at(eps):
+        sw = nk.Swimmers()
+        sw.addSwimmer(c, f, NN, [0, 0, 0], [1, 0, 0, 0, 1, 0], np.zeros_like(c), F, M)
+        sw.genTree(nodeCapacity=60, nearest=1)
+        sw.genKIFMM([eps, 1.0], GMRES=1, format=2)
+        return sw.mobility(), nk.mobilityRHS(sw)
+
+    m2, b2 = mob_at(0.02)
+    xp, flag, _, _ = m2.solve(b2, tol=1e-8, maxIter=300)
+    assert flag == 0
+    m1, b1 = mob_at(0.01)
+    cold, flag_c, res_c, it_c = m1.solve(b1, tol=1e-8, maxIter=300)
+    x0 = nk.hegedus(m1.apply, b1, xp)
+    warm, flag_w, res_w, it_w = m1.solve(b1, tol=1e-8, maxIter=300, x0=x0)
+    assert flag_c == 0 and flag_w == 0 and res_w <= 1e-8
+    assert np.linalg.norm(m1.apply(warm) - b1) <= 2e-8 * np.linalg.norm(b1)
+    # the rigid velocities agree to the solves' accuracy (the force densities of the
+    # first-kind system less so)
+    assert np.linalg.norm(warm[-6:] - cold[-6:]) <= 1e-6 * np.linalg.norm(cold[-6:])
+    assert it_w <= it_c

@@ -187,3 +187,16 @@ def test_resistance_formulas_invert_the_dense_mobility_matrix():
         Mob[:, j] = np.linalg.solve(om.dense_mobility_matrix(asm, eps, mu, True), om.mobility_rhs(asm))[-6:]
     assert np.linalg.norm(R @ Mob - np.eye(6)) <= 1e-8
     assert np.linalg.norm(R - R.T) <= 1e-6 * np.linalg.norm(R)  # the grand resistance matrix is symmetric
+
+
+def test_hegedus_scale_minimises_the_residual():
+    """x0 = scale * xp with scale = (b' A xp) / ||A xp||^2 minimises
+    ||b - A x0|| over multiples of xp (Tests/HegadusTrickTest.m)."""
+    from nnkifmm.mobility import hegedus
+    rng = np.random.default_rng(6)
+    A = rng.standard_normal((30, 30)) + 30 * np.eye(30)
+    b, xp = rng.standard_normal(30), rng.standard_normal(30)
+    x0 = hegedus(lambda v: A @ v, b, xp)
+    r = lambda s: np.linalg.norm(b - A @ (s * xp))
+    s0 = float(x0 @ xp / (xp @ xp))
+    assert r(s0) <= min(r(s0 * 1.001), r(s0 * 0.999))
