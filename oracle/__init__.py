@@ -4,8 +4,8 @@ matvec and the GMRES mobility solve.
 TEST INFRASTRUCTURE ONLY.  Nothing in the product (the CUDA library and its
 Python binding under ``stokes-nnkifmm_b200/``) imports, links or executes this
 package.  Only ``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline``
-/ ``--impl reference`` legs of ``bench.py`` use it, and only as the checker or
-as the timed CPU baseline.
+/ ``--impl reference`` legs of ``bench.py`` use it, and only as the reference
+answer the GPU results are compared with, or as the timed CPU baseline.
 
 Parity status.  The reference is 100 % MATLAB and cannot run on this machine
 (no MATLAB, no Octave), and it ships no golden vectors.  The only known answer

@@ -660,7 +660,7 @@ void BatchMobility::solve(const double* rhs, double* x, const nnk_solve_params& 
     solve_plain(r.p, d.p, sp, itol, act, inf);
     for (int s = 0; s < S_; ++s) out[s].iters += inf[s].iters;
     dev_axpby(ctx_, 1.0, x, 1.0, d.p, x, n_);
-    // the FP64 residual of bodies with no system solved this round is the
+    // the FP64 residual of bodies with no system solved in this refinement pass is the
     // previous one (their x did not change): those trees are skipped and
     // their relres kept
     const std::vector<char> bon = deflate_ ? body_flags(act) : std::vector<char>(B_, 1);
