@@ -8,7 +8,6 @@
 #include <array>
 #include <cmath>
 #include <cstring>
-#include <unordered_map>
 
 #include "../../include/nnkifmm.h"
 #include "common.h"
@@ -21,14 +20,6 @@ struct Key3 {
   uint64_t a, b, c;
   bool operator==(const Key3& o) const { return a == o.a && b == o.b && c == o.c; }
 };
-struct Key3Hash {
-  size_t operator()(const Key3& k) const {
-    uint64_t h = k.a * 0x9E3779B97F4A7C15ull;
-    h ^= (k.b + 0x632BE59BD9B4E019ull + (h << 6) + (h >> 2));
-    h ^= (k.c + 0x85EBCA77C2B2AE63ull + (h << 6) + (h >> 2));
-    return (size_t)h;
-  }
-};
 inline uint64_t bits(double v) {
   v = v + 0.0;  // -0.0 -> +0.0: MATLAB compares rows by value
   uint64_t u;
@@ -36,6 +27,49 @@ inline uint64_t bits(double v) {
   return u;
 }
 inline Key3 key(const double* p) { return Key3{bits(p[0]), bits(p[1]), bits(p[2])}; }
+
+// The SplitMix64 finaliser (Steele, Lea and Flood, "Fast splittable
+// pseudorandom number generators", OOPSLA 2014) as a bit mixer.
+inline uint64_t mix64(uint64_t x) {
+  x ^= x >> 30;
+  x *= 0xBF58476D1CE4E5B9ull;
+  x ^= x >> 27;
+  x *= 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Point ids keyed by their rows in `pts` (bit patterns, -0.0 == +0.0), open
+// addressing with linear probing.  insert() may run on many threads at once
+// while `pts` does not change.
+class PointTable {
+ public:
+  PointTable(int64_t expected, const std::vector<double>& pts) : pts_(pts) {
+    size_t cap = 16;
+    while (cap < (size_t)expected * 2) cap <<= 1;
+    slots_.assign(cap, -1);
+    mask_ = cap - 1;
+  }
+  // Inserts point id (its row is already in pts) unless an equal row is
+  // present; returns the id that holds the row.
+  int64_t insert(int64_t id) {
+    const Key3 k = key(&pts_[3 * id]);
+    size_t h = (size_t)mix64(k.a ^ mix64(k.b ^ mix64(k.c))) & mask_;
+    for (;;) {
+      int64_t cur = __atomic_load_n(&slots_[h], __ATOMIC_ACQUIRE);
+      if (cur < 0 && __atomic_compare_exchange_n(&slots_[h], &cur, id, false, __ATOMIC_ACQ_REL,
+                                                 __ATOMIC_ACQUIRE))
+        return id;
+      // cur: the id in the slot (a failed exchange loads it)
+      if (key(&pts_[3 * cur]) == k) return cur;
+      h = (h + 1) & mask_;
+    }
+  }
+
+ private:
+  const std::vector<double>& pts_;
+  std::vector<int64_t> slots_;
+  size_t mask_ = 0;
+};
 
 struct Builder {
   HostTree& t;
@@ -120,7 +154,12 @@ static void build_lists(HostTree& t) {
   t.colleagues.assign(N, {});
   t.colleagues[0].push_back(0);
   for (int L = 1; L <= t.max_level; ++L) {
-    for (int32_t c : t.by_level[L]) {
+    const std::vector<int32_t>& lv = t.by_level[L];
+    const int64_t nl = (int64_t)lv.size();
+    // nodes of one level are independent (they read their parents' lists)
+#pragma omp parallel for schedule(static) if (nl > 2048)
+    for (int64_t j = 0; j < nl; ++j) {
+      const int32_t c = lv[j];
       const int32_t P = t.parent[c];
       auto& out = t.colleagues[c];
       for (int32_t C : t.colleagues[P]) {
@@ -148,7 +187,11 @@ static void build_lists(HostTree& t) {
   }
 
   std::vector<std::vector<int32_t>> U(N), V(N), W(N);
+  // every node's lists are independent of the others'
+#pragma omp parallel if (N > 2048)
+  {
   std::vector<int32_t> stack;
+#pragma omp for schedule(dynamic, 64)
   for (int32_t i = 1; i < N; ++i) {
     // V (OcTree.m:330-339): children of the parent's non-leaf same-level
     // touching nodes (other than the parent) that do not touch i.
@@ -228,6 +271,7 @@ static void build_lists(HostTree& t) {
       }
     }
   }
+  }
   auto to_csr = [&](std::vector<std::vector<int32_t>>& L, Csr& out) {
     out.off.assign(N + 1, 0);
     for (int32_t i = 0; i < N; ++i) out.off[i + 1] = out.off[i] + (int64_t)L[i].size();
@@ -285,27 +329,34 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
   }
   // points = unique([pot;tgt],'rows','stable'); masks by ismember (OcTree.m:80-82)
   {
-    std::unordered_map<Key3, int64_t, Key3Hash> seen;
-    seen.reserve((size_t)(n_pot + (same ? 0 : n_tgt)) * 2 + 16);
-    auto add = [&](const double* q3) {
-      auto it = seen.emplace(key(q3), t.n);
-      if (it.second) {
-        t.pts.insert(t.pts.end(), q3, q3 + 3);
-        t.n++;
-      }
-      return it.first->second;
-    };
-    t.is_pot.clear();
-    std::vector<int64_t> pot_pt(n_pot);
-    for (int64_t i = 0; i < n_pot; ++i) pot_pt[i] = add(pot + 3 * i);
-    if (t.n != n_pot) {
+    // potPoints rows must be distinct, so they are points 0..n_pot-1
+    t.pts.reserve(3 * (size_t)(n_pot + (same ? 0 : n_tgt)));
+    t.pts.assign(pot, pot + 3 * n_pot);
+    PointTable seen(n_pot + (same ? 0 : n_tgt), t.pts);
+    int dup = 0;
+#pragma omp parallel for schedule(static) reduction(| : dup) if (n_pot > 65536)
+    for (int64_t i = 0; i < n_pot; ++i) dup |= (seen.insert(i) != i);
+    if (dup) {
       msg = "potPoints contains duplicate rows";
       return NNK_E_ARG;
     }
+    t.n = n_pot;
+    std::vector<int64_t> pot_pt(n_pot);
+    for (int64_t i = 0; i < n_pot; ++i) pot_pt[i] = i;
     std::vector<int64_t> tgt_pt;
     if (!same) {
+      // targets in order: a new row becomes the next point
       tgt_pt.resize(n_tgt);
-      for (int64_t i = 0; i < n_tgt; ++i) tgt_pt[i] = add(tgt + 3 * i);
+      for (int64_t i = 0; i < n_tgt; ++i) {
+        t.pts.insert(t.pts.end(), tgt + 3 * i, tgt + 3 * i + 3);
+        const int64_t id = seen.insert(t.n);
+        if (id == t.n) {
+          t.n++;
+        } else {
+          t.pts.resize(3 * t.n);
+        }
+        tgt_pt[i] = id;
+      }
     }
     t.is_pot.assign(t.n, 0);
     t.is_tgt.assign(t.n, 0);
@@ -402,23 +453,40 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
     if (nn_rowptr) {
       t.nn_rowptr.assign(nn_rowptr, nn_rowptr + q + 1);
       const int64_t nnz = t.nn_rowptr[q];
+      // rowptr first: 0, non-decreasing, so every row lies inside [0, nnz)
       if (t.nn_rowptr[0] != 0 || nnz < 0) { msg = "bad NN rowptr"; return NNK_E_ARG; }
+      for (int64_t r = 0; r < q; ++r)
+        if (t.nn_rowptr[r + 1] < t.nn_rowptr[r]) { msg = "bad NN rowptr"; return NNK_E_ARG; }
       t.nn_col.assign(nn_col, nn_col + nnz);
       t.nn_val.assign(nn_val, nn_val + nnz);
+      int bad = 0;
+      int32_t* col = t.nn_col.data();
+      double* val = t.nn_val.data();
+      const int64_t* rp = t.nn_rowptr.data();
+#pragma omp parallel for schedule(static) reduction(| : bad) if (q > 65536)
       for (int64_t r = 0; r < q; ++r) {
-        if (t.nn_rowptr[r + 1] < t.nn_rowptr[r]) { msg = "bad NN rowptr"; return NNK_E_ARG; }
-        // sort columns within the row (MATLAB sparse storage order)
-        std::vector<std::pair<int32_t, double>> row;
-        for (int64_t k = t.nn_rowptr[r]; k < t.nn_rowptr[r + 1]; ++k) {
-          if (t.nn_col[k] < 0 || t.nn_col[k] >= n_pot) { msg = "NN column out of range"; return NNK_E_ARG; }
-          row.push_back({t.nn_col[k], t.nn_val[k]});
-        }
-        std::sort(row.begin(), row.end());
-        for (size_t k = 0; k < row.size(); ++k) {
-          t.nn_col[t.nn_rowptr[r] + k] = row[k].first;
-          t.nn_val[t.nn_rowptr[r] + k] = row[k].second;
+        const int64_t a = rp[r], b = rp[r + 1];
+        int row_bad = 0;
+        for (int64_t k = a; k < b; ++k) row_bad |= (col[k] < 0 || col[k] >= n_pot);
+        bad |= row_bad;
+        if (row_bad) continue;
+        // columns ascending within the row (MATLAB sparse storage order), by
+        // (column, weight) like a sort of the pairs; rows hold a handful of
+        // tied neighbours, so insertion sort
+        for (int64_t k = a + 1; k < b; ++k) {
+          const int32_t c = col[k];
+          const double v = val[k];
+          int64_t j = k;
+          while (j > a && (col[j - 1] > c || (col[j - 1] == c && val[j - 1] > v))) {
+            col[j] = col[j - 1];
+            val[j] = val[j - 1];
+            --j;
+          }
+          col[j] = c;
+          val[j] = v;
         }
       }
+      if (bad) { msg = "NN column out of range"; return NNK_E_ARG; }
     } else if (gpu) {
       nearest_matrix_gpu(gpu, pot, n_pot, fine, q, t.nn_rowptr, t.nn_col, t.nn_val);
     } else {
@@ -453,7 +521,7 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
     // NEAREST: fine points with a nonzero NN entry in the leaf's columns,
     // ascending fine index, each carrying kron(NN_sub,I3)*f
     // (upwardPass.m:303-314, downwardPass.m:89-101).
-    struct T { int32_t leaf; int64_t q; int32_t col; double w; };
+    struct T { int64_t q; int32_t col; double w; };
     std::vector<int64_t> cnt(N + 1, 0);
     const int64_t nnz = t.nn_rowptr[q];
     for (int64_t k = 0; k < nnz; ++k) {
@@ -461,30 +529,52 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
       cnt[t.point_index[t.nn_col[k]] + 1]++;
     }
     for (int32_t i = 0; i < N; ++i) cnt[i + 1] += cnt[i];
-    std::vector<T> trip(cnt[N]);
-    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
-    for (int64_t r = 0; r < q; ++r)
-      for (int64_t k = t.nn_rowptr[r]; k < t.nn_rowptr[r + 1]; ++k) {
-        if (t.nn_val[k] == 0.0) continue;
-        const int32_t leaf = t.point_index[t.nn_col[k]];
-        trip[pos[leaf]++] = T{leaf, r, t.nn_col[k], t.nn_val[k]};
-      }
-    int64_t e = 0;
+    const int64_t G = cnt[N];
+    // NN entries bucketed by leaf, ascending fine index inside a bucket
+    std::vector<T> trip(G);
+    {
+      std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
+      for (int64_t r = 0; r < q; ++r)
+        for (int64_t k = t.nn_rowptr[r]; k < t.nn_rowptr[r + 1]; ++k) {
+          if (t.nn_val[k] == 0.0) continue;
+          const int32_t leaf = t.point_index[t.nn_col[k]];
+          trip[pos[leaf]++] = T{r, t.nn_col[k], t.nn_val[k]};
+        }
+    }
+    // one entry per distinct fine point of a bucket; entries numbered leaf by
+    // leaf, so each leaf fills its own slice of the arrays
+    std::vector<int64_t> ecnt(N + 1, 0);
+#pragma omp parallel for schedule(dynamic, 256) if (G > 65536)
     for (int32_t i = 0; i < N; ++i) {
-      t.src_start[i] = e;
+      int64_t c = 0;
+      for (int64_t k = cnt[i]; k < cnt[i + 1]; ++k) c += (k == cnt[i] || trip[k].q != trip[k - 1].q);
+      ecnt[i + 1] = c;
+    }
+    for (int32_t i = 0; i < N; ++i) ecnt[i + 1] += ecnt[i];
+    const int64_t E = ecnt[N];
+    t.src_pos.resize(3 * E);
+    t.src_origin.resize(E);
+    t.src_goff.resize(E + 1);
+    t.src_gidx.resize(G);
+    t.src_gw.resize(G);
+#pragma omp parallel for schedule(dynamic, 256) if (G > 65536)
+    for (int32_t i = 0; i < N; ++i) {
+      t.src_start[i] = ecnt[i];
+      int64_t e = ecnt[i];
       for (int64_t k = cnt[i]; k < cnt[i + 1]; ++k) {
-        if (k == cnt[i] || trip[k].q != trip[k - 1].q) {
-          if (k != cnt[i]) t.src_goff.push_back((int64_t)t.src_gidx.size());
-          t.src_pos.insert(t.src_pos.end(), &t.fine[3 * trip[k].q], &t.fine[3 * trip[k].q] + 3);
-          t.src_origin.push_back(trip[k].q);
+        const T& x = trip[k];
+        if (k == cnt[i] || x.q != trip[k - 1].q) {
+          t.src_goff[e] = k;
+          std::memcpy(&t.src_pos[3 * e], &t.fine[3 * x.q], 3 * sizeof(double));
+          t.src_origin[e] = x.q;
           ++e;
         }
-        t.src_gidx.push_back((int32_t)t.pot_rank[trip[k].col]);
-        t.src_gw.push_back(trip[k].w);
+        t.src_gidx[k] = (int32_t)t.pot_rank[x.col];
+        t.src_gw[k] = x.w;
       }
-      if (cnt[i + 1] > cnt[i]) t.src_goff.push_back((int64_t)t.src_gidx.size());
     }
-    t.src_start[N] = e;
+    t.src_goff[E] = G;
+    t.src_start[N] = E;
   }
   return NNK_OK;
 }

@@ -8,7 +8,7 @@ import pytest
 import scipy.sparse as sp
 
 import nnkifmm as nk
-from conftest import GOLDEN
+from conftest import GOLDEN, ROOT
 from oracle.geometry import sphere
 from oracle.nearest import nearest_matrix
 from oracle.octree import OcTree as OracleTree
@@ -125,3 +125,55 @@ def test_bad_inputs_rejected():
         nk.OcTree(y, y)
     with pytest.raises(nk.NNKError):  # NEAREST needs targets == potentials
         nk.OcTree(x, x[:5], nearest=1, finePoints=x)
+
+
+_TREE_ARRAYS = """
+import sys, numpy as np, scipy.sparse as sp
+import nnkifmm as nk
+x = np.load(sys.argv[1]); f = np.load(sys.argv[2])
+NN = nk.nearestMatrix(x, f, builder="host")
+t = nk.OcTree(x, x, nodeCapacity=8, nearest=1, finePoints=f, NN=NN, builder="host")
+out = dict(level=t.nodeLevel, parent=t.nodeParents, children=t.nodeChildren, corners=t.nodeCorners,
+           point_index=t.pointIndex, nn_indptr=NN.indptr, nn_indices=NN.indices, nn_data=NN.data)
+for k in range(4):
+    out[f"off{k}"], out[f"ids{k}"] = t.interaction_list(k)
+np.savez(sys.argv[3], **out)
+"""
+
+
+def test_large_tree_independent_of_thread_count(tmp_path):
+    """Above a few thousand nodes (or 65,536 points) the host builder checks
+    the points for duplicates, builds the U/V/W lists and sorts the NN rows on
+    OpenMP threads; a process held to one thread gives the same arrays."""
+    import subprocess
+    import sys
+    rng = np.random.default_rng(21)
+    x = mixed(rng, 120_000)
+    f = np.concatenate([mixed(rng, 150_000), x[:2000] + 1e-4])
+    np.save(tmp_path / "x.npy", x)
+    np.save(tmp_path / "f.npy", f)
+    script = tmp_path / "arrays.py"
+    script.write_text(_TREE_ARRAYS)
+    runs = {}
+    for threads in ("1", "4"):
+        path = os.pathsep.join([ROOT, os.path.join(ROOT, "stokes-nnkifmm_b200"), os.environ.get("PYTHONPATH", "")])
+        env = dict(os.environ, OMP_NUM_THREADS=threads, PYTHONPATH=path)
+        out = tmp_path / f"t{threads}.npz"
+        subprocess.run([sys.executable, str(script), str(tmp_path / "x.npy"), str(tmp_path / "f.npy"), str(out)],
+                       check=True, env=env, timeout=600)
+        runs[threads] = np.load(out)
+    a, b = runs["1"], runs["4"]
+    assert a["level"].size > 2048
+    for k in a.files:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_large_duplicate_rows_rejected():
+    """The duplicate check of potPoints on many threads: a repeated row, and a
+    row equal to another up to the sign of zero (rows compare by value)."""
+    x = np.random.default_rng(22).random((100_000, 3))
+    x[500] = [0.0, 0.25, 0.75]
+    for extra in (x[77:78], np.array([[-0.0, 0.25, 0.75]])):
+        y = np.concatenate([x[:60_000], extra, x[60_000:]])
+        with pytest.raises(nk.NNKError, match="duplicate"):
+            nk.OcTree(y, y, nodeCapacity=64, builder="host")
