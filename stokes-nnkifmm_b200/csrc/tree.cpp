@@ -457,6 +457,7 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
       if (t.nn_rowptr[0] != 0 || nnz < 0) { msg = "bad NN rowptr"; return NNK_E_ARG; }
       for (int64_t r = 0; r < q; ++r)
         if (t.nn_rowptr[r + 1] < t.nn_rowptr[r]) { msg = "bad NN rowptr"; return NNK_E_ARG; }
+      if (nnz > 0 && (!nn_col || !nn_val)) { msg = "NN columns or values missing"; return NNK_E_ARG; }
       t.nn_col.assign(nn_col, nn_col + nnz);
       t.nn_val.assign(nn_val, nn_val + nnz);
       int bad = 0;
