@@ -140,6 +140,12 @@ Mobility::Mobility(Fmm* fmm, int nbodies, const int64_t* body_start, const int64
   for (int b = 0; b < nb_; ++b)
     if (bstart_[b + 1] < bstart_[b]) throw Error(NNK_E_ARG, "bad body_start");
   const int64_t Nsw = bstart_[nb_];
+  if (Nsw > 0 && !rel_points) throw Error(NNK_E_ARG, "rel_points missing");
+  if (t.params.nearest && fine_start) {
+    if (fine_start[0] != 0 || fine_start[nb_] > t.q) throw Error(NNK_E_ARG, "bad fine_start");
+    for (int b = 0; b < nb_; ++b)
+      if (fine_start[b + 1] < fine_start[b]) throw Error(NNK_E_ARG, "bad fine_start");
+  }
   std::vector<int32_t> body(N_, -1);
   for (int b = 0; b < nb_; ++b)
     for (int64_t n = bstart_[b]; n < bstart_[b + 1]; ++n) body[n] = b;
