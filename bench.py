@@ -443,6 +443,69 @@ def reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def roofline(per_step, stats, precision, peaks):
+    """Roofline of the dominant phase of one matvec, from the live per-phase
+    CUDA-event times (per_step: phase -> (ms, launches) per step) and the
+    algorithmic work of the tree statistics; `pair_kernels` adds the same for
+    all pair phases together (S2M/M2M/L2L/L2T, P2L/M2T and the near field)."""
+    dom = max((k for k in per_step if per_step[k][1] > 0), key=lambda k: per_step[k][0])
+    # pairs_down counts the V list as P x P pairs per M2L; when the M2L runs as
+    # its own phase (tensor cores or Fourier space) the down pairs are the rest
+    m2l_apart = per_step.get("m2l", (0.0, 0))[1] > 0
+    down = stats["pairs_down"] - (stats["m2l_pairs"] * stats["surface_points"] ** 2 if m2l_apart else 0)
+    pairs = {"up_pairs": stats["pairs_up"], "down_pairs": down, "leaf_pairs": stats["pairs_leaf"]}
+    if dom == "m2l":
+        n3 = 3 * stats["surface_points"]
+        rk = stats["m2l_rank"] or n3
+        terms = 2 if stats["m2l_rank"] else 1  # the compressed form splits the densities into two TF32 terms
+        flops = terms * 2.0 * rk * rk * stats["m2l_pairs"]
+        tf32_peak = peaks.get("bf16_tflops", 1590.0) / 2
+        roof = {"kernel": ("m2l_ws_kernel (tcgen05 kind::tf32, TMEM accumulator, warp-specialised) on rank-"
+                           f"{rk} compressed operators" if stats["m2l_rank"] else
+                           "m2l_img_kernel (tcgen05 kind::tf32, TMEM accumulator)"),
+                "bound": "tensor",
+                "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": tf32_peak, "unit": "TFLOP/s",
+                "peak_source": "TF32 dense = 1/2 of the measured cuBLAS bf16 burst peak in MEASURED_PEAKS.json"
+                               if peaks else "TF32 dense = 1/2 of the fallback bf16 peak",
+                "algorithmic": f"{stats['m2l_pairs']} V pairs x {terms} TF32 density terms x 2 x {rk}^2 flops per "
+                               f"step (useful rows only, no padding; the phase also holds the FP32 basis projection "
+                               f"and expansion, 2 x 2 x 456 x {rk} flops per node)",
+                "padded_rows_over_useful": stats["m2l_tile_rows"] / max(stats["m2l_pairs"], 1),
+                "launches_per_step": per_step[dom][1], "ms_per_launch": per_step[dom][0] / per_step[dom][1],
+                "traffic": None}
+    elif dom in pairs:
+        flops = pairs[dom] * FLOPS_PER_PAIR
+        fp64 = precision == "fp64"
+        peak = FP32_NOMINAL_TFLOPS / (2 if fp64 else 1)
+        roof = {"kernel": f"p2p_kernel ({dom})", "bound": "fp64" if fp64 else "fp32",
+                "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "peak_source": "nominal SIMT FP32 (148 SM x 128 lanes x 2 x 1.965 GHz); MEASURED_PEAKS.json "
+                               "holds only HBM and bf16 tensor figures",
+                "launches_per_step": per_step[dom][1], "ms_per_launch": per_step[dom][0] / per_step[dom][1],
+                "algorithmic": f"{pairs[dom]} pairs x {FLOPS_PER_PAIR} flops per step", "traffic": None}
+    else:
+        n = 3 * stats["surface_points"]
+        flops = 2.0 * n * n * stats["c2e_columns"]
+        roof = {"kernel": f"c2e_kernel ({dom})", "bound": "fp64", "achieved": flops / (per_step[dom][0] / 1e3) / 1e12,
+                "algorithmic": "2 x (3P)^2 flops per node per pass",
+                "peak": FP32_NOMINAL_TFLOPS / 2, "unit": "TFLOP/s", "traffic": None}
+    roof["frac"] = roof["achieved"] / roof["peak"]
+    roof["phases_ms_per_step"] = {k: round(v[0], 4) for k, v in per_step.items()}
+    if peaks:
+        roof["hbm_measured_gbs"] = peaks.get("hbm_gbs")
+    pair_ms = sum(per_step.get(k, (0.0, 0))[0] for k in ("up_pairs", "down_pairs", "leaf_pairs"))
+    if pair_ms > 0:
+        npairs = sum(pairs.values())
+        peak = FP32_NOMINAL_TFLOPS / (2 if precision == "fp64" else 1)
+        achieved = npairs * FLOPS_PER_PAIR / (pair_ms / 1e3) / 1e12
+        roof["pair_kernels"] = {"kernel": "p2p_kernel (up, down and leaf pair phases)",
+                                "bound": "fp64" if precision == "fp64" else "fp32", "achieved": achieved,
+                                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "ms_per_step": pair_ms,
+                                "algorithmic": f"{npairs} pairs x {FLOPS_PER_PAIR} flops per step",
+                                "peak_source": "nominal SIMT FP32 (148 SM x 128 lanes x 2 x 1.965 GHz)"}
+    return roof
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init(args)
@@ -501,47 +564,7 @@ def main():
     # roofline of the dominant phase (live CUDA events over the timed region)
     peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
     per_step = {k: (v[0] / args.steps, v[1] / args.steps) for k, v in prof.items()}
-    dom = max((k for k in per_step if per_step[k][1] > 0), key=lambda k: per_step[k][0])
-    pairs = {"up_pairs": stats["pairs_up"], "down_pairs": stats["pairs_down"], "leaf_pairs": stats["pairs_leaf"]}
-    if dom == "m2l":
-        n3 = 3 * stats["surface_points"]
-        rk = stats["m2l_rank"] or n3
-        terms = 2 if stats["m2l_rank"] else 1  # the compressed form splits the densities into two TF32 terms
-        flops = terms * 2.0 * rk * rk * stats["m2l_pairs"]
-        tf32_peak = peaks.get("bf16_tflops", 1590.0) / 2
-        roof = {"kernel": ("m2l_ws_kernel (tcgen05 kind::tf32, TMEM accumulator, warp-specialised) on rank-"
-                           f"{rk} compressed operators" if stats["m2l_rank"] else
-                           "m2l_img_kernel (tcgen05 kind::tf32, TMEM accumulator)"),
-                "bound": "tensor",
-                "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": tf32_peak, "unit": "TFLOP/s",
-                "peak_source": "TF32 dense = 1/2 of the measured cuBLAS bf16 burst peak in MEASURED_PEAKS.json"
-                               if peaks else "TF32 dense = 1/2 of the fallback bf16 peak",
-                "algorithmic": f"{stats['m2l_pairs']} V pairs x {terms} TF32 density terms x 2 x {rk}^2 flops per "
-                               f"step (useful rows only, no padding; the phase also holds the FP32 basis projection "
-                               f"and expansion, 2 x 2 x 456 x {rk} flops per node)",
-                "padded_rows_over_useful": stats["m2l_tile_rows"] / max(stats["m2l_pairs"], 1),
-                "launches_per_step": per_step[dom][1], "ms_per_launch": per_step[dom][0] / per_step[dom][1],
-                "traffic": None}
-    elif dom in pairs:
-        flops = pairs[dom] * FLOPS_PER_PAIR
-        fp64 = args.precision == "fp64"
-        peak = FP32_NOMINAL_TFLOPS / (2 if fp64 else 1)
-        roof = {"kernel": f"p2p_kernel ({dom})", "bound": "fp64" if fp64 else "fp32",
-                "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
-                "peak_source": "nominal SIMT FP32 (148 SM x 128 lanes x 2 x 1.965 GHz); MEASURED_PEAKS.json "
-                               "holds only HBM and bf16 tensor figures",
-                "launches_per_step": per_step[dom][1], "ms_per_launch": per_step[dom][0] / per_step[dom][1],
-                "algorithmic": f"{pairs[dom]} pairs x {FLOPS_PER_PAIR} flops per step", "traffic": None}
-    else:
-        n = 3 * stats["surface_points"]
-        flops = 2.0 * n * n * stats["c2e_columns"]
-        roof = {"kernel": f"c2e_kernel ({dom})", "bound": "fp64", "achieved": flops / (per_step[dom][0] / 1e3) / 1e12,
-                "algorithmic": "2 x (3P)^2 flops per node per pass",
-                "peak": FP32_NOMINAL_TFLOPS / 2, "unit": "TFLOP/s", "traffic": None}
-    roof["frac"] = roof["achieved"] / roof["peak"]
-    roof["phases_ms_per_step"] = {k: round(v[0], 4) for k, v in per_step.items()}
-    if peaks:
-        roof["hbm_measured_gbs"] = peaks.get("hbm_gbs")
+    roof = roofline(per_step, stats, args.precision, peaks)
 
     line = {"metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",

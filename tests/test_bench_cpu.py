@@ -1,0 +1,56 @@
+"""The bench's roofline arithmetic on CPU: per-phase CUDA-event times and the
+tree statistics of the 250k / 1M-point matvec give each phase's achieved rate
+against its peak, for every branch the dominant phase can take."""
+import pytest
+
+import bench
+
+STATS = {"pairs_up": 476_380_160, "pairs_down": 35_120_308_320, "pairs_leaf": 1_093_206_582,
+         "pairs_p2p": 592_857_390, "surface_points": 152, "m2l_rank": 256, "m2l_pairs": 1_426_620,
+         "m2l_tile_rows": 1_500_000, "c2e_columns": 28_000}
+PHASES = {"gather": (0.015, 1), "up_pairs": (0.61, 5), "up_c2e": (0.62, 7), "down_pairs": (2.08, 7),
+          "down_c2e": (0.66, 8), "leaf_pairs": (1.19, 3), "scatter": (0.008, 1), "m2l": (2.52, 3)}
+PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def test_m2l_dominant_phase():
+    r = bench.roofline(PHASES, STATS, "mixed", PEAKS)
+    assert r["bound"] == "tensor" and "m2l_ws_kernel" in r["kernel"]
+    flops = 2 * 2.0 * 256 * 256 * STATS["m2l_pairs"]
+    assert r["achieved"] == pytest.approx(flops / 2.52e-3 / 1e12)
+    assert r["peak"] == pytest.approx(795.0) and r["frac"] == pytest.approx(r["achieved"] / 795.0)
+    assert r["launches_per_step"] == 3 and r["hbm_measured_gbs"] == 6650.0
+    p = r["pair_kernels"]
+    # the V pairs run in the M2L phase, not in the down pairs
+    npairs = STATS["pairs_up"] + STATS["pairs_down"] - STATS["m2l_pairs"] * 152 ** 2 + STATS["pairs_leaf"]
+    assert p["ms_per_step"] == pytest.approx(0.61 + 2.08 + 1.19)
+    assert p["achieved"] == pytest.approx(npairs * bench.FLOPS_PER_PAIR / (3.88e-3) / 1e12)
+    assert p["peak"] == pytest.approx(bench.FP32_NOMINAL_TFLOPS) and 0 < p["frac"] < 1.5
+
+
+def test_pair_dominant_phase_fp64():
+    # M2L as pair segments of the down pass: no M2L phase, the V pairs count
+    phases = dict(PHASES, down_pairs=(40.0, 7), m2l=(0.0, 0))
+    r = bench.roofline(phases, STATS, "fp64", {})
+    assert r["kernel"] == "p2p_kernel (down_pairs)" and r["bound"] == "fp64"
+    assert r["achieved"] == pytest.approx(STATS["pairs_down"] * bench.FLOPS_PER_PAIR / 40e-3 / 1e12)
+    assert r["peak"] == pytest.approx(bench.FP32_NOMINAL_TFLOPS / 2)
+    assert r["pair_kernels"]["bound"] == "fp64" and "hbm_measured_gbs" not in r
+
+
+def test_c2e_dominant_phase_and_uncompressed_m2l():
+    r = bench.roofline(dict(PHASES, up_c2e=(9.0, 7)), STATS, "fp64", PEAKS)
+    assert r["kernel"] == "c2e_kernel (up_c2e)"
+    assert r["achieved"] == pytest.approx(2.0 * 456 * 456 * STATS["c2e_columns"] / 9e-3 / 1e12)
+    full = bench.roofline(PHASES, dict(STATS, m2l_rank=0), "mixed", PEAKS)
+    assert "m2l_img_kernel" in full["kernel"]
+    assert full["achieved"] == pytest.approx(2.0 * 456 * 456 * STATS["m2l_pairs"] / 2.52e-3 / 1e12)
+
+
+def test_pair_kernels_of_the_250k_matvec():
+    """The live phase split and statistics of the 250k / 1M-point mixed
+    matvec: the pair phases reach 41% of the nominal FP32 rate (32 flops per
+    pair), the M2L phase 19% of the TF32 rate."""
+    r = bench.roofline(PHASES, STATS, "mixed", PEAKS)
+    assert r["pair_kernels"]["frac"] == pytest.approx(0.41, abs=0.01)
+    assert r["frac"] == pytest.approx(0.186, abs=0.005)
