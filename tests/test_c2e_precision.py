@@ -1,0 +1,63 @@
+"""Why the check-to-equivalent product stays FP64 in mixed precision, checked
+on the CPU with the oracle's kernel and surfaces.  For a leaf-sized box
+(eps = 1e-3, p = 6, Tikhonov operator lam = 1e-5 sigma_max, cond(K) ~ 2e10),
+the far field of the upward equivalent density, at V-list distances, against
+the direct sum of the box's sources:
+  * FP64 operator and FP64 accumulation, on an FP32 check potential (the GPU's
+    mixed mode): the FP64 error, ~1e-5;
+  * FP32 accumulation, even of an exact (two-float) operator: ~1e-4 and above,
+    the mixed mode's whole error budget;
+  * one TF32 product: above 1e-2.
+So a tensor-core form of this product needs exact accumulation (an integer
+slice scheme), not TF32 terms accumulated in FP32."""
+import numpy as np
+import pytest
+
+from oracle.kernel import apply_kernel, kernel
+from oracle.surfaces import downsurf, upsurf
+
+
+def tf32(a):
+    """Round to TF32 (10 explicit mantissa bits), nearest, ties away."""
+    x = np.asarray(a, np.float32).copy()
+    u = x.view(np.uint32)
+    u += np.uint32(0x1000)
+    u &= np.uint32(0xFFFFE000)
+    return x
+
+
+def setup(w, seed):
+    rng = np.random.default_rng(seed)
+    eps = 1e-3
+    lo = np.array([0.3, 0.4, 0.5])
+    box = np.concatenate([lo, lo + w])
+    us, ds = upsurf(box), downsurf(box)
+    K = kernel(us, ds, eps, 1.0)
+    lam = 1e-5 * np.linalg.norm(K, 2)
+    A = np.linalg.solve(K.T @ K + lam ** 2 * np.eye(K.shape[1]), K.T)
+    src = lo + w * rng.random((300, 3))
+    f = rng.standard_normal((300, 3))
+    check = apply_kernel(src, ds, f, eps, 1.0).reshape(-1)
+    d = rng.standard_normal((400, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    tgt = lo + w / 2 + d * w * rng.uniform(2.5, 3.5, (400, 1))
+    direct = apply_kernel(src, tgt, f, eps, 1.0).reshape(-1)
+
+    def err(e):
+        u = apply_kernel(us, tgt, np.asarray(e, np.float64).reshape(-1, 3), eps, 1.0).reshape(-1)
+        return np.linalg.norm(u - direct) / np.linalg.norm(direct)
+    return A, check, err
+
+
+@pytest.mark.parametrize("w", [1 / 8, 1 / 32])
+def test_c2e_needs_fp64_accumulation(w):
+    A, check, err = setup(w, 1)
+    c32 = check.astype(np.float32)
+    e64 = err(A @ check)
+    assert e64 < 3e-5
+    assert err(A @ c32.astype(np.float64)) < 1.2 * e64           # FP32 check, FP64 operator and sums
+    Ah = A.astype(np.float32)
+    Al = (A - Ah).astype(np.float32)
+    assert err(Ah @ c32 + Al @ c32) > 3 * e64                      # exact operator, FP32 sums
+    assert err(Ah @ c32) > 5 * e64                                 # FP32 operator
+    assert err(tf32(A).astype(np.float64) @ tf32(c32).astype(np.float64)) > 1e-2  # one TF32 product
