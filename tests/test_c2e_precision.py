@@ -8,8 +8,11 @@ the direct sum of the box's sources:
   * FP32 accumulation, even of an exact (two-float) operator: ~1e-4 and above,
     the mixed mode's whole error budget;
   * one TF32 product: above 1e-2.
-So a tensor-core form of this product needs exact accumulation (an integer
-slice scheme), not TF32 terms accumulated in FP32."""
+So a tensor-core form of this product needs exact accumulation, not TF32
+terms accumulated in FP32: int8 slices of the operator (5, one exponent per
+row) and of the check potentials (4, one exponent per column), multiplied with
+exact integer sums and combined in FP64 (the Ozaki scheme), give the FP64
+product's error with 14 slice products."""
 import numpy as np
 import pytest
 
@@ -61,3 +64,39 @@ def test_c2e_needs_fp64_accumulation(w):
     assert err(Ah @ c32 + Al @ c32) > 3 * e64                      # exact operator, FP32 sums
     assert err(Ah @ c32) > 5 * e64                                 # FP32 operator
     assert err(tf32(A).astype(np.float64) @ tf32(c32).astype(np.float64)) > 1e-2  # one TF32 product
+
+
+def int8_slices(X, k, axis):
+    """k int8 slices of X, X ~ 2^e * sum_t D_t 128^-(t+1), one power-of-two
+    exponent e per row (axis=1) or per column (axis=0) (the Ozaki scheme)."""
+    m = np.abs(X).max(axis=axis, keepdims=True)
+    e = np.ceil(np.log2(np.where(m > 0, m, 1.0)))
+    r = X / 2.0 ** e
+    D = []
+    for _ in range(k):
+        r = r * 128.0
+        d = np.clip(np.rint(r), -127, 127)
+        r = r - d
+        D.append(d.astype(np.int64))
+    return D, e
+
+
+@pytest.mark.parametrize("w", [1 / 8, 1 / 32, 1 / 128])
+def test_int8_slice_product_keeps_the_fp64_accuracy(w):
+    """5 operator slices x 4 check slices, the 14 products with t + u <= 4,
+    each an exact integer sum (|sum| < 2^31: 456 x 127^2 x 4 products of one
+    scale), combined in FP64: the far-field error of the FP64 product."""
+    A, check, err = setup(w, 1)
+    c = check.astype(np.float32).astype(np.float64).reshape(-1, 1)
+    DA, ea = int8_slices(A, 5, 1)
+    DC, ec = int8_slices(c, 4, 0)
+    acc = {}
+    for t in range(5):
+        for u in range(4):
+            if t + u <= 4:
+                acc[t + u] = acc.get(t + u, 0) + DA[t] @ DC[u]
+    assert max(np.abs(v).max() for v in acc.values()) < 2 ** 31
+    e = sum(acc[s].astype(np.float64) * 2.0 ** (-7 * (s + 2)) for s in sorted(acc, reverse=True))
+    e = (e * 2.0 ** ea * 2.0 ** ec).ravel()
+    e64 = err(A @ c.ravel())
+    assert err(e) < 1.05 * e64
