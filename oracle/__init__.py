@@ -29,6 +29,8 @@ Modules
                Tools/Nearest/*Nearest.m, Mobility/ReducedSolve.m, Classes/KIFMM.m)
   gmres     -- unrestarted GMRES with relative-residual stop (MATLAB gmres semantics)
   mobility  -- Swimmers assembly, B/BT/A1/A2, mobility matvec, preconditioner,
-               mobilityProblem (Classes/Swimmers.m, Mobility/*.m)
-  direct    -- dense direct sums and dense solves used as accuracy oracles
+               mobilityProblem, the dense FP64 system (Classes/Swimmers.m, Mobility/*.m)
+  gradient  -- dense FP64 adjoint gradient of a rigid-velocity loss
+  parfor    -- the kifmm matvec with the reference's parfor loops over the nodes
+               of a level on worker processes (upwardPass.m:40, downwardPass.m:45,177)
 """

@@ -85,33 +85,103 @@ def _leaf_sources(tree, node, pot):
     return tree.points[tree.potentials][pmask], pot[pmask]
 
 
+def up_node(tree, node, pot, uppot, eps, mu, res, shells, pot_leaf):
+    """One iteration of upwardPass.m's parfor over the nodes of a level
+    (:40-98; Up.m:31-33): the check potential on the node's downsurf from its
+    leaf sources or its children's equivalent densities, then
+    kernel(upsurf, downsurf) \\ check."""
+    us = upsurf(tree.corners[node], res, shells)
+    ds = downsurf(tree.corners[node], res, shells)
+    if pot_leaf:
+        src, g = _leaf_sources(tree, node, pot)
+        check = apply_kernel(src, ds, g, eps, mu)
+    else:
+        ch = tree.children[node]
+        csurf = np.concatenate([upsurf(tree.corners[c], res, shells) for c in ch])
+        cpot = np.concatenate([uppot[c].reshape(-1, 3) for c in ch])
+        check = apply_kernel(csurf, ds, cpot, eps, mu)
+    K = kernel(us, ds, eps, mu)
+    return sla.solve(K, check.reshape(-1))
+
+
+def up_levels(tree, res, shells):
+    """Per level, from the deepest to the root, the nodes upwardPass.m visits:
+    the non-empty potential leaves and the non-leaves (:33-35), with their
+    leaf flags."""
+    ids = tree.ids()
+    pot_leaf = tree.is_leaf_potential(ids)
+    nonleaf = ~tree.is_leaf_all(ids)
+    out = []
+    for level in range(int(tree.level[1:].max()), -1, -1):
+        sel = (tree.level[1:] == level) & (pot_leaf | nonleaf)
+        out.append((ids[sel], pot_leaf[sel]))
+    return out
+
+
 def upward_pass(tree, pot, eps, mu, res=6, shells=1):
     """Tools/Passes/upwardPass.m:18-100.  Levels max..0; nodes of a level are
     the non-empty potential leaves and the non-leaves (:33-35); returns
     uppot[(nodeCount+1), 3P] with rows [x y z] interleaved per surface point."""
     P = surface_count(res, shells)
-    nc = tree.node_count
-    uppot = np.zeros((nc + 1, 3 * P))
-    ids = tree.ids()
-    pot_leaf = tree.is_leaf_potential(ids)
-    nonleaf = ~tree.is_leaf_all(ids)
-    for level in range(int(tree.level[1:].max()), -1, -1):
-        nodes = ids[(tree.level[1:] == level) & (pot_leaf | nonleaf)]
-        for node in nodes:
-            us = upsurf(tree.corners[node], res, shells)
-            ds = downsurf(tree.corners[node], res, shells)
-            if pot_leaf[node - 1]:
-                src, g = _leaf_sources(tree, node, pot)
-                check = apply_kernel(src, ds, g, eps, mu)
-            else:
-                ch = tree.children[node]
-                csurf = np.concatenate([upsurf(tree.corners[c], res, shells) for c in ch])
-                cpot = np.concatenate([uppot[c].reshape(-1, 3) for c in ch])
-                check = apply_kernel(csurf, ds, cpot, eps, mu)
-            # Up.m:31-33: kernel(upsurf, downsurf) \ check
-            K = kernel(us, ds, eps, mu)
-            uppot[node] = sla.solve(K, check.reshape(-1))
+    uppot = np.zeros((tree.node_count + 1, 3 * P))
+    for nodes, leaf in up_levels(tree, res, shells):
+        for node, pl in zip(nodes, leaf):
+            uppot[node] = up_node(tree, node, pot, uppot, eps, mu, res, shells, pl)
     return uppot
+
+
+def down_node(tree, node, pot, uppot, downpot, eps, mu, res, shells):
+    """One iteration of downwardPass.m's parfor over the nodes of a level
+    (:45-166; DownNonleaf.m:42-46): the check potential on the node's upsurf
+    from V (M2L), X (P2L) and the parent's downsurf (L2L), then
+    kernel(downsurf, upsurf) \\ check."""
+    P = surface_count(res, shells)
+    us = upsurf(tree.corners[node], res, shells)
+    ds = downsurf(tree.corners[node], res, shells)
+    rhs = np.zeros((P, 3))
+    v = tree.V[node]
+    if len(v):
+        vs = np.concatenate([upsurf(tree.corners[k], res, shells) for k in v])
+        vp = np.concatenate([uppot[k].reshape(-1, 3) for k in v])
+        rhs += apply_kernel(vs, us, vp, eps, mu)
+    for xn in tree.X[node]:
+        src, g = _leaf_sources(tree, xn, pot)
+        if len(src):
+            rhs += apply_kernel(src, us, g, eps, mu)
+    par = tree.parent[node]
+    ps = downsurf(tree.corners[par], res, shells)
+    rhs += apply_kernel(ps, us, downpot[par].reshape(-1, 3), eps, mu)
+    K = kernel(ds, us, eps, mu)
+    return sla.solve(K, rhs.reshape(-1))
+
+
+def leaf_velocity(tree, node, pot, uppot, downpot, eps, mu, res, shells):
+    """One iteration of downwardPass.m's parfor over the target leaves
+    (:177-294): L2T + U (P2P) + W (M2T); returns the leaf's target mask and
+    velocities."""
+    targets = tree.points[tree.targets]
+    tmask = tree.point_index[tree.targets] == node
+    tp = targets[tmask]
+    ds = downsurf(tree.corners[node], res, shells)
+    u = apply_kernel(ds, tp, downpot[node].reshape(-1, 3), eps, mu)
+    for un in tree.U[node]:
+        src, g = _leaf_sources(tree, un, pot)
+        if len(src):
+            u += apply_kernel(src, tp, g, eps, mu)
+    w = tree.W[node]
+    if len(w):
+        ws = np.concatenate([upsurf(tree.corners[k], res, shells) for k in w])
+        wp = np.concatenate([uppot[k].reshape(-1, 3) for k in w])
+        u += apply_kernel(ws, tp, wp, eps, mu)
+    return tmask, u
+
+
+def down_levels(tree):
+    """The nodes of levels 1..max (downwardPass.m:39-44; the root's downward
+    expansion is zero) and the non-empty target leaves (:170-176)."""
+    ids = tree.ids()
+    levels = [ids[tree.level[1:] == level] for level in range(1, int(tree.level[1:].max()) + 1)]
+    return levels, ids[tree.is_leaf_target(ids)]
 
 
 def downward_pass(tree, pot, uppot, eps, mu, res=6, shells=1):
@@ -120,46 +190,14 @@ def downward_pass(tree, pot, uppot, eps, mu, res=6, shells=1):
     X (P2L) and the parent's downsurf (L2L), then kernel(downsurf,upsurf)\\RHS.
     Then for every non-empty target leaf: L2T + U (P2P) + W (M2T)."""
     P = surface_count(res, shells)
-    nc = tree.node_count
-    downpot = np.zeros((nc + 1, 3 * P))
-    ids = tree.ids()
-    for level in range(1, int(tree.level[1:].max()) + 1):
-        for node in ids[tree.level[1:] == level]:
-            us = upsurf(tree.corners[node], res, shells)
-            ds = downsurf(tree.corners[node], res, shells)
-            rhs = np.zeros((P, 3))
-            v = tree.V[node]
-            if len(v):
-                vs = np.concatenate([upsurf(tree.corners[k], res, shells) for k in v])
-                vp = np.concatenate([uppot[k].reshape(-1, 3) for k in v])
-                rhs += apply_kernel(vs, us, vp, eps, mu)
-            for xn in tree.X[node]:
-                src, g = _leaf_sources(tree, xn, pot)
-                if len(src):
-                    rhs += apply_kernel(src, us, g, eps, mu)
-            par = tree.parent[node]
-            ps = downsurf(tree.corners[par], res, shells)
-            rhs += apply_kernel(ps, us, downpot[par].reshape(-1, 3), eps, mu)
-            K = kernel(ds, us, eps, mu)
-            downpot[node] = sla.solve(K, rhs.reshape(-1))
-    targets = tree.points[tree.targets]
-    tidx = tree.point_index[tree.targets]
-    vel = np.zeros((len(targets), 3))
-    leaves = ids[tree.is_leaf_target(ids)]
+    downpot = np.zeros((tree.node_count + 1, 3 * P))
+    levels, leaves = down_levels(tree)
+    for nodes in levels:
+        for node in nodes:
+            downpot[node] = down_node(tree, node, pot, uppot, downpot, eps, mu, res, shells)
+    vel = np.zeros((int(tree.targets.sum()), 3))
     for node in leaves:
-        tmask = tidx == node
-        tp = targets[tmask]
-        ds = downsurf(tree.corners[node], res, shells)
-        u = apply_kernel(ds, tp, downpot[node].reshape(-1, 3), eps, mu)
-        for un in tree.U[node]:
-            src, g = _leaf_sources(tree, un, pot)
-            if len(src):
-                u += apply_kernel(src, tp, g, eps, mu)
-        w = tree.W[node]
-        if len(w):
-            ws = np.concatenate([upsurf(tree.corners[k], res, shells) for k in w])
-            wp = np.concatenate([uppot[k].reshape(-1, 3) for k in w])
-            u += apply_kernel(ws, tp, wp, eps, mu)
+        tmask, u = leaf_velocity(tree, node, pot, uppot, downpot, eps, mu, res, shells)
         vel[tmask] = u
     return vel
 

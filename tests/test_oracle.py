@@ -4,6 +4,8 @@ The reference ships no golden vectors; its one built-in known answer is the
 Stokes drag of the unit sphere, [6*pi; 0; 0]
 (Data Generation/DirectMethodComparison.m:34, Benchmarkresistance.m:12,35).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -200,3 +202,31 @@ def test_hegedus_scale_minimises_the_residual():
     r = lambda s: np.linalg.norm(b - A @ (s * xp))
     s0 = float(x0 @ xp / (xp @ xp))
     assert r(s0) <= min(r(s0 * 1.001), r(s0 * 0.999))
+
+
+def test_parfor_matvec_matches_the_serial_oracle():
+    """The reference arm's matvec (the reference's parfor loops over the nodes
+    of a level on spawned worker processes, one BLAS thread each) gives the
+    serial oracle's velocities on the NEAREST golden case."""
+    import scipy.sparse as sp
+    from threadpoolctl import threadpool_limits
+
+    from conftest import GOLDEN
+    from oracle.kifmm import KIFMM
+    from oracle.octree import OcTree
+    from oracle.parfor import ParforKIFMM
+    g = np.load(os.path.join(GOLDEN, "adaptive_nearest_1200.npz"))
+    NN = sp.csr_matrix((g["nn_data"], g["nn_indices"], g["nn_indptr"]))
+    tree = OcTree(g["coarse"], g["coarse"], node_capacity=int(g["cap"]), nearest=1, fine_points=g["fine"], NN=NN)
+    fmm = ParforKIFMM(tree, float(g["eps"]), float(g["mu"]), 2)
+    try:
+        v = fmm.compute_vel(g["F"])
+        v2 = fmm.compute_vel(2.0 * g["F"])
+    finally:
+        fmm.close()
+    with threadpool_limits(1):
+        ref = KIFMM(tree, float(g["eps"]), float(g["mu"])).compute_vel(g["F"])
+    assert np.abs(v - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert np.abs(v2 - 2.0 * ref).max() <= 1e-12 * np.abs(ref).max()  # state reset between calls
+    # the fixture was made with multi-threaded BLAS: LU rounding, lifted by cond ~1e10
+    assert np.abs(v - g["vel"]).max() <= 1e-7 * np.abs(ref).max()
