@@ -131,7 +131,7 @@ def batched_bodies(n_bodies=64, seed=20261206, nmin=2000, nmax=40000):
 
 
 def sphere_problem():
-    """Config-1 geometry: Sphere(1,[0 0 0],10) force nodes and Sphere(1,[0 0 0],40)
+    """The single rigid sphere: Sphere(1,[0 0 0],10) force nodes and Sphere(1,[0 0 0],40)
     quadrature nodes; eps = 0.01, mu = 1, nodeCapacity 60."""
     return dict(coarse=cube_sphere(1.0, (0, 0, 0), 10), fine=cube_sphere(1.0, (0, 0, 0), 40), eps=0.01, mu=1.0,
                 cap=60)

@@ -57,7 +57,7 @@ def test_tree_split_sources_targets():
     assert_same_tree(OracleTree(s, t, node_capacity=25), nk.OcTree(s, t, nodeCapacity=25))
 
 
-def test_tree_sphere_config1():
+def test_tree_sphere_488_points():
     c = sphere(1.0, [0, 0, 0], 10)
     assert_same_tree(OracleTree(c, c, node_capacity=60), nk.OcTree(c, c, nodeCapacity=60))
 
