@@ -63,17 +63,44 @@ def parse():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (SM clock, throttle reasons)."""
+    """SM clock and clock-event reasons sampled during the timed region: NVML
+    (nvidia-ml-py, read-only queries) from a thread every `period` seconds,
+    one sample taken at start() so the region always holds some; nvidia-smi
+    every 100 ms where NVML is unavailable."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # (name, NVML constant, its value in the NVML header)
+    REASONS = (("hw_slowdown", "nvmlClocksThrottleReasonHwSlowdown", 0x8),
+               ("hw_thermal_slowdown", "nvmlClocksThrottleReasonHwThermalSlowdown", 0x40),
+               ("sw_thermal_slowdown", "nvmlClocksThrottleReasonSwThermalSlowdown", 0x20),
+               ("sw_power_cap", "nvmlClocksThrottleReasonSwPowerCap", 0x4))
 
-    def __init__(self, device):
+    def __init__(self, device, period=0.005):
         self.device = device
+        self.period = period
         self.p = None
+        self.nv = None
 
     def start(self):
+        self.samples = []
+        try:
+            import threading
+
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.device)
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.nv = (nv, h, reasons, float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)))
+            self._sample()
+            self._halt = threading.Event()
+            self._thread = threading.Thread(target=self._loop, daemon=True)
+            self._thread.start()
+            return
+        except Exception:
+            self.nv = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
                                        "--format=csv,noheader,nounits", "-lms", "100"],
@@ -81,7 +108,34 @@ class Clocks:
         except OSError:
             self.p = None
 
+    def _sample(self):
+        nv, h, reasons, _ = self.nv
+        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(reasons(h))))
+
+    def _loop(self):
+        while not self._halt.wait(self.period):
+            try:
+                self._sample()
+            except Exception:
+                return
+
     def stop(self):
+        if self.nv:
+            self._halt.set()
+            self._thread.join(timeout=5)
+            nv, _, _, mx = self.nv
+            try:
+                self._sample()
+                nv.nvmlShutdown()
+            except Exception:
+                pass
+            self.nv = None
+            bits = 0
+            for _, r in self.samples:
+                bits |= r
+            active = sorted(n for n, const, val in self.REASONS if bits & int(getattr(nv, const, val)))
+            return {"sm_mhz": float(np.median([c for c, _ in self.samples])), "sm_max_mhz": mx,
+                    "samples": len(self.samples), "reasons": active, "source": f"nvml every {self.period * 1e3:g} ms"}
         if not self.p:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -101,7 +155,7 @@ class Clocks:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                "samples": len(sm), "reasons": sorted(reasons), "source": "nvidia-smi every 100 ms"}
 
 
 def dist_init(args):

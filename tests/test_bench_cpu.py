@@ -54,3 +54,56 @@ def test_pair_kernels_of_the_250k_matvec():
     r = bench.roofline(PHASES, STATS, "mixed", PEAKS)
     assert r["pair_kernels"]["frac"] == pytest.approx(0.41, abs=0.01)
     assert r["frac"] == pytest.approx(0.186, abs=0.005)
+
+
+class FakeNVML:
+    """Read-only NVML stand-in: an SM clock and a reason mask that change
+    once a few samples have been taken."""
+    NVML_CLOCK_SM = 1
+    nvmlClocksThrottleReasonSwPowerCap = 0x4
+
+    def __init__(self):
+        self.calls = 0
+        self.shut = False
+
+    def nvmlInit(self):
+        pass
+
+    def nvmlShutdown(self):
+        self.shut = True
+
+    def nvmlDeviceGetHandleByIndex(self, i):
+        return ("gpu", i)
+
+    def nvmlDeviceGetMaxClockInfo(self, h, kind):
+        return 1965
+
+    def nvmlDeviceGetClockInfo(self, h, kind):
+        self.calls += 1
+        return 1965 if self.calls < 4 else 1800
+
+    def nvmlDeviceGetCurrentClocksEventReasons(self, h):
+        return 0x1 if self.calls < 4 else 0x1 | 0x4  # idle, then power cap
+
+
+def test_clock_sampler_on_a_fake_nvml(monkeypatch):
+    import sys
+    import time
+    fake = FakeNVML()
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    c = bench.Clocks(0, period=0.002)
+    c.start()
+    time.sleep(0.05)
+    out = c.stop()
+    assert fake.shut and out["samples"] >= 5 and out["sm_max_mhz"] == 1965.0
+    assert out["reasons"] == ["sw_power_cap"] and out["source"].startswith("nvml")
+    assert out["sm_mhz"] in (1800.0, 1965.0, (1800.0 + 1965.0) / 2)
+
+
+def test_clock_sampler_without_nvml(monkeypatch):
+    import sys
+    monkeypatch.setitem(sys.modules, "pynvml", None)  # import fails
+    monkeypatch.setattr(bench.subprocess, "Popen", lambda *a, **k: (_ for _ in ()).throw(OSError("no nvidia-smi")))
+    c = bench.Clocks(0)
+    c.start()
+    assert c.stop()["reasons"] == ["nvidia-smi unavailable"]
