@@ -516,6 +516,15 @@ def reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def throughputs(ws, n_force, n_quad, stats, step_ms):
+    """The matvec's rates over all ranks besides target points per second:
+    sources (quadrature points, NEAREST) per second and near-field (U-list
+    P2P) pairs per second."""
+    sec = step_ms / 1e3
+    return {"targets_per_s": ws * n_force / sec, "sources_per_s": ws * n_quad / sec,
+            "near_pairs_per_s": ws * stats["pairs_p2p"] / sec}
+
+
 def roofline(per_step, stats, precision, peaks):
     """Roofline of the dominant phase of one matvec, from the live per-phase
     CUDA-event times (per_step: phase -> (ms, launches) per step) and the
@@ -649,7 +658,8 @@ def main():
                        "pairs_p2p": stats["pairs_p2p"], "pairs_up": stats["pairs_up"],
                        "pairs_down": stats["pairs_down"], "setup_s": round(setup_s, 2)},
             "roofline": roof, "e2e": e2e, "gpu_launches": gpu_launches * args.steps // max(args.steps, 1),
-            "gpu_launches_per_step": gpu_launches / args.steps, "clocks": clk}
+            "gpu_launches_per_step": gpu_launches / args.steps, "clocks": clk,
+            "throughput": throughputs(ws, args.n_force, args.n_quad, stats, step_ms)}
 
     if rank == 0 and not args.no_errors:
         rng = np.random.default_rng(7)

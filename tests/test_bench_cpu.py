@@ -107,3 +107,10 @@ def test_clock_sampler_without_nvml(monkeypatch):
     c = bench.Clocks(0)
     c.start()
     assert c.stop()["reasons"] == ["nvidia-smi unavailable"]
+
+
+def test_throughputs():
+    t = bench.throughputs(2, 250_000, 1_000_000, STATS, 7.8)
+    assert t["targets_per_s"] == pytest.approx(2 * 250_000 / 7.8e-3)
+    assert t["sources_per_s"] == pytest.approx(2 * 1_000_000 / 7.8e-3)
+    assert t["near_pairs_per_s"] == pytest.approx(2 * STATS["pairs_p2p"] / 7.8e-3)
