@@ -177,3 +177,57 @@ def test_large_duplicate_rows_rejected():
         y = np.concatenate([x[:60_000], extra, x[60_000:]])
         with pytest.raises(nk.NNKError, match="duplicate"):
             nk.OcTree(y, y, nodeCapacity=64, builder="host")
+
+
+def _lattice(n):
+    g = np.arange(n) / (n - 1.0)
+    return np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+
+
+@pytest.mark.parametrize("case", ["on_split_planes", "planar", "line", "two_scales", "negative_zero"])
+def test_tree_degenerate_inputs_match_oracle(case):
+    """Inputs where the reference's rules decide: points exactly on the
+    midpoint planes (strict p > centre), a flat and a one-dimensional cloud,
+    two clusters five decades apart, and -0.0 coordinates."""
+    rng = np.random.default_rng(31)
+    if case == "on_split_planes":
+        x, cap = _lattice(9), 20  # 729 points, every dyadic midpoint is a lattice plane
+    elif case == "planar":
+        x = rng.random((1500, 3))
+        x[:, 2] = 0.25
+        cap = 30
+    elif case == "line":
+        x = np.zeros((800, 3))
+        x[:, 0] = np.sort(rng.random(800))
+        x[:, 1] = 0.5
+        cap = 16
+    elif case == "two_scales":
+        x = np.concatenate([rng.random((600, 3)), 0.3 + 1e-5 * rng.random((300, 3))])
+        cap = 40
+    else:
+        x = rng.random((900, 3)) - 0.5
+        x[:40, 1] = -0.0
+        x[40:80, 1] = 0.0
+        x[40:80, 0] += 1e-3  # distinct rows, equal coordinates of either sign
+        cap = 25
+    depth = 23 if case == "two_scales" else 21  # 23: the library's largest maxDepth
+    t = nk.OcTree(x, x, nodeCapacity=cap, maxDepth=depth)
+    assert_same_tree(OracleTree(x, x, node_capacity=cap, max_depth=depth), t)
+    if case == "two_scales":
+        assert t.nodeLevel.max() >= 17
+
+
+def test_nearest_matrix_coincident_and_planar_ties():
+    """Fine points on coarse points (distance 0), on edge midpoints of a flat
+    lattice (2-way ties) and on its cell centres (4-way ties), bit for bit
+    against the oracle, host and default builders."""
+    g = np.arange(7) / 6.0
+    c = np.stack(np.meshgrid(g, g, indexing="ij"), -1).reshape(-1, 2)
+    c = np.concatenate([c, np.full((len(c), 1), 0.5)], axis=1)
+    h = 0.5 / 6.0
+    f = np.concatenate([c, c[:-1] + [h, 0, 0], c[:30] + [h, h, 0], c[5:25] + [0, 0, 0.3]])
+    A = nearest_matrix(c, f)
+    for builder in ("host", "auto"):
+        B = nk.nearestMatrix(c, f, builder=builder)
+        assert (A != B).nnz == 0 and A.nnz == B.nnz
+    assert B.getnnz(axis=1).max() == 4 and np.all(B[:len(c)].getnnz(axis=1) == 1)
