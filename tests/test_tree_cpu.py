@@ -231,3 +231,42 @@ def test_nearest_matrix_coincident_and_planar_ties():
         B = nk.nearestMatrix(c, f, builder=builder)
         assert (A != B).nnz == 0 and A.nnz == B.nnz
     assert B.getnnz(axis=1).max() == 4 and np.all(B[:len(c)].getnnz(axis=1) == 1)
+
+
+@pytest.mark.parametrize("case,code,message", [
+    ("nan_potential", 3, "non-finite potential point"),
+    ("inf_target", 3, "non-finite target point"),
+    ("inf_fine", 3, "non-finite fine point"),
+    ("no_points", 1, "no points"),
+    ("max_depth_above_23", 1, "maxDepth above 23"),
+])
+def test_host_fault_injection(case, code, message):
+    """Bad inputs come back as status codes with the reference's or a plain
+    message, before any device work (host builder)."""
+    rng = np.random.default_rng(51)
+    x = rng.random((60, 3))
+    t = rng.random((30, 3))
+    f = rng.random((90, 3))
+    kw = dict(nodeCapacity=10, builder="host")
+    if case == "nan_potential":
+        x[7, 2] = np.nan
+        args = (x, t)
+    elif case == "inf_target":
+        t[3, 0] = np.inf
+        args = (x, t)
+    elif case == "inf_fine":
+        f[11, 1] = -np.inf
+        args, kw = (x, x), dict(kw, nearest=1, finePoints=f, NN=nk.nearestMatrix(x, rng.random((90, 3)), builder="host"))
+    elif case == "no_points":
+        args = (np.zeros((0, 3)), np.zeros((0, 3)))
+    else:
+        args, kw = (x, x), dict(kw, maxDepth=24)
+    with pytest.raises(nk.NNKError, match=message) as e:
+        nk.OcTree(*args, **kw)
+    assert e.value.code == code
+
+
+def test_nearest_without_fine_points_rejected():
+    x = np.random.default_rng(52).random((40, 3))
+    with pytest.raises(ValueError, match="finePoints"):  # the host mirror, before the C ABI
+        nk.OcTree(x, x, nodeCapacity=10, nearest=1, builder="host")
