@@ -484,7 +484,9 @@ def reference_arm(args, ws, rank):
     from oracle.nearest import nearest_matrix
     from oracle.octree import OcTree as OTree
     from oracle.parfor import ParforKIFMM
-    workers = min(os.cpu_count() or 1, 64)
+    # the threads this process may run on (its CPU set), not the machine's count
+    avail = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    workers = min(avail, 64)
     nf = max(1000, 250 * workers)
     nq = 4 * nf
     w = matvec_at_scale(nf, nq)
