@@ -56,6 +56,8 @@ class KIFMM:
             xin = x.contiguous().to(torch.float64)
             if not xin.is_cuda:
                 raise ValueError("torch inputs must be CUDA tensors; pass numpy arrays for host data")
+            if xin.device.index != self.ctx.device:
+                raise ValueError(f"input on {xin.device}, the FMM on cuda:{self.ctx.device}")
             out = torch.empty(nrhs * 3 * n_out, dtype=torch.float64, device=xin.device)
             dev = 1
         else:
