@@ -35,6 +35,11 @@ WORKLOAD = ("FMM matvec at scale: 250k force / 1M quadrature points (50% uniform
             "20 spheres r=0.05-0.2), NEAREST, eps=1e-3, mu=1, nodeCapacity 64, p=6")
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SIMT FP32 FMA pipes at max clock
+# DRAM bytes (read + write) of one compressed tensor-core M2L launch on the 250k
+# workload, scaled by V pairs from the one-launch ncu capture of the 60k case
+# (profiles/m2l_compressed_kernel_60k.md: 0.433 GB read + 9.4 MB written for
+# 329,328 V pairs)
+M2L_TRAFFIC_250K = (0.433e9 + 9.4e6) * 1426620 / 329328
 FLOPS_PER_PAIR = 32  # regularized Stokeslet pair: 3 sub, 5 r^2, 1 +eps^2, 1 rsqrt, 2 cube, 5 r.f, 3 scale, 12 acc
 
 
@@ -44,7 +49,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"],
+                    help="the matvec arm timed for `value` (the other arm is timed after it and reported "
+                         "under its own key unless --one-arm)")
+    ap.add_argument("--one-arm", action="store_true", help="time only the --precision arm (profiling runs)")
     ap.add_argument("--n-force", type=int, default=250_000)
     ap.add_argument("--n-quad", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -54,7 +62,8 @@ def parse():
     ap.add_argument("--no-gradient", action="store_true")
     ap.add_argument("--no-squirmers", action="store_true")
     ap.add_argument("--m2l", default="auto", choices=["auto", "images", "generate", "pairs", "fft"],
-                    help="M2L form of the mixed matvec (auto: tensor cores on rank-256 compressed operators)")
+                    help="M2L form of the mixed matvec (auto: tensor cores on rank-256 compressed operators); "
+                         "the FP64 matvec runs its Fourier-space M2L unless this is 'pairs'")
     ap.add_argument("--batch-apply", type=int, default=0,
                     help="only build the mixed batch of --batch-bodies bodies and time this many matvecs "
                          "(6 rigid-mode right-hand sides each; for profiling the batch kernels)")
@@ -189,9 +198,13 @@ def allmax(ws, v):
 def build(nk, w, precision, m2l="auto"):
     NN = nk.nearestMatrix(w["coarse"], w["fine"])
     tree = nk.OcTree(w["coarse"], w["coarse"], nodeCapacity=w["cap"], nearest=1, finePoints=w["fine"], NN=NN)
+    return NN, tree, make_fmm(nk, w, tree, precision, m2l)
+
+
+def make_fmm(nk, w, tree, precision, m2l="auto"):
     fmm = nk.KIFMM(tree, [w["eps"], w["mu"]], precision=precision, m2l=m2l)
     fmm.autotune(1)  # pair-kernel tile per launch group (part of the set-up)
-    return NN, tree, fmm
+    return fmm
 
 
 def time_device(torch, fmm, fin, fout, steps, warmup, flush, prof=False):
@@ -448,6 +461,17 @@ def squirmer_benchmark(torch, nk, args):
     return out
 
 
+def workloads_module():
+    """nnkifmm/workloads.py (numpy only) loaded on its own: the reference arm
+    must not import the package, whose import maps libnnkifmm.so."""
+    import importlib.util
+    path = os.path.join(ROOT, "stokes-nnkifmm_b200", "nnkifmm", "workloads.py")
+    spec = importlib.util.spec_from_file_location("nnk_workloads_standalone", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def cpu_baseline_sample(n_force, n_quad, steps=1, threads=1):
     """The oracle (reference structure, per-node LU, FP64 numpy) on a reduced
     instance of the same workload distribution, its BLAS/LAPACK calls on
@@ -480,7 +504,7 @@ def reference_arm(args, ws, rank):
     (250 force points each) so that every level keeps them busy."""
     if rank != 0:
         return
-    from nnkifmm.workloads import matvec_at_scale
+    matvec_at_scale = workloads_module().matvec_at_scale
     from oracle.nearest import nearest_matrix
     from oracle.octree import OcTree as OTree
     from oracle.parfor import ParforKIFMM
@@ -527,18 +551,25 @@ def throughputs(ws, n_force, n_quad, stats, step_ms):
             "near_pairs_per_s": ws * stats["pairs_p2p"] / sec}
 
 
-def roofline(per_step, stats, precision, peaks):
+def roofline(per_step, stats, precision, peaks, m2l_form):
     """Roofline of the dominant phase of one matvec, from the live per-phase
     CUDA-event times (per_step: phase -> (ms, launches) per step) and the
     algorithmic work of the tree statistics; `pair_kernels` adds the same for
-    all pair phases together (S2M/M2M/L2L/L2T, P2L/M2T and the near field)."""
+    all pair phases together (S2M/M2M/L2L/L2T, P2L/M2T and the near field).
+    m2l_form: 'tensor' (compressed tcgen05 M2L), 'fourier' or 'pairs'."""
     dom = max((k for k in per_step if per_step[k][1] > 0), key=lambda k: per_step[k][0])
+    fp64 = precision == "fp64"
+    simt_peak = FP32_NOMINAL_TFLOPS / (2 if fp64 else 1)
+    simt_src = ("nominal SIMT FP64 (148 SM x 64 lanes x 2 x 1.965 GHz)" if fp64 else
+                "nominal SIMT FP32 (148 SM x 128 lanes x 2 x 1.965 GHz)") + \
+        "; MEASURED_PEAKS.json holds only HBM and bf16 tensor figures"
     # pairs_down counts the V list as P x P pairs per M2L; when the M2L runs as
     # its own phase (tensor cores or Fourier space) the down pairs are the rest
     m2l_apart = per_step.get("m2l", (0.0, 0))[1] > 0
     down = stats["pairs_down"] - (stats["m2l_pairs"] * stats["surface_points"] ** 2 if m2l_apart else 0)
     pairs = {"up_pairs": stats["pairs_up"], "down_pairs": down, "leaf_pairs": stats["pairs_leaf"]}
-    if dom == "m2l":
+    ms_l = per_step[dom][0] / per_step[dom][1]
+    if dom == "m2l" and m2l_form == "tensor":
         n3 = 3 * stats["surface_points"]
         rk = stats["m2l_rank"] or n3
         terms = 2 if stats["m2l_rank"] else 1  # the compressed form splits the densities into two TF32 terms
@@ -555,24 +586,32 @@ def roofline(per_step, stats, precision, peaks):
                                f"step (useful rows only, no padding; the phase also holds the FP32 basis projection "
                                f"and expansion, 2 x 2 x 456 x {rk} flops per node)",
                 "padded_rows_over_useful": stats["m2l_tile_rows"] / max(stats["m2l_pairs"], 1),
-                "launches_per_step": per_step[dom][1], "ms_per_launch": per_step[dom][0] / per_step[dom][1],
-                "traffic": None}
+                "launches_per_step": per_step[dom][1], "ms_per_launch": ms_l,
+                "traffic": M2L_TRAFFIC_250K if stats["m2l_rank"] else None,
+                "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of the 60k capture (one launch), "
+                                  "scaled by V pairs to the 250k launch (profiles/m2l_compressed_kernel_60k.md)"}
+    elif dom == "m2l" and m2l_form == "fourier":
+        res = 6
+        nk_freq = (2 * res) ** 2 * (res + 1)
+        flops = 72.0 * nk_freq * stats["m2l_pairs"]  # 9 complex multiply-adds per pair and frequency
+        roof = {"kernel": f"fft_accumulate_kernel ({'FP64' if fp64 else 'FP32'} spectra) with the forward and "
+                          "inverse lattice transforms", "bound": "fp64" if fp64 else "fp32",
+                "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": simt_peak, "unit": "TFLOP/s",
+                "peak_source": simt_src, "launches_per_step": per_step[dom][1], "ms_per_launch": ms_l,
+                "algorithmic": f"{stats['m2l_pairs']} V pairs x {nk_freq} frequencies x 9 complex multiply-adds "
+                               f"(72 flops) per step; the transforms are not counted", "traffic": None}
     elif dom in pairs:
         flops = pairs[dom] * FLOPS_PER_PAIR
-        fp64 = precision == "fp64"
-        peak = FP32_NOMINAL_TFLOPS / (2 if fp64 else 1)
         roof = {"kernel": f"p2p_kernel ({dom})", "bound": "fp64" if fp64 else "fp32",
-                "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
-                "peak_source": "nominal SIMT FP32 (148 SM x 128 lanes x 2 x 1.965 GHz); MEASURED_PEAKS.json "
-                               "holds only HBM and bf16 tensor figures",
-                "launches_per_step": per_step[dom][1], "ms_per_launch": per_step[dom][0] / per_step[dom][1],
+                "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": simt_peak, "unit": "TFLOP/s",
+                "peak_source": simt_src, "launches_per_step": per_step[dom][1], "ms_per_launch": ms_l,
                 "algorithmic": f"{pairs[dom]} pairs x {FLOPS_PER_PAIR} flops per step", "traffic": None}
     else:
         n = 3 * stats["surface_points"]
         flops = 2.0 * n * n * stats["c2e_columns"]
         roof = {"kernel": f"c2e_kernel ({dom})", "bound": "fp64", "achieved": flops / (per_step[dom][0] / 1e3) / 1e12,
-                "algorithmic": "2 x (3P)^2 flops per node per pass",
-                "peak": FP32_NOMINAL_TFLOPS / 2, "unit": "TFLOP/s", "traffic": None}
+                "algorithmic": "2 x (3P)^2 flops per node per pass", "peak": FP32_NOMINAL_TFLOPS / 2,
+                "peak_source": "nominal SIMT FP64", "unit": "TFLOP/s", "traffic": None}
     roof["frac"] = roof["achieved"] / roof["peak"]
     roof["phases_ms_per_step"] = {k: round(v[0], 4) for k, v in per_step.items()}
     if peaks:
@@ -580,14 +619,45 @@ def roofline(per_step, stats, precision, peaks):
     pair_ms = sum(per_step.get(k, (0.0, 0))[0] for k in ("up_pairs", "down_pairs", "leaf_pairs"))
     if pair_ms > 0:
         npairs = sum(pairs.values())
-        peak = FP32_NOMINAL_TFLOPS / (2 if precision == "fp64" else 1)
         achieved = npairs * FLOPS_PER_PAIR / (pair_ms / 1e3) / 1e12
         roof["pair_kernels"] = {"kernel": "p2p_kernel (up, down and leaf pair phases)",
-                                "bound": "fp64" if precision == "fp64" else "fp32", "achieved": achieved,
-                                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "ms_per_step": pair_ms,
+                                "bound": "fp64" if fp64 else "fp32", "achieved": achieved,
+                                "peak": simt_peak, "unit": "TFLOP/s", "frac": achieved / simt_peak,
+                                "ms_per_step": pair_ms,
                                 "algorithmic": f"{npairs} pairs x {FLOPS_PER_PAIR} flops per step",
-                                "peak_source": "nominal SIMT FP32 (148 SM x 128 lanes x 2 x 1.965 GHz)"}
+                                "peak_source": simt_src}
     return roof
+
+
+def time_arm(torch, nk, w, tree, precision, m2l, args, flush, clocks=None):
+    """One matvec arm: builds the FMM, times args.steps device-resident
+    matvecs (CUDA events, L2 flushed between steps) with per-phase events,
+    then the same through the C ABI with pinned host buffers (e2e)."""
+    fmm = make_fmm(nk, w, tree, precision, m2l)
+    fin = torch.tensor(w["forces"], device="cuda").contiguous()
+    fout = torch.empty_like(fin)
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    ms, prof = time_device(torch, fmm, fin, fout, args.steps, args.warmup, flush, prof=True)
+    torch.cuda.synchronize()
+    clk = clocks.stop() if clocks else None
+    hin = torch.tensor(w["forces"]).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        fmm.apply_raw(hin.data_ptr(), hout.data_ptr(), on_device=0)
+    st = torch.cuda.current_stream()
+    e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        fmm.apply_raw(hin.data_ptr(), hout.data_ptr(), on_device=0)
+        b.record(st)
+        torch.cuda.synchronize()
+        e_ms.append(a.elapsed_time(b))
+    return {"fmm": fmm, "ms": ms, "prof": prof, "clocks": clk, "out": fout.cpu().numpy(), "e2e_ms": e_ms,
+            "h2d": int(hin.numel() * 8), "d2h": int(hout.numel() * 8)}
 
 
 def main():
@@ -607,77 +677,85 @@ def main():
         return
     t0 = time.time()
     w = matvec_at_scale(args.n_force, args.n_quad)
-    NN, tree, fmm = build(nk, w, args.precision, args.m2l if args.precision == "mixed" else "auto")
-    setup_s = time.time() - t0
-    stats = fmm.stats()
-    fin = torch.tensor(w["forces"], device="cuda").contiguous()
-    fout = torch.empty_like(fin)
+    NN = nk.nearestMatrix(w["coarse"], w["fine"])
+    tree = nk.OcTree(w["coarse"], w["coarse"], nodeCapacity=w["cap"], nearest=1, finePoints=w["fine"], NN=NN)
+    tree_s = time.time() - t0
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    clocks = Clocks(local)
-
-    barrier(ws)
-    torch.cuda.synchronize()
-    clocks.start()
-    ms, prof = time_device(torch, fmm, fin, fout, args.steps, args.warmup, flush, prof=True)
-    torch.cuda.synchronize()
-    barrier(ws)
-    clk = clocks.stop()
-    step_ms = allmax(ws, float(np.mean(ms)))
-    value = ws * args.n_force / (step_ms / 1e3)
-    gpu_launches = int(sum(n for _, n in prof.values()))
-
-    # e2e: pinned host buffers through the C ABI (H2D + matvec + D2H per step)
-    hin = torch.tensor(w["forces"]).pin_memory()
-    hout = torch.empty_like(hin).pin_memory()
-    for _ in range(max(1, args.warmup)):
-        fmm.apply_raw(hin.data_ptr(), hout.data_ptr(), on_device=0)
-    st = torch.cuda.current_stream()
-    e_ms = []
-    for _ in range(args.steps):
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(st)
-        fmm.apply_raw(hin.data_ptr(), hout.data_ptr(), on_device=0)
-        b.record(st)
-        torch.cuda.synchronize()
-        e_ms.append(a.elapsed_time(b))
-    e2e_ms = allmax(ws, float(np.mean(e_ms)))
-    e2e = {"value": ws * args.n_force / (e2e_ms / 1e3), "unit": "pts/s", "ms_per_step": e2e_ms,
-           "h2d_bytes_per_step": int(hin.numel() * 8), "d2h_bytes_per_step": int(hout.numel() * 8)}
-
-    # roofline of the dominant phase (live CUDA events over the timed region)
     peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
-    per_step = {k: (v[0] / args.steps, v[1] / args.steps) for k, v in prof.items()}
-    roof = roofline(per_step, stats, args.precision, peaks)
+    m2l_of = {"fp64": "pairs" if args.m2l == "pairs" else "auto", "mixed": args.m2l}
+    form_of = {"fp64": "pairs" if args.m2l == "pairs" else "fourier",
+               "mixed": {"auto": "tensor", "images": "tensor", "generate": "tensor", "pairs": "pairs",
+                         "fft": "fourier"}[args.m2l]}
+    head = args.precision
+    arms = [head] if args.one_arm else [head, "mixed" if head == "fp64" else "fp64"]
+    res = {}
+    for k, prec in enumerate(arms):
+        barrier(ws)
+        t1 = time.time()
+        r = time_arm(torch, nk, w, tree, prec, m2l_of[prec], args, flush, Clocks(local) if k == 0 else None)
+        r["setup_s"] = time.time() - t1
+        barrier(ws)
+        r["step_ms"] = allmax(ws, float(np.mean(r["ms"])))
+        r["e2e_step_ms"] = allmax(ws, float(np.mean(r["e2e_ms"])))
+        r["per_step"] = {kk: (v[0] / args.steps, v[1] / args.steps) for kk, v in r["prof"].items()}
+        r["stats"] = r["fmm"].stats()
+        r["roofline"] = roofline(r["per_step"], r["stats"], prec, peaks, form_of[prec])
+        res[prec] = r
+    H = res[head]
+    stats = H["stats"]
+    step_ms = H["step_ms"]
+    value = ws * args.n_force / (step_ms / 1e3)
+    gpu_launches = int(sum(n for _, n in H["prof"].values()))
+    e2e = {"value": ws * args.n_force / (H["e2e_step_ms"] / 1e3), "unit": "pts/s", "ms_per_step": H["e2e_step_ms"],
+           "h2d_bytes_per_step": H["h2d"], "d2h_bytes_per_step": H["d2h"]}
 
-    line = {"metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "precision": args.precision, "parallelism": f"replicas x{ws}",
-                       "l2": "flushed between timed steps (256 MiB write, outside the step events)",
-                       "nodes": tree.nodeCount, "levels": int(tree.info.max_level) + 1,
-                       "m2l_pairs": stats["m2l_pairs"], "pairs_leaf": stats["pairs_leaf"],
-                       "pairs_p2p": stats["pairs_p2p"], "pairs_up": stats["pairs_up"],
-                       "pairs_down": stats["pairs_down"], "setup_s": round(setup_s, 2)},
-            "roofline": roof, "e2e": e2e, "gpu_launches": gpu_launches * args.steps // max(args.steps, 1),
-            "gpu_launches_per_step": gpu_launches / args.steps, "clocks": clk,
-            "throughput": throughputs(ws, args.n_force, args.n_quad, stats, step_ms)}
-
+    # errors against an FP64 direct sum on 4096 sampled targets, before the line is built
+    errors = None
     if rank == 0 and not args.no_errors:
         rng = np.random.default_rng(7)
         idx = np.sort(rng.choice(args.n_force, 4096, replace=False))
         ref = sampled_direct(torch, w, NN, idx)
-        v = fout.cpu().numpy()
-        other = nk.KIFMM(tree, [w["eps"], w["mu"]], precision="fp64" if args.precision == "mixed" else "mixed")
-        other.autotune(1)
-        fo = torch.empty_like(fin)
-        ms2, _ = time_device(torch, other, fin, fo, max(3, args.steps // 2), 2, flush)
-        v2 = fo.cpu().numpy()
         rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
-        mine, oth = ("mixed", "fp64") if args.precision == "mixed" else ("fp64", "mixed")
-        line["errors"] = {f"{mine}_vs_direct_4096": rel(v[idx], ref), f"{oth}_vs_direct_4096": rel(v2[idx], ref),
-                          "mixed_vs_fp64": rel(v if mine == "mixed" else v2, v2 if mine == "mixed" else v)}
-        line[f"{oth}_gpu"] = {"value": args.n_force / (float(np.mean(ms2)) / 1e3), "ms_per_step": float(np.mean(ms2))}
+        errors = {f"{p}_vs_direct_4096": rel(res[p]["out"][idx], ref) for p in res}
+        if len(res) == 2:
+            errors["mixed_vs_fp64"] = rel(res["mixed"]["out"], res["fp64"]["out"])
+    note = None
+    if head == "mixed" and errors and errors.get("mixed_vs_fp64", 0.0) > 1e-4:
+        # the metric holds at <= 1e-4 relative error against the FP64 operator
+        note = (f"mixed matvec is {errors['mixed_vs_fp64']:.2e} from the FP64 matvec (> 1e-4): value withheld; "
+                "the FP64 arm's rate is under fp64_gpu")
+        value = None
+
+    line = {"metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": head,
+                       "m2l": {"fp64": "FP64 Fourier-space (FP64 spectra)", "mixed": "TF32 tensor cores (tcgen05), "
+                               "rank-256 compressed operators"}[head] if args.m2l == "auto" else args.m2l,
+                       "parallelism": f"replicas x{ws}",
+                       "l2": "flushed between timed steps (256 MiB write, outside the step events)",
+                       "nodes": tree.nodeCount, "levels": int(tree.info.max_level) + 1,
+                       "m2l_pairs": stats["m2l_pairs"], "pairs_leaf": stats["pairs_leaf"],
+                       "pairs_p2p": stats["pairs_p2p"], "pairs_up": stats["pairs_up"],
+                       "pairs_down": stats["pairs_down"], "tree_nn_s": round(tree_s, 2),
+                       "fmm_setup_s": round(H["setup_s"], 2)},
+            "roofline": H["roofline"], "e2e": e2e, "gpu_launches": gpu_launches // max(args.steps, 1),
+            "gpu_launches_per_step": gpu_launches / args.steps, "clocks": H["clocks"],
+            "throughput": throughputs(ws, args.n_force, args.n_quad, stats, step_ms)}
+    if note:
+        line["note"] = note
+    if errors:
+        line["errors"] = errors
+    for p in res:
+        if p == head:
+            continue
+        o = res[p]
+        line[f"{p}_gpu"] = {"value": ws * args.n_force / (o["step_ms"] / 1e3), "unit": "pts/s",
+                            "ms_per_step": o["step_ms"], "dtype": "f32" if p == "mixed" else "f64",
+                            "e2e_value": ws * args.n_force / (o["e2e_step_ms"] / 1e3),
+                            "speedup_vs_" + head: H["step_ms"] / o["step_ms"], "roofline": o["roofline"],
+                            "fmm_setup_s": round(o["setup_s"], 2)}
+    del res
     if rank == 0 and not args.no_solves:
         line["mobility_solves"] = solve_benchmarks(torch, nk, args)
     if rank == 0 and not args.no_gradient:

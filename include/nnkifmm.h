@@ -99,7 +99,10 @@ typedef struct nnk_fmm_params {
                             2 tensor cores + in-kernel operators, 3 FP32 pair
                             kernel (no tensor cores; FP32-rounding accuracy),
                             4 FP32 Fourier-space product (FFT of the surface
-                            lattice; FP32-rounding accuracy)                  */
+                            lattice; FP32-rounding accuracy).
+                            FP64 mode: 3 the FP64 pair kernel, any other value
+                            the FP64 Fourier-space product (at most 4
+                            right-hand sides per pass)                        */
   double reg;            /* relative Tikhonov weight of the check-to-equivalent
                             pseudo-inverse: NNK_PREC_MIXED 0 = default 1e-5;
                             NNK_PREC_FP64 0 = exact LU inverse (reference)   */
@@ -159,6 +162,19 @@ int nnk_nearest_matrix_host(nnk_ctx* ctx, const double* coarse, int64_t n, const
 int nnk_nearest_matrix(nnk_ctx* ctx, const double* coarse, int64_t n,
                        const double* fine, int64_t q, int64_t* nnz,
                        int64_t* rowptr, int32_t* col, double* val);
+/* The tie weights of nearestMatrix.m as written (nearestMatrix.m:23-39), for
+ * callers that need the reference's matrix entry for entry.  The reference
+ * cuts the fine points into blocks of floor(blockSize 2^27 / (9 q)) and, per
+ * block, pairs the tied (fine, coarse) entries taken in column-major order
+ * (find) with the weights 1/k taken in row-major order (logical indexing of
+ * the transpose): where rows with different tie counts share a block,
+ * weights move to other rows and rows stop summing to one.  Rewrites val of
+ * a matrix from nnk_nearest_matrix (rowptr q+1, ascending col per row) in
+ * place into that pairing; tie-free rows keep weight 1.  NNK_E_ARG when the
+ * block is empty (the reference builds no matrix then).  Host only. */
+int nnk_nearest_reference_weights(nnk_ctx* ctx, int64_t q, const int64_t* rowptr,
+                                  const int32_t* col, double* val,
+                                  double block_size);
 
 /* --------------------------------------------------------------- tree -- */
 /* OcTree(potPoints, targetPoints, ...) (OcTree.m:77-129).
@@ -252,6 +268,17 @@ int nnk_fmm_grad_positions(nnk_fmm* fmm, const double* forces, const double* wei
 
 int nnk_fmm_profile(nnk_fmm* fmm, int32_t enable);
 int nnk_fmm_profile_read(nnk_fmm* fmm, double* ms, int64_t* launches);
+/* No counterpart in the reference (its waits are MATLAB's): failure-path test
+ * of the bounded device waits.  Every wait of the tensor-core M2L kernel on an
+ * mbarrier gives up after a limit, sets the FMM's error flag and lets the
+ * kernel drain and return; the call that launched it (or, with on_device = 1,
+ * a later call on the same FMM) returns NNK_E_TIMEOUT and the flag is cleared.
+ * This runs that kernel of a mixed FMM once with every thread first waiting,
+ * at most `polls` polls, on a barrier that nothing completes: the wait gives
+ * up before any copy or MMA is issued, the kernel frees its tensor memory and
+ * returns, and the call returns NNK_E_TIMEOUT.  Later applies run normally.
+ * NNK_E_STATE for an FMM without the tensor-core M2L. */
+int nnk_fmm_test_wait_timeout(nnk_fmm* fmm, uint32_t polls);
 int nnk_fmm_destroy(nnk_fmm* fmm);
 
 /* Device GMRES on the FMM operator: solves computeVel(x) = b, the resistance

@@ -85,6 +85,15 @@ void finish_out(nnk_ctx* ctx, nnk::DBuf<double>& buf, double* p, size_t count, i
     NNK_CUDA(cudaMemcpyAsync(p, buf.p, count * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   if (!on_device) NNK_CUDA(cudaStreamSynchronize(ctx->stream));
 }
+// Device-side failures of the call's launches (a bounded wait that gave up)
+// become the call's status: after a host-output call, which has waited for
+// the stream anyway, or after a solve (synchronized at every step), every
+// flag is read; a device-output call reads the flags whose copies have
+// completed, and a later call on the same FMM reports the rest.
+void device_errors(nnk::Fmm& F, int waited) {
+  if (waited) F.check_errors();
+  else F.poll_errors();
+}
 
 }  // namespace
 
@@ -170,6 +179,15 @@ int nnk_nearest_matrix(nnk_ctx* ctx, const double* coarse, int64_t n, const doub
 int nnk_nearest_matrix_host(nnk_ctx* ctx, const double* coarse, int64_t n, const double* fine, int64_t q,
                             int64_t* nnz, int64_t* rowptr, int32_t* col, double* val) {
   return nearest_common(ctx, coarse, n, fine, q, nnz, rowptr, col, val, true);
+}
+
+int nnk_nearest_reference_weights(nnk_ctx* ctx, int64_t q, const int64_t* rowptr, const int32_t* col, double* val,
+                                  double block_size) {
+  if (q < 0 || (q > 0 && (!rowptr || !col || !val)) || !(block_size > 0))
+    return fail(ctx, NNK_E_ARG, "bad arguments");
+  API_TRY
+  nnk::nearest_reference_weights(q, rowptr, col, val, block_size);
+  API_CATCH(ctx)
 }
 
 int nnk_tree_build(nnk_ctx* ctx, const double* pot, int64_t n_pot, const double* tgt, int64_t n_tgt,
@@ -303,6 +321,7 @@ static int fmm_apply_common(nnk_fmm* fmm, const double* in, double* out, int32_t
   else if (which == 2) F.reduced_apply(din, dout, layout);
   else F.reduced_solve(din, dout, layout);
   finish_out(ctx, F.io_out, out, nout, on_device);
+  device_errors(F, !on_device);
   API_CATCH(ctx)
 }
 
@@ -335,6 +354,7 @@ int nnk_fmm_apply_adjoint(nnk_fmm* fmm, const double* in, double* out, int32_t l
   double* dout = stage_out(F.io_out, out, nout, on_device);
   F.apply_adjoint(din, dout, layout, nrhs);
   finish_out(ctx, F.io_out, out, nout, on_device);
+  device_errors(F, !on_device);
   API_CATCH(ctx)
 }
 
@@ -418,6 +438,18 @@ int nnk_fmm_profile_read(nnk_fmm* fmm, double* ms, int64_t* launches) {
   API_CATCH(ctx)
 }
 
+int nnk_fmm_test_wait_timeout(nnk_fmm* fmm, uint32_t polls) {
+  if (!fmm || polls == 0) return fail(fmm ? fmm->ctx : nullptr, NNK_E_ARG, "bad arguments");
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  const int flag = fmm->f->m2l_stall_probe(polls);
+  if (flag)
+    return fail(ctx, NNK_E_TIMEOUT, "tensor-core M2L gave up a bounded wait (flag " + std::to_string(flag) + ")");
+  return fail(ctx, NNK_E_STATE, "the probe's bounded wait did not give up");
+  API_CATCH(ctx)
+}
+
 int nnk_fmm_destroy(nnk_fmm* fmm) {
   if (!fmm) return NNK_E_ARG;
   nnk_ctx* c = fmm->ctx;
@@ -445,6 +477,7 @@ int nnk_fmm_solve(nnk_fmm* fmm, const double* b, double* x, int32_t layout, cons
   auto op = [&](const double* in, double* outp) { F.apply(in, outp, layout, 1); };
   g.solve(op, nullptr, db, dx, *sp, inf);
   finish_out(ctx, F.io_out, x, n, on_device);
+  device_errors(F, 1);
   if (info) *info = inf;
   if (inf.flag != 0) return fail(ctx, NNK_E_NOCONV, "gmres stopped at maxit above tol");
   API_CATCH(ctx)
@@ -474,6 +507,7 @@ int nnk_mob_apply(nnk_mob* mob, const double* x, double* y, int32_t on_device) {
   double* dy = stage_out(M.io_out, y, n, on_device);
   M.apply(dx, dy);
   finish_out(ctx, M.io_out, y, n, on_device);
+  device_errors(*mob->fmm->f, !on_device);
   API_CATCH(ctx)
 }
 
@@ -497,6 +531,7 @@ int nnk_mob_precon(nnk_mob* mob, const double* x, double* y, int32_t on_device) 
   double* dy = stage_out(M.io_out, y, n, on_device);
   M.precon(dx, dy);
   finish_out(ctx, M.io_out, y, n, on_device);
+  device_errors(*mob->fmm->f, !on_device);
   API_CATCH(ctx)
 }
 
@@ -513,6 +548,7 @@ int nnk_mob_solve(nnk_mob* mob, const double* rhs, double* x, const nnk_solve_pa
   nnk_solve_info inf{};
   M.solve(db, dx, *sp, precondition != 0, inf);
   finish_out(ctx, M.io_out, x, n, on_device);
+  device_errors(*mob->fmm->f, 1);
   if (info) *info = inf;
   if (inf.flag != 0) return fail(ctx, NNK_E_NOCONV, "gmres stopped at maxit above tol");
   API_CATCH(ctx)
@@ -539,6 +575,7 @@ int nnk_mob_apply_adjoint(nnk_mob* mob, const double* x, double* y, int32_t on_d
   double* dy = stage_out(M.io_out, y, n, on_device);
   M.apply_adjoint(dx, dy);
   finish_out(ctx, M.io_out, y, n, on_device);
+  device_errors(*mob->fmm->f, !on_device);
   API_CATCH(ctx)
 }
 
@@ -554,6 +591,7 @@ int nnk_mob_apply_fmm(nnk_mob* mob, nnk_fmm* fmm, const double* x, double* y, in
   double* dy = stage_out(M.io_out, y, n, on_device);
   M.apply_with(fmm->f.get(), dx, dy);
   finish_out(ctx, M.io_out, y, n, on_device);
+  device_errors(*fmm->f, !on_device);
   API_CATCH(ctx)
 }
 
@@ -570,6 +608,7 @@ int nnk_mob_solve_adjoint(nnk_mob* mob, const double* rhs, double* x, const nnk_
   nnk_solve_info inf{};
   M.solve_adjoint(db, dx, *sp, inf);
   finish_out(ctx, M.io_out, x, n, on_device);
+  device_errors(*mob->fmm->f, 1);
   if (info) *info = inf;
   if (inf.flag != 0) return fail(ctx, NNK_E_NOCONV, "gmres stopped at maxit above tol");
   API_CATCH(ctx)

@@ -186,6 +186,21 @@ void Fmm::set_profile(bool on) {
   if (sparse_) sparse_->set_profile(on);
 }
 
+void Fmm::check_errors() {
+  if (tensor_m2l_) check_m2l_error(m2l_, ctx_->stream);
+  if (sparse_) sparse_->check_errors();
+}
+
+void Fmm::poll_errors() {
+  if (tensor_m2l_) poll_m2l_error(m2l_, ctx_->stream);
+  if (sparse_) sparse_->poll_errors();
+}
+
+int Fmm::m2l_stall_probe(uint32_t polls) {
+  if (!tensor_m2l_) throw Error(NNK_E_STATE, "the failure-path probe needs the tensor-core M2L (mixed precision)");
+  return stall_m2l_probe(m2l_, polls, ctx_->stream);
+}
+
 void Fmm::read_profile(double* ms, int64_t* launches) {
   NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
   if (tensor_m2l_) check_m2l_error(m2l_, ctx_->stream);
@@ -602,10 +617,16 @@ __global__ void add_diag_kernel(double* G, int n, double v) {
 void Fmm::build_operators() {
   const HostTree& t = *t_;
   if (p_.m2l_mode < 0 || p_.m2l_mode > 4) throw Error(NNK_E_ARG, "m2l_mode must be 0..4");
-  if (p_.precision == NNK_PREC_MIXED && p_.m2l_mode == 4) {
+  // Fourier-space M2L: mode 4 in mixed precision (FP32 spectra); in FP64
+  // every mode but 3 (the FP64 pair kernel) when the transforms of one
+  // right-hand side fit shared memory (FP64 spectra)
+  const bool fp64 = p_.precision == NNK_PREC_FP64;
+  const int fft_cap = fft_m2l_max_rhs(p_.res, fp64);
+  if ((!fp64 && p_.m2l_mode == 4) || (fp64 && p_.m2l_mode != 3 && fft_cap >= 1)) {
     std::vector<int> node_op(N_);
     for (int32_t v = 0; v < N_; ++v) node_op[v] = op_of_[(size_t)t.group_of(v) * (maxl_ + 1) + t.level[v]];
-    build_fft_m2l(t, p_.res, p_.shells, p_.eps, p_.mu, op_w_, node_op, R_, fft_, ctx_->stream);
+    build_fft_m2l(t, p_.res, p_.shells, p_.eps, p_.mu, op_w_, node_op, std::min(R_, std::max(fft_cap, 1)), fp64,
+                  fft_, ctx_->stream);
     fft_m2l_ = true;
   }
   if (p_.precision == NNK_PREC_MIXED && p_.m2l_mode != 3 && p_.m2l_mode != 4) {
@@ -747,10 +768,9 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
   // when the relation is symmetric (it is for every tree of the reference)
   const bool fast = &ts == &fwd_ || v_symmetric_;
   const bool tm = fast && tensor_m2l_ && std::is_same<Real, float>::value;
-  const bool fm = fast && fft_m2l_ && std::is_same<Real, float>::value;
+  const bool fm = fast && fft_m2l_;
   if (tm && R != 1) throw Error(NNK_E_STATE, "tensor-core M2L takes one right-hand side per pass");
-  if (tm && m2l_.h_err && *m2l_.h_err)
-    throw Error(NNK_E_TIMEOUT, "tensor-core M2L gave up a bounded wait in an earlier call");
+  if (tm) poll_m2l_error(m2l_, st);  // a wait that gave up in an earlier call
   const int* na = &ts == &fwd_ ? nact() : nullptr;
   // upward pass
   for (int L = maxl_; L >= 1; --L) {
@@ -774,7 +794,7 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
   if (fm) {
     // M2L of every level at once in Fourier space
     NNK_CUDA(cudaMemsetAsync(check, 0, sizeof(Real) * (size_t)N_ * n * R, st));
-    phase(NNK_PHASE_M2L, [&] { launch_fft_m2l(fft_, (const float*)str, regionA, R, (float*)check, st, na); });
+    phase(NNK_PHASE_M2L, [&] { launch_fft_m2l(fft_, (const Real*)str, regionA, R, check, st, na); });
   }
   const std::vector<TaskGroup>& dgroups = (tm || fm) ? ts.down_nov : ts.down;
   for (int L = 1; L <= maxl_; ++L) {
@@ -895,7 +915,7 @@ void Fmm::apply(const double* d_in, double* d_out, int layout, int nrhs) {
 
 void Fmm::apply_mapped(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int nrhs) {
   if (t_->n_tgt == 0) return;
-  const int cap = tensor_m2l_ ? 1 : R_;
+  const int cap = rhs_cap(false);
   for (int k0 = 0; k0 < nrhs;) {
     const int R = rhs_chunk(nrhs - k0, cap);
     if (p_.precision == NNK_PREC_FP64)
@@ -918,7 +938,7 @@ void Fmm::apply_adjoint(const double* d_in, double* d_out, int layout, int nrhs)
 void Fmm::apply_adjoint_mapped(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int nrhs) {
   if (t_->n_pot == 0) return;
   build_adjoint();
-  const int cap = (tensor_m2l_ && v_symmetric_) ? 1 : R_;
+  const int cap = rhs_cap(true);
   for (int k0 = 0; k0 < nrhs;) {
     const int R = rhs_chunk(nrhs - k0, cap);
     if (p_.precision == NNK_PREC_FP64)
@@ -988,7 +1008,7 @@ double tune_groups(Fmm* self, std::vector<TaskGroup*>& groups, const std::vector
 std::pair<double, double> Fmm::autotune(int nrhs) {
   bump_version();
   const HostTree& t = *t_;
-  const int R = rhs_chunk(nrhs, tensor_m2l_ ? 1 : R_);
+  const int R = rhs_chunk(nrhs, rhs_cap(false));
   cudaStream_t st = ctx_->stream;
   // one pass with real data, so the tuned launches see the real sources
   DBuf<double> in(3 * (size_t)t.n_pot * R), out(3 * (size_t)t.n_tgt * R);
@@ -1023,6 +1043,16 @@ std::pair<double, double> Fmm::autotune(int nrhs) {
   // the tuned launches overwrote work buffers: nothing to keep
   NNK_CUDA(cudaStreamSynchronize(st));
   return res;
+}
+
+// Right-hand sides per pass: the work buffers hold R_; the tensor-core M2L
+// takes one and the Fourier M2L its plan's count (the adjoint uses them
+// only when V is symmetric).
+int Fmm::rhs_cap(bool adjoint) const {
+  const bool fast = !adjoint || v_symmetric_;
+  if (fast && tensor_m2l_) return 1;
+  if (fast && fft_m2l_) return std::min(R_, fft_.Rcap);
+  return R_;
 }
 
 int64_t Fmm::source_origins() const { return t_->params.nearest ? t_->q : t_->n_pot; }

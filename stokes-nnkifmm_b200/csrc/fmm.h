@@ -152,6 +152,15 @@ class Fmm {
   // preconditioner.
   void reduced_solve_inv(const double* d_in, double* d_out, int layout);
   nnk_fmm_stats stats() const { return stats_; }
+  // Device-side failures of earlier launches (a bounded wait of the
+  // tensor-core M2L that gave up): check_errors waits for the stream and
+  // throws NNK_E_TIMEOUT; poll_errors reads only flags whose copy to the host
+  // has completed, without waiting.  A reported flag is cleared.
+  void check_errors();
+  void poll_errors();
+  // Failure-path probe of the tensor-core M2L (see stall_m2l_probe); returns
+  // the error flag the probe launch set (nonzero when the wait gave up).
+  int m2l_stall_probe(uint32_t polls);
   // per-phase CUDA-event timing (NNK_PHASE_*)
   void set_profile(bool on);
   bool profiling() const { return prof_; }
@@ -173,6 +182,7 @@ class Fmm {
   template <typename Real>
   void grad_impl(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs);
   void build_adjoint();
+  int rhs_cap(bool adjoint) const;
   void build_taskset(TaskSet& ts, const TaskRoles& roles, bool stats);
   void build_points();
   void build_tasks();

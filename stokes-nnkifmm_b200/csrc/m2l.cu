@@ -56,9 +56,9 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait on an mbarrier phase; false after kWaitLimit polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+// Bounded wait on an mbarrier phase; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kWaitLimit) {
+  for (uint32_t i = 0; i < limit; ++i) {
     if (mbar_test(bar, parity)) return true;
     if (i > 32) __nanosleep(20);
   }
@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
                    const int* __restrict__ tile_slot0, const int* __restrict__ slot_op,
                    const int* __restrict__ slot_src, const float* __restrict__ images,
                    const float* __restrict__ src, const float* __restrict__ src_lo, float* __restrict__ out,
-                   int ldc, int NP, int* err, int ns) {
+                   int ldc, int NP, int* err, int ns, uint32_t wlim, int probe) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* sbase = smem_raw + (((raw + 1023u) & ~1023u) - raw);
@@ -463,6 +463,7 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
   uint64_t* accb = bars + 2 * ns;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * ns + 1);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  uint64_t* probe_bar = bars + 2 * ns + 2;  // failure-path test only: nothing arrives here
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const M2LUnit u = units[blockIdx.x];
@@ -474,6 +475,7 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
       mbar_init(&done[k], 1);
     }
     mbar_init(accb, 1);
+    mbar_init(probe_bar, 1);
     *abort_s = 0;
     fence_barrier_init();
   }
@@ -482,6 +484,15 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  if (probe) {
+    // every thread waits on a barrier that no thread or copy completes; the
+    // bounded wait gives up before any copy or MMA is issued
+    if (!mbar_wait(probe_bar, 0, wlim)) {
+      *abort_s = 1;
+      if (tid == 0) atomicOr(err, 32);
+    }
+    __syncthreads();
+  }
   const int slot_base = tile_slot0[u.tile] + u.slot0;
   const int nsteps = u.nslot * nchunks;
   int issued = 0, copies = 0;  // lane 0 of warp 0
@@ -495,10 +506,10 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
         bulk_g2s(sB0 + st * B_BYTES, gB, B_BYTES, &full[st]);
         ++copies;
       };
-      for (int s = 0; s < ns && s < nsteps; ++s) copy(s);
+      for (int s = 0; s < ns && s < nsteps && !*abort_s; ++s) copy(s);
       for (int s = 0; s < nsteps && !*abort_s; ++s) {
         const int st = s % ns;
-        if (!mbar_wait(&full[st], (s / ns) & 1)) {
+        if (!mbar_wait(&full[st], (s / ns) & 1, wlim)) {
           *abort_s = 1;
           atomicOr(err, 2);
           break;
@@ -516,7 +527,7 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
         // refill the stage of step s-1 with step s-1+ns once its MMAs are done
         const int prev = s - 1, nxt = s - 1 + ns;
         if (prev >= 0 && nxt < nsteps) {
-          if (!mbar_wait(&done[prev % ns], (prev / ns) & 1)) {
+          if (!mbar_wait(&done[prev % ns], (prev / ns) & 1, wlim)) {
             *abort_s = 1;
             atomicOr(err, 1);
             break;
@@ -533,7 +544,7 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
     const float* __restrict__ term = q ? src_lo : src;
     for (int s = 0; s < nsteps && !*abort_s; ++s) {
       const int st = s % ns, use = s / ns;
-      if (use >= 1 && !mbar_wait(&done[st], (use - 1) & 1)) {
+      if (use >= 1 && !mbar_wait(&done[st], (use - 1) & 1, wlim)) {
         *abort_s = 1;
         atomicOr(err, 16);
         break;
@@ -560,12 +571,12 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
   // every role waits for the accumulator (committed after the last MMA); the
   // read-back below is warp-collective, so a warp reads only if all its lanes
   // saw the accumulator complete
-  const bool acc_ok = __all_sync(0xffffffffu, mbar_wait(accb, 0));
+  const bool acc_ok = __all_sync(0xffffffffu, mbar_wait(accb, 0, wlim));
   if (!acc_ok && lane == 0) atomicOr(err, 4);
   // operator copies issued for steps whose MMAs never ran land before exit
   if (tid == 0)
     for (int s = issued; s < copies; ++s)
-      if (!mbar_wait(&full[s % ns], (s / ns) & 1)) atomicOr(err, 8);
+      if (!mbar_wait(&full[s % ns], (s / ns) & 1, wlim)) atomicOr(err, 8);
   tc_fence_after();
   if (warp >= 1 && warp <= 4 && !*abort_s && acc_ok && nsteps > 0) {
     const int q4 = warp & 3;  // TMEM lane quarter of this warp
@@ -845,6 +856,7 @@ struct Compressor {
 
 M2LPlan::~M2LPlan() {
   if (h_err) cudaFreeHost(h_err);
+  if (err_ev) cudaEventDestroy(err_ev);
 }
 
 void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double mu, M2LPlan& plan,
@@ -1052,6 +1064,7 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
   plan.err.zero(st);
   if (!plan.h_err) NNK_CUDA(cudaMallocHost((void**)&plan.h_err, sizeof(int)));
   *plan.h_err = 0;
+  if (!plan.err_ev) NNK_CUDA(cudaEventCreateWithFlags(&plan.err_ev, cudaEventDisableTiming));
   // image kernel: 3 stages where they fit (the compressed form's 64 KB stages), else 2
   const size_t na = plan.compressed ? 2 : 1;
   auto img_smem = [&](size_t ns) { return 1024 + ns * (na * kTileRows * 128 + (size_t)NP * 128) + 128; };
@@ -1067,6 +1080,15 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
   plan.ready = true;
 }
 
+namespace {
+// Copies the error flag to its pinned host mirror after a launch and marks
+// the copy with the plan's event.
+void mirror_err(M2LPlan& plan, cudaStream_t st) {
+  NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  NNK_CUDA(cudaEventRecord(plan.err_ev, st));
+}
+}  // namespace
+
 void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st, const float* up, long long ld_up) {
   if (!plan.nunits) return;
   if (plan.compressed) {
@@ -1078,9 +1100,9 @@ void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st, const flo
     NNK_CUDA(cudaMemsetAsync(plan.chat.p, 0, plan.chat.bytes(), st));
     m2l_ws_kernel<<<plan.nunits, 32 * (1 + kWsGatherWarps), plan.smem_bytes, st>>>(
         plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p, plan.slot_op.p, plan.slot_src.p, plan.images.p,
-        plan.src.p, plan.src_lo.p, plan.chat.p, RC, RC, plan.err.p, plan.stages);
+        plan.src.p, plan.src_lo.p, plan.chat.p, RC, RC, plan.err.p, plan.stages, plan.wait_limit, 0);
     NNK_CHECK_LAUNCH();
-    NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    mirror_err(plan, st);
     basis_apply_kernel<<<dim3((plan.n3 + 63) / 64, plan.nbtiles), 256, 0, st>>>(
         plan.basis.p, plan.n3, RC, 0, plan.btiles.p, plan.bnodes.p, plan.chat.p, RC, check, ldc);
     NNK_CHECK_LAUNCH();
@@ -1092,21 +1114,58 @@ void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st, const flo
                                                               plan.src.p, check, ldc, plan.NP, plan.err.p, nullptr,
                                                               plan.stages);
     NNK_CHECK_LAUNCH();
-    NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    mirror_err(plan, st);
     return;
   }
   m2l_gen_kernel<<<plan.nunits, 128, plan.smem_bytes, st>>>(
       plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p, plan.slot_code.p, plan.slot_h.p, plan.slot_src.p,
       plan.lat.p, plan.P, plan.res, plan.e2, plan.scale, plan.src.p, check, ldc, plan.NP, plan.err.p);
   NNK_CHECK_LAUNCH();
-  NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  mirror_err(plan, st);
 }
+
+namespace {
+// Reads the mirrored flag once its copy has completed; clears a set flag
+// (device and host) and returns it.
+int take_err(M2LPlan& plan, cudaStream_t st) {
+  if (!plan.h_err || !plan.err_ev) return 0;
+  const cudaError_t q = cudaEventQuery(plan.err_ev);
+  if (q == cudaErrorNotReady) return 0;
+  NNK_CUDA(q);
+  const int f = *plan.h_err;
+  if (f) {
+    *plan.h_err = 0;
+    NNK_CUDA(cudaMemsetAsync(plan.err.p, 0, sizeof(int), st));
+  }
+  return f;
+}
+}  // namespace
 
 void check_m2l_error(M2LPlan& plan, cudaStream_t st) {
   if (!plan.h_err) return;
   NNK_CUDA(cudaStreamSynchronize(st));
-  if (*plan.h_err) throw Error(NNK_E_TIMEOUT, "tensor-core M2L gave up a bounded wait (flag " +
-                                                  std::to_string(*plan.h_err) + ")");
+  poll_m2l_error(plan, st);
+}
+
+void poll_m2l_error(M2LPlan& plan, cudaStream_t st) {
+  const int f = take_err(plan, st);
+  if (f) throw Error(NNK_E_TIMEOUT, "tensor-core M2L gave up a bounded wait (flag " + std::to_string(f) + ")");
+}
+
+int stall_m2l_probe(M2LPlan& plan, uint32_t polls, cudaStream_t st) {
+  if (!plan.compressed || !plan.nunits)
+    throw Error(NNK_E_STATE, "the failure-path probe needs the compressed tensor-core M2L with V pairs");
+  if (polls == 0) throw Error(NNK_E_ARG, "the probe needs a positive wait limit");
+  check_m2l_error(plan, st);  // an earlier flag is not the probe's
+  m2l_ws_kernel<<<plan.nunits, 32 * (1 + kWsGatherWarps), plan.smem_bytes, st>>>(
+      plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p, plan.slot_op.p, plan.slot_src.p, plan.images.p,
+      plan.src.p, plan.src_lo.p, plan.chat.p, plan.RC, plan.RC, plan.err.p, plan.stages, polls, 1);
+  NNK_CHECK_LAUNCH();
+  mirror_err(plan, st);
+  NNK_CUDA(cudaStreamSynchronize(st));
+  const int f = take_err(plan, st);
+  NNK_CUDA(cudaStreamSynchronize(st));
+  return f;
 }
 
 }  // namespace nnk

@@ -87,6 +87,8 @@ struct M2LPlan {
   DBuf<float> src_lo;           // nodes * RC: second TF32 term of B^T u
   DBuf<int> err;                // bounded-wait timeout flag
   int* h_err = nullptr;         // pinned mirror of err
+  cudaEvent_t err_ev = nullptr; // recorded after each copy of err into h_err
+  uint32_t wait_limit = 1u << 26;  // polls per bounded mbarrier wait (~1-3 s)
   size_t smem_bytes = 0;
   int stages = 2;               // image kernel pipeline depth
   bool ready = false;
@@ -101,7 +103,18 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
 // (k < 3P); the uncompressed one reads plan.src, filled by the up C2E.
 void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st, const float* up = nullptr,
                 long long ld_up = 0);
-// Throws NNK_E_TIMEOUT if an earlier M2L launch gave up a bounded wait.
+// Waits for the stream, then throws NNK_E_TIMEOUT if an M2L launch gave up a
+// bounded wait.  The flag is cleared when it is reported, so the next call
+// on the same plan runs normally.
 void check_m2l_error(M2LPlan& plan, cudaStream_t st);
+// The same without waiting: reads the flag only if the copy that mirrors it
+// to the host has completed (a flag still in flight is seen by a later poll).
+void poll_m2l_error(M2LPlan& plan, cudaStream_t st);
+// Failure-path test of the compressed tensor-core kernel: one launch whose
+// threads first wait, `polls` times at most, on an mbarrier that nothing
+// arrives at.  The wait gives up, the kernel sets the error flag, issues no
+// copy or MMA, frees its tensor memory and returns; the host reads the flag.
+// Returns the flag (nonzero: the timeout was seen), cleared afterwards.
+int stall_m2l_probe(M2LPlan& plan, uint32_t polls, cudaStream_t st);
 
 }  // namespace nnk

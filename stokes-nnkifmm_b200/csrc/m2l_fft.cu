@@ -17,20 +17,30 @@ namespace nnk {
 
 namespace {
 
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
+template <typename Real> struct Cplx;
+template <> struct Cplx<float> { using t = float2; };
+template <> struct Cplx<double> { using t = double2; };
+
+__device__ __forceinline__ float2 cmake(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 cmake(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ void cmac(float2& acc, float2 a, float2 b) {
   acc.x = fmaf(a.x, b.x, fmaf(-a.y, b.y, acc.x));
   acc.y = fmaf(a.x, b.y, fmaf(a.y, b.x, acc.y));
 }
+__device__ __forceinline__ void cmac(double2& acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, fma(-a.y, b.y, acc.x));
+  acc.y = fma(a.x, b.y, fma(a.y, b.x, acc.y));
+}
 
 // e^{sign * 2 pi i m / G}, m in [0, G)
-__device__ __forceinline__ void twiddles(float2* tw, int G, double sign) {
+template <typename Real>
+__device__ __forceinline__ void twiddles(typename Cplx<Real>::t* tw, int G, double sign) {
   for (int m = threadIdx.x; m < G; m += blockDim.x) {
     double s, c;
     sincospi(2.0 * m / G, &s, &c);
-    tw[m] = make_float2((float)c, (float)(sign * s));
+    tw[m] = cmake((Real)c, (Real)(sign * s));
   }
 }
 
@@ -39,9 +49,10 @@ __device__ __forceinline__ void twiddles(float2* tw, int G, double sign) {
 // FP64, one component at a time:
 //   Kgrid[d] = K((d - (res - 1) o) h) / (8 pi mu G^3) for |d|_inf <= res - 1
 // (d the signed index of the grid point, 0 elsewhere), then three DFT passes.
+template <typename Real>
 __global__ void fft_spectra_kernel(int G, int res, const double* __restrict__ slot_w,
                                    const int* __restrict__ slot_code, double e2, double scale,
-                                   float2* __restrict__ spec, int NK) {
+                                   typename Cplx<Real>::t* __restrict__ spec, int NK) {
   extern __shared__ double sm[];
   const int H = G / 2 + 1;
   double* K = sm;                         // [x][y][z]
@@ -110,7 +121,7 @@ __global__ void fft_spectra_kernel(int G, int res, const double* __restrict__ sl
         re += b.x * c - b.y * sn;
         im += b.x * sn + b.y * c;
       }
-      spec[((size_t)s * 6 + comp) * NK + e] = make_float2((float)re, (float)im);
+      spec[((size_t)s * 6 + comp) * NK + e] = cmake((Real)re, (Real)im);
     }
     __syncthreads();
   }
@@ -121,25 +132,28 @@ __global__ void fft_spectra_kernel(int G, int res, const double* __restrict__ sl
 // (interior zero), transformed along z (res -> H), y (res -> G), x (res -> G).
 // RES > 0: the lattice size at compile time (loops unrolled, per-thread
 // arrays in registers); RES = 0 takes it from `res_rt`.
-template <int RES>
+template <int RES, typename Real>
 __global__ void fft_forward_kernel(int G_rt, int res_rt, int P, const int* __restrict__ lat,
-                                   const int* __restrict__ src_node, const float* __restrict__ str, long long upbase,
-                                   int R, float2* __restrict__ qhat, int NK, const int* __restrict__ nact) {
-  extern __shared__ float2 smq[];
+                                   const int* __restrict__ src_node, const Real* __restrict__ str, long long upbase,
+                                   int R, typename Cplx<Real>::t* __restrict__ qhat, int NK,
+                                   const int* __restrict__ nact) {
+  using T2 = typename Cplx<Real>::t;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  T2* smq = reinterpret_cast<T2*>(fft_smem);
   const int res = RES > 0 ? RES : res_rt;
   const int G = RES > 0 ? 2 * RES : G_rt;
   const int H = G / 2 + 1, C = 3 * R, r3 = res * res * res;
-  float2* tw = smq;                          // G
-  float2* Z = tw + G;                        // [cr][x][y][kz]   C res res H
-  float2* Y = Z + C * res * res * H;         // [cr][x][ky][kz]  C res G H
-  float* g = reinterpret_cast<float*>(Y + C * res * G * H);  // [cr][x][y][z] C res^3
+  T2* tw = smq;                          // G
+  T2* Z = tw + G;                        // [cr][x][y][kz]   C res res H
+  T2* Y = Z + C * res * res * H;         // [cr][x][ky][kz]  C res G H
+  Real* g = reinterpret_cast<Real*>(Y + C * res * G * H);  // [cr][x][y][z] C res^3
   const int node = src_node[blockIdx.x];
   if (nact && !nact[node]) return;  // a masked tree of the forest
   const int tid = threadIdx.x, nt = blockDim.x;
-  twiddles(tw, G, -1.0);
-  for (int e = tid; e < C * r3; e += nt) g[e] = 0.f;
+  twiddles<Real>(tw, G, -1.0);
+  for (int e = tid; e < C * r3; e += nt) g[e] = 0;
   __syncthreads();
-  const float* src = str + (upbase + (long long)P * node) * C;
+  const Real* src = str + (upbase + (long long)P * node) * C;
   for (int e = tid; e < P * C; e += nt) {
     const int p = e / C, cr = e - p * C;
     const int l = lat[p];
@@ -147,15 +161,15 @@ __global__ void fft_forward_kernel(int G_rt, int res_rt, int P, const int* __res
   }
   __syncthreads();
   for (int e = tid; e < C * res * res; e += nt) {  // z: one (cr, x, y) per thread
-    const float* gz = g + e * res;
+    const Real* gz = g + e * res;
 #pragma unroll
     for (int kz = 0; kz < H; ++kz) {
-      float2 a = make_float2(0.f, 0.f);
+      T2 a = cmake((Real)0, (Real)0);
 #pragma unroll
       for (int z = 0; z < res; ++z) {
-        const float2 w = tw[(kz * z) % G];
-        a.x = fmaf(gz[z], w.x, a.x);
-        a.y = fmaf(gz[z], w.y, a.y);
+        const T2 w = tw[(kz * z) % G];
+        a.x = rfma(gz[z], w.x, a.x);
+        a.y = rfma(gz[z], w.y, a.y);
       }
       Z[e * H + kz] = a;
     }
@@ -163,13 +177,13 @@ __global__ void fft_forward_kernel(int G_rt, int res_rt, int P, const int* __res
   __syncthreads();
   for (int e = tid; e < C * res * H; e += nt) {  // y: one (cr, x, kz) per thread
     const int crx = e / H, kz = e % H;
-    float2 in[8];
+    T2 in[8];
 #pragma unroll
     for (int y = 0; y < (RES > 0 ? RES : 8); ++y)
       if (y < res) in[y] = Z[(crx * res + y) * H + kz];
 #pragma unroll
     for (int ky = 0; ky < G; ++ky) {
-      float2 a = make_float2(0.f, 0.f);
+      T2 a = cmake((Real)0, (Real)0);
 #pragma unroll
       for (int y = 0; y < (RES > 0 ? RES : 8); ++y)
         if (y < res) cmac(a, in[y], tw[(ky * y) % G]);
@@ -177,16 +191,16 @@ __global__ void fft_forward_kernel(int G_rt, int res_rt, int P, const int* __res
     }
   }
   __syncthreads();
-  float2* out = qhat + (size_t)blockIdx.x * C * NK;
+  T2* out = qhat + (size_t)blockIdx.x * C * NK;
   for (int e = tid; e < C * G * H; e += nt) {  // x: one (cr, ky, kz) per thread
     const int cr = e / (G * H), kyz = e % (G * H);
-    float2 in[8];
+    T2 in[8];
 #pragma unroll
     for (int x = 0; x < (RES > 0 ? RES : 8); ++x)
       if (x < res) in[x] = Y[(cr * res + x) * G * H + kyz];
 #pragma unroll
     for (int kx = 0; kx < G; ++kx) {
-      float2 a = make_float2(0.f, 0.f);
+      T2 a = cmake((Real)0, (Real)0);
 #pragma unroll
       for (int x = 0; x < (RES > 0 ? RES : 8); ++x)
         if (x < res) cmac(a, in[x], tw[(kx * x) % G]);
@@ -199,32 +213,32 @@ __global__ void fft_forward_kernel(int G_rt, int res_rt, int P, const int* __res
 // C_i(k) = sum_{v in V(i)} Khat_{w,o}(k) Q_v(k): one target and frequency per
 // thread; blocks run frequency-block-major so that the spectra in use at a
 // time are a slice that stays in L2.
-template <int R>
+template <int R, typename Real>
 __global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* __restrict__ voff,
                                                              const int* __restrict__ vsrc,
                                                              const int* __restrict__ vspec,
-                                                             const float2* __restrict__ spec,
-                                                             const float2* __restrict__ qhat,
-                                                             float2* __restrict__ chat,
+                                                             const typename Cplx<Real>::t* __restrict__ spec,
+                                                             const typename Cplx<Real>::t* __restrict__ qhat,
+                                                             typename Cplx<Real>::t* __restrict__ chat,
                                                              const int* __restrict__ tgt_node,
                                                              const int* __restrict__ nact) {
+  using T2 = typename Cplx<Real>::t;
   constexpr int C = 3 * R;
   const int t = blockIdx.x;
   const int k = blockIdx.y * blockDim.x + threadIdx.x;
   if (k >= NK) return;
   if (nact && !nact[tgt_node[t]]) return;
-  float2 acc[C];
+  T2 acc[C];
 #pragma unroll
-  for (int c = 0; c < C; ++c) acc[c] = make_float2(0.f, 0.f);
+  for (int c = 0; c < C; ++c) acc[c] = cmake((Real)0, (Real)0);
   const int e1 = voff[t + 1];
   for (int e = voff[t]; e < e1; ++e) {
-    const float2* Kp = spec + (size_t)vspec[e] * 6 * NK + k;
-    const float2 kxx = Kp[0], kxy = Kp[NK], kxz = Kp[2 * NK], kyy = Kp[3 * NK], kyz = Kp[4 * NK],
-                 kzz = Kp[5 * NK];
-    const float2* Q = qhat + (size_t)vsrc[e] * C * NK + k;
+    const T2* Kp = spec + (size_t)vspec[e] * 6 * NK + k;
+    const T2 kxx = Kp[0], kxy = Kp[NK], kxz = Kp[2 * NK], kyy = Kp[3 * NK], kyz = Kp[4 * NK], kzz = Kp[5 * NK];
+    const T2* Q = qhat + (size_t)vsrc[e] * C * NK + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const float2 qx = Q[(3 * r) * NK], qy = Q[(3 * r + 1) * NK], qz = Q[(3 * r + 2) * NK];
+      const T2 qx = Q[(3 * r) * NK], qy = Q[(3 * r + 1) * NK], qz = Q[(3 * r + 2) * NK];
       cmac(acc[3 * r], kxx, qx);
       cmac(acc[3 * r], kxy, qy);
       cmac(acc[3 * r], kxz, qz);
@@ -236,7 +250,7 @@ __global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* 
       cmac(acc[3 * r + 2], kzz, qz);
     }
   }
-  float2* out = chat + (size_t)t * C * NK + k;
+  T2* out = chat + (size_t)t * C * NK + k;
 #pragma unroll
   for (int c = 0; c < C; ++c) out[(size_t)c * NK] = acc[c];
 }
@@ -244,32 +258,34 @@ __global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* 
 // ---------------------------------------------------------------- inverse
 // check of one target node at its shell lattice points from C_i: inverse
 // passes along x (G -> res), y (G -> res) and z (half spectrum -> res, real).
-template <int RES>
+template <int RES, typename Real>
 __global__ void fft_inverse_kernel(int G_rt, int res_rt, int P, const int* __restrict__ lat,
-                                   const int* __restrict__ tgt_node, const float2* __restrict__ chat, int R,
-                                   float* __restrict__ check, int NK, const int* __restrict__ nact) {
-  extern __shared__ float2 smc[];
+                                   const int* __restrict__ tgt_node, const typename Cplx<Real>::t* __restrict__ chat,
+                                   int R, Real* __restrict__ check, int NK, const int* __restrict__ nact) {
+  using T2 = typename Cplx<Real>::t;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  T2* smc = reinterpret_cast<T2*>(fft_smem);
   const int res = RES > 0 ? RES : res_rt;
   const int G = RES > 0 ? 2 * RES : G_rt;
   const int H = G / 2 + 1, C = 3 * R, r3 = res * res * res;
-  float2* tw = smc;                   // G
-  float2* X = tw + G;                 // [cr][x][ky][kz]  C res G H
-  float2* Yv = X + C * res * G * H;   // [cr][x][y][kz]   C res res H
-  float* out = reinterpret_cast<float*>(X);  // [cr][x][y][z] (X is dead by then)
+  T2* tw = smc;                   // G
+  T2* X = tw + G;                 // [cr][x][ky][kz]  C res G H
+  T2* Yv = X + C * res * G * H;   // [cr][x][y][kz]   C res res H
+  Real* out = reinterpret_cast<Real*>(X);  // [cr][x][y][z] (X is dead by then)
   const int node = tgt_node[blockIdx.x];
   if (nact && !nact[node]) return;
   const int tid = threadIdx.x, nt = blockDim.x;
-  twiddles(tw, G, 1.0);
+  twiddles<Real>(tw, G, 1.0);
   __syncthreads();
-  const float2* ci = chat + (size_t)blockIdx.x * C * NK;
+  const T2* ci = chat + (size_t)blockIdx.x * C * NK;
   for (int e = tid; e < C * G * H; e += nt) {  // x: one (cr, ky, kz) per thread
     const int cr = e / (G * H), kyz = e % (G * H);
-    float2 a[8];
+    T2 a[8];
 #pragma unroll
-    for (int x = 0; x < 8; ++x) a[x] = make_float2(0.f, 0.f);
+    for (int x = 0; x < 8; ++x) a[x] = cmake((Real)0, (Real)0);
 #pragma unroll
     for (int kx = 0; kx < G; ++kx) {
-      const float2 v = ci[(size_t)cr * NK + kx * G * H + kyz];
+      const T2 v = ci[(size_t)cr * NK + kx * G * H + kyz];
 #pragma unroll
       for (int x = 0; x < (RES > 0 ? RES : 8); ++x)
         if (x < res) cmac(a[x], v, tw[(kx * x) % G]);
@@ -281,12 +297,12 @@ __global__ void fft_inverse_kernel(int G_rt, int res_rt, int P, const int* __res
   __syncthreads();
   for (int e = tid; e < C * res * H; e += nt) {  // y: one (cr, x, kz) per thread
     const int crx = e / H, kz = e % H;
-    float2 a[8];
+    T2 a[8];
 #pragma unroll
-    for (int y = 0; y < 8; ++y) a[y] = make_float2(0.f, 0.f);
+    for (int y = 0; y < 8; ++y) a[y] = cmake((Real)0, (Real)0);
 #pragma unroll
     for (int ky = 0; ky < G; ++ky) {
-      const float2 v = X[(crx * G + ky) * H + kz];
+      const T2 v = X[(crx * G + ky) * H + kz];
 #pragma unroll
       for (int y = 0; y < (RES > 0 ? RES : 8); ++y)
         if (y < res) cmac(a[y], v, tw[(ky * y) % G]);
@@ -297,23 +313,23 @@ __global__ void fft_inverse_kernel(int G_rt, int res_rt, int P, const int* __res
   }
   __syncthreads();
   for (int e = tid; e < C * res * res; e += nt) {  // z: one (cr, x, y) per thread, real output
-    const float2* yz = Yv + e * H;
+    const T2* yz = Yv + e * H;
 #pragma unroll
     for (int z = 0; z < (RES > 0 ? RES : 8); ++z) {
       if (z >= res) break;
-      float v = 0.f;
+      Real v = 0;
 #pragma unroll
       for (int kz = 0; kz < (RES > 0 ? RES + 1 : 9); ++kz) {
         if (kz >= H) break;
-        const float w = (kz == 0 || 2 * kz == G) ? 1.f : 2.f;
-        const float2 t = tw[(kz * z) % G];
-        v = fmaf(w, yz[kz].x * t.x - yz[kz].y * t.y, v);
+        const Real w = (kz == 0 || 2 * kz == G) ? (Real)1 : (Real)2;
+        const T2 t = tw[(kz * z) % G];
+        v = rfma(w, yz[kz].x * t.x - yz[kz].y * t.y, v);
       }
       out[e * res + z] = v;
     }
   }
   __syncthreads();
-  float* dst = check + (long long)P * node * C;
+  Real* dst = check + (long long)P * node * C;
   for (int e = tid; e < P * C; e += nt) {
     const int p = e / C, cr = e - p * C;
     const int l = lat[p];
@@ -321,21 +337,86 @@ __global__ void fft_inverse_kernel(int G_rt, int res_rt, int P, const int* __res
   }
 }
 
-size_t forward_smem(int G, int res, int R) {
+// es: bytes of one real number (a complex one takes 2 es)
+size_t forward_smem(int G, int res, int R, size_t es) {
   const int H = G / 2 + 1, C = 3 * R;
-  return sizeof(float2) * (G + (size_t)C * res * res * H + (size_t)C * res * G * H) +
-         sizeof(float) * (size_t)C * res * res * res;
+  return 2 * es * (G + (size_t)C * res * res * H + (size_t)C * res * G * H) + es * (size_t)C * res * res * res;
 }
-size_t inverse_smem(int G, int res, int R) {
+size_t inverse_smem(int G, int res, int R, size_t es) {
   const int H = G / 2 + 1, C = 3 * R;
-  return sizeof(float2) * (G + (size_t)C * res * G * H + (size_t)C * res * res * H);
+  return 2 * es * (G + (size_t)C * res * G * H + (size_t)C * res * res * H);
+}
+
+int optin_smem() {
+  int dev = 0, optin = 0;
+  NNK_CUDA(cudaGetDevice(&dev));
+  NNK_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  return optin;
+}
+
+template <typename Real>
+void set_smem_attributes(int optin) {
+  // The limit is an attribute of the kernel, shared by every plan of the
+  // process (a p = 4 plan built after a p = 6 one must not lower it): set
+  // the device's opt-in maximum.
+  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<0, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<0, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<4, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<4, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<6, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<6, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+}
+
+template <typename Real>
+void run_fft_m2l(FftM2L& f, const Real* str, long long upbase, int R, Real* check, cudaStream_t st,
+                 const int* nact, typename Cplx<Real>::t* spec, typename Cplx<Real>::t* qhat,
+                 typename Cplx<Real>::t* chat) {
+  if (f.ntgt == 0) return;
+  if (R > f.Rcap) throw Error(NNK_E_STATE, "Fourier M2L sized for fewer right-hand sides");
+  const int G = f.G, res = f.res;
+  const size_t es = sizeof(Real);
+  auto fwd = res == 6 ? fft_forward_kernel<6, Real> : res == 4 ? fft_forward_kernel<4, Real>
+                                                                : fft_forward_kernel<0, Real>;
+  auto inv = res == 6 ? fft_inverse_kernel<6, Real> : res == 4 ? fft_inverse_kernel<4, Real>
+                                                                : fft_inverse_kernel<0, Real>;
+  fwd<<<f.nsrc, 256, forward_smem(G, res, R, es), st>>>(G, res, f.P, f.lat.p, f.src_node.p, str, upbase, R, qhat,
+                                                        f.NK, nact);
+  NNK_CHECK_LAUNCH();
+  dim3 grid(f.ntgt, (f.NK + 127) / 128);
+#define NNK_FFT_ACC(RR)                                                                                       \
+  fft_accumulate_kernel<RR, Real><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, spec, qhat, chat, \
+                                                        f.tgt_node.p, nact)
+  switch (R) {
+    case 1: NNK_FFT_ACC(1); break;
+    case 2: NNK_FFT_ACC(2); break;
+    case 3: NNK_FFT_ACC(3); break;
+    case 4: NNK_FFT_ACC(4); break;
+    case 6: NNK_FFT_ACC(6); break;
+    default:
+      throw Error(NNK_E_ARG, "Fourier M2L supports 1, 2, 3, 4 or 6 right-hand sides per pass");
+  }
+#undef NNK_FFT_ACC
+  NNK_CHECK_LAUNCH();
+  inv<<<f.ntgt, 256, inverse_smem(G, res, R, es), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, chat, R, check, f.NK,
+                                                        nact);
+  NNK_CHECK_LAUNCH();
 }
 
 }  // namespace
 
+int fft_m2l_max_rhs(int res, bool fp64) {
+  const int optin = optin_smem();
+  const size_t es = fp64 ? sizeof(double) : sizeof(float);
+  for (int R : {6, 4, 3, 2, 1})
+    if (forward_smem(2 * res, res, R, es) <= (size_t)optin && inverse_smem(2 * res, res, R, es) <= (size_t)optin)
+      return R;
+  return 0;
+}
+
 void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu, const std::vector<double>& op_w,
-                   const std::vector<int>& node_op, int Rmax, FftM2L& f, cudaStream_t st) {
+                   const std::vector<int>& node_op, int Rmax, bool fp64, FftM2L& f, cudaStream_t st) {
   if (res > 8) throw Error(NNK_E_ARG, "Fourier M2L supports coronaRes up to 8");
+  f.fp64 = fp64;
   f.res = res;
   f.G = 2 * res;
   const int G = f.G, H = G / 2 + 1;
@@ -404,79 +485,58 @@ void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu
   f.voff.upload(voff, st);
   f.vsrc.upload(vsrc, st);
   f.vspec.upload(vspec, st);
-  f.spec.alloc(std::max<size_t>(1, (size_t)f.nspec * 6 * f.NK));
-  f.qhat.alloc(std::max<size_t>(1, (size_t)f.nsrc * 3 * Rmax * f.NK));
-  f.chat.alloc(std::max<size_t>(1, (size_t)f.ntgt * 3 * Rmax * f.NK));
+  const size_t nspec = std::max<size_t>(1, (size_t)f.nspec * 6 * f.NK);
+  const size_t nq = std::max<size_t>(1, (size_t)f.nsrc * 3 * Rmax * f.NK);
+  const size_t nc = std::max<size_t>(1, (size_t)f.ntgt * 3 * Rmax * f.NK);
+  if (fp64) {
+    f.spec64.alloc(nspec);
+    f.qhat64.alloc(nq);
+    f.chat64.alloc(nc);
+  } else {
+    f.spec.alloc(nspec);
+    f.qhat.alloc(nq);
+    f.chat.alloc(nc);
+  }
   if (f.nspec) {
     DBuf<double> dw;
     DBuf<int> dc;
     dw.upload(slot_w, st);
     dc.upload(slot_code, st);
     const size_t sm = sizeof(double) * (size_t)G * G * G + 2 * sizeof(double2) * (size_t)G * G * H;
-    NNK_CUDA(cudaFuncSetAttribute(fft_spectra_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    fft_spectra_kernel<<<f.nspec, 256, sm, st>>>(G, res, dw.p, dc.p, eps * eps,
-                                                  1.0 / (8.0 * M_PI * mu * (double)G * G * G), f.spec.p, f.NK);
+    const double scale = 1.0 / (8.0 * M_PI * mu * (double)G * G * G);
+    if (fp64) {
+      NNK_CUDA(cudaFuncSetAttribute(fft_spectra_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sm));
+      fft_spectra_kernel<double><<<f.nspec, 256, sm, st>>>(G, res, dw.p, dc.p, eps * eps, scale, f.spec64.p, f.NK);
+    } else {
+      NNK_CUDA(cudaFuncSetAttribute(fft_spectra_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sm));
+      fft_spectra_kernel<float><<<f.nspec, 256, sm, st>>>(G, res, dw.p, dc.p, eps * eps, scale, f.spec.p, f.NK);
+    }
     NNK_CHECK_LAUNCH();
     NNK_CUDA(cudaStreamSynchronize(st));
   }
-  f.fwd_smem = forward_smem(G, res, Rmax);
-  f.inv_smem = inverse_smem(G, res, Rmax);
-  int dev = 0, optin = 0;
-  NNK_CUDA(cudaGetDevice(&dev));
-  NNK_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const size_t es = fp64 ? sizeof(double) : sizeof(float);
+  f.fwd_smem = forward_smem(G, res, Rmax, es);
+  f.inv_smem = inverse_smem(G, res, Rmax, es);
+  const int optin = optin_smem();
   if (f.fwd_smem > (size_t)optin || f.inv_smem > (size_t)optin)
     throw Error(NNK_E_ARG, "Fourier M2L: too many right-hand sides per pass for shared memory");
-  // The limit is an attribute of the kernel, shared by every plan of the
-  // process (a p = 4 plan built after a p = 6 one must not lower it): set
-  // the device's opt-in maximum.
-  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-  NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-  NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  if (fp64) set_smem_attributes<double>(optin);
+  else set_smem_attributes<float>(optin);
   NNK_CUDA(cudaStreamSynchronize(st));
 }
 
 void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float* check, cudaStream_t st,
                     const int* nact) {
-  if (f.ntgt == 0) return;
-  if (R > f.Rcap) throw Error(NNK_E_STATE, "Fourier M2L sized for fewer right-hand sides");
-  const int G = f.G, res = f.res;
-  auto fwd = res == 6 ? fft_forward_kernel<6> : res == 4 ? fft_forward_kernel<4> : fft_forward_kernel<0>;
-  auto inv = res == 6 ? fft_inverse_kernel<6> : res == 4 ? fft_inverse_kernel<4> : fft_inverse_kernel<0>;
-  fwd<<<f.nsrc, 256, forward_smem(G, res, R), st>>>(G, res, f.P, f.lat.p, f.src_node.p, str, upbase, R, f.qhat.p,
-                                                    f.NK, nact);
-  NNK_CHECK_LAUNCH();
-  dim3 grid(f.ntgt, (f.NK + 127) / 128);
-  switch (R) {
-    case 1:
-      fft_accumulate_kernel<1><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p,
-                                                       f.tgt_node.p, nact);
-      break;
-    case 2:
-      fft_accumulate_kernel<2><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p,
-                                                       f.tgt_node.p, nact);
-      break;
-    case 3:
-      fft_accumulate_kernel<3><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p,
-                                                       f.tgt_node.p, nact);
-      break;
-    case 4:
-      fft_accumulate_kernel<4><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p,
-                                                       f.tgt_node.p, nact);
-      break;
-    case 6:
-      fft_accumulate_kernel<6><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, f.spec.p, f.qhat.p, f.chat.p,
-                                                       f.tgt_node.p, nact);
-      break;
-    default:
-      throw Error(NNK_E_ARG, "Fourier M2L supports 1, 2, 3, 4 or 6 right-hand sides per pass");
-  }
-  NNK_CHECK_LAUNCH();
-  inv<<<f.ntgt, 256, inverse_smem(G, res, R), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, f.chat.p, R, check,
-                                                    f.NK, nact);
-  NNK_CHECK_LAUNCH();
+  if (f.fp64) throw Error(NNK_E_STATE, "Fourier M2L built for FP64 densities");
+  run_fft_m2l<float>(f, str, upbase, R, check, st, nact, f.spec.p, f.qhat.p, f.chat.p);
+}
+
+void launch_fft_m2l(FftM2L& f, const double* str, long long upbase, int R, double* check, cudaStream_t st,
+                    const int* nact) {
+  if (!f.fp64) throw Error(NNK_E_STATE, "Fourier M2L built for FP32 densities");
+  run_fft_m2l<double>(f, str, upbase, R, check, st, nact, f.spec64.p, f.qhat64.p, f.chat64.p);
 }
 
 }  // namespace nnk

@@ -13,9 +13,9 @@
 // grid, Q_v the spectrum of v's densities.  Per V pair this costs
 // 9 complex multiply-adds per frequency and right-hand side on
 // G^2 (G/2 + 1) frequencies (real-to-complex), against (3P)^2 for the dense
-// matrix.  Spectra are FP32; the kernel spectra are computed in FP64 once per
-// (box width, offset) with 1/(8 pi mu) and the 1/G^3 of the inverse
-// transform folded in.
+// matrix.  Spectra are FP32 (mixed mode) or FP64 (FP64 mode); the kernel
+// spectra are computed in FP64 once per (box width, offset) with 1/(8 pi mu)
+// and the 1/G^3 of the inverse transform folded in.
 #pragma once
 #include <vector>
 
@@ -29,6 +29,7 @@ struct FftM2L {
   int nsrc = 0, ntgt = 0, nspec = 0, Rcap = 1;
   int64_t pairs = 0;
   DBuf<int> lat;        // per surface point: x | y << 8 | z << 16 lattice indices
+  bool fp64 = false;    // FP64 spectra and transforms (the *64 buffers)
   DBuf<float2> spec;    // nspec x 6 x NK (xx, xy, xz, yy, yz, zz)
   DBuf<int> src_node;   // per source slot: node
   DBuf<int> tgt_node;   // per target slot: node
@@ -37,18 +38,24 @@ struct FftM2L {
   DBuf<int> vspec;      // per pair: kernel spectrum
   DBuf<float2> qhat;    // nsrc x 3R x NK
   DBuf<float2> chat;    // ntgt x 3R x NK
+  DBuf<double2> spec64, qhat64, chat64;
   size_t fwd_smem = 0, inv_smem = 0;
 };
 
+// Largest right-hand side count per pass (6, 4, 3, 2 or 1; 0 if none) whose
+// transforms fit the device's shared memory.
+int fft_m2l_max_rhs(int res, bool fp64);
 // node_op[n]: check-to-equivalent operator index of node n's (tree, level);
 // op_w[op]: its box width.  Rmax: right-hand sides per pass.
 void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu, const std::vector<double>& op_w,
-                   const std::vector<int>& node_op, int Rmax, FftM2L& f, cudaStream_t st);
+                   const std::vector<int>& node_op, int Rmax, bool fp64, FftM2L& f, cudaStream_t st);
 // check[((P * node + p) * R + r) * 3 + c] = M2L result for every node with a
 // V-list (other entries untouched); str holds the up-equivalent densities of
 // node n at str[((upbase + P * n + p) * R + r) * 3 + c].  nact (per node,
 // or nullptr): nodes with nact = 0 are neither transformed nor written.
 void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float* check, cudaStream_t st,
+                    const int* nact = nullptr);
+void launch_fft_m2l(FftM2L& f, const double* str, long long upbase, int R, double* check, cudaStream_t st,
                     const int* nact = nullptr);
 
 }  // namespace nnk

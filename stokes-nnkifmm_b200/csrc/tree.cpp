@@ -746,4 +746,31 @@ void merge_forest(const std::vector<const HostTree*>& trees, HostTree& f) {
   for (int32_t n = 0; n < f.nodes; ++n) f.by_level[f.level[n]].push_back(n);
 }
 
+void nearest_reference_weights(int64_t q, const int64_t* rowptr, const int32_t* col, double* val,
+                               double block_size) {
+  if (q <= 0) return;
+  const double bn = std::floor(block_size * 134217728.0 / (9.0 * (double)q));  // nearestMatrix.m:23
+  if (!(bn >= 1.0))
+    throw Error(NNK_E_ARG, "blockSize too small: nearestMatrix.m builds no block (blockNodes = 0)");
+  const int64_t block = bn > (double)q ? q : (int64_t)bn;
+  std::vector<int64_t> cm;
+  std::vector<double> w;
+  for (int64_t s = 0; s < q; s += block) {
+    const int64_t e = std::min(q, s + block);
+    const int64_t a = rowptr[s], b = rowptr[e];
+    // the tie weights 1/k_q in row-major order (by fine point, then coarse index)
+    w.clear();
+    for (int64_t r = s; r < e; ++r) {
+      for (int64_t k = rowptr[r] + 1; k < rowptr[r + 1]; ++k)
+        if (col[k] <= col[k - 1]) throw Error(NNK_E_ARG, "NN columns must ascend within a row");
+      for (int64_t k = rowptr[r]; k < rowptr[r + 1]; ++k) w.push_back(1.0 / (double)(rowptr[r + 1] - rowptr[r]));
+    }
+    // the tied pairs in column-major order (by coarse index, then fine point)
+    cm.resize(b - a);
+    for (int64_t k = a; k < b; ++k) cm[k - a] = k;
+    std::stable_sort(cm.begin(), cm.end(), [&](int64_t x, int64_t y) { return col[x] < col[y]; });
+    for (size_t j = 0; j < cm.size(); ++j) val[cm[j]] = w[j];
+  }
+}
+
 }  // namespace nnk

@@ -107,6 +107,14 @@ void nearest_matrix_gpu(struct ::nnk_ctx* ctx, const double* coarse, int64_t n, 
 void merge_forest(const std::vector<const HostTree*>& trees, HostTree& out);
 
 // nearestMatrix (Tools/Nearest/nearestMatrix.m:17-41), exact FP64 ties.
+// Rewrites the tie weights of a nearest-neighbour matrix (CSR by fine point,
+// every tied pair present with weight 1/k) into the pairing that
+// Tools/Nearest/nearestMatrix.m:23-39 produces as written: per block of
+// floor(block_size 2^27 / (9 q)) fine points, the j-th tied pair in
+// column-major order receives the j-th weight in row-major order.  Throws
+// NNK_E_ARG when that block size is 0 (the reference then builds no matrix).
+void nearest_reference_weights(int64_t q, const int64_t* rowptr, const int32_t* col, double* val,
+                               double block_size);
 void nearest_matrix(const double* coarse, int64_t n, const double* fine, int64_t q,
                     std::vector<int64_t>& rowptr, std::vector<int32_t>& col,
                     std::vector<double>& val);

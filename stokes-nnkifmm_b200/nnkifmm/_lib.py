@@ -72,6 +72,7 @@ SIGNATURES = {
     "nnk_last_error": (C.c_char_p, [_vp]),
     "nnk_nearest_matrix": (_i32, [_vp, _vp, _i64, _vp, _i64, _pi64, _vp, _vp, _vp]),
     "nnk_nearest_matrix_host": (_i32, [_vp, _vp, _i64, _vp, _i64, _pi64, _vp, _vp, _vp]),
+    "nnk_nearest_reference_weights": (_i32, [_vp, _i64, _vp, _vp, _vp, _f64]),
     "nnk_tree_build": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _vp, C.POINTER(TreeParams),
                               C.POINTER(_vp)]),
     "nnk_tree_info_get": (_i32, [_vp, C.POINTER(TreeInfo)]),
@@ -93,6 +94,7 @@ SIGNATURES = {
     "nnk_fmm_grad_positions": (_i32, [_vp, _vp, _vp, _i32, _vp, _vp, _i32]),
     "nnk_fmm_profile": (_i32, [_vp, _i32]),
     "nnk_fmm_profile_read": (_i32, [_vp, _vp, _vp]),
+    "nnk_fmm_test_wait_timeout": (_i32, [_vp, C.c_uint32]),
     "nnk_fmm_solve": (_i32, [_vp, _vp, _vp, _i32, C.POINTER(SolveParams), C.POINTER(SolveInfo), _i32]),
     "nnk_mob_create": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, C.POINTER(_vp)]),
     "nnk_mob_apply": (_i32, [_vp, _vp, _vp, _i32]),

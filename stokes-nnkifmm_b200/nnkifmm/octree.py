@@ -162,10 +162,17 @@ class OcTree:
         return self.finePoints
 
 
-def nearestMatrix(coarse, fine, blockSize=0.2, threads=0, device=0, builder="auto"):
+def nearestMatrix(coarse, fine, blockSize=0.2, threads=0, device=0, builder="auto", ties="share"):
     """nearestMatrix (Tools/Nearest/nearestMatrix.m:17-41) through the library:
     returns the (Q x N) scipy CSR matrix with exact FP64 ties sharing 1/k
-    (on the GPU when there is one, or on the host with builder="host")."""
+    (on the GPU when there is one, or on the host with builder="host").
+
+    ties="reference" gives the tie weights as nearestMatrix.m writes them
+    (per block of floor(blockSize 2^27 / (9 Q)) fine points, the tied pairs in
+    column-major order take the 1/k weights in row-major order, so rows with
+    ties need not sum to one); the default "share" keeps 1/k per tied pair."""
+    if ties not in ("share", "reference"):
+        raise ValueError("ties must be 'share' or 'reference'")
     ctx = L.context(device)
     fn = L.lib.nnk_nearest_matrix_host if builder == "host" else L.lib.nnk_nearest_matrix
     c = _as_points(coarse)
@@ -178,4 +185,7 @@ def nearestMatrix(coarse, fine, blockSize=0.2, threads=0, device=0, builder="aut
     val = np.zeros(max(nnz.value, 1), np.float64)
     L.check(fn(ctx.h, L.ptr(c), c.shape[0], L.ptr(f), f.shape[0], C.byref(nnz), L.ptr(rp), L.ptr(col), L.ptr(val)),
             ctx.h, "nearestMatrix")
+    if ties == "reference":
+        L.check(L.lib.nnk_nearest_reference_weights(ctx.h, f.shape[0], L.ptr(rp), L.ptr(col), L.ptr(val),
+                                                     float(blockSize)), ctx.h, "nearestMatrix")
     return sp.csr_matrix((val[:nnz.value], col[:nnz.value], rp), shape=(f.shape[0], c.shape[0]))

@@ -14,12 +14,13 @@ PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
 def test_m2l_dominant_phase():
-    r = bench.roofline(PHASES, STATS, "mixed", PEAKS)
+    r = bench.roofline(PHASES, STATS, "mixed", PEAKS, "tensor")
     assert r["bound"] == "tensor" and "m2l_ws_kernel" in r["kernel"]
     flops = 2 * 2.0 * 256 * 256 * STATS["m2l_pairs"]
     assert r["achieved"] == pytest.approx(flops / 2.52e-3 / 1e12)
     assert r["peak"] == pytest.approx(795.0) and r["frac"] == pytest.approx(r["achieved"] / 795.0)
     assert r["launches_per_step"] == 3 and r["hbm_measured_gbs"] == 6650.0
+    assert r["traffic"] == pytest.approx(bench.M2L_TRAFFIC_250K) and r["traffic"] > 1e9
     p = r["pair_kernels"]
     # the V pairs run in the M2L phase, not in the down pairs
     npairs = STATS["pairs_up"] + STATS["pairs_down"] - STATS["m2l_pairs"] * 152 ** 2 + STATS["pairs_leaf"]
@@ -31,7 +32,7 @@ def test_m2l_dominant_phase():
 def test_pair_dominant_phase_fp64():
     # M2L as pair segments of the down pass: no M2L phase, the V pairs count
     phases = dict(PHASES, down_pairs=(40.0, 7), m2l=(0.0, 0))
-    r = bench.roofline(phases, STATS, "fp64", {})
+    r = bench.roofline(phases, STATS, "fp64", {}, "pairs")
     assert r["kernel"] == "p2p_kernel (down_pairs)" and r["bound"] == "fp64"
     assert r["achieved"] == pytest.approx(STATS["pairs_down"] * bench.FLOPS_PER_PAIR / 40e-3 / 1e12)
     assert r["peak"] == pytest.approx(bench.FP32_NOMINAL_TFLOPS / 2)
@@ -39,19 +40,44 @@ def test_pair_dominant_phase_fp64():
 
 
 def test_c2e_dominant_phase_and_uncompressed_m2l():
-    r = bench.roofline(dict(PHASES, up_c2e=(9.0, 7)), STATS, "fp64", PEAKS)
+    r = bench.roofline(dict(PHASES, up_c2e=(9.0, 7)), STATS, "fp64", PEAKS, "fourier")
     assert r["kernel"] == "c2e_kernel (up_c2e)"
     assert r["achieved"] == pytest.approx(2.0 * 456 * 456 * STATS["c2e_columns"] / 9e-3 / 1e12)
-    full = bench.roofline(PHASES, dict(STATS, m2l_rank=0), "mixed", PEAKS)
+    full = bench.roofline(PHASES, dict(STATS, m2l_rank=0), "mixed", PEAKS, "tensor")
     assert "m2l_img_kernel" in full["kernel"]
     assert full["achieved"] == pytest.approx(2.0 * 456 * 456 * STATS["m2l_pairs"] / 2.52e-3 / 1e12)
+
+
+def test_fourier_m2l_dominant_phase_fp64():
+    """FP64 matvec with its Fourier-space M2L as the longest phase: 9 complex
+    multiply-adds (72 flops) per V pair and frequency (12^2 x 7 = 1008 for
+    p = 6) against the nominal FP64 SIMT rate."""
+    phases = dict(PHASES, m2l=(6.0, 3))
+    r = bench.roofline(phases, STATS, "fp64", PEAKS, "fourier")
+    assert "fft_accumulate_kernel (FP64" in r["kernel"] and r["bound"] == "fp64"
+    assert r["achieved"] == pytest.approx(72.0 * 1008 * STATS["m2l_pairs"] / 6e-3 / 1e12)
+    assert r["peak"] == pytest.approx(bench.FP32_NOMINAL_TFLOPS / 2)
+    assert r["ms_per_launch"] == pytest.approx(2.0)
+
+
+def test_reference_arm_does_not_load_the_library():
+    """The reference arm reads the workload generator without importing the
+    package (whose import maps libnnkifmm.so)."""
+    import subprocess
+    import sys
+    code = ("import sys, bench; m = bench.workloads_module(); w = m.matvec_at_scale(200, 800); "
+            "assert w['coarse'].shape == (200, 3); "
+            "assert 'nnkifmm' not in sys.modules and 'nnkifmm._lib' not in sys.modules; "
+            "maps = open('/proc/self/maps').read(); assert 'libnnkifmm' not in maps; print('ok')")
+    out = subprocess.run([sys.executable, "-c", code], cwd=bench.ROOT, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0 and "ok" in out.stdout, out.stderr
 
 
 def test_pair_kernels_of_the_250k_matvec():
     """The live phase split and statistics of the 250k / 1M-point mixed
     matvec: the pair phases reach 41% of the nominal FP32 rate (32 flops per
     pair), the M2L phase 19% of the TF32 rate."""
-    r = bench.roofline(PHASES, STATS, "mixed", PEAKS)
+    r = bench.roofline(PHASES, STATS, "mixed", PEAKS, "tensor")
     assert r["pair_kernels"]["frac"] == pytest.approx(0.41, abs=0.01)
     assert r["frac"] == pytest.approx(0.186, abs=0.005)
 
