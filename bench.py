@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"],
+    ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64", "near32"],
                     help="the matvec arm timed for `value` (the other arm is timed after it and reported "
                          "under its own key unless --one-arm)")
     ap.add_argument("--one-arm", action="store_true", help="time only the --precision arm (profiling runs)")
@@ -682,12 +682,12 @@ def main():
     tree_s = time.time() - t0
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
-    m2l_of = {"fp64": "pairs" if args.m2l == "pairs" else "auto", "mixed": args.m2l}
-    form_of = {"fp64": "pairs" if args.m2l == "pairs" else "fourier",
+    m2l_of = {"fp64": "pairs" if args.m2l == "pairs" else "auto", "near32": "auto", "mixed": args.m2l}
+    form_of = {"fp64": "pairs" if args.m2l == "pairs" else "fourier", "near32": "fourier",
                "mixed": {"auto": "tensor", "images": "tensor", "generate": "tensor", "pairs": "pairs",
                          "fft": "fourier"}[args.m2l]}
     head = args.precision
-    arms = [head] if args.one_arm else [head, "mixed" if head == "fp64" else "fp64"]
+    arms = [head] if args.one_arm else [head] + [p for p in ("fp64", "near32", "mixed") if p != head]
     res = {}
     for k, prec in enumerate(arms):
         barrier(ws)
@@ -699,7 +699,9 @@ def main():
         r["e2e_step_ms"] = allmax(ws, float(np.mean(r["e2e_ms"])))
         r["per_step"] = {kk: (v[0] / args.steps, v[1] / args.steps) for kk, v in r["prof"].items()}
         r["stats"] = r["fmm"].stats()
-        r["roofline"] = roofline(r["per_step"], r["stats"], prec, peaks, form_of[prec])
+        r["roofline"] = roofline(r["per_step"], r["stats"], "fp64" if prec == "near32" else prec, peaks,
+                                 form_of[prec])
+        del r["fmm"]  # one arm's device buffers at a time
         res[prec] = r
     H = res[head]
     stats = H["stats"]
@@ -717,21 +719,25 @@ def main():
         ref = sampled_direct(torch, w, NN, idx)
         rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
         errors = {f"{p}_vs_direct_4096": rel(res[p]["out"][idx], ref) for p in res}
-        if len(res) == 2:
-            errors["mixed_vs_fp64"] = rel(res["mixed"]["out"], res["fp64"]["out"])
+        if "fp64" in res:
+            for p in res:
+                if p != "fp64":
+                    errors[f"{p}_vs_fp64"] = rel(res[p]["out"], res["fp64"]["out"])
     note = None
-    if head == "mixed" and errors and errors.get("mixed_vs_fp64", 0.0) > 1e-4:
+    if head != "fp64" and errors and errors.get(f"{head}_vs_fp64", 0.0) > 1e-4:
         # the metric holds at <= 1e-4 relative error against the FP64 operator
-        note = (f"mixed matvec is {errors['mixed_vs_fp64']:.2e} from the FP64 matvec (> 1e-4): value withheld; "
-                "the FP64 arm's rate is under fp64_gpu")
+        note = (f"{head} matvec is {errors[f'{head}_vs_fp64']:.2e} from the FP64 matvec (> 1e-4): value "
+                "withheld; the FP64 arm's rate is under fp64_gpu")
         value = None
 
     line = {"metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": {"fp64": "f64", "near32": "f64+f32", "mixed": "f32"}[head],
+            "data": "synthetic",
             "config": {"workload": WORKLOAD, "precision": head,
-                       "m2l": {"fp64": "FP64 Fourier-space (FP64 spectra)", "mixed": "TF32 tensor cores (tcgen05), "
-                               "rank-256 compressed operators"}[head] if args.m2l == "auto" else args.m2l,
+                       "m2l": {"fp64": "FP64 Fourier-space (FP64 spectra)", "near32": "FP64 Fourier-space",
+                               "mixed": "TF32 tensor cores (tcgen05), rank-256 compressed operators"}[head]
+                       if args.m2l == "auto" else args.m2l,
                        "parallelism": f"replicas x{ws}",
                        "l2": "flushed between timed steps (256 MiB write, outside the step events)",
                        "nodes": tree.nodeCount, "levels": int(tree.info.max_level) + 1,
@@ -751,7 +757,14 @@ def main():
             continue
         o = res[p]
         line[f"{p}_gpu"] = {"value": ws * args.n_force / (o["step_ms"] / 1e3), "unit": "pts/s",
-                            "ms_per_step": o["step_ms"], "dtype": "f32" if p == "mixed" else "f64",
+                            "ms_per_step": o["step_ms"],
+                            "dtype": {"fp64": "f64", "near32": "f64+f32", "mixed": "f32"}[p],
+                            "operator": {"fp64": "reference (exact check-to-equivalent inverses), all FP64",
+                                         "near32": "reference (exact inverses); U-list P2P and X-list P2L in "
+                                                   "FP32, every sum over equivalent densities in FP64",
+                                         "mixed": "Tikhonov-regularized check-to-equivalent operators, FP32 "
+                                                  "pairs, TF32 tensor-core M2L (not the reference's operator "
+                                                  "where NEAREST sources leave their leaf boxes)"}[p],
                             "e2e_value": ws * args.n_force / (o["e2e_step_ms"] / 1e3),
                             "speedup_vs_" + head: H["step_ms"] / o["step_ms"], "roofline": o["roofline"],
                             "fmm_setup_s": round(o["setup_s"], 2)}

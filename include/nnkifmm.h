@@ -51,6 +51,12 @@ extern "C" {
 
 #define NNK_PREC_FP64 0    /* every FMM step in FP64                            */
 #define NNK_PREC_MIXED 1   /* FP32 pair kernels, tensor-core M2L, FP64 C2E ops   */
+#define NNK_PREC_NEAR32 2  /* the FP64 operator (exact check-to-equivalent
+                              inverses) with the pair sums whose sources are
+                              the forces themselves -- U-list P2P and X-list
+                              P2L -- in FP32; every sum over equivalent
+                              densities stays FP64.  Adjoint and gradients of
+                              such an FMM run in FP64.                       */
 
 typedef struct nnk_ctx nnk_ctx;
 typedef struct nnk_tree nnk_tree;
@@ -91,7 +97,7 @@ typedef struct nnk_fmm_params {
   double mu;             /* kernelPar(2)                                       */
   int32_t corona_res;    /* 'coronaRes' (default 6)                            */
   int32_t corona_shells; /* 'coronaShells' (default 1)                         */
-  int32_t precision;     /* NNK_PREC_FP64 or NNK_PREC_MIXED                    */
+  int32_t precision;     /* NNK_PREC_FP64, NNK_PREC_MIXED or NNK_PREC_NEAR32   */
   int32_t m2l_mode;      /* mixed mode M2L: 0 auto (tensor cores on rank-256
                             compressed operators B C_o B^T when 3P > 256, else
                             images when they fit 8 GiB), 1 tensor cores +
@@ -100,9 +106,9 @@ typedef struct nnk_fmm_params {
                             kernel (no tensor cores; FP32-rounding accuracy),
                             4 FP32 Fourier-space product (FFT of the surface
                             lattice; FP32-rounding accuracy).
-                            FP64 mode: 3 the FP64 pair kernel, any other value
-                            the FP64 Fourier-space product (at most 4
-                            right-hand sides per pass)                        */
+                            FP64 and NEAR32 modes: 3 the FP64 pair kernel, any
+                            other value the FP64 Fourier-space product (at
+                            most 4 right-hand sides per pass)                 */
   double reg;            /* relative Tikhonov weight of the check-to-equivalent
                             pseudo-inverse: NNK_PREC_MIXED 0 = default 1e-5;
                             NNK_PREC_FP64 0 = exact LU inverse (reference)   */
@@ -386,19 +392,24 @@ int nnk_batch_destroy(nnk_batch* batch);
 
 /* ------------------------------------------------- allocation-free call -- */
 /* No counterpart in the reference: an extra entry point for callers that
- * cannot allocate device memory when they call (during CUDA graph capture,
- * inside a MEX gateway whose device memory MATLAB owns, or in a loop with a
- * fixed memory budget).  It evaluates the NEAREST velocity by direct
- * summation, vel(t) = S(fine -> t) * kron(NN,I3) * forces, the dense product
- * of nearestBlockComputation.m, with every input and output a device pointer
+ * cannot allocate device memory when they call -- a MEX gateway whose device
+ * memory belongs to MATLAB's own pool, or a loop that fixed its memory budget
+ * up front and must not pay cudaMalloc/cudaFree (which can synchronize the
+ * device) per step.  It evaluates the NEAREST velocity by direct summation,
+ * vel(t) = S(fine -> t) * kron(NN,I3) * forces, the dense product of
+ * nearestBlockComputation.m, with every input and output a device pointer
  * supplied by the caller (forces n x 3, NN CSR by fine point with 0-based
  * columns into forces, fine q x 3, targets m x 3, vel m x 3, row-major FP64),
- * issued on `stream`.  Its one scratch buffer, the fine-point forces, is a
- * static device array of NNK_NOALLOC_MAX_FINE rows that every GPU loading the
- * library holds until exit; larger q is rejected with NNK_E_ARG.  The first
- * call on a device looks up that array's address and should come before any
- * stream capture.  Calls share the array: calls that overlap on the GPU race.
- * Returns without synchronizing. */
+ * issued on `stream` (which must belong to `device`; NULL is the legacy
+ * default stream).  Its one scratch buffer, the fine-point forces, is a static
+ * device array of NNK_NOALLOC_MAX_FINE rows that every GPU loading the library
+ * holds until exit; larger q is rejected with NNK_E_ARG.  The first call on a
+ * device looks up that array's address and should come before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race.  A
+ * column index outside [0, n) is not read: the velocities it reaches come out
+ * NaN.  A CUDA error already pending on the calling thread is returned as
+ * NNK_E_CUDA without launching and left in place.  Returns without
+ * synchronizing. */
 #define NNK_NOALLOC_MAX_FINE 262144
 int nnk_direct_nearest_noalloc(int32_t device, void* stream, const double* forces,
                                int64_t n, const int64_t* nn_rowptr,

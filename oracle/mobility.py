@@ -164,3 +164,26 @@ def rigid_output(asm, x, bodies):
     for i, b in enumerate(bodies):
         out.extend([U[i], np.cross(Om[i], b.b1), np.cross(Om[i], b.b2)])
     return np.concatenate(out) if out else np.zeros(0)
+
+
+def mobility_precon(f, asm, fmm, nearest=True):
+    r"""The block preconditioner of Mobility/MobilityPrecon.m:17-39 applied to
+    f = [force (3N, blocked x|y|z); U (3 nb); Omega (3 nb)].
+
+    ``fmm`` is an oracle KIFMM (``gmres=1, fmt=2``, the blocked vector layout
+    MobilityPrecon.m:26 selects) on the swimmers' tree (all force points,
+    NEAREST with the block NN):
+      b(force) = reducedSolve(force)                                  (:29-30)
+      out      = -A2 \ (BT' * computeVelSparse(B' * (A1 \ UOm)))      (:32-34)
+      b(force) = b(force) - reducedSolve(BT * out)                     (:38-39)
+    with [B, BT, A1, A2] of genMatrixComponets.m (dense here)."""
+    nb = asm["nb"]
+    f = np.asarray(f, dtype=np.float64).ravel()
+    force, UOm = f[:-6 * nb], f[-6 * nb:]
+    B, BT, A1, A2 = gen_matrix_components(asm, nearest)
+    b = np.zeros_like(f)
+    b[:-6 * nb] = fmm.reduced_solve(force)
+    out = -np.linalg.solve(A2, BT.T @ fmm.compute_vel_sparse(B.T @ np.linalg.solve(A1, UOm)))
+    b[-6 * nb:] = out
+    b[:-6 * nb] -= fmm.reduced_solve(BT @ out)
+    return b

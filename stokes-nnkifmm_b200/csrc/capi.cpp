@@ -292,7 +292,7 @@ int nnk_fmm_create(nnk_ctx* ctx, const nnk_tree* tree, const nnk_fmm_params* par
   p.precision = params->precision;
   p.m2l_mode = params->m2l_mode;
   p.reg = params->reg;
-  if (p.precision != NNK_PREC_FP64 && p.precision != NNK_PREC_MIXED)
+  if (p.precision != NNK_PREC_FP64 && p.precision != NNK_PREC_MIXED && p.precision != NNK_PREC_NEAR32)
     return fail(ctx, NNK_E_ARG, "unknown precision mode");
   std::unique_ptr<nnk_fmm> f(new nnk_fmm());
   f->ctx = ctx;

@@ -260,13 +260,14 @@ void Fmm::build_points() {
     }
   }
   const int64_t nt = (int64_t)t.tgt_row.size();
-  if (p_.precision == NNK_PREC_FP64) {
+  if (f64()) {
     pos64_.upload(pos, st);
     tpos64_.upload(t.tgt_pos, st);
     str64_.alloc(3 * tot_ * R_);
     check64_.alloc((size_t)N_ * 3 * P_ * R_);
     vel64_.alloc(3 * nt * R_);
-  } else {
+  }
+  if (!f64() || near32()) {
     std::vector<float> p4(4 * (size_t)tot_);
     for (int64_t i = 0; i < tot_; ++i) {
       const double* sh = &shift_[3 * (size_t)pgroup[i]];
@@ -283,7 +284,7 @@ void Fmm::build_points() {
       }
     }
     tpos32_.upload(t4, st);
-    str32_.alloc(3 * tot_ * R_);
+    str32_.alloc(3 * (near32() ? E_ : tot_) * R_);  // NEAR32: the forces of the leaf entries only
     check32_.alloc((size_t)N_ * 3 * P_ * R_);
     vel32_.alloc(3 * nt * R_);
   }
@@ -326,13 +327,14 @@ void Fmm::build_tasks() {
     for (int g = 0; g < t.groups(); ++g) roots[g] = t.root_of(g);
     roots_.upload(roots, st);
   }
+  fwd_.near = near32();
   build_taskset(fwd_, r, true);
   stats_.c2e_columns = (int64_t)ln.size() + (int64_t)fwd_.up_nodes_host.size();
   stats_.surface_points = P_;
   stats_.levels = maxl_ + 1;
   const int64_t slots = std::max<int64_t>(3 * fwd_.partial_slots * R_, 1);
-  if (p_.precision == NNK_PREC_FP64) partial64_.alloc(slots);
-  else partial32_.alloc(slots);
+  if (f64()) partial64_.alloc(slots);
+  if (!f64() || near32()) partial32_.alloc(slots);
   NNK_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -437,6 +439,56 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
     tasks.push_back(tk);
   }
   ts.leaf.count = (int64_t)tasks.size() - ts.leaf.first;
+  if (ts.near) {
+    // the same sums split by the precision of their sources: X-list P2L of
+    // every level (forces, FP32) apart from each level's L2L (FP64); the leaf
+    // stage's U-list P2P (forces, FP32) apart from its L2T and W-list (FP64)
+    ts.l2l.assign(maxl_ + 1, {});
+    ts.x_only.first = (int64_t)tasks.size();
+    for (int L = 1; L <= maxl_; ++L)
+      for (int32_t n : t.by_level[L]) {
+        if (r.X->off[n + 1] == r.X->off[n]) continue;
+        TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0, n, 0};
+        for (int64_t k = r.X->off[n]; k < r.X->off[n + 1]; ++k) src_seg(r.X->idx[k]);
+        tk.nseg = (int)segs.size() - tk.seg0;
+        if (tk.nseg) tasks.push_back(tk);
+      }
+    ts.x_only.count = (int64_t)tasks.size() - ts.x_only.first;
+    for (int L = 2; L <= maxl_; ++L) {
+      ts.l2l[L].first = (int64_t)tasks.size();
+      for (int32_t n : t.by_level[L]) {
+        TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 1, 0, n, 0};
+        segs.push_back(SegD{dnB + (long long)P_ * t.parent[n], P_, 0});
+        tk.partial = 0;
+        tasks.push_back(tk);
+      }
+      ts.l2l[L].count = (int64_t)tasks.size() - ts.l2l[L].first;
+    }
+    ts.leaf_u.first = (int64_t)tasks.size();
+    for (int32_t i = 0; i < N_; ++i) {
+      if (!(*r.tgt_leaf)[i]) continue;
+      const int nt = (int)(tr[i + 1] - tr[i]);
+      if (nt == 0) continue;
+      TaskD tk{tr[i], tr[i], nt, (int)segs.size(), 0, 0, i, 0};
+      for (int64_t k = r.U->off[i]; k < r.U->off[i + 1]; ++k) src_seg(r.U->idx[k]);
+      tk.nseg = (int)segs.size() - tk.seg0;
+      if (tk.nseg) tasks.push_back(tk);
+    }
+    ts.leaf_u.count = (int64_t)tasks.size() - ts.leaf_u.first;
+    ts.leaf_far.first = (int64_t)tasks.size();
+    for (int32_t i = 0; i < N_; ++i) {
+      if (!(*r.tgt_leaf)[i]) continue;
+      const int nt = (int)(tr[i + 1] - tr[i]);
+      if (nt == 0) continue;
+      TaskD tk{tr[i], tr[i], nt, (int)segs.size(), 0, 0, i, 0};
+      for (int64_t k = r.W->off[i]; k < r.W->off[i + 1]; ++k)
+        segs.push_back(SegD{upB + (long long)P_ * r.W->idx[k], P_, 0});
+      segs.push_back(SegD{dnB + (long long)P_ * i, P_, 0});
+      tk.nseg = (int)segs.size() - tk.seg0;
+      tasks.push_back(tk);
+    }
+    ts.leaf_far.count = (int64_t)tasks.size() - ts.leaf_far.first;
+  }
   cudaStream_t st = ctx_->stream;
   {
     std::vector<C2ETile> ut;
@@ -559,6 +611,12 @@ void Fmm::split_tasks(TaskSet& ts, std::vector<TaskD>& tasks, std::vector<SegD>&
   for (auto& g : ts.down_nov) process(g);
   for (auto& g : ts.down) process(g);
   process(ts.leaf);
+  if (ts.near) {
+    process(ts.x_only);
+    for (auto& g : ts.l2l) process(g);
+    process(ts.leaf_u);
+    process(ts.leaf_far);
+  }
   tasks.swap(nt);
   segs.swap(ns);
   ts.reds.upload(reds, ctx_->stream);
@@ -620,7 +678,7 @@ void Fmm::build_operators() {
   // Fourier-space M2L: mode 4 in mixed precision (FP32 spectra); in FP64
   // every mode but 3 (the FP64 pair kernel) when the transforms of one
   // right-hand side fit shared memory (FP64 spectra)
-  const bool fp64 = p_.precision == NNK_PREC_FP64;
+  const bool fp64 = f64();
   const int fft_cap = fft_m2l_max_rhs(p_.res, fp64);
   if ((!fp64 && p_.m2l_mode == 4) || (fp64 && p_.m2l_mode != 3 && fft_cap >= 1)) {
     std::vector<int> node_op(N_);
@@ -644,7 +702,7 @@ void Fmm::build_operators() {
   auto lat = shell_lattice(p_.res, p_.shells);
   // FP64 mode uses the exact inverse (the reference's LU solve) unless a
   // Tikhonov weight is given; mixed mode always regularizes.
-  const bool exact = p_.precision == NNK_PREC_FP64 && !(p_.reg > 0);
+  const bool exact = f64() && !(p_.reg > 0);
   const double reg = p_.reg > 0 ? p_.reg : 1e-5;
   // host part, in parallel over operators: K_up = kernel(upsurf, downsurf)
   // (up-equivalent densities -> down check) and, for the Tikhonov form,
@@ -752,10 +810,23 @@ __global__ void zero_roots_kernel(const int32_t* __restrict__ roots, long long b
 }
 }  // namespace
 
+namespace {
+// a[i] += b[i] (the FP32 near-field sums into the FP64 ones)
+__global__ void add_f32_kernel(long long n, const float* __restrict__ b, double* __restrict__ a) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] += (double)b[i];
+}
+void add_f32(long long n, const float* b, double* a, cudaStream_t st) {
+  if (n <= 0) return;
+  add_f32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, b, a);
+  NNK_CHECK_LAUNCH();
+}
+}  // namespace
+
 template <typename Real>
-void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R) {
+void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R, bool near) {
   cudaStream_t st = ctx_->stream;
-  Real* check = p_.precision == NNK_PREC_FP64 ? (Real*)check64_.p : (Real*)check32_.p;
+  Real* check = f64() ? (Real*)check64_.p : (Real*)check32_.p;
   const Real e2 = (Real)(p_.eps * p_.eps);
   const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
   const int n = 3 * P_;
@@ -796,11 +867,24 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     NNK_CUDA(cudaMemsetAsync(check, 0, sizeof(Real) * (size_t)N_ * n * R, st));
     phase(NNK_PHASE_M2L, [&] { launch_fft_m2l(fft_, (const Real*)str, regionA, R, check, st, na); });
   }
-  const std::vector<TaskGroup>& dgroups = (tm || fm) ? ts.down_nov : ts.down;
+  if (near) {
+    // NEAR32: the X-list P2L of every level in FP32 (its sources are the
+    // leaf entries' forces), added to the FP64 M2L result
+    if (!fm || !std::is_same<Real, double>::value || !ts.near)
+      throw Error(NNK_E_STATE, "NEAR32 needs the FP64 Fourier-space M2L");
+    const size_t nc = (size_t)N_ * n * R;
+    NNK_CUDA(cudaMemsetAsync(check32_.p, 0, sizeof(float) * nc, st));
+    run_group<float>(ts, ts.x_only, pos32_.p, str32_.p, pos32_.p, check32_.p, (float)(p_.eps * p_.eps),
+                     (float)(1.0 / (8.0 * M_PI * p_.mu)), 1, NNK_PHASE_DOWN_PAIRS, R);
+    phase(NNK_PHASE_DOWN_PAIRS, [&] { add_f32((long long)nc, check32_.p, (double*)check, st); });
+  }
+  const std::vector<TaskGroup>& dgroups = near ? ts.l2l : (tm || fm) ? ts.down_nov : ts.down;
   for (int L = 1; L <= maxl_; ++L) {
-    if (dgroups[L].count == 0) continue;
-    run_group<Real>(ts, dgroups[L], spos, str, spos, check, e2, scale, (tm || fm) ? 1 : 0, NNK_PHASE_DOWN_PAIRS, R);
+    if (dgroups[L].count > 0)
+      run_group<Real>(ts, dgroups[L], spos, str, spos, check, e2, scale, (tm || fm) ? 1 : 0, NNK_PHASE_DOWN_PAIRS,
+                      R);
     const int64_t nt = dn_toff_[L + 1] - dn_toff_[L];
+    if (nt == 0) continue;
     phase(NNK_PHASE_DOWN_C2E, [&] {
       launch_c2e<Real>(ops_.p, n, 1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str,
                        regionA + (int64_t)P_ * N_, P_, R, st, nullptr, 0, c2e_part_.p, c2e_part_.n, na);
@@ -812,17 +896,29 @@ template <typename Real>
 void Fmm::apply_impl(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int k0, int R) {
   cudaStream_t st = ctx_->stream;
   const HostTree& t = *t_;
-  Real* str = p_.precision == NNK_PREC_FP64 ? (Real*)str64_.p : (Real*)str32_.p;
-  const Real* pos = p_.precision == NNK_PREC_FP64 ? (const Real*)pos64_.p : (const Real*)pos32_.p;
-  const Real* tpos = p_.precision == NNK_PREC_FP64 ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
-  Real* vel = p_.precision == NNK_PREC_FP64 ? (Real*)vel64_.p : (Real*)vel32_.p;
+  Real* str = f64() ? (Real*)str64_.p : (Real*)str32_.p;
+  const Real* pos = f64() ? (const Real*)pos64_.p : (const Real*)pos32_.p;
+  const Real* tpos = f64() ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
+  Real* vel = f64() ? (Real*)vel64_.p : (Real*)vel32_.p;
   const Real e2 = (Real)(p_.eps * p_.eps);
   const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
   // forces on the leaf source entries (kron(NN,I3)*f per leaf)
   phase(NNK_PHASE_GATHER, [&] { launch_gather<Real>(E_, goff_.p, gidx_.p, gw_.p, d_in, in, k0, R, str, st); });
-  far_field<Real>(fwd_, pos, str, E_, R);
+  const bool near = near32() && std::is_same<Real, double>::value;
+  if (near)  // the same forces in FP32 for the near-field sums
+    phase(NNK_PHASE_GATHER, [&] { launch_gather<float>(E_, goff_.p, gidx_.p, gw_.p, d_in, in, k0, R, str32_.p, st); });
+  far_field<Real>(fwd_, pos, str, E_, R, near);
   // leaf stage
-  run_group<Real>(fwd_, fwd_.leaf, pos, str, tpos, vel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS, R);
+  if (near) {
+    run_group<Real>(fwd_, fwd_.leaf_far, pos, str, tpos, vel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS, R);
+    const size_t nv = 3 * t.tgt_row.size() * (size_t)R;
+    NNK_CUDA(cudaMemsetAsync(vel32_.p, 0, sizeof(float) * nv, st));
+    run_group<float>(fwd_, fwd_.leaf_u, pos32_.p, str32_.p, tpos32_.p, vel32_.p, (float)(p_.eps * p_.eps),
+                     (float)(1.0 / (8.0 * M_PI * p_.mu)), 1, NNK_PHASE_LEAF_PAIRS, R);
+    phase(NNK_PHASE_LEAF_PAIRS, [&] { add_f32((long long)nv, vel32_.p, (double*)vel, st); });
+  } else {
+    run_group<Real>(fwd_, fwd_.leaf, pos, str, tpos, vel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS, R);
+  }
   phase(NNK_PHASE_SCATTER, [&] {
     launch_scatter<Real>((int64_t)t.tgt_row.size(), trow_.p, vel, out, k0, R, d_out, st, tgt_leaf_.p, nact());
   });
@@ -837,10 +933,10 @@ void Fmm::adjoint_impl(const double* d_in, const IoMap& in, double* d_out, const
   cudaStream_t st = ctx_->stream;
   const HostTree& t = *t_;
   const int64_t nt = (int64_t)t.tgt_row.size();
-  Real* astr = p_.precision == NNK_PREC_FP64 ? (Real*)astr64_.p : (Real*)astr32_.p;
-  const Real* apos = p_.precision == NNK_PREC_FP64 ? (const Real*)apos64_.p : (const Real*)apos32_.p;
-  const Real* pos = p_.precision == NNK_PREC_FP64 ? (const Real*)pos64_.p : (const Real*)pos32_.p;
-  Real* avel = p_.precision == NNK_PREC_FP64 ? (Real*)avel64_.p : (Real*)avel32_.p;
+  Real* astr = f64() ? (Real*)astr64_.p : (Real*)astr32_.p;
+  const Real* apos = f64() ? (const Real*)apos64_.p : (const Real*)apos32_.p;
+  const Real* pos = f64() ? (const Real*)pos64_.p : (const Real*)pos32_.p;
+  Real* avel = f64() ? (Real*)avel64_.p : (Real*)avel32_.p;
   const Real e2 = (Real)(p_.eps * p_.eps);
   const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
   phase(NNK_PHASE_GATHER, [&] { launch_gather<Real>(nt, agoff_.p, agidx_.p, agw_.p, d_in, in, k0, R, astr, st); });
@@ -863,14 +959,14 @@ void Fmm::grad_impl(const double* d_f, const double* d_w, int layout, double* d_
   cudaStream_t st = ctx_->stream;
   const HostTree& t = *t_;
   const int64_t nt = (int64_t)t.tgt_row.size();
-  Real* str = p_.precision == NNK_PREC_FP64 ? (Real*)str64_.p : (Real*)str32_.p;
-  const Real* pos = p_.precision == NNK_PREC_FP64 ? (const Real*)pos64_.p : (const Real*)pos32_.p;
-  const Real* tpos = p_.precision == NNK_PREC_FP64 ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
-  Real* vel = p_.precision == NNK_PREC_FP64 ? (Real*)vel64_.p : (Real*)vel32_.p;
-  Real* astr = p_.precision == NNK_PREC_FP64 ? (Real*)astr64_.p : (Real*)astr32_.p;
-  const Real* apos = p_.precision == NNK_PREC_FP64 ? (const Real*)apos64_.p : (const Real*)apos32_.p;
-  Real* avel = p_.precision == NNK_PREC_FP64 ? (Real*)avel64_.p : (Real*)avel32_.p;
-  Real* partial = p_.precision == NNK_PREC_FP64 ? (Real*)partial64_.p : (Real*)partial32_.p;
+  Real* str = f64() ? (Real*)str64_.p : (Real*)str32_.p;
+  const Real* pos = f64() ? (const Real*)pos64_.p : (const Real*)pos32_.p;
+  const Real* tpos = f64() ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
+  Real* vel = f64() ? (Real*)vel64_.p : (Real*)vel32_.p;
+  Real* astr = f64() ? (Real*)astr64_.p : (Real*)astr32_.p;
+  const Real* apos = f64() ? (const Real*)apos64_.p : (const Real*)apos32_.p;
+  Real* avel = f64() ? (Real*)avel64_.p : (Real*)avel32_.p;
+  Real* partial = f64() ? (Real*)partial64_.p : (Real*)partial32_.p;
   const Real e2 = (Real)(p_.eps * p_.eps);
   const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
   IoMap fin, win;
@@ -918,7 +1014,7 @@ void Fmm::apply_mapped(const double* d_in, const IoMap& in, double* d_out, const
   const int cap = rhs_cap(false);
   for (int k0 = 0; k0 < nrhs;) {
     const int R = rhs_chunk(nrhs - k0, cap);
-    if (p_.precision == NNK_PREC_FP64)
+    if (f64())
       apply_impl<double>(d_in, in, d_out, out, k0, R);
     else
       apply_impl<float>(d_in, in, d_out, out, k0, R);
@@ -941,7 +1037,7 @@ void Fmm::apply_adjoint_mapped(const double* d_in, const IoMap& in, double* d_ou
   const int cap = rhs_cap(true);
   for (int k0 = 0; k0 < nrhs;) {
     const int R = rhs_chunk(nrhs - k0, cap);
-    if (p_.precision == NNK_PREC_FP64)
+    if (f64())
       adjoint_impl<double>(d_in, in, d_out, out, k0, R);
     else
       adjoint_impl<float>(d_in, in, d_out, out, k0, R);
@@ -1014,6 +1110,35 @@ std::pair<double, double> Fmm::autotune(int nrhs) {
   DBuf<double> in(3 * (size_t)t.n_pot * R), out(3 * (size_t)t.n_tgt * R);
   in.zero(st);
   apply(in.p, out.p, NNK_LAYOUT_ROWS, R);
+  if (near32()) {
+    // FP64 groups (S2M/M2M, L2L, L2T + W-list) and FP32 groups (X-list P2L,
+    // U-list P2P) of the NEAR32 split, each tuned in its own arithmetic
+    std::vector<TaskGroup*> g64, g32;
+    for (auto& g : fwd_.up) g64.push_back(&g);
+    for (auto& g : fwd_.l2l) g64.push_back(&g);
+    g64.push_back(&fwd_.leaf_far);
+    g32.push_back(&fwd_.x_only);
+    g32.push_back(&fwd_.leaf_u);
+    const double e2 = p_.eps * p_.eps, sc = 1.0 / (8.0 * M_PI * p_.mu);
+    auto run64 = [&](const TaskGroup& g, int r) {
+      const bool leaf = g.first == fwd_.leaf_far.first;
+      run_group<double>(fwd_, g, pos64_.p, str64_.p, leaf ? tpos64_.p : pos64_.p, leaf ? vel64_.p : check64_.p, e2,
+                        sc, 0, NNK_PHASE_LEAF_PAIRS, r);
+    };
+    auto run32 = [&](const TaskGroup& g, int r) {
+      const bool leaf = g.first == fwd_.leaf_u.first;
+      run_group<float>(fwd_, g, pos32_.p, str32_.p, leaf ? tpos32_.p : pos32_.p, leaf ? vel32_.p : check32_.p,
+                       (float)e2, (float)sc, 0, NNK_PHASE_LEAF_PAIRS, r);
+    };
+    std::vector<int> kinds;
+    std::pair<double, double> res;
+    res.first = tune_groups<double>(this, g64, kinds, R, run64, st, false) +
+                tune_groups<float>(this, g32, kinds, R, run32, st, false);
+    res.second = tune_groups<double>(this, g64, kinds, R, run64, st, true) +
+                 tune_groups<float>(this, g32, kinds, R, run32, st, true);
+    NNK_CUDA(cudaStreamSynchronize(st));
+    return res;
+  }
   std::vector<TaskGroup*> groups;
   const bool nov = tensor_m2l_ || fft_m2l_;
   for (auto& g : fwd_.up) groups.push_back(&g);
@@ -1022,11 +1147,11 @@ std::pair<double, double> Fmm::autotune(int nrhs) {
   std::pair<double, double> res;
   auto go = [&](auto tag) {
     using Real = decltype(tag);
-    Real* str = p_.precision == NNK_PREC_FP64 ? (Real*)str64_.p : (Real*)str32_.p;
-    const Real* pos = p_.precision == NNK_PREC_FP64 ? (const Real*)pos64_.p : (const Real*)pos32_.p;
-    const Real* tpos = p_.precision == NNK_PREC_FP64 ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
-    Real* check = p_.precision == NNK_PREC_FP64 ? (Real*)check64_.p : (Real*)check32_.p;
-    Real* vel = p_.precision == NNK_PREC_FP64 ? (Real*)vel64_.p : (Real*)vel32_.p;
+    Real* str = f64() ? (Real*)str64_.p : (Real*)str32_.p;
+    const Real* pos = f64() ? (const Real*)pos64_.p : (const Real*)pos32_.p;
+    const Real* tpos = f64() ? (const Real*)tpos64_.p : (const Real*)tpos32_.p;
+    Real* check = f64() ? (Real*)check64_.p : (Real*)check32_.p;
+    Real* vel = f64() ? (Real*)vel64_.p : (Real*)vel32_.p;
     const Real e2 = (Real)(p_.eps * p_.eps);
     const Real scale = (Real)(1.0 / (8.0 * M_PI * p_.mu));
     auto run = [&](const TaskGroup& g, int r) {
@@ -1038,7 +1163,7 @@ std::pair<double, double> Fmm::autotune(int nrhs) {
     res.first = tune_groups<Real>(this, groups, kinds, R, run, st, false);
     res.second = tune_groups<Real>(this, groups, kinds, R, run, st, true);
   };
-  if (p_.precision == NNK_PREC_FP64) go(double());
+  if (f64()) go(double());
   else go(float());
   // the tuned launches overwrote work buffers: nothing to keep
   NNK_CUDA(cudaStreamSynchronize(st));
@@ -1060,7 +1185,7 @@ int64_t Fmm::source_origins() const { return t_->params.nearest ? t_->q : t_->n_
 void Fmm::grad_positions(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs) {
   if (t_->n_tgt == 0 || t_->n_pot == 0) return;
   build_adjoint();
-  if (p_.precision == NNK_PREC_FP64)
+  if (f64())
     grad_impl<double>(d_f, d_w, layout, d_gt, d_gs);
   else
     grad_impl<float>(d_f, d_w, layout, d_gt, d_gs);
@@ -1109,7 +1234,7 @@ void Fmm::build_adjoint() {
   r.X = &inv_W_;  // node t receives from the targets of leaves s with t in W(s)
   build_taskset(adj_, r, false);
   const int64_t slots = 3 * std::max(fwd_.partial_slots, adj_.partial_slots) * R_;
-  if (p_.precision == NNK_PREC_FP64) {
+  if (f64()) {
     if ((int64_t)partial64_.n < slots) partial64_.alloc(slots);
   } else if ((int64_t)partial32_.n < slots) {
     partial32_.alloc(slots);
@@ -1138,7 +1263,7 @@ void Fmm::build_adjoint() {
       pg[nt + (size_t)P_ * N_ + (size_t)P_ * n + k] = g;
     }
   }
-  if (p_.precision == NNK_PREC_FP64) {
+  if (f64()) {
     apos64_.upload(pos, st);
     astr64_.alloc(3 * atot * R_);
     avel64_.alloc(std::max<int64_t>(3 * E_ * R_, 1));

@@ -90,6 +90,12 @@ struct TaskSet {
   DBuf<RedD> reds;
   std::vector<TaskGroup> up, down, down_nov;  // per level
   TaskGroup leaf;
+  // NEAR32 split (the matvec's task set only): the X-list P2L of every level
+  // and the U-list P2P, whose sources are the forces (FP32), apart from the
+  // L2L of each level and the L2T + W-list of the leaves (FP64)
+  bool near = false;
+  std::vector<TaskGroup> l2l;  // per level
+  TaskGroup x_only, leaf_u, leaf_far;
   std::vector<int32_t> up_nodes_host;  // nodes whose up-equivalent density is formed, by level
   DBuf<int32_t> up_nodes;
   std::vector<int64_t> up_off;
@@ -168,6 +174,10 @@ class Fmm {
   const HostTree& tree() const { return *t_; }
   nnk_ctx* ctx() const { return ctx_; }
   const FmmParams& params() const { return p_; }
+  // FP64 work arrays (FP64 and NEAR32 modes); NEAR32 adds FP32 copies of the
+  // points and forces for its near-field pair sums
+  bool f64() const { return p_.precision != NNK_PREC_MIXED; }
+  bool near32() const { return p_.precision == NNK_PREC_NEAR32; }
   // scratch for host-pointer calls
   DBuf<double> io_in, io_out;
 
@@ -177,8 +187,9 @@ class Fmm {
   template <typename Real>
   void adjoint_impl(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int k0, int R);
   // upward and downward passes of one direction (everything before the leaf stage)
+  // near: the NEAR32 split of the matvec (FP32 X-list sums from str32_)
   template <typename Real>
-  void far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R);
+  void far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R, bool near = false);
   template <typename Real>
   void grad_impl(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs);
   void build_adjoint();

@@ -255,6 +255,99 @@ __global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* 
   for (int c = 0; c < C; ++c) out[(size_t)c * NK] = acc[c];
 }
 
+// Parent-grouped accumulation (see FftFamily): thread (family, frequency k)
+// holds the 8 children's accumulators of one right-hand side at a time; per
+// (P, N) record the 8 source spectra go to this thread's own shared-memory
+// slots, then for each of the 27 values of pos_v - pos_i present in the
+// record the kernel spectrum of offset 2 d + delta is loaded once and applied
+// to every pair with that difference.  Loop bounds and child positions are
+// compile-time, so accumulators stay in registers.  Every right-hand side
+// sums its pairs in the same order, so a pass of R right-hand sides gives
+// each of them bitwise the result of a pass of one.
+template <typename Real>
+__global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
+    int NK, const FftFamily* __restrict__ fams, const FftFamilyPair* __restrict__ pairs,
+    const int* __restrict__ spec_of, const typename Cplx<Real>::t* __restrict__ spec,
+    const typename Cplx<Real>::t* __restrict__ qhat, typename Cplx<Real>::t* __restrict__ chat,
+    const int* __restrict__ tgt_node, const int* __restrict__ nact, int R) {
+  using T2 = typename Cplx<Real>::t;
+  constexpr int BLK = 128;
+  __shared__ T2 sq[24 * BLK];  // this thread's source spectra: [pos * 3 + c][thread]
+  const FftFamily fam = fams[blockIdx.x];
+  const int k = blockIdx.y * BLK + threadIdx.x;
+  if (nact) {
+    int t0 = 0;
+    while (t0 < 7 && fam.tgt[t0] < 0) ++t0;
+    if (!nact[tgt_node[fam.tgt[t0]]]) return;
+  }
+  if (k >= NK) return;
+  const int C = 3 * R;
+  T2* my = sq + threadIdx.x;
+  for (int r = 0; r < R; ++r) {
+  T2 acc[8][3];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[a][c] = cmake((Real)0, (Real)0);
+  for (int pr = fam.first; pr < fam.first + fam.count; ++pr) {
+    const FftFamilyPair rec = pairs[pr];
+    const uint64_t mask = (uint64_t)rec.mask_lo | ((uint64_t)rec.mask_hi << 32);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int sl = rec.src[b];
+      if (sl >= 0) {
+        const T2* Q = qhat + ((size_t)sl * C + 3 * r) * NK + k;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) my[(b * 3 + c) * BLK] = Q[(size_t)c * NK];
+      }
+    }
+    const int dx2 = 2 * (rec.dcode / 9 - 1), dy2 = 2 * ((rec.dcode / 3) % 3 - 1), dz2 = 2 * (rec.dcode % 3 - 1);
+    const int* so = spec_of + (size_t)rec.op * 343;
+#pragma unroll
+    for (int dl = 0; dl < 27; ++dl) {
+      const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
+      uint64_t gm = 0;
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
+        if (bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)
+          gm |= 1ull << (a * 8 + (bx * 4 + by * 2 + bz));
+      }
+      const uint64_t bits = mask & gm;
+      if (bits == 0) continue;
+      const int code = (dx2 + ex + 3) * 49 + (dy2 + ey + 3) * 7 + (dz2 + ez + 3);
+      const T2* Kp = spec + (size_t)so[code] * 6 * NK + k;
+      const T2 kxx = Kp[0], kxy = Kp[NK], kxz = Kp[2 * NK], kyy = Kp[3 * NK], kyz = Kp[4 * NK], kzz = Kp[5 * NK];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
+        if (!(bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)) continue;
+        const int b = bx * 4 + by * 2 + bz;
+        if (!((bits >> (a * 8 + b)) & 1)) continue;
+        const T2 qx = my[(b * 3) * BLK], qy = my[(b * 3 + 1) * BLK], qz = my[(b * 3 + 2) * BLK];
+        cmac(acc[a][0], kxx, qx);
+        cmac(acc[a][0], kxy, qy);
+        cmac(acc[a][0], kxz, qz);
+        cmac(acc[a][1], kxy, qx);
+        cmac(acc[a][1], kyy, qy);
+        cmac(acc[a][1], kyz, qz);
+        cmac(acc[a][2], kxz, qx);
+        cmac(acc[a][2], kyz, qy);
+        cmac(acc[a][2], kzz, qz);
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int t = fam.tgt[a];
+    if (t < 0) continue;
+    T2* out = chat + ((size_t)t * C + 3 * r) * NK + k;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[(size_t)c * NK] = acc[a][c];
+  }
+  }
+}
+
 // ---------------------------------------------------------------- inverse
 // check of one target node at its shell lattice points from C_i: inverse
 // passes along x (G -> res), y (G -> res) and z (half spectrum -> res, real).
@@ -347,6 +440,85 @@ size_t inverse_smem(int G, int res, int R, size_t es) {
   return 2 * es * (G + (size_t)C * res * G * H + (size_t)C * res * res * H);
 }
 
+// The parent-grouped plan (FftFamily): families in parent order, records in
+// colleague order.  Leaves f.family false if some V pair does not join
+// children of two touching parents of one level.
+void build_families(const HostTree& t, const std::vector<int>& tgt, const std::vector<int>& src,
+                    const std::vector<int>& voff, const std::vector<int>& vsrc, const std::vector<int>& node_op,
+                    const std::map<int64_t, int>& spec_slot, size_t nops, FftM2L& f, cudaStream_t st) {
+  f.family = false;
+  f.nfam = 0;
+  if (tgt.empty()) return;
+  auto pos = [&](int32_t c, int32_t p, int d) {
+    const std::vector<int32_t>& v = d == 0 ? t.ix : d == 1 ? t.iy : t.iz;
+    return v[c] - 2 * v[p];
+  };
+  auto pcode = [&](int32_t c, int32_t p) {
+    int code = 0;
+    for (int d = 0; d < 3; ++d) {
+      const int q = pos(c, p, d);
+      if (q < 0 || q > 1) return -1;
+      code = code * 2 + q;
+    }
+    return code;
+  };
+  std::map<int32_t, int> fam_of;                      // parent -> family
+  std::vector<FftFamily> fams;
+  std::vector<std::map<int32_t, FftFamilyPair>> recs;  // per family: colleague -> record
+  for (size_t ts = 0; ts < tgt.size(); ++ts) {
+    const int32_t i = tgt[ts], P = t.parent[i];
+    if (P < 0) return;
+    const int pa = pcode(i, P);
+    if (pa < 0) return;
+    auto it = fam_of.find(P);
+    if (it == fam_of.end()) {
+      it = fam_of.emplace(P, (int)fams.size()).first;
+      FftFamily fm{};
+      for (int a = 0; a < 8; ++a) fm.tgt[a] = -1;
+      fams.push_back(fm);
+      recs.emplace_back();
+    }
+    FftFamily& fm = fams[it->second];
+    fm.tgt[pa] = (int)ts;
+    for (int e = voff[ts]; e < voff[ts + 1]; ++e) {
+      const int32_t v = src[vsrc[e]], N = t.parent[v];
+      if (N < 0 || N == P || t.level[v] != t.level[i] || t.level[N] != t.level[P]) return;
+      const int dx = t.ix[N] - t.ix[P], dy = t.iy[N] - t.iy[P], dz = t.iz[N] - t.iz[P];
+      if (std::abs(dx) > 1 || std::abs(dy) > 1 || std::abs(dz) > 1) return;
+      const int pb = pcode(v, N);
+      if (pb < 0) return;
+      auto& m = recs[it->second];
+      auto rit = m.find(N);
+      if (rit == m.end()) {
+        FftFamilyPair r{};
+        r.dcode = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
+        r.op = node_op[i];
+        for (int b = 0; b < 8; ++b) r.src[b] = -1;
+        rit = m.emplace(N, r).first;
+      }
+      FftFamilyPair& r = rit->second;
+      if (r.op != node_op[i]) return;
+      const int bit = pa * 8 + pb;
+      if (bit < 32) r.mask_lo |= 1u << bit;
+      else r.mask_hi |= 1u << (bit - 32);
+      r.src[pb] = vsrc[e];
+    }
+  }
+  std::vector<FftFamilyPair> pairs;
+  for (size_t fi = 0; fi < fams.size(); ++fi) {
+    fams[fi].first = (int)pairs.size();
+    for (auto& kv : recs[fi]) pairs.push_back(kv.second);
+    fams[fi].count = (int)pairs.size() - fams[fi].first;
+  }
+  std::vector<int> spec_of(std::max<size_t>(nops, 1) * 343, -1);
+  for (const auto& kv : spec_slot) spec_of[(size_t)(kv.first / 343) * 343 + (size_t)(kv.first % 343)] = kv.second;
+  f.fams.upload(fams, st);
+  f.fpairs.upload(pairs, st);
+  f.spec_of.upload(spec_of, st);
+  f.nfam = (int)fams.size();
+  f.family = true;
+}
+
 int optin_smem() {
   int dev = 0, optin = 0;
   NNK_CUDA(cudaGetDevice(&dev));
@@ -382,6 +554,15 @@ void run_fft_m2l(FftM2L& f, const Real* str, long long upbase, int R, Real* chec
   fwd<<<f.nsrc, 256, forward_smem(G, res, R, es), st>>>(G, res, f.P, f.lat.p, f.src_node.p, str, upbase, R, qhat,
                                                         f.NK, nact);
   NNK_CHECK_LAUNCH();
+  if (f.family) {
+    fft_accumulate_family_kernel<Real><<<dim3(f.nfam, (f.NK + 127) / 128), 128, 0, st>>>(
+        f.NK, f.fams.p, f.fpairs.p, f.spec_of.p, spec, qhat, chat, f.tgt_node.p, nact, R);
+    NNK_CHECK_LAUNCH();
+    inv<<<f.ntgt, 256, inverse_smem(G, res, R, es), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, chat, R, check, f.NK,
+                                                          nact);
+    NNK_CHECK_LAUNCH();
+    return;
+  }
   dim3 grid(f.ntgt, (f.NK + 127) / 128);
 #define NNK_FFT_ACC(RR)                                                                                       \
   fft_accumulate_kernel<RR, Real><<<grid, 128, 0, st>>>(f.NK, f.voff.p, f.vsrc.p, f.vspec.p, spec, qhat, chat, \
@@ -479,6 +660,7 @@ void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu
   f.nsrc = (int)src.size();
   f.nspec = (int)slot_w.size();
   f.pairs = (int64_t)vsrc.size();
+  build_families(t, tgt, src, voff, vsrc, node_op, spec_slot, op_w.size(), f, st);
   f.lat.upload(lat, st);
   f.tgt_node.upload(tgt, st);
   f.src_node.upload(src, st);

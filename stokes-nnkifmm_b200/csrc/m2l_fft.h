@@ -24,6 +24,26 @@
 
 namespace nnk {
 
+// Parent-grouped form of the accumulation for one right-hand side: every V
+// pair (i, v) of the reference's lists joins a child i of a parent P with a
+// child v of a colleague N of P (same level, touching P).  One record per
+// (P, N) holds which of the 8 x 8 (child of P, child of N) pairs are V pairs,
+// indexed by child position (x * 4 + y * 2 + z within the parent box), and
+// the direction d = N - P; the pair's offset is 2 d + (pos_v - pos_i).  A
+// thread accumulates all 8 children of P at one frequency: each kernel
+// spectrum it loads serves every pair with the same pos_v - pos_i, and each
+// source spectrum every child of P.
+struct FftFamily {
+  int first, count;  // its (P, N) records
+  int tgt[8];        // target slot of the child at each position (-1 none)
+};
+struct FftFamilyPair {
+  uint32_t mask_lo, mask_hi;  // bit 8 * pos_i + pos_v
+  int dcode;                  // (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)
+  int op;                     // operator (box width) of the children's level
+  int src[8];                 // source slot of N's child at each position (-1 none)
+};
+
 struct FftM2L {
   int res = 0, G = 0, NK = 0, P = 0;
   int nsrc = 0, ntgt = 0, nspec = 0, Rcap = 1;
@@ -39,6 +59,12 @@ struct FftM2L {
   DBuf<float2> qhat;    // nsrc x 3R x NK
   DBuf<float2> chat;    // ntgt x 3R x NK
   DBuf<double2> spec64, qhat64, chat64;
+  // parent-grouped accumulation, when every V pair fits it
+  bool family = false;
+  int nfam = 0;
+  DBuf<FftFamily> fams;
+  DBuf<FftFamilyPair> fpairs;
+  DBuf<int> spec_of;  // per (operator, offset code): spectrum slot (-1 unused)
   size_t fwd_smem = 0, inv_smem = 0;
 };
 

@@ -1,11 +1,12 @@
 // Direct NEAREST velocity evaluation that allocates nothing.
 //
-// Who needs it: callers that must not allocate device memory at call time --
-// code that runs while a CUDA graph is being captured (cudaMalloc is not
-// allowed there), a MATLAB MEX gateway whose device memory is owned by
-// MATLAB's pool, or a real-time loop that has fixed its memory budget up
-// front.  They pass their own device buffers for every input and output; the
-// only scratch this evaluation needs, the fine-point forces g = kron(NN,I3)*f,
+// Who needs it: callers that must not allocate device memory when they call
+// -- a MATLAB MEX gateway whose device memory belongs to MATLAB's own pool
+// (an allocation of ours there competes with MATLAB's and is invisible to
+// it), or a real-time loop that fixed its memory budget up front and must not
+// pay cudaMalloc/cudaFree (which can synchronize the whole device) per step.
+// They pass their own device buffers for every input and output; the only
+// scratch this evaluation needs, the fine-point forces g = kron(NN,I3)*f,
 // lives in the file-scope array below, which every GPU that loads the library
 // holds until the process exits.
 //
@@ -17,14 +18,16 @@
 // calls, and rows past q keep whatever an earlier call left.
 //
 // The first call on a device looks up the array's device address with
-// cudaGetSymbolAddress (once per device, with that device current); make
-// that first call before any stream capture begins.
+// cudaGetSymbolAddress (once per device, with that device current) and keeps
+// it for the life of the process's context on that device (a cudaDeviceReset
+// ends that context and with it the address; this library does not support
+// calls after one).  Make that first call before any stream capture begins.
 #include <cuda_runtime.h>
 
 #include <mutex>
 
 #include "../../include/nnkifmm.h"
-#include "kernels.cuh"
+#include "common.h"
 
 namespace {
 
@@ -87,6 +90,33 @@ __global__ void __launch_bounds__(256) direct_kernel(long long m, const double* 
   }
 }
 
+// The gather of kron(NN,I3)*f into the scratch rows, for column indices the
+// caller supplied on the device and the host cannot see: an index outside
+// [0, n) is not read, and its fine point's force becomes NaN, so every
+// velocity it reaches comes out non-finite instead of from memory out of
+// bounds.
+__global__ void checked_gather_kernel(long long q, const long long* __restrict__ rowptr,
+                                      const int* __restrict__ col, const double* __restrict__ val,
+                                      const double* __restrict__ f, long long n, double* __restrict__ g) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= q) return;
+  double x = 0, y = 0, z = 0;
+  for (long long k = rowptr[e]; k < rowptr[e + 1]; ++k) {
+    const int c = col[k];
+    if (c < 0 || c >= n) {
+      x = y = z = __longlong_as_double(0x7ff8000000000000LL);  // quiet NaN
+      break;
+    }
+    const double w = val[k];
+    x += w * f[3 * (long long)c];
+    y += w * f[3 * (long long)c + 1];
+    z += w * f[3 * (long long)c + 2];
+  }
+  g[3 * e] = x;
+  g[3 * e + 1] = y;
+  g[3 * e + 2] = z;
+}
+
 }  // namespace
 
 extern "C" int nnk_direct_nearest_noalloc(int32_t device, void* stream, const double* forces, int64_t n,
@@ -98,6 +128,15 @@ extern "C" int nnk_direct_nearest_noalloc(int32_t device, void* stream, const do
   if (!(eps > 0) || !(mu > 0)) return NNK_E_ARG;
   if ((n && !forces) || (q && (!nn_rowptr || !nn_col || !nn_val || !fine)) || (m && (!targets || !vel)))
     return NNK_E_ARG;
+  // an error already pending on this thread belongs to the caller: report
+  // it without launching and leave it in place for the caller to read
+  if (cudaPeekAtLastError() != cudaSuccess) return NNK_E_CUDA;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (st && st != cudaStreamLegacy && st != cudaStreamPerThread) {
+    int sdev = -1;
+    if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) return NNK_E_ARG;
+    if (sdev != device) return NNK_E_ARG;  // the stream belongs to another device
+  }
   int prev = 0;
   if (cudaGetDevice(&prev) != cudaSuccess) return NNK_E_CUDA;
   if (prev != device && cudaSetDevice(device) != cudaSuccess) return NNK_E_CUDA;
@@ -113,17 +152,9 @@ extern "C" int nnk_direct_nearest_noalloc(int32_t device, void* stream, const do
     scratch = g_addr[device];
   }
   if (rc == NNK_OK && m > 0) {
-    // the launch check below reads this thread's last runtime error: drop
-    // one left by an earlier call of the library (a destroy function, whose
-    // errors are ignored); a sticky error still shows at the launch
-    (void)cudaGetLastError();
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    nnk::IoMap rows;
-    rows.layout = NNK_LAYOUT_ROWS;
-    rows.nrows = n;
     if (q > 0)
-      nnk::gather_kernel<double><<<(unsigned)((q + 255) / 256), 256, 0, st>>>(
-          (long long)q, (const long long*)nn_rowptr, nn_col, nn_val, forces, rows, 0, 1, scratch);
+      checked_gather_kernel<<<(unsigned)((q + 255) / 256), 256, 0, st>>>(
+          (long long)q, (const long long*)nn_rowptr, nn_col, nn_val, forces, (long long)n, scratch);
     direct_kernel<<<(unsigned)((m + 255) / 256), 256, 0, st>>>((long long)m, targets, (long long)q, fine, scratch,
                                                               eps * eps, 1.0 / (8.0 * M_PI * mu), vel);
     if (cudaGetLastError() != cudaSuccess) rc = NNK_E_CUDA;

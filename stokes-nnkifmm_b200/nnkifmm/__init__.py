@@ -7,7 +7,7 @@ libnnkifmm.so (include/nnkifmm.h).  All FMM work runs on the GPU; the
 library refuses to create an FMM without a CUDA device.
 """
 from ._lib import (NNKError, MaxDepthError, NoConvergence, context, lib, LIB_PATH,  # noqa: F401
-                   LAYOUT_ROWS, LAYOUT_BLOCKED, PREC_FP64, PREC_MIXED)
+                   LAYOUT_ROWS, LAYOUT_BLOCKED, PREC_FP64, PREC_MIXED, PREC_NEAR32)
 from .octree import OcTree, nearestMatrix  # noqa: F401
 from .kifmm import KIFMM  # noqa: F401
 from .mobility import (Swimmers, Mobility, hegedus, mobilityProblem, mobilityProblemGravity,  # noqa: F401

@@ -24,6 +24,7 @@ LAYOUT_ROWS = 1
 LAYOUT_BLOCKED = 2
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_NEAR32 = 2
 NOALLOC_MAX_FINE = 262144
 PHASES = ["gather", "up_pairs", "up_c2e", "down_pairs", "down_c2e", "leaf_pairs", "scatter", "m2l"]
 

@@ -5,7 +5,10 @@
 
 Same name-value options as KIFMM.m:50-60 (``GPU`` and ``parThreads`` are
 accepted for compatibility; the work always runs on the GPU) plus
-``precision`` ('fp64' or 'mixed').  Inputs may be numpy arrays (host) or
+``precision``: 'fp64' (every step in FP64, the reference's operator),
+'near32' (the same operator with the U-list P2P and X-list P2L, whose
+sources are the forces themselves, in FP32) or 'mixed' (FP32 pairs, TF32
+tensor-core M2L, Tikhonov-regularized check-to-equivalent operators).  Inputs may be numpy arrays (host) or
 CUDA torch tensors (device); results come back the same way.
 """
 import ctypes as C
@@ -24,7 +27,7 @@ class KIFMM:
         self.arguments = dict(GPU=GPU, parThreads=parThreads, blockSize=blockSize, GMRES=GMRES,
                               coronaRes=coronaRes, coronaShells=coronaShells, format=format,
                               kernelPar=(eps, mu), precision=precision)
-        prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
+        prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED, "near32": L.PREC_NEAR32}[precision]
         mode = {"auto": 0, "images": 1, "generate": 2, "pairs": 3, "fft": 4}[m2l]
         p = L.FmmParams(eps, mu, int(coronaRes), int(coronaShells), prec, mode, float(reg))
         h = C.c_void_p()

@@ -151,8 +151,33 @@ def split_case():
     np.savez_compressed(os.path.join(OUT, "split_1500_700.npz"), **d)
 
 
+def matvec_case():
+    """The matvec-at-scale distribution (50% uniform in the unit cube, 50% on
+    20 spheres, NEAREST with 4x quadrature, eps = 1e-3, nodeCapacity 64) at
+    4000 force / 16000 quadrature points, drawn by the same seeded generator
+    as the 250k / 1M benchmark (nnkifmm/workloads.py, loaded on its own)."""
+    import importlib.util
+    path = os.path.join(ROOT, "stokes-nnkifmm_b200", "nnkifmm", "workloads.py")
+    spec = importlib.util.spec_from_file_location("nnk_workloads_standalone", path)
+    wl = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(wl)
+    w = wl.matvec_at_scale(4000, 16000)
+    c, f, F = w["coarse"], w["fine"], w["forces"]
+    NN = nearest_matrix(c, f)
+    tree = OcTree(c, c, node_capacity=w["cap"], nearest=1, fine_points=f, NN=NN)
+    t = time.time()
+    vel = KIFMM(tree, w["eps"], w["mu"]).compute_vel(F)
+    direct = apply_kernel(f, c, NN @ F, w["eps"], w["mu"])
+    print(f"matvec 4000/16000: {time.time() - t:.1f}s, nodes {tree.node_count}, "
+          f"fmm vs direct {np.linalg.norm(vel - direct) / np.linalg.norm(direct):.2e}")
+    d = dict(coarse=c, fine=f, F=F, eps=w["eps"], mu=w["mu"], cap=w["cap"], vel=vel, direct=direct)
+    d.update(nn_arrays(NN))
+    d.update(tree_arrays(tree))
+    np.savez_compressed(os.path.join(OUT, "matvec_4000_16000.npz"), **d)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["sphere", "plain", "nearest", "split"]
+    which = sys.argv[1:] or ["sphere", "plain", "nearest", "split", "matvec"]
     if "sphere" in which:
         sphere_case()
     if "plain" in which:
@@ -161,3 +186,5 @@ if __name__ == "__main__":
         adaptive_nearest_case()
     if "split" in which:
         split_case()
+    if "matvec" in which:
+        matvec_case()

@@ -36,7 +36,7 @@ def tree_of(g):
 
 
 FP64_TOL = {"sphere10_40": 1e-6, "adaptive_plain_1600": 1e-6, "adaptive_nearest_1200": 1e-6,
-            "split_1500_700": 1e-6}
+            "split_1500_700": 1e-6, "matvec_4000_16000": 1e-6}
 
 
 @pytest.mark.parametrize("name", sorted(FP64_TOL))
@@ -49,6 +49,44 @@ def test_fp64_matches_oracle(name):
     e = rel(v, g["vel"])
     print(name, "fp64 vs oracle", e, "oracle vs direct", rel(g["vel"], g["direct"]))
     assert e <= FP64_TOL[name]
+
+
+@pytest.mark.parametrize("name", sorted(FP64_TOL))
+def test_near32_matches_fp64_and_oracle(name):
+    """NEAR32: the reference's operator (exact check-to-equivalent inverses,
+    every sum over equivalent densities in FP64) with the U-list P2P and the
+    X-list P2L, whose sources are the forces, in FP32.  Their FP32 rounding
+    reaches the velocities without passing an ill-conditioned inverse
+    amplified, so the result stays within 1e-5 of FP64 mode and of the oracle
+    on every fixture, the ill-posed NEAREST clouds included."""
+    g = load(name)
+    t = tree_of(g)
+    kp = [float(g["eps"]), float(g["mu"])]
+    v64 = nk.KIFMM(t, kp).computeVel(g["F"])
+    fmm = nk.KIFMM(t, kp, precision="near32")
+    fmm.autotune(1)
+    v = fmm.computeVel(g["F"])
+    print(name, "near32 vs fp64", rel(v, v64), "vs oracle", rel(v, g["vel"]))
+    assert rel(v, v64) <= 1e-5 and rel(v, g["vel"]) <= 1e-5
+    two = fmm.computeVel(np.stack([g["F"], -2.0 * g["F"]]), nrhs=2)
+    assert np.array_equal(two[0], v) and rel(two[1], -2.0 * v) <= 1e-12
+
+
+def test_near32_matches_fp64_at_scale():
+    """The matvec-at-scale distribution at 60k force / 240k quadrature points
+    (NEAREST sources outside their leaf boxes make the reference's exact
+    check-to-equivalent solves ill-posed): NEAR32 within 1e-4 of FP64 mode,
+    where the Tikhonov-regularized mixed mode is a different operator."""
+    from nnkifmm.workloads import matvec_at_scale
+    w = matvec_at_scale(60000, 240000)
+    NN = nk.nearestMatrix(w["coarse"], w["fine"])
+    t = nk.OcTree(w["coarse"], w["coarse"], nodeCapacity=64, nearest=1, finePoints=w["fine"], NN=NN)
+    kp, F = [w["eps"], w["mu"]], w["forces"]
+    v64 = nk.KIFMM(t, kp).computeVel(F)
+    v = nk.KIFMM(t, kp, precision="near32").computeVel(F)
+    vm = nk.KIFMM(t, kp, precision="mixed").computeVel(F)
+    print("60k near32 vs fp64", rel(v, v64), "mixed vs fp64", rel(vm, v64))
+    assert rel(v, v64) <= 1e-4
 
 
 @pytest.mark.parametrize("name", ["sphere10_40", "adaptive_plain_1600", "split_1500_700"])
@@ -125,6 +163,20 @@ def test_compressed_m2l_matches_full_operators(name):
     assert rel(a, c) <= max(1.5 * rel(b, c), 2e-5)
     if name in ("sphere10_40", "adaptive_plain_1600"):
         assert rel(a, c) <= 1e-4
+
+
+@pytest.mark.parametrize("name", ["adaptive_nearest_1200", "matvec_4000_16000"])
+def test_fp64_fourier_m2l_matches_fp64_pairs(name):
+    """FP64 mode's Fourier-space M2L (FP64 spectra, the default) against its
+    FP64 pair-kernel M2L: the same operator to rounding, amplified by the
+    exact check-to-equivalent inverses (cond ~2e10)."""
+    g = load(name)
+    t = tree_of(g)
+    kp = [float(g["eps"]), float(g["mu"])]
+    a = nk.KIFMM(t, kp, m2l="pairs").computeVel(g["F"])
+    b = nk.KIFMM(t, kp).computeVel(g["F"])
+    print(name, "fp64 fourier vs fp64 pairs", rel(b, a), "vs oracle", rel(b, g["vel"]), rel(a, g["vel"]))
+    assert rel(b, a) <= 1e-7
 
 
 @pytest.mark.parametrize("name", sorted(FP64_TOL))

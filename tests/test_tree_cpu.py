@@ -62,7 +62,8 @@ def test_tree_sphere_488_points():
     assert_same_tree(OracleTree(c, c, node_capacity=60), nk.OcTree(c, c, nodeCapacity=60))
 
 
-@pytest.mark.parametrize("name", ["sphere10_40", "adaptive_plain_1600", "adaptive_nearest_1200", "split_1500_700"])
+@pytest.mark.parametrize("name", ["sphere10_40", "adaptive_plain_1600", "adaptive_nearest_1200", "split_1500_700",
+                                  "matvec_4000_16000"])
 def test_tree_matches_golden(name):
     g = np.load(os.path.join(GOLDEN, name + ".npz"))
     if "coarse" in g:
@@ -270,3 +271,12 @@ def test_nearest_without_fine_points_rejected():
     x = np.random.default_rng(52).random((40, 3))
     with pytest.raises(ValueError, match="finePoints"):  # the host mirror, before the C ABI
         nk.OcTree(x, x, nodeCapacity=10, nearest=1, builder="host")
+
+
+def test_nearest_matrix_matches_golden_4000_16000():
+    """NN of the matvec-at-scale distribution at 4000 / 16000 points (host
+    builder) against the oracle's fixture, bit for bit."""
+    g = np.load(os.path.join(GOLDEN, "matvec_4000_16000.npz"))
+    A = sp.csr_matrix((g["nn_data"], g["nn_indices"], g["nn_indptr"]), shape=(len(g["fine"]), len(g["coarse"])))
+    B = nk.nearestMatrix(g["coarse"], g["fine"], builder="host")
+    assert (A != B).nnz == 0 and A.nnz == B.nnz

@@ -83,3 +83,21 @@ def test_gpu_nearest_matrix_matches_host(case):
     assert np.array_equal(a.data, b.data)
     if case == "lattice_ties":
         assert np.diff(a.indptr).max() == 8  # the cube centres: 8 nearest corners, weight 1/8
+
+
+def test_gpu_tree_lists_and_nn_match_oracle_4000_16000():
+    """Tree, lists and NN built on the GPU (NN searched on the device, nodes
+    partitioned on the device) for the matvec-at-scale distribution at 4000 /
+    16000 points, against the oracle's fixture directly, bit for bit."""
+    g = np.load(os.path.join(GOLDEN, "matvec_4000_16000.npz"))
+    NN = nk.nearestMatrix(g["coarse"], g["fine"])
+    A = sp.csr_matrix((g["nn_data"], g["nn_indices"], g["nn_indptr"]), shape=NN.shape)
+    assert (A != NN).nnz == 0 and A.nnz == NN.nnz
+    t = nk.OcTree(g["coarse"], g["coarse"], nodeCapacity=int(g["cap"]), nearest=1, finePoints=g["fine"])
+    assert (t.NN != A).nnz == 0
+    assert np.array_equal(t.nodeLevel, g["level"]) and np.array_equal(t.nodeParents, g["parent"])
+    assert np.array_equal(t.nodeChildren, g["children"]) and np.array_equal(t.nodeCorners, g["corners"])
+    assert np.array_equal(t.pointIndex, g["point_index"])
+    for k, name in enumerate("UVWX"):
+        off, ids = t.interaction_list(k)
+        assert np.array_equal(off, g[f"list_{name}_off"]) and np.array_equal(ids, g[f"list_{name}_ids"]), name

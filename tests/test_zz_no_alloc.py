@@ -1,8 +1,9 @@
 """The allocation-free entry point nnk_direct_nearest_noalloc, through the C ABI.
 
-Some callers cannot allocate device memory at call time (a CUDA graph being
-captured, a MATLAB MEX gateway whose device memory MATLAB owns, a loop with a
-fixed memory budget).  This entry point evaluates the NEAREST velocity by
+Some callers cannot allocate device memory at call time (a MATLAB MEX
+gateway whose device memory belongs to MATLAB's pool, a loop with a fixed
+memory budget that must not pay cudaMalloc/cudaFree and their device
+synchronization per step).  This entry point evaluates the NEAREST velocity by
 direct summation using only caller-supplied device buffers plus a static
 scratch array inside the library.  Here it is compared, on two calls in a row
 with different forces, with the existing allocating entry point computeVel
@@ -63,3 +64,36 @@ def test_noalloc_rejects_too_many_fine_points():
     n = L.NOALLOC_MAX_FINE + 1
     rc = L.lib.nnk_direct_nearest_noalloc(0, None, 1, 1, 1, 1, 1, 1, n, 1, 1, 1e-3, 1.0, 1)
     assert rc == L.NNK_E_ARG
+
+
+def test_noalloc_empty_inputs_and_bad_columns():
+    """q = 0 gives zero velocities, m = 0 does nothing, and a column index
+    outside [0, n) turns the velocities it reaches into NaN instead of reading
+    out of bounds."""
+    import torch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    d = lambda a, dt=torch.float64: torch.tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+    rng = np.random.default_rng(5)
+    F, tgt = d(rng.standard_normal((4, 3))), d(rng.random((3, 3)))
+    vel = torch.full((3, 3), 7.0, dtype=torch.float64, device=dev)
+    rp0 = d(np.zeros(1, np.int64), torch.int64)
+    one = d(np.zeros(1, np.int32), torch.int32)
+    rc = L.lib.nnk_direct_nearest_noalloc(0, stream, F.data_ptr(), 4, rp0.data_ptr(), one.data_ptr(),
+                                          F.data_ptr(), F.data_ptr(), 0, tgt.data_ptr(), 3, 1e-3, 1.0,
+                                          vel.data_ptr())
+    assert rc == L.NNK_OK
+    torch.cuda.synchronize()
+    assert torch.count_nonzero(vel).item() == 0
+    assert L.lib.nnk_direct_nearest_noalloc(0, stream, F.data_ptr(), 4, rp0.data_ptr(), one.data_ptr(),
+                                            F.data_ptr(), F.data_ptr(), 0, None, 0, 1e-3, 1.0, None) == L.NNK_OK
+    fine = d(rng.random((2, 3)))
+    rp = d(np.array([0, 1, 2], np.int64), torch.int64)
+    col = d(np.array([1, 4], np.int32), torch.int32)  # 4 is outside [0, 4)
+    val = d(np.array([1.0, 1.0]))
+    rc = L.lib.nnk_direct_nearest_noalloc(0, stream, F.data_ptr(), 4, rp.data_ptr(), col.data_ptr(),
+                                          val.data_ptr(), fine.data_ptr(), 2, tgt.data_ptr(), 3, 1e-3, 1.0,
+                                          vel.data_ptr())
+    assert rc == L.NNK_OK
+    torch.cuda.synchronize()
+    assert torch.isnan(vel).all().item()
