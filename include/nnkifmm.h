@@ -271,6 +271,16 @@ int nnk_fmm_source_count(const nnk_fmm* fmm, int64_t* count);
  * forces and weights in `layout`; either output may be NULL. */
 int nnk_fmm_grad_positions(nnk_fmm* fmm, const double* forces, const double* weights, int32_t layout,
                            double* grad_targets, double* grad_sources, int32_t on_device);
+/* *out = weights^T (dF/deps) forces for the FMM operator F (FP64 with the
+ * exact check-to-equivalent inverses, reg = 0; NNK_E_STATE otherwise): every
+ * stage differentiated -- the kernel's eps-derivative (Tools/kernel.m:29-47
+ * differentiated) in every pair sum and in the M2L, and
+ * d(K^-1)/deps = -K^-1 (dK/deps) K^-1 in the check-to-equivalent solves --
+ * and contracted with the matvec's inputs to the stage and the transpose
+ * pass's sensitivities of its output.  Costs one matvec, one transpose and
+ * one derivative pass.  forces and weights in `layout`. */
+int nnk_fmm_grad_eps(nnk_fmm* fmm, const double* forces, const double* weights, int32_t layout, double* out,
+                     int32_t on_device);
 
 int nnk_fmm_profile(nnk_fmm* fmm, int32_t enable);
 int nnk_fmm_profile_read(nnk_fmm* fmm, double* ms, int64_t* launches);
@@ -338,6 +348,12 @@ int nnk_mob_solve_adjoint(nnk_mob* mob, const double* rhs, double* x, const nnk_
  * NN is held fixed (it is piecewise constant in the positions). */
 int nnk_mob_grad_positions(nnk_mob* mob, const double* z, const double* lam, double* grad_points,
                            double* grad_fine, int32_t on_device);
+/* *out = -lam^T (dA/deps) z, the eps part of a loss gradient (only the FMM
+ * block of the mobility matrix depends on eps), through nnk_fmm_grad_eps of
+ * `fp64` -- an exact FP64 FMM on the mobility object's tree -- or of the
+ * mobility object's own FMM when fp64 is NULL. */
+int nnk_mob_grad_eps(nnk_mob* mob, nnk_fmm* fp64, const double* z, const double* lam, double* out,
+                     int32_t on_device);
 int nnk_mob_destroy(nnk_mob* mob);
 
 /* ---------------------------------------------------- batched mobility -- */

@@ -438,6 +438,22 @@ int nnk_fmm_profile_read(nnk_fmm* fmm, double* ms, int64_t* launches) {
   API_CATCH(ctx)
 }
 
+int nnk_fmm_grad_eps(nnk_fmm* fmm, const double* forces, const double* weights, int32_t layout, double* out,
+                     int32_t on_device) {
+  if (!fmm || !forces || !weights || !out || (layout != NNK_LAYOUT_ROWS && layout != NNK_LAYOUT_BLOCKED))
+    return fail(fmm ? fmm->ctx : nullptr, NNK_E_ARG, "bad arguments");
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  nnk::Fmm& F = *fmm->f;
+  const nnk::HostTree& t = F.tree();
+  nnk::DBuf<double> wbuf;
+  const double* df = stage_in(ctx, F.io_in, forces, 3 * (size_t)t.n_pot, on_device);
+  const double* dw = stage_in(ctx, wbuf, weights, 3 * (size_t)t.n_tgt, on_device);
+  *out = F.grad_eps(df, dw, layout);
+  API_CATCH(ctx)
+}
+
 int nnk_fmm_test_wait_timeout(nnk_fmm* fmm, uint32_t polls) {
   if (!fmm || polls == 0) return fail(fmm ? fmm->ctx : nullptr, NNK_E_ARG, "bad arguments");
   nnk_ctx* ctx = fmm->ctx;
@@ -637,6 +653,25 @@ int nnk_mob_grad_positions(nnk_mob* mob, const double* z, const double* lam, dou
     if (gy) NNK_CUDA(cudaMemcpyAsync(grad_fine, gy, ny * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     NNK_CUDA(cudaStreamSynchronize(ctx->stream));
   }
+  API_CATCH(ctx)
+}
+
+int nnk_mob_grad_eps(nnk_mob* mob, nnk_fmm* fp64, const double* z, const double* lam, double* out,
+                     int32_t on_device) {
+  if (!mob || !z || !lam || !out) return NNK_E_ARG;
+  nnk_ctx* ctx = mob->fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  if (fp64 && &fp64->f->tree() != &mob->fmm->f->tree())
+    return fail(ctx, NNK_E_ARG, "the FMM must share the mobility tree");
+  nnk::Mobility& M = *mob->m;
+  nnk::Fmm& F = fp64 ? *fp64->f : *mob->fmm->f;
+  const size_t n = (size_t)M.size();
+  nnk::DBuf<double> lbuf;
+  const double* dz = stage_in(ctx, M.io_in, z, n, on_device);
+  const double* dl = stage_in(ctx, lbuf, lam, n, on_device);
+  // [f (3N, blocked) | U | Omega]: the FMM block reads the first 3N values
+  *out = -F.grad_eps(dz, dl, NNK_LAYOUT_BLOCKED);
   API_CATCH(ctx)
 }
 

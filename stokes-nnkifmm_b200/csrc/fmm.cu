@@ -67,6 +67,39 @@ void kernel_matrix(const std::vector<double>& src, const std::vector<double>& tg
     }
 }
 
+// dS/deps (Tools/kernel.m:23-47 differentiated), the layout of kernel_matrix:
+//   eps [(r^2 - 2 eps^2) I - 3 r r^T] / (8 pi mu (r^2 + eps^2)^{5/2}).
+void kernel_deriv_matrix(const std::vector<double>& src, const std::vector<double>& tgt, double eps, double mu,
+                         std::vector<double>& Kcm, int ld) {
+  const size_t ns = src.size() / 3, nt = tgt.size() / 3;
+  const double c = eps / (8.0 * M_PI * mu), e2 = eps * eps;
+  for (size_t a = 0; a < nt; ++a)
+    for (size_t b = 0; b < ns; ++b) {
+      const double r[3] = {tgt[3 * a] - src[3 * b], tgt[3 * a + 1] - src[3 * b + 1],
+                           tgt[3 * a + 2] - src[3 * b + 2]};
+      const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      const double inv = c / std::pow(r2 + e2, 2.5);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          Kcm[(3 * b + j) * (size_t)ld + 3 * a + i] = ((i == j ? r2 - 2 * e2 : 0.0) - 3 * r[i] * r[j]) * inv;
+    }
+}
+
+__global__ void dot_partial_kernel(long long n, const double* __restrict__ a, const double* __restrict__ b,
+                                   double* __restrict__ part) {
+  __shared__ double red[256];
+  double s = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s += a[i] * b[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
 struct Solver {
   cusolverDnHandle_t s = nullptr;
   cublasHandle_t b = nullptr;
@@ -703,6 +736,8 @@ void Fmm::build_operators() {
   // FP64 mode uses the exact inverse (the reference's LU solve) unless a
   // Tikhonov weight is given; mixed mode always regularizes.
   const bool exact = f64() && !(p_.reg > 0);
+  exact_ops_ = exact;
+  deps_ready_ = false;
   const double reg = p_.reg > 0 ? p_.reg : 1e-5;
   // host part, in parallel over operators: K_up = kernel(upsurf, downsurf)
   // (up-equivalent densities -> down check) and, for the Tikhonov form,
@@ -854,6 +889,8 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
                        na);
     });
   }
+  if (save_up_) NNK_CUDA(cudaMemcpyAsync(save_up_, check, sizeof(Real) * (size_t)N_ * n * R, cudaMemcpyDeviceToDevice,
+                                         st));
   // downward pass
   if (tm) {
     // M2L of every level at once: the V-list only reads up densities
@@ -1178,6 +1215,141 @@ int Fmm::rhs_cap(bool adjoint) const {
   if (fast && tensor_m2l_) return 1;
   if (fast && fft_m2l_) return std::min(R_, fft_.Rcap);
   return R_;
+}
+
+// A deterministic FP64 dot product on the device (fixed blocks, partial
+// sums added on the host in block order).
+double Fmm::dot_dev(const double* a, const double* b, int64_t n) {
+  constexpr int kBlocks = 592;  // 4 per SM
+  if (gpart_.n < (size_t)kBlocks) gpart_.alloc(kBlocks);
+  cudaStream_t st = ctx_->stream;
+  dot_partial_kernel<<<kBlocks, 256, 0, st>>>((long long)n, a, b, gpart_.p);
+  NNK_CHECK_LAUNCH();
+  std::vector<double> h(kBlocks);
+  NNK_CUDA(cudaMemcpyAsync(h.data(), gpart_.p, sizeof(double) * kBlocks, cudaMemcpyDeviceToHost, st));
+  NNK_CUDA(cudaStreamSynchronize(st));
+  double s = 0;
+  for (double v : h) s += v;
+  return s;
+}
+
+// dA/deps = -A (dK/deps) A per operator (A = K^-1, K = kernel(upsurf,
+// downsurf) of the box width), and the M2L's derivative spectra.
+void Fmm::build_deps() {
+  if (deps_ready_) return;
+  const int n = 3 * P_;
+  cudaStream_t st = ctx_->stream;
+  auto lat = shell_lattice(p_.res, p_.shells);
+  std::vector<std::vector<double>> dKs(nops_);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int o = 0; o < nops_; ++o) {
+    const double w = op_w_[o];
+    const double lo[3] = {0, 0, 0}, hi[3] = {w, w, w};
+    const double dlo[3] = {-w, -w, -w}, dhi[3] = {2 * w, 2 * w, 2 * w};
+    std::vector<double> us(3 * P_), ds(3 * P_);
+    surface(lo, hi, p_.res, lat, us.data());
+    surface(dlo, dhi, p_.res, lat, ds.data());
+    dKs[o].assign((size_t)n * n, 0.0);
+    kernel_deriv_matrix(us, ds, p_.eps, p_.mu, dKs[o], n);
+  }
+  Solver sv(st);
+  dops_.alloc((size_t)nops_ * n * n);
+  DBuf<double> dK((size_t)n * n), T((size_t)n * n);
+  for (int o = 0; o < nops_; ++o) {
+    NNK_CUDA(cudaMemcpyAsync(dK.p, dKs[o].data(), dKs[o].size() * 8, cudaMemcpyHostToDevice, st));
+    const double* A = ops_.p + (size_t)o * n * n;
+    const double one = 1.0, zero = 0.0, mone = -1.0;
+    if (cublasDgemm(sv.b, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, dK.p, n, A, n, &zero, T.p, n) !=
+            CUBLAS_STATUS_SUCCESS ||
+        cublasDgemm(sv.b, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &mone, A, n, T.p, n, &zero, dops_.p + (size_t)o * n * n,
+                    n) != CUBLAS_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "dA/deps products failed");
+    NNK_CUDA(cudaStreamSynchronize(st));  // dKs[o] is pageable host memory
+  }
+  if (fft_m2l_) build_fft_deriv(fft_, p_.eps, p_.mu, st);
+  const int64_t nt = (int64_t)t_->tgt_row.size();
+  const size_t nc = (size_t)N_ * n;
+  gsave_cup_.alloc(nc);
+  gsave_d_.alloc(nc);
+  gsave_avt_.alloc(nc);
+  gdchk_.alloc(nc);
+  gdscr_.alloc(nc);
+  gdvel_.alloc(std::max<size_t>(3 * (size_t)nt, 1));
+  NNK_CUDA(cudaStreamSynchronize(st));
+  deps_ready_ = true;
+}
+
+double Fmm::grad_eps(const double* d_f, const double* d_w, int layout) {
+  const HostTree& t = *t_;
+  if (!f64() || near32() || !exact_ops_)
+    throw Error(NNK_E_STATE, "the eps-derivative needs an FP64 FMM with the exact check-to-equivalent inverses");
+  if (t.groups() > 1) throw Error(NNK_E_STATE, "the eps-derivative is for a single tree");
+  if (t.n_tgt == 0 || t.n_pot == 0) return 0.0;
+  build_adjoint();
+  build_deps();
+  cudaStream_t st = ctx_->stream;
+  const int n = 3 * P_;
+  const size_t nc = (size_t)N_ * n;
+  const int64_t nt = (int64_t)t.tgt_row.size();
+  IoMap fin, win;
+  fin.layout = win.layout = layout;
+  fin.nrows = t.n_pot;
+  win.nrows = t.n_tgt;
+  const double e2 = p_.eps * p_.eps, sc = p_.eps / (8.0 * M_PI * p_.mu);
+  // forward pass: f, u, v stay in str64_; the up and down check potentials are saved
+  launch_gather<double>(E_, goff_.p, gidx_.p, gw_.p, d_f, fin, 0, 1, str64_.p, st);
+  NNK_CUDA(cudaMemsetAsync(check64_.p, 0, sizeof(double) * nc, st));
+  save_up_ = gsave_cup_.p;
+  far_field<double>(fwd_, pos64_.p, str64_.p, E_, 1);
+  save_up_ = nullptr;
+  NNK_CUDA(cudaMemcpyAsync(gsave_d_.p, check64_.p, sizeof(double) * nc, cudaMemcpyDeviceToDevice, st));
+  // transpose pass: its up checks are the sensitivities of the down
+  // densities, its up densities those of the down checks, its down checks
+  // those of the up densities and its down densities those of the up checks
+  launch_gather<double>(nt, agoff_.p, agidx_.p, agw_.p, d_w, win, 0, 1, astr64_.p, st);
+  NNK_CUDA(cudaMemsetAsync(check64_.p, 0, sizeof(double) * nc, st));
+  save_up_ = gsave_avt_.p;
+  far_field<double>(adj_, apos64_.p, astr64_.p, nt, 1);
+  save_up_ = nullptr;
+  const double* adj_up = astr64_.p + 3 * nt;                          // sensitivities of the down checks
+  const double* adj_dn = astr64_.p + 3 * (nt + (int64_t)P_ * N_);     // sensitivities of the up checks
+  auto deps_group = [&](const TaskGroup& g, const double* tpos, double* out) {
+    if (g.count == 0) return;
+    launch_p2p_deps(fwd_.tasks.p + g.first, (int)g.count, fwd_.segs.p, pos64_.p, str64_.p, tpos, out, partial64_.p,
+                    e2, sc, st, 1);
+    if (g.red_count) launch_reduce<double>(fwd_.reds.p + g.red_first, (int)g.red_count, partial64_.p, out, 1, st, 1);
+  };
+  double g = 0;
+  // S2M and M2M with dS/deps, against the up checks' sensitivities
+  NNK_CUDA(cudaMemsetAsync(gdchk_.p, 0, sizeof(double) * nc, st));
+  for (int L = maxl_; L >= 1; --L) deps_group(fwd_.up[L], pos64_.p, gdchk_.p);
+  g += dot_dev(gdchk_.p, adj_dn, (int64_t)nc);
+  // M2L (Fourier, derivative spectra, or V pairs), P2L and L2L, against the down checks' sensitivities
+  NNK_CUDA(cudaMemsetAsync(gdchk_.p, 0, sizeof(double) * nc, st));
+  if (fft_m2l_) launch_fft_m2l_deriv(fft_, str64_.p, E_, gdchk_.p, st);
+  for (int L = 1; L <= maxl_; ++L) deps_group(fft_m2l_ ? fwd_.down_nov[L] : fwd_.down[L], pos64_.p, gdchk_.p);
+  g += dot_dev(gdchk_.p, adj_up, (int64_t)nc);
+  // L2T, P2P and M2T with dS/deps, against the weights
+  NNK_CUDA(cudaMemsetAsync(gdvel_.p, 0, sizeof(double) * 3 * nt, st));
+  deps_group(fwd_.leaf, tpos64_.p, gdvel_.p);
+  g += dot_dev(gdvel_.p, astr64_.p, 3 * nt);
+  // check-to-equivalent solves: <sens(u), dA c> over the up nodes and
+  // <sens(v), dA^T d> over the nodes below the root
+  NNK_CUDA(cudaMemsetAsync(gdscr_.p, 0, sizeof(double) * nc, st));
+  for (int L = maxl_; L >= 1; --L) {
+    const int64_t ntl = fwd_.up_toff[L + 1] - fwd_.up_toff[L];
+    launch_c2e<double>(dops_.p, n, 0, fwd_.up_tiles.p + fwd_.up_toff[L], (int)ntl, fwd_.up_nodes.p, gsave_cup_.p,
+                       gdscr_.p, 0, P_, 1, st, nullptr, 0, c2e_part_.p, c2e_part_.n);
+  }
+  g += dot_dev(gdscr_.p, check64_.p, (int64_t)nc);
+  NNK_CUDA(cudaMemsetAsync(gdscr_.p, 0, sizeof(double) * nc, st));
+  for (int L = 1; L <= maxl_; ++L) {
+    const int64_t ntl = dn_toff_[L + 1] - dn_toff_[L];
+    launch_c2e<double>(dops_.p, n, 1, dn_tiles_.p + dn_toff_[L], (int)ntl, lvl_nodes_.p, gsave_d_.p, gdscr_.p, 0, P_,
+                       1, st, nullptr, 0, c2e_part_.p, c2e_part_.n);
+  }
+  g += dot_dev(gdscr_.p, gsave_avt_.p, (int64_t)nc);
+  return g;
 }
 
 int64_t Fmm::source_origins() const { return t_->params.nearest ? t_->q : t_->n_pot; }

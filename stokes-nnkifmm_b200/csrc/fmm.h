@@ -132,6 +132,15 @@ class Fmm {
   // (n_tgt x 3, target order) and at the sources (potential rows in plain
   // mode, fine points in NEAREST mode; n x 3).  Either output may be null.
   void grad_positions(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs);
+  // w^T (dF/deps) f for the FMM operator F of this object (FP64 with the
+  // exact check-to-equivalent inverses): every stage's derivative -- the
+  // kernel's eps-derivative in each pair sum and in the M2L, and
+  // d(K^-1)/deps = -K^-1 (dK/deps) K^-1 of the check-to-equivalent solves --
+  // contracted with the forward pass's inputs to the stage and the
+  // transpose pass's sensitivities of its output (one forward, one
+  // transpose and one derivative pass).  f at the potentials, w at the
+  // targets, both in `layout`.
+  double grad_eps(const double* d_f, const double* d_w, int layout);
   int64_t source_origins() const;
   // Rebuild every eps-dependent part (check-to-equivalent operators, M2L
   // images or spectra) for a new eps; the tree-dependent task lists stay.
@@ -194,6 +203,14 @@ class Fmm {
   void grad_impl(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs);
   void build_adjoint();
   int rhs_cap(bool adjoint) const;
+  void build_deps();
+  double dot_dev(const double* a, const double* b, int64_t n);
+  // eps-derivative (grad_eps): dA/deps per operator, saved pass quantities
+  bool deps_ready_ = false;
+  bool exact_ops_ = false;
+  DBuf<double> dops_;
+  DBuf<double> gsave_cup_, gsave_d_, gsave_avt_, gdchk_, gdvel_, gdscr_, gpart_;
+  double* save_up_ = nullptr;  // far_field copies the up pass's check potentials here when set
   void build_taskset(TaskSet& ts, const TaskRoles& roles, bool stats);
   void build_points();
   void build_tasks();

@@ -96,7 +96,11 @@ template <typename Real> struct Vec4T;
 template <> struct Vec4T<float> { using t4 = float4; using t2 = float2; };
 template <> struct Vec4T<double> { using t4 = double4; using t2 = double2; };
 
-template <typename Real>
+// KD = true: the kernel's derivative with respect to eps (times 1/eps, the
+// caller folds eps into `scale`):
+//   dS/deps = eps [(r^2 - 2 eps^2) I - 3 r r^T] / (8 pi mu D^{5/2}),  D = r^2 + eps^2
+// (Tools/kernel.m:29-47 differentiated).
+template <typename Real, bool KD = false>
 __device__ __forceinline__ void pair_acc(Real tx, Real ty, Real tz, const typename Vec4T<Real>::t4& s4,
                                          const typename Vec4T<Real>::t2& s2, Real e2, Real& ax, Real& ay,
                                          Real& az) {
@@ -105,14 +109,21 @@ __device__ __forceinline__ void pair_acc(Real tx, Real ty, Real tz, const typena
   const Real d = r2 + e2;
   const Real inv = rsq(d);
   const Real inv3 = inv * inv * inv;
-  const Real a = e2 * inv3 + inv;  // (r^2 + 2 eps^2) / d^{3/2} = d^{-1/2} + eps^2 d^{-3/2}
-  const Real b = (dx * s4.w + dy * s2.x + dz * s2.y) * inv3;
+  Real a, b;
+  if (KD) {
+    const Real inv5 = inv3 * inv * inv;
+    a = (r2 - 2 * e2) * inv5;
+    b = -3 * (dx * s4.w + dy * s2.x + dz * s2.y) * inv5;
+  } else {
+    a = e2 * inv3 + inv;  // (r^2 + 2 eps^2) / d^{3/2} = d^{-1/2} + eps^2 d^{-3/2}
+    b = (dx * s4.w + dy * s2.x + dz * s2.y) * inv3;
+  }
   ax += a * s4.w + b * dx;
   ay += a * s2.x + b * dy;
   az += a * s2.y + b * dz;
 }
 
-template <typename Real, int BS>
+template <typename Real, int BS, bool KD = false>
 __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks,
                                                  const SegD* __restrict__ segs,
                                                  const Real* __restrict__ spos,
@@ -195,7 +206,7 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
         if (f0 + BS + tid < total) fetch(f0 + BS + tid, pa, pb);
         const int nj = min(BS, total - f0);
         if (act0) {
-          if constexpr (std::is_same<Real, float>::value) {
+          if constexpr (std::is_same<Real, float>::value && !KD) {
             // the two targets in the two lanes of packed FP32 arithmetic
             const float2 X = make_float2(tx, ux), Y = make_float2(ty, uy), Z = make_float2(tz, uz);
             const float2 E = make_float2(e2, e2);
@@ -233,8 +244,8 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
             for (int j = ms; j < nj; j += splits) {
               const T4 a = s4[j];
               const T2 b = s2[j];
-              pair_acc<Real>(tx, ty, tz, a, b, e2, ax, ay, az);
-              pair_acc<Real>(ux, uy, uz, a, b, e2, bx, by, bz);  // dummy target (0,0,0) when !act1
+              pair_acc<Real, KD>(tx, ty, tz, a, b, e2, ax, ay, az);
+              pair_acc<Real, KD>(ux, uy, uz, a, b, e2, bx, by, bz);  // dummy target (0,0,0) when !act1
             }
           }
         }
@@ -545,6 +556,17 @@ inline void launch_p2p(const TaskD* tasks, int ntasks, const SegD* segs, const R
     launch_p2p_bs<Real, 256>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R, nact);
   else
     launch_p2p_bs<Real, 128>(tasks, ntasks, segs, spos, sstr, tpos, out, partial, e2, scale, st, accumulate, R, nact);
+  NNK_CHECK_LAUNCH();
+}
+
+// Pair sums with the kernel's eps-derivative (one right-hand side, FP64):
+// out = sum (dS/deps) str over the tasks' sources, `scale` = eps / (8 pi mu).
+inline void launch_p2p_deps(const TaskD* tasks, int ntasks, const SegD* segs, const double* spos,
+                            const double* sstr, const double* tpos, double* out, double* partial, double e2,
+                            double scale, cudaStream_t st, int accumulate) {
+  if (ntasks == 0) return;
+  p2p_kernel<double, 128, true><<<ntasks, 128, 0, st>>>(tasks, segs, spos, sstr, tpos, out, partial, e2, scale,
+                                                        accumulate, nullptr);
   NNK_CHECK_LAUNCH();
 }
 

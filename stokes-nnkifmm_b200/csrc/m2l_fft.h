@@ -59,6 +59,9 @@ struct FftM2L {
   DBuf<float2> qhat;    // nsrc x 3R x NK
   DBuf<float2> chat;    // ntgt x 3R x NK
   DBuf<double2> spec64, qhat64, chat64;
+  DBuf<double2> dspec64;  // spectra of the kernel's eps-derivative (built on demand)
+  std::vector<double> slot_w_host;  // per spectrum: box width
+  std::vector<int> slot_code_host;  // per spectrum: offset code
   // parent-grouped accumulation, when every V pair fits it
   bool family = false;
   int nfam = 0;
@@ -83,5 +86,9 @@ void launch_fft_m2l(FftM2L& f, const float* str, long long upbase, int R, float*
                     const int* nact = nullptr);
 void launch_fft_m2l(FftM2L& f, const double* str, long long upbase, int R, double* check, cudaStream_t st,
                     const int* nact = nullptr);
+// The same M2L with the kernel's eps-derivative (FP64 plans, one right-hand
+// side); build_fft_deriv computes its spectra.
+void build_fft_deriv(FftM2L& f, double eps, double mu, cudaStream_t st);
+void launch_fft_m2l_deriv(FftM2L& f, const double* str, long long upbase, double* check, cudaStream_t st);
 
 }  // namespace nnk

@@ -421,7 +421,8 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
       if (t.is_pot[pt]) t.pleaf[i] = 1;
     }
   }
-  build_lists(t);
+  if (gpu) build_lists_gpu(gpu, t);
+  else build_lists(t);
 
   // ---- targets sorted by leaf (downwardPass.m:297-305 scatter order)
   t.tgt_start.assign(N + 1, 0);

@@ -105,6 +105,9 @@ void nearest_matrix_gpu(struct ::nnk_ctx* ctx, const double* coarse, int64_t n, 
 // two trees, so the FMM of the forest is the block-diagonal operator of the
 // separate trees.  A tree may appear several times.
 void merge_forest(const std::vector<const HostTree*>& trees, HostTree& out);
+// The U/V/W/X lists of a tree whose node arrays are built (lists_gpu.cu),
+// identical to the host builder's.
+void build_lists_gpu(struct ::nnk_ctx* ctx, HostTree& t);
 
 // nearestMatrix (Tools/Nearest/nearestMatrix.m:17-41), exact FP64 ties.
 // Rewrites the tie weights of a nearest-neighbour matrix (CSR by fine point,

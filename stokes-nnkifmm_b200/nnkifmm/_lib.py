@@ -93,6 +93,7 @@ SIGNATURES = {
     "nnk_fmm_set_eps": (_i32, [_vp, _f64]),
     "nnk_fmm_autotune": (_i32, [_vp, _i32, _pd, _pd]),
     "nnk_fmm_grad_positions": (_i32, [_vp, _vp, _vp, _i32, _vp, _vp, _i32]),
+    "nnk_fmm_grad_eps": (_i32, [_vp, _vp, _vp, _i32, _pd, _i32]),
     "nnk_fmm_profile": (_i32, [_vp, _i32]),
     "nnk_fmm_profile_read": (_i32, [_vp, _vp, _vp]),
     "nnk_fmm_test_wait_timeout": (_i32, [_vp, C.c_uint32]),
@@ -107,6 +108,7 @@ SIGNATURES = {
     "nnk_mob_apply_fmm": (_i32, [_vp, _vp, _vp, _vp, _i32]),
     "nnk_mob_solve_adjoint": (_i32, [_vp, _vp, _vp, C.POINTER(SolveParams), C.POINTER(SolveInfo), _i32]),
     "nnk_mob_grad_positions": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32]),
+    "nnk_mob_grad_eps": (_i32, [_vp, _vp, _vp, _vp, _pd, _i32]),
     "nnk_mob_destroy": (_i32, [_vp]),
     "nnk_batch_create": (_i32, [_vp, _i32, _vp, _vp, _vp, C.POINTER(FmmParams), _i32, C.POINTER(_vp)]),
     "nnk_batch_layout": (_i32, [_vp, _pi64, _vp]),

@@ -13,10 +13,14 @@ reference's path.  Backward, for a loss L(z) of the solution z = [f; U; Om]:
     derivative evaluated through the FMM's leaf stages and the rigid-body
     blocks (nnk_mob_grad_positions); NN is held fixed (piecewise constant in
     the positions);
-  * dL/deps = -lam^T (dA/deps) z, with dA/deps z the central difference of
-    two FMM matvecs at eps (1 +- 1e-4) (the operators rebuilt at each eps).
-In mixed precision the solves use FP32 pairs with FP64 refinement, and the
-eps-difference uses FP64 operators with the same Tikhonov weight.
+  * dL/deps = -lam^T (dA/deps) z by the analytic eps-derivative of the FMM
+    (nnk_mob_grad_eps): the kernel's eps-derivative in every pair sum and in
+    the M2L, and d(K^-1)/deps of the check-to-equivalent solves, contracted
+    with the forward and transpose passes' quantities, on an FP64 FMM with
+    the exact inverses (the mobility object's own in FP64 mode).  With
+    Tikhonov operators (reg > 0) it is the central difference of two FP64
+    matvecs at eps (1 +- 1e-3) instead.
+In mixed precision the solves use FP32 pairs with FP64 refinement.
 """
 import numpy as np
 import torch
@@ -59,20 +63,19 @@ class _RigidVelocity(torch.autograd.Function):
         if flag != 0:
             raise RuntimeError(f"adjoint GMRES stopped at relres {relres:.3e} after {it} iterations")
         gX, gY = mob.grad_positions(z, lam)
-        # dA/deps z by a central difference of FP64 matvecs on Tikhonov
-        # operators: the exact inverse (condition ~1e10) would put its rounding
-        # into the difference; the regularized FMM differs from it by the FMM
-        # approximation only, smoothly in eps
-        d = 1e-3 * e
-        f64 = getattr(sw, "FMM64", None)
-        if f64 is None:
-            f64 = KIFMM(sw.Tree, [e, opts["mu"]], GMRES=1, format=2, precision="fp64", reg=opts["reg"] or 1e-5)
-        f64.setEps(e + d)
-        Ap = mob.apply_with(f64, z)
-        f64.setEps(e - d)
-        Am = mob.apply_with(f64, z)
-        f64.setEps(e)
-        geps = -float(lam @ (Ap - Am)) / (2 * d)
+        if opts["reg"] > 0:
+            # Tikhonov operators: a central difference of two FP64 matvecs
+            d = 1e-3 * e
+            f64 = KIFMM(sw.Tree, [e, opts["mu"]], GMRES=1, format=2, precision="fp64", reg=opts["reg"])
+            f64.setEps(e + d)
+            Ap = mob.apply_with(f64, z)
+            f64.setEps(e - d)
+            Am = mob.apply_with(f64, z)
+            geps = -float(lam @ (Ap - Am)) / (2 * d)
+        else:
+            exact = None if opts["precision"] == "fp64" else \
+                KIFMM(sw.Tree, [e, opts["mu"]], GMRES=1, format=2, precision="fp64")
+            geps = mob.grad_eps(z, lam, exact)
         ctx.grad_info = dict(iters=it, relres=relres)
         X_dtype, dev = gout.dtype, gout.device
         return (torch.as_tensor(gX, dtype=X_dtype, device=dev), torch.as_tensor(gY, dtype=X_dtype, device=dev),

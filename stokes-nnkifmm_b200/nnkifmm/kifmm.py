@@ -148,6 +148,18 @@ class KIFMM:
         L.check(L.lib.nnk_fmm_stats_get(self.h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in L.FmmStats._fields_}
 
+    def grad_eps(self, forces, weights):
+        """weights^T (dF/deps) forces: the analytic eps-derivative of this FMM
+        operator (FP64, exact check-to-equivalent inverses), nnk_fmm_grad_eps.
+        forces (n_pot x 3) and weights (n_tgt x 3) as numpy arrays in the
+        object's vector layout."""
+        f = np.ascontiguousarray(np.asarray(forces, dtype=np.float64))
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
+        out = C.c_double()
+        L.check(L.lib.nnk_fmm_grad_eps(self.h, L.ptr(f), L.ptr(w), self._layout(), C.byref(out), 0), self.ctx.h,
+                "grad_eps")
+        return out.value
+
     def profile(self, enable=True):
         """Per-phase CUDA-event timing of later computeVel calls."""
         L.check(L.lib.nnk_fmm_profile(self.h, int(bool(enable))))

@@ -247,6 +247,17 @@ class Mobility:
                                              L.ptr(gy) if info.num_fine else None, 0), self.ctx.h, "gradient")
         return gx, gy
 
+    def grad_eps(self, z, lam, fmm64=None):
+        """-lam^T (dA/deps) z through the analytic eps-derivative of the FMM
+        (nnk_mob_grad_eps); fmm64: an FP64 KIFMM with the exact
+        check-to-equivalent inverses on the same tree, when this object's own
+        FMM is not one."""
+        z, lam = self._vec(z), self._vec(lam)
+        out = C.c_double()
+        L.check(L.lib.nnk_mob_grad_eps(self.h, fmm64.h if fmm64 is not None else None, L.ptr(z), L.ptr(lam),
+                                       C.byref(out), 0), self.ctx.h, "grad_eps")
+        return out.value
+
     def use_graphs(self, enable=True):
         """Replay the matvec from a CUDA graph (default) or launch kernel by kernel."""
         L.check(L.lib.nnk_mob_use_graphs(self.h, int(bool(enable))), self.ctx.h, "use_graphs")
