@@ -67,9 +67,9 @@ class KIFMM:
 def _leaf_sources(tree, node, pot):
     """Sources of leaf ``node`` and their force densities.
 
-    Plain mode: the potential points of the leaf (upwardPass.m:299-317).
+    Plain mode: the potential points of the leaf (upwardPass.m:54-77).
     NEAREST mode: the fine points with a nonzero NN entry in the leaf's
-    columns, ascending, carrying kron(NN_sub, I3)*f (upwardPass.m:303-314,
+    columns, ascending, carrying kron(NN_sub, I3)*f (upwardPass.m:58-66,
     nearestBlockComputation.m:26-29).  As in downwardPass.m:92,221 the
     NEAREST gather slices columns by ``pointIndex == node`` over all points,
     which presumes potentials and targets are the same set.
@@ -119,7 +119,7 @@ def up_levels(tree, res, shells):
 
 
 def upward_pass(tree, pot, eps, mu, res=6, shells=1):
-    """Tools/Passes/upwardPass.m:18-100.  Levels max..0; nodes of a level are
+    """Tools/Passes/upwardPass.m:18-99.  Levels max..0; nodes of a level are
     the non-empty potential leaves and the non-leaves (:33-35); returns
     uppot[(nodeCount+1), 3P] with rows [x y z] interleaved per surface point."""
     P = surface_count(res, shells)

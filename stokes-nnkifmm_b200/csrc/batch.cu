@@ -91,7 +91,7 @@ __device__ __forceinline__ void cross3(const double* a, const double* b, double*
 }
 
 // y_f += BT [U; Om] = -U + xrel x Om on every force point, for each
-// right-hand side of its body (genMatrixComponets.m:182-198)
+// right-hand side of its body (genMatrixComponets.m:34-50)
 __global__ void batch_bt_kernel(long long Nt, int R, const int* __restrict__ row_body,
                                 const int* __restrict__ row_local, const long long* __restrict__ sys_off,
                                 const int* __restrict__ sys_n, const double* __restrict__ xrel,
@@ -112,7 +112,7 @@ __global__ void batch_bt_kernel(long long Nt, int R, const int* __restrict__ row
   }
 }
 
-// y_UOm = B f = [sum af f ; sum xm x f] per system (genMatrixComponets.m:201-245)
+// y_UOm = B f = [sum af f ; sum xm x f] per system (genMatrixComponets.m:53-95)
 __global__ void batch_bsum_kernel(const long long* __restrict__ body_row0, int R, const long long* __restrict__ sys_off,
                                   const int* __restrict__ sys_n, const double* __restrict__ af,
                                   const double* __restrict__ xm, const double* __restrict__ x,

@@ -387,7 +387,7 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
   ts.up.assign(maxl_ + 1, {});
   ts.down.assign(maxl_ + 1, {});
   ts.down_nov.assign(maxl_ + 1, {});
-  // upward pass (upwardPass.m:32-100): leaves with sources and non-leaves,
+  // upward pass (upwardPass.m:32-99): leaves with sources and non-leaves,
   // level by level from the bottom.  The root's expansion is never used by
   // any list, so level 0 is skipped.
   for (int L = maxl_; L >= 1; --L) {

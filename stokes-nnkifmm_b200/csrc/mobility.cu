@@ -14,7 +14,7 @@ __device__ __forceinline__ void cross3(const double* a, const double* b, double*
   o[2] = a[0] * b[1] - a[1] * b[0];
 }
 
-// y_c(n) += -U_b,c + (x_n x Om_b)_c : BT*[U;Om] (genMatrixComponets.m:182-198)
+// y_c(n) += -U_b,c + (x_n x Om_b)_c : BT*[U;Om] (genMatrixComponets.m:34-50)
 // out6 = per body its 6x6 inverse times in6 (layout [U_x(1..nb) U_y U_z Om_x Om_y Om_z])
 __global__ void small_solve_kernel(int nb, const double* __restrict__ inv, const double* __restrict__ in6,
                                    double* __restrict__ out6) {
@@ -40,7 +40,7 @@ __global__ void bt_kernel(int64_t N, int nb, const int* __restrict__ body, const
   for (int k = 0; k < 3; ++k) y[k * N + n] += -U[k] + c[k];
 }
 
-// out = B * f: F_b = sum af_n f_n, M_b = sum xm_n x f_n (genMatrixComponets.m:201-245)
+// out = B * f: F_b = sum af_n f_n, M_b = sum xm_n x f_n (genMatrixComponets.m:53-95)
 // mode 1: out = BT^T v: [-sum v_n ; sum v_n x xrel_n]
 __global__ void body_reduce_kernel(int64_t N, int nb, const int64_t* __restrict__ bstart,
                                    const double* __restrict__ w, const double* __restrict__ arm,
@@ -170,7 +170,7 @@ Mobility::Mobility(Fmm* fmm, int nbodies, const int64_t* body_start, const int64
       for (int d = 0; d < 3; ++d) xm[3 * n + d] = xrel[3 * n + d];
     }
   }
-  // A1 = B B^T and A2 = BT^T BT per body (genMatrixComponets.m:247-248)
+  // A1 = B B^T and A2 = BT^T BT per body (genMatrixComponets.m:99-100)
   a1inv_.assign(36 * (size_t)nb_, 0.0);
   a2inv_.assign(36 * (size_t)nb_, 0.0);
   for (int b = 0; b < nb_; ++b) {

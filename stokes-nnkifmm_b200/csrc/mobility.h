@@ -1,7 +1,7 @@
 // Rigid-body mobility system on one FMM (Mobility/*.m):
 //   [ S*NN  BT ] [ f     ]   [ u_slip - u_bg ]
 //   [ B     0  ] [ U; Om ] = [ F; M          ]
-// Vector layout (mobilityProblem.m:45-46, MobilityMatrixMulti.m:96-107):
+// Vector layout (mobilityProblem.m:45-46, MobilityMatrixMulti.m:19-36):
 //   [ f_x(1..N) f_y(1..N) f_z(1..N) | U_x(1..nb) U_y U_z | Om_x(1..nb) Om_y Om_z ].
 #pragma once
 #include <memory>
@@ -65,7 +65,7 @@ class Mobility {
   DBuf<int32_t> body_of_;   // per point: body or -1 (boundary)
   DBuf<int64_t> bstart_d_;
   DBuf<double> xrel_;       // per point rotated untranslated position (BT, Swimmers.m:177-189)
-  DBuf<double> xm_;         // per point torque arm: sum_q NN(q,n) X_q (NEAREST) or xrel (genMatrixComponets.m:217-222)
+  DBuf<double> xm_;         // per point torque arm: sum_q NN(q,n) X_q (NEAREST) or xrel (genMatrixComponets.m:69-75)
   DBuf<double> af_;         // per point force weight: column sum of NN (NEAREST) or 1 (:208-209, :228)
   std::vector<double> a1inv_, a2inv_;  // per body 6x6 inverses of B B^T and BT^T BT
   DBuf<double> a1inv_d_, a2inv_d_;     // the same on the device

@@ -504,7 +504,7 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
   t.src_gw.clear();
   t.src_origin.clear();
   if (!p.nearest) {
-    // plain: potential points of each leaf (upwardPass.m:299-317)
+    // plain: potential points of each leaf (upwardPass.m:54-77)
     for (int32_t i = 0; i < N; ++i) {
       t.src_start[i] = (int64_t)t.src_goff.size() - 1;
       if (t.child0[i] >= 0) continue;
@@ -522,7 +522,7 @@ int build_tree(const double* pot, int64_t n_pot, const double* tgt, int64_t n_tg
   } else {
     // NEAREST: fine points with a nonzero NN entry in the leaf's columns,
     // ascending fine index, each carrying kron(NN_sub,I3)*f
-    // (upwardPass.m:303-314, downwardPass.m:89-101).
+    // (upwardPass.m:58-66, downwardPass.m:89-101).
     struct T { int64_t q; int32_t col; double w; };
     std::vector<int64_t> cnt(N + 1, 0);
     const int64_t nnz = t.nn_rowptr[q];

@@ -1,0 +1,63 @@
+"""The differentiation configuration at its stated size: a prolate spheroid
+(a = 1, c = 3) with about 50k force and 200k quadrature points, eps = 0.005,
+free space, a unit force in x; loss ||[U; Om] - U*||^2 with U* ~ N(0,1).
+The gradient of rigid_velocity (adjoint GMRES, the kernel's position
+derivative through the FMM's leaf stages, the rigid-body blocks) against
+central finite differences of the solve itself (h = 1e-6, FP64) along 32
+random directions of the force and quadrature points, for the FP64 and the
+mixed-precision solves.  The points are jittered so that no quadrature point
+is within 1e-9 of a tie between two force points (the nearest map is then
+fixed at +-h); the FD solves run on FP64 Tikhonov operators (rounding ~1e-11
+instead of the exact inverse's ~1e-9), the analytic gradients on the same
+operators.  Takes about two minutes on a B200."""
+import numpy as np
+import pytest
+import torch
+
+import nnkifmm as nk
+from nnkifmm.autograd import rigid_velocity
+from nnkifmm.workloads import _spacing_for_count, prolate_spheroid
+
+pytestmark = pytest.mark.gpu
+
+
+def test_gradient_against_32_fd_directions_at_50k():
+    rng = np.random.default_rng(20261210)
+    h0 = _spacing_for_count(1.0, 3.0, 50_000)
+    X0 = prolate_spheroid(1.0, 3.0, h0)
+    Y0 = prolate_spheroid(1.0, 3.0, h0 / 2)
+    X0 = X0 + 1e-3 * h0 * rng.standard_normal(X0.shape)
+    Y0 = Y0 + 1e-3 * h0 * rng.standard_normal(Y0.shape)
+    eps, F, M = 0.005, np.array([1.0, 0.0, 0.0]), np.zeros(3)
+    Us = rng.standard_normal(6)
+    NN = nk.nearestMatrix(X0, Y0)
+    opts = dict(cap=64, tol=1e-11, maxIter=1000, reg=1e-5)
+
+    def loss(X, Y):
+        U = rigid_velocity(torch.tensor(X), torch.tensor(Y), eps, F, M, precision="fp64", **opts)
+        return float(((U - torch.tensor(Us)) ** 2).sum())
+
+    grads = {}
+    for prec, tol in [("fp64", 1e-11), ("mixed", 1e-8)]:
+        X = torch.tensor(X0, requires_grad=True)
+        Y = torch.tensor(Y0, requires_grad=True)
+        U = rigid_velocity(X, Y, eps, F, M, precision=prec, **dict(opts, tol=tol))
+        ((U - torch.tensor(Us)) ** 2).sum().backward()
+        grads[prec] = (X.grad.numpy().copy(), Y.grad.numpy().copy())
+    h = 1e-6
+    fd, an = [], {p: [] for p in grads}
+    for k in range(32):
+        dX = rng.standard_normal(X0.shape)
+        dY = rng.standard_normal(Y0.shape)
+        nrm = np.sqrt((dX * dX).sum() + (dY * dY).sum())
+        dX, dY = dX / nrm, dY / nrm
+        for s in (-1, 1):  # the nearest map must stay fixed along the direction
+            assert (nk.nearestMatrix(X0 + s * h * dX, Y0 + s * h * dY) != NN).nnz == 0
+        fd.append((loss(X0 + h * dX, Y0 + h * dY) - loss(X0 - h * dX, Y0 - h * dY)) / (2 * h))
+        for p, (gX, gY) in grads.items():
+            an[p].append(float((gX * dX).sum() + (gY * dY).sum()))
+    fd = np.array(fd)
+    errs = {p: float(np.linalg.norm(np.array(v) - fd) / np.linalg.norm(fd)) for p, v in an.items()}
+    print("points", len(X0), len(Y0), "directional-derivative error vs FD over 32 directions:", errs)
+    assert errs["fp64"] <= 1e-3
+    assert errs["mixed"] <= 1e-2
