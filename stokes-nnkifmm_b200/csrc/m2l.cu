@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
                    const int* __restrict__ tile_slot0, const int* __restrict__ slot_op,
                    const int* __restrict__ slot_src, const float* __restrict__ images,
                    const float* __restrict__ src, const float* __restrict__ src_lo, float* __restrict__ out,
-                   int ldc, int NP, int* err, int ns, uint32_t wlim, int probe) {
+                   int ldc, int NP, int* err, int ns, uint32_t wlim, int probe, float* __restrict__ part) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* sbase = smem_raw + (((raw + 1023u) & ~1023u) - raw);
@@ -587,6 +587,13 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
       float vals[16];
       tmem_ld16(lane_addr + col, vals);
       if (node >= 0) {
+        if (part) {  // this unit's own block; the tile's blocks are added in order afterwards
+          float4* dst = reinterpret_cast<float4*>(part + ((size_t)blockIdx.x * kTileRows + row) * NP + col);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            dst[q] = make_float4(vals[4 * q], vals[4 * q + 1], vals[4 * q + 2], vals[4 * q + 3]);
+          continue;
+        }
         float* dst = out + (size_t)node * ldc;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -601,6 +608,33 @@ __global__ void __launch_bounds__(32 * (1 + kWsGatherWarps), 1)
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
+// out[node] = sum over the tile's units, in unit order, of their partial
+// blocks (rows of empty tile slots are skipped).  One block per tile.
+__global__ void __launch_bounds__(256) m2l_unit_reduce_kernel(const int* __restrict__ tile_uoff,
+                                                              const int* __restrict__ tile_units,
+                                                              const int* __restrict__ tile_nodes,
+                                                              const float* __restrict__ part, int NP,
+                                                              float* __restrict__ out, int ldc) {
+  const int t = blockIdx.x;
+  const int u0 = tile_uoff[t], u1 = tile_uoff[t + 1];
+  const int n4 = NP / 4;
+  const float4* p4 = reinterpret_cast<const float4*>(part);
+  for (int idx = threadIdx.x; idx < kTileRows * n4; idx += blockDim.x) {
+    const int r = idx / n4, c4 = idx - r * n4;
+    const int node = tile_nodes[t * kTileRows + r];
+    if (node < 0) continue;
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = u0; k < u1; ++k) {
+      const float4 v = p4[((size_t)tile_units[k] * kTileRows + r) * n4 + c4];
+      s.x += v.x;
+      s.y += v.y;
+      s.z += v.z;
+      s.w += v.w;
+    }
+    reinterpret_cast<float4*>(out + (size_t)node * ldc)[c4] = s;
+  }
 }
 
 // T_{L,o}[n = 3a+al][k = 3b+be] = S_al,be(x_a - y_b) / (8 pi mu),
@@ -983,6 +1017,15 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
   }
   plan.ntiles = (int)tile_slot0.size();
   plan.nunits = (int)units.size();
+  {
+    std::vector<int> uoff(plan.ntiles + 1, 0), tu(units.size());
+    for (const M2LUnit& u : units) uoff[u.tile + 1]++;
+    for (int t2 = 0; t2 < plan.ntiles; ++t2) uoff[t2 + 1] += uoff[t2];
+    std::vector<int> at(uoff.begin(), uoff.end() - 1);
+    for (size_t k = 0; k < units.size(); ++k) tu[at[units[k].tile]++] = (int)k;
+    plan.tile_uoff.upload(uoff, st);
+    plan.tile_units.upload(tu, st);
+  }
   plan.useful_pairs = useful;
   plan.tile_slots = tslots;
   plan.tile_nodes.upload(tile_nodes, st);
@@ -1037,6 +1080,7 @@ void build_m2l_plan(const HostTree& t, int res, int shells, double eps, double m
     plan.bnodes.upload(bn, st);
     plan.nbtiles = (int)bt.size();
     plan.chat.alloc((size_t)t.nodes * RC);
+    plan.part.alloc(std::max<size_t>((size_t)plan.nunits * kTileRows * RC, 1));
     plan.src_lo.alloc((size_t)t.nodes * RC);
     plan.src_lo.zero(st);
   } else if (plan.use_images && !img_code.empty()) {
@@ -1100,9 +1144,12 @@ void launch_m2l(M2LPlan& plan, float* check, int ldc, cudaStream_t st, const flo
     NNK_CUDA(cudaMemsetAsync(plan.chat.p, 0, plan.chat.bytes(), st));
     m2l_ws_kernel<<<plan.nunits, 32 * (1 + kWsGatherWarps), plan.smem_bytes, st>>>(
         plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p, plan.slot_op.p, plan.slot_src.p, plan.images.p,
-        plan.src.p, plan.src_lo.p, plan.chat.p, RC, RC, plan.err.p, plan.stages, plan.wait_limit, 0);
+        plan.src.p, plan.src_lo.p, plan.chat.p, RC, RC, plan.err.p, plan.stages, plan.wait_limit, 0, plan.part.p);
     NNK_CHECK_LAUNCH();
     mirror_err(plan, st);
+    m2l_unit_reduce_kernel<<<plan.ntiles, 256, 0, st>>>(plan.tile_uoff.p, plan.tile_units.p, plan.tile_nodes.p,
+                                                        plan.part.p, RC, plan.chat.p, RC);
+    NNK_CHECK_LAUNCH();
     basis_apply_kernel<<<dim3((plan.n3 + 63) / 64, plan.nbtiles), 256, 0, st>>>(
         plan.basis.p, plan.n3, RC, 0, plan.btiles.p, plan.bnodes.p, plan.chat.p, RC, check, ldc);
     NNK_CHECK_LAUNCH();
@@ -1159,7 +1206,7 @@ int stall_m2l_probe(M2LPlan& plan, uint32_t polls, cudaStream_t st) {
   check_m2l_error(plan, st);  // an earlier flag is not the probe's
   m2l_ws_kernel<<<plan.nunits, 32 * (1 + kWsGatherWarps), plan.smem_bytes, st>>>(
       plan.units.p, plan.tile_nodes.p, plan.tile_slot0.p, plan.slot_op.p, plan.slot_src.p, plan.images.p,
-      plan.src.p, plan.src_lo.p, plan.chat.p, plan.RC, plan.RC, plan.err.p, plan.stages, polls, 1);
+      plan.src.p, plan.src_lo.p, plan.chat.p, plan.RC, plan.RC, plan.err.p, plan.stages, polls, 1, plan.part.p);
   NNK_CHECK_LAUNCH();
   mirror_err(plan, st);
   NNK_CUDA(cudaStreamSynchronize(st));

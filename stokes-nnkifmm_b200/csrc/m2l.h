@@ -27,7 +27,9 @@
 // leading terms carry the sums, and their TF32 rounding errors do not
 // average out).  Per matvec: u^ = B^T u for every node that is a V source
 // (FP32 GEMM, split into two TF32 terms), c^ = sum_o C_o u^_v on the tensor
-// cores (the image kernel with NP = RC, both terms into one accumulator),
+// cores (the image kernel with NP = RC, both terms into one accumulator;
+// each work unit writes its own partial block, and the blocks of a tile are
+// added in unit order, so the result is the same bit for bit on every run),
 // check += B c^ for every V target.  RC = 256 for p = 6: 2 x (RC/NP)^2 = 57%
 // of the tensor work and 28% of the operator bytes; the truncation error of
 // the summed M2L on physical densities is ~1e-6, the TF32 rounding of C_o
@@ -84,6 +86,9 @@ struct M2LPlan {
   DBuf<int> bnodes;
   int nbtiles = 0;
   DBuf<float> chat;             // nodes * RC: compressed check potentials
+  DBuf<float> part;             // compressed form: nunits * 128 * RC partial sums, one block per unit
+  DBuf<int> tile_uoff;          // per tile: its units (ntiles + 1 offsets into tile_units)
+  DBuf<int> tile_units;         // unit ids of each tile, ascending (the order their partials are added)
   DBuf<float> src_lo;           // nodes * RC: second TF32 term of B^T u
   DBuf<int> err;                // bounded-wait timeout flag
   int* h_err = nullptr;         // pinned mirror of err
