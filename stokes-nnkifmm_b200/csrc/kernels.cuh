@@ -23,7 +23,19 @@ __device__ __forceinline__ void ldpos(const float* __restrict__ p, long long j, 
   y = v.y;
   z = v.z;
 }
-__device__ __forceinline__ double rsq(double d) { return rsqrt(d); }
+// 1/sqrt(d) for d > 0 (here d = r^2 + eps^2 >= eps^2): the hardware's FP64
+// approximation (PTX rsqrt.approx.ftz.f64, ~1e-6 relative) refined by two
+// Newton-Raphson steps y <- y (3 - d y^2) / 2, each of which squares the
+// relative error (measured on a B200 over d in [1e-12, 1e4]: 1.3e-12 after
+// one step, 3.1e-16 after two, against 1/sqrt in FP64).
+__device__ __forceinline__ double rsq(double d) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+  const double h = 0.5 * d;
+  y = y * fma(-h * y, y, 1.5);
+  y = y * fma(-h * y, y, 1.5);
+  return y;
+}
 __device__ __forceinline__ float rsq(float d) { return rsqrtf(d); }
 
 // ------------------------------------------------------------ vector I/O
@@ -105,14 +117,13 @@ __device__ __forceinline__ void pair_acc(Real tx, Real ty, Real tz, const typena
                                          const typename Vec4T<Real>::t2& s2, Real e2, Real& ax, Real& ay,
                                          Real& az) {
   const Real dx = tx - s4.x, dy = ty - s4.y, dz = tz - s4.z;
-  const Real r2 = dx * dx + dy * dy + dz * dz;
-  const Real d = r2 + e2;
+  const Real d = fma(dz, dz, fma(dy, dy, fma(dx, dx, e2)));  // r^2 + eps^2
   const Real inv = rsq(d);
   const Real inv3 = inv * inv * inv;
   Real a, b;
   if (KD) {
     const Real inv5 = inv3 * inv * inv;
-    a = (r2 - 2 * e2) * inv5;
+    a = (d - 3 * e2) * inv5;  // (r^2 - 2 eps^2) / D^{5/2}
     b = -3 * (dx * s4.w + dy * s2.x + dz * s2.y) * inv5;
   } else {
     a = e2 * inv3 + inv;  // (r^2 + 2 eps^2) / d^{3/2} = d^{-1/2} + eps^2 d^{-3/2}

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <map>
 
@@ -261,115 +262,96 @@ __global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* 
   for (int c = 0; c < C; ++c) out[(size_t)c * NK] = acc[c];
 }
 
-// Parent-grouped accumulation (see FftFamily).  A block covers 64
-// frequencies of one family; thread (half h, frequency k) holds the
-// accumulators of the 4 children of P with x position h, for one right-hand
-// side at a time.  Per (P, N) record the two halves load the 8 source
-// spectra of the frequency into shared memory, then for each of the 27
-// values of pos_v - pos_i present among the half's pairs the kernel spectrum
-// of offset 2 d + delta is loaded once and applied to every such pair.  Loop
-// bounds and child positions are compile-time, so accumulators stay in
-// registers.  Every right-hand side sums its pairs in the same order, so a
-// pass of R right-hand sides gives each of them bitwise the result of a pass
-// of one.
-constexpr int kFamFreq = 64;
-
-template <int H, typename T2>
-__device__ __forceinline__ void family_record(const FftFamilyPair& rec, const int* __restrict__ so,
-                                              const T2* __restrict__ spec, int NK, int k, const T2* sq, int kk,
-                                              T2 (&acc)[4][3]) {
-  const uint64_t mask = (uint64_t)rec.mask_lo | ((uint64_t)rec.mask_hi << 32);
-  const int dx2 = 2 * (rec.dcode / 9 - 1), dy2 = 2 * ((rec.dcode / 3) % 3 - 1), dz2 = 2 * (rec.dcode % 3 - 1);
-#pragma unroll
-  for (int dl = 0; dl < 27; ++dl) {
-    const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
-    uint64_t gm = 0;
-#pragma unroll
-    for (int a = 4 * H; a < 4 * H + 4; ++a) {
-      const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
-      if (bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)
-        gm |= 1ull << (a * 8 + (bx * 4 + by * 2 + bz));
-    }
-    if (gm == 0) continue;
-    const uint64_t bits = mask & gm;
-    if (bits == 0) continue;
-    const int code = (dx2 + ex + 3) * 49 + (dy2 + ey + 3) * 7 + (dz2 + ez + 3);
-    const T2* Kp = spec + (size_t)so[code] * 6 * NK + k;
-    const T2 kxx = Kp[0], kxy = Kp[NK], kxz = Kp[2 * NK], kyy = Kp[3 * NK], kyz = Kp[4 * NK], kzz = Kp[5 * NK];
-#pragma unroll
-    for (int a = 4 * H; a < 4 * H + 4; ++a) {
-      const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
-      if (!(bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)) continue;
-      const int b = bx * 4 + by * 2 + bz;
-      if (!((bits >> (a * 8 + b)) & 1)) continue;
-      const T2 qx = sq[(b * 3) * kFamFreq + kk], qy = sq[(b * 3 + 1) * kFamFreq + kk],
-               qz = sq[(b * 3 + 2) * kFamFreq + kk];
-      T2* o = acc[a - 4 * H];
-      cmac(o[0], kxx, qx);
-      cmac(o[0], kxy, qy);
-      cmac(o[0], kxz, qz);
-      cmac(o[1], kxy, qx);
-      cmac(o[1], kyy, qy);
-      cmac(o[1], kyz, qz);
-      cmac(o[2], kxz, qx);
-      cmac(o[2], kyz, qy);
-      cmac(o[2], kzz, qz);
-    }
-  }
-}
-
+// Parent-grouped accumulation (see FftFamily): thread (family, frequency k)
+// holds the 8 children's accumulators of one right-hand side at a time; per
+// (P, N) record the 8 source spectra go to this thread's own shared-memory
+// slots, then for each of the 27 values of pos_v - pos_i present in the
+// record the kernel spectrum of offset 2 d + delta is loaded once and applied
+// to every pair with that difference.  Loop bounds and child positions are
+// compile-time, so accumulators stay in registers.  Every right-hand side
+// sums its pairs in the same order, so a pass of R right-hand sides gives
+// each of them bitwise the result of a pass of one.
 template <typename Real>
-__global__ void __launch_bounds__(2 * kFamFreq, 5) fft_accumulate_family_kernel(
+__global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
     int NK, const FftFamily* __restrict__ fams, const FftFamilyPair* __restrict__ pairs,
     const int* __restrict__ spec_of, const typename Cplx<Real>::t* __restrict__ spec,
     const typename Cplx<Real>::t* __restrict__ qhat, typename Cplx<Real>::t* __restrict__ chat,
     const int* __restrict__ tgt_node, const int* __restrict__ nact, int R) {
   using T2 = typename Cplx<Real>::t;
-  __shared__ T2 sq[24 * kFamFreq];  // the record's source spectra: [pos * 3 + c][frequency]
+  constexpr int BLK = 128;
+  __shared__ T2 sq[24 * BLK];  // this thread's source spectra: [pos * 3 + c][thread]
   const FftFamily fam = fams[blockIdx.x];
+  const int k = blockIdx.y * BLK + threadIdx.x;
   if (nact) {
     int t0 = 0;
     while (t0 < 7 && fam.tgt[t0] < 0) ++t0;
-    if (!nact[tgt_node[fam.tgt[t0]]]) return;  // the whole block returns
+    if (!nact[tgt_node[fam.tgt[t0]]]) return;
   }
-  const int h = threadIdx.x / kFamFreq, kk = threadIdx.x % kFamFreq;
-  const int k = blockIdx.y * kFamFreq + kk;
-  const bool on = k < NK;
-  const int kc = on ? k : NK - 1;  // threads past the spectrum compute on a valid index, store nothing
+  if (k >= NK) return;
   const int C = 3 * R;
+  T2* my = sq + threadIdx.x;
   for (int r = 0; r < R; ++r) {
-    T2 acc[4][3];
+  T2 acc[8][3];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 8; ++a)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) acc[a][c] = cmake((Real)0, (Real)0);
-    for (int pr = fam.first; pr < fam.first + fam.count; ++pr) {
-      const FftFamilyPair rec = pairs[pr];
-      __syncthreads();  // the previous record's spectra are read
+    for (int c = 0; c < 3; ++c) acc[a][c] = cmake((Real)0, (Real)0);
+  for (int pr = fam.first; pr < fam.first + fam.count; ++pr) {
+    const FftFamilyPair rec = pairs[pr];
+    const uint64_t mask = (uint64_t)rec.mask_lo | ((uint64_t)rec.mask_hi << 32);
 #pragma unroll
-      for (int bb = 0; bb < 4; ++bb) {
-        const int b = 4 * h + bb, sl = rec.src[b];
-        if (sl >= 0) {
-          const T2* Q = qhat + ((size_t)sl * C + 3 * r) * NK + kc;
+    for (int b = 0; b < 8; ++b) {
+      const int sl = rec.src[b];
+      if (sl >= 0) {
+        const T2* Q = qhat + ((size_t)sl * C + 3 * r) * NK + k;
 #pragma unroll
-          for (int c = 0; c < 3; ++c) sq[(b * 3 + c) * kFamFreq + kk] = Q[(size_t)c * NK];
-        }
-      }
-      __syncthreads();
-      const int* so = spec_of + (size_t)rec.op * 343;
-      if (h == 0) family_record<0>(rec, so, spec, NK, kc, sq, kk, acc);
-      else family_record<1>(rec, so, spec, NK, kc, sq, kk, acc);
-    }
-    if (on) {
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int t = fam.tgt[4 * h + a];
-        if (t < 0) continue;
-        T2* out = chat + ((size_t)t * C + 3 * r) * NK + k;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) out[(size_t)c * NK] = acc[a][c];
+        for (int c = 0; c < 3; ++c) my[(b * 3 + c) * BLK] = Q[(size_t)c * NK];
       }
     }
+    const int dx2 = 2 * (rec.dcode / 9 - 1), dy2 = 2 * ((rec.dcode / 3) % 3 - 1), dz2 = 2 * (rec.dcode % 3 - 1);
+    const int* so = spec_of + (size_t)rec.op * 343;
+#pragma unroll
+    for (int dl = 0; dl < 27; ++dl) {
+      const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
+      uint64_t gm = 0;
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
+        if (bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)
+          gm |= 1ull << (a * 8 + (bx * 4 + by * 2 + bz));
+      }
+      const uint64_t bits = mask & gm;
+      if (bits == 0) continue;
+      const int code = (dx2 + ex + 3) * 49 + (dy2 + ey + 3) * 7 + (dz2 + ez + 3);
+      const T2* Kp = spec + (size_t)so[code] * 6 * NK + k;
+      const T2 kxx = Kp[0], kxy = Kp[NK], kxz = Kp[2 * NK], kyy = Kp[3 * NK], kyz = Kp[4 * NK], kzz = Kp[5 * NK];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
+        if (!(bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)) continue;
+        const int b = bx * 4 + by * 2 + bz;
+        if (!((bits >> (a * 8 + b)) & 1)) continue;
+        const T2 qx = my[(b * 3) * BLK], qy = my[(b * 3 + 1) * BLK], qz = my[(b * 3 + 2) * BLK];
+        cmac(acc[a][0], kxx, qx);
+        cmac(acc[a][0], kxy, qy);
+        cmac(acc[a][0], kxz, qz);
+        cmac(acc[a][1], kxy, qx);
+        cmac(acc[a][1], kyy, qy);
+        cmac(acc[a][1], kyz, qz);
+        cmac(acc[a][2], kxz, qx);
+        cmac(acc[a][2], kyz, qy);
+        cmac(acc[a][2], kzz, qz);
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int t = fam.tgt[a];
+    if (t < 0) continue;
+    T2* out = chat + ((size_t)t * C + 3 * r) * NK + k;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[(size_t)c * NK] = acc[a][c];
+  }
   }
 }
 
@@ -580,7 +562,7 @@ void run_fft_m2l(FftM2L& f, const Real* str, long long upbase, int R, Real* chec
                                                         f.NK, nact);
   NNK_CHECK_LAUNCH();
   if (f.family) {
-    fft_accumulate_family_kernel<Real><<<dim3(f.nfam, (f.NK + kFamFreq - 1) / kFamFreq), 2 * kFamFreq, 0, st>>>(
+    fft_accumulate_family_kernel<Real><<<dim3(f.nfam, (f.NK + 127) / 128), 128, 0, st>>>(
         f.NK, f.fams.p, f.fpairs.p, f.spec_of.p, spec, qhat, chat, f.tgt_node.p, nact, R);
     NNK_CHECK_LAUNCH();
     inv<<<f.ntgt, 256, inverse_smem(G, res, R, es), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, chat, R, check, f.NK,

@@ -83,8 +83,16 @@ def sphere_case():
     rsol = fmm.reduced_solve(U)
     direct = apply_kernel(f, c, NN @ F, eps, mu)
     print(f"sphere: {time.time() - t:.1f}s, fmm vs direct {np.linalg.norm(vel - direct) / np.linalg.norm(direct):.2e}")
+    # eps-derivative of the reference operator: w^T (dF/deps) F by a central
+    # difference of the oracle's per-node-LU passes (h = 1e-4 eps; 1e-3 gives
+    # the same to 1e-8)
+    wts = rng.standard_normal((len(c), 3))
+    h = 1e-4 * eps
+    vp = KIFMM(tree, eps + h, mu).compute_vel(F)
+    vm = KIFMM(tree, eps - h, mu).compute_vel(F)
+    deps_fd = float((wts * (vp - vm)).sum()) / (2 * h)
     d = dict(coarse=c, fine=f, F=F, U=U, eps=eps, mu=mu, cap=60, vel=vel, vel_sparse=vel4, reduced=red,
-             reduced_solve=rsol, direct=direct)
+             reduced_solve=rsol, direct=direct, deps_w=wts, deps_fd=deps_fd)
     d.update(nn_arrays(NN))
     d.update(tree_arrays(tree))
     np.savez_compressed(os.path.join(OUT, "sphere10_40.npz"), **d)

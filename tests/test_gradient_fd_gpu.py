@@ -5,9 +5,10 @@ The gradient of rigid_velocity (adjoint GMRES, the kernel's position
 derivative through the FMM's leaf stages, the rigid-body blocks) against
 central finite differences of the solve itself (h = 1e-6, FP64) along 32
 random directions of the force and quadrature points, for the FP64 and the
-mixed-precision solves.  The points are jittered so that no quadrature point
-is within 1e-9 of a tie between two force points (the nearest map is then
-fixed at +-h); the FD solves run on FP64 Tikhonov operators (rounding ~1e-11
+mixed-precision solves.  The points are jittered, and a direction along
+which some quadrature point changes its nearest force point within +-h is
+drawn again (the gradient holds the nearest map fixed); the FD solves run on
+FP64 Tikhonov operators (rounding ~1e-11
 instead of the exact inverse's ~1e-9), the analytic gradients on the same
 operators.  Takes about two minutes on a B200."""
 import numpy as np
@@ -46,18 +47,25 @@ def test_gradient_against_32_fd_directions_at_50k():
         grads[prec] = (X.grad.numpy().copy(), Y.grad.numpy().copy())
     h = 1e-6
     fd, an = [], {p: [] for p in grads}
-    for k in range(32):
+    tries = 0
+    while len(fd) < 32:
+        tries += 1
+        assert tries <= 200, "too few directions keep the nearest map"
         dX = rng.standard_normal(X0.shape)
         dY = rng.standard_normal(Y0.shape)
         nrm = np.sqrt((dX * dX).sum() + (dY * dY).sum())
         dX, dY = dX / nrm, dY / nrm
-        for s in (-1, 1):  # the nearest map must stay fixed along the direction
-            assert (nk.nearestMatrix(X0 + s * h * dX, Y0 + s * h * dY) != NN).nnz == 0
+        # the gradient holds the nearest map fixed; a direction along which a
+        # quadrature point changes its nearest force point within +-h is
+        # drawn again
+        if any((nk.nearestMatrix(X0 + s * h * dX, Y0 + s * h * dY) != NN).nnz for s in (-1, 1)):
+            continue
         fd.append((loss(X0 + h * dX, Y0 + h * dY) - loss(X0 - h * dX, Y0 - h * dY)) / (2 * h))
         for p, (gX, gY) in grads.items():
             an[p].append(float((gX * dX).sum() + (gY * dY).sum()))
     fd = np.array(fd)
     errs = {p: float(np.linalg.norm(np.array(v) - fd) / np.linalg.norm(fd)) for p, v in an.items()}
-    print("points", len(X0), len(Y0), "directional-derivative error vs FD over 32 directions:", errs)
+    print("points", len(X0), len(Y0), "directions drawn", tries,
+          "directional-derivative error vs FD over 32 directions:", errs)
     assert errs["fp64"] <= 1e-3
     assert errs["mixed"] <= 1e-2
