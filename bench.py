@@ -595,9 +595,10 @@ def roofline(per_step, stats, precision, peaks, m2l_form):
                                   "scaled by V pairs to the 250k launch (profiles/m2l_compressed_kernel_60k.md)"}
     elif dom == "m2l" and m2l_form == "fourier":
         res = 6
-        nk_freq = (2 * res) ** 2 * (res + 1)
+        grid = 2 * res - 1  # cyclic transform length without wrap-around
+        nk_freq = grid * grid * (grid // 2 + 1)
         flops = 72.0 * nk_freq * stats["m2l_pairs"]  # 9 complex multiply-adds per pair and frequency
-        roof = {"kernel": f"fft_accumulate_kernel ({'FP64' if fp64 else 'FP32'} spectra) with the forward and "
+        roof = {"kernel": f"fft_accumulate_family_kernel ({'FP64' if fp64 else 'FP32'} spectra) with the forward and "
                           "inverse lattice transforms", "bound": "fp64" if fp64 else "fp32",
                 "achieved": flops / (per_step[dom][0] / 1e3) / 1e12, "peak": simt_peak, "unit": "TFLOP/s",
                 "peak_source": simt_src, "launches_per_step": per_step[dom][1], "ms_per_launch": ms_l,

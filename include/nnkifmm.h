@@ -127,7 +127,8 @@ typedef struct nnk_fmm_stats {
   int32_t levels;
   int32_t m2l_rank;     /* compressed tensor-core M2L: rank of the per-level
                            bases (its GEMMs are m2l_rank square); 0 otherwise */
-  int32_t reserved;
+  int32_t folded;       /* 1: the matvec runs M2M and L2L folded into the
+                           check-to-equivalent products (nnk_fmm_set_fold)  */
 } nnk_fmm_stats;
 
 /* GMRES options/result (MATLAB gmres(A,b,restart,tol,maxit), x0 = 0). */
@@ -262,6 +263,17 @@ int nnk_fmm_autotune(nnk_fmm* fmm, int32_t nrhs, double* ms_before, double* ms_a
  * spectra) for kernelPar(1) = eps, keeping the tree-dependent task lists:
  * the cheap way to evaluate the operator at eps +- d for its eps-derivative. */
 int nnk_fmm_set_eps(nnk_fmm* fmm, double eps);
+/* Folded M2M / L2L in the matvec (on by default where available): a
+ * parent's up-equivalent density becomes one FP64 product
+ * A(w) [M2M_0 .. M2M_7] with its 8 children's (Up.m:31-33 applied to the
+ * M2M sums of upwardPass.m:81-93), and the L2L part of a child's
+ * down-equivalent density the product A(w)^T L2L_k with its parent's
+ * (the parentsurf term of DownNonleaf.m:42-46), in place of the pair sums followed by the
+ * check-to-equivalent step: the same operator up to FP64 rounding.
+ * Available with the Fourier-space or tensor-core M2L, for trees whose
+ * folded operators take at most 1 GiB; the transpose, the gradients and
+ * the eps-derivative always run unfolded.  on = 0 turns it off. */
+int nnk_fmm_set_fold(nnk_fmm* fmm, int32_t on);
 /* Number of source origins: fine points (NEAREST) or potential rows. */
 int nnk_fmm_source_count(const nnk_fmm* fmm, int64_t* count);
 /* Gradient of <weights, apply(forces)> with respect to the positions, with

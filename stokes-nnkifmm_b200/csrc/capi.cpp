@@ -420,7 +420,17 @@ int nnk_fmm_grad_positions(nnk_fmm* fmm, const double* forces, const double* wei
 int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats) {
   if (!fmm || !stats) return NNK_E_ARG;
   *stats = fmm->f->stats();
+  stats->folded = fmm->f->folded() ? 1 : 0;
   return NNK_OK;
+}
+
+int nnk_fmm_set_fold(nnk_fmm* fmm, int32_t on) {
+  if (!fmm) return NNK_E_ARG;
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  fmm->f->set_fold(on != 0);
+  API_CATCH(ctx)
 }
 
 int nnk_fmm_profile(nnk_fmm* fmm, int32_t enable) {

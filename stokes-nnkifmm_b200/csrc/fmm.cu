@@ -362,6 +362,7 @@ void Fmm::build_tasks() {
   }
   fwd_.near = near32();
   build_taskset(fwd_, r, true);
+  build_fold_lists();
   stats_.c2e_columns = (int64_t)ln.size() + (int64_t)fwd_.up_nodes_host.size();
   stats_.surface_points = P_;
   stats_.levels = maxl_ + 1;
@@ -522,7 +523,51 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
     }
     ts.leaf_far.count = (int64_t)tasks.size() - ts.leaf_far.first;
   }
+  if (&ts == &fwd_) {
+    // folded form: the leaves' S2M of each level; the X-list P2L of each
+    // level (NEAR32: none, its X-list runs in FP32 from x_only)
+    ts.fold = true;
+    ts.up_leaf.assign(maxl_ + 1, {});
+    ts.down_x.assign(maxl_ + 1, {});
+    ts.upl_nodes_host.clear();
+    ts.upl_off.assign(maxl_ + 2, 0);
+    for (int L = maxl_; L >= 1; --L) {
+      ts.up_leaf[L].first = (int64_t)tasks.size();
+      for (int32_t n : t.by_level[L]) {
+        if (t.child0[n] >= 0 || !(*r.src_leaf)[n]) continue;
+        TaskD tk{dnB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0, n, 0};
+        src_seg(n);
+        tk.nseg = (int)segs.size() - tk.seg0;
+        tasks.push_back(tk);
+      }
+      ts.up_leaf[L].count = (int64_t)tasks.size() - ts.up_leaf[L].first;
+    }
+    for (int L = 0; L <= maxl_; ++L) {
+      ts.upl_off[L] = (int64_t)ts.upl_nodes_host.size();
+      if (L == 0) continue;
+      for (int32_t n : t.by_level[L])
+        if (t.child0[n] < 0 && (*r.src_leaf)[n]) ts.upl_nodes_host.push_back(n);
+    }
+    ts.upl_off[maxl_ + 1] = (int64_t)ts.upl_nodes_host.size();
+    for (int L = 1; L <= maxl_; ++L) {
+      ts.down_x[L].first = (int64_t)tasks.size();
+      if (!ts.near)
+        for (int32_t n : t.by_level[L]) {
+          TaskD tk{upB + (long long)P_ * n, (long long)P_ * n, P_, (int)segs.size(), 0, 0, n, 0};
+          for (int64_t k = r.X->off[n]; k < r.X->off[n + 1]; ++k) src_seg(r.X->idx[k]);
+          tk.nseg = (int)segs.size() - tk.seg0;
+          if (tk.nseg) tasks.push_back(tk);
+        }
+      ts.down_x[L].count = (int64_t)tasks.size() - ts.down_x[L].first;
+    }
+  }
   cudaStream_t st = ctx_->stream;
+  if (ts.fold) {
+    std::vector<C2ETile> ut;
+    build_c2e_tiles(ts.upl_nodes_host, ts.upl_off, ut, ts.upl_toff);
+    ts.upl_tiles.upload(ut, st);
+    ts.upl_nodes.upload(ts.upl_nodes_host, st);
+  }
   {
     std::vector<C2ETile> ut;
     build_c2e_tiles(ts.up_nodes_host, ts.up_off, ut, ts.up_toff);
@@ -532,8 +577,8 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
     size_t need = 0;
     for (int R = 1; R <= R_; ++R)
       for (int L = 1; L <= maxl_; ++L) {
-        need = std::max(need, c2e_part_size(3 * P_, (int)(ts.up_toff[L + 1] - ts.up_toff[L]), R));
-        need = std::max(need, c2e_part_size(3 * P_, (int)(dn_toff_[L + 1] - dn_toff_[L]), R));
+        need = std::max(need, c2e_part_size(3 * P_, 3 * P_, (int)(ts.up_toff[L + 1] - ts.up_toff[L]), R));
+        need = std::max(need, c2e_part_size(3 * P_, 3 * P_, (int)(dn_toff_[L + 1] - dn_toff_[L]), R));
       }
     if (need > c2e_part_.n) c2e_part_.alloc(need);
   }
@@ -553,7 +598,7 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
 // Per level, runs of nodes of the same tree cut into tiles of at most
 // kC2ETileNodes nodes, each tile with the operator of its (tree, level).
 void Fmm::build_c2e_tiles(const std::vector<int32_t>& nodes, const std::vector<int64_t>& off,
-                          std::vector<C2ETile>& tiles, std::vector<int64_t>& toff) {
+                          std::vector<C2ETile>& tiles, std::vector<int64_t>& toff, int dl) {
   const HostTree& t = *t_;
   toff.assign(off.size(), 0);
   for (size_t L = 0; L + 1 < off.size(); ++L) {
@@ -563,7 +608,7 @@ void Fmm::build_c2e_tiles(const std::vector<int32_t>& nodes, const std::vector<i
       const int32_t g = t.group_of(nodes[i]);
       int64_t j = i;
       while (j < off[L + 1] && j - i < kC2ETileNodes && t.group_of(nodes[j]) == g) ++j;
-      const int op = op_of_[(size_t)g * (maxl_ + 1) + L];
+      const int op = L + dl <= maxl_ ? op_of_[(size_t)g * (maxl_ + 1) + L + dl] : -1;
       if (op < 0) throw Error(NNK_E_STATE, "node above its tree's depth");
       tiles.push_back(C2ETile{op, (int)i, (int)(j - i), 0});
       i = j;
@@ -644,6 +689,8 @@ void Fmm::split_tasks(TaskSet& ts, std::vector<TaskD>& tasks, std::vector<SegD>&
   for (auto& g : ts.down_nov) process(g);
   for (auto& g : ts.down) process(g);
   process(ts.leaf);
+  for (auto& g : ts.up_leaf) process(g);
+  for (auto& g : ts.down_x) process(g);
   if (ts.near) {
     process(ts.x_only);
     for (auto& g : ts.l2l) process(g);
@@ -671,6 +718,128 @@ void Fmm::run_group(const TaskSet& ts, const TaskGroup& g, const Real* spos, con
     phase(phase_id, [&] {
       launch_reduce<Real>(ts.reds.p + g.red_first, (int)g.red_count, partial, out, accumulate, st, R, na);
     });
+}
+
+// Non-leaf nodes of levels 1 .. max-1 (the root's up expansion is never used
+// and its down expansion is zero), their first children, and the tiles of
+// the folded upward (operator of the parent's level) and downward (operator
+// of the children's level) products.  Folding needs child k of every parent
+// at the same position in its parent box.
+void Fmm::build_fold_lists() {
+  const HostTree& t = *t_;
+  fold_pos_.fill(-1);
+  bool consistent = true;
+  std::vector<int32_t> par, ch;
+  fpar_off_.assign(maxl_ + 2, 0);
+  for (int L = 0; L <= maxl_; ++L) {
+    fpar_off_[L] = (int64_t)par.size();
+    for (int32_t n : t.by_level[L]) {
+      if (t.child0[n] < 0) continue;
+      for (int k = 0; k < 8; ++k) {
+        const int32_t c = t.child0[n] + k;
+        const int qx = t.ix[c] - 2 * t.ix[n], qy = t.iy[c] - 2 * t.iy[n], qz = t.iz[c] - 2 * t.iz[n];
+        const bool in = qx >= 0 && qx <= 1 && qy >= 0 && qy <= 1 && qz >= 0 && qz <= 1;
+        const int q = qx * 4 + qy * 2 + qz;
+        if (!in || (fold_pos_[k] >= 0 && fold_pos_[k] != q)) consistent = false;
+        fold_pos_[k] = q;
+      }
+      if (L >= 1) {
+        par.push_back(n);
+        ch.push_back(t.child0[n]);
+      }
+    }
+  }
+  fpar_off_[maxl_ + 1] = (int64_t)par.size();
+  fold_lists_ok_ = consistent && !par.empty();
+  if (!fold_lists_ok_) return;
+  cudaStream_t st = ctx_->stream;
+  fpar_.upload(par, st);
+  fch_.upload(ch, st);
+  std::vector<C2ETile> tu, td;
+  build_c2e_tiles(par, fpar_off_, tu, fup_toff_);
+  build_c2e_tiles(par, fpar_off_, td, fdn_toff_, 1);
+  fup_tiles_.upload(tu, st);
+  fdn_tiles_.upload(td, st);
+  const int n = 3 * P_;
+  size_t need = c2e_part_.n;
+  for (int R = 1; R <= R_; ++R)
+    for (int L = 1; L <= maxl_; ++L) {
+      need = std::max(need, c2e_part_size(n, 8 * n, (int)(fup_toff_[L + 1] - fup_toff_[L]), R));
+      need = std::max(need, c2e_part_size(8 * n, n, (int)(fdn_toff_[L + 1] - fdn_toff_[L]), R));
+      need = std::max(need, c2e_part_size(n, n, (int)(fwd_.upl_toff[L + 1] - fwd_.upl_toff[L]), R));
+    }
+  if (need > c2e_part_.n) c2e_part_.alloc(need);
+  NNK_CUDA(cudaStreamSynchronize(st));
+}
+
+// The folded operators U and D of every box width (see fmm.h), from the
+// check-to-equivalent operators A: on canonical boxes (a parent [0, w]^3 with
+// its children, or [0, 2w]^3), kernel matrices on the host, products on the
+// device (cuBLAS, FP64).  Needs a matvec whose M2L runs apart from the pair
+// tasks (Fourier-space or tensor-core M2L), and at most 1 GiB of operators.
+void Fmm::build_fold_operators() {
+  fold_ok_ = false;
+  if (!fold_lists_ok_ || !(fft_m2l_ || tensor_m2l_)) return;
+  const int n = 3 * P_;
+  const size_t blk = (size_t)n * n, per = 8 * blk;
+  if ((size_t)nops_ * 2 * per * sizeof(double) > ((size_t)1 << 30)) return;
+  cudaStream_t st = ctx_->stream;
+  fold_up_.alloc(nops_ * per);
+  fold_dn_.alloc(nops_ * per);
+  const auto lat = shell_lattice(p_.res, p_.shells);
+  std::vector<double> Mh(per), Lh(per);
+  DBuf<double> dM(per), dL(per);
+  Solver sv(st);
+  const double one = 1.0, zero = 0.0;
+  for (int o = 0; o < nops_; ++o) {
+    const double w = op_w_[o];
+    std::vector<double> pds(3 * P_), pds2(3 * P_), cus(3 * P_);
+    const double a[3] = {-w, -w, -w}, b[3] = {2 * w, 2 * w, 2 * w};
+    surface(a, b, p_.res, lat, pds.data());  // down surface of the parent [0, w]^3
+    const double a2[3] = {-2 * w, -2 * w, -2 * w}, b2[3] = {4 * w, 4 * w, 4 * w};
+    surface(a2, b2, p_.res, lat, pds2.data());  // down surface of the parent [0, 2w]^3
+    std::vector<double> Kb(blk);
+    for (int k = 0; k < 8; ++k) {
+      const int q = fold_pos_[k];
+      const int qd[3] = {(q >> 2) & 1, (q >> 1) & 1, q & 1};
+      double lo[3], hi[3];
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = qd[d] * 0.5 * w;
+        hi[d] = lo[d] + 0.5 * w;
+      }
+      surface(lo, hi, p_.res, lat, cus.data());  // child k of [0, w]^3: up surface
+      kernel_matrix(cus, pds, p_.eps, p_.mu, Kb, n);
+      std::copy(Kb.begin(), Kb.end(), Mh.begin() + k * blk);
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = qd[d] * w;
+        hi[d] = lo[d] + w;
+      }
+      surface(lo, hi, p_.res, lat, cus.data());  // child k of [0, 2w]^3: up surface
+      kernel_matrix(pds2, cus, p_.eps, p_.mu, Kb, n);
+      std::copy(Kb.begin(), Kb.end(), Lh.begin() + k * blk);
+    }
+    NNK_CUDA(cudaMemcpyAsync(dM.p, Mh.data(), per * 8, cudaMemcpyHostToDevice, st));
+    NNK_CUDA(cudaMemcpyAsync(dL.p, Lh.data(), per * 8, cudaMemcpyHostToDevice, st));
+    const double* A = ops_.p + (size_t)o * blk;
+    // U = A [M2M_0 .. M2M_7]  (n x 8n)
+    if (cublasDgemm(sv.b, CUBLAS_OP_N, CUBLAS_OP_N, n, 8 * n, n, &one, A, n, dM.p, n, &zero,
+                    fold_up_.p + (size_t)o * per, n) != CUBLAS_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "folded M2M operator product failed");
+    // D rows k n .. k n + n - 1 = A^T L2L_k  (8n x n)
+    for (int k = 0; k < 8; ++k)
+      if (cublasDgemm(sv.b, CUBLAS_OP_T, CUBLAS_OP_N, n, n, n, &one, A, n, dL.p + k * blk, n, &zero,
+                      fold_dn_.p + (size_t)o * per + (size_t)k * n, 8 * n) != CUBLAS_STATUS_SUCCESS)
+        throw Error(NNK_E_CUDA, "folded L2L operator product failed");
+    // the host copies above read pageable memory: keep Mh, Lh until done
+    NNK_CUDA(cudaStreamSynchronize(st));
+  }
+  fold_ok_ = true;
+}
+
+void Fmm::set_fold(bool on) {
+  NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
+  fold_on_ = on;
+  bump_version();
 }
 
 // Operator index of every (tree, level): one per distinct box width.
@@ -832,6 +1001,7 @@ void Fmm::build_operators() {
   for (int o = 0; o < nops_; ++o)
     if (info[o] != 0)
       throw Error(NNK_E_CUDA, "surface matrix factorization reported info=" + std::to_string(info[o]));
+  build_fold_operators();
 }
 
 namespace {
@@ -859,7 +1029,7 @@ void add_f32(long long n, const float* b, double* a, cudaStream_t st) {
 }  // namespace
 
 template <typename Real>
-void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R, bool near) {
+void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R, bool near, bool fold) {
   cudaStream_t st = ctx_->stream;
   Real* check = f64() ? (Real*)check64_.p : (Real*)check32_.p;
   const Real e2 = (Real)(p_.eps * p_.eps);
@@ -878,15 +1048,32 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
   if (tm && R != 1) throw Error(NNK_E_STATE, "tensor-core M2L takes one right-hand side per pass");
   if (tm) poll_m2l_error(m2l_, st);  // a wait that gave up in an earlier call
   const int* na = &ts == &fwd_ ? nact() : nullptr;
+  // folded M2M / L2L: the M2L must run apart from the pair tasks (it writes
+  // every check first), and nothing may need a non-leaf's check afterwards
+  const bool fo = fold && ts.fold && folded() && (tm || fm) && !save_up_;
+  float* m2l_src = tm && !m2l_.compressed ? m2l_.src.p : nullptr;
   // upward pass
   for (int L = maxl_; L >= 1; --L) {
+    if (fo) {
+      // leaves: S2M + C2E; non-leaves: U applied to their 8 children
+      run_group<Real>(ts, ts.up_leaf[L], spos, str, spos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS, R);
+      const int64_t nt = ts.upl_toff[L + 1] - ts.upl_toff[L];
+      const int64_t nf = fup_toff_[L + 1] - fup_toff_[L];
+      phase(NNK_PHASE_UP_C2E, [&] {
+        launch_c2e<Real>(ops_.p, n, 0, ts.upl_tiles.p + ts.upl_toff[L], (int)nt, ts.upl_nodes.p, check, str, regionA,
+                         P_, R, st, m2l_src, m2l_.NP, c2e_part_.p, c2e_part_.n, na);
+        NodeGemm g{fold_up_.p, (size_t)8 * n * n, n, 8 * n, 0, fup_tiles_.p + fup_toff_[L], fpar_.p, fch_.p,
+                   (long long)regionA, P_, R, 0, m2l_src, m2l_.NP};
+        launch_node_gemm<Real>(g, (int)nf, str + (size_t)C * regionA, str, st, c2e_part_.p, c2e_part_.n, na);
+      });
+      continue;
+    }
     if (ts.up[L].count == 0) continue;
     run_group<Real>(ts, ts.up[L], spos, str, spos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS, R);
     const int64_t nt = ts.up_toff[L + 1] - ts.up_toff[L];
     phase(NNK_PHASE_UP_C2E, [&] {
       launch_c2e<Real>(ops_.p, n, 0, ts.up_tiles.p + ts.up_toff[L], (int)nt, ts.up_nodes.p, check, str, regionA, P_,
-                       R, st, tm && !m2l_.compressed ? m2l_.src.p : nullptr, m2l_.NP, c2e_part_.p, c2e_part_.n,
-                       na);
+                       R, st, m2l_src, m2l_.NP, c2e_part_.p, c2e_part_.n, na);
     });
   }
   if (save_up_) NNK_CUDA(cudaMemcpyAsync(save_up_, check, sizeof(Real) * (size_t)N_ * n * R, cudaMemcpyDeviceToDevice,
@@ -915,7 +1102,9 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
                      (float)(1.0 / (8.0 * M_PI * p_.mu)), 1, NNK_PHASE_DOWN_PAIRS, R);
     phase(NNK_PHASE_DOWN_PAIRS, [&] { add_f32((long long)nc, check32_.p, (double*)check, st); });
   }
-  const std::vector<TaskGroup>& dgroups = near ? ts.l2l : (tm || fm) ? ts.down_nov : ts.down;
+  const std::vector<TaskGroup>& dgroups =
+      fo ? ts.down_x : near ? ts.l2l : (tm || fm) ? ts.down_nov : ts.down;
+  const int64_t dnB = regionA + (int64_t)P_ * N_;
   for (int L = 1; L <= maxl_; ++L) {
     if (dgroups[L].count > 0)
       run_group<Real>(ts, dgroups[L], spos, str, spos, check, e2, scale, (tm || fm) ? 1 : 0, NNK_PHASE_DOWN_PAIRS,
@@ -923,8 +1112,15 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     const int64_t nt = dn_toff_[L + 1] - dn_toff_[L];
     if (nt == 0) continue;
     phase(NNK_PHASE_DOWN_C2E, [&] {
-      launch_c2e<Real>(ops_.p, n, 1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str,
-                       regionA + (int64_t)P_ * N_, P_, R, st, nullptr, 0, c2e_part_.p, c2e_part_.n, na);
+      launch_c2e<Real>(ops_.p, n, 1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str, dnB, P_, R, st,
+                       nullptr, 0, c2e_part_.p, c2e_part_.n, na);
+      if (fo && L >= 2) {
+        // + D applied to the parents (level L - 1) for their 8 children
+        const int64_t nf = fdn_toff_[L] - fdn_toff_[L - 1];
+        NodeGemm g{fold_dn_.p, (size_t)8 * n * n, 8 * n, n, 0, fdn_tiles_.p + fdn_toff_[L - 1], fch_.p, fpar_.p,
+                   (long long)dnB, P_, R, 1, nullptr, 0};
+        launch_node_gemm<Real>(g, (int)nf, str + (size_t)C * dnB, str, st, c2e_part_.p, c2e_part_.n, na);
+      }
     });
   }
 }
@@ -944,7 +1140,7 @@ void Fmm::apply_impl(const double* d_in, const IoMap& in, double* d_out, const I
   const bool near = near32() && std::is_same<Real, double>::value;
   if (near)  // the same forces in FP32 for the near-field sums
     phase(NNK_PHASE_GATHER, [&] { launch_gather<float>(E_, goff_.p, gidx_.p, gw_.p, d_in, in, k0, R, str32_.p, st); });
-  far_field<Real>(fwd_, pos, str, E_, R, near);
+  far_field<Real>(fwd_, pos, str, E_, R, near, true);
   // leaf stage
   if (near) {
     run_group<Real>(fwd_, fwd_.leaf_far, pos, str, tpos, vel, e2, scale, 0, NNK_PHASE_LEAF_PAIRS, R);
@@ -1151,8 +1347,9 @@ std::pair<double, double> Fmm::autotune(int nrhs) {
     // FP64 groups (S2M/M2M, L2L, L2T + W-list) and FP32 groups (X-list P2L,
     // U-list P2P) of the NEAR32 split, each tuned in its own arithmetic
     std::vector<TaskGroup*> g64, g32;
-    for (auto& g : fwd_.up) g64.push_back(&g);
-    for (auto& g : fwd_.l2l) g64.push_back(&g);
+    for (auto& g : folded() ? fwd_.up_leaf : fwd_.up) g64.push_back(&g);
+    if (!folded())
+      for (auto& g : fwd_.l2l) g64.push_back(&g);
     g64.push_back(&fwd_.leaf_far);
     g32.push_back(&fwd_.x_only);
     g32.push_back(&fwd_.leaf_u);
@@ -1178,8 +1375,9 @@ std::pair<double, double> Fmm::autotune(int nrhs) {
   }
   std::vector<TaskGroup*> groups;
   const bool nov = tensor_m2l_ || fft_m2l_;
-  for (auto& g : fwd_.up) groups.push_back(&g);
-  for (auto& g : (nov ? fwd_.down_nov : fwd_.down)) groups.push_back(&g);
+  const bool fo = folded() && nov;
+  for (auto& g : fo ? fwd_.up_leaf : fwd_.up) groups.push_back(&g);
+  for (auto& g : (fo ? fwd_.down_x : nov ? fwd_.down_nov : fwd_.down)) groups.push_back(&g);
   groups.push_back(&fwd_.leaf);
   std::pair<double, double> res;
   auto go = [&](auto tag) {

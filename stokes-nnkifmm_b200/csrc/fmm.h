@@ -8,8 +8,12 @@
 //   [ leaf source entries | up-equivalent surfaces | down-equivalent surfaces ].
 // The per-node check-to-equivalent solves (kernel(...) \ check, Up.m:31-33,
 // DownNonleaf.m:42-46) become one precomputed FP64 operator per level, applied
-// to all nodes of the level as a batched product.
+// to all nodes of the level as a batched product.  With the M2L outside the
+// pair tasks, the M2M and L2L sums are folded into those products: one FP64
+// operator maps a parent's 8 children to its up-equivalent density, another
+// a parent to the L2L part of its children's down-equivalent densities.
 #pragma once
+#include <array>
 #include <memory>
 #include <vector>
 
@@ -101,6 +105,17 @@ struct TaskSet {
   std::vector<int64_t> up_off;
   DBuf<C2ETile> up_tiles;
   std::vector<int64_t> up_toff;
+  // folded form (the matvec's task set only): the M2M and L2L steps run as
+  // products with operators that include the check-to-equivalent step, so
+  // the pair tasks are the leaves' S2M (up_leaf) and the X-list P2L (down_x),
+  // and the C2E step of the upward pass covers the leaves only (upl_*)
+  bool fold = false;
+  std::vector<TaskGroup> up_leaf, down_x;  // per level
+  std::vector<int32_t> upl_nodes_host;
+  DBuf<int32_t> upl_nodes;
+  std::vector<int64_t> upl_off;
+  DBuf<C2ETile> upl_tiles;
+  std::vector<int64_t> upl_toff;
   int64_t partial_slots = 0;
 };
 
@@ -186,6 +201,10 @@ class Fmm {
   // FP64 work arrays (FP64 and NEAR32 modes); NEAR32 adds FP32 copies of the
   // points and forces for its near-field pair sums
   bool f64() const { return p_.precision != NNK_PREC_MIXED; }
+  // Folded M2M / L2L in the matvec (on by default where available); whether
+  // the matvec uses it.
+  void set_fold(bool on);
+  bool folded() const { return fold_ok_ && fold_on_; }
   bool near32() const { return p_.precision == NNK_PREC_NEAR32; }
   // scratch for host-pointer calls
   DBuf<double> io_in, io_out;
@@ -197,8 +216,10 @@ class Fmm {
   void adjoint_impl(const double* d_in, const IoMap& in, double* d_out, const IoMap& out, int k0, int R);
   // upward and downward passes of one direction (everything before the leaf stage)
   // near: the NEAR32 split of the matvec (FP32 X-list sums from str32_)
+  // fold: the folded M2M / L2L (the matvec only; ignored where not built)
   template <typename Real>
-  void far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R, bool near = false);
+  void far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R, bool near = false,
+                 bool fold = false);
   template <typename Real>
   void grad_impl(const double* d_f, const double* d_w, int layout, double* d_gt, double* d_gs);
   void build_adjoint();
@@ -221,8 +242,10 @@ class Fmm {
   template <typename Real>
   void run_group(const TaskSet& ts, const TaskGroup& g, const Real* spos, const Real* sstr, const Real* tpos,
                  Real* out, Real e2, Real scale, int accumulate, int phase_id, int R);
+  // dl: the tiles take the operator of level L + dl (the children's level
+  // for the folded L2L over parents at level L)
   void build_c2e_tiles(const std::vector<int32_t>& nodes, const std::vector<int64_t>& off,
-                       std::vector<C2ETile>& tiles, std::vector<int64_t>& toff);
+                       std::vector<C2ETile>& tiles, std::vector<int64_t>& toff, int dl = 0);
 
   nnk_ctx* ctx_;
   const HostTree* t_;
@@ -267,6 +290,22 @@ class Fmm {
   std::vector<double> op_w_;          // box width of each operator
   std::vector<int> op_of_;            // (group * (maxl + 1) + level) -> operator
   DBuf<C2ETile> dn_tiles_;  // per level, tiles of nodes sharing an operator
+  // folded M2M / L2L: per operator (box width w), U = A(w) [M2M_0 .. M2M_7]
+  // (3P x 8 * 3P; M2M_k: child k's up surface -> the down surface of its
+  // parent of width w) and D = [A(w)^T L2L_0; ..; A(w)^T L2L_7] (8 * 3P x 3P;
+  // L2L_k: the down surface of the parent of width 2w -> child k's up
+  // surface), child k = child0 + k; over the non-leaf nodes of each level
+  bool fold_ok_ = false;  // the tree and the operators allow folding
+  bool fold_lists_ok_ = false;
+  std::array<int, 8> fold_pos_{};  // position code (x * 4 + y * 2 + z) of child k in its parent
+  bool fold_on_ = true;   // the caller's choice
+  DBuf<double> fold_up_, fold_dn_;
+  DBuf<int32_t> fpar_, fch_;  // non-leaf nodes by level, and their first children
+  std::vector<int64_t> fpar_off_;
+  DBuf<C2ETile> fup_tiles_, fdn_tiles_;
+  std::vector<int64_t> fup_toff_, fdn_toff_;
+  void build_fold_lists();
+  void build_fold_operators();
   DBuf<double> c2e_part_;   // K-split partial sums of the small C2E launches
   std::vector<int64_t> dn_toff_;
   // transpose (built on first use): tasks with inverted lists, unified

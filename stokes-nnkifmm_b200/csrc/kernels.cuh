@@ -24,17 +24,19 @@ __device__ __forceinline__ void ldpos(const float* __restrict__ p, long long j, 
   z = v.z;
 }
 // 1/sqrt(d) for d > 0 (here d = r^2 + eps^2 >= eps^2): the hardware's FP64
-// approximation (PTX rsqrt.approx.ftz.f64, ~1e-6 relative) refined by two
-// Newton-Raphson steps y <- y (3 - d y^2) / 2, each of which squares the
-// relative error (measured on a B200 over d in [1e-12, 1e4]: 1.3e-12 after
-// one step, 3.1e-16 after two, against 1/sqrt in FP64).
+// approximation y (PTX rsqrt.approx.ftz.f64, relative error e ~ 1e-6) refined
+// by one third-order step of the binomial series
+//   d^(-1/2) = y (1 - t)^(-1/2) = y (1 + t/2 + 3 t^2/8 + 5 t^3/16 + ...),
+//   t = 1 - d y^2 ~ -2e,
+// truncated after t^2, so the step leaves 5 t^3 / 16 ~ 2.5 e^3 ~ 1e-18: below
+// FP64 rounding, in 5 FP64 operations where two Newton-Raphson steps take 7
+// (measured on a B200 over d in [1e-12, 1e4] against 1/sqrt in FP64: 1.3e-12
+// after one Newton step, 3.1e-16 after two, 2.6e-16 after this step).
 __device__ __forceinline__ double rsq(double d) {
   double y;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
-  const double h = 0.5 * d;
-  y = y * fma(-h * y, y, 1.5);
-  y = y * fma(-h * y, y, 1.5);
-  return y;
+  const double t = fma(-d * y, y, 1.0);
+  return fma(y * t, fma(0.375, t, 0.5), y);
 }
 __device__ __forceinline__ float rsq(float d) { return rsqrtf(d); }
 
@@ -625,69 +627,99 @@ inline void launch_reduce(const RedD* reds, int nreds, const Real* partial, Real
 }
 
 // -------------------------------------------------------------------- C2E
-// Check-to-equivalent step for the nodes of one level:
-//   dst(node, k) = Aop * check(node, k), Aop = A (upward) or A^T (downward),
-// for right-hand sides k < R, FP64 arithmetic.  A tile is up to 64 nodes that
-// share one operator (a level of one tree of the forest); A is the n x n
-// column-major operator ops + op * n^2.  check and dst hold, per surface
-// point p of a node, R consecutive 3-vectors: check[(node * P + p) * R + k].
-// 64 x 64 output tile (operator rows x (node, right-hand side) columns) per
-// CTA of 256 threads, each accumulating 4 x 4 in FP64; K in steps of 16 with
-// the next step's operands fetched into registers while the current one is
-// multiplied from shared memory.
+// Products of one fixed FP64 operator with the vectors of a list of nodes,
+//   dst(node, k) (+)= Aop * src(in_node, k),   k < R,
+// FP64 arithmetic.  Aop is M x Kd, column-major at ops + op * op_stride, or
+// (trans, square) its transpose.  src and dst hold, per surface point p of a
+// node, R consecutive 3-vectors: src[(in_node * P + p) * R + k], p < Kd / 3,
+// and dst[(base + node * P + p) * R + k], p < M / 3; a vector longer than one
+// node's 3P values runs on into the next node ids.  A tile is up to 64 nodes
+// sharing one operator (a level of one tree of the forest).  Uses:
+//   * the check-to-equivalent step of a level (M = Kd = 3P, in_node = node):
+//     Aop = A (upward, A = K_up^-1) or A^T (downward);
+//   * the upward step of a parent from its 8 children, folded into one
+//     operator (M = 3P, Kd = 8 * 3P, in_node = first child, node = parent);
+//   * the downward step of the 8 children from their parent, folded
+//     (M = 8 * 3P, Kd = 3P, in_node = parent, node = first child), added to
+//     the children's check-to-equivalent result.
+// 128 x 64 output tile (operator rows x (node, right-hand side) columns) per
+// CTA of 128 threads, each accumulating 8 x 8 in FP64: rows 4 ty + i and
+// 64 + 4 ty + i, columns 4 tx + j and 32 + 4 tx + j (ty = tid / 8, tx =
+// tid % 8), read from shared memory as 16-byte pairs (8 FMAs per load).  K in
+// steps of 8, the next step's operands fetched into registers while the
+// current one is multiplied from shared memory.
 constexpr int kC2ETileNodes = 64;
+constexpr int kC2EBM = 128;
+
+struct NodeGemm {
+  const double* ops;
+  size_t op_stride;
+  int M, Kd, trans;
+  const C2ETile* tiles;
+  const int* nodes;     // output node per tile column
+  const int* in_nodes;  // input node per tile column (nullptr: nodes)
+  long long base;
+  int P, R, accumulate;
+  float* m2l_dst;  // optional TF32 copy of the result (rows < NP)
+  int NP;
+};
+__device__ __forceinline__ C2ETile tiles_at(const NodeGemm& g, int i) { return g.tiles[i]; }
 
 template <typename Real>
-__global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops, int n, int trans,
-                                                  const C2ETile* __restrict__ tiles, const int* __restrict__ nodes,
-                                                  const Real* __restrict__ check, Real* __restrict__ dst,
-                                                  long long base, int P, int R, float* __restrict__ m2l_dst, int NP,
-                                                  int ksplit, int kper, double* __restrict__ part,
-                                                  const int* __restrict__ nact) {
-  constexpr int BM = 64, BN = 64, BK = 16;
-  __shared__ double As[BK][BM + 1];
-  __shared__ double Bs[BK][BN + 1];
+__global__ void __launch_bounds__(128, 2) c2e_kernel(NodeGemm g, const Real* __restrict__ check, Real* __restrict__ dst,
+                                                     int ksplit, int kper, double* __restrict__ part,
+                                                     const int* __restrict__ nact) {
+  constexpr int BM = kC2EBM, BN = 64, BK = 8, LA = BM + 2, LB = BN + 2;  // padded rows: conflict-free stores
+  __shared__ __align__(16) double As[BK * LA];
+  __shared__ __align__(16) double Bs[BK * LB];
   __shared__ int col_node[BN];
+  __shared__ int col_in[BN];
   __shared__ int col_k[BN];
-  const C2ETile tl = tiles[blockIdx.y];
-  if (nact && !nact[nodes[tl.first]]) return;  // the nodes of a tile belong to one tree
+  const C2ETile tl = tiles_at(g, blockIdx.y);
+  if (nact && !nact[g.nodes[tl.first]]) return;  // the nodes of a tile belong to one tree
+  const int M = g.M, Kd = g.Kd, P = g.P, R = g.R, trans = g.trans;
   const int zch = gridDim.z / ksplit;
   const int split = blockIdx.z / zch, zc = blockIdx.z - split * zch;
-  const int kbeg = split * kper, kend = min(n, kbeg + kper);
+  const int kbeg = split * kper, kend = min(Kd, kbeg + kper);
   const int m0 = blockIdx.x * BM, j0 = zc * BN;
   const int ncol = tl.count * R;
   if (j0 >= ncol) return;
-  const double* __restrict__ A = ops + (size_t)tl.op * n * n;
+  const double* __restrict__ A = g.ops + (size_t)tl.op * g.op_stride;
   const int tid = threadIdx.x;
   if (tid < BN) {
     const int j = j0 + tid;
-    col_node[tid] = j < ncol ? nodes[tl.first + j / R] : -1;
+    col_node[tid] = j < ncol ? g.nodes[tl.first + j / R] : -1;
+    col_in[tid] = j < ncol ? (g.in_nodes ? g.in_nodes : g.nodes)[tl.first + j / R] : -1;
     col_k[tid] = j < ncol ? j % R : 0;
   }
   __syncthreads();
-  const int tr = tid % 16, tc = tid / 16;
-  double acc[4][4];
+  const int tx = tid & 7, ty = tid >> 3;
+  double acc[8][8];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0;
-  // register staging: 4 A values and 4 B values per thread per K step
-  double ra[4], rb[4];
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0;
+  // staging: 8 operator values (BK x BM / 128) and 4 source values (BK x BN / 128)
+  double ra[8], rb[4];
+  // operator element e of the step: Aop[r][c] at c M + r (contiguous in r)
+  // or, transposed, A[c][r] at r Kd + c (contiguous in c = the K index)
+  auto a_index = [&](int e, int& kk, int& mm) {
+    if (!trans) { mm = e % BM; kk = e / BM; }
+    else { kk = e % BK; mm = e / BK; }
+  };
   auto load = [&](int k0) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int e = tid + 256 * q;  // 0 .. 1023 = BK * BM
+    for (int q = 0; q < 8; ++q) {
       int kk, mm;
-      if (!trans) { mm = e % BM; kk = e / BM; }   // A[r][c] at c*n + r: contiguous in r
-      else { kk = e % BK; mm = e / BK; }          // A^T[r][c] = A[c][r] at r*n + c: contiguous in c
+      a_index(tid + 128 * q, kk, mm);
       const int r = m0 + mm, c = k0 + kk;
-      ra[q] = (r < n && c < kend) ? (trans ? A[(size_t)r * n + c] : A[(size_t)c * n + r]) : 0.0;
+      ra[q] = (r < M && c < kend) ? (trans ? A[(size_t)r * Kd + c] : A[(size_t)c * M + r]) : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int e = tid + 256 * q;  // BK * BN
+      const int e = tid + 128 * q;
       const int kk = e % BK, nn = e / BK;
-      const int c = k0 + kk, node = col_node[nn];
+      const int c = k0 + kk, node = col_in[nn];
       double v = 0;
       if (c < kend && node >= 0) {
         const int p = c / 3, comp = c - 3 * p;
@@ -698,17 +730,15 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
   };
   auto store = [&]() {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int e = tid + 256 * q;
+    for (int q = 0; q < 8; ++q) {
       int kk, mm;
-      if (!trans) { mm = e % BM; kk = e / BM; }
-      else { kk = e % BK; mm = e / BK; }
-      As[kk][mm] = ra[q];
+      a_index(tid + 128 * q, kk, mm);
+      As[kk * LA + mm] = ra[q];
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int e = tid + 256 * q;
-      Bs[e % BK][e / BK] = rb[q];
+      const int e = tid + 128 * q;
+      Bs[(e % BK) * LB + e / BK] = rb[q];
     }
   };
   load(kbeg);
@@ -718,37 +748,50 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
     if (k0 + BK < kend) load(k0 + BK);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
-      double a[4], b[4];
+      double a[8], b[8];
+      const double2* a2 = reinterpret_cast<const double2*>(As + kk * LA);
+      const double2* b2 = reinterpret_cast<const double2*>(Bs + kk * LB);
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][tr + 16 * i];
+      for (int h = 0; h < 2; ++h) {
+        const double2 x0 = a2[(h * 64 + 4 * ty) / 2], x1 = a2[(h * 64 + 4 * ty) / 2 + 1];
+        a[4 * h] = x0.x;
+        a[4 * h + 1] = x0.y;
+        a[4 * h + 2] = x1.x;
+        a[4 * h + 3] = x1.y;
+        const double2 y0 = b2[(h * 32 + 4 * tx) / 2], y1 = b2[(h * 32 + 4 * tx) / 2 + 1];
+        b[4 * h] = y0.x;
+        b[4 * h + 1] = y0.y;
+        b[4 * h + 2] = y1.x;
+        b[4 * h + 3] = y1.y;
+      }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tc + 16 * j];
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int r = m0 + tr + 16 * i, jj = tc + 16 * j;
+    for (int j = 0; j < 8; ++j) {
+      const int r = m0 + (i >> 2) * 64 + 4 * ty + (i & 3);
+      const int jj = (j >> 2) * 32 + 4 * tx + (j & 3);
       const int node = col_node[jj];
       if (ksplit > 1) {
         // partial sum of this K range: part[split][tile][column][row]
-        if (r < n && node >= 0)
-          part[(((size_t)split * gridDim.y + blockIdx.y) * (kC2ETileNodes * R) + j0 + jj) * n + r] = acc[i][j];
+        if (r < M && node >= 0)
+          part[(((size_t)split * gridDim.y + blockIdx.y) * (kC2ETileNodes * R) + j0 + jj) * M + r] = acc[i][j];
         continue;
       }
-      if (r < n && node >= 0) {
+      if (r < M && node >= 0) {
         const int p = r / 3, comp = r - 3 * p;
-        dst[((base + (long long)P * node + p) * R + col_k[jj]) * 3 + comp] = (Real)acc[i][j];
-        if (m2l_dst) {
+        Real* o = dst + ((g.base + (long long)P * node + p) * R + col_k[jj]) * 3 + comp;
+        *o = g.accumulate ? (Real)((double)*o + acc[i][j]) : (Real)acc[i][j];
+        if (g.m2l_dst && r < g.NP) {
           uint32_t t;
           asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"((float)acc[i][j]));
-          m2l_dst[(size_t)node * NP + r] = __uint_as_float(t);
+          g.m2l_dst[(size_t)node * g.NP + r] = __uint_as_float(t);
         }
       }
     }
@@ -757,64 +800,71 @@ __global__ void __launch_bounds__(256) c2e_kernel(const double* __restrict__ ops
 // Sum of the K-range partials in split order (deterministic), written out
 // like the single-pass epilogue.
 template <typename Real>
-__global__ void c2e_reduce_kernel(const C2ETile* __restrict__ tiles, const int* __restrict__ nodes, int n, int R,
-                                  int ksplit, int ntiles, const double* __restrict__ part, Real* __restrict__ dst,
-                                  long long base, int P, float* __restrict__ m2l_dst, int NP,
-                                  const int* __restrict__ nact) {
+__global__ void c2e_reduce_kernel(NodeGemm g, int ksplit, int ntiles, const double* __restrict__ part,
+                                  Real* __restrict__ dst, const int* __restrict__ nact) {
   const int tile = blockIdx.y;
-  const C2ETile tl = tiles[tile];
-  if (nact && !nact[nodes[tl.first]]) return;
+  const C2ETile tl = tiles_at(g, tile);
+  if (nact && !nact[g.nodes[tl.first]]) return;
+  const int M = g.M, R = g.R;
   const int cols = kC2ETileNodes * R;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)cols * n;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)cols * M;
        e += (long long)gridDim.x * blockDim.x) {
-    const int j = (int)(e / n), r = (int)(e - (long long)j * n);
+    const int j = (int)(e / M), r = (int)(e - (long long)j * M);
     if (j >= tl.count * R) continue;
     double s = 0;
-    for (int q = 0; q < ksplit; ++q) s += part[(((size_t)q * ntiles + tile) * cols + j) * n + r];
-    const int node = nodes[tl.first + j / R], k = j % R;
+    for (int q = 0; q < ksplit; ++q) s += part[(((size_t)q * ntiles + tile) * cols + j) * M + r];
+    const int node = g.nodes[tl.first + j / R], k = j % R;
     const int p = r / 3, comp = r - 3 * p;
-    dst[((base + (long long)P * node + p) * R + k) * 3 + comp] = (Real)s;
-    if (m2l_dst) {
+    Real* o = dst + ((g.base + (long long)g.P * node + p) * R + k) * 3 + comp;
+    *o = g.accumulate ? (Real)((double)*o + s) : (Real)s;
+    if (g.m2l_dst && r < g.NP) {
       uint32_t t;
       asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"((float)s));
-      m2l_dst[(size_t)node * NP + r] = __uint_as_float(t);
+      g.m2l_dst[(size_t)node * g.NP + r] = __uint_as_float(t);
     }
   }
 }
 
-// K splits for a launch of `blocks` CTAs: enough CTAs for two per SM.
-inline int c2e_splits(int n, int blocks) {
+// K splits for a launch of `blocks` CTAs (two resident per SM): enough CTAs
+// for two per SM, each K range at least 64 long.
+inline int c2e_splits(int Kd, int blocks) {
   int k = 1;
-  while (k < 8 && blocks * k < 2 * 148 && n / (2 * k) >= 32) k *= 2;
+  while (k < 8 && blocks * k < 2 * 148 && Kd / (2 * k) >= 32) k *= 2;
   return k;
 }
-inline size_t c2e_part_size(int n, int ntiles, int R) {
-  const int blocks = ((n + 63) / 64) * ntiles * R;
-  const int k = c2e_splits(n, blocks);
-  return k > 1 ? (size_t)k * ntiles * kC2ETileNodes * R * n : 0;
+inline size_t c2e_part_size(int M, int Kd, int ntiles, int R) {
+  const int blocks = ((M + kC2EBM - 1) / kC2EBM) * ntiles * R;
+  const int k = c2e_splits(Kd, blocks);
+  return k > 1 ? (size_t)k * ntiles * kC2ETileNodes * R * M : 0;
 }
 
+template <typename Real>
+inline void launch_node_gemm(NodeGemm g, int ntiles, const Real* src, Real* dst, cudaStream_t st,
+                             double* part = nullptr, size_t part_n = 0, const int* nact = nullptr) {
+  if (ntiles == 0) return;
+  const int zch = (kC2ETileNodes * g.R + 63) / 64;
+  const int blocks = ((g.M + kC2EBM - 1) / kC2EBM) * ntiles * zch;
+  int ksplit = c2e_splits(g.Kd, blocks);
+  if (!part || part_n < c2e_part_size(g.M, g.Kd, ntiles, g.R)) ksplit = 1;
+  const int kper = ((g.Kd + ksplit - 1) / ksplit + 15) / 16 * 16;
+  dim3 grid((g.M + kC2EBM - 1) / kC2EBM, ntiles, zch * ksplit);
+  c2e_kernel<Real><<<grid, 128, 0, st>>>(g, src, dst, ksplit, kper, part, nact);
+  NNK_CHECK_LAUNCH();
+  if (ksplit > 1) {
+    dim3 g2(std::max(1, std::min(64, (kC2ETileNodes * g.R * g.M + 255) / 256)), ntiles);
+    c2e_reduce_kernel<Real><<<g2, 256, 0, st>>>(g, ksplit, ntiles, part, dst, nact);
+    NNK_CHECK_LAUNCH();
+  }
+}
+
+// The check-to-equivalent step of a level (n = 3P).
 template <typename Real>
 inline void launch_c2e(const double* ops, int n, int trans, const C2ETile* tiles, int ntiles, const int32_t* nodes,
                        const Real* check, Real* dst, int64_t base, int P, int R, cudaStream_t st,
                        float* m2l_dst = nullptr, int NP = 0, double* part = nullptr, size_t part_n = 0,
                        const int* nact = nullptr) {
-  if (ntiles == 0) return;
-  const int zch = (kC2ETileNodes * R + 63) / 64;
-  const int blocks = ((n + 63) / 64) * ntiles * zch;
-  int ksplit = c2e_splits(n, blocks);
-  if (!part || part_n < c2e_part_size(n, ntiles, R)) ksplit = 1;
-  const int kper = ((n + ksplit - 1) / ksplit + 15) / 16 * 16;
-  dim3 grid((n + 63) / 64, ntiles, zch * ksplit);
-  c2e_kernel<Real><<<grid, 256, 0, st>>>(ops, n, trans, tiles, nodes, check, dst, base, P, R, m2l_dst, NP, ksplit,
-                                         kper, part, nact);
-  NNK_CHECK_LAUNCH();
-  if (ksplit > 1) {
-    dim3 g2(std::max(1, std::min(64, (kC2ETileNodes * R * n + 255) / 256)), ntiles);
-    c2e_reduce_kernel<Real><<<g2, 256, 0, st>>>(tiles, nodes, n, R, ksplit, ntiles, part, dst, base, P, m2l_dst, NP,
-                                                nact);
-    NNK_CHECK_LAUNCH();
-  }
+  NodeGemm g{ops, (size_t)n * n, n, n, trans, tiles, nodes, nullptr, (long long)base, P, R, 0, m2l_dst, NP};
+  launch_node_gemm<Real>(g, ntiles, check, dst, st, part, part_n, nact);
 }
 
 // ---------------------------------------------------------------- scatter

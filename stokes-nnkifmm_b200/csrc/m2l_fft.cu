@@ -1,7 +1,7 @@
 // Fourier-space M2L (see m2l_fft.h).
 //
 // Transforms are separable DFTs of length G over the zero-padded lattice,
-// written out as small sums in shared memory (G = 12 for res = 6): each pass
+// written out as small sums in shared memory: each pass
 // maps one axis, and only the res non-zero inputs (forward) or res needed
 // outputs (inverse) of that axis are touched.  Frequency index
 // k = (kx * G + ky) * H + kz, H = G / 2 + 1 (half spectrum along z).
@@ -67,7 +67,7 @@ __global__ void fft_spectra_kernel(int G, int res, const double* __restrict__ sl
   const int code = slot_code[s];
   const int o[3] = {code / 49 - 3, (code / 7) % 7 - 3, code % 7 - 3};
   const int tid = threadIdx.x, nt = blockDim.x;
-  auto sd = [&](int a) { return a < G / 2 ? a : a - G; };
+  auto sd = [&](int a) { return 2 * a < G ? a : a - G; };  // signed grid index
   auto tw = [&](int m, double& c, double& sn) {  // e^{-2 pi i m / G}
     double si;
     sincospi(2.0 * (m % G) / G, &si, &c);
@@ -148,7 +148,7 @@ __global__ void fft_forward_kernel(int G_rt, int res_rt, int P, const int* __res
   extern __shared__ __align__(16) unsigned char fft_smem[];
   T2* smq = reinterpret_cast<T2*>(fft_smem);
   const int res = RES > 0 ? RES : res_rt;
-  const int G = RES > 0 ? 2 * RES : G_rt;
+  const int G = RES > 0 ? fft_grid(RES) : G_rt;
   const int H = G / 2 + 1, C = 3 * R, r3 = res * res * res;
   T2* tw = smq;                          // G
   T2* Z = tw + G;                        // [cr][x][y][kz]   C res res H
@@ -262,15 +262,47 @@ __global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* 
   for (int c = 0; c < C; ++c) out[(size_t)c * NK] = acc[c];
 }
 
+template <typename Real>
+constexpr size_t family_smem() {
+  return 36 * 128 * sizeof(typename Cplx<Real>::t) + 343 * sizeof(int);
+}
+
+// Asynchronous 8- or 16-byte copy global -> shared (cp.async; 16 bytes bypass
+// L1), and its group commit / wait: this thread's copies land in its own
+// shared-memory slots, so no barrier is needed, only the wait.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Offset-code increment of difference dl = (ex+1) * 9 + (ey+1) * 3 + (ez+1)
+// over difference (-1, -1, -1); codes are (x+3) * 49 + (y+3) * 7 + (z+3).
+__device__ __forceinline__ int code_step(int dl) { return (dl / 9) * 49 + ((dl / 3) % 3) * 7 + dl % 3; }
+
+// This thread's 6 kernel spectra at frequency k (Kp) into its slots kb.
+template <typename T2>
+__device__ __forceinline__ void issue_kernel_spectra(T2* kb, const T2* Kp, int NK) {
+#pragma unroll
+  for (int c = 0; c < 6; ++c) cp_async<sizeof(T2)>(kb + c * 128, Kp + (size_t)c * NK);
+}
+
 // Parent-grouped accumulation (see FftFamily): thread (family, frequency k)
 // holds the 8 children's accumulators of one right-hand side at a time; per
 // (P, N) record the 8 source spectra go to this thread's own shared-memory
 // slots, then for each of the 27 values of pos_v - pos_i present in the
-// record the kernel spectrum of offset 2 d + delta is loaded once and applied
-// to every pair with that difference.  Loop bounds and child positions are
-// compile-time, so accumulators stay in registers.  Every right-hand side
-// sums its pairs in the same order, so a pass of R right-hand sides gives
-// each of them bitwise the result of a pass of one.
+// record the kernel spectrum of offset 2 d + delta is applied to every pair
+// with that difference.  The kernel spectra come in by cp.async into two
+// shared-memory buffers per thread: the next present difference's spectrum
+// is in flight while the current one is applied.  Loop bounds and child
+// positions are compile-time, so accumulators stay in registers.  Every
+// right-hand side sums its pairs in the same order, so a pass of R
+// right-hand sides gives each of them bitwise the result of a pass of one.
 template <typename Real>
 __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
     int NK, const FftFamily* __restrict__ fams, const FftFamilyPair* __restrict__ pairs,
@@ -279,37 +311,38 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
     const int* __restrict__ tgt_node, const int* __restrict__ nact, int R) {
   using T2 = typename Cplx<Real>::t;
   constexpr int BLK = 128;
-  __shared__ T2 sq[24 * BLK];  // this thread's source spectra: [pos * 3 + c][thread]
-  const FftFamily fam = fams[blockIdx.x];
+  extern __shared__ __align__(16) unsigned char fam_smem[];  // family_smem<Real>() bytes
+  T2* sq = reinterpret_cast<T2*>(fam_smem);  // this thread's source spectra: [pos * 3 + c][thread]
+  T2* sk = sq + 24 * BLK;                    // its kernel spectra, two buffers: [buf * 6 + c][thread]
+  int* sso = reinterpret_cast<int*>(sk + 12 * BLK);  // spectrum slot of each offset code at the family's width
+  const FftFamily* fam = fams + blockIdx.x;
+  const int first = fam->first, count = fam->count;
+  // every record of a family has the same operator (checked at build)
+  const int* so = spec_of + (size_t)(count ? pairs[first].op : 0) * 343;
+  for (int e = threadIdx.x; e < 343; e += BLK) sso[e] = so[e];
+  __syncthreads();
   const int k = blockIdx.y * BLK + threadIdx.x;
   if (nact) {
     int t0 = 0;
-    while (t0 < 7 && fam.tgt[t0] < 0) ++t0;
-    if (!nact[tgt_node[fam.tgt[t0]]]) return;
+    while (t0 < 7 && fam->tgt[t0] < 0) ++t0;
+    if (!nact[tgt_node[fam->tgt[t0]]]) return;
   }
   if (k >= NK) return;
   const int C = 3 * R;
   T2* my = sq + threadIdx.x;
+  T2* kb = sk + threadIdx.x;
   for (int r = 0; r < R; ++r) {
   T2 acc[8][3];
 #pragma unroll
   for (int a = 0; a < 8; ++a)
 #pragma unroll
     for (int c = 0; c < 3; ++c) acc[a][c] = cmake((Real)0, (Real)0);
-  for (int pr = fam.first; pr < fam.first + fam.count; ++pr) {
+  for (int pr = first; pr < first + count; ++pr) {
     const FftFamilyPair rec = pairs[pr];
     const uint64_t mask = (uint64_t)rec.mask_lo | ((uint64_t)rec.mask_hi << 32);
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const int sl = rec.src[b];
-      if (sl >= 0) {
-        const T2* Q = qhat + ((size_t)sl * C + 3 * r) * NK + k;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) my[(b * 3 + c) * BLK] = Q[(size_t)c * NK];
-      }
-    }
     const int dx2 = 2 * (rec.dcode / 9 - 1), dy2 = 2 * ((rec.dcode / 3) % 3 - 1), dz2 = 2 * (rec.dcode % 3 - 1);
-    const int* so = spec_of + (size_t)rec.op * 343;
+    // the differences present in this record
+    uint32_t gmask = 0;
 #pragma unroll
     for (int dl = 0; dl < 27; ++dl) {
       const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
@@ -320,17 +353,39 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
         if (bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)
           gm |= 1ull << (a * 8 + (bx * 4 + by * 2 + bz));
       }
-      const uint64_t bits = mask & gm;
-      if (bits == 0) continue;
-      const int code = (dx2 + ex + 3) * 49 + (dy2 + ey + 3) * 7 + (dz2 + ez + 3);
-      const T2* Kp = spec + (size_t)so[code] * 6 * NK + k;
-      const T2 kxx = Kp[0], kxy = Kp[NK], kxz = Kp[2 * NK], kyy = Kp[3 * NK], kyz = Kp[4 * NK], kzz = Kp[5 * NK];
+      if (mask & gm) gmask |= 1u << dl;
+    }
+    const int cbase = (dx2 + 2) * 49 + (dy2 + 2) * 7 + (dz2 + 2);  // code of difference (-1, -1, -1)
+    const int ncode = __ffs(gmask) - 1;
+    if (gmask) issue_kernel_spectra<T2>(kb, spec + (size_t)sso[cbase + code_step(ncode)] * 6 * NK + k, NK);
+    cp_async_commit();
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int sl = rec.src[b];
+      if (sl >= 0) {
+        const T2* Q = qhat + ((size_t)sl * C + 3 * r) * NK + k;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) my[(b * 3 + c) * BLK] = Q[(size_t)c * NK];
+      }
+    }
+    int buf = 0;
+#pragma unroll
+    for (int dl = 0; dl < 27; ++dl) {
+      if (!((gmask >> dl) & 1)) continue;
+      const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
+      const uint32_t rest = gmask & ~((2u << dl) - 1u);
+      if (rest) issue_kernel_spectra<T2>(kb + (buf ^ 1) * 6 * BLK, spec + (size_t)sso[cbase + code_step(__ffs(rest) - 1)] * 6 * NK + k, NK);
+      cp_async_commit();
+      cp_async_wait_prior();  // this difference's spectrum has landed
+      const T2* K = kb + buf * 6 * BLK;
+      const T2 kxx = K[0], kxy = K[BLK], kxz = K[2 * BLK], kyy = K[3 * BLK], kyz = K[4 * BLK], kzz = K[5 * BLK];
+      buf ^= 1;
 #pragma unroll
       for (int a = 0; a < 8; ++a) {
         const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
         if (!(bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)) continue;
         const int b = bx * 4 + by * 2 + bz;
-        if (!((bits >> (a * 8 + b)) & 1)) continue;
+        if (!((mask >> (a * 8 + b)) & 1)) continue;
         const T2 qx = my[(b * 3) * BLK], qy = my[(b * 3 + 1) * BLK], qz = my[(b * 3 + 2) * BLK];
         cmac(acc[a][0], kxx, qx);
         cmac(acc[a][0], kxy, qy);
@@ -346,7 +401,7 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
   }
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
-    const int t = fam.tgt[a];
+    const int t = fam->tgt[a];
     if (t < 0) continue;
     T2* out = chat + ((size_t)t * C + 3 * r) * NK + k;
 #pragma unroll
@@ -366,7 +421,7 @@ __global__ void fft_inverse_kernel(int G_rt, int res_rt, int P, const int* __res
   extern __shared__ __align__(16) unsigned char fft_smem[];
   T2* smc = reinterpret_cast<T2*>(fft_smem);
   const int res = RES > 0 ? RES : res_rt;
-  const int G = RES > 0 ? 2 * RES : G_rt;
+  const int G = RES > 0 ? fft_grid(RES) : G_rt;
   const int H = G / 2 + 1, C = 3 * R, r3 = res * res * res;
   T2* tw = smc;                   // G
   T2* X = tw + G;                 // [cr][x][ky][kz]  C res G H
@@ -514,7 +569,11 @@ void build_families(const HostTree& t, const std::vector<int>& tgt, const std::v
   std::vector<FftFamilyPair> pairs;
   for (size_t fi = 0; fi < fams.size(); ++fi) {
     fams[fi].first = (int)pairs.size();
-    for (auto& kv : recs[fi]) pairs.push_back(kv.second);
+    for (auto& kv : recs[fi]) {
+      // the accumulation reads one row of spec_of per family
+      if (kv.second.op != recs[fi].begin()->second.op) return;
+      pairs.push_back(kv.second);
+    }
     fams[fi].count = (int)pairs.size() - fams[fi].first;
   }
   std::vector<int> spec_of(std::max<size_t>(nops, 1) * 343, -1);
@@ -544,6 +603,8 @@ void set_smem_attributes(int optin) {
   NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<4, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<6, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<6, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_accumulate_family_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)family_smem<Real>()));
 }
 
 template <typename Real>
@@ -562,7 +623,7 @@ void run_fft_m2l(FftM2L& f, const Real* str, long long upbase, int R, Real* chec
                                                         f.NK, nact);
   NNK_CHECK_LAUNCH();
   if (f.family) {
-    fft_accumulate_family_kernel<Real><<<dim3(f.nfam, (f.NK + 127) / 128), 128, 0, st>>>(
+    fft_accumulate_family_kernel<Real><<<dim3(f.nfam, (f.NK + 127) / 128), 128, family_smem<Real>(), st>>>(
         f.NK, f.fams.p, f.fpairs.p, f.spec_of.p, spec, qhat, chat, f.tgt_node.p, nact, R);
     NNK_CHECK_LAUNCH();
     inv<<<f.ntgt, 256, inverse_smem(G, res, R, es), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, chat, R, check, f.NK,
@@ -596,7 +657,8 @@ int fft_m2l_max_rhs(int res, bool fp64) {
   const int optin = optin_smem();
   const size_t es = fp64 ? sizeof(double) : sizeof(float);
   for (int R : {6, 4, 3, 2, 1})
-    if (forward_smem(2 * res, res, R, es) <= (size_t)optin && inverse_smem(2 * res, res, R, es) <= (size_t)optin)
+    if (forward_smem(fft_grid(res), res, R, es) <= (size_t)optin &&
+        inverse_smem(fft_grid(res), res, R, es) <= (size_t)optin)
       return R;
   return 0;
 }
@@ -606,7 +668,7 @@ void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu
   if (res > 8) throw Error(NNK_E_ARG, "Fourier M2L supports coronaRes up to 8");
   f.fp64 = fp64;
   f.res = res;
-  f.G = 2 * res;
+  f.G = fft_grid(res);
   const int G = f.G, H = G / 2 + 1;
   f.NK = G * G * H;
   f.Rcap = Rmax;

@@ -5,9 +5,9 @@
 // v in V(i) at offset o = (v - i) in box widths, the reference adds
 //   check_i(a) += sum_b K((a - b - (res - 1) o) h) q_v(b)
 // over lattice points a, b (the kernel matrix of upsurf(v) -> upsurf(i)).
-// This is a discrete convolution, so with the densities zero-padded to a
-// G^3 grid (G = 2 res >= 2 res - 1, no wrap-around) it becomes a pointwise
-// product of spectra:
+// This is a discrete convolution: a - b spans 2 res - 1 values per axis, so
+// with the densities zero-padded to a G^3 grid, G = 2 res - 1, the cyclic
+// convolution has no wrap-around and becomes a pointwise product of spectra:
 //   C_i(k) = sum_{v in V(i)} Khat_{w,o}(k) Q_v(k),
 // Khat the 3 x 3 (symmetric) spectrum of the kernel sampled on the difference
 // grid, Q_v the spectrum of v's densities.  Per V pair this costs
@@ -23,6 +23,10 @@
 #include "tree.h"
 
 namespace nnk {
+
+// Grid size of the transforms for a res^3 lattice (11 for res = 6: 11 x 11 x 6
+// = 726 frequencies in the half spectrum).
+__host__ __device__ constexpr int fft_grid(int res) { return 2 * res - 1; }
 
 // Parent-grouped form of the accumulation for one right-hand side: every V
 // pair (i, v) of the reference's lists joins a child i of a parent P with a

@@ -52,7 +52,7 @@ class FmmParams(C.Structure):
 class FmmStats(C.Structure):
     _fields_ = [("pairs_leaf", _i64), ("pairs_p2p", _i64), ("pairs_up", _i64), ("pairs_down", _i64),
                 ("m2l_pairs", _i64), ("c2e_columns", _i64), ("m2l_tile_rows", _i64), ("surface_points", _i32),
-                ("levels", _i32), ("m2l_rank", _i32), ("reserved", _i32)]
+                ("levels", _i32), ("m2l_rank", _i32), ("folded", _i32)]
 
 
 class SolveParams(C.Structure):
@@ -87,6 +87,7 @@ SIGNATURES = {
     "nnk_fmm_reduced_apply": (_i32, [_vp, _vp, _vp, _i32, _i32]),
     "nnk_fmm_reduced_solve": (_i32, [_vp, _vp, _vp, _i32, _i32]),
     "nnk_fmm_stats_get": (_i32, [_vp, C.POINTER(FmmStats)]),
+    "nnk_fmm_set_fold": (_i32, [_vp, _i32]),
     "nnk_fmm_destroy": (_i32, [_vp]),
     "nnk_fmm_apply_adjoint": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32]),
     "nnk_fmm_source_count": (_i32, [_vp, _pi64]),

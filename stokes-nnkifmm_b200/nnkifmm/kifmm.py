@@ -108,6 +108,12 @@ class KIFMM:
         L.check(L.lib.nnk_fmm_set_eps(self.h, float(eps)), self.ctx.h, "setEps")
         self.arguments["kernelPar"] = (float(eps), self.arguments["kernelPar"][1])
 
+    def setFold(self, on=True):
+        """Run the matvec's M2M and L2L folded into the check-to-equivalent
+        products (default where available; stats()["folded"] says whether it
+        is in use) or as pair sums followed by those products."""
+        L.check(L.lib.nnk_fmm_set_fold(self.h, 1 if on else 0), self.ctx.h, "setFold")
+
     def sourceCount(self):
         c = C.c_int64()
         L.check(L.lib.nnk_fmm_source_count(self.h, C.byref(c)))

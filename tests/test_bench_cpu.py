@@ -50,12 +50,12 @@ def test_c2e_dominant_phase_and_uncompressed_m2l():
 
 def test_fourier_m2l_dominant_phase_fp64():
     """FP64 matvec with its Fourier-space M2L as the longest phase: 9 complex
-    multiply-adds (72 flops) per V pair and frequency (12^2 x 7 = 1008 for
-    p = 6) against the nominal FP64 SIMT rate."""
+    multiply-adds (72 flops) per V pair and frequency (11^2 x 6 = 726 for
+    p = 6: transform length 2 p - 1) against the nominal FP64 SIMT rate."""
     phases = dict(PHASES, m2l=(6.0, 3))
     r = bench.roofline(phases, STATS, "fp64", PEAKS, "fourier")
-    assert "fft_accumulate_kernel (FP64" in r["kernel"] and r["bound"] == "fp64"
-    assert r["achieved"] == pytest.approx(72.0 * 1008 * STATS["m2l_pairs"] / 6e-3 / 1e12)
+    assert "fft_accumulate_family_kernel (FP64" in r["kernel"] and r["bound"] == "fp64"
+    assert r["achieved"] == pytest.approx(72.0 * 726 * STATS["m2l_pairs"] / 6e-3 / 1e12)
     assert r["peak"] == pytest.approx(bench.FP32_NOMINAL_TFLOPS / 2)
     assert r["ms_per_launch"] == pytest.approx(2.0)
 
