@@ -263,17 +263,21 @@ int nnk_fmm_autotune(nnk_fmm* fmm, int32_t nrhs, double* ms_before, double* ms_a
  * spectra) for kernelPar(1) = eps, keeping the tree-dependent task lists:
  * the cheap way to evaluate the operator at eps +- d for its eps-derivative. */
 int nnk_fmm_set_eps(nnk_fmm* fmm, double eps);
-/* Folded M2M / L2L in the matvec (on by default where available): a
+/* Folded M2M / L2L in the matvec: mode 0 off (the default), 1 where it
+ * pays (at least 64 non-leaf nodes per box width), 2 wherever available.  A
  * parent's up-equivalent density becomes one FP64 product
  * A(w) [M2M_0 .. M2M_7] with its 8 children's (Up.m:31-33 applied to the
  * M2M sums of upwardPass.m:81-93), and the L2L part of a child's
  * down-equivalent density the product A(w)^T L2L_k with its parent's
- * (the parentsurf term of DownNonleaf.m:42-46), in place of the pair sums followed by the
- * check-to-equivalent step: the same operator up to FP64 rounding.
- * Available with the Fourier-space or tensor-core M2L, for trees whose
- * folded operators take at most 1 GiB; the transpose, the gradients and
- * the eps-derivative always run unfolded.  on = 0 turns it off. */
-int nnk_fmm_set_fold(nnk_fmm* fmm, int32_t on);
+ * (the parentsurf term of DownNonleaf.m:42-46), in place of the pair sums
+ * followed by the check-to-equivalent step.  Only for regularized
+ * operators (NNK_PREC_MIXED, or reg > 0), where it is the same operator to
+ * ~3e-7; with the exact inverses the folded products lift FP64 rounding by
+ * the surface matrices' condition number (4e-5 on a NEAREST cloud), so
+ * there the call leaves the pair sums in place.  Needs the Fourier-space or
+ * tensor-core M2L and at most 1 GiB of folded operators; the transpose, the
+ * gradients and the eps-derivative always run unfolded. */
+int nnk_fmm_set_fold(nnk_fmm* fmm, int32_t mode);
 /* Number of source origins: fine points (NEAREST) or potential rows. */
 int nnk_fmm_source_count(const nnk_fmm* fmm, int64_t* count);
 /* Gradient of <weights, apply(forces)> with respect to the positions, with

@@ -429,7 +429,7 @@ int nnk_fmm_set_fold(nnk_fmm* fmm, int32_t on) {
   nnk_ctx* ctx = fmm->ctx;
   API_TRY
   need_gpu(ctx);
-  fmm->f->set_fold(on != 0);
+  fmm->f->set_fold(on);
   API_CATCH(ctx)
 }
 

@@ -772,14 +772,40 @@ void Fmm::build_fold_lists() {
   NNK_CUDA(cudaStreamSynchronize(st));
 }
 
+namespace {
+// Kernel matrix in the layout of kernel_matrix (row 3a+i: target a, column
+// 3b+j: source b; column-major, leading dimension ld), on the device.
+__global__ void kernel_matrix_kernel(const double* __restrict__ src, int ns, const double* __restrict__ tgt, int nt,
+                                     double e2, double c, double* __restrict__ K, int ld) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)ns * nt) return;
+  const int a = (int)(e % nt), b = (int)(e / nt);
+  const double r[3] = {tgt[3 * a] - src[3 * b], tgt[3 * a + 1] - src[3 * b + 1], tgt[3 * a + 2] - src[3 * b + 2]};
+  const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+  const double d = r2 + e2;
+  const double inv = c / (d * sqrt(d));
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      K[(size_t)(3 * b + j) * ld + 3 * a + i] = (r[i] * r[j] + (i == j ? r2 + 2 * e2 : 0.0)) * inv;
+}
+}  // namespace
+
 // The folded operators U and D of every box width (see fmm.h), from the
 // check-to-equivalent operators A: on canonical boxes (a parent [0, w]^3 with
-// its children, or [0, 2w]^3), kernel matrices on the host, products on the
-// device (cuBLAS, FP64).  Needs a matvec whose M2L runs apart from the pair
-// tasks (Fourier-space or tensor-core M2L), and at most 1 GiB of operators.
-void Fmm::build_fold_operators() {
+// its children, or [0, 2w]^3), kernel matrices and products on the device
+// (FP64; the products by cuBLAS).  Built for regularized (Tikhonov)
+// check-to-equivalent operators only: with the exact inverses (cond ~1e10)
+// the folded operators A M2M_k carry FP64 rounding relative to |A| |M2M_k|
+// into the very large equivalent densities of NEAREST trees, 4e-5 away from
+// the pair sums on a 1200-point NEAREST cloud, where the regularized ones
+// stay within 3e-7.  Also needs a matvec whose M2L runs apart from the pair
+// tasks (Fourier-space or tensor-core M2L), at most 1 GiB of operators, and
+// (unless forced) at least 64 non-leaf nodes per operator: below that the
+// set-up costs more than the folded products save.
+void Fmm::build_fold_operators(bool force) {
   fold_ok_ = false;
-  if (!fold_lists_ok_ || !(fft_m2l_ || tensor_m2l_)) return;
+  if (exact_ops_ || !fold_lists_ok_ || !(fft_m2l_ || tensor_m2l_)) return;
+  if (!force && fpar_off_.back() < 64 * (int64_t)nops_) return;
   const int n = 3 * P_;
   const size_t blk = (size_t)n * n, per = 8 * blk;
   if ((size_t)nops_ * 2 * per * sizeof(double) > ((size_t)1 << 30)) return;
@@ -787,39 +813,48 @@ void Fmm::build_fold_operators() {
   fold_up_.alloc(nops_ * per);
   fold_dn_.alloc(nops_ * per);
   const auto lat = shell_lattice(p_.res, p_.shells);
-  std::vector<double> Mh(per), Lh(per);
-  DBuf<double> dM(per), dL(per);
-  Solver sv(st);
-  const double one = 1.0, zero = 0.0;
+  // per operator: [parent down surface (w), parent down surface (2w),
+  // 8 children's up surfaces of [0, w]^3, 8 of [0, 2w]^3]
+  const size_t ps = 3 * (size_t)P_;
+  std::vector<double> surf((size_t)nops_ * 18 * ps);
   for (int o = 0; o < nops_; ++o) {
     const double w = op_w_[o];
-    std::vector<double> pds(3 * P_), pds2(3 * P_), cus(3 * P_);
+    double* S = surf.data() + (size_t)o * 18 * ps;
     const double a[3] = {-w, -w, -w}, b[3] = {2 * w, 2 * w, 2 * w};
-    surface(a, b, p_.res, lat, pds.data());  // down surface of the parent [0, w]^3
+    surface(a, b, p_.res, lat, S);
     const double a2[3] = {-2 * w, -2 * w, -2 * w}, b2[3] = {4 * w, 4 * w, 4 * w};
-    surface(a2, b2, p_.res, lat, pds2.data());  // down surface of the parent [0, 2w]^3
-    std::vector<double> Kb(blk);
+    surface(a2, b2, p_.res, lat, S + ps);
     for (int k = 0; k < 8; ++k) {
       const int q = fold_pos_[k];
       const int qd[3] = {(q >> 2) & 1, (q >> 1) & 1, q & 1};
-      double lo[3], hi[3];
+      double lo[3], hi[3], lo2[3], hi2[3];
       for (int d = 0; d < 3; ++d) {
         lo[d] = qd[d] * 0.5 * w;
         hi[d] = lo[d] + 0.5 * w;
+        lo2[d] = qd[d] * w;
+        hi2[d] = lo2[d] + w;
       }
-      surface(lo, hi, p_.res, lat, cus.data());  // child k of [0, w]^3: up surface
-      kernel_matrix(cus, pds, p_.eps, p_.mu, Kb, n);
-      std::copy(Kb.begin(), Kb.end(), Mh.begin() + k * blk);
-      for (int d = 0; d < 3; ++d) {
-        lo[d] = qd[d] * w;
-        hi[d] = lo[d] + w;
-      }
-      surface(lo, hi, p_.res, lat, cus.data());  // child k of [0, 2w]^3: up surface
-      kernel_matrix(pds2, cus, p_.eps, p_.mu, Kb, n);
-      std::copy(Kb.begin(), Kb.end(), Lh.begin() + k * blk);
+      surface(lo, hi, p_.res, lat, S + (2 + k) * ps);
+      surface(lo2, hi2, p_.res, lat, S + (10 + k) * ps);
     }
-    NNK_CUDA(cudaMemcpyAsync(dM.p, Mh.data(), per * 8, cudaMemcpyHostToDevice, st));
-    NNK_CUDA(cudaMemcpyAsync(dL.p, Lh.data(), per * 8, cudaMemcpyHostToDevice, st));
+  }
+  DBuf<double> dS;
+  dS.upload(surf, st);
+  DBuf<double> dM(per), dL(per);
+  Solver sv(st);
+  const double one = 1.0, zero = 0.0;
+  const double e2 = p_.eps * p_.eps, c = 1.0 / (8.0 * M_PI * p_.mu);
+  const unsigned kb = (unsigned)(((size_t)P_ * P_ + 255) / 256);
+  for (int o = 0; o < nops_; ++o) {
+    const double* S = dS.p + (size_t)o * 18 * ps;
+    for (int k = 0; k < 8; ++k) {
+      // M2M_k: child k's up surface -> the parent's down surface
+      kernel_matrix_kernel<<<kb, 256, 0, st>>>(S + (2 + k) * ps, P_, S, P_, e2, c, dM.p + k * blk, n);
+      NNK_CHECK_LAUNCH();
+      // L2L_k: the parent's down surface -> child k's up surface
+      kernel_matrix_kernel<<<kb, 256, 0, st>>>(S + ps, P_, S + (10 + k) * ps, P_, e2, c, dL.p + k * blk, n);
+      NNK_CHECK_LAUNCH();
+    }
     const double* A = ops_.p + (size_t)o * blk;
     // U = A [M2M_0 .. M2M_7]  (n x 8n)
     if (cublasDgemm(sv.b, CUBLAS_OP_N, CUBLAS_OP_N, n, 8 * n, n, &one, A, n, dM.p, n, &zero,
@@ -830,15 +865,16 @@ void Fmm::build_fold_operators() {
       if (cublasDgemm(sv.b, CUBLAS_OP_T, CUBLAS_OP_N, n, n, n, &one, A, n, dL.p + k * blk, n, &zero,
                       fold_dn_.p + (size_t)o * per + (size_t)k * n, 8 * n) != CUBLAS_STATUS_SUCCESS)
         throw Error(NNK_E_CUDA, "folded L2L operator product failed");
-    // the host copies above read pageable memory: keep Mh, Lh until done
-    NNK_CUDA(cudaStreamSynchronize(st));
   }
+  NNK_CUDA(cudaStreamSynchronize(st));  // dS, dM, dL are freed on return
   fold_ok_ = true;
 }
 
-void Fmm::set_fold(bool on) {
+void Fmm::set_fold(int mode) {
+  if (mode < 0 || mode > 2) throw Error(NNK_E_ARG, "fold mode must be 0, 1 or 2");
   NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
-  fold_on_ = on;
+  fold_on_ = mode;
+  if (mode > 0 && !fold_ok_) build_fold_operators(mode == 2);
   bump_version();
 }
 
@@ -1001,7 +1037,7 @@ void Fmm::build_operators() {
   for (int o = 0; o < nops_; ++o)
     if (info[o] != 0)
       throw Error(NNK_E_CUDA, "surface matrix factorization reported info=" + std::to_string(info[o]));
-  build_fold_operators();
+  build_fold_operators(fold_on_ == 2);
 }
 
 namespace {

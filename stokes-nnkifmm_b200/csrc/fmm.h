@@ -201,10 +201,11 @@ class Fmm {
   // FP64 work arrays (FP64 and NEAR32 modes); NEAR32 adds FP32 copies of the
   // points and forces for its near-field pair sums
   bool f64() const { return p_.precision != NNK_PREC_MIXED; }
-  // Folded M2M / L2L in the matvec (on by default where available); whether
-  // the matvec uses it.
-  void set_fold(bool on);
-  bool folded() const { return fold_ok_ && fold_on_; }
+  // Folded M2M / L2L in the matvec (regularized operators only): 0 off (the
+  // default), 1 where it pays, 2 wherever available; whether the matvec
+  // uses it.
+  void set_fold(int mode);
+  bool folded() const { return fold_ok_ && fold_on_ > 0; }
   bool near32() const { return p_.precision == NNK_PREC_NEAR32; }
   // scratch for host-pointer calls
   DBuf<double> io_in, io_out;
@@ -298,14 +299,14 @@ class Fmm {
   bool fold_ok_ = false;  // the tree and the operators allow folding
   bool fold_lists_ok_ = false;
   std::array<int, 8> fold_pos_{};  // position code (x * 4 + y * 2 + z) of child k in its parent
-  bool fold_on_ = true;   // the caller's choice
+  int fold_on_ = 0;       // the caller's choice (set_fold)
   DBuf<double> fold_up_, fold_dn_;
   DBuf<int32_t> fpar_, fch_;  // non-leaf nodes by level, and their first children
   std::vector<int64_t> fpar_off_;
   DBuf<C2ETile> fup_tiles_, fdn_tiles_;
   std::vector<int64_t> fup_toff_, fdn_toff_;
   void build_fold_lists();
-  void build_fold_operators();
+  void build_fold_operators(bool force);
   DBuf<double> c2e_part_;   // K-split partial sums of the small C2E launches
   std::vector<int64_t> dn_toff_;
   // transpose (built on first use): tasks with inverted lists, unified

@@ -825,12 +825,24 @@ __global__ void c2e_reduce_kernel(NodeGemm g, int ksplit, int ntiles, const doub
   }
 }
 
-// K splits for a launch of `blocks` CTAs (two resident per SM): enough CTAs
-// for two per SM, each K range at least 64 long.
+// K splits for a launch of `blocks` CTAs (two resident per SM): the count
+// in {1, 2, 4, 8} with the fewest full-CTA waves (a wave of split CTAs
+// takes 1/k of the time), each K range at least 64 long, a split launch
+// charged 0.1 wave for its reduction -- e.g. 304 CTAs on 296 slots run as
+// 4 x 304 quarter-CTAs (1.25 waves) instead of two full waves.
 inline int c2e_splits(int Kd, int blocks) {
-  int k = 1;
-  while (k < 8 && blocks * k < 2 * 148 && Kd / (2 * k) >= 32) k *= 2;
-  return k;
+  constexpr int slots = 2 * 148;
+  int best = 1;
+  double best_cost = 1e30;
+  for (int k = 1; k <= 8; k *= 2) {
+    if (k > 1 && Kd / k < 64) break;
+    const double cost = (double)((blocks * k + slots - 1) / slots) / k + (k > 1 ? 0.1 : 0.0);
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      best = k;
+    }
+  }
+  return best;
 }
 inline size_t c2e_part_size(int M, int Kd, int ntiles, int R) {
   const int blocks = ((M + kC2EBM - 1) / kC2EBM) * ntiles * R;

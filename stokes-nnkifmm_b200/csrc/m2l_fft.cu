@@ -53,6 +53,10 @@ __device__ __forceinline__ void twiddles(typename Cplx<Real>::t* tw, int G, doub
 // deriv = 1: the kernel's eps-derivative,
 //   eps [(r^2 - 2 eps^2) I - 3 r r^T] / D^{5/2}, D = r^2 + eps^2
 // (scale then carries the eps factor).
+// Doubles of the spectra kernel's real grid, rounded up to an even count so
+// that the complex arrays after it stay 16-byte aligned (G is odd).
+__host__ __device__ constexpr int spectra_real_len(int G) { return (G * G * G + 1) & ~1; }
+
 template <typename Real>
 __global__ void fft_spectra_kernel(int G, int res, const double* __restrict__ slot_w,
                                    const int* __restrict__ slot_code, double e2, double scale,
@@ -60,7 +64,7 @@ __global__ void fft_spectra_kernel(int G, int res, const double* __restrict__ sl
   extern __shared__ double sm[];
   const int H = G / 2 + 1;
   double* K = sm;                         // [x][y][z]
-  double2* A = (double2*)(K + G * G * G);  // [x][y][kz]
+  double2* A = (double2*)(K + spectra_real_len(G));  // [x][y][kz]
   double2* B = A + G * G * H;              // [x][ky][kz]
   const int s = blockIdx.x;
   const double h = slot_w[s] / (res - 1);
@@ -281,6 +285,28 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
+// Child pairs of a (P, N) record at difference dl = (ex+1) * 9 + (ey+1) * 3 +
+// (ez+1): bit 8 a + b for every child a of P whose neighbour b = a + (ex, ey,
+// ez) lies in N's box.
+struct GroupMasks {
+  uint64_t m[27];
+};
+constexpr GroupMasks make_group_masks() {
+  GroupMasks g{};
+  for (int dl = 0; dl < 27; ++dl) {
+    const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
+    uint64_t gm = 0;
+    for (int a = 0; a < 8; ++a) {
+      const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
+      if (bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)
+        gm |= 1ull << (a * 8 + (bx * 4 + by * 2 + bz));
+    }
+    g.m[dl] = gm;
+  }
+  return g;
+}
+__constant__ GroupMasks kGroupMasks = make_group_masks();
+
 // Offset-code increment of difference dl = (ex+1) * 9 + (ey+1) * 3 + (ez+1)
 // over difference (-1, -1, -1); codes are (x+3) * 49 + (y+3) * 7 + (z+3).
 __device__ __forceinline__ int code_step(int dl) { return (dl / 9) * 49 + ((dl / 3) % 3) * 7 + dl % 3; }
@@ -344,20 +370,10 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
     // the differences present in this record
     uint32_t gmask = 0;
 #pragma unroll
-    for (int dl = 0; dl < 27; ++dl) {
-      const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
-      uint64_t gm = 0;
-#pragma unroll
-      for (int a = 0; a < 8; ++a) {
-        const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
-        if (bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)
-          gm |= 1ull << (a * 8 + (bx * 4 + by * 2 + bz));
-      }
-      if (mask & gm) gmask |= 1u << dl;
-    }
+    for (int dl = 0; dl < 27; ++dl)
+      if (mask & kGroupMasks.m[dl]) gmask |= 1u << dl;
     const int cbase = (dx2 + 2) * 49 + (dy2 + 2) * 7 + (dz2 + 2);  // code of difference (-1, -1, -1)
-    const int ncode = __ffs(gmask) - 1;
-    if (gmask) issue_kernel_spectra<T2>(kb, spec + (size_t)sso[cbase + code_step(ncode)] * 6 * NK + k, NK);
+    if (gmask) issue_kernel_spectra<T2>(kb, spec + (size_t)sso[cbase + code_step(__ffs(gmask) - 1)] * 6 * NK + k, NK);
     cp_async_commit();
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
@@ -368,24 +384,27 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
         for (int c = 0; c < 3; ++c) my[(b * 3 + c) * BLK] = Q[(size_t)c * NK];
       }
     }
+    // one pass per present difference (a runtime loop: the code stays small
+    // enough for the instruction cache); every branch is uniform over the
+    // block, whose threads share the record
     int buf = 0;
-#pragma unroll
-    for (int dl = 0; dl < 27; ++dl) {
-      if (!((gmask >> dl) & 1)) continue;
-      const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
-      const uint32_t rest = gmask & ~((2u << dl) - 1u);
-      if (rest) issue_kernel_spectra<T2>(kb + (buf ^ 1) * 6 * BLK, spec + (size_t)sso[cbase + code_step(__ffs(rest) - 1)] * 6 * NK + k, NK);
+    for (uint32_t gl = gmask; gl; gl &= gl - 1) {
+      const int dl = __ffs(gl) - 1;
+      const uint32_t rest = gl & (gl - 1);
+      if (rest)
+        issue_kernel_spectra<T2>(kb + (buf ^ 1) * 6 * BLK,
+                                 spec + (size_t)sso[cbase + code_step(__ffs(rest) - 1)] * 6 * NK + k, NK);
       cp_async_commit();
       cp_async_wait_prior();  // this difference's spectrum has landed
       const T2* K = kb + buf * 6 * BLK;
       const T2 kxx = K[0], kxy = K[BLK], kxz = K[2 * BLK], kyy = K[3 * BLK], kyz = K[4 * BLK], kzz = K[5 * BLK];
       buf ^= 1;
+      const uint64_t bits = mask & kGroupMasks.m[dl];
+      const int dpos = (dl / 9) * 4 + ((dl / 3) % 3) * 2 + dl % 3 - 7;  // pos_v - pos_i as a position code
 #pragma unroll
       for (int a = 0; a < 8; ++a) {
-        const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
-        if (!(bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)) continue;
-        const int b = bx * 4 + by * 2 + bz;
-        if (!((mask >> (a * 8 + b)) & 1)) continue;
+        if (!((bits >> (8 * a)) & 0xFF)) continue;  // child a has no pair at this difference
+        const int b = a + dpos;
         const T2 qx = my[(b * 3) * BLK], qy = my[(b * 3 + 1) * BLK], qz = my[(b * 3 + 2) * BLK];
         cmac(acc[a][0], kxx, qx);
         cmac(acc[a][0], kxy, qy);
@@ -755,7 +774,7 @@ void build_fft_m2l(const HostTree& t, int res, int shells, double eps, double mu
     DBuf<int> dc;
     dw.upload(slot_w, st);
     dc.upload(slot_code, st);
-    const size_t sm = sizeof(double) * (size_t)G * G * G + 2 * sizeof(double2) * (size_t)G * G * H;
+    const size_t sm = sizeof(double) * (size_t)spectra_real_len(G) + 2 * sizeof(double2) * (size_t)G * G * H;
     const double scale = 1.0 / (8.0 * M_PI * mu * (double)G * G * G);
     if (fp64) {
       NNK_CUDA(cudaFuncSetAttribute(fft_spectra_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -801,7 +820,7 @@ void build_fft_deriv(FftM2L& f, double eps, double mu, cudaStream_t st) {
   DBuf<int> dc;
   dw.upload(f.slot_w_host, st);
   dc.upload(f.slot_code_host, st);
-  const size_t sm = sizeof(double) * (size_t)G * G * G + 2 * sizeof(double2) * (size_t)G * G * H;
+  const size_t sm = sizeof(double) * (size_t)spectra_real_len(G) + 2 * sizeof(double2) * (size_t)G * G * H;
   NNK_CUDA(cudaFuncSetAttribute(fft_spectra_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   fft_spectra_kernel<double><<<f.nspec, 256, sm, st>>>(G, f.res, dw.p, dc.p, eps * eps,
                                                         eps / (8.0 * M_PI * mu * (double)G * G * G), f.dspec64.p,

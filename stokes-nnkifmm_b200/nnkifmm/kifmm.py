@@ -108,11 +108,12 @@ class KIFMM:
         L.check(L.lib.nnk_fmm_set_eps(self.h, float(eps)), self.ctx.h, "setEps")
         self.arguments["kernelPar"] = (float(eps), self.arguments["kernelPar"][1])
 
-    def setFold(self, on=True):
+    def setFold(self, mode=1):
         """Run the matvec's M2M and L2L folded into the check-to-equivalent
-        products (default where available; stats()["folded"] says whether it
-        is in use) or as pair sums followed by those products."""
-        L.check(L.lib.nnk_fmm_set_fold(self.h, 1 if on else 0), self.ctx.h, "setFold")
+        products -- mode 1 where it pays (the default), 2 wherever available
+        -- or, mode 0, as pair sums followed by those products;
+        stats()["folded"] says whether the matvec folds."""
+        L.check(L.lib.nnk_fmm_set_fold(self.h, int(mode)), self.ctx.h, "setFold")
 
     def sourceCount(self):
         c = C.c_int64()
