@@ -108,7 +108,7 @@ typedef struct nnk_fmm_params {
                             lattice; FP32-rounding accuracy).
                             FP64 and NEAR32 modes: 3 the FP64 pair kernel, any
                             other value the FP64 Fourier-space product (at
-                            most 4 right-hand sides per pass)                 */
+                            most 6 right-hand sides per pass)                 */
   double reg;            /* relative Tikhonov weight of the check-to-equivalent
                             pseudo-inverse: NNK_PREC_MIXED 0 = default 1e-5;
                             NNK_PREC_FP64 0 = exact LU inverse (reference)   */
@@ -278,6 +278,23 @@ int nnk_fmm_set_eps(nnk_fmm* fmm, double eps);
  * tensor-core M2L and at most 1 GiB of folded operators; the transpose, the
  * gradients and the eps-derivative always run unfolded. */
 int nnk_fmm_set_fold(nnk_fmm* fmm, int32_t mode);
+/* Host wall time (milliseconds) of the set-up steps of nnk_fmm_create, in
+ * the order of the NNK_SETUP_* indices: the unified point array and its
+ * surfaces, the pair task lists, the M2L plan (Fourier-space spectra and
+ * families, or the tensor-core plan), the check-to-equivalent operators
+ * (kernel matrices and their LU or Tikhonov solves), the folded operators,
+ * and the whole of it.  Writes min(n, NNK_SETUP_COUNT) values; the last
+ * nnk_fmm_set_eps updates the M2L, operator and fold entries. */
+enum {
+  NNK_SETUP_POINTS = 0,
+  NNK_SETUP_TASKS = 1,
+  NNK_SETUP_M2L = 2,
+  NNK_SETUP_OPERATORS = 3,
+  NNK_SETUP_FOLD = 4,
+  NNK_SETUP_TOTAL = 5,
+  NNK_SETUP_COUNT = 6
+};
+int nnk_fmm_setup_times(const nnk_fmm* fmm, double* ms, int32_t n);
 /* Number of source origins: fine points (NEAREST) or potential rows. */
 int nnk_fmm_source_count(const nnk_fmm* fmm, int64_t* count);
 /* Gradient of <weights, apply(forces)> with respect to the positions, with

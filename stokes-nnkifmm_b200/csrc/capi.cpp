@@ -5,6 +5,9 @@
 #include <memory>
 #include <new>
 
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
 #include "../../include/nnkifmm.h"
 #include "common.h"
 #include "fmm.h"
@@ -51,9 +54,11 @@ void ctx_retain(nnk_ctx* c) { c->refs.fetch_add(1, std::memory_order_relaxed); }
 
 void ctx_release(nnk_ctx* c) {
   if (c->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
-  if (c->has_gpu && c->own_stream && c->stream) {
+  if (c->has_gpu) {
     cudaSetDevice(c->device);
-    cudaStreamDestroy(c->stream);
+    if (c->dn_solver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(c->dn_solver));
+    if (c->blas) cublasDestroy(static_cast<cublasHandle_t>(c->blas));
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     cudaGetLastError();  // an error here must not surface at a later call's launch check
   }
   delete c;
@@ -421,6 +426,12 @@ int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats) {
   if (!fmm || !stats) return NNK_E_ARG;
   *stats = fmm->f->stats();
   stats->folded = fmm->f->folded() ? 1 : 0;
+  return NNK_OK;
+}
+
+int nnk_fmm_setup_times(const nnk_fmm* fmm, double* ms, int32_t n) {
+  if (!fmm || (!ms && n > 0) || n < 0) return NNK_E_ARG;
+  for (int i = 0; i < n && i < NNK_SETUP_COUNT; ++i) ms[i] = fmm->f->setup_ms()[i];
   return NNK_OK;
 }
 

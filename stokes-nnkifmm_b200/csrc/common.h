@@ -76,4 +76,9 @@ struct nnk_ctx {
   // the caller's handle plus one per tree, FMM and batch made from it: the
   // context (and its stream) goes when the last of them is destroyed
   std::atomic<int> refs{1};
+  // cuSOLVER / cuBLAS handles of the set-up steps, created on first use and
+  // kept with the context (creating them costs milliseconds, which every
+  // right-hand side of a time step that rebuilds its FMM would pay)
+  void* dn_solver = nullptr;  // cusolverDnHandle_t
+  void* blas = nullptr;       // cublasHandle_t
 };

@@ -3,6 +3,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <array>
 #include <type_traits>
@@ -100,19 +101,27 @@ __global__ void dot_partial_kernel(long long n, const double* __restrict__ a, co
   if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
+// The context's cuSOLVER / cuBLAS handles (created on first use), bound to
+// its stream.
 struct Solver {
   cusolverDnHandle_t s = nullptr;
   cublasHandle_t b = nullptr;
-  Solver(cudaStream_t st) {
-    if (cusolverDnCreate(&s) != CUSOLVER_STATUS_SUCCESS) throw Error(NNK_E_CUDA, "cusolverDnCreate failed");
-    cusolverDnSetStream(s, st);
-    if (cublasCreate(&b) != CUBLAS_STATUS_SUCCESS) throw Error(NNK_E_CUDA, "cublasCreate failed");
-    cublasSetStream(b, st);
+  explicit Solver(nnk_ctx* ctx) {
+    if (!ctx->dn_solver) {
+      cusolverDnHandle_t h = nullptr;
+      if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) throw Error(NNK_E_CUDA, "cusolverDnCreate failed");
+      ctx->dn_solver = h;
+    }
+    if (!ctx->blas) {
+      cublasHandle_t h = nullptr;
+      if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) throw Error(NNK_E_CUDA, "cublasCreate failed");
+      ctx->blas = h;
+    }
+    s = static_cast<cusolverDnHandle_t>(ctx->dn_solver);
+    b = static_cast<cublasHandle_t>(ctx->blas);
+    cusolverDnSetStream(s, ctx->stream);
+    cublasSetStream(b, ctx->stream);
     cudaGetLastError();  // library set-up may leave a handled error behind
-  }
-  ~Solver() {
-    if (s) cusolverDnDestroy(s);
-    if (b) cublasDestroy(b);
   }
 };
 
@@ -135,10 +144,19 @@ Fmm::Fmm(nnk_ctx* ctx, const HostTree* tree, const FmmParams& p) : ctx_(ctx), t_
   E_ = t_->src_start[N_];
   tot_ = E_ + 2LL * P_ * N_;
   maxl_ = t_->max_level;
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  auto lap = [&](int i, clk::time_point a) {
+    setup_ms_[i] = std::chrono::duration<double, std::milli>(clk::now() - a).count();
+    return clk::now();
+  };
   assign_operators();
   build_points();
+  auto t = lap(NNK_SETUP_POINTS, t0);
   build_tasks();
+  t = lap(NNK_SETUP_TASKS, t);
   build_operators();
+  lap(NNK_SETUP_TOTAL, t0);
   if (t_->groups() > 1) {
     // tree mask of a forest, all trees on; allocated here because applies
     // may be captured into CUDA graphs that read it by address
@@ -841,7 +859,7 @@ void Fmm::build_fold_operators(bool force) {
   DBuf<double> dS;
   dS.upload(surf, st);
   DBuf<double> dM(per), dL(per);
-  Solver sv(st);
+  Solver sv(ctx_);
   const double one = 1.0, zero = 0.0;
   const double e2 = p_.eps * p_.eps, c = 1.0 / (8.0 * M_PI * p_.mu);
   const unsigned kb = (unsigned)(((size_t)P_ * P_ + 255) / 256);
@@ -916,6 +934,9 @@ void Fmm::build_operators() {
   // Fourier-space M2L: mode 4 in mixed precision (FP32 spectra); in FP64
   // every mode but 3 (the FP64 pair kernel) when the transforms of one
   // right-hand side fit shared memory (FP64 spectra)
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
+  auto tm2l = clk::now();
   const bool fp64 = f64();
   const int fft_cap = fft_m2l_max_rhs(p_.res, fp64);
   if ((!fp64 && p_.m2l_mode == 4) || (fp64 && p_.m2l_mode != 3 && fft_cap >= 1)) {
@@ -934,6 +955,8 @@ void Fmm::build_operators() {
     stats_.m2l_tile_rows = m2l_.tile_slots * 128;
     stats_.m2l_rank = m2l_.compressed ? m2l_.RC : 0;
   }
+  setup_ms_[NNK_SETUP_M2L] = ms_since(tm2l);
+  const auto tops = clk::now();
   const int n = 3 * P_;
   cudaStream_t st = ctx_->stream;
   ops_.alloc((size_t)nops_ * n * n);
@@ -983,7 +1006,7 @@ void Fmm::build_operators() {
       lam2[o] = (reg * smax) * (reg * smax);
     }
   }
-  Solver sv(st);
+  Solver sv(ctx_);
   DBuf<double> dK((size_t)n * n), dG((size_t)n * n);
   DBuf<int> dpiv(n), dinfo(std::max(nops_, 1));
   dinfo.zero(st);
@@ -1037,7 +1060,10 @@ void Fmm::build_operators() {
   for (int o = 0; o < nops_; ++o)
     if (info[o] != 0)
       throw Error(NNK_E_CUDA, "surface matrix factorization reported info=" + std::to_string(info[o]));
+  setup_ms_[NNK_SETUP_OPERATORS] = ms_since(tops);
+  const auto tfold = clk::now();
   build_fold_operators(fold_on_ == 2);
+  setup_ms_[NNK_SETUP_FOLD] = ms_since(tfold);
 }
 
 namespace {
@@ -1486,7 +1512,7 @@ void Fmm::build_deps() {
     dKs[o].assign((size_t)n * n, 0.0);
     kernel_deriv_matrix(us, ds, p_.eps, p_.mu, dKs[o], n);
   }
-  Solver sv(st);
+  Solver sv(ctx_);
   dops_.alloc((size_t)nops_ * n * n);
   DBuf<double> dK((size_t)n * n), T((size_t)n * n);
   for (int o = 0; o < nops_; ++o) {

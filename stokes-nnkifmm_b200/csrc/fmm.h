@@ -206,6 +206,8 @@ class Fmm {
   // uses it.
   void set_fold(int mode);
   bool folded() const { return fold_ok_ && fold_on_ > 0; }
+  // host wall time of the set-up steps (NNK_SETUP_*), milliseconds
+  const double* setup_ms() const { return setup_ms_; }
   bool near32() const { return p_.precision == NNK_PREC_NEAR32; }
   // scratch for host-pointer calls
   DBuf<double> io_in, io_out;
@@ -296,6 +298,7 @@ class Fmm {
   // parent of width w) and D = [A(w)^T L2L_0; ..; A(w)^T L2L_7] (8 * 3P x 3P;
   // L2L_k: the down surface of the parent of width 2w -> child k's up
   // surface), child k = child0 + k; over the non-leaf nodes of each level
+  double setup_ms_[NNK_SETUP_COUNT] = {};
   bool fold_ok_ = false;  // the tree and the operators allow folding
   bool fold_lists_ok_ = false;
   std::array<int, 8> fold_pos_{};  // position code (x * 4 + y * 2 + z) of child k in its parent

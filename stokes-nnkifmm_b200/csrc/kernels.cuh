@@ -642,14 +642,14 @@ inline void launch_reduce(const RedD* reds, int nreds, const Real* partial, Real
 //   * the downward step of the 8 children from their parent, folded
 //     (M = 8 * 3P, Kd = 3P, in_node = parent, node = first child), added to
 //     the children's check-to-equivalent result.
-// 128 x 64 output tile (operator rows x (node, right-hand side) columns) per
-// CTA of 128 threads, each accumulating 8 x 8 in FP64: rows 4 ty + i and
-// 64 + 4 ty + i, columns 4 tx + j and 32 + 4 tx + j (ty = tid / 8, tx =
-// tid % 8), read from shared memory as 16-byte pairs (8 FMAs per load).  K in
-// steps of 8, the next step's operands fetched into registers while the
-// current one is multiplied from shared memory.
+// 64 x 64 output tile (operator rows x (node, right-hand side) columns) per
+// CTA of 256 threads, each accumulating 4 x 4 in FP64; K in steps of 16 with
+// the next step's operands fetched into registers while the current one is
+// multiplied from shared memory.  (A 128 x 64 tile with 8 x 8 per thread and
+// 16-byte shared loads ran 10-20% slower here: with 8 warps per SM the
+// global-load latency of each K step stayed exposed.)
 constexpr int kC2ETileNodes = 64;
-constexpr int kC2EBM = 128;
+constexpr int kC2EBM = 64;
 
 struct NodeGemm {
   const double* ops;
@@ -663,19 +663,18 @@ struct NodeGemm {
   float* m2l_dst;  // optional TF32 copy of the result (rows < NP)
   int NP;
 };
-__device__ __forceinline__ C2ETile tiles_at(const NodeGemm& g, int i) { return g.tiles[i]; }
 
 template <typename Real>
-__global__ void __launch_bounds__(128, 2) c2e_kernel(NodeGemm g, const Real* __restrict__ check, Real* __restrict__ dst,
-                                                     int ksplit, int kper, double* __restrict__ part,
-                                                     const int* __restrict__ nact) {
-  constexpr int BM = kC2EBM, BN = 64, BK = 8, LA = BM + 2, LB = BN + 2;  // padded rows: conflict-free stores
-  __shared__ __align__(16) double As[BK * LA];
-  __shared__ __align__(16) double Bs[BK * LB];
+__global__ void __launch_bounds__(256) c2e_kernel(NodeGemm g, const Real* __restrict__ check, Real* __restrict__ dst,
+                                                  int ksplit, int kper, double* __restrict__ part,
+                                                  const int* __restrict__ nact) {
+  constexpr int BM = kC2EBM, BN = 64, BK = 16;
+  __shared__ double As[BK][BM + 1];
+  __shared__ double Bs[BK][BN + 1];
   __shared__ int col_node[BN];
   __shared__ int col_in[BN];
   __shared__ int col_k[BN];
-  const C2ETile tl = tiles_at(g, blockIdx.y);
+  const C2ETile tl = g.tiles[blockIdx.y];
   if (nact && !nact[g.nodes[tl.first]]) return;  // the nodes of a tile belong to one tree
   const int M = g.M, Kd = g.Kd, P = g.P, R = g.R, trans = g.trans;
   const int zch = gridDim.z / ksplit;
@@ -693,14 +692,14 @@ __global__ void __launch_bounds__(128, 2) c2e_kernel(NodeGemm g, const Real* __r
     col_k[tid] = j < ncol ? j % R : 0;
   }
   __syncthreads();
-  const int tx = tid & 7, ty = tid >> 3;
-  double acc[8][8];
+  const int tr = tid % 16, tc = tid / 16;
+  double acc[4][4];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0;
-  // staging: 8 operator values (BK x BM / 128) and 4 source values (BK x BN / 128)
-  double ra[8], rb[4];
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0;
+  // register staging: 4 operator values and 4 source values per thread per K step
+  double ra[4], rb[4];
   // operator element e of the step: Aop[r][c] at c M + r (contiguous in r)
   // or, transposed, A[c][r] at r Kd + c (contiguous in c = the K index)
   auto a_index = [&](int e, int& kk, int& mm) {
@@ -709,15 +708,15 @@ __global__ void __launch_bounds__(128, 2) c2e_kernel(NodeGemm g, const Real* __r
   };
   auto load = [&](int k0) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < 4; ++q) {
       int kk, mm;
-      a_index(tid + 128 * q, kk, mm);
+      a_index(tid + 256 * q, kk, mm);
       const int r = m0 + mm, c = k0 + kk;
       ra[q] = (r < M && c < kend) ? (trans ? A[(size_t)r * Kd + c] : A[(size_t)c * M + r]) : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int e = tid + 128 * q;
+      const int e = tid + 256 * q;  // BK * BN
       const int kk = e % BK, nn = e / BK;
       const int c = k0 + kk, node = col_in[nn];
       double v = 0;
@@ -730,15 +729,15 @@ __global__ void __launch_bounds__(128, 2) c2e_kernel(NodeGemm g, const Real* __r
   };
   auto store = [&]() {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < 4; ++q) {
       int kk, mm;
-      a_index(tid + 128 * q, kk, mm);
-      As[kk * LA + mm] = ra[q];
+      a_index(tid + 256 * q, kk, mm);
+      As[kk][mm] = ra[q];
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int e = tid + 128 * q;
-      Bs[(e % BK) * LB + e / BK] = rb[q];
+      const int e = tid + 256 * q;
+      Bs[e % BK][e / BK] = rb[q];
     }
   };
   load(kbeg);
@@ -748,35 +747,23 @@ __global__ void __launch_bounds__(128, 2) c2e_kernel(NodeGemm g, const Real* __r
     if (k0 + BK < kend) load(k0 + BK);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
-      double a[8], b[8];
-      const double2* a2 = reinterpret_cast<const double2*>(As + kk * LA);
-      const double2* b2 = reinterpret_cast<const double2*>(Bs + kk * LB);
+      double a[4], b[4];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const double2 x0 = a2[(h * 64 + 4 * ty) / 2], x1 = a2[(h * 64 + 4 * ty) / 2 + 1];
-        a[4 * h] = x0.x;
-        a[4 * h + 1] = x0.y;
-        a[4 * h + 2] = x1.x;
-        a[4 * h + 3] = x1.y;
-        const double2 y0 = b2[(h * 32 + 4 * tx) / 2], y1 = b2[(h * 32 + 4 * tx) / 2 + 1];
-        b[4 * h] = y0.x;
-        b[4 * h + 1] = y0.y;
-        b[4 * h + 2] = y1.x;
-        b[4 * h + 3] = y1.y;
-      }
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][tr + 16 * i];
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tc + 16 * j];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int r = m0 + (i >> 2) * 64 + 4 * ty + (i & 3);
-      const int jj = (j >> 2) * 32 + 4 * tx + (j & 3);
+    for (int j = 0; j < 4; ++j) {
+      const int r = m0 + tr + 16 * i, jj = tc + 16 * j;
       const int node = col_node[jj];
       if (ksplit > 1) {
         // partial sum of this K range: part[split][tile][column][row]
@@ -803,7 +790,7 @@ template <typename Real>
 __global__ void c2e_reduce_kernel(NodeGemm g, int ksplit, int ntiles, const double* __restrict__ part,
                                   Real* __restrict__ dst, const int* __restrict__ nact) {
   const int tile = blockIdx.y;
-  const C2ETile tl = tiles_at(g, tile);
+  const C2ETile tl = g.tiles[tile];
   if (nact && !nact[g.nodes[tl.first]]) return;
   const int M = g.M, R = g.R;
   const int cols = kC2ETileNodes * R;
@@ -825,24 +812,12 @@ __global__ void c2e_reduce_kernel(NodeGemm g, int ksplit, int ntiles, const doub
   }
 }
 
-// K splits for a launch of `blocks` CTAs (two resident per SM): the count
-// in {1, 2, 4, 8} with the fewest full-CTA waves (a wave of split CTAs
-// takes 1/k of the time), each K range at least 64 long, a split launch
-// charged 0.1 wave for its reduction -- e.g. 304 CTAs on 296 slots run as
-// 4 x 304 quarter-CTAs (1.25 waves) instead of two full waves.
+// K splits for a launch of `blocks` CTAs: enough CTAs for two per SM, each
+// K range at least 32 long.
 inline int c2e_splits(int Kd, int blocks) {
-  constexpr int slots = 2 * 148;
-  int best = 1;
-  double best_cost = 1e30;
-  for (int k = 1; k <= 8; k *= 2) {
-    if (k > 1 && Kd / k < 64) break;
-    const double cost = (double)((blocks * k + slots - 1) / slots) / k + (k > 1 ? 0.1 : 0.0);
-    if (cost < best_cost - 1e-9) {
-      best_cost = cost;
-      best = k;
-    }
-  }
-  return best;
+  int k = 1;
+  while (k < 8 && blocks * k < 2 * 148 && Kd / (2 * k) >= 32) k *= 2;
+  return k;
 }
 inline size_t c2e_part_size(int M, int Kd, int ntiles, int R) {
   const int blocks = ((M + kC2EBM - 1) / kC2EBM) * ntiles * R;
@@ -860,7 +835,7 @@ inline void launch_node_gemm(NodeGemm g, int ntiles, const Real* src, Real* dst,
   if (!part || part_n < c2e_part_size(g.M, g.Kd, ntiles, g.R)) ksplit = 1;
   const int kper = ((g.Kd + ksplit - 1) / ksplit + 15) / 16 * 16;
   dim3 grid((g.M + kC2EBM - 1) / kC2EBM, ntiles, zch * ksplit);
-  c2e_kernel<Real><<<grid, 128, 0, st>>>(g, src, dst, ksplit, kper, part, nact);
+  c2e_kernel<Real><<<grid, 256, 0, st>>>(g, src, dst, ksplit, kper, part, nact);
   NNK_CHECK_LAUNCH();
   if (ksplit > 1) {
     dim3 g2(std::max(1, std::min(64, (kC2ETileNodes * g.R * g.M + 255) / 256)), ntiles);

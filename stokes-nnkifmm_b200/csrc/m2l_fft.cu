@@ -266,69 +266,15 @@ __global__ void __launch_bounds__(128) fft_accumulate_kernel(int NK, const int* 
   for (int c = 0; c < C; ++c) out[(size_t)c * NK] = acc[c];
 }
 
-template <typename Real>
-constexpr size_t family_smem() {
-  return 36 * 128 * sizeof(typename Cplx<Real>::t) + 343 * sizeof(int);
-}
-
-// Asynchronous 8- or 16-byte copy global -> shared (cp.async; 16 bytes bypass
-// L1), and its group commit / wait: this thread's copies land in its own
-// shared-memory slots, so no barrier is needed, only the wait.
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  if constexpr (BYTES == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(BYTES) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
-// Child pairs of a (P, N) record at difference dl = (ex+1) * 9 + (ey+1) * 3 +
-// (ez+1): bit 8 a + b for every child a of P whose neighbour b = a + (ex, ey,
-// ez) lies in N's box.
-struct GroupMasks {
-  uint64_t m[27];
-};
-constexpr GroupMasks make_group_masks() {
-  GroupMasks g{};
-  for (int dl = 0; dl < 27; ++dl) {
-    const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
-    uint64_t gm = 0;
-    for (int a = 0; a < 8; ++a) {
-      const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
-      if (bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)
-        gm |= 1ull << (a * 8 + (bx * 4 + by * 2 + bz));
-    }
-    g.m[dl] = gm;
-  }
-  return g;
-}
-__constant__ GroupMasks kGroupMasks = make_group_masks();
-
-// Offset-code increment of difference dl = (ex+1) * 9 + (ey+1) * 3 + (ez+1)
-// over difference (-1, -1, -1); codes are (x+3) * 49 + (y+3) * 7 + (z+3).
-__device__ __forceinline__ int code_step(int dl) { return (dl / 9) * 49 + ((dl / 3) % 3) * 7 + dl % 3; }
-
-// This thread's 6 kernel spectra at frequency k (Kp) into its slots kb.
-template <typename T2>
-__device__ __forceinline__ void issue_kernel_spectra(T2* kb, const T2* Kp, int NK) {
-#pragma unroll
-  for (int c = 0; c < 6; ++c) cp_async<sizeof(T2)>(kb + c * 128, Kp + (size_t)c * NK);
-}
-
 // Parent-grouped accumulation (see FftFamily): thread (family, frequency k)
 // holds the 8 children's accumulators of one right-hand side at a time; per
 // (P, N) record the 8 source spectra go to this thread's own shared-memory
 // slots, then for each of the 27 values of pos_v - pos_i present in the
-// record the kernel spectrum of offset 2 d + delta is applied to every pair
-// with that difference.  The kernel spectra come in by cp.async into two
-// shared-memory buffers per thread: the next present difference's spectrum
-// is in flight while the current one is applied.  Loop bounds and child
-// positions are compile-time, so accumulators stay in registers.  Every
-// right-hand side sums its pairs in the same order, so a pass of R
-// right-hand sides gives each of them bitwise the result of a pass of one.
+// record the kernel spectrum of offset 2 d + delta is loaded once and applied
+// to every pair with that difference.  Loop bounds and child positions are
+// compile-time, so accumulators stay in registers.  Every right-hand side
+// sums its pairs in the same order, so a pass of R right-hand sides gives
+// each of them bitwise the result of a pass of one.
 template <typename Real>
 __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
     int NK, const FftFamily* __restrict__ fams, const FftFamilyPair* __restrict__ pairs,
@@ -337,44 +283,26 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
     const int* __restrict__ tgt_node, const int* __restrict__ nact, int R) {
   using T2 = typename Cplx<Real>::t;
   constexpr int BLK = 128;
-  extern __shared__ __align__(16) unsigned char fam_smem[];  // family_smem<Real>() bytes
-  T2* sq = reinterpret_cast<T2*>(fam_smem);  // this thread's source spectra: [pos * 3 + c][thread]
-  T2* sk = sq + 24 * BLK;                    // its kernel spectra, two buffers: [buf * 6 + c][thread]
-  int* sso = reinterpret_cast<int*>(sk + 12 * BLK);  // spectrum slot of each offset code at the family's width
-  const FftFamily* fam = fams + blockIdx.x;
-  const int first = fam->first, count = fam->count;
-  // every record of a family has the same operator (checked at build)
-  const int* so = spec_of + (size_t)(count ? pairs[first].op : 0) * 343;
-  for (int e = threadIdx.x; e < 343; e += BLK) sso[e] = so[e];
-  __syncthreads();
+  __shared__ T2 sq[24 * BLK];  // this thread's source spectra: [pos * 3 + c][thread]
+  const FftFamily fam = fams[blockIdx.x];
   const int k = blockIdx.y * BLK + threadIdx.x;
   if (nact) {
     int t0 = 0;
-    while (t0 < 7 && fam->tgt[t0] < 0) ++t0;
-    if (!nact[tgt_node[fam->tgt[t0]]]) return;
+    while (t0 < 7 && fam.tgt[t0] < 0) ++t0;
+    if (!nact[tgt_node[fam.tgt[t0]]]) return;
   }
   if (k >= NK) return;
   const int C = 3 * R;
   T2* my = sq + threadIdx.x;
-  T2* kb = sk + threadIdx.x;
   for (int r = 0; r < R; ++r) {
   T2 acc[8][3];
 #pragma unroll
   for (int a = 0; a < 8; ++a)
 #pragma unroll
     for (int c = 0; c < 3; ++c) acc[a][c] = cmake((Real)0, (Real)0);
-  for (int pr = first; pr < first + count; ++pr) {
+  for (int pr = fam.first; pr < fam.first + fam.count; ++pr) {
     const FftFamilyPair rec = pairs[pr];
     const uint64_t mask = (uint64_t)rec.mask_lo | ((uint64_t)rec.mask_hi << 32);
-    const int dx2 = 2 * (rec.dcode / 9 - 1), dy2 = 2 * ((rec.dcode / 3) % 3 - 1), dz2 = 2 * (rec.dcode % 3 - 1);
-    // the differences present in this record
-    uint32_t gmask = 0;
-#pragma unroll
-    for (int dl = 0; dl < 27; ++dl)
-      if (mask & kGroupMasks.m[dl]) gmask |= 1u << dl;
-    const int cbase = (dx2 + 2) * 49 + (dy2 + 2) * 7 + (dz2 + 2);  // code of difference (-1, -1, -1)
-    if (gmask) issue_kernel_spectra<T2>(kb, spec + (size_t)sso[cbase + code_step(__ffs(gmask) - 1)] * 6 * NK + k, NK);
-    cp_async_commit();
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
       const int sl = rec.src[b];
@@ -384,27 +312,29 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
         for (int c = 0; c < 3; ++c) my[(b * 3 + c) * BLK] = Q[(size_t)c * NK];
       }
     }
-    // one pass per present difference (a runtime loop: the code stays small
-    // enough for the instruction cache); every branch is uniform over the
-    // block, whose threads share the record
-    int buf = 0;
-    for (uint32_t gl = gmask; gl; gl &= gl - 1) {
-      const int dl = __ffs(gl) - 1;
-      const uint32_t rest = gl & (gl - 1);
-      if (rest)
-        issue_kernel_spectra<T2>(kb + (buf ^ 1) * 6 * BLK,
-                                 spec + (size_t)sso[cbase + code_step(__ffs(rest) - 1)] * 6 * NK + k, NK);
-      cp_async_commit();
-      cp_async_wait_prior();  // this difference's spectrum has landed
-      const T2* K = kb + buf * 6 * BLK;
-      const T2 kxx = K[0], kxy = K[BLK], kxz = K[2 * BLK], kyy = K[3 * BLK], kyz = K[4 * BLK], kzz = K[5 * BLK];
-      buf ^= 1;
-      const uint64_t bits = mask & kGroupMasks.m[dl];
-      const int dpos = (dl / 9) * 4 + ((dl / 3) % 3) * 2 + dl % 3 - 7;  // pos_v - pos_i as a position code
+    const int dx2 = 2 * (rec.dcode / 9 - 1), dy2 = 2 * ((rec.dcode / 3) % 3 - 1), dz2 = 2 * (rec.dcode % 3 - 1);
+    const int* so = spec_of + (size_t)rec.op * 343;
+#pragma unroll
+    for (int dl = 0; dl < 27; ++dl) {
+      const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
+      uint64_t gm = 0;
 #pragma unroll
       for (int a = 0; a < 8; ++a) {
-        if (!((bits >> (8 * a)) & 0xFF)) continue;  // child a has no pair at this difference
-        const int b = a + dpos;
+        const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
+        if (bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)
+          gm |= 1ull << (a * 8 + (bx * 4 + by * 2 + bz));
+      }
+      const uint64_t bits = mask & gm;
+      if (bits == 0) continue;
+      const int code = (dx2 + ex + 3) * 49 + (dy2 + ey + 3) * 7 + (dz2 + ez + 3);
+      const T2* Kp = spec + (size_t)so[code] * 6 * NK + k;
+      const T2 kxx = Kp[0], kxy = Kp[NK], kxz = Kp[2 * NK], kyy = Kp[3 * NK], kyz = Kp[4 * NK], kzz = Kp[5 * NK];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
+        if (!(bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)) continue;
+        const int b = bx * 4 + by * 2 + bz;
+        if (!((bits >> (a * 8 + b)) & 1)) continue;
         const T2 qx = my[(b * 3) * BLK], qy = my[(b * 3 + 1) * BLK], qz = my[(b * 3 + 2) * BLK];
         cmac(acc[a][0], kxx, qx);
         cmac(acc[a][0], kxy, qy);
@@ -420,7 +350,7 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
   }
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
-    const int t = fam->tgt[a];
+    const int t = fam.tgt[a];
     if (t < 0) continue;
     T2* out = chat + ((size_t)t * C + 3 * r) * NK + k;
 #pragma unroll
@@ -622,8 +552,6 @@ void set_smem_attributes(int optin) {
   NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<4, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<6, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<6, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-  NNK_CUDA(cudaFuncSetAttribute(fft_accumulate_family_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)family_smem<Real>()));
 }
 
 template <typename Real>
@@ -642,7 +570,7 @@ void run_fft_m2l(FftM2L& f, const Real* str, long long upbase, int R, Real* chec
                                                         f.NK, nact);
   NNK_CHECK_LAUNCH();
   if (f.family) {
-    fft_accumulate_family_kernel<Real><<<dim3(f.nfam, (f.NK + 127) / 128), 128, family_smem<Real>(), st>>>(
+    fft_accumulate_family_kernel<Real><<<dim3(f.nfam, (f.NK + 127) / 128), 128, 0, st>>>(
         f.NK, f.fams.p, f.fpairs.p, f.spec_of.p, spec, qhat, chat, f.tgt_node.p, nact, R);
     NNK_CHECK_LAUNCH();
     inv<<<f.ntgt, 256, inverse_smem(G, res, R, es), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, chat, R, check, f.NK,

@@ -115,6 +115,13 @@ class KIFMM:
         stats()["folded"] says whether the matvec folds."""
         L.check(L.lib.nnk_fmm_set_fold(self.h, int(mode)), self.ctx.h, "setFold")
 
+    def setup_times(self):
+        """Host wall time (ms) of the set-up steps: points, tasks, m2l,
+        operators, fold, total (nnk_fmm_setup_times)."""
+        v = (C.c_double * 6)()
+        L.check(L.lib.nnk_fmm_setup_times(self.h, v, 6))
+        return dict(zip(("points", "tasks", "m2l", "operators", "fold", "total"), list(v)))
+
     def sourceCount(self):
         c = C.c_int64()
         L.check(L.lib.nnk_fmm_source_count(self.h, C.byref(c)))

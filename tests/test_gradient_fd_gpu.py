@@ -8,9 +8,13 @@ random directions of the force and quadrature points, for the FP64 and the
 mixed-precision solves.  The points are jittered; the gradient holds the
 nearest map fixed, so the directions leave still the quadrature points
 whose two nearest force points are within 1e-7 of a tie (52 of the 200k
-here; displacements are ~1e-8) and those force points, and a direction
-along which some nearest force point still changes within +-h is drawn
-again; the FD solves run on
+here; displacements are ~1e-8) and those force points; the gradient is
+that of the FMM operator on its tree, so the points that set the root cube
+and the force points within 1e-7 of a box face stay still too (otherwise
+the finite difference also sees the FMM's approximation error change with
+the box geometry: 9% on these directions); a direction along which some
+nearest force point still changes within +-h is drawn again; the FD solves
+run on
 FP64 Tikhonov operators (rounding ~1e-11
 instead of the exact inverse's ~1e-9), the analytic gradients on the same
 operators.  Takes about two minutes on a B200."""
@@ -57,6 +61,19 @@ def test_gradient_against_32_fd_directions_at_50k():
     tied = d2[:, 1] - d2[:, 0] < 1e-7
     still_x = np.zeros(len(X0), bool)
     still_x[i2[tied].ravel()] = True
+    # the FMM's boxes must not move either (the gradient is that of the FMM
+    # operator on a fixed tree): the points on the bounding box, which sets
+    # the root cube, stay still, and so do the force points within 1e-7 of a
+    # box face, whose leaf would change
+    for P, still in ((X0, still_x), (Y0, tied)):
+        for ax in range(3):
+            still |= (P[:, ax] <= P[:, ax].min() + 1e-12) | (P[:, ax] >= P[:, ax].max() - 1e-12)
+    T = nk.OcTree(X0, X0, nodeCapacity=opts["cap"], nearest=1, finePoints=Y0, NN=NN)
+    root = np.asarray(T.nodeCorners)[0]  # node 0 is the root: [lo hi]
+    cell = (root[3] - root[0]) / 2.0 ** int(np.asarray(T.nodeLevel).max())
+    u = (X0 - root[:3]) / cell
+    still_x |= (np.abs(u - np.rint(u)) * cell < 1e-7).any(axis=1)
+    del T
     fd, an = [], {p: [] for p in grads}
     tries = 0
     while len(fd) < 32:
@@ -78,7 +95,8 @@ def test_gradient_against_32_fd_directions_at_50k():
             an[p].append(float((gX * dX).sum() + (gY * dY).sum()))
     fd = np.array(fd)
     errs = {p: float(np.linalg.norm(np.array(v) - fd) / np.linalg.norm(fd)) for p, v in an.items()}
-    print("points", len(X0), len(Y0), "still", int(tied.sum()), int(still_x.sum()), "directions drawn", tries,
+    print("points", len(X0), len(Y0), "still", int(tied.sum()), int(still_x.sum()), "root", root, "cell", cell,
+          "directions drawn", tries,
           "directional-derivative error vs FD over 32 directions:", errs)
     assert errs["fp64"] <= 1e-3
     assert errs["mixed"] <= 1e-2
