@@ -636,11 +636,16 @@ void Fmm::build_c2e_tiles(const std::vector<int32_t>& nodes, const std::vector<i
 }
 
 // Load balance: within each launch group, tasks run heaviest first, and a
-// task above kMaxPairs target-source pairs is cut into pieces over its
-// flattened sources; each piece writes its own partial-sum slot and one
-// reduction per task adds the slots in a fixed order.
+// task above the group's piece size is cut into pieces over its flattened
+// sources; each piece writes its own partial-sum slot and one reduction per
+// task adds the slots in a fixed order.  The piece size is 65,536
+// target-source pairs, or a 1/1184 share (8 per SM) of the group's pairs if
+// that is larger: a group of thousands of heavy tasks (a forest of NEAREST
+// bodies) balances without cutting them, and its partial-sum slots (3R
+// values per piece and target) stay small.
 void Fmm::split_tasks(TaskSet& ts, std::vector<TaskD>& tasks, std::vector<SegD>& segs) {
-  constexpr int64_t kMaxPairs = 1 << 16;
+  constexpr int64_t kMinPiecePairs = 1 << 16;
+  constexpr int64_t kPiecesPerGroup = 148 * 8;
   constexpr int64_t kMinSources = 64;
   std::vector<TaskD> nt;
   std::vector<SegD> ns;
@@ -659,10 +664,13 @@ void Fmm::split_tasks(TaskSet& ts, std::vector<TaskD>& tasks, std::vector<SegD>&
       order[i] = i;
     }
     std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+    int64_t total = 0;
+    for (int64_t i = 0; i < g.count; ++i) total += cost[i];
+    const int64_t piece = std::max(kMinPiecePairs, total / kPiecesPerGroup);
     const int64_t first = (int64_t)nt.size(), rfirst = (int64_t)reds.size();
     for (int64_t i : order) {
       const TaskD r = tasks[g.first + i];
-      int64_t k = (cost[i] + kMaxPairs - 1) / kMaxPairs;
+      int64_t k = (cost[i] + piece - 1) / piece;
       k = std::max<int64_t>(1, std::min<int64_t>(k, nsrc[i] / kMinSources));
       if (k <= 1) {
         TaskD c = r;
@@ -922,6 +930,11 @@ void Fmm::assign_operators() {
 }
 
 namespace {
+// G = I (n x n)
+__global__ void identity_kernel(double* G, int n) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < (size_t)n * n) G[e] = (e % (n + 1) == 0) ? 1.0 : 0.0;
+}
 __global__ void add_diag_kernel(double* G, int n, double v) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) G[(size_t)i * n + i] += v;
@@ -970,6 +983,8 @@ void Fmm::build_operators() {
   // host part, in parallel over operators: K_up = kernel(upsurf, downsurf)
   // (up-equivalent densities -> down check) and, for the Tikhonov form,
   // sigma_max(K) by power iteration
+  // per operator: its up surface [0, w]^3 and down surface [-w, 2w]^3
+  std::vector<double> surf(2 * (size_t)n * std::max(nops_, 1));
   std::vector<std::vector<double>> Ks(nops_);
   std::vector<double> lam2(nops_, 0.0);
 #pragma omp parallel for schedule(dynamic, 1)
@@ -977,13 +992,15 @@ void Fmm::build_operators() {
     const double w = op_w_[o];
     const double lo[3] = {0, 0, 0}, hi[3] = {w, w, w};
     const double dlo[3] = {-w, -w, -w}, dhi[3] = {2 * w, 2 * w, 2 * w};
-    std::vector<double> us(3 * P_), ds(3 * P_);
-    surface(lo, hi, p_.res, lat, us.data());
-    surface(dlo, dhi, p_.res, lat, ds.data());
-    std::vector<double>& K = Ks[o];
-    K.assign((size_t)n * n, 0.0);
-    kernel_matrix(us, ds, p_.eps, p_.mu, K, n);
+    surface(lo, hi, p_.res, lat, &surf[2 * (size_t)n * o]);
+    surface(dlo, dhi, p_.res, lat, &surf[2 * (size_t)n * o + n]);
     if (!exact) {
+      // Tikhonov form: K on the host, for sigma_max(K) by power iteration
+      std::vector<double> us(surf.begin() + 2 * (size_t)n * o, surf.begin() + 2 * (size_t)n * o + n);
+      std::vector<double> ds(surf.begin() + 2 * (size_t)n * o + n, surf.begin() + 2 * (size_t)n * (o + 1));
+      std::vector<double>& K = Ks[o];
+      K.assign((size_t)n * n, 0.0);
+      kernel_matrix(us, ds, p_.eps, p_.mu, K, n);
       std::vector<double> v(n, 1.0), u(n);
       double smax = 0;
       for (int it = 0; it < 40; ++it) {
@@ -1006,6 +1023,8 @@ void Fmm::build_operators() {
       lam2[o] = (reg * smax) * (reg * smax);
     }
   }
+  DBuf<double> dsurf;
+  dsurf.upload(surf, st);
   Solver sv(ctx_);
   DBuf<double> dK((size_t)n * n), dG((size_t)n * n);
   DBuf<int> dpiv(n), dinfo(std::max(nops_, 1));
@@ -1020,21 +1039,26 @@ void Fmm::build_operators() {
       throw Error(NNK_E_CUDA, "potrf_bufferSize failed");
   }
   DBuf<double> dwork(std::max(lwork, 1));
-  std::vector<double> I((size_t)n * n, 0.0), KT;
-  for (int i = 0; i < n; ++i) I[(size_t)i * n + i] = 1.0;
+  std::vector<double> KT;
   for (int o = 0; o < nops_; ++o) {
-    const std::vector<double>& K = Ks[o];
     double* dst = ops_.p + (size_t)o * n * n;
-    NNK_CUDA(cudaMemcpyAsync(dK.p, K.data(), K.size() * 8, cudaMemcpyHostToDevice, st));
     if (exact) {
-      // A = K^-1 by LU with partial pivoting, as MATLAB's mldivide
-      NNK_CUDA(cudaMemcpyAsync(dst, I.data(), I.size() * 8, cudaMemcpyHostToDevice, st));
+      // K = kernel(upsurf, downsurf) on the device; A = K^-1 by LU with
+      // partial pivoting, as MATLAB's mldivide (the identity solved in place)
+      const double* S = dsurf.p + 2 * (size_t)n * o;
+      kernel_matrix_kernel<<<(unsigned)(((size_t)P_ * P_ + 255) / 256), 256, 0, st>>>(
+          S, P_, S + n, P_, p_.eps * p_.eps, 1.0 / (8.0 * M_PI * p_.mu), dK.p, n);
+      NNK_CHECK_LAUNCH();
+      identity_kernel<<<(unsigned)(((size_t)n * n + 255) / 256), 256, 0, st>>>(dst, n);
+      NNK_CHECK_LAUNCH();
       if (cusolverDnDgetrf(sv.s, n, n, dK.p, n, dwork.p, dpiv.p, dinfo.p + o) != CUSOLVER_STATUS_SUCCESS ||
           cusolverDnDgetrs(sv.s, CUBLAS_OP_N, n, n, dK.p, n, dpiv.p, dst, n, dinfo.p + o) !=
               CUSOLVER_STATUS_SUCCESS)
         throw Error(NNK_E_CUDA, "LU of the surface matrix failed");
     } else {
       // A = (K^T K + lam^2 I)^-1 K^T, lam = reg * sigma_max(K)
+      const std::vector<double>& K = Ks[o];
+      NNK_CUDA(cudaMemcpyAsync(dK.p, K.data(), K.size() * 8, cudaMemcpyHostToDevice, st));
       KT.resize((size_t)n * n);
       for (int r = 0; r < n; ++r)
         for (int c = 0; c < n; ++c) KT[(size_t)c * n + r] = K[(size_t)r * n + c];
@@ -1050,9 +1074,9 @@ void Fmm::build_operators() {
           cusolverDnDpotrs(sv.s, CUBLAS_FILL_MODE_LOWER, n, n, dG.p, n, dst, n, dinfo.p + o) !=
               CUSOLVER_STATUS_SUCCESS)
         throw Error(NNK_E_CUDA, "Cholesky of the regularized surface matrix failed");
+      // the host copies above read pageable memory; keep K and KT alive until done
+      NNK_CUDA(cudaStreamSynchronize(st));
     }
-    // the host copies above read pageable memory; keep K alive until done
-    NNK_CUDA(cudaStreamSynchronize(st));
   }
   std::vector<int> info(std::max(nops_, 1), 0);
   NNK_CUDA(cudaMemcpyAsync(info.data(), dinfo.p, info.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
