@@ -283,10 +283,11 @@ __host__ __device__ constexpr uint64_t group_mask(int dl) {
 // holds the 8 children's accumulators of one right-hand side at a time; per
 // (P, N) record the 8 source spectra go to this thread's own shared-memory
 // slots, then for each of the 27 values of pos_v - pos_i present in the
-// record the kernel spectrum of offset 2 d + delta is loaded once (one
-// difference ahead, into registers) and applied to every pair with that
-// difference.  Loop bounds and child positions are compile-time, so
-// accumulators stay in registers.  Every right-hand side
+// record the kernel spectrum of offset 2 d + delta is loaded once and applied
+// to every pair with that difference.  Loop bounds and child positions are
+// compile-time, so accumulators stay in registers (loading the next
+// difference's spectrum one step ahead costs 42 more registers, 2 blocks per
+// SM instead of 3, and ran 45% slower).  Every right-hand side
 // sums its pairs in the same order, so a pass of R right-hand sides gives
 // each of them bitwise the result of a pass of one.
 template <typename Real>
@@ -328,28 +329,14 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
     }
     const int dx2 = 2 * (rec.dcode / 9 - 1), dy2 = 2 * ((rec.dcode / 3) % 3 - 1), dz2 = 2 * (rec.dcode % 3 - 1);
     const int* so = spec_of + (size_t)rec.op * 343;
-    // the differences present in the record; the kernel spectrum of the next
-    // one is loaded into registers while the current one is applied
-    uint32_t gmask = 0;
-#pragma unroll
-    for (int dl = 0; dl < 27; ++dl)
-      if (mask & group_mask(dl)) gmask |= 1u << dl;
-    const int cbase = (dx2 + 2) * 49 + (dy2 + 2) * 7 + (dz2 + 2);  // code of difference (-1, -1, -1)
-    T2 nk6[6];
-    auto kload = [&](int dl) {
-      const T2* Kp = spec + (size_t)so[cbase + (dl / 9) * 49 + ((dl / 3) % 3) * 7 + dl % 3] * 6 * NK + k;
-#pragma unroll
-      for (int c = 0; c < 6; ++c) nk6[c] = Kp[(size_t)c * NK];
-    };
-    if (gmask) kload(__ffs(gmask) - 1);
 #pragma unroll
     for (int dl = 0; dl < 27; ++dl) {
       const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
       const uint64_t bits = mask & group_mask(dl);
       if (bits == 0) continue;
-      const T2 kxx = nk6[0], kxy = nk6[1], kxz = nk6[2], kyy = nk6[3], kyz = nk6[4], kzz = nk6[5];
-      const uint32_t rest = gmask & ~((2u << dl) - 1u);
-      if (rest) kload(__ffs(rest) - 1);
+      const int code = (dx2 + ex + 3) * 49 + (dy2 + ey + 3) * 7 + (dz2 + ez + 3);
+      const T2* Kp = spec + (size_t)so[code] * 6 * NK + k;
+      const T2 kxx = Kp[0], kxy = Kp[NK], kxz = Kp[2 * NK], kyy = Kp[3 * NK], kyz = Kp[4 * NK], kzz = Kp[5 * NK];
 #pragma unroll
       for (int a = 0; a < 8; ++a) {
         const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
