@@ -41,6 +41,10 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SIMT FP32 FMA pipes at m
 # 329,328 V pairs)
 M2L_TRAFFIC_250K = (0.433e9 + 9.4e6) * 1426620 / 329328
 FLOPS_PER_PAIR = 32  # regularized Stokeslet pair: 3 sub, 5 r^2, 1 +eps^2, 1 rsqrt, 2 cube, 5 r.f, 3 scale, 12 acc
+# the FP64 family accumulate kernel at 60k force / 240k quadrature points (329,328 V pairs):
+# DRAM read + write of one launch (profiles/fft_accumulate_family_60k.md)
+FAMILY_FP64_60K_BYTES = 277.43e6 + 107.10e6
+FAMILY_FP64_60K_PAIRS = 329328
 
 
 def parse():
@@ -604,6 +608,11 @@ def roofline(per_step, stats, precision, peaks, m2l_form):
                 "peak_source": simt_src, "launches_per_step": per_step[dom][1], "ms_per_launch": ms_l,
                 "algorithmic": f"{stats['m2l_pairs']} V pairs x {nk_freq} frequencies x 9 complex multiply-adds "
                                f"(72 flops) per step; the transforms are not counted", "traffic": None}
+        if fp64:
+            # DRAM bytes of one 60k capture of the FP64 accumulate kernel, scaled by V pairs
+            roof["traffic"] = FAMILY_FP64_60K_BYTES * stats["m2l_pairs"] / FAMILY_FP64_60K_PAIRS
+            roof["traffic_source"] = ("dram__bytes_read.sum + dram__bytes_write.sum of the 60k capture (one "
+                                      "launch), scaled by V pairs (profiles/fft_accumulate_family_60k.md)")
     elif dom in pairs:
         flops = pairs[dom] * FLOPS_PER_PAIR
         roof = {"kernel": f"p2p_kernel ({dom})", "bound": "fp64" if fp64 else "fp32",
@@ -710,6 +719,9 @@ def main():
         r["per_step"] = {kk: (v[0] / args.steps, v[1] / args.steps) for kk, v in r["prof"].items()}
         r["stats"] = r["fmm"].stats()
         r["setup_ms"] = {k: round(v, 1) for k, v in r["fmm"].setup_times().items()}
+        r["c2e_form"] = ("tensor cores: tcgen05 kind::i8 digit products, exact int32 sums combined in FP64 "
+                         f"({'9 x 9' if prec != 'mixed' else '5 x 4'} digits)" if r["fmm"].c2eMode() == 1
+                         else "FP64 SIMT")
         r["roofline"] = roofline(r["per_step"], r["stats"], "fp64" if prec == "near32" else prec, peaks,
                                  form_of[prec])
         del r["fmm"]  # one arm's device buffers at a time
@@ -756,6 +768,7 @@ def main():
                        "pairs_p2p": stats["pairs_p2p"], "pairs_up": stats["pairs_up"],
                        "pairs_down": stats["pairs_down"], "nn_gpu_s": round(nn_s, 3),
                        "tree_lists_s": tree_s,
+                       "c2e": H["c2e_form"],
                        "arm_wall_s": round(H["setup_s"], 2),
                        "fmm_setup_ms": H["setup_ms"]},
             "roofline": H["roofline"], "e2e": e2e, "gpu_launches": gpu_launches // max(args.steps, 1),

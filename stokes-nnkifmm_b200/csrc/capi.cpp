@@ -435,6 +435,21 @@ int nnk_fmm_setup_times(const nnk_fmm* fmm, double* ms, int32_t n) {
   return NNK_OK;
 }
 
+int nnk_fmm_set_c2e(nnk_fmm* fmm, int32_t mode) {
+  if (!fmm) return NNK_E_ARG;
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  fmm->f->set_c2e_mode(mode);
+  API_CATCH(ctx)
+}
+
+int nnk_fmm_c2e_mode(const nnk_fmm* fmm, int32_t* mode) {
+  if (!fmm || !mode) return NNK_E_ARG;
+  *mode = fmm->f->c2e_mode();
+  return NNK_OK;
+}
+
 int nnk_fmm_set_fold(nnk_fmm* fmm, int32_t on) {
   if (!fmm) return NNK_E_ARG;
   nnk_ctx* ctx = fmm->ctx;

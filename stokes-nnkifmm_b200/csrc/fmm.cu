@@ -239,11 +239,13 @@ void Fmm::set_profile(bool on) {
 
 void Fmm::check_errors() {
   if (tensor_m2l_) check_m2l_error(m2l_, ctx_->stream);
+  if (c2e_tc_.ready) check_c2e_tc_error(c2e_tc_, ctx_->stream);
   if (sparse_) sparse_->check_errors();
 }
 
 void Fmm::poll_errors() {
   if (tensor_m2l_) poll_m2l_error(m2l_, ctx_->stream);
+  if (c2e_tc_.ready) poll_c2e_tc_error(c2e_tc_, ctx_->stream);
   if (sparse_) sparse_->poll_errors();
 }
 
@@ -1084,6 +1086,13 @@ void Fmm::build_operators() {
   for (int o = 0; o < nops_; ++o)
     if (info[o] != 0)
       throw Error(NNK_E_CUDA, "surface matrix factorization reported info=" + std::to_string(info[o]));
+  // their int8 digits for the tensor-core products: 9 x 9 digits, levels
+  // t + u < 9 with FP64 check vectors; 5 x 4, t + u < 5 with FP32 ones
+  if (n <= 512) {
+    if (f64()) build_c2e_tc(c2e_tc_, ops_.p, nops_, n, 9, 9, 9, st);
+    else build_c2e_tc(c2e_tc_, ops_.p, nops_, n, 5, 4, 5, st);
+    reserve_tc_scratch();
+  }
   setup_ms_[NNK_SETUP_OPERATORS] = ms_since(tops);
   const auto tfold = clk::now();
   build_fold_operators(fold_on_ == 2);
@@ -1113,6 +1122,38 @@ void add_f32(long long n, const float* b, double* a, cudaStream_t st) {
   NNK_CHECK_LAUNCH();
 }
 }  // namespace
+
+template <typename Real>
+void Fmm::c2e(int trans, const C2ETile* tiles, int ntiles, const int32_t* nodes, const Real* check, Real* dst,
+              int64_t base, int R, float* m2l_dst, int NP, const int* nact) {
+  if (tc_c2e())
+    launch_c2e_tc<Real>(c2e_tc_, trans, tiles, ntiles, nodes, check, dst, base, P_, R, ctx_->stream, m2l_dst, NP,
+                        nact);
+  else
+    launch_c2e<Real>(ops_.p, 3 * P_, trans, tiles, ntiles, nodes, check, dst, base, P_, R, ctx_->stream, m2l_dst, NP,
+                     c2e_part_.p, c2e_part_.n, nact);
+}
+
+// Scratch of the tensor-core C2E for the largest launch of either task set.
+void Fmm::reserve_tc_scratch() {
+  if (!c2e_tc_.ready) return;
+  size_t need = 0;
+  auto scan = [&](const std::vector<int64_t>& toff) {
+    for (size_t L = 0; L + 1 < toff.size(); ++L) need = std::max(need, c2e_tc_blocks((int)(toff[L + 1] - toff[L]), R_));
+  };
+  scan(dn_toff_);
+  scan(fwd_.up_toff);
+  if (fwd_.fold) scan(fwd_.upl_toff);
+  if (!adj_.up_toff.empty()) scan(adj_.up_toff);  // the transpose's, once built
+  reserve_c2e_tc(c2e_tc_, need);
+}
+
+void Fmm::set_c2e_mode(int mode) {
+  if (mode < 0 || mode > 1) throw Error(NNK_E_ARG, "C2E mode must be 0 or 1");
+  NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
+  c2e_mode_ = mode;
+  bump_version();
+}
 
 template <typename Real>
 void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, int R, bool near, bool fold) {
@@ -1146,8 +1187,8 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
       const int64_t nt = ts.upl_toff[L + 1] - ts.upl_toff[L];
       const int64_t nf = fup_toff_[L + 1] - fup_toff_[L];
       phase(NNK_PHASE_UP_C2E, [&] {
-        launch_c2e<Real>(ops_.p, n, 0, ts.upl_tiles.p + ts.upl_toff[L], (int)nt, ts.upl_nodes.p, check, str, regionA,
-                         P_, R, st, m2l_src, m2l_.NP, c2e_part_.p, c2e_part_.n, na);
+        c2e<Real>(0, ts.upl_tiles.p + ts.upl_toff[L], (int)nt, ts.upl_nodes.p, check, str, regionA, R, m2l_src,
+                  m2l_.NP, na);
         NodeGemm g{fold_up_.p, (size_t)8 * n * n, n, 8 * n, 0, fup_tiles_.p + fup_toff_[L], fpar_.p, fch_.p,
                    (long long)regionA, P_, R, 0, m2l_src, m2l_.NP};
         launch_node_gemm<Real>(g, (int)nf, str + (size_t)C * regionA, str, st, c2e_part_.p, c2e_part_.n, na);
@@ -1158,8 +1199,8 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     run_group<Real>(ts, ts.up[L], spos, str, spos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS, R);
     const int64_t nt = ts.up_toff[L + 1] - ts.up_toff[L];
     phase(NNK_PHASE_UP_C2E, [&] {
-      launch_c2e<Real>(ops_.p, n, 0, ts.up_tiles.p + ts.up_toff[L], (int)nt, ts.up_nodes.p, check, str, regionA, P_,
-                       R, st, m2l_src, m2l_.NP, c2e_part_.p, c2e_part_.n, na);
+      c2e<Real>(0, ts.up_tiles.p + ts.up_toff[L], (int)nt, ts.up_nodes.p, check, str, regionA, R, m2l_src, m2l_.NP,
+                na);
     });
   }
   if (save_up_) NNK_CUDA(cudaMemcpyAsync(save_up_, check, sizeof(Real) * (size_t)N_ * n * R, cudaMemcpyDeviceToDevice,
@@ -1198,8 +1239,7 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     const int64_t nt = dn_toff_[L + 1] - dn_toff_[L];
     if (nt == 0) continue;
     phase(NNK_PHASE_DOWN_C2E, [&] {
-      launch_c2e<Real>(ops_.p, n, 1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str, dnB, P_, R, st,
-                       nullptr, 0, c2e_part_.p, c2e_part_.n, na);
+      c2e<Real>(1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str, dnB, R, nullptr, 0, na);
       if (fo && L >= 2) {
         // + D applied to the parents (level L - 1) for their 8 children
         const int64_t nf = fdn_toff_[L] - fdn_toff_[L - 1];
@@ -1689,6 +1729,7 @@ void Fmm::build_adjoint() {
   r.W = &inv_X_;  // leaves s receive from upsurf(t) for t with s in X(t)
   r.X = &inv_W_;  // node t receives from the targets of leaves s with t in W(s)
   build_taskset(adj_, r, false);
+  reserve_tc_scratch();
   const int64_t slots = 3 * std::max(fwd_.partial_slots, adj_.partial_slots) * R_;
   if (f64()) {
     if ((int64_t)partial64_.n < slots) partial64_.alloc(slots);

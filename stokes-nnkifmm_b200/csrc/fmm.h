@@ -20,6 +20,7 @@
 #include "common.h"
 #include "m2l.h"
 #include "m2l_fft.h"
+#include "c2e_tc.h"
 #include "tree.h"
 
 namespace nnk {
@@ -206,6 +207,10 @@ class Fmm {
   // uses it.
   void set_fold(int mode);
   bool folded() const { return fold_ok_ && fold_on_ > 0; }
+  // Check-to-equivalent products: 1 tensor cores (where 3P <= 512), 0 FP64
+  // SIMT; the mode in use.
+  void set_c2e_mode(int mode);
+  int c2e_mode() const { return tc_c2e() ? 1 : 0; }
   // host wall time of the set-up steps (NNK_SETUP_*), milliseconds
   const double* setup_ms() const { return setup_ms_; }
   bool near32() const { return p_.precision == NNK_PREC_NEAR32; }
@@ -293,6 +298,18 @@ class Fmm {
   std::vector<double> op_w_;          // box width of each operator
   std::vector<int> op_of_;            // (group * (maxl + 1) + level) -> operator
   DBuf<C2ETile> dn_tiles_;  // per level, tiles of nodes sharing an operator
+  // check-to-equivalent products on the tensor cores (int8 digits, FP64
+  // accuracy; c2e_tc.h) or on the FP64 SIMT units
+  C2ETcPlan c2e_tc_;
+  int c2e_mode_ = -1;       // 1 tensor cores where available, 0 SIMT, -1 the precision's default
+  // default: tensor cores for the mixed mode's FP32 check vectors (5 x 4
+  // digits), FP64 SIMT for FP64 ones (9 x 9 digits on N = 32 tiles ran
+  // slower than the SIMT product)
+  bool tc_c2e() const { return (c2e_mode_ < 0 ? !f64() : c2e_mode_ == 1) && c2e_tc_.ready; }
+  void reserve_tc_scratch();
+  template <typename Real>
+  void c2e(int trans, const C2ETile* tiles, int ntiles, const int32_t* nodes, const Real* check, Real* dst,
+           int64_t base, int R, float* m2l_dst, int NP, const int* nact);
   // folded M2M / L2L: per operator (box width w), U = A(w) [M2M_0 .. M2M_7]
   // (3P x 8 * 3P; M2M_k: child k's up surface -> the down surface of its
   // parent of width w) and D = [A(w)^T L2L_0; ..; A(w)^T L2L_7] (8 * 3P x 3P;

@@ -88,6 +88,8 @@ SIGNATURES = {
     "nnk_fmm_reduced_solve": (_i32, [_vp, _vp, _vp, _i32, _i32]),
     "nnk_fmm_stats_get": (_i32, [_vp, C.POINTER(FmmStats)]),
     "nnk_fmm_set_fold": (_i32, [_vp, _i32]),
+    "nnk_fmm_set_c2e": (_i32, [_vp, _i32]),
+    "nnk_fmm_c2e_mode": (_i32, [_vp, C.POINTER(_i32)]),
     "nnk_fmm_setup_times": (_i32, [_vp, C.POINTER(C.c_double), _i32]),
     "nnk_fmm_destroy": (_i32, [_vp]),
     "nnk_fmm_apply_adjoint": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32]),

@@ -115,6 +115,17 @@ class KIFMM:
         stats()["folded"] says whether the matvec folds."""
         L.check(L.lib.nnk_fmm_set_fold(self.h, int(mode)), self.ctx.h, "setFold")
 
+    def setC2E(self, mode=1):
+        """Check-to-equivalent products on the tensor cores (1, the default
+        where available: int8 digit products with FP64 accuracy) or as FP64
+        SIMT products (0)."""
+        L.check(L.lib.nnk_fmm_set_c2e(self.h, int(mode)), self.ctx.h, "setC2E")
+
+    def c2eMode(self):
+        m = C.c_int32()
+        L.check(L.lib.nnk_fmm_c2e_mode(self.h, C.byref(m)))
+        return m.value
+
     def setup_times(self):
         """Host wall time (ms) of the set-up steps: points, tasks, m2l,
         operators, fold, total (nnk_fmm_setup_times)."""

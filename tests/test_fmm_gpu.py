@@ -208,6 +208,40 @@ def test_folded_m2m_l2l_matches_pair_sums(name):
     assert exact.stats()["folded"] == 0
 
 
+C2E_TC_TOL = {"fp64": 1e-7, "near32": 1e-7, "mixed": 1e-5}
+
+
+@pytest.mark.parametrize("precision", sorted(C2E_TC_TOL))
+@pytest.mark.parametrize("name", ["sphere10_40", "adaptive_nearest_1200", "split_1500_700", "matvec_4000_16000"])
+def test_tensor_core_c2e_matches_fp64_simt(name, precision):
+    """Check-to-equivalent products on the tensor cores (int8 digits, exact
+    int32 sums combined in FP64) against the FP64 SIMT products:
+    the same FP64 product to rounding, lifted by the exact inverses'
+    condition number in FP64 mode (6e-9 to 1.3e-8, where FP64 mode is 1e-8
+    to 6e-8 from the oracle with either); in mixed mode the 4 digits of a
+    check column keep 28 bits below its largest entry and the 5 of an
+    operator row 35, 1e-6 to 5e-6 from the SIMT product, within the mixed
+    matvec's own 5e-5.  FP64 mode
+    still matches the oracle."""
+    g = load(name)
+    t = tree_of(g)
+    fmm = nk.KIFMM(t, [float(g["eps"]), float(g["mu"])], precision=precision)
+    assert fmm.c2eMode() == (1 if precision == "mixed" else 0)  # the defaults
+    fmm.setC2E(1)
+    assert fmm.c2eMode() == 1
+    a = fmm.computeVel(g["F"])
+    fmm.setC2E(0)
+    assert fmm.c2eMode() == 0
+    b = fmm.computeVel(g["F"])
+    fmm.setC2E(1)
+    c = fmm.computeVel(g["F"])
+    print(name, precision, "tensor-core C2E vs SIMT", rel(a, b), "vs oracle", rel(a, g["vel"]), rel(b, g["vel"]))
+    assert np.array_equal(a, c)
+    assert rel(a, b) <= C2E_TC_TOL[precision]
+    if precision == "fp64":
+        assert rel(a, g["vel"]) <= FP64_TOL[name]
+
+
 @pytest.mark.parametrize("name", sorted(FP64_TOL))
 def test_fourier_m2l_matches_pair_m2l(name):
     """The Fourier-space M2L (FP32 spectra) gives the FP32 pair-kernel M2L
