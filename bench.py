@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--fp64-batch", action="store_true",
                     help="also time the FP64 forest batch (the batched configuration's third arm)")
     ap.add_argument("--no-gradient", action="store_true")
+    ap.add_argument("--no-tc-c2e", dest="tc_c2e_check", action="store_false",
+                    help="skip timing each arm again with the tensor-core check-to-equivalent products")
     ap.add_argument("--no-squirmers", action="store_true")
     ap.add_argument("--m2l", default="auto", choices=["auto", "images", "generate", "pairs", "fft"],
                     help="M2L form of the mixed matvec (auto: tensor cores on rank-256 compressed operators); "
@@ -669,8 +671,21 @@ def time_arm(torch, nk, w, tree, precision, m2l, args, flush, clocks=None):
         b.record(st)
         torch.cuda.synchronize()
         e_ms.append(a.elapsed_time(b))
-    return {"fmm": fmm, "ms": ms, "prof": prof, "clocks": clk, "out": fout.cpu().numpy(), "e2e_ms": e_ms,
-            "h2d": int(hin.numel() * 8), "d2h": int(hout.numel() * 8)}
+    out = {"fmm": fmm, "ms": ms, "prof": prof, "clocks": clk, "out": fout.cpu().numpy(), "e2e_ms": e_ms,
+           "h2d": int(hin.numel() * 8), "d2h": int(hout.numel() * 8)}
+    if args.tc_c2e_check:
+        # the same matvecs with the check-to-equivalent products on the tensor
+        # cores (int8 digits, exact int32 sums combined in FP64): time and
+        # difference from the default FP64 SIMT products
+        fmm.setC2E(1)
+        ms_tc, prof_tc = time_device(torch, fmm, fin, fout, args.steps, args.warmup, flush, prof=True)
+        fmm.setC2E(0)
+        c2e = lambda p: sum(p[k][0] for k in ("up_c2e", "down_c2e") if k in p) / max(args.steps, 1)
+        o, tcv = out["out"], fout.cpu().numpy()
+        out["tc_c2e"] = {"ms_per_step": float(np.mean(ms_tc)), "c2e_ms_per_step": c2e(prof_tc),
+                         "simt_c2e_ms_per_step": c2e(prof),
+                         "rel_diff_vs_simt": float(np.linalg.norm(tcv - o) / np.linalg.norm(o))}
+    return out
 
 
 def main():
@@ -778,6 +793,8 @@ def main():
         line["note"] = note
     if errors:
         line["errors"] = errors
+    if H.get("tc_c2e"):
+        line["tc_c2e"] = H["tc_c2e"]
     for p in res:
         if p == head:
             continue
@@ -795,6 +812,8 @@ def main():
                             "speedup_vs_" + head: H["step_ms"] / o["step_ms"], "roofline": o["roofline"],
                             "arm_wall_s": round(o["setup_s"], 2),
                             "fmm_setup_ms": o["setup_ms"]}
+        if o.get("tc_c2e"):
+            line[f"{p}_gpu"]["tc_c2e"] = o["tc_c2e"]
     del res
     if rank == 0 and not args.no_solves:
         line["mobility_solves"] = solve_benchmarks(torch, nk, args)

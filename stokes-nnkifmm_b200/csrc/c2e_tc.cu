@@ -261,30 +261,8 @@ __global__ void __launch_bounds__(128, 1)
 
 size_t tc_smem(int sA, int sB) { return 1024 + (size_t)sA * kATile + (size_t)sB * kBTile + 64; }
 
-void mirror_err(C2ETcPlan& plan, cudaStream_t st) {
-  NNK_CUDA(cudaMemcpyAsync(plan.h_err, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-  NNK_CUDA(cudaEventRecord(plan.err_ev, st));
-}
-
-int take_err(C2ETcPlan& plan, cudaStream_t st) {
-  if (!plan.h_err || !plan.err_ev) return 0;
-  const cudaError_t q = cudaEventQuery(plan.err_ev);
-  if (q == cudaErrorNotReady) return 0;
-  NNK_CUDA(q);
-  const int f = *plan.h_err;
-  if (f) {
-    *plan.h_err = 0;
-    NNK_CUDA(cudaMemsetAsync(plan.err.p, 0, sizeof(int), st));
-  }
-  return f;
-}
-
 }  // namespace
 
-C2ETcPlan::~C2ETcPlan() {
-  if (h_err) cudaFreeHost(h_err);
-  if (err_ev) cudaEventDestroy(err_ev);
-}
 
 size_t c2e_tc_blocks(int ntiles, int R) { return (size_t)ntiles * ((kC2ETileNodes * R + kCols - 1) / kCols); }
 
@@ -306,9 +284,6 @@ void build_c2e_tc(C2ETcPlan& plan, const double* ops, int nops, int n, int sA, i
     plan.err.alloc(1);
     plan.err.zero(st);
   }
-  if (!plan.h_err) NNK_CUDA(cudaMallocHost((void**)&plan.h_err, sizeof(int)));
-  *plan.h_err = 0;
-  if (!plan.err_ev) NNK_CUDA(cudaEventCreateWithFlags(&plan.err_ev, cudaEventDisableTiming));
   plan.smem_bytes = tc_smem(sA, sB);
   NNK_CUDA(cudaFuncSetAttribute(c2e_tc_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)plan.smem_bytes));
@@ -340,7 +315,6 @@ void launch_c2e_tc(C2ETcPlan& plan, int trans, const C2ETile* tiles, int ntiles,
       plan.adig.p, plan.aexp.p, trans ? 1 : 0, plan.sA, plan.sB, plan.L, tiles, nodes, zch, plan.bdig.p,
       plan.bexp.p, plan.n, P, R, dst, (long long)base, m2l_dst, NP, plan.err.p, plan.wait_limit, nact);
   NNK_CHECK_LAUNCH();
-  mirror_err(plan, st);
 }
 
 template void launch_c2e_tc<double>(C2ETcPlan&, int, const C2ETile*, int, const int32_t*, const double*, double*,
@@ -348,15 +322,15 @@ template void launch_c2e_tc<double>(C2ETcPlan&, int, const C2ETile*, int, const 
 template void launch_c2e_tc<float>(C2ETcPlan&, int, const C2ETile*, int, const int32_t*, const float*, float*,
                                    int64_t, int, int, cudaStream_t, float*, int, const int*);
 
-void poll_c2e_tc_error(C2ETcPlan& plan, cudaStream_t st) {
-  const int f = take_err(plan, st);
-  if (f) throw Error(NNK_E_TIMEOUT, "tensor-core C2E gave up a bounded wait (flag " + std::to_string(f) + ")");
-}
-
 void check_c2e_tc_error(C2ETcPlan& plan, cudaStream_t st) {
-  if (!plan.h_err) return;
+  if (!plan.err.p) return;
   NNK_CUDA(cudaStreamSynchronize(st));
-  poll_c2e_tc_error(plan, st);
+  int f = 0;
+  NNK_CUDA(cudaMemcpy(&f, plan.err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (f) {
+    NNK_CUDA(cudaMemsetAsync(plan.err.p, 0, sizeof(int), st));
+    throw Error(NNK_E_TIMEOUT, "tensor-core C2E gave up a bounded wait (flag " + std::to_string(f) + ")");
+  }
 }
 
 }  // namespace nnk

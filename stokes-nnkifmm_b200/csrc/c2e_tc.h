@@ -39,13 +39,10 @@ struct C2ETcPlan {
   DBuf<int8_t> bdig;          // launch scratch: [block][4][sB][32 x 128]
   DBuf<int> bexp;             // launch scratch: [block][32]
   size_t bblocks = 0;         // blocks the scratch holds
-  DBuf<int> err;              // bounded-wait timeout flag
-  int* h_err = nullptr;       // pinned mirror of err
-  cudaEvent_t err_ev = nullptr;
+  DBuf<int> err;              // bounded-wait timeout flag (read at the caller's synchronizations)
   uint32_t wait_limit = 1u << 26;
   size_t smem_bytes = 0;
   bool ready = false;
-  ~C2ETcPlan();
 };
 
 // Digits of the n x n column-major operators ops[op] (A and A^T) for the
@@ -60,9 +57,9 @@ template <typename Real>
 void launch_c2e_tc(C2ETcPlan& plan, int trans, const C2ETile* tiles, int ntiles, const int32_t* nodes,
                    const Real* check, Real* dst, int64_t base, int P, int R, cudaStream_t st,
                    float* m2l_dst = nullptr, int NP = 0, const int* nact = nullptr);
-// A flag set by an earlier launch: NNK_E_TIMEOUT (poll: without waiting for
-// the stream; check: after synchronizing it).
-void poll_c2e_tc_error(C2ETcPlan& plan, cudaStream_t st);
+// A flag set by an earlier launch: NNK_E_TIMEOUT.  Synchronizes the stream
+// and reads the flag (no event is recorded with the launches, so they can be
+// captured into CUDA graphs).
 void check_c2e_tc_error(C2ETcPlan& plan, cudaStream_t st);
 
 }  // namespace nnk

@@ -245,7 +245,6 @@ void Fmm::check_errors() {
 
 void Fmm::poll_errors() {
   if (tensor_m2l_) poll_m2l_error(m2l_, ctx_->stream);
-  if (c2e_tc_.ready) poll_c2e_tc_error(c2e_tc_, ctx_->stream);
   if (sparse_) sparse_->poll_errors();
 }
 
@@ -1086,13 +1085,8 @@ void Fmm::build_operators() {
   for (int o = 0; o < nops_; ++o)
     if (info[o] != 0)
       throw Error(NNK_E_CUDA, "surface matrix factorization reported info=" + std::to_string(info[o]));
-  // their int8 digits for the tensor-core products: 9 x 9 digits, levels
-  // t + u < 9 with FP64 check vectors; 5 x 4, t + u < 5 with FP32 ones
-  if (n <= 512) {
-    if (f64()) build_c2e_tc(c2e_tc_, ops_.p, nops_, n, 9, 9, 9, st);
-    else build_c2e_tc(c2e_tc_, ops_.p, nops_, n, 5, 4, 5, st);
-    reserve_tc_scratch();
-  }
+  // their int8 digits, when the tensor-core products are asked for
+  if (c2e_mode_ == 1) build_tc_digits();
   setup_ms_[NNK_SETUP_OPERATORS] = ms_since(tops);
   const auto tfold = clk::now();
   build_fold_operators(fold_on_ == 2);
@@ -1148,10 +1142,21 @@ void Fmm::reserve_tc_scratch() {
   reserve_c2e_tc(c2e_tc_, need);
 }
 
+// Digits of the operators for the tensor-core products: 9 x 9 digits, levels
+// t + u < 9 with FP64 check vectors; 5 x 4, t + u < 5 with FP32 ones.
+void Fmm::build_tc_digits() {
+  const int n = 3 * P_;
+  if (n > 512) return;  // the products stay on the SIMT units
+  if (f64()) build_c2e_tc(c2e_tc_, ops_.p, nops_, n, 9, 9, 9, ctx_->stream);
+  else build_c2e_tc(c2e_tc_, ops_.p, nops_, n, 5, 4, 5, ctx_->stream);
+  reserve_tc_scratch();
+}
+
 void Fmm::set_c2e_mode(int mode) {
   if (mode < 0 || mode > 1) throw Error(NNK_E_ARG, "C2E mode must be 0 or 1");
   NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
   c2e_mode_ = mode;
+  if (mode == 1 && !c2e_tc_.ready) build_tc_digits();
   bump_version();
 }
 

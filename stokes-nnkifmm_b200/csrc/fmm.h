@@ -301,11 +301,9 @@ class Fmm {
   // check-to-equivalent products on the tensor cores (int8 digits, FP64
   // accuracy; c2e_tc.h) or on the FP64 SIMT units
   C2ETcPlan c2e_tc_;
-  int c2e_mode_ = -1;       // 1 tensor cores where available, 0 SIMT, -1 the precision's default
-  // default: tensor cores for the mixed mode's FP32 check vectors (5 x 4
-  // digits), FP64 SIMT for FP64 ones (9 x 9 digits on N = 32 tiles ran
-  // slower than the SIMT product)
-  bool tc_c2e() const { return (c2e_mode_ < 0 ? !f64() : c2e_mode_ == 1) && c2e_tc_.ready; }
+  int c2e_mode_ = 0;        // 1 tensor cores where available, 0 SIMT (the default: faster here)
+  bool tc_c2e() const { return c2e_mode_ == 1 && c2e_tc_.ready; }
+  void build_tc_digits();
   void reserve_tc_scratch();
   template <typename Real>
   void c2e(int trans, const C2ETile* tiles, int ntiles, const int32_t* nodes, const Real* check, Real* dst,

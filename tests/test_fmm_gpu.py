@@ -226,7 +226,7 @@ def test_tensor_core_c2e_matches_fp64_simt(name, precision):
     g = load(name)
     t = tree_of(g)
     fmm = nk.KIFMM(t, [float(g["eps"]), float(g["mu"])], precision=precision)
-    assert fmm.c2eMode() == (1 if precision == "mixed" else 0)  # the defaults
+    assert fmm.c2eMode() == 0  # the default
     fmm.setC2E(1)
     assert fmm.c2eMode() == 1
     a = fmm.computeVel(g["F"])
