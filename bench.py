@@ -673,18 +673,23 @@ def time_arm(torch, nk, w, tree, precision, m2l, args, flush, clocks=None):
         e_ms.append(a.elapsed_time(b))
     out = {"fmm": fmm, "ms": ms, "prof": prof, "clocks": clk, "out": fout.cpu().numpy(), "e2e_ms": e_ms,
            "h2d": int(hin.numel() * 8), "d2h": int(hout.numel() * 8)}
+    out["c2e_mode"] = fmm.c2eMode()  # the form autotune kept (timed above)
     if args.tc_c2e_check:
-        # the same matvecs with the check-to-equivalent products on the tensor
-        # cores (int8 digits, exact int32 sums combined in FP64): time and
-        # difference from the default FP64 SIMT products
-        fmm.setC2E(1)
-        ms_tc, prof_tc = time_device(torch, fmm, fin, fout, args.steps, args.warmup, flush, prof=True)
-        fmm.setC2E(0)
+        # the same matvecs with each form of the check-to-equivalent products
+        # forced: the tensor cores (int8 digits, exact int32 sums combined in
+        # FP64) and the FP64 SIMT units; then back to the autotuned choice
         c2e = lambda p: sum(p[k][0] for k in ("up_c2e", "down_c2e") if k in p) / max(args.steps, 1)
-        o, tcv = out["out"], fout.cpu().numpy()
-        out["tc_c2e"] = {"ms_per_step": float(np.mean(ms_tc)), "c2e_ms_per_step": c2e(prof_tc),
-                         "simt_c2e_ms_per_step": c2e(prof),
-                         "rel_diff_vs_simt": float(np.linalg.norm(tcv - o) / np.linalg.norm(o))}
+        forms = {}
+        for mode, key in ((1, "tensor_cores"), (0, "simt")):
+            fmm.setC2E(mode)
+            ms_f, prof_f = time_device(torch, fmm, fin, fout, args.steps, args.warmup, flush, prof=True)
+            forms[key] = {"ms_per_step": float(np.mean(ms_f)), "c2e_ms_per_step": c2e(prof_f),
+                          "out": fout.cpu().numpy()}
+        fmm.setC2E(-1)
+        a, b = forms["tensor_cores"].pop("out"), forms["simt"].pop("out")
+        forms["rel_diff"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        forms["kept"] = "tensor_cores" if out["c2e_mode"] == 1 else "simt"
+        out["tc_c2e"] = forms
     return out
 
 
@@ -735,8 +740,8 @@ def main():
         r["stats"] = r["fmm"].stats()
         r["setup_ms"] = {k: round(v, 1) for k, v in r["fmm"].setup_times().items()}
         r["c2e_form"] = ("tensor cores: tcgen05 kind::i8 digit products, exact int32 sums combined in FP64 "
-                         f"({'9 x 9' if prec != 'mixed' else '5 x 4'} digits)" if r["fmm"].c2eMode() == 1
-                         else "FP64 SIMT")
+                         f"({'9 x 9' if prec != 'mixed' else '5 x 4'} digits)" if r["c2e_mode"] == 1
+                         else "FP64 SIMT") + " (the faster of the two as timed by autotune)"
         r["roofline"] = roofline(r["per_step"], r["stats"], "fp64" if prec == "near32" else prec, peaks,
                                  form_of[prec])
         del r["fmm"]  # one arm's device buffers at a time
@@ -794,7 +799,7 @@ def main():
     if errors:
         line["errors"] = errors
     if H.get("tc_c2e"):
-        line["tc_c2e"] = H["tc_c2e"]
+        line["c2e_forms"] = H["tc_c2e"]
     for p in res:
         if p == head:
             continue
@@ -812,8 +817,9 @@ def main():
                             "speedup_vs_" + head: H["step_ms"] / o["step_ms"], "roofline": o["roofline"],
                             "arm_wall_s": round(o["setup_s"], 2),
                             "fmm_setup_ms": o["setup_ms"]}
+        line[f"{p}_gpu"]["c2e"] = o["c2e_form"]
         if o.get("tc_c2e"):
-            line[f"{p}_gpu"]["tc_c2e"] = o["tc_c2e"]
+            line[f"{p}_gpu"]["c2e_forms"] = o["tc_c2e"]
     del res
     if rank == 0 and not args.no_solves:
         line["mobility_solves"] = solve_benchmarks(torch, nk, args)

@@ -293,6 +293,15 @@ void build_c2e_tc(C2ETcPlan& plan, const double* ops, int nops, int n, int sA, i
   plan.ready = true;
 }
 
+void release_c2e_tc(C2ETcPlan& plan) {
+  plan.adig.release();
+  plan.aexp.release();
+  plan.bdig.release();
+  plan.bexp.release();
+  plan.bblocks = 0;
+  plan.ready = false;
+}
+
 void reserve_c2e_tc(C2ETcPlan& plan, size_t blocks) {
   if (blocks <= plan.bblocks) return;
   plan.bdig.alloc(blocks * 4 * plan.sB * kBTile);

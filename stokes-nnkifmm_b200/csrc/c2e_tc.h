@@ -48,6 +48,8 @@ struct C2ETcPlan {
 // Digits of the n x n column-major operators ops[op] (A and A^T) for the
 // given digit counts; device work on st.
 void build_c2e_tc(C2ETcPlan& plan, const double* ops, int nops, int n, int sA, int sB, int L, cudaStream_t st);
+// Frees the digits and the scratch (the plan is no longer ready).
+void release_c2e_tc(C2ETcPlan& plan);
 // Scratch for launches of up to `blocks` 32-column blocks.
 void reserve_c2e_tc(C2ETcPlan& plan, size_t blocks);
 // Blocks (32 columns each) a launch over ntiles tiles of R right-hand sides needs.

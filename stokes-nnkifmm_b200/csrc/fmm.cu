@@ -1085,8 +1085,8 @@ void Fmm::build_operators() {
   for (int o = 0; o < nops_; ++o)
     if (info[o] != 0)
       throw Error(NNK_E_CUDA, "surface matrix factorization reported info=" + std::to_string(info[o]));
-  // their int8 digits, when the tensor-core products are asked for
-  if (c2e_mode_ == 1) build_tc_digits();
+  // their int8 digits, when the tensor-core products are asked for or chosen
+  if (c2e_mode_ == 1 || (c2e_mode_ < 0 && tc_auto_)) build_tc_digits();
   setup_ms_[NNK_SETUP_OPERATORS] = ms_since(tops);
   const auto tfold = clk::now();
   build_fold_operators(fold_on_ == 2);
@@ -1153,7 +1153,7 @@ void Fmm::build_tc_digits() {
 }
 
 void Fmm::set_c2e_mode(int mode) {
-  if (mode < 0 || mode > 1) throw Error(NNK_E_ARG, "C2E mode must be 0 or 1");
+  if (mode < -1 || mode > 1) throw Error(NNK_E_ARG, "C2E mode must be -1, 0 or 1");
   NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
   c2e_mode_ = mode;
   if (mode == 1 && !c2e_tc_.ready) build_tc_digits();
@@ -1466,6 +1466,48 @@ double tune_groups(Fmm* self, std::vector<TaskGroup*>& groups, const std::vector
 }  // namespace
 
 std::pair<double, double> Fmm::autotune(int nrhs) {
+  const std::pair<double, double> r = autotune_tiles(nrhs);
+  if (c2e_mode_ < 0) tune_c2e(rhs_chunk(nrhs, rhs_cap(false)));
+  return r;
+}
+
+// The check-to-equivalent products' form in auto mode: one matvec of R
+// right-hand sides timed (best of three) with each, the faster kept; the
+// operator digits are dropped when the SIMT products win.
+void Fmm::tune_c2e(int R) {
+  if (3 * P_ > 512) return;
+  if (!c2e_tc_.ready) build_tc_digits();
+  if (!c2e_tc_.ready) return;
+  const HostTree& t = *t_;
+  cudaStream_t st = ctx_->stream;
+  DBuf<double> in(3 * (size_t)t.n_pot * R), out(3 * (size_t)t.n_tgt * R);
+  in.zero(st);
+  cudaEvent_t a, b;
+  NNK_CUDA(cudaEventCreate(&a));
+  NNK_CUDA(cudaEventCreate(&b));
+  float best[2] = {1e30f, 1e30f};
+  for (int m = 0; m < 2; ++m) {
+    tc_auto_ = m == 1;
+    bump_version();
+    apply(in.p, out.p, NNK_LAYOUT_ROWS, R);  // warm
+    for (int rep = 0; rep < 3; ++rep) {
+      NNK_CUDA(cudaEventRecord(a, st));
+      apply(in.p, out.p, NNK_LAYOUT_ROWS, R);
+      NNK_CUDA(cudaEventRecord(b, st));
+      NNK_CUDA(cudaEventSynchronize(b));
+      float x = 0;
+      NNK_CUDA(cudaEventElapsedTime(&x, a, b));
+      best[m] = std::min(best[m], x);
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  tc_auto_ = best[1] < best[0];
+  if (!tc_auto_) release_c2e_tc(c2e_tc_);
+  bump_version();
+}
+
+std::pair<double, double> Fmm::autotune_tiles(int nrhs) {
   bump_version();
   const HostTree& t = *t_;
   const int R = rhs_chunk(nrhs, rhs_cap(false));

@@ -208,7 +208,7 @@ class Fmm {
   void set_fold(int mode);
   bool folded() const { return fold_ok_ && fold_on_ > 0; }
   // Check-to-equivalent products: 1 tensor cores (where 3P <= 512), 0 FP64
-  // SIMT; the mode in use.
+  // SIMT, -1 the faster as timed by autotune; the form in use (0 or 1).
   void set_c2e_mode(int mode);
   int c2e_mode() const { return tc_c2e() ? 1 : 0; }
   // host wall time of the set-up steps (NNK_SETUP_*), milliseconds
@@ -301,8 +301,13 @@ class Fmm {
   // check-to-equivalent products on the tensor cores (int8 digits, FP64
   // accuracy; c2e_tc.h) or on the FP64 SIMT units
   C2ETcPlan c2e_tc_;
-  int c2e_mode_ = 0;        // 1 tensor cores where available, 0 SIMT (the default: faster here)
-  bool tc_c2e() const { return c2e_mode_ == 1 && c2e_tc_.ready; }
+  // 1 tensor cores where available, 0 SIMT, -1 (the default) the faster of
+  // the two as timed by autotune (SIMT until then)
+  int c2e_mode_ = -1;
+  bool tc_auto_ = false;
+  bool tc_c2e() const { return (c2e_mode_ < 0 ? tc_auto_ : c2e_mode_ == 1) && c2e_tc_.ready; }
+  void tune_c2e(int R);
+  std::pair<double, double> autotune_tiles(int nrhs);
   void build_tc_digits();
   void reserve_tc_scratch();
   template <typename Real>

@@ -116,9 +116,9 @@ class KIFMM:
         L.check(L.lib.nnk_fmm_set_fold(self.h, int(mode)), self.ctx.h, "setFold")
 
     def setC2E(self, mode=1):
-        """Check-to-equivalent products on the tensor cores (1, the default
-        where available: int8 digit products with FP64 accuracy) or as FP64
-        SIMT products (0)."""
+        """Check-to-equivalent products on the tensor cores (1: int8 digit
+        products with FP64 accuracy), as FP64 SIMT products (0), or (-1, the
+        default) the faster of the two as timed by autotune()."""
         L.check(L.lib.nnk_fmm_set_c2e(self.h, int(mode)), self.ctx.h, "setC2E")
 
     def c2eMode(self):

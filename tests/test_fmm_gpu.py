@@ -237,6 +237,14 @@ def test_tensor_core_c2e_matches_fp64_simt(name, precision):
     c = fmm.computeVel(g["F"])
     print(name, precision, "tensor-core C2E vs SIMT", rel(a, b), "vs oracle", rel(a, g["vel"]), rel(b, g["vel"]))
     assert np.array_equal(a, c)
+    # auto (-1): autotune keeps the faster form; the matvec is then that form's
+    # (compared after autotune, which may also change the pair-kernel tiles)
+    fmm.setC2E(-1)
+    fmm.autotune()
+    kept = fmm.c2eMode()
+    d = fmm.computeVel(g["F"])
+    fmm.setC2E(kept)
+    assert np.array_equal(d, fmm.computeVel(g["F"]))
     assert rel(a, b) <= C2E_TC_TOL[precision]
     if precision == "fp64":
         assert rel(a, g["vel"]) <= FP64_TOL[name]
