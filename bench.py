@@ -673,11 +673,11 @@ def time_arm(torch, nk, w, tree, precision, m2l, args, flush, clocks=None):
         e_ms.append(a.elapsed_time(b))
     out = {"fmm": fmm, "ms": ms, "prof": prof, "clocks": clk, "out": fout.cpu().numpy(), "e2e_ms": e_ms,
            "h2d": int(hin.numel() * 8), "d2h": int(hout.numel() * 8)}
-    out["c2e_mode"] = fmm.c2eMode()  # the form autotune kept (timed above)
+    out["c2e_mode"] = fmm.c2eMode()  # the form timed above
     if args.tc_c2e_check:
         # the same matvecs with each form of the check-to-equivalent products
         # forced: the tensor cores (int8 digits, exact int32 sums combined in
-        # FP64) and the FP64 SIMT units; then back to the autotuned choice
+        # FP64) and the FP64 SIMT units; then back to the form timed above
         c2e = lambda p: sum(p[k][0] for k in ("up_c2e", "down_c2e") if k in p) / max(args.steps, 1)
         forms = {}
         for mode, key in ((1, "tensor_cores"), (0, "simt")):
@@ -685,10 +685,9 @@ def time_arm(torch, nk, w, tree, precision, m2l, args, flush, clocks=None):
             ms_f, prof_f = time_device(torch, fmm, fin, fout, args.steps, args.warmup, flush, prof=True)
             forms[key] = {"ms_per_step": float(np.mean(ms_f)), "c2e_ms_per_step": c2e(prof_f),
                           "out": fout.cpu().numpy()}
-        fmm.setC2E(-1)
+        fmm.setC2E(out["c2e_mode"])
         a, b = forms["tensor_cores"].pop("out"), forms["simt"].pop("out")
         forms["rel_diff"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
-        forms["kept"] = "tensor_cores" if out["c2e_mode"] == 1 else "simt"
         out["tc_c2e"] = forms
     return out
 
@@ -741,7 +740,7 @@ def main():
         r["setup_ms"] = {k: round(v, 1) for k, v in r["fmm"].setup_times().items()}
         r["c2e_form"] = ("tensor cores: tcgen05 kind::i8 digit products, exact int32 sums combined in FP64 "
                          f"({'9 x 9' if prec != 'mixed' else '5 x 4'} digits)" if r["c2e_mode"] == 1
-                         else "FP64 SIMT") + " (the faster of the two as timed by autotune)"
+                         else "FP64 SIMT (the default; c2e_forms times both)")
         r["roofline"] = roofline(r["per_step"], r["stats"], "fp64" if prec == "near32" else prec, peaks,
                                  form_of[prec])
         del r["fmm"]  # one arm's device buffers at a time

@@ -267,12 +267,15 @@ int nnk_fmm_set_eps(nnk_fmm* fmm, double eps);
  * Up.m:31-33 and DownNonleaf.m:42-46): mode 1 on the tensor cores as int8
  * digit products with exact int32 sums combined in FP64 -- 9 x 9 digits for
  * FP64 check vectors, 5 x 4 for the mixed mode's FP32 ones, the FP64
- * product's accuracy either way (needs 3P <= 512) -- or mode 0 as FP64 SIMT
- * products; mode -1, the default, keeps whichever nnk_fmm_autotune times
- * faster on one matvec (the SIMT products until it runs).  On the workloads
- * measured the tensor cores win for the mixed mode's large trees and lose
- * for FP64 check vectors (45 digit products on N = 32 column tiles: tensor
- * memory holds one int32 accumulator per digit level).  nnk_fmm_c2e_mode
+ * product's accuracy either way (needs 3P <= 512) -- or mode 0, the default,
+ * as FP64 SIMT products; mode -1 keeps whichever nnk_fmm_autotune times
+ * faster on one matvec (the SIMT products until it runs).  Measured on the
+ * 250k matvec: the tensor cores win for the mixed mode's FP32 check vectors
+ * (0.90 against 1.31 ms a matvec) and lose for FP64 ones (1.97 against 1.12:
+ * 45 digit products on N = 32 column tiles, tensor memory holding one int32
+ * accumulator per digit level); in the mixed batched solves the 5 x 4 digit
+ * form (3.8e-6 from the SIMT product) raised the GMRES iterations of the
+ * refinement by a fifth, so solves keep the SIMT products.  nnk_fmm_c2e_mode
  * reports the form in use (0 or 1). */
 int nnk_fmm_set_c2e(nnk_fmm* fmm, int32_t mode);
 int nnk_fmm_c2e_mode(const nnk_fmm* fmm, int32_t* mode);

@@ -301,9 +301,9 @@ class Fmm {
   // check-to-equivalent products on the tensor cores (int8 digits, FP64
   // accuracy; c2e_tc.h) or on the FP64 SIMT units
   C2ETcPlan c2e_tc_;
-  // 1 tensor cores where available, 0 SIMT, -1 (the default) the faster of
+  // 1 tensor cores where available, 0 SIMT (the default), -1 the faster of
   // the two as timed by autotune (SIMT until then)
-  int c2e_mode_ = -1;
+  int c2e_mode_ = 0;
   bool tc_auto_ = false;
   bool tc_c2e() const { return (c2e_mode_ < 0 ? tc_auto_ : c2e_mode_ == 1) && c2e_tc_.ready; }
   void tune_c2e(int R);

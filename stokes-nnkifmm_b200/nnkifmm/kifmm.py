@@ -117,8 +117,8 @@ class KIFMM:
 
     def setC2E(self, mode=1):
         """Check-to-equivalent products on the tensor cores (1: int8 digit
-        products with FP64 accuracy), as FP64 SIMT products (0), or (-1, the
-        default) the faster of the two as timed by autotune()."""
+        products with FP64 accuracy), as FP64 SIMT products (0, the default),
+        or (-1) the faster of the two as timed by autotune()."""
         L.check(L.lib.nnk_fmm_set_c2e(self.h, int(mode)), self.ctx.h, "setC2E")
 
     def c2eMode(self):
