@@ -100,3 +100,55 @@ def test_int8_slice_product_keeps_the_fp64_accuracy(w):
     e = (e * 2.0 ** ea * 2.0 ** ec).ravel()
     e64 = err(A @ c.ravel())
     assert err(e) < 1.05 * e64
+
+
+def truncation_digits(X, k, axis):
+    """The digits of the tensor-core C2E (csrc/c2e_tc.cu): exponent e with
+    |x| / 2^e < 1 over the row (axis=1) or column (axis=0), then k digits by
+    truncation toward zero, so every digit is in [-127, 127] and every step is
+    exact in FP64."""
+    m = np.abs(X).max(axis=axis, keepdims=True)
+    e = np.where(m > 0, np.floor(np.log2(np.where(m > 0, m, 1.0))) + 1, 0.0)
+    r = X / 2.0 ** e
+    D = []
+    for _ in range(k):
+        r = r * 128.0
+        d = np.trunc(r)
+        r = r - d
+        D.append(d.astype(np.int64))
+    return D, e
+
+
+@pytest.mark.parametrize("w", [1 / 16, 1 / 64])
+def test_nine_digit_product_matches_fp64_on_the_exact_inverse(w):
+    """FP64 mode: the exact inverse (cond ~1e10) on a NEAREST-like check
+    (sources up to 0.3 widths outside the box), whose rows cancel by ~1e5.
+    9 x 9 digits, levels t + u < 9 (45 products, each level an exact int32
+    sum), against the product in extended precision: 5e-13, ten times closer
+    than the FP64 product itself (6e-12: its sums round, the digit sums do
+    not); 8 x 8 digits: 6e-11."""
+    rng = np.random.default_rng(1)
+    eps = 1e-3
+    lo = np.array([0.3, 0.4, 0.5])
+    box = np.concatenate([lo, lo + w])
+    us, ds = upsurf(box), downsurf(box)
+    A = np.linalg.inv(kernel(us, ds, eps, 1.0))
+    src = lo - 0.3 * w + 1.6 * w * rng.random((300, 3))
+    f = rng.standard_normal((300, 3))
+    c = apply_kernel(src, ds, f, eps, 1.0).reshape(-1, 1)
+    ref = (A.astype(np.longdouble) @ c.astype(np.longdouble)).astype(np.float64).ravel()
+    fp64 = np.linalg.norm((A @ c).ravel() - ref) / np.linalg.norm(ref)
+    errs = {}
+    for s_ in (8, 9):
+        DA, ea = truncation_digits(A, s_, 1)
+        DC, ec = truncation_digits(c, s_, 0)
+        lev = {}
+        for t in range(s_):
+            for u in range(s_ - t):
+                lev[t + u] = lev.get(t + u, 0) + DA[t] @ DC[u]
+        assert max(np.abs(v).max() for v in lev.values()) < 2 ** 31
+        out = sum(lev[l].astype(np.float64) * 2.0 ** (-7 * (l + 2)) for l in sorted(lev, reverse=True))
+        out = (out * 2.0 ** ea * 2.0 ** ec).ravel()
+        errs[s_] = np.linalg.norm(out - ref) / np.linalg.norm(ref)
+    assert errs[9] <= 2 * max(fp64, 1e-13)
+    assert errs[8] > errs[9]
