@@ -99,6 +99,12 @@ void device_errors(nnk::Fmm& F, int waited) {
   if (waited) F.check_errors();
   else F.poll_errors();
 }
+// The same for the FMMs of a forest batch (its matvec and, with FP64
+// refinement, the FP64 residual FMM).
+void batch_errors(nnk::BatchMobility& M, int waited) {
+  device_errors(M.fmm(), waited);
+  if (M.ref64()) device_errors(*M.ref64(), waited);
+}
 
 }  // namespace
 
@@ -764,6 +770,7 @@ int nnk_batch_apply(nnk_batch* batch, const double* x, double* y, int32_t on_dev
   double* dy = stage_out(batch->io_out, y, n, on_device);
   batch->m->apply(dx, dy);
   finish_out(ctx, batch->io_out, y, n, on_device);
+  batch_errors(*batch->m, !on_device);
   API_CATCH(ctx)
 }
 
@@ -780,6 +787,7 @@ int nnk_batch_solve(nnk_batch* batch, const double* rhs, double* x, const nnk_so
   std::vector<nnk_solve_info> inf(M.systems());
   M.solve(db, dx, *sp, inf.data());
   finish_out(ctx, batch->io_out, x, n, on_device);
+  batch_errors(M, 1);
   if (info) std::copy(inf.begin(), inf.end(), info);
   for (const auto& i : inf)
     if (i.flag != 0) return fail(ctx, NNK_E_NOCONV, "gmres stopped at maxit above tol for some system");

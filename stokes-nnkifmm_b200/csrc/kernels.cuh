@@ -106,6 +106,27 @@ inline void launch_gather(int64_t E, const int64_t* goff, const int32_t* gidx, c
 // sources, then reduce through shared memory.
 //   u(t) = 1/(8 pi mu) sum_s [ (r^2 + 2 eps^2) f_s + (r.f_s) r ] / (r^2+eps^2)^{3/2},
 //   r = t - s (Tools/kernel.m:23-47).
+// Inclusive prefix sums of one int per thread over a block of BS threads (BS
+// a multiple of 32): within each warp by shuffles, then the warps' totals
+// through wsum (BS / 32 ints), with one barrier.  Every thread of the block
+// calls it; wsum is read until the caller's next barrier.
+template <int BS>
+__device__ __forceinline__ int block_inclusive_scan(int v, int* wsum) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += u;
+  }
+  if (lane == 31) wsum[warp] = v;
+  __syncthreads();
+  int add = 0;
+#pragma unroll
+  for (int w = 0; w < BS / 32; ++w)
+    if (w < warp) add += wsum[w];
+  return v + add;
+}
+
 template <typename Real> struct Vec4T;
 template <> struct Vec4T<float> { using t4 = float4; using t2 = float2; };
 template <> struct Vec4T<double> { using t4 = double4; using t2 = double2; };
@@ -146,10 +167,11 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
                                                  int accumulate_main, const int* __restrict__ nact = nullptr) {
   using T4 = typename Vec4T<Real>::t4;
   using T2 = typename Vec4T<Real>::t2;
-  __shared__ T4 s4[BS];
-  __shared__ T2 s2[BS];
+  __shared__ T4 s4[2][BS];  // source tiles, double-buffered: one barrier a tile
+  __shared__ T2 s2[2][BS];
   __shared__ long long seg_start[BS];
   __shared__ int seg_end[BS];  // inclusive prefix sums of the counts
+  __shared__ int wsum[BS / 32];
   __shared__ Real red[3 * BS];
   const TaskD tk = tasks[blockIdx.x];
   if (nact && !nact[tk.node]) return;  // a tree of the forest whose systems all converged
@@ -179,14 +201,8 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
         seg_start[tid] = sg.start;
         cnt = sg.count;
       }
-      seg_end[tid] = cnt;
+      seg_end[tid] = block_inclusive_scan<BS>(cnt, wsum);
       __syncthreads();
-      for (int o = 1; o < BS; o <<= 1) {  // inclusive scan
-        const int v = tid >= o ? seg_end[tid - o] : 0;
-        __syncthreads();
-        seg_end[tid] += v;
-        __syncthreads();
-      }
       const int total = seg_end[nsb - 1];
       // software pipeline: the next tile's source is fetched into registers
       // while the current tile is computed from shared memory
@@ -210,13 +226,19 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
       T4 pa;
       T2 pb;
       if (tid < total) fetch(tid, pa, pb);
-      for (int f0 = 0; f0 < total; f0 += BS) {
+      int buf = 0;
+      // a tile is written to one buffer while the previous one is read from
+      // the other; a thread writes a buffer again only after the next
+      // barrier, which every thread reaches after reading it
+      for (int f0 = 0; f0 < total; f0 += BS, buf ^= 1) {
         if (f0 + tid < total) {
-          s4[tid] = pa;
-          s2[tid] = pb;
+          s4[buf][tid] = pa;
+          s2[buf][tid] = pb;
         }
         __syncthreads();
         if (f0 + BS + tid < total) fetch(f0 + BS + tid, pa, pb);
+        const T4* __restrict__ S4 = s4[buf];
+        const T2* __restrict__ S2 = s2[buf];
         const int nj = min(BS, total - f0);
         if (act0) {
           if constexpr (std::is_same<Real, float>::value && !KD) {
@@ -226,8 +248,8 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
             float2 cx = make_float2(ax, bx), cy = make_float2(ay, by), cz = make_float2(az, bz);
 #pragma unroll 4
             for (int j = ms; j < nj; j += splits) {
-              const float4 a = s4[j];
-              const float2 b = s2[j];
+              const float4 a = S4[j];
+              const float2 b = S2[j];
               const float2 dx = __fadd2_rn(X, make_float2(-a.x, -a.x));
               const float2 dy = __fadd2_rn(Y, make_float2(-a.y, -a.y));
               const float2 dz = __fadd2_rn(Z, make_float2(-a.z, -a.z));
@@ -255,14 +277,13 @@ __global__ void __launch_bounds__(BS) p2p_kernel(const TaskD* __restrict__ tasks
           } else {
 #pragma unroll 4
             for (int j = ms; j < nj; j += splits) {
-              const T4 a = s4[j];
-              const T2 b = s2[j];
+              const T4 a = S4[j];
+              const T2 b = S2[j];
               pair_acc<Real, KD>(tx, ty, tz, a, b, e2, ax, ay, az);
               pair_acc<Real, KD>(ux, uy, uz, a, b, e2, bx, by, bz);  // dummy target (0,0,0) when !act1
             }
           }
         }
-        __syncthreads();
       }
     }
     __shared__ Real red2[3 * BS];
@@ -325,6 +346,7 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
   constexpr bool kPacked = std::is_same<Real, float>::value && R % 2 == 0 && !GRAD;
   __shared__ long long seg_start[BS];
   __shared__ int seg_end[BS];
+  __shared__ int wsum[BS / 32];
   __shared__ Real red[C][BS];
   const TaskD tk = tasks[blockIdx.x];
   if (nact && !nact[tk.node]) return;
@@ -359,14 +381,8 @@ __global__ void __launch_bounds__(BS) p2p_multi_kernel(const TaskD* __restrict__
         seg_start[tid] = sg.start;
         cnt = sg.count;
       }
-      seg_end[tid] = cnt;
+      seg_end[tid] = block_inclusive_scan<BS>(cnt, wsum);
       __syncthreads();
-      for (int o = 1; o < BS; o <<= 1) {  // inclusive scan
-        const int v = tid >= o ? seg_end[tid - o] : 0;
-        __syncthreads();
-        seg_end[tid] += v;
-        __syncthreads();
-      }
       const int total = seg_end[nsb - 1];
       auto fetch = [&](int f, T4& a, Real* b) {
         int lo = 0, hi = nsb - 1;

@@ -279,17 +279,55 @@ __host__ __device__ constexpr uint64_t group_mask(int dl) {
   return gm;
 }
 
+// The pairs of one difference (ex, ey, ez) of a (P, N) record: child a of P
+// takes child b = a + (ex, ey, ez) of N through the kernel spectrum K (xx, xy,
+// xz, yy, yz, zz) when its bit 8 a + b is set; my[(b * 3 + c) * BLK] holds
+// N's child spectra.
+template <int BLK, typename T2>
+__device__ __forceinline__ void family_group(T2 (&acc)[8][3], const T2 (&K)[6], const T2* my, int ex, int ey,
+                                             int ez, uint64_t bits) {
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
+    if (!(bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)) continue;
+    const int b = bx * 4 + by * 2 + bz;
+    if (!((bits >> (a * 8 + b)) & 1)) continue;
+    const T2 qx = my[(b * 3) * BLK], qy = my[(b * 3 + 1) * BLK], qz = my[(b * 3 + 2) * BLK];
+    cmac(acc[a][0], K[0], qx);
+    cmac(acc[a][0], K[1], qy);
+    cmac(acc[a][0], K[2], qz);
+    cmac(acc[a][1], K[1], qx);
+    cmac(acc[a][1], K[3], qy);
+    cmac(acc[a][1], K[4], qz);
+    cmac(acc[a][2], K[2], qx);
+    cmac(acc[a][2], K[4], qy);
+    cmac(acc[a][2], K[5], qz);
+  }
+}
+
+constexpr int kFamBlk = 128;  // frequencies per block of the direct-load form
+template <typename Real>
+size_t family_smem() {
+  return sizeof(typename Cplx<Real>::t) * 24 * kFamBlk + sizeof(int) * 343;
+}
+
 // Parent-grouped accumulation (see FftFamily): thread (family, frequency k)
 // holds the 8 children's accumulators of one right-hand side at a time; per
 // (P, N) record the 8 source spectra go to this thread's own shared-memory
 // slots, then for each of the 27 values of pos_v - pos_i present in the
 // record the kernel spectrum of offset 2 d + delta is loaded once and applied
-// to every pair with that difference.  Loop bounds and child positions are
-// compile-time, so accumulators stay in registers (loading the next
-// difference's spectrum one step ahead costs 42 more registers, 2 blocks per
-// SM instead of 3, and ran 45% slower).  Every right-hand side
-// sums its pairs in the same order, so a pass of R right-hand sides gives
-// each of them bitwise the result of a pass of one.
+// to every pair with that difference (the spectrum slots of the family's
+// operator, one per offset code, are read into shared memory once, so a
+// spectrum's address needs no global load).  Loop bounds and child positions
+// are compile-time, so accumulators stay in registers.  The kernel is bound
+// by moving kernel spectra from L2 (96 bytes a frequency per difference, for
+// 2.5 pairs on average): hiding their latency did not pay -- loading the
+// next difference's spectrum one step ahead into registers (42 more
+// registers, 2 blocks per SM instead of 3) ran 45% slower, an L1 prefetch of
+// it 32% slower, a producer warp staging spectra in a 5-stage shared-memory
+// ring with bulk copies 27% slower.  Every right-hand side sums its pairs in
+// the same order, so a pass of R right-hand sides gives each of them bitwise
+// the result of a pass of one.
 template <typename Real>
 __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
     int NK, const FftFamily* __restrict__ fams, const FftFamilyPair* __restrict__ pairs,
@@ -297,8 +335,10 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
     const typename Cplx<Real>::t* __restrict__ qhat, typename Cplx<Real>::t* __restrict__ chat,
     const int* __restrict__ tgt_node, const int* __restrict__ nact, int R) {
   using T2 = typename Cplx<Real>::t;
-  constexpr int BLK = 128;
-  __shared__ T2 sq[24 * BLK];  // this thread's source spectra: [pos * 3 + c][thread]
+  constexpr int BLK = kFamBlk;
+  extern __shared__ __align__(16) unsigned char fam_direct_smem[];
+  T2* sq = reinterpret_cast<T2*>(fam_direct_smem);  // this thread's source spectra: [pos * 3 + c][thread]
+  int* so = reinterpret_cast<int*>(sq + 24 * BLK);   // spectrum slot of each offset code (the family's operator)
   const FftFamily fam = fams[blockIdx.x];
   const int k = blockIdx.y * BLK + threadIdx.x;
   if (nact) {
@@ -306,6 +346,8 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
     while (t0 < 7 && fam.tgt[t0] < 0) ++t0;
     if (!nact[tgt_node[fam.tgt[t0]]]) return;
   }
+  for (int c = threadIdx.x; c < 343; c += BLK) so[c] = spec_of[(size_t)fam.op * 343 + c];
+  __syncthreads();
   if (k >= NK) return;
   const int C = 3 * R;
   T2* my = sq + threadIdx.x;
@@ -328,7 +370,6 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
       }
     }
     const int dx2 = 2 * (rec.dcode / 9 - 1), dy2 = 2 * ((rec.dcode / 3) % 3 - 1), dz2 = 2 * (rec.dcode % 3 - 1);
-    const int* so = spec_of + (size_t)rec.op * 343;
 #pragma unroll
     for (int dl = 0; dl < 27; ++dl) {
       const int ex = dl / 9 - 1, ey = (dl / 3) % 3 - 1, ez = dl % 3 - 1;
@@ -336,24 +377,8 @@ __global__ void __launch_bounds__(128) fft_accumulate_family_kernel(
       if (bits == 0) continue;
       const int code = (dx2 + ex + 3) * 49 + (dy2 + ey + 3) * 7 + (dz2 + ez + 3);
       const T2* Kp = spec + (size_t)so[code] * 6 * NK + k;
-      const T2 kxx = Kp[0], kxy = Kp[NK], kxz = Kp[2 * NK], kyy = Kp[3 * NK], kyz = Kp[4 * NK], kzz = Kp[5 * NK];
-#pragma unroll
-      for (int a = 0; a < 8; ++a) {
-        const int bx = (a >> 2) + ex, by = ((a >> 1) & 1) + ey, bz = (a & 1) + ez;
-        if (!(bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1)) continue;
-        const int b = bx * 4 + by * 2 + bz;
-        if (!((bits >> (a * 8 + b)) & 1)) continue;
-        const T2 qx = my[(b * 3) * BLK], qy = my[(b * 3 + 1) * BLK], qz = my[(b * 3 + 2) * BLK];
-        cmac(acc[a][0], kxx, qx);
-        cmac(acc[a][0], kxy, qy);
-        cmac(acc[a][0], kxz, qz);
-        cmac(acc[a][1], kxy, qx);
-        cmac(acc[a][1], kyy, qy);
-        cmac(acc[a][1], kyz, qz);
-        cmac(acc[a][2], kxz, qx);
-        cmac(acc[a][2], kyz, qy);
-        cmac(acc[a][2], kzz, qz);
-      }
+      const T2 K[6] = {Kp[0], Kp[NK], Kp[2 * NK], Kp[3 * NK], Kp[4 * NK], Kp[5 * NK]};
+      family_group<BLK>(acc, K, my, ex, ey, ez, bits);
     }
   }
 #pragma unroll
@@ -526,9 +551,10 @@ void build_families(const HostTree& t, const std::vector<int>& tgt, const std::v
   std::vector<FftFamilyPair> pairs;
   for (size_t fi = 0; fi < fams.size(); ++fi) {
     fams[fi].first = (int)pairs.size();
+    fams[fi].op = recs[fi].empty() ? 0 : recs[fi].begin()->second.op;
     for (auto& kv : recs[fi]) {
       // the accumulation reads one row of spec_of per family
-      if (kv.second.op != recs[fi].begin()->second.op) return;
+      if (kv.second.op != fams[fi].op) return;
       pairs.push_back(kv.second);
     }
     fams[fi].count = (int)pairs.size() - fams[fi].first;
@@ -560,6 +586,8 @@ void set_smem_attributes(int optin) {
   NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<4, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   NNK_CUDA(cudaFuncSetAttribute(fft_forward_kernel<6, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   NNK_CUDA(cudaFuncSetAttribute(fft_inverse_kernel<6, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  NNK_CUDA(cudaFuncSetAttribute(fft_accumulate_family_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)family_smem<Real>()));
 }
 
 template <typename Real>
@@ -578,8 +606,9 @@ void run_fft_m2l(FftM2L& f, const Real* str, long long upbase, int R, Real* chec
                                                         f.NK, nact);
   NNK_CHECK_LAUNCH();
   if (f.family) {
-    fft_accumulate_family_kernel<Real><<<dim3(f.nfam, (f.NK + 127) / 128), 128, 0, st>>>(
-        f.NK, f.fams.p, f.fpairs.p, f.spec_of.p, spec, qhat, chat, f.tgt_node.p, nact, R);
+    fft_accumulate_family_kernel<Real><<<dim3(f.nfam, (f.NK + kFamBlk - 1) / kFamBlk), kFamBlk, family_smem<Real>(),
+                                         st>>>(f.NK, f.fams.p, f.fpairs.p, f.spec_of.p, spec, qhat, chat,
+                                               f.tgt_node.p, nact, R);
     NNK_CHECK_LAUNCH();
     inv<<<f.ntgt, 256, inverse_smem(G, res, R, es), st>>>(G, res, f.P, f.lat.p, f.tgt_node.p, chat, R, check, f.NK,
                                                           nact);

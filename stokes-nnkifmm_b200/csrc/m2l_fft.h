@@ -39,6 +39,7 @@ __host__ __device__ constexpr int fft_grid(int res) { return 2 * res - 1; }
 // source spectrum every child of P.
 struct FftFamily {
   int first, count;  // its (P, N) records
+  int op;            // operator (box width) of the children's level
   int tgt[8];        // target slot of the child at each position (-1 none)
 };
 struct FftFamilyPair {
