@@ -325,7 +325,9 @@ size_t family_smem() {
 // next difference's spectrum one step ahead into registers (42 more
 // registers, 2 blocks per SM instead of 3) ran 45% slower, an L1 prefetch of
 // it 32% slower, a producer warp staging spectra in a 5-stage shared-memory
-// ring with bulk copies 27% slower.  Every right-hand side sums its pairs in
+// ring 27% slower with bulk copies and 36% slower with 16-byte cp.async
+// (the ring and the source slots leave 8 arithmetic warps per SM, whose
+// per-record source loads stay exposed).  Every right-hand side sums its pairs in
 // the same order, so a pass of R right-hand sides gives each of them bitwise
 // the result of a pass of one.
 template <typename Real>
