@@ -429,7 +429,11 @@ int nnk_batch_apply(nnk_batch* batch, const double* x, double* y, int32_t on_dev
 /* Unpreconditioned gmres per system (own Krylov space and stopping test,
  * MATLAB semantics as nnk_mob_solve), all systems advancing together;
  * info receives one record per system (may be NULL).  Returns NNK_E_NOCONV
- * if any system stopped above tol. */
+ * if any system stopped above tol.  Like the single-FMM calls, a batch apply
+ * or solve returns NNK_E_TIMEOUT when a bounded device wait of one of its
+ * FMMs (the forest's, or the FP64 refinement FMM's) gave up (an apply with
+ * on_device = 1 reads the flags whose copies have completed; a later call
+ * reports the rest). */
 int nnk_batch_solve(nnk_batch* batch, const double* rhs, double* x,
                     const nnk_solve_params* sp, nnk_solve_info* info, int32_t on_device);
 /* Mixed-precision iterative refinement for a MIXED batch: fp64 != 0 builds an
