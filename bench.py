@@ -560,12 +560,14 @@ def throughputs(ws, n_force, n_quad, stats, step_ms):
             "near_pairs_per_s": ws * stats["pairs_p2p"] / sec}
 
 
-def roofline(per_step, stats, precision, peaks, m2l_form):
+def roofline(per_step, stats, precision, peaks, m2l_form, l2_gbs=None):
     """Roofline of the dominant phase of one matvec, from the live per-phase
     CUDA-event times (per_step: phase -> (ms, launches) per step) and the
     algorithmic work of the tree statistics; `pair_kernels` adds the same for
     all pair phases together (S2M/M2M/L2L/L2T, P2L/M2T and the near field).
-    m2l_form: 'tensor' (compressed tcgen05 M2L), 'fourier' or 'pairs'."""
+    m2l_form: 'tensor' (compressed tcgen05 M2L), 'fourier' or 'pairs';
+    l2_gbs: the device's measured L2 read bandwidth (the parent-grouped
+    Fourier accumulation's second roofline)."""
     dom = max((k for k in per_step if per_step[k][1] > 0), key=lambda k: per_step[k][0])
     fp64 = precision == "fp64"
     simt_peak = FP32_NOMINAL_TFLOPS / (2 if fp64 else 1)
@@ -615,6 +617,22 @@ def roofline(per_step, stats, precision, peaks, m2l_form):
             roof["traffic"] = FAMILY_FP64_60K_BYTES * stats["m2l_pairs"] / FAMILY_FP64_60K_PAIRS
             roof["traffic_source"] = ("dram__bytes_read.sum + dram__bytes_write.sum of the 60k capture (one "
                                       "launch), scaled by V pairs (profiles/fft_accumulate_family_60k.md)")
+        if stats.get("m2l_family") and l2_gbs:
+            # the parent-grouped accumulation reads one kernel spectrum (6 complex values a
+            # frequency) per (record, child difference) group and 8 children's source
+            # spectra (3 complex values each) per record, all from L2
+            cb = 16 if fp64 else 8
+            kb = stats["m2l_groups"] * 6 * cb * nk_freq
+            sb = stats["m2l_records"] * 24 * cb * nk_freq
+            achieved = (kb + sb) / (ms_l / 1e3) / 1e9
+            roof["l2"] = {"bound": "l2", "achieved": achieved, "peak": l2_gbs, "unit": "GB/s",
+                          "frac": achieved / l2_gbs, "bytes_per_launch": kb + sb,
+                          "algorithmic": f"{stats['m2l_groups']} (record, difference) groups x 6 x {nk_freq} "
+                                         f"complex kernel-spectrum values + {stats['m2l_records']} records x 24 x "
+                                         f"{nk_freq} complex source-spectrum values, read per launch; over the M2L "
+                                         f"phase time (the transforms included)",
+                          "peak_source": "nnk_measure_l2_read in this run: streaming read of an L2-resident "
+                                         "buffer on this GPU"}
     elif dom in pairs:
         flops = pairs[dom] * FLOPS_PER_PAIR
         roof = {"kernel": f"p2p_kernel ({dom})", "bound": "fp64" if fp64 else "fp32",
@@ -720,6 +738,7 @@ def main():
         tree_s["gpu" if builder == "auto" else "host"] = round(time.time() - t0, 3)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
+    l2_gbs = nk.context(local).measure_l2_read()  # the L2 roofline's denominator, on this GPU
     m2l_of = {"fp64": "pairs" if args.m2l == "pairs" else "auto", "near32": "auto", "mixed": args.m2l}
     form_of = {"fp64": "pairs" if args.m2l == "pairs" else "fourier", "near32": "fourier",
                "mixed": {"auto": "tensor", "images": "tensor", "generate": "tensor", "pairs": "pairs",
@@ -742,7 +761,7 @@ def main():
                          f"({'9 x 9' if prec != 'mixed' else '5 x 4'} digits)" if r["c2e_mode"] == 1
                          else "FP64 SIMT (the default; c2e_forms times both)")
         r["roofline"] = roofline(r["per_step"], r["stats"], "fp64" if prec == "near32" else prec, peaks,
-                                 form_of[prec])
+                                 form_of[prec], l2_gbs)
         del r["fmm"]  # one arm's device buffers at a time
         res[prec] = r
     H = res[head]

@@ -129,6 +129,15 @@ typedef struct nnk_fmm_stats {
                            bases (its GEMMs are m2l_rank square); 0 otherwise */
   int32_t folded;       /* 1: the matvec runs M2M and L2L folded into the
                            check-to-equivalent products (nnk_fmm_set_fold)  */
+  int32_t m2l_frequencies; /* Fourier-space M2L: frequencies of the half
+                              spectrum (0 without it)                       */
+  int32_t m2l_family;   /* 1: its parent-grouped accumulation is used         */
+  int64_t m2l_records;  /* parent-grouped: (parent, colleague) records; each
+                           reads its colleague's 8 children's source spectra
+                           (3 complex values a frequency each)              */
+  int64_t m2l_groups;   /* parent-grouped: (record, child difference) groups;
+                           each reads one kernel spectrum (6 complex values a
+                           frequency) for all its V pairs                   */
 } nnk_fmm_stats;
 
 /* GMRES options/result (MATLAB gmres(A,b,restart,tol,maxit), x0 = 0). */
@@ -294,6 +303,12 @@ int nnk_fmm_c2e_mode(const nnk_fmm* fmm, int32_t* mode);
  * tensor-core M2L and at most 1 GiB of folded operators; the transpose, the
  * gradients and the eps-derivative always run unfolded. */
 int nnk_fmm_set_fold(nnk_fmm* fmm, int32_t mode);
+/* No counterpart in the reference: the device's L2 read bandwidth in GB/s,
+ * measured on the context's stream with a streaming read of an L2-resident
+ * buffer (16-byte loads from 8 and 16 blocks of 256 threads per SM over 24
+ * and 48 MiB; the best of the four), the denominator of the L2 roofline of
+ * the Fourier-space M2L accumulation.  Allocates and frees 48 MiB. */
+int nnk_measure_l2_read(nnk_ctx* ctx, double* gbs);
 /* Host wall time (milliseconds) of the set-up steps of nnk_fmm_create, in
  * the order of the NNK_SETUP_* indices: the unified point array and its
  * surfaces, the pair task lists, the M2L plan (Fourier-space spectra and

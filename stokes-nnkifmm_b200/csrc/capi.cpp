@@ -11,6 +11,7 @@
 #include "../../include/nnkifmm.h"
 #include "common.h"
 #include "fmm.h"
+#include "probe.h"
 #include "gmres.h"
 #include "batch.h"
 #include "mobility.h"
@@ -433,6 +434,14 @@ int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats) {
   *stats = fmm->f->stats();
   stats->folded = fmm->f->folded() ? 1 : 0;
   return NNK_OK;
+}
+
+int nnk_measure_l2_read(nnk_ctx* ctx, double* gbs) {
+  if (!ctx || !gbs) return NNK_E_ARG;
+  API_TRY
+  need_gpu(ctx);
+  *gbs = nnk::measure_l2_read_gbs(ctx->stream);
+  API_CATCH(ctx)
 }
 
 int nnk_fmm_setup_times(const nnk_fmm* fmm, double* ms, int32_t n) {

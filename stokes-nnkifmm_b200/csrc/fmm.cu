@@ -959,6 +959,10 @@ void Fmm::build_operators() {
     build_fft_m2l(t, p_.res, p_.shells, p_.eps, p_.mu, op_w_, node_op, std::min(R_, std::max(fft_cap, 1)), fp64,
                   fft_, ctx_->stream);
     fft_m2l_ = true;
+    stats_.m2l_frequencies = fft_.NK;
+    stats_.m2l_family = fft_.family ? 1 : 0;
+    stats_.m2l_records = fft_.family ? fft_.records : 0;
+    stats_.m2l_groups = fft_.family ? fft_.groups : 0;
   }
   if (p_.precision == NNK_PREC_MIXED && p_.m2l_mode != 3 && p_.m2l_mode != 4) {
     if (p_.m2l_mode == 1) m2l_.image_budget = ~(size_t)0;

@@ -561,6 +561,12 @@ void build_families(const HostTree& t, const std::vector<int>& tgt, const std::v
     }
     fams[fi].count = (int)pairs.size() - fams[fi].first;
   }
+  f.records = (int64_t)pairs.size();
+  f.groups = 0;
+  for (const FftFamilyPair& r : pairs) {
+    const uint64_t mask = (uint64_t)r.mask_lo | ((uint64_t)r.mask_hi << 32);
+    for (int dl = 0; dl < 27; ++dl) f.groups += (mask & group_mask(dl)) != 0;
+  }
   std::vector<int> spec_of(std::max<size_t>(nops, 1) * 343, -1);
   for (const auto& kv : spec_slot) spec_of[(size_t)(kv.first / 343) * 343 + (size_t)(kv.first % 343)] = kv.second;
   f.fams.upload(fams, st);

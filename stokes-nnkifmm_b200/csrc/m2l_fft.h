@@ -73,6 +73,7 @@ struct FftM2L {
   DBuf<FftFamily> fams;
   DBuf<FftFamilyPair> fpairs;
   DBuf<int> spec_of;  // per (operator, offset code): spectrum slot (-1 unused)
+  int64_t records = 0, groups = 0;  // (P, N) records; (record, difference) groups
   size_t fwd_smem = 0, inv_smem = 0;
 };
 

@@ -58,6 +58,24 @@ def test_fourier_m2l_dominant_phase_fp64():
     assert r["achieved"] == pytest.approx(72.0 * 726 * STATS["m2l_pairs"] / 6e-3 / 1e12)
     assert r["peak"] == pytest.approx(bench.FP32_NOMINAL_TFLOPS / 2)
     assert r["ms_per_launch"] == pytest.approx(2.0)
+    assert "l2" not in r  # no parent-grouped statistics, no L2 roofline
+
+
+def test_fourier_m2l_l2_roofline():
+    """The parent-grouped accumulation's L2 roofline: per launch one kernel
+    spectrum (6 complex FP64 values a frequency) per (record, difference)
+    group and 8 x 3 source spectra per record, over the launch time, against
+    the measured L2 read rate."""
+    stats = dict(STATS, m2l_family=1, m2l_groups=570_000, m2l_records=25_000, m2l_frequencies=726)
+    r = bench.roofline(dict(PHASES, m2l=(6.0, 1)), stats, "fp64", PEAKS, "fourier", l2_gbs=12000.0)
+    l2 = r["l2"]
+    nbytes = (570_000 * 6 + 25_000 * 24) * 16 * 726
+    assert l2["bytes_per_launch"] == nbytes and l2["unit"] == "GB/s" and l2["peak"] == 12000.0
+    assert l2["achieved"] == pytest.approx(nbytes / 6e-3 / 1e9)
+    assert l2["frac"] == pytest.approx(l2["achieved"] / 12000.0)
+    # FP32 spectra: 8-byte complex values
+    r32 = bench.roofline(dict(PHASES, m2l=(6.0, 1)), stats, "mixed", PEAKS, "fourier", l2_gbs=12000.0)
+    assert r32["l2"]["bytes_per_launch"] == nbytes // 2
 
 
 def test_reference_arm_does_not_load_the_library():

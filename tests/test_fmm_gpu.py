@@ -347,3 +347,40 @@ def test_fmm_after_its_context_handle_is_destroyed():
     assert np.array_equal(out, ref.computeVel(f).ravel())
     assert L.lib.nnk_fmm_destroy(fmm) == L.NNK_OK
     assert L.lib.nnk_tree_destroy(tree) == L.NNK_OK
+
+
+@pytest.mark.parametrize("name", ["adaptive_nearest_1200", "matvec_4000_16000"])
+def test_fourier_m2l_family_statistics(name):
+    """The parent-grouped Fourier M2L's record and group counts (the L2
+    traffic of its accumulation) against a count from the exported tree: a
+    record per (parent of a V-list target, parent of its V-list source), a
+    group per record and child difference (pos_v - pos_i, both child positions
+    in their parents)."""
+    g = load(name)
+    t = tree_of(g)
+    st = nk.KIFMM(t, [float(g["eps"]), float(g["mu"])]).stats()
+    par = np.asarray(t.nodeParents).ravel().astype(np.int64) - 1  # 1-based ids, 0 = none
+    cor = np.asarray(t.nodeCorners)
+    root = int(np.where(par < 0)[0][0])
+    wid = cor[:, 3] - cor[:, 0]
+    ijk = np.rint((cor[:, :3] - cor[root, :3]) / wid[:, None]).astype(np.int64)
+    off, ids = t.interaction_list(1)
+    ids = ids.astype(np.int64) - 1
+    records, groups = set(), set()
+    for i in range(len(par)):
+        for v in ids[off[i]:off[i + 1]]:
+            P, N = int(par[i]), int(par[v])
+            e = tuple(int(x) for x in (ijk[v] - 2 * ijk[N]) - (ijk[i] - 2 * ijk[P]))
+            records.add((P, N))
+            groups.add((P, N, e))
+    assert st["m2l_family"] == 1 and st["m2l_frequencies"] == 11 * 11 * 6
+    assert st["m2l_records"] == len(records) and st["m2l_groups"] == len(groups)
+    assert st["m2l_pairs"] == int(off[-1])
+
+
+def test_measure_l2_read():
+    """The L2 read rate used as the Fourier accumulation's second roofline:
+    a streaming read of an L2-resident buffer runs well above the HBM rate."""
+    gbs = nk.context(0).measure_l2_read()
+    print("L2 read", gbs, "GB/s")
+    assert 8000.0 < gbs < 40000.0
