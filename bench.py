@@ -695,10 +695,11 @@ def time_arm(torch, nk, w, tree, precision, m2l, args, flush, clocks=None):
     if args.tc_c2e_check:
         # the same matvecs with each form of the check-to-equivalent products
         # forced: the tensor cores (int8 digits, exact int32 sums combined in
-        # FP64) and the FP64 SIMT units; then back to the form timed above
+        # FP64), one cuBLAS DGEMM per run of nodes sharing an operator, and
+        # the FP64 SIMT units; then back to the form timed above
         c2e = lambda p: sum(p[k][0] for k in ("up_c2e", "down_c2e") if k in p) / max(args.steps, 1)
         forms = {}
-        for mode, key in ((1, "tensor_cores"), (0, "simt")):
+        for mode, key in ((1, "tensor_cores"), (2, "cublas_dgemm"), (0, "simt")):
             fmm.setC2E(mode)
             ms_f, prof_f = time_device(torch, fmm, fin, fout, args.steps, args.warmup, flush, prof=True)
             forms[key] = {"ms_per_step": float(np.mean(ms_f)), "c2e_ms_per_step": c2e(prof_f),
@@ -706,6 +707,8 @@ def time_arm(torch, nk, w, tree, precision, m2l, args, flush, clocks=None):
         fmm.setC2E(out["c2e_mode"])
         a, b = forms["tensor_cores"].pop("out"), forms["simt"].pop("out")
         forms["rel_diff"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        c = forms["cublas_dgemm"].pop("out")
+        forms["rel_diff_cublas"] = float(np.linalg.norm(c - b) / np.linalg.norm(b))
         out["tc_c2e"] = forms
     return out
 
@@ -757,9 +760,11 @@ def main():
         r["per_step"] = {kk: (v[0] / args.steps, v[1] / args.steps) for kk, v in r["prof"].items()}
         r["stats"] = r["fmm"].stats()
         r["setup_ms"] = {k: round(v, 1) for k, v in r["fmm"].setup_times().items()}
-        r["c2e_form"] = ("tensor cores: tcgen05 kind::i8 digit products, exact int32 sums combined in FP64 "
-                         f"({'9 x 9' if prec != 'mixed' else '5 x 4'} digits)" if r["c2e_mode"] == 1
-                         else "FP64 SIMT (the default; c2e_forms times both)")
+        r["c2e_form"] = {1: "tensor cores: tcgen05 kind::i8 digit products, exact int32 sums combined in FP64 "
+                            f"({'9 x 9' if prec != 'mixed' else '5 x 4'} digits)",
+                         2: "one cuBLAS DGEMM per run of nodes sharing an operator on gathered check vectors "
+                            "(the default; c2e_forms times every form)",
+                         0: "FP64 SIMT product kernel"}[r["c2e_mode"]]
         r["roofline"] = roofline(r["per_step"], r["stats"], "fp64" if prec == "near32" else prec, peaks,
                                  form_of[prec], l2_gbs)
         del r["fmm"]  # one arm's device buffers at a time

@@ -273,19 +273,20 @@ int nnk_fmm_autotune(nnk_fmm* fmm, int32_t nrhs, double* ms_before, double* ms_a
  * the cheap way to evaluate the operator at eps +- d for its eps-derivative. */
 int nnk_fmm_set_eps(nnk_fmm* fmm, double eps);
 /* Check-to-equivalent products (the batched form of the LU solves of
- * Up.m:31-33 and DownNonleaf.m:42-46): mode 1 on the tensor cores as int8
- * digit products with exact int32 sums combined in FP64 -- 9 x 9 digits for
- * FP64 check vectors, 5 x 4 for the mixed mode's FP32 ones, the FP64
- * product's accuracy either way (needs 3P <= 512) -- or mode 0, the default,
- * as FP64 SIMT products; mode -1 keeps whichever nnk_fmm_autotune times
- * faster on one matvec (the SIMT products until it runs).  Measured on the
- * 250k matvec: the tensor cores win for the mixed mode's FP32 check vectors
- * (0.90 against 1.31 ms a matvec) and lose for FP64 ones (1.97 against 1.12:
- * 45 digit products on N = 32 column tiles, tensor memory holding one int32
- * accumulator per digit level); in the mixed batched solves the 5 x 4 digit
- * form (3.8e-6 from the SIMT product) raised the GMRES iterations of the
- * refinement by a fifth, so solves keep the SIMT products.  nnk_fmm_c2e_mode
- * reports the form in use (0 or 1). */
+ * Up.m:31-33 and DownNonleaf.m:42-46).  Mode 2, the default: per run of
+ * nodes of one level sharing an operator, their check vectors gathered into
+ * one matrix, one cuBLAS DGEMM with the FP64 operator, the products
+ * scattered back (single-tree FMMs; forests, and a matvec being captured
+ * into a CUDA graph, use mode 0).  Mode 0: our FP64 SIMT product kernel.
+ * Mode 1: on the tensor cores as int8 digit products with exact int32 sums
+ * combined in FP64 -- 9 x 9 digits for FP64 check vectors, 5 x 4 for the
+ * mixed mode's FP32 ones, the FP64 product's accuracy either way (needs 3P
+ * <= 512).  Mode -1 keeps whichever nnk_fmm_autotune times fastest on one
+ * matvec (SIMT until it runs).  Measured on the 250k matvec (C2E time per
+ * matvec): FP64 check vectors 0.78 ms (mode 2), 1.12 (0), 1.97 (1); the
+ * mixed mode's FP32 ones 0.78, 1.32, 0.91; the modes agree to 1.4e-8 (FP64)
+ * and 3e-7 / 4e-6 (mixed, modes 2 / 1 against 0).  nnk_fmm_c2e_mode
+ * reports the form in use (0, 1 or 2). */
 int nnk_fmm_set_c2e(nnk_fmm* fmm, int32_t mode);
 int nnk_fmm_c2e_mode(const nnk_fmm* fmm, int32_t* mode);
 /* Folded M2M / L2L in the matvec: mode 0 off (the default), 1 where it

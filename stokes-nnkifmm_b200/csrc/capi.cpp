@@ -59,6 +59,7 @@ void ctx_release(nnk_ctx* c) {
     cudaSetDevice(c->device);
     if (c->dn_solver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(c->dn_solver));
     if (c->blas) cublasDestroy(static_cast<cublasHandle_t>(c->blas));
+    if (c->blas_ws) cudaFree(c->blas_ws);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     cudaGetLastError();  // an error here must not surface at a later call's launch check
   }

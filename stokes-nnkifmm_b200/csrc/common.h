@@ -81,4 +81,8 @@ struct nnk_ctx {
   // right-hand side of a time step that rebuilds its FMM would pay)
   void* dn_solver = nullptr;  // cusolverDnHandle_t
   void* blas = nullptr;       // cublasHandle_t
+  // the cuBLAS handle's workspace, owned here so that no cuBLAS call
+  // allocates while a matvec is captured into a CUDA graph
+  void* blas_ws = nullptr;
+  size_t blas_ws_bytes = 0;
 };

@@ -120,8 +120,19 @@ struct Solver {
     s = static_cast<cusolverDnHandle_t>(ctx->dn_solver);
     b = static_cast<cublasHandle_t>(ctx->blas);
     cusolverDnSetStream(s, ctx->stream);
-    cublasSetStream(b, ctx->stream);
+    cublasSetStream(b, ctx->stream);  // (this also drops a workspace set on the handle)
     cudaGetLastError();  // library set-up may leave a handled error behind
+  }
+  // The context's own cuBLAS workspace (allocated once), set on the handle,
+  // so that GEMMs captured into CUDA graphs allocate nothing.
+  void own_workspace(nnk_ctx* ctx) {
+    constexpr size_t kBytes = (size_t)32 << 20;
+    if (!ctx->blas_ws) {
+      NNK_CUDA(cudaMalloc(&ctx->blas_ws, kBytes));
+      ctx->blas_ws_bytes = kBytes;
+    }
+    if (cublasSetWorkspace(b, ctx->blas_ws, ctx->blas_ws_bytes) != CUBLAS_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "cublasSetWorkspace failed");
   }
 };
 
@@ -156,6 +167,13 @@ Fmm::Fmm(nnk_ctx* ctx, const HostTree* tree, const FmmParams& p) : ctx_(ctx), t_
   build_tasks();
   t = lap(NNK_SETUP_TASKS, t);
   build_operators();
+  if (blas_c2e()) {
+    // the library-GEMM products' scratch and workspace before any matvec,
+    // which may be captured into a CUDA graph
+    reserve_blas_scratch();
+    Solver sv(ctx_);
+    sv.own_workspace(ctx_);
+  }
   lap(NNK_SETUP_TOTAL, t0);
   if (t_->groups() > 1) {
     // tree mask of a forest, all trees on; allocated here because applies
@@ -372,6 +390,7 @@ void Fmm::build_tasks() {
     std::vector<C2ETile> dt;
     build_c2e_tiles(ln, lvl_off_, dt, dn_toff_);
     dn_tiles_.upload(dt, st);
+    dn_tiles_host_ = dt;
   }
   lvl_nodes_.upload(ln, st);
   {
@@ -584,6 +603,7 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
   if (ts.fold) {
     std::vector<C2ETile> ut;
     build_c2e_tiles(ts.upl_nodes_host, ts.upl_off, ut, ts.upl_toff);
+    ts.upl_tiles_host = ut;
     ts.upl_tiles.upload(ut, st);
     ts.upl_nodes.upload(ts.upl_nodes_host, st);
   }
@@ -591,6 +611,7 @@ void Fmm::build_taskset(TaskSet& ts, const TaskRoles& r, bool stats) {
     std::vector<C2ETile> ut;
     build_c2e_tiles(ts.up_nodes_host, ts.up_off, ut, ts.up_toff);
     ts.up_tiles.upload(ut, st);
+    ts.up_tiles_host = ut;
     // scratch of the K-split C2E launches (allocated here: applies may be
     // captured into CUDA graphs, where allocation is not allowed)
     size_t need = 0;
@@ -1090,7 +1111,7 @@ void Fmm::build_operators() {
     if (info[o] != 0)
       throw Error(NNK_E_CUDA, "surface matrix factorization reported info=" + std::to_string(info[o]));
   // their int8 digits, when the tensor-core products are asked for or chosen
-  if (c2e_mode_ == 1 || (c2e_mode_ < 0 && tc_auto_)) build_tc_digits();
+  if (c2e_mode_ == 1 || (c2e_mode_ < 0 && auto_form_ == 1)) build_tc_digits();
   setup_ms_[NNK_SETUP_OPERATORS] = ms_since(tops);
   const auto tfold = clk::now();
   build_fold_operators(fold_on_ == 2);
@@ -1122,14 +1143,73 @@ void add_f32(long long n, const float* b, double* a, cudaStream_t st) {
 }  // namespace
 
 template <typename Real>
-void Fmm::c2e(int trans, const C2ETile* tiles, int ntiles, const int32_t* nodes, const Real* check, Real* dst,
-              int64_t base, int R, float* m2l_dst, int NP, const int* nact) {
+void Fmm::c2e(int trans, const C2ETile* tiles, const C2ETile* tiles_host, int ntiles, const int32_t* nodes,
+              const Real* check, Real* dst, int64_t base, int R, float* m2l_dst, int NP, const int* nact) {
+  if (blas_c2e() && tiles_host && !nact && (!m2l_dst || R == 1)) {
+    c2e_blas<Real>(trans, tiles_host, ntiles, nodes, check, dst, base, R, m2l_dst, NP);
+    return;
+  }
   if (tc_c2e())
     launch_c2e_tc<Real>(c2e_tc_, trans, tiles, ntiles, nodes, check, dst, base, P_, R, ctx_->stream, m2l_dst, NP,
                         nact);
   else
     launch_c2e<Real>(ops_.p, 3 * P_, trans, tiles, ntiles, nodes, check, dst, base, P_, R, ctx_->stream, m2l_dst, NP,
                      c2e_part_.p, c2e_part_.n, nact);
+}
+
+template <typename Real>
+void Fmm::c2e_blas(int trans, const C2ETile* tiles_host, int ntiles, const int32_t* nodes, const Real* check,
+                   Real* dst, int64_t base, int R, float* m2l_dst, int NP) {
+  const int n3 = 3 * P_;
+  cudaStream_t st = ctx_->stream;
+  if (!blas_x_.p) reserve_blas_scratch();  // normally done at construction
+  Solver sv(ctx_);
+  sv.own_workspace(ctx_);
+  const double one = 1.0, zero = 0.0;
+  for (int i = 0; i < ntiles;) {
+    // a run of tiles with one operator over consecutive entries of `nodes`
+    int j = i + 1;
+    while (j < ntiles && tiles_host[j].op == tiles_host[i].op &&
+           tiles_host[j].first == tiles_host[j - 1].first + tiles_host[j - 1].count)
+      ++j;
+    const int first = tiles_host[i].first;
+    const int ncol = (tiles_host[j - 1].first + tiles_host[j - 1].count - first) * R;
+    if ((size_t)ncol * n3 > blas_x_.n)  // sized for every level's nodes x max_rhs at construction
+      throw Error(NNK_E_STATE, "check-to-equivalent GEMM scratch smaller than a level");
+    const int blocks = (int)std::min<long long>(148 * 8, ((long long)ncol * n3 + 255) / 256);
+    c2e_gather_kernel<Real><<<blocks, 256, 0, st>>>(check, nodes, first, ncol, R, P_, blas_x_.p);
+    NNK_CHECK_LAUNCH();
+    const double* A = ops_.p + (size_t)tiles_host[i].op * n3 * n3;
+    if (cublasDgemm(sv.b, trans ? CUBLAS_OP_T : CUBLAS_OP_N, CUBLAS_OP_N, n3, ncol, n3, &one, A, n3, blas_x_.p, n3,
+                    &zero, blas_y_.p, n3) != CUBLAS_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "cublasDgemm (check-to-equivalent products) failed");
+    c2e_scatter_kernel<Real><<<blocks, 256, 0, st>>>(blas_y_.p, nodes, first, ncol, R, P_, base, 0, dst, m2l_dst, NP);
+    NNK_CHECK_LAUNCH();
+    i = j;
+  }
+}
+
+// Scratch of the library-GEMM C2E for the longest run of one operator in any
+// level of either task set.
+void Fmm::reserve_blas_scratch() {
+  size_t need = 0;
+  auto scan = [&](const std::vector<C2ETile>& t) {
+    for (size_t i = 0; i < t.size();) {
+      size_t j = i + 1;
+      while (j < t.size() && t[j].op == t[i].op && t[j].first == t[j - 1].first + t[j - 1].count) ++j;
+      need = std::max(need, (size_t)(t[j - 1].first + t[j - 1].count - t[i].first));
+      i = j;
+    }
+  };
+  scan(dn_tiles_host_);
+  scan(fwd_.up_tiles_host);
+  scan(fwd_.upl_tiles_host);
+  scan(adj_.up_tiles_host);
+  need *= (size_t)3 * P_ * R_;
+  if (need > blas_x_.n) {
+    blas_x_.alloc(need);
+    blas_y_.alloc(need);
+  }
 }
 
 // Scratch of the tensor-core C2E for the largest launch of either task set.
@@ -1157,10 +1237,11 @@ void Fmm::build_tc_digits() {
 }
 
 void Fmm::set_c2e_mode(int mode) {
-  if (mode < -1 || mode > 1) throw Error(NNK_E_ARG, "C2E mode must be -1, 0 or 1");
+  if (mode < -1 || mode > 2) throw Error(NNK_E_ARG, "C2E mode must be -1, 0, 1 or 2");
   NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
   c2e_mode_ = mode;
   if (mode == 1 && !c2e_tc_.ready) build_tc_digits();
+  if (mode == 2) reserve_blas_scratch();
   bump_version();
 }
 
@@ -1196,7 +1277,8 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
       const int64_t nt = ts.upl_toff[L + 1] - ts.upl_toff[L];
       const int64_t nf = fup_toff_[L + 1] - fup_toff_[L];
       phase(NNK_PHASE_UP_C2E, [&] {
-        c2e<Real>(0, ts.upl_tiles.p + ts.upl_toff[L], (int)nt, ts.upl_nodes.p, check, str, regionA, R, m2l_src,
+        c2e<Real>(0, ts.upl_tiles.p + ts.upl_toff[L], ts.upl_tiles_host.data() + ts.upl_toff[L], (int)nt,
+                  ts.upl_nodes.p, check, str, regionA, R, m2l_src,
                   m2l_.NP, na);
         NodeGemm g{fold_up_.p, (size_t)8 * n * n, n, 8 * n, 0, fup_tiles_.p + fup_toff_[L], fpar_.p, fch_.p,
                    (long long)regionA, P_, R, 0, m2l_src, m2l_.NP};
@@ -1208,7 +1290,8 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     run_group<Real>(ts, ts.up[L], spos, str, spos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS, R);
     const int64_t nt = ts.up_toff[L + 1] - ts.up_toff[L];
     phase(NNK_PHASE_UP_C2E, [&] {
-      c2e<Real>(0, ts.up_tiles.p + ts.up_toff[L], (int)nt, ts.up_nodes.p, check, str, regionA, R, m2l_src, m2l_.NP,
+      c2e<Real>(0, ts.up_tiles.p + ts.up_toff[L], ts.up_tiles_host.data() + ts.up_toff[L], (int)nt, ts.up_nodes.p,
+                check, str, regionA, R, m2l_src, m2l_.NP,
                 na);
     });
   }
@@ -1248,7 +1331,8 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     const int64_t nt = dn_toff_[L + 1] - dn_toff_[L];
     if (nt == 0) continue;
     phase(NNK_PHASE_DOWN_C2E, [&] {
-      c2e<Real>(1, dn_tiles_.p + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str, dnB, R, nullptr, 0, na);
+      c2e<Real>(1, dn_tiles_.p + dn_toff_[L], dn_tiles_host_.data() + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str,
+                dnB, R, nullptr, 0, na);
       if (fo && L >= 2) {
         // + D applied to the parents (level L - 1) for their 8 children
         const int64_t nf = fdn_toff_[L] - fdn_toff_[L - 1];
@@ -1479,9 +1563,8 @@ std::pair<double, double> Fmm::autotune(int nrhs) {
 // right-hand sides timed (best of three) with each, the faster kept; the
 // operator digits are dropped when the SIMT products win.
 void Fmm::tune_c2e(int R) {
-  if (3 * P_ > 512) return;
-  if (!c2e_tc_.ready) build_tc_digits();
-  if (!c2e_tc_.ready) return;
+  // the candidates: SIMT, tensor cores (where 3P <= 512), library DGEMM (one tree)
+  if (3 * P_ <= 512 && !c2e_tc_.ready) build_tc_digits();
   const HostTree& t = *t_;
   cudaStream_t st = ctx_->stream;
   DBuf<double> in(3 * (size_t)t.n_pot * R), out(3 * (size_t)t.n_tgt * R);
@@ -1489,9 +1572,10 @@ void Fmm::tune_c2e(int R) {
   cudaEvent_t a, b;
   NNK_CUDA(cudaEventCreate(&a));
   NNK_CUDA(cudaEventCreate(&b));
-  float best[2] = {1e30f, 1e30f};
-  for (int m = 0; m < 2; ++m) {
-    tc_auto_ = m == 1;
+  float best[3] = {1e30f, 1e30f, 1e30f};
+  for (int m = 0; m < 3; ++m) {
+    if ((m == 1 && !c2e_tc_.ready) || (m == 2 && t.groups() != 1)) continue;
+    auto_form_ = m;
     bump_version();
     apply(in.p, out.p, NNK_LAYOUT_ROWS, R);  // warm
     for (int rep = 0; rep < 3; ++rep) {
@@ -1506,8 +1590,8 @@ void Fmm::tune_c2e(int R) {
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  tc_auto_ = best[1] < best[0];
-  if (!tc_auto_) release_c2e_tc(c2e_tc_);
+  auto_form_ = (int)(std::min_element(best, best + 3) - best);
+  if (auto_form_ != 1 && c2e_tc_.ready) release_c2e_tc(c2e_tc_);
   bump_version();
 }
 

@@ -105,6 +105,7 @@ struct TaskSet {
   DBuf<int32_t> up_nodes;
   std::vector<int64_t> up_off;
   DBuf<C2ETile> up_tiles;
+  std::vector<C2ETile> up_tiles_host;  // host copies (the library-GEMM C2E form groups them)
   std::vector<int64_t> up_toff;
   // folded form (the matvec's task set only): the M2M and L2L steps run as
   // products with operators that include the check-to-equivalent step, so
@@ -116,6 +117,7 @@ struct TaskSet {
   DBuf<int32_t> upl_nodes;
   std::vector<int64_t> upl_off;
   DBuf<C2ETile> upl_tiles;
+  std::vector<C2ETile> upl_tiles_host;
   std::vector<int64_t> upl_toff;
   int64_t partial_slots = 0;
 };
@@ -207,10 +209,13 @@ class Fmm {
   // uses it.
   void set_fold(int mode);
   bool folded() const { return fold_ok_ && fold_on_ > 0; }
-  // Check-to-equivalent products: 1 tensor cores (where 3P <= 512), 0 FP64
-  // SIMT, -1 the faster as timed by autotune; the form in use (0 or 1).
+  // Check-to-equivalent products: 2 (the default) one cuBLAS DGEMM per run
+  // of nodes sharing an operator on gathered check vectors (single-tree
+  // FMMs; a matvec being captured into a CUDA graph, and forests, use the
+  // SIMT products), 0 FP64 SIMT, 1 tensor cores (where 3P <= 512), -1 the
+  // fastest as timed by autotune; the form in use (0, 1 or 2).
   void set_c2e_mode(int mode);
-  int c2e_mode() const { return tc_c2e() ? 1 : 0; }
+  int c2e_mode() const { return blas_c2e() ? 2 : tc_c2e() ? 1 : 0; }
   // host wall time of the set-up steps (NNK_SETUP_*), milliseconds
   const double* setup_ms() const { return setup_ms_; }
   bool near32() const { return p_.precision == NNK_PREC_NEAR32; }
@@ -298,21 +303,30 @@ class Fmm {
   std::vector<double> op_w_;          // box width of each operator
   std::vector<int> op_of_;            // (group * (maxl + 1) + level) -> operator
   DBuf<C2ETile> dn_tiles_;  // per level, tiles of nodes sharing an operator
+  std::vector<C2ETile> dn_tiles_host_;
+  DBuf<double> blas_x_, blas_y_;  // gathered check vectors and products of the library-GEMM C2E form
   // check-to-equivalent products on the tensor cores (int8 digits, FP64
-  // accuracy; c2e_tc.h) or on the FP64 SIMT units
+  // accuracy; c2e_tc.h), as library DGEMMs or on the FP64 SIMT units
   C2ETcPlan c2e_tc_;
-  // 1 tensor cores where available, 0 SIMT (the default), -1 the faster of
-  // the two as timed by autotune (SIMT until then)
-  int c2e_mode_ = 0;
-  bool tc_auto_ = false;
-  bool tc_c2e() const { return (c2e_mode_ < 0 ? tc_auto_ : c2e_mode_ == 1) && c2e_tc_.ready; }
+  // 2 library DGEMM (the default), 1 tensor cores where available, 0 SIMT,
+  // -1 the fastest as timed by autotune (SIMT until then)
+  int c2e_mode_ = 2;
+  int auto_form_ = 0;  // the form autotune chose for mode -1 (0, 1 or 2)
+  bool tc_c2e() const { return (c2e_mode_ < 0 ? auto_form_ == 1 : c2e_mode_ == 1) && c2e_tc_.ready; }
+  bool blas_c2e() const { return t_->groups() == 1 && (c2e_mode_ < 0 ? auto_form_ == 2 : c2e_mode_ == 2); }
   void tune_c2e(int R);
   std::pair<double, double> autotune_tiles(int nrhs);
   void build_tc_digits();
   void reserve_tc_scratch();
   template <typename Real>
-  void c2e(int trans, const C2ETile* tiles, int ntiles, const int32_t* nodes, const Real* check, Real* dst,
-           int64_t base, int R, float* m2l_dst, int NP, const int* nact);
+  void c2e(int trans, const C2ETile* tiles, const C2ETile* tiles_host, int ntiles, const int32_t* nodes,
+           const Real* check, Real* dst, int64_t base, int R, float* m2l_dst, int NP, const int* nact);
+  // the library-GEMM form: per run of tiles with one operator, gather the
+  // check vectors, one cuBLAS DGEMM, scatter the products
+  template <typename Real>
+  void c2e_blas(int trans, const C2ETile* tiles_host, int ntiles, const int32_t* nodes, const Real* check, Real* dst,
+                int64_t base, int R, float* m2l_dst, int NP);
+  void reserve_blas_scratch();
   // folded M2M / L2L: per operator (box width w), U = A(w) [M2M_0 .. M2M_7]
   // (3P x 8 * 3P; M2M_k: child k's up surface -> the down surface of its
   // parent of width w) and D = [A(w)^T L2L_0; ..; A(w)^T L2L_7] (8 * 3P x 3P;

@@ -116,9 +116,11 @@ class KIFMM:
         L.check(L.lib.nnk_fmm_set_fold(self.h, int(mode)), self.ctx.h, "setFold")
 
     def setC2E(self, mode=1):
-        """Check-to-equivalent products on the tensor cores (1: int8 digit
-        products with FP64 accuracy), as FP64 SIMT products (0, the default),
-        or (-1) the faster of the two as timed by autotune()."""
+        """Check-to-equivalent products as one cuBLAS DGEMM per run of nodes
+        sharing an operator (2, the default; forests and graph-captured
+        matvecs use 0), as our FP64 SIMT products (0), on the tensor cores
+        (1: int8 digit products with FP64 accuracy), or (-1) the fastest as
+        timed by autotune()."""
         L.check(L.lib.nnk_fmm_set_c2e(self.h, int(mode)), self.ctx.h, "setC2E")
 
     def c2eMode(self):

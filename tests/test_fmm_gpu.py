@@ -226,7 +226,7 @@ def test_tensor_core_c2e_matches_fp64_simt(name, precision):
     g = load(name)
     t = tree_of(g)
     fmm = nk.KIFMM(t, [float(g["eps"]), float(g["mu"])], precision=precision)
-    assert fmm.c2eMode() == 0  # the default
+    assert fmm.c2eMode() == 2  # the default: library DGEMM
     fmm.setC2E(1)
     assert fmm.c2eMode() == 1
     a = fmm.computeVel(g["F"])
@@ -245,6 +245,33 @@ def test_tensor_core_c2e_matches_fp64_simt(name, precision):
     d = fmm.computeVel(g["F"])
     fmm.setC2E(kept)
     assert np.array_equal(d, fmm.computeVel(g["F"]))
+    assert rel(a, b) <= C2E_TC_TOL[precision]
+    if precision == "fp64":
+        assert rel(a, g["vel"]) <= FP64_TOL[name]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "near32", "mixed"])
+@pytest.mark.parametrize("name", ["sphere10_40", "adaptive_nearest_1200", "matvec_4000_16000"])
+def test_library_dgemm_c2e_matches_simt(name, precision):
+    """Check-to-equivalent products as one cuBLAS DGEMM per run of nodes
+    sharing an operator (mode 2, the check vectors gathered and the products
+    scattered) against the FP64 SIMT products: the same FP64 product summed
+    in another order, lifted by the exact inverses' condition number (the
+    tensor-core form's bound holds with room); FP64 mode still matches the
+    oracle, and repeated calls give the same bits."""
+    g = load(name)
+    t = tree_of(g)
+    fmm = nk.KIFMM(t, [float(g["eps"]), float(g["mu"])], precision=precision)
+    assert fmm.c2eMode() == 2  # the default
+    fmm.setC2E(0)
+    b = fmm.computeVel(g["F"])
+    fmm.setC2E(2)
+    assert fmm.c2eMode() == 2
+    a = fmm.computeVel(g["F"])
+    assert np.array_equal(a, fmm.computeVel(g["F"]))
+    fmm.setC2E(0)
+    assert np.array_equal(b, fmm.computeVel(g["F"]))
+    print(name, precision, "dgemm C2E vs SIMT", rel(a, b))
     assert rel(a, b) <= C2E_TC_TOL[precision]
     if precision == "fp64":
         assert rel(a, g["vel"]) <= FP64_TOL[name]
