@@ -578,7 +578,9 @@ def roofline(per_step, stats, precision, peaks, m2l_form, l2_gbs=None):
     # its own phase (tensor cores or Fourier space) the down pairs are the rest
     m2l_apart = per_step.get("m2l", (0.0, 0))[1] > 0
     down = stats["pairs_down"] - (stats["m2l_pairs"] * stats["surface_points"] ** 2 if m2l_apart else 0)
-    pairs = {"up_pairs": stats["pairs_up"], "down_pairs": down, "leaf_pairs": stats["pairs_leaf"]}
+    # M2M / L2L as kernel-matrix products run in the check-to-equivalent phases
+    mp, lp = stats.get("m2m_product_pairs", 0), stats.get("l2l_product_pairs", 0)
+    pairs = {"up_pairs": stats["pairs_up"] - mp, "down_pairs": down - lp, "leaf_pairs": stats["pairs_leaf"]}
     ms_l = per_step[dom][0] / per_step[dom][1]
     if dom == "m2l" and m2l_form == "tensor":
         n3 = 3 * stats["surface_points"]

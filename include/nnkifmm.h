@@ -138,6 +138,11 @@ typedef struct nnk_fmm_stats {
   int64_t m2l_groups;   /* parent-grouped: (record, child difference) groups;
                            each reads one kernel spectrum (6 complex values a
                            frequency) for all its V pairs                   */
+  int64_t m2m_product_pairs; /* M2M as products with its kernel matrices
+                           (nnk_fmm_set_m2m_form): the target-source pairs
+                           that pairs_up counts but the pair kernels no
+                           longer evaluate (0 with the pair form)           */
+  int64_t l2l_product_pairs; /* the same for L2L and pairs_down (form 2)    */
 } nnk_fmm_stats;
 
 /* GMRES options/result (MATLAB gmres(A,b,restart,tol,maxit), x0 = 0). */
@@ -289,6 +294,20 @@ int nnk_fmm_set_eps(nnk_fmm* fmm, double eps);
  * reports the form in use (0, 1 or 2). */
 int nnk_fmm_set_c2e(nnk_fmm* fmm, int32_t mode);
 int nnk_fmm_c2e_mode(const nnk_fmm* fmm, int32_t* mode);
+/* M2M and L2L in the matvec (the parent sums of upwardPass.m:81-93 and the
+ * parentsurf term of DownNonleaf.m:42-46) as products with their kernel
+ * matrices -- per box width [M2M_0 .. M2M_7] from a parent's 8 children and
+ * [L2L_0; ..; L2L_7] from a parent to its 8 children, one cuBLAS DGEMM per
+ * level on gathered densities, into the check potentials, before the
+ * check-to-equivalent step -- or as pair sums: form 2, the default where
+ * the tree allows it (one tree; the Fourier-space or tensor-core M2L), both
+ * as products; form 1 M2M as products and L2L as pair sums; form 0 both as
+ * pair sums.  Measured on the 250k FP64 matvec: 13.47 ms (form 2), 13.80
+ * (1), 14.20 (0), 1.9e-8 apart.  Both give the reference's check potentials to FP64 rounding
+ * (unlike folding, which pre-multiplies by the inverse), so the exact
+ * inverses allow it.  The per-phase profile counts the products with the
+ * check-to-equivalent phases. */
+int nnk_fmm_set_m2m_form(nnk_fmm* fmm, int32_t form);
 /* Folded M2M / L2L in the matvec: mode 0 off (the default), 1 where it
  * pays (at least 64 non-leaf nodes per box width), 2 wherever available.  A
  * parent's up-equivalent density becomes one FP64 product

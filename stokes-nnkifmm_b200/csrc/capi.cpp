@@ -434,6 +434,8 @@ int nnk_fmm_stats_get(const nnk_fmm* fmm, nnk_fmm_stats* stats) {
   if (!fmm || !stats) return NNK_E_ARG;
   *stats = fmm->f->stats();
   stats->folded = fmm->f->folded() ? 1 : 0;
+  stats->m2m_product_pairs = fmm->f->m2m_form() ? fmm->f->m2m_pairs() : 0;
+  stats->l2l_product_pairs = fmm->f->m2m_form() == 2 ? fmm->f->m2m_pairs() : 0;
   return NNK_OK;
 }
 
@@ -464,6 +466,15 @@ int nnk_fmm_c2e_mode(const nnk_fmm* fmm, int32_t* mode) {
   if (!fmm || !mode) return NNK_E_ARG;
   *mode = fmm->f->c2e_mode();
   return NNK_OK;
+}
+
+int nnk_fmm_set_m2m_form(nnk_fmm* fmm, int32_t form) {
+  if (!fmm) return NNK_E_ARG;
+  nnk_ctx* ctx = fmm->ctx;
+  API_TRY
+  need_gpu(ctx);
+  fmm->f->set_m2m_form(form);
+  API_CATCH(ctx)
 }
 
 int nnk_fmm_set_fold(nnk_fmm* fmm, int32_t on) {

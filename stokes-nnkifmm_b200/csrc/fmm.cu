@@ -167,7 +167,7 @@ Fmm::Fmm(nnk_ctx* ctx, const HostTree* tree, const FmmParams& p) : ctx_(ctx), t_
   build_tasks();
   t = lap(NNK_SETUP_TASKS, t);
   build_operators();
-  if (blas_c2e()) {
+  if (blas_c2e() || m2m_products()) {
     // the library-GEMM products' scratch and workspace before any matvec,
     // which may be captured into a CUDA graph
     reserve_blas_scratch();
@@ -808,6 +808,8 @@ void Fmm::build_fold_lists() {
   build_c2e_tiles(par, fpar_off_, td, fdn_toff_, 1);
   fup_tiles_.upload(tu, st);
   fdn_tiles_.upload(td, st);
+  fup_tiles_host_ = tu;
+  fdn_tiles_host_ = td;
   const int n = 3 * P_;
   size_t need = c2e_part_.n;
   for (int R = 1; R <= R_; ++R)
@@ -838,31 +840,10 @@ __global__ void kernel_matrix_kernel(const double* __restrict__ src, int ns, con
 }
 }  // namespace
 
-// The folded operators U and D of every box width (see fmm.h), from the
-// check-to-equivalent operators A: on canonical boxes (a parent [0, w]^3 with
-// its children, or [0, 2w]^3), kernel matrices and products on the device
-// (FP64; the products by cuBLAS).  Built for regularized (Tikhonov)
-// check-to-equivalent operators only: with the exact inverses (cond ~1e10)
-// the folded operators A M2M_k carry FP64 rounding relative to |A| |M2M_k|
-// into the very large equivalent densities of NEAREST trees, 4e-5 away from
-// the pair sums on a 1200-point NEAREST cloud, where the regularized ones
-// stay within 3e-7.  Also needs a matvec whose M2L runs apart from the pair
-// tasks (Fourier-space or tensor-core M2L), at most 1 GiB of operators, and
-// (unless forced) at least 64 non-leaf nodes per operator: below that the
-// set-up costs more than the folded products save.
-void Fmm::build_fold_operators(bool force) {
-  fold_ok_ = false;
-  if (exact_ops_ || !fold_lists_ok_ || !(fft_m2l_ || tensor_m2l_)) return;
-  if (!force && fpar_off_.back() < 64 * (int64_t)nops_) return;
-  const int n = 3 * P_;
-  const size_t blk = (size_t)n * n, per = 8 * blk;
-  if ((size_t)nops_ * 2 * per * sizeof(double) > ((size_t)1 << 30)) return;
-  cudaStream_t st = ctx_->stream;
-  fold_up_.alloc(nops_ * per);
-  fold_dn_.alloc(nops_ * per);
+// Canonical surfaces per operator: [parent down surface (w), parent down
+// surface (2w), 8 children's up surfaces of [0, w]^3, 8 of [0, 2w]^3].
+std::vector<double> Fmm::fold_surfaces() const {
   const auto lat = shell_lattice(p_.res, p_.shells);
-  // per operator: [parent down surface (w), parent down surface (2w),
-  // 8 children's up surfaces of [0, w]^3, 8 of [0, 2w]^3]
   const size_t ps = 3 * (size_t)P_;
   std::vector<double> surf((size_t)nops_ * 18 * ps);
   for (int o = 0; o < nops_; ++o) {
@@ -886,23 +867,57 @@ void Fmm::build_fold_operators(bool force) {
       surface(lo2, hi2, p_.res, lat, S + (10 + k) * ps);
     }
   }
+  return surf;
+}
+
+// M2M_k (child k's up surface -> the down surface of its parent of width w)
+// into dM + k (3P)^2 and L2L_k (the down surface of the parent of width 2w ->
+// child k's up surface) into dL + k (3P)^2, for operator o (surf: the device
+// copy of fold_surfaces()).
+void Fmm::kernel_blocks(int o, const double* surf, double* dM, double* dL) {
+  const int n = 3 * P_;
+  const size_t blk = (size_t)n * n, ps = 3 * (size_t)P_;
+  const double e2 = p_.eps * p_.eps, c = 1.0 / (8.0 * M_PI * p_.mu);
+  const unsigned kb = (unsigned)(((size_t)P_ * P_ + 255) / 256);
+  const double* S = surf + (size_t)o * 18 * ps;
+  cudaStream_t st = ctx_->stream;
+  for (int k = 0; k < 8; ++k) {
+    kernel_matrix_kernel<<<kb, 256, 0, st>>>(S + (2 + k) * ps, P_, S, P_, e2, c, dM + k * blk, n);
+    NNK_CHECK_LAUNCH();
+    kernel_matrix_kernel<<<kb, 256, 0, st>>>(S + ps, P_, S + (10 + k) * ps, P_, e2, c, dL + k * blk, n);
+    NNK_CHECK_LAUNCH();
+  }
+}
+
+// The folded operators U and D of every box width (see fmm.h), from the
+// check-to-equivalent operators A: on canonical boxes (a parent [0, w]^3 with
+// its children, or [0, 2w]^3), kernel matrices and products on the device
+// (FP64; the products by cuBLAS).  Built for regularized (Tikhonov)
+// check-to-equivalent operators only: with the exact inverses (cond ~1e10)
+// the folded operators A M2M_k carry FP64 rounding relative to |A| |M2M_k|
+// into the very large equivalent densities of NEAREST trees, 4e-5 away from
+// the pair sums on a 1200-point NEAREST cloud, where the regularized ones
+// stay within 3e-7.  Also needs a matvec whose M2L runs apart from the pair
+// tasks (Fourier-space or tensor-core M2L), at most 1 GiB of operators, and
+// (unless forced) at least 64 non-leaf nodes per operator: below that the
+// set-up costs more than the folded products save.
+void Fmm::build_fold_operators(bool force) {
+  fold_ok_ = false;
+  if (exact_ops_ || !fold_lists_ok_ || !(fft_m2l_ || tensor_m2l_)) return;
+  if (!force && fpar_off_.back() < 64 * (int64_t)nops_) return;
+  const int n = 3 * P_;
+  const size_t blk = (size_t)n * n, per = 8 * blk;
+  if ((size_t)nops_ * 2 * per * sizeof(double) > ((size_t)1 << 30)) return;
+  cudaStream_t st = ctx_->stream;
+  fold_up_.alloc(nops_ * per);
+  fold_dn_.alloc(nops_ * per);
   DBuf<double> dS;
-  dS.upload(surf, st);
+  dS.upload(fold_surfaces(), st);
   DBuf<double> dM(per), dL(per);
   Solver sv(ctx_);
   const double one = 1.0, zero = 0.0;
-  const double e2 = p_.eps * p_.eps, c = 1.0 / (8.0 * M_PI * p_.mu);
-  const unsigned kb = (unsigned)(((size_t)P_ * P_ + 255) / 256);
   for (int o = 0; o < nops_; ++o) {
-    const double* S = dS.p + (size_t)o * 18 * ps;
-    for (int k = 0; k < 8; ++k) {
-      // M2M_k: child k's up surface -> the parent's down surface
-      kernel_matrix_kernel<<<kb, 256, 0, st>>>(S + (2 + k) * ps, P_, S, P_, e2, c, dM.p + k * blk, n);
-      NNK_CHECK_LAUNCH();
-      // L2L_k: the parent's down surface -> child k's up surface
-      kernel_matrix_kernel<<<kb, 256, 0, st>>>(S + ps, P_, S + (10 + k) * ps, P_, e2, c, dL.p + k * blk, n);
-      NNK_CHECK_LAUNCH();
-    }
+    kernel_blocks(o, dS.p, dM.p, dL.p);
     const double* A = ops_.p + (size_t)o * blk;
     // U = A [M2M_0 .. M2M_7]  (n x 8n)
     if (cublasDgemm(sv.b, CUBLAS_OP_N, CUBLAS_OP_N, n, 8 * n, n, &one, A, n, dM.p, n, &zero,
@@ -916,6 +931,42 @@ void Fmm::build_fold_operators(bool force) {
   }
   NNK_CUDA(cudaStreamSynchronize(st));  // dS, dM, dL are freed on return
   fold_ok_ = true;
+}
+
+// The unfolded M2M / L2L operators (see fmm.h): for single-tree FMMs whose
+// M2L runs apart from the pair tasks, at most 1 GiB of them.
+void Fmm::build_m2m_operators() {
+  m2m_ok_ = false;
+  if (!fold_lists_ok_ || !(fft_m2l_ || tensor_m2l_) || t_->groups() != 1) return;
+  const int n = 3 * P_;
+  const size_t blk = (size_t)n * n, per = 8 * blk;
+  if ((size_t)nops_ * 2 * per * sizeof(double) > ((size_t)1 << 30)) return;
+  cudaStream_t st = ctx_->stream;
+  m2m_ops_.alloc(nops_ * per);
+  l2l_ops_.alloc(nops_ * per);
+  DBuf<double> dS;
+  dS.upload(fold_surfaces(), st);
+  DBuf<double> dL(per);
+  for (int o = 0; o < nops_; ++o) {
+    // [M2M_0 .. M2M_7] is the blocks side by side (n x 8n, leading dimension n)
+    kernel_blocks(o, dS.p, m2m_ops_.p + (size_t)o * per, dL.p);
+    // [L2L_0; ..; L2L_7]: block k in rows k n .. k n + n - 1 (8n x n, leading dimension 8n)
+    for (int k = 0; k < 8; ++k)
+      NNK_CUDA(cudaMemcpy2DAsync(l2l_ops_.p + (size_t)o * per + (size_t)k * n, 8 * n * sizeof(double),
+                                 dL.p + k * blk, n * sizeof(double), n * sizeof(double), n,
+                                 cudaMemcpyDeviceToDevice, st));
+  }
+  NNK_CUDA(cudaStreamSynchronize(st));  // dS, dL are freed on return
+  m2m_ok_ = true;
+}
+
+void Fmm::set_m2m_form(int form) {
+  if (form < 0 || form > 2) throw Error(NNK_E_ARG, "M2M / L2L form must be 0, 1 or 2");
+  NNK_CUDA(cudaStreamSynchronize(ctx_->stream));
+  m2m_on_ = form;
+  if (form && !m2m_ok_) build_m2m_operators();
+  if (m2m_products()) reserve_blas_scratch();
+  bump_version();
 }
 
 void Fmm::set_fold(int mode) {
@@ -1115,6 +1166,7 @@ void Fmm::build_operators() {
   setup_ms_[NNK_SETUP_OPERATORS] = ms_since(tops);
   const auto tfold = clk::now();
   build_fold_operators(fold_on_ == 2);
+  if (m2m_on_) build_m2m_operators();
   setup_ms_[NNK_SETUP_FOLD] = ms_since(tfold);
 }
 
@@ -1158,35 +1210,45 @@ void Fmm::c2e(int trans, const C2ETile* tiles, const C2ETile* tiles_host, int nt
 }
 
 template <typename Real>
-void Fmm::c2e_blas(int trans, const C2ETile* tiles_host, int ntiles, const int32_t* nodes, const Real* check,
-                   Real* dst, int64_t base, int R, float* m2l_dst, int NP) {
-  const int n3 = 3 * P_;
+void Fmm::node_gemm_blas(const double* ops, size_t op_stride, int M, int Kd, int trans, const C2ETile* tiles_host,
+                         int ntiles, const int32_t* out_nodes, const int32_t* in_nodes, const Real* src, Real* dst,
+                         int64_t base, int R, int accumulate, float* m2l_dst, int NP) {
   cudaStream_t st = ctx_->stream;
   if (!blas_x_.p) reserve_blas_scratch();  // normally done at construction
   Solver sv(ctx_);
   sv.own_workspace(ctx_);
   const double one = 1.0, zero = 0.0;
   for (int i = 0; i < ntiles;) {
-    // a run of tiles with one operator over consecutive entries of `nodes`
+    // a run of tiles with one operator over consecutive entries of the node lists
     int j = i + 1;
     while (j < ntiles && tiles_host[j].op == tiles_host[i].op &&
            tiles_host[j].first == tiles_host[j - 1].first + tiles_host[j - 1].count)
       ++j;
     const int first = tiles_host[i].first;
     const int ncol = (tiles_host[j - 1].first + tiles_host[j - 1].count - first) * R;
-    if ((size_t)ncol * n3 > blas_x_.n)  // sized for every level's nodes x max_rhs at construction
-      throw Error(NNK_E_STATE, "check-to-equivalent GEMM scratch smaller than a level");
-    const int blocks = (int)std::min<long long>(148 * 8, ((long long)ncol * n3 + 255) / 256);
-    c2e_gather_kernel<Real><<<blocks, 256, 0, st>>>(check, nodes, first, ncol, R, P_, blas_x_.p);
+    if ((size_t)ncol * std::max(M, Kd) > blas_x_.n)  // sized for every level's nodes x max_rhs at construction
+      throw Error(NNK_E_STATE, "node-product GEMM scratch smaller than a level");
+    const int bx = (int)std::min<long long>(148 * 8, ((long long)ncol * Kd + 255) / 256);
+    c2e_gather_kernel<Real><<<bx, 256, 0, st>>>(src, in_nodes, first, ncol, R, P_, Kd, blas_x_.p);
     NNK_CHECK_LAUNCH();
-    const double* A = ops_.p + (size_t)tiles_host[i].op * n3 * n3;
-    if (cublasDgemm(sv.b, trans ? CUBLAS_OP_T : CUBLAS_OP_N, CUBLAS_OP_N, n3, ncol, n3, &one, A, n3, blas_x_.p, n3,
-                    &zero, blas_y_.p, n3) != CUBLAS_STATUS_SUCCESS)
-      throw Error(NNK_E_CUDA, "cublasDgemm (check-to-equivalent products) failed");
-    c2e_scatter_kernel<Real><<<blocks, 256, 0, st>>>(blas_y_.p, nodes, first, ncol, R, P_, base, 0, dst, m2l_dst, NP);
+    const double* A = ops + (size_t)tiles_host[i].op * op_stride;
+    if (cublasDgemm(sv.b, trans ? CUBLAS_OP_T : CUBLAS_OP_N, CUBLAS_OP_N, M, ncol, Kd, &one, A, trans ? Kd : M,
+                    blas_x_.p, Kd, &zero, blas_y_.p, M) != CUBLAS_STATUS_SUCCESS)
+      throw Error(NNK_E_CUDA, "cublasDgemm (node products) failed");
+    const int by = (int)std::min<long long>(148 * 8, ((long long)ncol * M + 255) / 256);
+    c2e_scatter_kernel<Real><<<by, 256, 0, st>>>(blas_y_.p, out_nodes, first, ncol, R, P_, M, base, accumulate, dst,
+                                                m2l_dst, NP);
     NNK_CHECK_LAUNCH();
     i = j;
   }
+}
+
+template <typename Real>
+void Fmm::c2e_blas(int trans, const C2ETile* tiles_host, int ntiles, const int32_t* nodes, const Real* check,
+                   Real* dst, int64_t base, int R, float* m2l_dst, int NP) {
+  const int n3 = 3 * P_;
+  node_gemm_blas<Real>(ops_.p, (size_t)n3 * n3, n3, n3, trans, tiles_host, ntiles, nodes, nodes, check, dst, base, R,
+                       0, m2l_dst, NP);
 }
 
 // Scratch of the library-GEMM C2E for the longest run of one operator in any
@@ -1205,6 +1267,13 @@ void Fmm::reserve_blas_scratch() {
   scan(fwd_.up_tiles_host);
   scan(fwd_.upl_tiles_host);
   scan(adj_.up_tiles_host);
+  {  // the M2M / L2L products: 8 x 3P rows per parent
+    const size_t keep = need;
+    need = 0;
+    scan(fup_tiles_host_);
+    scan(fdn_tiles_host_);
+    need = std::max(keep, 8 * need);
+  }
   need *= (size_t)3 * P_ * R_;
   if (need > blas_x_.n) {
     blas_x_.alloc(need);
@@ -1268,9 +1337,29 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
   // folded M2M / L2L: the M2L must run apart from the pair tasks (it writes
   // every check first), and nothing may need a non-leaf's check afterwards
   const bool fo = fold && ts.fold && folded() && (tm || fm) && !save_up_;
+  // M2M / L2L as products with their kernel matrices (the same split of the
+  // pair tasks as folding, but into the checks)
+  const bool mo = !fo && fold && ts.fold && m2m_products() && (tm || fm) && !save_up_ && !na;
+  const bool lo = mo && l2l_products();
   float* m2l_src = tm && !m2l_.compressed ? m2l_.src.p : nullptr;
   // upward pass
   for (int L = maxl_; L >= 1; --L) {
+    if (mo) {
+      // leaves: S2M pairs; non-leaves: [M2M_0 .. M2M_7] on their 8 children; then C2E
+      run_group<Real>(ts, ts.up_leaf[L], spos, str, spos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS, R);
+      const int64_t nf = fup_toff_[L + 1] - fup_toff_[L];
+      const int64_t nt = ts.up_toff[L + 1] - ts.up_toff[L];
+      if (nf + nt > 0)
+        phase(NNK_PHASE_UP_C2E, [&] {  // the operator products: M2M, then check-to-equivalent
+          if (nf > 0)
+            node_gemm_blas<Real>(m2m_ops_.p, (size_t)8 * n * n, n, 8 * n, 0, fup_tiles_host_.data() + fup_toff_[L],
+                                 (int)nf, fpar_.p, fch_.p, str + (size_t)C * regionA, check, 0, R, 0, nullptr, 0);
+          if (nt > 0)
+            c2e<Real>(0, ts.up_tiles.p + ts.up_toff[L], ts.up_tiles_host.data() + ts.up_toff[L], (int)nt,
+                      ts.up_nodes.p, check, str, regionA, R, m2l_src, m2l_.NP, na);
+        });
+      continue;
+    }
     if (fo) {
       // leaves: S2M + C2E; non-leaves: U applied to their 8 children
       run_group<Real>(ts, ts.up_leaf[L], spos, str, spos, check, e2, scale, 0, NNK_PHASE_UP_PAIRS, R);
@@ -1322,7 +1411,7 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
     phase(NNK_PHASE_DOWN_PAIRS, [&] { add_f32((long long)nc, check32_.p, (double*)check, st); });
   }
   const std::vector<TaskGroup>& dgroups =
-      fo ? ts.down_x : near ? ts.l2l : (tm || fm) ? ts.down_nov : ts.down;
+      (fo || lo) ? ts.down_x : near ? ts.l2l : (tm || fm) ? ts.down_nov : ts.down;
   const int64_t dnB = regionA + (int64_t)P_ * N_;
   for (int L = 1; L <= maxl_; ++L) {
     if (dgroups[L].count > 0)
@@ -1330,7 +1419,14 @@ void Fmm::far_field(TaskSet& ts, const Real* spos, Real* str, int64_t regionA, i
                       R);
     const int64_t nt = dn_toff_[L + 1] - dn_toff_[L];
     if (nt == 0) continue;
-    phase(NNK_PHASE_DOWN_C2E, [&] {
+    phase(NNK_PHASE_DOWN_C2E, [&] {  // the operator products: L2L (product form), then check-to-equivalent
+      if (lo && L >= 2) {
+        // + [L2L_0; ..; L2L_7] from the parents (level L - 1) into their 8 children's checks
+        const int64_t nf = fdn_toff_[L] - fdn_toff_[L - 1];
+        if (nf > 0)
+          node_gemm_blas<Real>(l2l_ops_.p, (size_t)8 * n * n, 8 * n, n, 0, fdn_tiles_host_.data() + fdn_toff_[L - 1],
+                               (int)nf, fch_.p, fpar_.p, str + (size_t)C * dnB, check, 0, R, 1, nullptr, 0);
+      }
       c2e<Real>(1, dn_tiles_.p + dn_toff_[L], dn_tiles_host_.data() + dn_toff_[L], (int)nt, lvl_nodes_.p, check, str,
                 dnB, R, nullptr, 0, na);
       if (fo && L >= 2) {
@@ -1608,8 +1704,11 @@ std::pair<double, double> Fmm::autotune_tiles(int nrhs) {
     // FP64 groups (S2M/M2M, L2L, L2T + W-list) and FP32 groups (X-list P2L,
     // U-list P2P) of the NEAR32 split, each tuned in its own arithmetic
     std::vector<TaskGroup*> g64, g32;
-    for (auto& g : folded() ? fwd_.up_leaf : fwd_.up) g64.push_back(&g);
-    if (!folded())
+    // (the groups the matvec runs: S2M alone where M2M runs folded or as
+    // products, no L2L pairs where L2L does)
+    const bool nov = tensor_m2l_ || fft_m2l_;
+    for (auto& g : (folded() || (m2m_products() && nov)) ? fwd_.up_leaf : fwd_.up) g64.push_back(&g);
+    if (!folded() && !(l2l_products() && nov))
       for (auto& g : fwd_.l2l) g64.push_back(&g);
     g64.push_back(&fwd_.leaf_far);
     g32.push_back(&fwd_.x_only);
@@ -1637,8 +1736,9 @@ std::pair<double, double> Fmm::autotune_tiles(int nrhs) {
   std::vector<TaskGroup*> groups;
   const bool nov = tensor_m2l_ || fft_m2l_;
   const bool fo = folded() && nov;
-  for (auto& g : fo ? fwd_.up_leaf : fwd_.up) groups.push_back(&g);
-  for (auto& g : (fo ? fwd_.down_x : nov ? fwd_.down_nov : fwd_.down)) groups.push_back(&g);
+  const bool mo = m2m_products() && nov, lo = l2l_products() && nov;  // the groups the matvec runs
+  for (auto& g : (fo || mo) ? fwd_.up_leaf : fwd_.up) groups.push_back(&g);
+  for (auto& g : ((fo || lo) ? fwd_.down_x : nov ? fwd_.down_nov : fwd_.down)) groups.push_back(&g);
   groups.push_back(&fwd_.leaf);
   std::pair<double, double> res;
   auto go = [&](auto tag) {

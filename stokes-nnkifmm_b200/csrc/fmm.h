@@ -204,6 +204,13 @@ class Fmm {
   // FP64 work arrays (FP64 and NEAR32 modes); NEAR32 adds FP32 copies of the
   // points and forces for its near-field pair sums
   bool f64() const { return p_.precision != NNK_PREC_MIXED; }
+  // M2M and L2L (2, the default where the tree allows it), or M2M alone
+  // (1), in the matvec as products with their kernel matrices, or both as
+  // pair sums (0); the form in use.
+  void set_m2m_form(int form);
+  int m2m_form() const { return m2m_products() ? m2m_on_ : 0; }
+  // target-source pairs of each of M2M and L2L (non-leaf nodes x 8 P^2)
+  int64_t m2m_pairs() const { return fpar_off_.empty() ? 0 : fpar_off_.back() * 8 * (int64_t)P_ * P_; }
   // Folded M2M / L2L in the matvec (regularized operators only): 0 off (the
   // default), 1 where it pays, 2 wherever available; whether the matvec
   // uses it.
@@ -341,8 +348,33 @@ class Fmm {
   DBuf<int32_t> fpar_, fch_;  // non-leaf nodes by level, and their first children
   std::vector<int64_t> fpar_off_;
   DBuf<C2ETile> fup_tiles_, fdn_tiles_;
+  std::vector<C2ETile> fup_tiles_host_, fdn_tiles_host_;
   std::vector<int64_t> fup_toff_, fdn_toff_;
   void build_fold_lists();
+  // M2M and L2L as products with their kernel matrices, not folded: per
+  // operator (box width w) [M2M_0 .. M2M_7] (3P x 8 * 3P) from the 8
+  // children's up-equivalent densities to the parent's up check, and
+  // [L2L_0; ..; L2L_7] (8 * 3P x 3P) from the parent's down-equivalent
+  // density to the 8 children's down checks, each one library DGEMM per
+  // level on gathered densities.  The check potentials are the pair sums'
+  // to FP64 rounding, so the exact inverses allow it (unlike folding).
+  DBuf<double> m2m_ops_, l2l_ops_;
+  bool m2m_ok_ = false;  // the operators are built
+  int m2m_on_ = 2;       // the caller's choice (set_m2m_form): 2 M2M and L2L, 1 M2M
+  void build_m2m_operators();
+  // kernel matrices M2M_k (dM: k-th 3P x 3P block at k (3P)^2) and L2L_k (dL)
+  // of operator o, on the device
+  void kernel_blocks(int o, const double* surf, double* dM, double* dL);
+  std::vector<double> fold_surfaces() const;
+  bool m2m_products() const { return m2m_ok_ && m2m_on_ > 0 && t_->groups() == 1; }
+  bool l2l_products() const { return m2m_products() && m2m_on_ == 2; }
+  // dst(out node) [+]= op * src(in node) over runs of tiles sharing an
+  // operator (op: M x Kd column-major, op_stride apart): gather, one cuBLAS
+  // DGEMM per run, scatter
+  template <typename Real>
+  void node_gemm_blas(const double* ops, size_t op_stride, int M, int Kd, int trans, const C2ETile* tiles_host,
+                      int ntiles, const int32_t* out_nodes, const int32_t* in_nodes, const Real* src, Real* dst,
+                      int64_t base, int R, int accumulate, float* m2l_dst, int NP);
   void build_fold_operators(bool force);
   DBuf<double> c2e_part_;   // K-split partial sums of the small C2E launches
   std::vector<int64_t> dn_toff_;

@@ -860,31 +860,31 @@ inline void launch_node_gemm(NodeGemm g, int ntiles, const Real* src, Real* dst,
   }
 }
 
-// The library-GEMM form of the check-to-equivalent step: columns j of a run
-// of `ncol` = nodes x R columns (node nodes[first + j / R], right-hand side
-// j % R) gathered as FP64 into X (3P x ncol, column-major) ...
+// The library-GEMM form of a node product (NodeGemm): columns j of a run of
+// `ncol` = nodes x R columns (node nodes[first + j / R], right-hand side
+// j % R) gathered as FP64 into X (rows x ncol, column-major; row m is point
+// m / 3 from the node on, so rows = 8 x 3P spans a first child's 8
+// consecutive siblings) ...
 template <typename Real>
 __global__ void c2e_gather_kernel(const Real* __restrict__ check, const int32_t* __restrict__ nodes, int first,
-                                  int ncol, int R, int P, double* __restrict__ X) {
-  const int n3 = 3 * P;
-  const long long total = (long long)ncol * n3;
+                                  int ncol, int R, int P, int rows, double* __restrict__ X) {
+  const long long total = (long long)ncol * rows;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
-    const int j = (int)(e / n3), m = (int)(e - (long long)j * n3);
+    const int j = (int)(e / rows), m = (int)(e - (long long)j * rows);
     const int node = nodes[first + j / R], r = j - (j / R) * R;
     X[e] = (double)check[(((size_t)node * P + m / 3) * R + r) * 3 + m % 3];
   }
 }
-// ... and the products Y (3P x ncol) written like c2e_kernel's epilogue.
+// ... and the products Y (rows x ncol) written like c2e_kernel's epilogue.
 template <typename Real>
 __global__ void c2e_scatter_kernel(const double* __restrict__ Y, const int32_t* __restrict__ nodes, int first,
-                                   int ncol, int R, int P, long long base, int accumulate, Real* __restrict__ dst,
-                                   float* __restrict__ m2l_dst, int NP) {
-  const int n3 = 3 * P;
-  const long long total = (long long)ncol * n3;
+                                   int ncol, int R, int P, int rows, long long base, int accumulate,
+                                   Real* __restrict__ dst, float* __restrict__ m2l_dst, int NP) {
+  const long long total = (long long)ncol * rows;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
-    const int j = (int)(e / n3), m = (int)(e - (long long)j * n3);
+    const int j = (int)(e / rows), m = (int)(e - (long long)j * rows);
     const int node = nodes[first + j / R], r = j - (j / R) * R;
     Real* o = dst + ((base + (long long)P * node + m / 3) * R + r) * 3 + m % 3;
     const double y = Y[e];

@@ -53,7 +53,8 @@ class FmmStats(C.Structure):
     _fields_ = [("pairs_leaf", _i64), ("pairs_p2p", _i64), ("pairs_up", _i64), ("pairs_down", _i64),
                 ("m2l_pairs", _i64), ("c2e_columns", _i64), ("m2l_tile_rows", _i64), ("surface_points", _i32),
                 ("levels", _i32), ("m2l_rank", _i32), ("folded", _i32), ("m2l_frequencies", _i32),
-                ("m2l_family", _i32), ("m2l_records", _i64), ("m2l_groups", _i64)]
+                ("m2l_family", _i32), ("m2l_records", _i64), ("m2l_groups", _i64), ("m2m_product_pairs", _i64),
+                ("l2l_product_pairs", _i64)]
 
 
 class SolveParams(C.Structure):
@@ -90,6 +91,7 @@ SIGNATURES = {
     "nnk_fmm_stats_get": (_i32, [_vp, C.POINTER(FmmStats)]),
     "nnk_fmm_set_fold": (_i32, [_vp, _i32]),
     "nnk_fmm_set_c2e": (_i32, [_vp, _i32]),
+    "nnk_fmm_set_m2m_form": (_i32, [_vp, _i32]),
     "nnk_measure_l2_read": (_i32, [_vp, C.POINTER(_f64)]),
     "nnk_fmm_c2e_mode": (_i32, [_vp, C.POINTER(_i32)]),
     "nnk_fmm_setup_times": (_i32, [_vp, C.POINTER(C.c_double), _i32]),

@@ -115,6 +115,13 @@ class KIFMM:
         stats()["folded"] says whether the matvec folds."""
         L.check(L.lib.nnk_fmm_set_fold(self.h, int(mode)), self.ctx.h, "setFold")
 
+    def setM2MForm(self, form=2):
+        """M2M and L2L as products with their kernel matrices (2, the default
+        where the tree allows it), M2M alone (1), or both as pair sums (0);
+        stats()["m2m_product_pairs"] and ["l2l_product_pairs"] count what the
+        products take over."""
+        L.check(L.lib.nnk_fmm_set_m2m_form(self.h, int(form)), self.ctx.h, "setM2MForm")
+
     def setC2E(self, mode=1):
         """Check-to-equivalent products as one cuBLAS DGEMM per run of nodes
         sharing an operator (2, the default; forests and graph-captured

@@ -277,6 +277,40 @@ def test_library_dgemm_c2e_matches_simt(name, precision):
         assert rel(a, g["vel"]) <= FP64_TOL[name]
 
 
+@pytest.mark.parametrize("precision", ["fp64", "near32", "mixed"])
+@pytest.mark.parametrize("name", ["sphere10_40", "adaptive_nearest_1200", "split_1500_700", "matvec_4000_16000"])
+def test_m2m_l2l_products_match_pair_sums(name, precision):
+    """M2M and L2L as products with their kernel matrices (form 2, the
+    default; form 1 for M2M alone) against the pair sums: the same check potentials to FP64 rounding,
+    lifted by the check-to-equivalent inverses (the C2E forms' bound holds);
+    FP64 mode still matches the oracle.  The statistics count the pairs the
+    products take over (non-leaf nodes x 8 P^2 for each of M2M and L2L)."""
+    g = load(name)
+    t = tree_of(g)
+    fmm = nk.KIFMM(t, [float(g["eps"]), float(g["mu"])], precision=precision)
+    st = fmm.stats()
+    a = fmm.computeVel(g["F"])  # the default, form 2: M2M and L2L products
+    fmm.setM2MForm(1)  # M2M products, L2L pairs
+    c = fmm.computeVel(g["F"])
+    st1 = fmm.stats()
+    fmm.setM2MForm(0)
+    assert fmm.stats()["m2m_product_pairs"] == 0 and fmm.stats()["l2l_product_pairs"] == 0
+    b = fmm.computeVel(g["F"])
+    fmm.setM2MForm(2)
+    assert np.array_equal(a, fmm.computeVel(g["F"]))
+    par = np.asarray(t.nodeParents).ravel()
+    lev = np.asarray(t.nodeLevel).ravel()
+    # non-leaf nodes below the root (1-based parent ids, 0 = none); the root has no M2M of its own
+    nonleaf = len({int(p) - 1 for p in par if p > 0 and lev[int(p) - 1] >= 1})
+    pairs = nonleaf * 8 * st["surface_points"] ** 2
+    assert st["m2m_product_pairs"] == pairs and st["l2l_product_pairs"] == pairs
+    assert st1["m2m_product_pairs"] == pairs and st1["l2l_product_pairs"] == 0
+    print(name, precision, "M2M/L2L products vs pair sums", rel(a, b), rel(c, b))
+    assert rel(a, b) <= C2E_TC_TOL[precision] and rel(c, b) <= C2E_TC_TOL[precision]
+    if precision == "fp64":
+        assert rel(a, g["vel"]) <= FP64_TOL[name] and rel(c, g["vel"]) <= FP64_TOL[name]
+
+
 @pytest.mark.parametrize("name", sorted(FP64_TOL))
 def test_fourier_m2l_matches_pair_m2l(name):
     """The Fourier-space M2L (FP32 spectra) gives the FP32 pair-kernel M2L
